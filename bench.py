@@ -1,0 +1,431 @@
+#!/usr/bin/env python
+"""Throughput of the self-gravity Poisson solve on B200.
+
+Workload (one "step" = one solve): the time-step call of bipoly_hydro's
+potential_solver on the 130x98x256 grid (dr = dz = 1/126, isym 2, mmax 30):
+a bipolytropic binary (R1 0.3, R2 0.22, separation 0.9, mass ratio 0.5, core
+density x2 inside 0.4 R) rigidly rotated by one azimuthal zone per solve,
+each solve warm-started from the previous potential (5 ADI steps).  Every
+solve streams the 660 MB of FP64 Green tables, so the per-step working set is
+larger than the 126 MB L2.
+
+  value      solves/s with rho resident in HBM (device-array C ABI call)
+  e2e        solves/s through the host-array C ABI call: pinned rho copied in
+             and pot copied out inside every step
+  roofline   k_green_contract (the dominant kernel) against measured HBM
+  cpu_baseline  the CPU oracle (C restatement of the reference algorithm)
+             on this host
+
+--impl reference times that CPU restatement as the reference arm (the
+Fortran reference cannot be compiled on these machines).
+
+Multi-GPU (torchrun): every rank runs its own independent solve sequence
+(weak scaling, no collective on the data path); timing is max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GRID = dict(numr=130, numz=98, numphi=256, dr=1.0 / 126.0, isym=2, mmax=30)
+METRIC = "Poisson solves/s at 130x98x256 (FP64 drop-in, warm 5-step time-step solve)"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def compulsory_bytes(numr, numz, numphi, mmax, isym, warm=True, G=1):
+    """B_alg per solve: read rho, read warm Phi, write Phi, stream the tables once."""
+    n = numr * numz * numphi
+    nr, nz = numr - 2, numz - 2
+    rows = nr + nz + (nr if isym == 1 else 0)
+    return 8 * n * (1 + (1 if warm else 0) + 1) + 8 * nr * nz * rows * mmax / G
+
+
+def contract_bytes(numr, numz, mmax, isym):
+    """Algorithmic bytes of one k_green_contract launch: tables + moment vectors + S."""
+    nr, nz = numr - 2, numz - 2
+    rows = nr + nz + (nr if isym == 1 else 0)
+    return 8 * (nr * nz * rows * mmax + 2 * mmax * nr * nz + 2 * mmax * rows)
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def committed_traffic():
+    """dram bytes per launch of k_green_contract from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "green_contract_130x98x256.md")
+    try:
+        text = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", text)
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples of one GPU while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        import tempfile
+
+        fd, self.path = tempfile.mkstemp(prefix="bph_clocks_", suffix=".csv")
+        os.close(fd)
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "50"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.1)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), float(parts[2]), parts[3:]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        smax = max(r[1] for r in rows)
+        loaded = [r for r in rows if r[2] > 200.0] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in loaded:
+            for name, flag in zip(names, r[3][1:]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(loaded)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def cpu_oracle_rate(rho_seq, seconds: float, threads: int | None, max_solves: int):
+    """Warm solves/s of the CPU oracle on this host over a bounded sample."""
+    from oracle import oracle as O
+
+    O.build()
+    if threads:
+        O.set_num_threads(threads)
+    o = O.Oracle(GRID["numr"], GRID["numz"], GRID["numphi"], GRID["dr"], GRID["isym"], GRID["mmax"])
+    o.potential_solver(rho_seq(0), 0)  # cold start, untimed
+    o.potential_solver(rho_seq(1), 2)  # one warm solve, untimed
+    n, t0 = 0, time.perf_counter()
+    while True:
+        o.potential_solver(rho_seq(2 + n), 3 + n)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= max_solves:
+            break
+    o.close()
+    return n / el, n, el, O.num_threads()
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the CPU restatement on this host's cores, rank 0 only."""
+    if rank != 0:
+        return
+    from bipoly_hydro_b200 import fields
+
+    base = fields.bipolytrope_pair(GRID["numr"], GRID["numz"], GRID["numphi"], GRID["dr"], GRID["isym"])
+    cores = os.cpu_count() or 1
+    from oracle import oracle as O
+
+    O.build()
+    O.set_num_threads(cores)
+    o = O.Oracle(GRID["numr"], GRID["numz"], GRID["numphi"], GRID["dr"], GRID["isym"], GRID["mmax"])
+    o.potential_solver(base, 0)
+    for w in range(args.warmup):
+        o.potential_solver(fields.rotate(base, 1 + w), 2 + w)
+    times = []
+    t_all = time.perf_counter()
+    for i in range(args.steps):
+        rho = fields.rotate(base, 1 + args.warmup + i)
+        t0 = time.perf_counter()
+        o.potential_solver(rho, 2 + args.warmup + i)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_all > args.reference_budget_s:
+            break
+    o.close()
+    n = len(times)
+    total = sum(times)
+    v = n / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": n, "warmup": args.warmup, "ms_per_step": 1e3 * total / n, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "130x98x256 warm time-step solves, bipolytrope pair rotated 1 zone/solve",
+                   **GRID, "nsteps_adi": 5},
+        "p50_ms": 1e3 * float(np.percentile(times, 50)), "p99_ms": 1e3 * float(np.percentile(times, 99)),
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+                         "sample": f"{n} warm solves of the sequence (steps requested {args.steps}), "
+                                   f"C restatement of potential_solver with OpenMP over slots/rows"},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference Fortran+MPI cannot be compiled here (no Fortran compiler or MPI); "
+                "the arm runs the C restatement of its algorithm",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args, world, rank, local):
+    import torch
+
+    import bipoly_hydro_b200 as B
+    from bipoly_hydro_b200 import fields
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    numr, numz, numphi = GRID["numr"], GRID["numz"], GRID["numphi"]
+    ntot = numr * numz * numphi
+    solver = B.PotentialSolver(**GRID)
+    stream = torch.cuda.current_stream()
+    solver.set_stream(stream)
+
+    # Density sequence: rank-dependent seed/phase, all numphi rotations resident.
+    base = fields.bipolytrope_pair(numr, numz, numphi, GRID["dr"], GRID["isym"], mass_ratio=0.5)
+    base_t = torch.from_numpy(np.ascontiguousarray(base.ravel(order="F"))).to(dev)
+    c_view = base_t.view(numphi, numz, numr)  # C view of the Fortran (numr, numz, numphi) array
+    nrot = numphi
+    rhos = torch.empty((nrot, ntot), dtype=torch.float64, device=dev)
+    for i in range(nrot):
+        rhos[i].copy_(torch.roll(c_view, shifts=i + rank, dims=0).reshape(-1))
+    d_pot = torch.empty(ntot, dtype=torch.float64, device=dev)
+
+    # cold start, then warm-up solves
+    solver.potential_solver_device(rhos[0], d_pot, 0)
+    tstep = 2
+    for w in range(args.warmup):
+        solver.potential_solver_device(rhos[(1 + w) % nrot], d_pot, tstep)
+        tstep += 1
+    solver.synchronize()
+
+    # ---- value: device-resident inputs --------------------------------
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+        if not uuid.startswith("GPU-"):
+            uuid = "GPU-" + uuid
+    except Exception:
+        uuid = None
+    l0 = solver.launch_count
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(uuid) as clk:
+        e0.record(stream)
+        for i in range(args.steps):
+            solver.potential_solver_device(rhos[(1 + args.warmup + i) % nrot], d_pot, tstep)
+            tstep += 1
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    launches = solver.launch_count - l0
+    solver.synchronize()
+    ms_total = max_over_ranks(e0.elapsed_time(e1), world)
+    ms_per_step = ms_total / args.steps
+    value = world * args.steps / (ms_total / 1e3)
+    clocks = clk.summary()
+
+    # ---- per-phase kernel times (CUDA events on the launch stream) ------
+    def time_phase(phase, reps, **kw):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(3):
+            solver.run_phase(phase, **kw)
+        a.record(stream)
+        for _ in range(reps):
+            solver.run_phase(phase, **kw)
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    phases = {
+        "fft_fwd_rho": time_phase(B.solver.PHASE_FFT_RHO, 50, d_rho=rhos[0]),
+        "green_contract": time_phase(B.solver.PHASE_CONTRACT, 50),
+        "boundary_slots": time_phase(B.solver.PHASE_SLOTS, 50),
+        "adi_5steps": time_phase(B.solver.PHASE_ADI, 50, nsteps=5),
+        "fft_inv": time_phase(B.solver.PHASE_FFT_INV, 50, d_pot=d_pot),
+    }
+    solver.synchronize()
+    peak, peak_kind = hbm_peak()
+    cb = contract_bytes(numr, numz, GRID["mmax"], GRID["isym"])
+    achieved = cb / (phases["green_contract"] / 1e3) / 1e9
+    traffic = committed_traffic()
+    b_alg = compulsory_bytes(numr, numz, numphi, GRID["mmax"], GRID["isym"], warm=True)
+    solve_gbs = b_alg / (ms_per_step / 1e3) / 1e9
+
+    # ---- e2e: host-array C ABI call with pinned buffers ----------------
+    n_e2e = min(args.steps, args.e2e_steps)
+    npin = min(nrot, n_e2e)
+    h_rho = [torch.empty(ntot, dtype=torch.float64, pin_memory=True) for _ in range(npin)]
+    for i in range(npin):
+        h_rho[i].copy_(rhos[(1 + i) % nrot])
+    h_pot = torch.empty(ntot, dtype=torch.float64, pin_memory=True)
+    rho_np = [t.numpy() for t in h_rho]
+    pot_np = h_pot.numpy()
+    lib = B.load_library()
+    import ctypes
+
+    for i in range(3):
+        rc = lib.bph_potential_solver(solver._h, ctypes.c_void_p(rho_np[i % npin].ctypes.data),
+                                      ctypes.c_void_p(pot_np.ctypes.data), tstep)
+        tstep += 1
+        assert rc == 0, lib.bph_last_error()
+    barrier(world)
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lat = []
+    e2.record(stream)
+    for i in range(n_e2e):
+        t0 = time.perf_counter()
+        rc = lib.bph_potential_solver(solver._h, ctypes.c_void_p(rho_np[i % npin].ctypes.data),
+                                      ctypes.c_void_p(pot_np.ctypes.data), tstep)
+        lat.append(time.perf_counter() - t0)
+        tstep += 1
+        if rc != 0:
+            raise RuntimeError(lib.bph_last_error().decode())
+    e3.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms_e2e = max_over_ranks(e2.elapsed_time(e3), world)
+    e2e_value = world * n_e2e / (ms_e2e / 1e3)
+
+    # ---- CPU baseline (rank 0, N = 1 only) ------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        def rho_seq(i):
+            return fields.rotate(base, i)
+
+        rate, n, el, cores = cpu_oracle_rate(rho_seq, args.cpu_seconds, os.cpu_count(), 200)
+        cpu = {"value": rate, "unit": "solves/s", "cores": cores, "kind": "port",
+               "sample": f"{n} warm solves of the same sequence in {el:.1f} s after an untimed setup "
+                         f"(C restatement of potential_solver, OpenMP)"}
+
+    solver.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "130x98x256 warm time-step solves, bipolytrope pair rotated 1 zone/solve",
+                       **GRID, "nsteps_adi": 5, "parallelism": f"independent sequence per GPU x{world}",
+                       "l2": "per-solve working set (660 MB Green tables) > 126 MB L2"},
+            "zone_updates_per_s": value * ntot * 5,
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 8 * ntot,
+                    "d2h_bytes_per_step": 8 * ntot,
+                    "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99))},
+            "roofline": {"bound": "hbm", "kernel": "k_green_contract", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": traffic, "alg_bytes_per_launch": cb,
+                         "solve_alg_bytes": b_alg, "solve_gbs": solve_gbs, "solve_frac": solve_gbs / peak},
+            "phase_ms": phases,
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=500)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-budget-s", type=float, default=150.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        # The CPU reference arm uses no GPU and no collective: rank 0 runs it.
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
+    world, rank, local = dist_setup()
+    try:
+        run_gpu(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,606 @@
+// bph_api.cu -- the C ABI (include/bph.h): context setup (potsetup.F90),
+// the solve driver (potential_solver.F90) and its host/device entry points.
+//
+// One solve is five kernels on the context's stream:
+//   k_fft_fwd<rho>     rho -> R = -4 pi rho_hat (slot-major) + moments
+//   k_green_contract   moments x Green tables -> S
+//   k_boundary_slots   S -> Dirichlet slots of P (top, side, bottom)
+//   k_adi              nsteps ADI steps per slot on P
+//   k_fft_inv          P -> pot, with the axis and equator conditions
+// A warm start reuses the Fourier-space potential P of the previous solve,
+// which is what the reference's forward transform of its kept potp gives
+// (helmadi.F90:159) up to rounding, so no forward transform of the old
+// potential is needed.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "bph_internal.cuh"
+
+namespace bph {
+
+static thread_local char g_err[512];
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    set_error("CUDA error in %s: %s (%d)", what, cudaGetErrorString(e), (int)e);
+    return (e == cudaErrorMemoryAllocation) ? BPH_ERR_NOMEM : BPH_ERR_CUDA;
+}
+
+namespace {
+
+bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+template <typename T>
+int dev_alloc(bph_ctx *c, T **p, size_t count) {
+    size_t bytes = sizeof(T) * (count ? count : 1);
+    cudaError_t e = cudaMalloc((void **)p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        set_error("device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+        return BPH_ERR_NOMEM;
+    }
+    c->bytes += bytes;
+    return BPH_OK;
+}
+
+void dev_free(void *p) {
+    if (p) cudaFree(p);
+}
+
+// Grid coordinates (setup_frac.F90:374-463, one rank) and the ADI
+// coefficient arrays (potsetup.F90:151-252), evaluated on the host in the
+// reference's expression order: they are O(numr*numphi) setup constants.
+struct HostCoef {
+    std::vector<double> r_g, rhf_g, rinv_g, rhfinv_g, zhf_g;
+    std::vector<double> alphar, betar, brb, elz, bzb;
+};
+
+void host_coefficients(bph_ctx *c, HostCoef &h) {
+    const bph_grid_t &g = c->g;
+    const int numr = g.numr, numz = g.numz, N = g.numphi;
+    h.r_g.assign(numr, 0.0);
+    h.rhf_g.assign(numr, 0.0);
+    h.rinv_g.assign(numr, 0.0);
+    h.rhfinv_g.assign(numr, 0.0);
+    h.zhf_g.assign(numz, 0.0);
+    double x = 1.0;
+    for (int J = 1; J <= numr; ++J) {
+        h.r_g[J - 1] = (x - 2.0) * g.dr;
+        x = x + 1.0;
+    }
+    for (int J = 1; J <= numr; ++J) {
+        h.rhf_g[J - 1] = h.r_g[J - 1] + 0.5 * g.dr;
+        h.rinv_g[J - 1] = (h.r_g[J - 1] != 0.0) ? 1.0 / h.r_g[J - 1] : 0.0;
+        h.rhfinv_g[J - 1] = 1.0 / h.rhf_g[J - 1];
+    }
+    x = 1.0;
+    double offset = (g.isym != 1) ? 0.0 : -(double)(numz / 2) * c->dz;
+    for (int K = 1; K <= numz; ++K) {
+        h.zhf_g[K - 1] = (g.isym != 1) ? (x - 1.5) * c->dz : offset + (x - 0.5) * c->dz;
+        x = x + 1.0;
+    }
+    const double drinv2 = c->drinv * c->drinv, dphiinv2 = c->dphiinv * c->dphiinv;
+    h.alphar.assign(numr, 0.0);
+    h.betar.assign(numr, 0.0);
+    for (int J = 2; J <= numr - 1; ++J) {
+        h.alphar[J - 1] = -h.r_g[J] * h.rhfinv_g[J - 1] * drinv2;
+        h.betar[J - 1] = -h.r_g[J - 1] * h.rhfinv_g[J - 1] * drinv2;
+    }
+    h.brb.assign((size_t)N * numr, 0.0);
+    h.elz.assign((size_t)N * numr, 0.0);
+    const int lstop = N / 2 + 1;
+    for (int L = 1; L <= N; ++L) {
+        int mode;
+        if (g.isym == 3)
+            mode = (L <= lstop) ? (L - 1) * (L - 1) : (L - lstop) * (L - lstop);
+        else
+            mode = (L <= lstop) ? L - 1 : L - lstop;
+        double m1mode = (mode % 2 == 0) ? 1.0 : -1.0;
+        double em1 = std::cos((double)mode * c->dphi) - 1.0;
+        double *brb = h.brb.data() + (size_t)(L - 1) * numr;
+        double *elz = h.elz.data() + (size_t)(L - 1) * numr;
+        for (int J = 3; J <= numr - 1; ++J)
+            brb[J - 1] = 2.0 * drinv2 - 2.0 * em1 * dphiinv2 * h.rhfinv_g[J - 1] * h.rhfinv_g[J - 1];
+        double az2 = 2.0 * em1 * dphiinv2 * h.rhfinv_g[1] * h.rhfinv_g[1];
+        if (g.isym == 3)
+            brb[1] = -h.alphar[1] - 2.0 * h.betar[1] - az2;
+        else
+            brb[1] = -h.alphar[1] + (m1mode - 1.0) * h.betar[1] - az2;
+        for (int J = 2; J <= numr - 1; ++J)
+            elz[J - 1] = -2.0 * drinv2 + 2.0 * em1 * dphiinv2 * h.rhfinv_g[J - 1] * h.rhfinv_g[J - 1];
+        if (g.isym == 3)
+            elz[1] = h.alphar[1] + 2.0 * h.betar[1] + az2;
+        else
+            elz[1] = h.alphar[1] - (m1mode - 1.0) * h.betar[1] + az2;
+    }
+    h.bzb.assign(numz, 0.0);
+    for (int K = 2; K <= numz - 1; ++K) h.bzb[K - 1] = 2.0 * c->gamma;
+    if (g.isym != 1) h.bzb[1] = c->gamma;
+}
+
+// dt schedule of helmadi.F90:124-129.
+void dt_schedule(const HostCoef &h, int numr, int nsteps, double *dt) {
+    dt[nsteps - 1] = 4.0 * (h.rinv_g[numr - 1] * h.rinv_g[numr - 1]);
+    double alph = std::pow(h.r_g[numr - 1] * h.rinv_g[2], 2.0 / ((double)nsteps - 1.0));
+    for (int I = 2; I <= nsteps; ++I) {
+        int idx = nsteps + 1 - I;
+        dt[idx - 1] = alph * dt[idx];
+    }
+}
+
+void free_schedule(bph_ctx *c, Schedule &s) {
+    dev_free(s.d_dt);
+    dev_free(s.d_rad);
+    dev_free(s.d_ver);
+    free(s.h_dt);
+    s = Schedule();
+    (void)c;
+}
+
+// Builds (or returns the cached) schedule for nsteps ADI steps.
+int get_schedule(bph_ctx *c, int nsteps, Schedule **out) {
+    for (auto &s : c->sched)
+        if (s.nsteps == nsteps) {
+            *out = &s;
+            return BPH_OK;
+        }
+    Schedule &s = (nsteps == 5) ? c->sched[0] : (nsteps == 20) ? c->sched[1] : c->sched[2];
+    if (s.nsteps) free_schedule(c, s);
+    HostCoef h;
+    host_coefficients(c, h);
+    s.h_dt = (double *)malloc(sizeof(double) * nsteps);
+    dt_schedule(h, c->g.numr, nsteps, s.h_dt);
+    int rc;
+    if ((rc = dev_alloc(c, &s.d_dt, nsteps))) return rc;
+    if ((rc = dev_alloc(c, &s.d_rad, (size_t)nsteps * c->N * 3 * c->nr))) return rc;
+    if ((rc = dev_alloc(c, &s.d_ver, (size_t)nsteps * 3 * c->nz))) return rc;
+    BPH_CUDA(cudaMemcpyAsync(s.d_dt, s.h_dt, sizeof(double) * nsteps, cudaMemcpyHostToDevice, c->stream));
+    s.nsteps = nsteps;
+    BPH_CUDA(launch_adi_factors(c, s));
+    BPH_CUDA(cudaStreamSynchronize(c->stream));
+    *out = &s;
+    return BPH_OK;
+}
+
+int validate(const bph_grid_t *g) {
+    if (!g) {
+        set_error("grid is NULL");
+        return BPH_ERR_INVALID;
+    }
+    if (g->numr < 5 || g->numz < 5) {
+        set_error("numr and numz must be >= 5 (got %d, %d)", g->numr, g->numz);
+        return BPH_ERR_INVALID;
+    }
+    if (!is_pow2(g->numphi) || g->numphi < 16 || g->numphi > 512) {
+        set_error("numphi must be a power of two in [16, 512] (got %d)", g->numphi);
+        return BPH_ERR_INVALID;
+    }
+    if (g->isym < 1 || g->isym > 3) {
+        set_error("isym must be 1, 2 or 3 (got %d)", g->isym);
+        return BPH_ERR_INVALID;
+    }
+    if (g->mmax < 2 || g->mmax > kMaxMmax) {
+        set_error("mmax must be in [2, %d] (got %d)", kMaxMmax, g->mmax);
+        return BPH_ERR_INVALID;
+    }
+    int fm = (g->isym == 3) ? 2 : 1;
+    if (fm * (g->mmax - 1) >= g->numphi / 2) {
+        set_error("numphi=%d too small for mmax=%d (need numphi/2 > %d*(mmax-1))", g->numphi, g->mmax, fm);
+        return BPH_ERR_INVALID;
+    }
+    if (!(g->dr > 0.0) || !std::isfinite(g->dr)) {
+        set_error("dr must be positive and finite");
+        return BPH_ERR_INVALID;
+    }
+    return BPH_OK;
+}
+
+int upload(bph_ctx *c, void *dst, const void *src, size_t bytes) {
+    BPH_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    return BPH_OK;
+}
+
+int setup_impl(bph_ctx *c) {
+    const bph_grid_t &g = c->g;
+    int rc;
+    BPH_CUDA(cudaGetDevice(&c->device));
+    BPH_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
+    c->nr = g.numr - 2;
+    c->nz = g.numz - 2;
+    c->nb = (g.isym == 1) ? 2 * c->nr + c->nz : c->nr + c->nz;
+    c->N = g.numphi;
+    c->M = g.numphi / 2;
+    c->fm = (g.isym == 3) ? 2 : 1;
+    c->np = (long long)c->nr * c->nz;
+    c->nplane = (long long)g.numr * g.numz;
+    c->ntot = c->nplane * g.numphi;
+    c->pi = std::acos(-1.0);
+    c->dz = g.dr;
+    c->dphi = 2.0 * c->pi * (1.0 / (double)g.numphi);
+    c->drinv = 1.0 / g.dr;
+    c->dzinv = 1.0 / c->dz;
+    c->dphiinv = 1.0 / c->dphi;
+    c->gamma = c->dzinv * c->dzinv;
+    c->four_pi = 4.0 * c->pi;
+    c->factor = (g.isym == 3) ? -(2.0 * g.dr * c->dz * c->dphi) : -(g.dr * c->dz * c->dphi);
+
+    // Admission: refuse a context that cannot fit in free device memory.
+    size_t need = sizeof(double) * ((size_t)g.mmax * c->nb * c->np + (size_t)c->N * c->np +
+                                    (size_t)c->N * c->nplane + 2ull * g.mmax * c->np);
+    size_t free_b = 0, total_b = 0;
+    BPH_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    if (need + (64ull << 20) > free_b) {
+        set_error("context needs %zu bytes of device memory, %zu free", need, free_b);
+        return BPH_ERR_NOMEM;
+    }
+
+    HostCoef h;
+    host_coefficients(c, h);
+    std::vector<double> grid;
+    grid.insert(grid.end(), h.rhf_g.begin(), h.rhf_g.end());
+    grid.insert(grid.end(), h.rhfinv_g.begin(), h.rhfinv_g.end());
+    grid.insert(grid.end(), h.zhf_g.begin(), h.zhf_g.end());
+    // Twiddles, in long double then rounded: exact angles 2 pi k / M etc.
+    const long double pil = std::acos(-1.0L);
+    std::vector<double2> tw(c->M), tw2(c->M + 1), ph(g.mmax);
+    for (int k = 0; k < c->M; ++k) {
+        long double a = 2.0L * pil * (long double)k / (long double)c->M;
+        tw[k] = make_double2((double)std::cos(a), (double)std::sin(a));
+    }
+    for (int k = 0; k <= c->M; ++k) {
+        long double a = 2.0L * pil * (long double)k / (long double)c->N;
+        tw2[k] = make_double2((double)std::cos(a), (double)std::sin(a));
+    }
+    for (int m = 0; m < g.mmax; ++m) {
+        long double a = pil * (long double)(c->fm * m) / (long double)c->N;
+        ph[m] = make_double2((double)std::cos(a), (double)std::sin(a));
+    }
+
+    if ((rc = dev_alloc(c, &c->d_green, (size_t)g.mmax * c->nb * c->np))) return rc;
+    if ((rc = dev_alloc(c, &c->d_R, (size_t)c->N * c->np))) return rc;
+    if ((rc = dev_alloc(c, &c->d_P, (size_t)c->N * c->nplane))) return rc;
+    if ((rc = dev_alloc(c, &c->d_mom, (size_t)2 * g.mmax * c->np))) return rc;
+    if ((rc = dev_alloc(c, &c->d_S, (size_t)2 * g.mmax * c->nb))) return rc;
+    if ((rc = dev_alloc(c, &c->d_brb, (size_t)c->N * g.numr))) return rc;
+    if ((rc = dev_alloc(c, &c->d_elz, (size_t)c->N * g.numr))) return rc;
+    if ((rc = dev_alloc(c, &c->d_alphar, (size_t)g.numr))) return rc;
+    if ((rc = dev_alloc(c, &c->d_betar, (size_t)g.numr))) return rc;
+    if ((rc = dev_alloc(c, &c->d_bzb, (size_t)g.numz))) return rc;
+    if ((rc = dev_alloc(c, &c->d_qcoef, (size_t)g.mmax * (2 + kHyprUprBnd + 1)))) return rc;
+    if ((rc = dev_alloc(c, &c->d_grid, grid.size()))) return rc;
+    if ((rc = dev_alloc(c, &c->d_tw, (size_t)c->M))) return rc;
+    if ((rc = dev_alloc(c, &c->d_tw2, (size_t)c->M + 1))) return rc;
+    if ((rc = dev_alloc(c, &c->d_ph, (size_t)g.mmax))) return rc;
+    if ((rc = dev_alloc(c, &c->d_red, (size_t)2 * c->N))) return rc;
+    if ((rc = dev_alloc(c, &c->d_status, 1))) return rc;
+
+    if ((rc = upload(c, c->d_brb, h.brb.data(), sizeof(double) * h.brb.size()))) return rc;
+    if ((rc = upload(c, c->d_elz, h.elz.data(), sizeof(double) * h.elz.size()))) return rc;
+    if ((rc = upload(c, c->d_alphar, h.alphar.data(), sizeof(double) * h.alphar.size()))) return rc;
+    if ((rc = upload(c, c->d_betar, h.betar.data(), sizeof(double) * h.betar.size()))) return rc;
+    if ((rc = upload(c, c->d_bzb, h.bzb.data(), sizeof(double) * h.bzb.size()))) return rc;
+    if ((rc = upload(c, c->d_grid, grid.data(), sizeof(double) * grid.size()))) return rc;
+    if ((rc = upload(c, c->d_tw, tw.data(), sizeof(double2) * tw.size()))) return rc;
+    if ((rc = upload(c, c->d_tw2, tw2.data(), sizeof(double2) * tw2.size()))) return rc;
+    if ((rc = upload(c, c->d_ph, ph.data(), sizeof(double2) * ph.size()))) return rc;
+    BPH_CUDA(cudaMemsetAsync(c->d_P, 0, sizeof(double) * (size_t)c->N * c->nplane, c->stream));
+    BPH_CUDA(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+
+    BPH_CUDA(launch_qcoef(c));
+    BPH_CUDA(launch_green_tables(c));
+    if ((rc = fft_configure(c))) return rc;
+    if ((rc = adi_configure(c))) return rc;
+    if (c->adi_smem == 0) {
+        if ((rc = dev_alloc(c, &c->d_W, (size_t)c->N * c->nplane))) return rc;
+    }
+    Schedule *s;
+    if ((rc = get_schedule(c, 5, &s))) return rc;
+    if ((rc = get_schedule(c, 20, &s))) return rc;
+    BPH_CUDA(cudaStreamSynchronize(c->stream));
+    return BPH_OK;
+}
+
+// The five-kernel solve on device arrays (see the file comment).
+int solve_device(bph_ctx *c, const double *d_rho, double *d_pot, const Schedule &s, bool cold) {
+    BPH_CUDA(launch_fft_fwd_rho(c, d_rho));
+    BPH_CUDA(launch_green_contract(c));
+    BPH_CUDA(launch_boundary_slots(c));
+    BPH_CUDA(launch_adi(c, s, 0, s.nsteps, cold));
+    BPH_CUDA(launch_fft_inv(c, d_pot));
+    c->have_warm = true;
+    return BPH_OK;
+}
+
+int ensure_staging(bph_ctx *c) {
+    int rc;
+    if (!c->d_rho_stage && (rc = dev_alloc(c, &c->d_rho_stage, (size_t)c->ntot))) return rc;
+    if (!c->d_pot_stage && (rc = dev_alloc(c, &c->d_pot_stage, (size_t)c->ntot))) return rc;
+    return BPH_OK;
+}
+
+int read_status(bph_ctx *c) {
+    int st = 0;
+    BPH_CUDA(cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    BPH_CUDA(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+    BPH_CUDA(cudaStreamSynchronize(c->stream));
+    if (st & kStatusNonFinite) {
+        set_error("density contains NaN or Inf");
+        return BPH_ERR_NONFINITE;
+    }
+    return BPH_OK;
+}
+
+// Host-array wrapper: copy in, solve, copy out, wait, report.
+int solve_host(bph_ctx *c, const double *rho, double *pot, const Schedule &s, bool cold) {
+    int rc;
+    if ((rc = ensure_staging(c))) return rc;
+    const size_t bytes = sizeof(double) * (size_t)c->ntot;
+    BPH_CUDA(cudaMemcpyAsync(c->d_rho_stage, rho, bytes, cudaMemcpyHostToDevice, c->stream));
+    if ((rc = solve_device(c, c->d_rho_stage, c->d_pot_stage, s, cold))) return rc;
+    BPH_CUDA(cudaMemcpyAsync(pot, c->d_pot_stage, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return read_status(c);
+}
+
+int check_ctx(const bph_ctx *c) {
+    if (!c) {
+        set_error("context is NULL");
+        return BPH_ERR_INVALID;
+    }
+    return BPH_OK;
+}
+
+int set_device_of(bph_ctx *c) {
+    int cur = -1;
+    BPH_CUDA(cudaGetDevice(&cur));
+    if (cur != c->device) BPH_CUDA(cudaSetDevice(c->device));
+    return BPH_OK;
+}
+
+}  // namespace
+}  // namespace bph
+
+using namespace bph;
+
+extern "C" {
+
+const char *bph_last_error(void) { return g_err; }
+
+const char *bph_version(void) { return "bipoly_hydro_b200 0.1 (sm_100a)"; }
+
+int bph_setup(const bph_grid_t *grid, bph_ctx_t **ctx) {
+    g_err[0] = 0;
+    if (!ctx) {
+        set_error("ctx out-pointer is NULL");
+        return BPH_ERR_INVALID;
+    }
+    *ctx = nullptr;
+    int rc = validate(grid);
+    if (rc) return rc;
+    bph_ctx *c = new bph_ctx();
+    c->g = *grid;
+    rc = setup_impl(c);
+    if (rc) {
+        char keep[sizeof g_err];
+        memcpy(keep, g_err, sizeof keep);
+        bph_destroy(c);
+        memcpy(g_err, keep, sizeof keep);
+        return rc;
+    }
+    *ctx = c;
+    return BPH_OK;
+}
+
+int bph_destroy(bph_ctx_t *c) {
+    if (!c) return BPH_OK;
+    set_device_of(c);
+    if (c->own_stream) cudaStreamSynchronize(c->own_stream);
+    if (c->stream && c->stream != c->own_stream) cudaStreamSynchronize(c->stream);
+    for (auto &s : c->sched) free_schedule(c, s);
+    double *bufs[] = {c->d_green, c->d_brb,  c->d_elz, c->d_alphar, c->d_betar,     c->d_bzb,
+                      c->d_qcoef, c->d_grid, c->d_R,   c->d_P,      c->d_prev,      c->d_mom,
+                      c->d_S,     c->d_W,    c->d_P2,  c->d_red,    c->d_rho_stage, c->d_pot_stage};
+    for (double *p : bufs) dev_free(p);
+    dev_free(c->d_tw);
+    dev_free(c->d_tw2);
+    dev_free(c->d_ph);
+    dev_free(c->d_status);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return BPH_OK;
+}
+
+int bph_set_stream(bph_ctx_t *c, void *stream) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    c->stream = (cudaStream_t)stream;  // NULL is CUDA's default stream
+    return BPH_OK;
+}
+
+int bph_synchronize(bph_ctx_t *c) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    if ((rc = set_device_of(c))) return rc;
+    return read_status(c);
+}
+
+int bph_potential_solver(bph_ctx_t *c, const double *rho, double *pot, int tstep) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    if (!rho || !pot) {
+        set_error("rho and pot must be non-NULL");
+        return BPH_ERR_INVALID;
+    }
+    if ((rc = set_device_of(c))) return rc;
+    bool warm = tstep > 1;  // potential_solver.F90:80
+    Schedule *s;
+    if ((rc = get_schedule(c, warm ? 5 : 20, &s))) return rc;
+    return solve_host(c, rho, pot, *s, !warm);
+}
+
+int bph_potential_solver_device(bph_ctx_t *c, const double *d_rho, double *d_pot, int tstep) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    if (!d_rho || !d_pot) {
+        set_error("rho and pot must be non-NULL");
+        return BPH_ERR_INVALID;
+    }
+    if ((rc = set_device_of(c))) return rc;
+    bool warm = tstep > 1;
+    Schedule *s;
+    if ((rc = get_schedule(c, warm ? 5 : 20, &s))) return rc;
+    return solve_device(c, d_rho, d_pot, *s, !warm);
+}
+
+int bph_solve_nsteps(bph_ctx_t *c, const double *rho, double *pot, int nsteps, int cold, int on_device) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    if (!rho || !pot || nsteps < 1 || nsteps > 10000) {
+        set_error("invalid arguments (nsteps must be in [1, 10000])");
+        return BPH_ERR_INVALID;
+    }
+    if ((rc = set_device_of(c))) return rc;
+    Schedule *s;
+    if ((rc = get_schedule(c, nsteps, &s))) return rc;
+    if (on_device) return solve_device(c, rho, pot, *s, cold != 0);
+    return solve_host(c, rho, pot, *s, cold != 0);
+}
+
+int bph_solve_converged(bph_ctx_t *c, const double *rho, double *pot, int nsteps, int cold, double tol,
+                        int max_cycles, int on_device, int *cycles_out, double *resid_out) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    if (!rho || !pot || nsteps < 1 || nsteps > 10000 || max_cycles < 1 || !(tol >= 0.0)) {
+        set_error("invalid arguments");
+        return BPH_ERR_INVALID;
+    }
+    if ((rc = set_device_of(c))) return rc;
+    Schedule *s;
+    if ((rc = get_schedule(c, nsteps, &s))) return rc;
+    if (!c->d_prev && (rc = dev_alloc(c, &c->d_prev, (size_t)c->N * c->nplane))) return rc;
+    const size_t bytes = sizeof(double) * (size_t)c->ntot;
+    const double *d_rho = rho;
+    double *d_pot = pot;
+    if (!on_device) {
+        if ((rc = ensure_staging(c))) return rc;
+        BPH_CUDA(cudaMemcpyAsync(c->d_rho_stage, rho, bytes, cudaMemcpyHostToDevice, c->stream));
+        d_rho = c->d_rho_stage;
+        d_pot = c->d_pot_stage;
+    }
+    BPH_CUDA(launch_fft_fwd_rho(c, d_rho));
+    BPH_CUDA(launch_green_contract(c));
+    BPH_CUDA(launch_boundary_slots(c));
+    std::vector<double> h(2 * (size_t)c->N);
+    int cyc = 0;
+    for (;;) {
+        BPH_CUDA(cudaMemcpyAsync(c->d_prev, c->d_P, bytes, cudaMemcpyDeviceToDevice, c->stream));
+        BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, cold != 0 && cyc == 0));
+        ++cyc;
+        BPH_CUDA(launch_update_norm(c, c->d_red));
+        BPH_CUDA(cudaMemcpyAsync(h.data(), c->d_red, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+        BPH_CUDA(cudaStreamSynchronize(c->stream));
+        double num = 0.0, den = 0.0;
+        for (int i = 0; i < c->N; ++i) {
+            num += h[2 * i];
+            den += h[2 * i + 1];
+        }
+        double upd = den > 0.0 ? std::sqrt(num / den) : std::sqrt(num);
+        if (upd <= tol || cyc >= max_cycles) break;
+    }
+    if (resid_out) {
+        BPH_CUDA(launch_residual_norm(c, c->d_red));
+        BPH_CUDA(cudaMemcpyAsync(h.data(), c->d_red, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+        BPH_CUDA(cudaStreamSynchronize(c->stream));
+        double num = 0.0, den = 0.0;
+        for (int i = 0; i < c->N; ++i) {
+            num += h[2 * i];
+            den += h[2 * i + 1];
+        }
+        *resid_out = den > 0.0 ? std::sqrt(num / den) : std::sqrt(num);
+    }
+    if (cycles_out) *cycles_out = cyc;
+    BPH_CUDA(launch_fft_inv(c, d_pot));
+    c->have_warm = true;
+    if (!on_device) BPH_CUDA(cudaMemcpyAsync(pot, d_pot, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return read_status(c);
+}
+
+int bph_run_phase(bph_ctx_t *c, int phase, const double *d_rho, double *d_pot, int nsteps) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    if ((rc = set_device_of(c))) return rc;
+    switch (phase) {
+        case BPH_PHASE_FFT_RHO:
+            if (!d_rho) break;
+            BPH_CUDA(launch_fft_fwd_rho(c, d_rho));
+            return BPH_OK;
+        case BPH_PHASE_CONTRACT:
+            BPH_CUDA(launch_green_contract(c));
+            return BPH_OK;
+        case BPH_PHASE_SLOTS:
+            BPH_CUDA(launch_boundary_slots(c));
+            return BPH_OK;
+        case BPH_PHASE_ADI: {
+            if (nsteps < 1 || nsteps > 10000) break;
+            Schedule *s;
+            if ((rc = get_schedule(c, nsteps, &s))) return rc;
+            BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, false));
+            return BPH_OK;
+        }
+        case BPH_PHASE_FFT_INV:
+            if (!d_pot) break;
+            BPH_CUDA(launch_fft_inv(c, d_pot));
+            return BPH_OK;
+        default:
+            break;
+    }
+    set_error("invalid phase %d or arguments", phase);
+    return BPH_ERR_INVALID;
+}
+
+int bph_num_boundary_rows(const bph_ctx_t *c) { return c ? c->nb : 0; }
+
+int bph_copy_green(bph_ctx_t *c, double *out, size_t n) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    size_t need = (size_t)c->g.mmax * c->nb * c->np;
+    if (!out || n < need) {
+        set_error("output buffer too small (%zu < %zu)", n, need);
+        return BPH_ERR_INVALID;
+    }
+    if ((rc = set_device_of(c))) return rc;
+    BPH_CUDA(cudaMemcpyAsync(out, c->d_green, sizeof(double) * need, cudaMemcpyDeviceToHost, c->stream));
+    BPH_CUDA(cudaStreamSynchronize(c->stream));
+    return BPH_OK;
+}
+
+int bph_copy_moments(bph_ctx_t *c, double *out, size_t n) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    size_t need = (size_t)c->g.mmax * c->nb * 2;
+    if (!out || n < need) {
+        set_error("output buffer too small (%zu < %zu)", n, need);
+        return BPH_ERR_INVALID;
+    }
+    if ((rc = set_device_of(c))) return rc;
+    BPH_CUDA(cudaMemcpyAsync(out, c->d_S, sizeof(double) * need, cudaMemcpyDeviceToHost, c->stream));
+    BPH_CUDA(cudaStreamSynchronize(c->stream));
+    return BPH_OK;
+}
+
+long long bph_launch_count(const bph_ctx_t *c) { return c ? c->launches : 0; }
+
+size_t bph_device_bytes(const bph_ctx_t *c) { return c ? c->bytes : 0; }
+
+}  // extern "C"

@@ -1,0 +1,160 @@
+// bph_boundary.cu -- the boundary potential (bessel.F90:170-488).
+//
+// k_green_contract: S[m][b] = sum_p G[m][b][p] * (cos, sin moment)[m][p],
+// the per-mode contraction of the Green tables with the interior density
+// moments (bessel.F90:186-296).  The tables (8 bytes per element, read once
+// per solve) dominate the compulsory bytes of a solve, so the kernel is a
+// streaming GEMV with two right-hand sides: 16-byte evict-first loads of the
+// table rows, the moment vectors (small, L2-resident) read once per CTA
+// for BR rows, and a fixed-order CTA reduction (deterministic results).
+//
+// k_boundary_slots: the Dirichlet data of the ADI sweeps in Fourier-slot
+// space.  The reference synthesises the physical boundary potential
+//   Phi_B(l) = factor [S_C0 + 2 sum_{m>=1} (S_Cm cos k th_l + S_Sm sin k th_l)],
+// th_l = (l - 1/2) dphi, k = fm*m (bessel.F90:399-488), writes it into potp
+// and transforms it with the rest of potp (helmadi.F90:159).  For k < N/2
+// that transform is exact in closed form:
+//   F_0 = N factor S_C0,  F_k = e^{-i pi k/N} N factor (S_Cm + i S_Sm),
+// and zero at every other frequency, so the slots are written directly.
+#include "bph_internal.cuh"
+
+namespace bph {
+namespace {
+
+constexpr int kContractRows = 8;
+constexpr int kContractThreads = 256;
+
+template <bool kVec>
+__global__ void __launch_bounds__(kContractThreads)
+k_green_contract(const double *__restrict__ G, const double *__restrict__ mom, double *__restrict__ S,
+                 long long np, int nb) {
+    const int m = blockIdx.y;
+    const int b0 = blockIdx.x * kContractRows;
+    const int nrows = min(kContractRows, nb - b0);
+    const double *mc = mom + (2LL * m) * np;
+    const double *ms = mom + (2LL * m + 1) * np;
+    const double *g0 = G + ((long long)m * nb + b0) * np;
+    double ac[kContractRows], as[kContractRows];
+#pragma unroll
+    for (int r = 0; r < kContractRows; ++r) ac[r] = as[r] = 0.0;
+    if (kVec) {
+        const long long n2 = np / 2;
+        const double2 *mc2 = reinterpret_cast<const double2 *>(mc);
+        const double2 *ms2 = reinterpret_cast<const double2 *>(ms);
+        for (long long i = threadIdx.x; i < n2; i += kContractThreads) {
+            double2 vc = __ldg(mc2 + i), vs = __ldg(ms2 + i);
+#pragma unroll
+            for (int r = 0; r < kContractRows; ++r) {
+                if (r < nrows) {
+                    double2 g = __ldcs(reinterpret_cast<const double2 *>(g0 + r * np) + i);
+                    ac[r] = fma(g.x, vc.x, ac[r]);
+                    ac[r] = fma(g.y, vc.y, ac[r]);
+                    as[r] = fma(g.x, vs.x, as[r]);
+                    as[r] = fma(g.y, vs.y, as[r]);
+                }
+            }
+        }
+    } else {
+        for (long long i = threadIdx.x; i < np; i += kContractThreads) {
+            double vc = __ldg(mc + i), vs = __ldg(ms + i);
+#pragma unroll
+            for (int r = 0; r < kContractRows; ++r) {
+                if (r < nrows) {
+                    double g = __ldcs(g0 + r * np + i);
+                    ac[r] = fma(g, vc, ac[r]);
+                    as[r] = fma(g, vs, as[r]);
+                }
+            }
+        }
+    }
+    // Warp then CTA reduction in a fixed order.
+    __shared__ double red[kContractThreads / 32][2 * kContractRows];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int r = 0; r < kContractRows; ++r) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            ac[r] += __shfl_down_sync(0xffffffffu, ac[r], off);
+            as[r] += __shfl_down_sync(0xffffffffu, as[r], off);
+        }
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int r = 0; r < kContractRows; ++r) {
+            red[warp][2 * r] = ac[r];
+            red[warp][2 * r + 1] = as[r];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * nrows) {
+        double v = 0.0;
+#pragma unroll
+        for (int w = 0; w < kContractThreads / 32; ++w) v += red[w][threadIdx.x];
+        int r = threadIdx.x >> 1, cs = threadIdx.x & 1;
+        S[((long long)m * nb + b0 + r) * 2 + cs] = (m == 0 && cs == 1) ? 0.0 : v;
+    }
+}
+
+// One thread per (boundary row b, slot s); rows nb.. write the corner
+// columns, which stay zero (bessel.F90:417,452: pott(numr)=pots(numz)=0).
+__global__ void k_boundary_slots(const double *__restrict__ S, const double2 *__restrict__ ph,
+                                 double *__restrict__ P, int numr, int numz, int nr, int nz, int nb, int N,
+                                 int mmax, int fm, int isym, double nfactor) {
+    const int M = N / 2;
+    const int ncorner = (isym == 1) ? 2 : 1;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)(nb + ncorner) * N) return;
+    const int s = (int)(t % N), b = (int)(t / N);
+    const long long nplane = (long long)numr * numz;
+    int jz, kz;
+    if (b < nr) {
+        jz = b + 1;
+        kz = numz - 1;
+    } else if (b < nr + nz) {
+        jz = numr - 1;
+        kz = b - nr + 1;
+    } else if (b < nb) {
+        jz = b - nr - nz + 1;
+        kz = 0;
+    } else {
+        jz = numr - 1;
+        kz = (b == nb) ? numz - 1 : 0;
+        P[(long long)s * nplane + jz + (long long)numr * kz] = 0.0;
+        return;
+    }
+    const bool imag = s > M;
+    const int k = imag ? s - M : s;
+    double v = 0.0;
+    if (k < M && k % fm == 0 && k / fm < mmax) {
+        const int m = k / fm;
+        const double sc = S[((long long)m * nb + b) * 2], ss = S[((long long)m * nb + b) * 2 + 1];
+        const double2 w = ph[m];  // (cos, sin) of pi k / N
+        v = imag ? nfactor * (w.y * sc - w.x * ss) : nfactor * (w.x * sc + w.y * ss);
+    }
+    P[(long long)s * nplane + jz + (long long)numr * kz] = v;
+}
+
+}  // namespace
+
+cudaError_t launch_green_contract(bph_ctx *c) {
+    dim3 grid((unsigned)((c->nb + kContractRows - 1) / kContractRows), (unsigned)c->g.mmax);
+    ++c->launches;
+    if (c->np % 2 == 0)
+        k_green_contract<true><<<grid, kContractThreads, 0, c->stream>>>(c->d_green, c->d_mom, c->d_S, c->np, c->nb);
+    else
+        k_green_contract<false><<<grid, kContractThreads, 0, c->stream>>>(c->d_green, c->d_mom, c->d_S, c->np, c->nb);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_boundary_slots(bph_ctx *c) {
+    int ncorner = (c->g.isym == 1) ? 2 : 1;
+    long long n = (long long)(c->nb + ncorner) * c->N;
+    int threads = 256;
+    ++c->launches;
+    k_boundary_slots<<<(unsigned)((n + threads - 1) / threads), threads, 0, c->stream>>>(
+        c->d_S, c->d_ph, c->d_P, c->g.numr, c->g.numz, c->nr, c->nz, c->nb, c->N, c->g.mmax, c->fm, c->g.isym,
+        (double)c->N * c->factor);
+    return cudaGetLastError();
+}
+
+}  // namespace bph

@@ -1,0 +1,373 @@
+// bph_fft.cu -- azimuthal real FFTs (realft.F90 + the slot reorder of
+// helmadi.F90:132-183 and its inverse :357-411).
+//
+// A CTA takes a tile of 32 consecutive (J,K) columns and all numphi samples
+// of each: every row of the tile is a 256-byte coalesced segment of the
+// Fortran array (J fastest).  The N real samples of a column are packed as
+// M = N/2 complex values in shared memory, transformed by in-place Stockham
+// radix-4 (and one radix-2) passes -- each pass loads its butterfly inputs
+// to registers, synchronises, and stores -- and post-processed into the
+// real spectrum.  Results are written slot-major, which is the layout the
+// ADI kernel reads: the reference's swap_phi_r / swap_r_phi transposes are
+// this store / load layout.
+//
+// Forward convention (realft isign=+1): F_k = sum_l f_l exp(+2 pi i k l / N).
+#include <cmath>
+
+#include "bph_internal.cuh"
+
+namespace bph {
+namespace {
+
+constexpr int kTile = 32;  // columns per CTA
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
+    return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+
+// One in-place Stockham pass of radix R (4 or 2) over all tile columns.
+// C[n*kTile + c] holds element n of column c; tw[t] = e^{+2 pi i t / M}.
+// SIGN = +1 forward (e^{+i}), -1 inverse.
+template <int M, int R, int SIGN, int NT>
+__device__ __forceinline__ void stockham_pass(double2 *C, const double2 *tw, int Ns) {
+    constexpr int kTotal = kTile * (M / R);
+    constexpr int kItems = (kTotal + NT - 1) / NT;  // butterflies per thread
+    double2 v[kItems][R];
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+        int it = tid + i * NT;
+        if (kTotal % NT != 0 && it >= kTotal) break;
+        int c = it % kTile, j = it / kTile;
+        int k = j % Ns;
+        int tstep = k * (M / (Ns * R));
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            double2 x = C[(j + r * (M / R)) * kTile + c];
+            if (r > 0) {
+                double2 w = tw[r * tstep];
+                x = (SIGN > 0) ? cmul(x, w) : cmulc(x, w);
+            }
+            v[i][r] = x;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+        int it = tid + i * NT;
+        if (kTotal % NT != 0 && it >= kTotal) break;
+        int c = it % kTile, j = it / kTile;
+        int k = j % Ns;
+        int base = (j / Ns) * Ns * R + k;
+        if (R == 4) {
+            double2 a0 = cadd(v[i][0], v[i][2]), a1 = csub(v[i][0], v[i][2]);
+            double2 a2 = cadd(v[i][1], v[i][3]), d = csub(v[i][1], v[i][3]);
+            double2 a3 = (SIGN > 0) ? make_double2(-d.y, d.x) : make_double2(d.y, -d.x);
+            C[(base + 0 * Ns) * kTile + c] = cadd(a0, a2);
+            C[(base + 1 * Ns) * kTile + c] = cadd(a1, a3);
+            C[(base + 2 * Ns) * kTile + c] = csub(a0, a2);
+            C[(base + 3 * Ns) * kTile + c] = csub(a1, a3);
+        } else {
+            C[(base + 0 * Ns) * kTile + c] = cadd(v[i][0], v[i][1]);
+            C[(base + 1 * Ns) * kTile + c] = csub(v[i][0], v[i][1]);
+        }
+    }
+    __syncthreads();
+}
+
+template <int M, int SIGN, int NT>
+__device__ __forceinline__ void fft_tile(double2 *C, const double2 *tw) {
+    int Ns = 1;
+#pragma unroll
+    for (int len = M; len >= 4; len /= 4) {
+        stockham_pass<M, 4, SIGN, NT>(C, tw, Ns);
+        Ns *= 4;
+    }
+    if ((M & 0x55555555) == 0) {  // log2(M) odd: one radix-2 pass remains
+        stockham_pass<M, 2, SIGN, NT>(C, tw, Ns);
+    }
+}
+
+template <int M>
+struct FftShape {
+    static constexpr int kThreads = (M >= 256) ? 512 : 256;
+    static constexpr size_t kSmem = sizeof(double2) * ((size_t)M * kTile + M + (M + 1));
+};
+
+// Forward transform of interior columns.  kRho: write R = -4 pi rho_hat
+// (zero on the rows potential_solver.F90:66-78 zeroes) and the boundary
+// moments of the unzeroed density (bessel.F90:179-185, 226-274) obtained
+// from the same spectrum: sum_l rho_l e^{i k (l - 1/2) dphi} = e^{i pi k/N} F_k.
+// !kRho: write the warm-start potential into P's interior.
+template <int M, bool kRho>
+__global__ void __launch_bounds__(FftShape<M>::kThreads)
+k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__restrict__ mom,
+          const double2 *__restrict__ g_tw, const double2 *__restrict__ g_tw2, const double2 *__restrict__ g_ph,
+          int numr, int numz, int nr, int nz, int mmax, int fm, int isym, double four_pi,
+          int *__restrict__ status) {
+    constexpr int NT = FftShape<M>::kThreads;
+    extern __shared__ double2 smem[];
+    double2 *C = smem;
+    double2 *tw = C + M * kTile;
+    double2 *tw2 = tw + M;
+    const int tid = threadIdx.x;
+    const long long np = (long long)nr * nz;
+    const long long nplane = (long long)numr * numz;
+    const long long p0 = (long long)blockIdx.x * kTile;
+    for (int i = tid; i < M; i += NT) tw[i] = g_tw[i];
+    for (int i = tid; i <= M; i += NT) tw2[i] = g_tw2[i];
+    // Load: thread -> (column c, sample pair n).
+    bool bad = false;
+    for (int it = tid; it < kTile * M; it += NT) {
+        int c = it % kTile, n = it / kTile;
+        long long p = p0 + c;
+        double2 v = make_double2(0.0, 0.0);
+        if (p < np) {
+            int jz = (int)(p % nr) + 1, kz = (int)(p / nr) + 1;
+            const double *col = src + jz + (long long)numr * kz;
+            v.x = __ldg(col + nplane * (2 * n));
+            v.y = __ldg(col + nplane * (2 * n + 1));
+            if (kRho) bad |= !(isfinite(v.x) && isfinite(v.y));
+        }
+        C[n * kTile + c] = v;
+    }
+    if (kRho && bad) atomicOr(status, kStatusNonFinite);
+    __syncthreads();
+    fft_tile<M, +1, NT>(C, tw);
+    // Post-process pairs (k, M-k) into F_k, F_{M-k}; write slots.
+    for (int it = tid; it < kTile * (M / 2 + 1); it += NT) {
+        int c = it % kTile, k = it / kTile;
+        long long p = p0 + c;
+        if (p >= np) continue;
+        int jz = (int)(p % nr) + 1, kz = (int)(p / nr) + 1;
+        double2 Fk, Fm;  // F_k and F_{M-k} (for k = 0: F_0 and F_M, both real)
+        if (k == 0) {
+            double2 z = C[c];
+            Fk = make_double2(z.x + z.y, 0.0);
+            Fm = make_double2(z.x - z.y, 0.0);
+        } else if (2 * k == M) {
+            Fk = C[k * kTile + c];
+            Fm = Fk;
+        } else {
+            double2 zk = C[k * kTile + c], zm = C[(M - k) * kTile + c];
+            double2 e = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+            double2 d = make_double2(zk.x - zm.x, zk.y + zm.y);
+            double2 o = make_double2(0.5 * d.y, -0.5 * d.x);
+            Fk = cadd(e, cmul(tw2[k], o));
+            double2 e2 = make_double2(e.x, -e.y);
+            double2 d2 = make_double2(zm.x - zk.x, zm.y + zk.y);
+            double2 o2 = make_double2(0.5 * d2.y, -0.5 * d2.x);
+            Fm = cadd(e2, cmul(tw2[M - k], o2));
+        }
+        // Slot values: s = k -> Re F_k (F_0 at 0), s = M + k -> -Im F_k, s = M -> F_M.
+        const int ka = k, kb = M - k;
+        double sa_re = Fk.x, sa_im = -Fk.y, sb_re = Fm.x, sb_im = -Fm.y;
+        if (kRho) {
+            bool zeroed = (jz == numr - 2) || (kz == numz - 2) || (isym == 1 && kz == 1);
+            double *o = out + p;
+            if (k == 0) {
+                o[0] = zeroed ? 0.0 : -(four_pi * sa_re);
+                o[np * M] = zeroed ? 0.0 : -(four_pi * sb_re);
+            } else {
+                o[np * ka] = zeroed ? 0.0 : -(four_pi * sa_re);
+                o[np * (M + ka)] = zeroed ? 0.0 : -(four_pi * sa_im);
+                if (kb != ka) {
+                    o[np * kb] = zeroed ? 0.0 : -(four_pi * sb_re);
+                    o[np * (M + kb)] = zeroed ? 0.0 : -(four_pi * sb_im);
+                }
+            }
+            // Moments for boundary modes m with fm*m in {ka, kb}.
+#pragma unroll 1
+            for (int side = 0; side < 2; ++side) {
+                int kk = side ? kb : ka;
+                if (side && kb == ka) break;
+                if (kk == M) continue;
+                if (kk % fm) continue;
+                int m = kk / fm;
+                if (m >= mmax) continue;
+                double2 F = side ? Fm : Fk;
+                double tc, ts;
+                if (m == 0) {
+                    tc = F.x;
+                    ts = 0.0;
+                } else {
+                    double2 ph = g_ph[m];
+                    tc = ph.x * F.x - ph.y * F.y;
+                    ts = ph.y * F.x + ph.x * F.y;
+                }
+                mom[(2LL * m) * np + p] = tc;
+                mom[(2LL * m + 1) * np + p] = ts;
+            }
+        } else {
+            double *o = out + jz + (long long)numr * kz;
+            if (k == 0) {
+                o[0] = sa_re;
+                o[nplane * M] = sb_re;
+            } else {
+                o[nplane * ka] = sa_re;
+                o[nplane * (M + ka)] = sa_im;
+                if (kb != ka) {
+                    o[nplane * kb] = sb_re;
+                    o[nplane * (M + kb)] = sb_im;
+                }
+            }
+        }
+    }
+}
+
+// Inverse transform of every (J,K) column of the slot array into the
+// physical potential, 1/N normalised (the reference's 2/numphi times the
+// n/2-scaled NR inverse), with the axis condition phi(1,K,l) =
+// phi(2,K,l+N/2) (isym 3: phi(2,K,l)) and the equator condition
+// phi(J,1,l) = phi(J,2,l) (isym 2,3) taken at the source: those columns
+// transform the source column's spectrum (shifted by N/2 = sign (-1)^k).
+template <int M>
+__global__ void __launch_bounds__(FftShape<M>::kThreads)
+k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 *__restrict__ g_tw,
+          const double2 *__restrict__ g_tw2, int numr, int numz, int isym) {
+    constexpr int NT = FftShape<M>::kThreads;
+    extern __shared__ double2 smem[];
+    double2 *C = smem;
+    double2 *tw = C + M * kTile;
+    double2 *tw2 = tw + M;
+    const int tid = threadIdx.x;
+    const long long nplane = (long long)numr * numz;
+    const long long q0 = (long long)blockIdx.x * kTile;
+    for (int i = tid; i < M; i += NT) tw[i] = g_tw[i];
+    for (int i = tid; i <= M; i += NT) tw2[i] = g_tw2[i];
+    // Load slots: thread -> (column c, slot pair (k, M+k)).
+    for (int it = tid; it < kTile * M; it += NT) {
+        int c = it % kTile, k = it / kTile;
+        long long q = q0 + c;
+        double2 v = make_double2(0.0, 0.0);
+        if (q < nplane) {
+            int jz = (int)(q % numr), kz = (int)(q / numr);
+            bool flip = (jz == 0) && (isym != 3) && (k & 1);
+            int js = (jz == 0) ? 1 : jz;
+            int ks = (kz == 0 && isym != 1) ? 1 : kz;
+            const double *col = P + js + (long long)numr * ks;
+            double a = __ldg(col + nplane * k), b = __ldg(col + nplane * (M + k));
+            if (k == 0) {
+                v = make_double2(a, b);  // (F_0, F_M): both real
+            } else {
+                v = make_double2(a, -b);  // F_k = slot_k - i slot_{M+k}
+                if (flip) v = make_double2(-v.x, -v.y);
+            }
+        }
+        C[k * kTile + c] = v;
+    }
+    __syncthreads();
+    // Pre-process into Z_k = E_k + i O_k.
+    for (int it = tid; it < kTile * (M / 2 + 1); it += NT) {
+        int c = it % kTile, k = it / kTile;
+        if (k == 0) {
+            double2 f = C[c];
+            C[c] = make_double2(0.5 * (f.x + f.y), 0.5 * (f.x - f.y));
+        } else if (2 * k != M) {
+            double2 fk = C[k * kTile + c], fm = C[(M - k) * kTile + c];
+            double2 e = make_double2(0.5 * (fk.x + fm.x), 0.5 * (fk.y - fm.y));
+            double2 d = make_double2(0.5 * (fk.x - fm.x), 0.5 * (fk.y + fm.y));
+            double2 o = cmulc(d, tw2[k]);
+            double2 e2 = make_double2(e.x, -e.y);
+            double2 d2 = make_double2(0.5 * (fm.x - fk.x), 0.5 * (fm.y + fk.y));
+            double2 o2 = cmulc(d2, tw2[M - k]);
+            C[k * kTile + c] = make_double2(e.x - o.y, e.y + o.x);
+            C[(M - k) * kTile + c] = make_double2(e2.x - o2.y, e2.y + o2.x);
+        }
+    }
+    __syncthreads();
+    fft_tile<M, -1, NT>(C, tw);
+    const double scale = 1.0 / (double)M;
+    for (int it = tid; it < kTile * M; it += NT) {
+        int c = it % kTile, n = it / kTile;
+        long long q = q0 + c;
+        if (q >= nplane) continue;
+        double2 z = C[n * kTile + c];
+        pot[q + nplane * (2 * n)] = z.x * scale;
+        pot[q + nplane * (2 * n + 1)] = z.y * scale;
+    }
+}
+
+template <int M>
+cudaError_t set_fft_attrs(bph_ctx *c) {
+    size_t smem = FftShape<M>::kSmem;
+    cudaError_t e = cudaFuncSetAttribute(k_fft_fwd<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_fft_fwd<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_fft_inv<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    c->fft_smem_fwd = c->fft_smem_inv = (int)smem;
+    return e;
+}
+
+template <int M>
+cudaError_t fwd_rho(bph_ctx *c, const double *rho) {
+    unsigned blocks = (unsigned)((c->np + kTile - 1) / kTile);
+    k_fft_fwd<M, true><<<blocks, FftShape<M>::kThreads, FftShape<M>::kSmem, c->stream>>>(
+        rho, c->d_R, c->d_mom, c->d_tw, c->d_tw2, c->d_ph, c->g.numr, c->g.numz, c->nr, c->nz, c->g.mmax, c->fm,
+        c->g.isym, c->four_pi, c->d_status);
+    return cudaGetLastError();
+}
+
+template <int M>
+cudaError_t fwd_pot(bph_ctx *c, const double *pot) {
+    unsigned blocks = (unsigned)((c->np + kTile - 1) / kTile);
+    k_fft_fwd<M, false><<<blocks, FftShape<M>::kThreads, FftShape<M>::kSmem, c->stream>>>(
+        pot, c->d_P, nullptr, c->d_tw, c->d_tw2, c->d_ph, c->g.numr, c->g.numz, c->nr, c->nz, c->g.mmax, c->fm,
+        c->g.isym, c->four_pi, c->d_status);
+    return cudaGetLastError();
+}
+
+template <int M>
+cudaError_t inv(bph_ctx *c, double *pot) {
+    unsigned blocks = (unsigned)((c->nplane + kTile - 1) / kTile);
+    k_fft_inv<M><<<blocks, FftShape<M>::kThreads, FftShape<M>::kSmem, c->stream>>>(
+        c->d_P, pot, c->d_tw, c->d_tw2, c->g.numr, c->g.numz, c->g.isym);
+    return cudaGetLastError();
+}
+
+#define BPH_FFT_DISPATCH(FN, ...)                  \
+    switch (c->M) {                                \
+        case 8: return FN<8>(__VA_ARGS__);         \
+        case 16: return FN<16>(__VA_ARGS__);       \
+        case 32: return FN<32>(__VA_ARGS__);       \
+        case 64: return FN<64>(__VA_ARGS__);       \
+        case 128: return FN<128>(__VA_ARGS__);     \
+        case 256: return FN<256>(__VA_ARGS__);     \
+        default: return cudaErrorInvalidValue;     \
+    }
+
+cudaError_t set_attrs_dispatch(bph_ctx *c) { BPH_FFT_DISPATCH(set_fft_attrs, c) }
+cudaError_t fwd_rho_dispatch(bph_ctx *c, const double *rho) { BPH_FFT_DISPATCH(fwd_rho, c, rho) }
+cudaError_t fwd_pot_dispatch(bph_ctx *c, const double *pot) { BPH_FFT_DISPATCH(fwd_pot, c, pot) }
+cudaError_t inv_dispatch(bph_ctx *c, double *pot) { BPH_FFT_DISPATCH(inv, c, pot) }
+
+}  // namespace
+
+int fft_configure(bph_ctx *c) {
+    cudaError_t e = set_attrs_dispatch(c);
+    if (e != cudaSuccess) return cuda_fail(e, "fft_configure");
+    return BPH_OK;
+}
+
+cudaError_t launch_fft_fwd_rho(bph_ctx *c, const double *rho) {
+    ++c->launches;
+    return fwd_rho_dispatch(c, rho);
+}
+
+cudaError_t launch_fft_fwd_pot(bph_ctx *c, const double *pot) {
+    ++c->launches;
+    return fwd_pot_dispatch(c, pot);
+}
+
+cudaError_t launch_fft_inv(bph_ctx *c, double *pot) {
+    ++c->launches;
+    return inv_dispatch(c, pot);
+}
+
+}  // namespace bph

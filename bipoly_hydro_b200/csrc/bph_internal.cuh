@@ -1,0 +1,122 @@
+// bph_internal.cuh -- shared definitions of the B200 Poisson solver.
+//
+// HBM layout of one solve (numr x numz x numphi grid, N = numphi, M = N/2):
+//   rho, pot   Fortran column-major (J fastest, then K, then L), the
+//              reference's COMMON /poisson/ layout.
+//   P          Fourier-slot potential, slot-major P[s][K][J] (same plane
+//              layout per slot): interior from the forward FFT / ADI,
+//              boundary columns (J=numr, K=numz, K=1 for isym 1) from the
+//              Green-function boundary solve.  Slot s holds F_s (s = 0, M)
+//              or Re F_s (0 < s < M) or -Im F_{s-M} (s > M), the order
+//              helmadi.F90:133-156 gives its slots.  It also carries the
+//              warm-start state between calls.
+//   R          -4 pi rho_hat on the interior only, R[s][k][j] packed
+//              (j = J-2, k = K-2), zero on the zeroed rows of rhop.
+//   mom        interior density moments mom[m][cos|sin][p], p = j + nr*k.
+//   green      boundary Green tables G[m][b][p].
+//   S          boundary moments S[m][b][cos|sin].
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "bph.h"
+
+namespace bph {
+
+constexpr int kHyprUprBnd = 110;       // pot.h:7
+constexpr double kHyprCutoff = 1.025;  // pot.h:5
+constexpr int kMaxMmax = 64;
+constexpr int kNumSchedules = 3;       // 5 steps (warm), 20 steps (cold), one custom
+
+// Deferred device status bits (d_status).
+constexpr int kStatusNonFinite = 1;
+
+struct Schedule {
+    int nsteps = 0;
+    double *d_dt = nullptr;   // [nsteps]
+    double *d_rad = nullptr;  // [nsteps][N][3][nr]: 1/bet, ar/bet, gam (radial Thomas)
+    double *d_ver = nullptr;  // [nsteps][3][nz]:    1/bet, az/bet, gam (vertical Thomas)
+    double *h_dt = nullptr;   // host copy of the dt schedule
+};
+
+}  // namespace bph
+
+struct bph_ctx {
+    bph_grid_t g;
+    int nr = 0, nz = 0, nb = 0, N = 0, M = 0;
+    int fm = 1;  // azimuthal frequency of boundary mode m is fm*m (2 for isym 3)
+    long long np = 0, nplane = 0, ntot = 0;
+    double pi = 0, dz = 0, dphi = 0, drinv = 0, dzinv = 0, dphiinv = 0;
+    double gamma = 0, four_pi = 0, factor = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    int device = 0;
+
+    // Setup-time constants.
+    double *d_green = nullptr;   // [mmax][nb][np]
+    double *d_brb = nullptr;     // [N][numr]  radial diagonal without dt
+    double *d_elz = nullptr;     // [N][numr]  elambdazb
+    double *d_alphar = nullptr;  // [numr]
+    double *d_betar = nullptr;   // [numr]
+    double *d_bzb = nullptr;     // [numz]
+    double *d_qcoef = nullptr;   // [mmax] coefh, [mmax] nu, [mmax][111] dcoefh
+    double *d_grid = nullptr;    // rhf_g[numr], rhfinv_g[numr], zhf_g[numz]
+    double2 *d_tw = nullptr;     // e^{+2 pi i k / M}, k = 0..M-1
+    double2 *d_tw2 = nullptr;    // e^{+2 pi i k / N}, k = 0..M
+    double2 *d_ph = nullptr;     // e^{+i pi fm m / N}, m = 0..mmax-1
+    bph::Schedule sched[bph::kNumSchedules];
+
+    // Per-solve buffers.
+    double *d_R = nullptr;       // [N][np]
+    double *d_P = nullptr;       // [N][nplane]
+    double *d_prev = nullptr;    // [N][nplane] (converged form only)
+    double *d_mom = nullptr;     // [mmax][2][np]
+    double *d_S = nullptr;       // [mmax][nb][2]
+    double *d_W = nullptr;       // ADI work slabs when they do not fit on chip
+    double *d_P2 = nullptr;      // ADI potential slabs when they do not fit on chip
+    double *d_red = nullptr;     // reduction scratch
+    double *d_rho_stage = nullptr;
+    double *d_pot_stage = nullptr;
+    int *d_status = nullptr;
+
+    int adi_smem = 0;            // dynamic shared bytes of the on-chip ADI kernel (0: global variant)
+    int adi_threads = 256;
+    int fft_smem_fwd = 0, fft_smem_inv = 0;
+    bool have_warm = false;
+    long long launches = 0;
+    size_t bytes = 0;
+};
+
+namespace bph {
+
+// Error helpers (bph_api.cu).
+void set_error(const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define BPH_CUDA(call)                                          \
+    do {                                                        \
+        cudaError_t _e = (call);                                \
+        if (_e != cudaSuccess) return ::bph::cuda_fail(_e, #call); \
+    } while (0)
+
+// Launch wrappers (one per kernel family); each returns a cudaError_t of
+// the launch and counts it in ctx->launches.
+cudaError_t launch_qcoef(bph_ctx *c);
+cudaError_t launch_green_tables(bph_ctx *c);
+cudaError_t launch_adi_factors(bph_ctx *c, Schedule &s);
+cudaError_t launch_fft_fwd_rho(bph_ctx *c, const double *rho);
+cudaError_t launch_fft_fwd_pot(bph_ctx *c, const double *pot);
+cudaError_t launch_fft_inv(bph_ctx *c, double *pot);
+cudaError_t launch_green_contract(bph_ctx *c);
+cudaError_t launch_boundary_slots(bph_ctx *c);
+cudaError_t launch_adi(bph_ctx *c, const Schedule &s, int step0, int nsteps_run, bool cold);
+cudaError_t launch_update_norm(bph_ctx *c, double *d_out);
+cudaError_t launch_residual_norm(bph_ctx *c, double *d_out);
+
+int adi_configure(bph_ctx *c);
+int fft_configure(bph_ctx *c);
+
+}  // namespace bph

@@ -1,0 +1,261 @@
+"""Host-side mirror of the reference's solver interface over the C ABI.
+
+The reference exposes two argument-less Fortran subroutines that share COMMON
+blocks: ``potsetup`` (potsetup.F90:6) builds the Green tables and ADI
+coefficients once, and ``potential_solver`` (potential_solver.F90:6) turns
+``rho`` into ``pot`` every time step.  :class:`PotentialSolver` keeps the same
+two operations with the COMMON state made explicit: constructing it is
+``potsetup``, :meth:`PotentialSolver.potential_solver` is the per-step call
+with the same ``tstep`` warm/cold rule.
+
+All computation runs in ``libbph.so`` (CUDA, sm_100a).  There is no CPU path:
+if the library or a CUDA device is missing, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbph.so")
+
+BPH_OK = 0
+BPH_ERR_INVALID = -1
+BPH_ERR_NOMEM = -2
+BPH_ERR_NONFINITE = -3
+BPH_ERR_CUDA = -4
+BPH_ERR_TIMEOUT = -5
+BPH_ERR_STATE = -6
+
+_ERR_NAMES = {
+    BPH_ERR_INVALID: "BPH_ERR_INVALID",
+    BPH_ERR_NOMEM: "BPH_ERR_NOMEM",
+    BPH_ERR_NONFINITE: "BPH_ERR_NONFINITE",
+    BPH_ERR_CUDA: "BPH_ERR_CUDA",
+    BPH_ERR_TIMEOUT: "BPH_ERR_TIMEOUT",
+    BPH_ERR_STATE: "BPH_ERR_STATE",
+}
+
+#: Every symbol include/bph.h declares, in declaration order.
+EXPORTED_SYMBOLS = (
+    "bph_setup", "bph_potential_solver", "bph_potential_solver_device", "bph_solve_nsteps",
+    "bph_solve_converged", "bph_set_stream", "bph_synchronize", "bph_destroy", "bph_last_error",
+    "bph_version", "bph_num_boundary_rows", "bph_copy_green", "bph_copy_moments", "bph_run_phase",
+    "bph_launch_count", "bph_device_bytes",
+)
+
+#: bph_run_phase phase ids.
+PHASE_FFT_RHO, PHASE_CONTRACT, PHASE_SLOTS, PHASE_ADI, PHASE_FFT_INV = range(5)
+
+
+class BphError(RuntimeError):
+    """A non-zero status from the C ABI."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{_ERR_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+class Grid(ctypes.Structure):
+    """``bph_grid_t``: the runhydro.h / pot.h / fort.7 parameters of the solve."""
+
+    _fields_ = [
+        ("numr", ctypes.c_int),
+        ("numz", ctypes.c_int),
+        ("numphi", ctypes.c_int),
+        ("dr", ctypes.c_double),
+        ("isym", ctypes.c_int),
+        ("mmax", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def load_library(path: str | None = None):
+    """Load libbph.so and declare its prototypes.  Raises if it is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise ImportError(
+            f"{p} is not built; run `make -C bipoly_hydro_b200/csrc` (the solver has no CPU fallback)")
+    L = ctypes.CDLL(p)
+    vp, dp, i, sz = ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
+    L.bph_setup.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(vp)]
+    L.bph_potential_solver.argtypes = [vp, dp, dp, i]
+    L.bph_potential_solver_device.argtypes = [vp, dp, dp, i]
+    L.bph_solve_nsteps.argtypes = [vp, dp, dp, i, i, i]
+    L.bph_solve_converged.argtypes = [vp, dp, dp, i, i, ctypes.c_double, i, i, ctypes.POINTER(i),
+                                      ctypes.POINTER(ctypes.c_double)]
+    L.bph_set_stream.argtypes = [vp, vp]
+    L.bph_synchronize.argtypes = [vp]
+    L.bph_destroy.argtypes = [vp]
+    L.bph_last_error.restype = ctypes.c_char_p
+    L.bph_version.restype = ctypes.c_char_p
+    L.bph_num_boundary_rows.argtypes = [vp]
+    L.bph_copy_green.argtypes = [vp, dp, sz]
+    L.bph_copy_moments.argtypes = [vp, dp, sz]
+    L.bph_run_phase.argtypes = [vp, i, dp, dp, i]
+    L.bph_launch_count.argtypes = [vp]
+    L.bph_launch_count.restype = ctypes.c_longlong
+    L.bph_device_bytes.argtypes = [vp]
+    L.bph_device_bytes.restype = ctypes.c_size_t
+    for name in ("bph_setup", "bph_potential_solver", "bph_potential_solver_device", "bph_solve_nsteps",
+                 "bph_solve_converged", "bph_set_stream", "bph_synchronize", "bph_destroy",
+                 "bph_num_boundary_rows", "bph_copy_green", "bph_copy_moments", "bph_run_phase"):
+        getattr(L, name).restype = ctypes.c_int
+    if path is None:
+        _lib = L
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc != BPH_OK:
+        raise BphError(rc, load_library().bph_last_error().decode(errors="replace"))
+
+
+def _host_ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def _dev_ptr(x) -> int:
+    """Device address of a torch CUDA tensor, an object with data_ptr(), or an int."""
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return int(x.data_ptr())
+    raise TypeError("expected a device pointer (int) or a CUDA tensor")
+
+
+@dataclass
+class ConvergedInfo:
+    cycles: int
+    residual: float
+
+
+class PotentialSolver:
+    """potsetup + potential_solver for one grid on the current CUDA device.
+
+    ``rho``/``pot`` are ``(numr, numz, numphi)`` float64 arrays in Fortran
+    order, guard zones included (the reference's COMMON /poisson/ layout).
+    """
+
+    def __init__(self, numr: int, numz: int, numphi: int, dr: float, isym: int = 2, mmax: int = 30):
+        self._lib = load_library()
+        self.grid = Grid(int(numr), int(numz), int(numphi), float(dr), int(isym), int(mmax))
+        self.shape = (int(numr), int(numz), int(numphi))
+        self.isym, self.mmax, self.dr = int(isym), int(mmax), float(dr)
+        h = ctypes.c_void_p()
+        _check(self._lib.bph_setup(ctypes.byref(self.grid), ctypes.byref(h)))
+        self._h = h
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.bph_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> int:
+        return int(self._h.value)
+
+    # -- host-array API -----------------------------------------------------
+    def _rho_host(self, rho) -> np.ndarray:
+        a = np.asarray(rho, dtype=np.float64)
+        if a.shape != self.shape:
+            raise ValueError(f"rho has shape {a.shape}, expected {self.shape}")
+        return np.asfortranarray(a)
+
+    def potential_solver(self, rho, tstep: int, out: np.ndarray | None = None) -> np.ndarray:
+        """potential_solver.F90:6-109: tstep > 1 warm (5 ADI steps), else cold (20)."""
+        r = self._rho_host(rho)
+        pot = out if out is not None else np.empty(self.shape, dtype=np.float64, order="F")
+        if not pot.flags.f_contiguous or pot.dtype != np.float64 or pot.shape != self.shape:
+            raise ValueError("out must be a Fortran-ordered float64 array of the grid shape")
+        _check(self._lib.bph_potential_solver(self._h, _host_ptr(r), _host_ptr(pot), int(tstep)))
+        return pot
+
+    def solve_nsteps(self, rho, nsteps: int, cold: bool) -> np.ndarray:
+        r = self._rho_host(rho)
+        pot = np.empty(self.shape, dtype=np.float64, order="F")
+        _check(self._lib.bph_solve_nsteps(self._h, _host_ptr(r), _host_ptr(pot), int(nsteps), int(bool(cold)), 0))
+        return pot
+
+    def solve_converged(self, rho, nsteps: int = 20, cold: bool = True, tol: float = 1e-13,
+                        max_cycles: int = 200):
+        r = self._rho_host(rho)
+        pot = np.empty(self.shape, dtype=np.float64, order="F")
+        cyc, res = ctypes.c_int(0), ctypes.c_double(0.0)
+        _check(self._lib.bph_solve_converged(self._h, _host_ptr(r), _host_ptr(pot), int(nsteps), int(bool(cold)),
+                                             float(tol), int(max_cycles), 0, ctypes.byref(cyc), ctypes.byref(res)))
+        return pot, ConvergedInfo(cyc.value, res.value)
+
+    # -- device-array API ---------------------------------------------------
+    def set_stream(self, stream) -> None:
+        """Run later work on a CUDA stream: an int handle or a torch.cuda.Stream
+        (0 / None is CUDA's default stream)."""
+        handle = 0
+        if stream is not None:
+            handle = stream if isinstance(stream, int) else int(stream.cuda_stream)
+        _check(self._lib.bph_set_stream(self._h, ctypes.c_void_p(handle or None)))
+
+    def potential_solver_device(self, d_rho, d_pot, tstep: int) -> None:
+        """Enqueue one solve on device arrays (pointers or CUDA tensors)."""
+        _check(self._lib.bph_potential_solver_device(self._h, _dev_ptr(d_rho), _dev_ptr(d_pot), int(tstep)))
+
+    def solve_nsteps_device(self, d_rho, d_pot, nsteps: int, cold: bool) -> None:
+        _check(self._lib.bph_solve_nsteps(self._h, _dev_ptr(d_rho), _dev_ptr(d_pot), int(nsteps),
+                                          int(bool(cold)), 1))
+
+    def synchronize(self) -> None:
+        _check(self._lib.bph_synchronize(self._h))
+
+    # -- inspection ---------------------------------------------------------
+    @property
+    def nb(self) -> int:
+        return int(self._lib.bph_num_boundary_rows(self._h))
+
+    def green(self) -> np.ndarray:
+        nr, nz = self.shape[0] - 2, self.shape[1] - 2
+        out = np.empty(self.mmax * self.nb * nr * nz, dtype=np.float64)
+        _check(self._lib.bph_copy_green(self._h, _host_ptr(out), out.size))
+        return out.reshape(self.mmax, self.nb, nr * nz)
+
+    def moments_S(self) -> np.ndarray:
+        out = np.empty(self.mmax * self.nb * 2, dtype=np.float64)
+        _check(self._lib.bph_copy_moments(self._h, _host_ptr(out), out.size))
+        return out.reshape(self.mmax, self.nb, 2)
+
+    def run_phase(self, phase: int, d_rho=None, d_pot=None, nsteps: int = 5) -> None:
+        """Enqueue one kernel of the solve (timing diagnostics)."""
+        _check(self._lib.bph_run_phase(self._h, int(phase), _dev_ptr(d_rho) if d_rho is not None else None,
+                                       _dev_ptr(d_pot) if d_pot is not None else None, int(nsteps)))
+
+    @property
+    def launch_count(self) -> int:
+        return int(self._lib.bph_launch_count(self._h))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self._lib.bph_device_bytes(self._h))
+
+
+def version() -> str:
+    return load_library().bph_version().decode()

@@ -1,0 +1,131 @@
+/*
+ * bph.h -- C ABI of the B200 self-gravity Poisson solver (bipoly_hydro's
+ * potsetup + potential_solver path).
+ *
+ * Plain pointers and sizes only.  Host arrays are Fortran column-major
+ * real(8) rho(numr,numz,numphi) / pot(numr,numz,numphi) including the guard
+ * zones, exactly the COMMON /poisson/ pot, rho layout of the reference
+ * (potential_solver.F90:18-19).  Device arrays use the same layout.
+ *
+ * Every call returns an int status (BPH_OK = 0, negative on error) and
+ * bph_last_error() gives the text of the last failure on the calling
+ * thread.  A context is not thread-safe: use one per host thread or
+ * serialise calls on it.
+ */
+#ifndef BPH_H
+#define BPH_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BPH_OK 0
+#define BPH_ERR_INVALID (-1)   /* bad grid, argument or layout */
+#define BPH_ERR_NOMEM (-2)     /* device memory exhausted / admission refused */
+#define BPH_ERR_NONFINITE (-3) /* NaN or Inf in the density */
+#define BPH_ERR_CUDA (-4)      /* CUDA runtime failure (text in bph_last_error) */
+#define BPH_ERR_TIMEOUT (-5)   /* a bounded wait expired */
+#define BPH_ERR_STATE (-6)     /* call made in the wrong state */
+
+/* Grid and solver constants.  potsetup reads these from runhydro.h
+ * (numr, numz, numphi), setup_frac.F90:374-376 (dr; dz = dr), the fort.7
+ * deck (isym) and pot.h:3 (mmax).  One rank: numr_dd = numr, numz_dd = numz. */
+typedef struct bph_grid {
+    int numr;    /* radial zones incl. guard J=1 and boundary J=numr, >= 5 */
+    int numz;    /* vertical zones incl. guard K=1 and boundary K=numz, >= 5 */
+    int numphi;  /* azimuthal zones: power of two, >= 2*mmax (4*mmax for isym 3) */
+    double dr;   /* zone size in r and z */
+    int isym;    /* 1: no symmetry, 2: equatorial, 3: pi + equatorial */
+    int mmax;    /* boundary modes, 30 in the reference; 2..64 */
+} bph_grid_t;
+
+typedef struct bph_ctx bph_ctx_t;
+
+/* Replaces potsetup.F90:6 (called once at setup_frac.F90:689).  Builds the
+ * Green-function tables (tm.F90, sm.F90, bm.F90 with elle/ellf/rf/rd/
+ * gammln), the azimuthal trig data and the ADI coefficients, all on the
+ * current CUDA device, and returns a context that owns them. */
+int bph_setup(const bph_grid_t *grid, bph_ctx_t **ctx);
+
+/* Replaces potential_solver.F90:6 (called at setup_frac.F90:690 and
+ * main.F90:396).  rho and pot are HOST arrays.  tstep > 1 runs 5 ADI steps
+ * from the previous solution kept on the device; otherwise 20 steps from
+ * zero (potential_solver.F90:80-94).  Synchronous: returns after pot is
+ * written. */
+int bph_potential_solver(bph_ctx_t *ctx, const double *rho, double *pot, int tstep);
+
+/* Same solve on DEVICE arrays, enqueued on the context's stream; returns
+ * without waiting.  A non-finite density is reported by bph_synchronize. */
+int bph_potential_solver_device(bph_ctx_t *ctx, const double *d_rho, double *d_pot, int tstep);
+
+/* Explicit step count (helmadi(nsteps)); cold != 0 starts from zero.
+ * on_device != 0 means rho/pot are device arrays (asynchronous). */
+int bph_solve_nsteps(bph_ctx_t *ctx, const double *rho, double *pot, int nsteps, int cold,
+                     int on_device);
+
+/* Converged FP64 solve: the nsteps schedule is repeated until the relative
+ * change of the Fourier-space potential over one cycle is <= tol, or
+ * max_cycles ran.  Synchronous; cycles_out and resid_out (weighted
+ * relative residual ||-4 pi rho_hat - A phi_hat|| / ||4 pi rho_hat||) may
+ * be NULL.  The reference has no such mode (it always runs 5 or 20 steps);
+ * this is the fully converged discrete solution the mixed-precision solver
+ * is measured against. */
+int bph_solve_converged(bph_ctx_t *ctx, const double *rho, double *pot, int nsteps, int cold,
+                        double tol, int max_cycles, int on_device, int *cycles_out,
+                        double *resid_out);
+
+/* Stream used for all later work of this context (a cudaStream_t; NULL is
+ * CUDA's default stream).  Until the first call the context uses a
+ * non-blocking stream of its own. */
+int bph_set_stream(bph_ctx_t *ctx, void *cuda_stream);
+
+/* Wait for the context's stream; returns the first deferred error
+ * (e.g. BPH_ERR_NONFINITE) of the calls since the last synchronize. */
+int bph_synchronize(bph_ctx_t *ctx);
+
+/* Frees every device allocation of the context. */
+int bph_destroy(bph_ctx_t *ctx);
+
+/* Text of the last error on this thread ("" if none). */
+const char *bph_last_error(void);
+
+/* Library version string. */
+const char *bph_version(void);
+
+/* ---- inspection (tests and diagnostics) --------------------------- */
+
+/* Number of boundary rows nb: (numr-2)+(numz-2), plus (numr-2) for isym 1. */
+int bph_num_boundary_rows(const bph_ctx_t *ctx);
+
+/* Copies the Green tables to host memory, layout G[m][b][p] with
+ * p = (jl-2) + (numr-2)*(kl-2) and b = top jg-2 | side (numr-2)+kg-2 |
+ * bottom (isym 1).  n = mmax*nb*(numr-2)*(numz-2) doubles. */
+int bph_copy_green(bph_ctx_t *ctx, double *host_out, size_t n);
+
+/* Copies the boundary moments S[m][b][2] (cos, sin) of the last solve. */
+int bph_copy_moments(bph_ctx_t *ctx, double *host_out, size_t n);
+
+/* Phases of one solve, for timing a single kernel (bph_run_phase). */
+#define BPH_PHASE_FFT_RHO 0   /* k_fft_fwd: rho -> -4 pi rho_hat + moments */
+#define BPH_PHASE_CONTRACT 1  /* k_green_contract: tables x moments -> S */
+#define BPH_PHASE_SLOTS 2     /* k_boundary_slots: S -> Dirichlet slots */
+#define BPH_PHASE_ADI 3       /* k_adi: nsteps warm ADI steps */
+#define BPH_PHASE_FFT_INV 4   /* k_fft_inv: slots -> pot */
+
+/* Enqueues exactly one phase of a solve on the context's stream (device
+ * arrays; nsteps only for BPH_PHASE_ADI).  Diagnostic: phases run in order
+ * reproduce bph_solve_nsteps with on_device=1 and cold=0. */
+int bph_run_phase(bph_ctx_t *ctx, int phase, const double *d_rho, double *d_pot, int nsteps);
+
+/* Number of kernels this context has launched so far. */
+long long bph_launch_count(const bph_ctx_t *ctx);
+
+/* Device bytes held by the context. */
+size_t bph_device_bytes(const bph_ctx_t *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

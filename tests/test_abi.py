@@ -1,0 +1,65 @@
+"""The C ABI library loads and exports every symbol include/bph.h declares
+(no compute calls: these run without a GPU)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "bph.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return re.findall(r"\b(bph_[a-z_]+)\s*\(", text)
+
+
+def test_header_declares_the_mirrored_symbols(bph):
+    syms = declared_symbols()
+    assert len(syms) == len(set(syms))
+    assert set(syms) == set(bph.EXPORTED_SYMBOLS)
+
+
+def test_library_exports_every_declared_symbol(bph):
+    lib = ctypes.CDLL(bph.LIB_PATH)
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+
+
+def test_version_string(bph):
+    assert "sm_100a" in bph.version()
+
+
+@pytest.mark.parametrize("grid,msg", [
+    ((4, 10, 16, 0.1, 2, 4), "numr"),
+    ((10, 10, 24, 0.1, 2, 4), "power of two"),
+    ((10, 10, 1024, 0.1, 2, 4), "power of two"),
+    ((10, 10, 16, 0.1, 4, 4), "isym"),
+    ((10, 10, 16, 0.1, 2, 1), "mmax"),
+    ((10, 10, 64, 0.1, 2, 40), "too small"),
+    ((10, 10, 64, 0.1, 3, 20), "too small"),
+    ((10, 10, 16, -0.1, 2, 4), "dr"),
+])
+def test_invalid_grids_are_rejected_before_any_device_work(bph, grid, msg):
+    with pytest.raises(bph.BphError) as ei:
+        bph.PotentialSolver(*grid)
+    assert ei.value.code == bph.BPH_ERR_INVALID
+    assert msg in str(ei.value)
+
+
+def test_null_context_is_an_error(bph):
+    lib = bph.load_library()
+    assert lib.bph_potential_solver(None, None, None, 0) == bph.BPH_ERR_INVALID
+    assert lib.bph_destroy(None) == bph.BPH_OK
+
+
+def test_product_does_not_import_the_oracle():
+    """The product package never imports, links or loads the CPU oracle."""
+    pkg = os.path.join(ROOT, "bipoly_hydro_b200")
+    bad = re.compile(r"(import\s+oracle|from\s+oracle|liborc|bph_oracle|orc_[a-z])")
+    for dirpath, _, files in os.walk(pkg):
+        for f in files:
+            if f.endswith((".py", ".cu", ".cuh", ".h", ".cpp", "Makefile")):
+                src = open(os.path.join(dirpath, f)).read()
+                assert not bad.search(src), f

@@ -1,0 +1,150 @@
+"""CUDA solver vs the CPU oracle through the C ABI (FP64 drop-in parity).
+
+The bar is the one the north star sets for the FP64 form: relative L2 error of
+the potential <= 1e-12 against the reference algorithm with the same ADI step
+count.  Tables and boundary moments are compared on their own as well.
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import rel_l2, smooth_density
+
+pytestmark = pytest.mark.gpu
+
+POT_TOL = 1e-12
+
+# (numr, numz, numphi, dr, isym, mmax)
+SMALL_GRIDS = [
+    (18, 18, 16, 1.0 / 14.0, 2, 6),
+    (20, 14, 32, 1.0 / 18.0, 1, 8),
+    (18, 16, 32, 1.0 / 16.0, 3, 6),
+    (34, 26, 64, 1.0 / 30.0, 2, 30),
+    (35, 21, 64, 1.0 / 31.0, 2, 12),   # odd interior sizes
+]
+
+
+def _pair(oracle_mod, bph, grid):
+    numr, numz, numphi, dr, isym, mmax = grid
+    o = oracle_mod.Oracle(numr, numz, numphi, dr, isym, mmax)
+    g = bph.PotentialSolver(numr, numz, numphi, dr, isym, mmax)
+    return o, g
+
+
+@pytest.mark.parametrize("grid", SMALL_GRIDS, ids=lambda g: "x".join(map(str, g[:3])) + f"-isym{g[4]}")
+def test_green_tables_match(oracle_mod, bph, grid):
+    o, g = _pair(oracle_mod, bph, grid)
+    Go, Gg = o.green(), g.green()
+    assert Go.shape == Gg.shape
+    assert np.all(np.isfinite(Gg))
+    assert rel_l2(Gg, Go) <= 1e-13
+    for m in range(Go.shape[0]):
+        scale = np.abs(Go[m]).max()
+        assert np.abs(Gg[m] - Go[m]).max() <= 1e-11 * scale, f"mode {m}"
+    g.close()
+
+
+@pytest.mark.parametrize("grid", SMALL_GRIDS, ids=lambda g: "x".join(map(str, g[:3])) + f"-isym{g[4]}")
+def test_cold_then_warm_matches_oracle(oracle_mod, bph, grid):
+    numr, numz, numphi, dr, isym, _ = grid
+    o, g = _pair(oracle_mod, bph, grid)
+    rho = smooth_density(numr, numz, numphi, dr, isym)
+    po = o.potential_solver(rho, 0)
+    pg = g.potential_solver(rho, 0)
+    assert rel_l2(pg, po) <= POT_TOL
+    So, Sg = o.moments_S(), g.moments_S()
+    assert rel_l2(Sg, So) <= 1e-13
+    # warm steps with a rotated density (the time-step call)
+    for tstep in (2, 3):
+        rho = np.asfortranarray(np.roll(rho, 1, axis=2))
+        po = o.potential_solver(rho, tstep)
+        pg = g.potential_solver(rho, tstep)
+        assert rel_l2(pg, po) <= POT_TOL, f"tstep {tstep}"
+    g.close()
+
+
+def test_tstep_one_is_cold(oracle_mod, bph):
+    """tstep > 1 selects the warm start, tstep = 1 is cold (potential_solver.F90:80)."""
+    grid = SMALL_GRIDS[0]
+    numr, numz, numphi, dr, isym, _ = grid
+    o, g = _pair(oracle_mod, bph, grid)
+    rho = smooth_density(numr, numz, numphi, dr, isym)
+    g.potential_solver(rho, 0)
+    o.potential_solver(rho, 0)
+    rho2 = np.asfortranarray(rho * 1.1)
+    assert rel_l2(g.potential_solver(rho2, 1), o.potential_solver(rho2, 1)) <= POT_TOL
+    cold = o.solve_nsteps(rho2, 20, True)
+    assert rel_l2(g.potential_solver(rho2, 1), cold) <= POT_TOL
+    g.close()
+
+
+def test_config1_drop_in_sequence(oracle_mod, bph):
+    """66x66x64, dr=1/62, isym 2, mmax 30: cold start then warm rotated steps."""
+    from bipoly_hydro_b200 import fields
+
+    o, g = _pair(oracle_mod, bph, (66, 66, 64, 1.0 / 62.0, 2, 30))
+    rho = fields.two_polytropes()
+    for tstep in range(0, 5):
+        po = o.potential_solver(rho, tstep)
+        pg = g.potential_solver(rho, tstep)
+        assert rel_l2(pg, po) <= POT_TOL, f"tstep {tstep}"
+        rho = fields.rotate(rho)
+    g.close()
+
+
+@pytest.mark.parametrize("nsteps", [1, 3, 8])
+def test_explicit_step_counts(oracle_mod, bph, nsteps):
+    grid = SMALL_GRIDS[3]
+    numr, numz, numphi, dr, isym, _ = grid
+    o, g = _pair(oracle_mod, bph, grid)
+    rho = smooth_density(numr, numz, numphi, dr, isym, seed=nsteps)
+    assert rel_l2(g.solve_nsteps(rho, nsteps, True), o.solve_nsteps(rho, nsteps, True)) <= POT_TOL
+    assert rel_l2(g.solve_nsteps(rho, nsteps, False), o.solve_nsteps(rho, nsteps, False)) <= POT_TOL
+    g.close()
+
+
+def test_converged_matches_oracle(oracle_mod, bph):
+    grid = (34, 26, 64, 1.0 / 30.0, 2, 30)
+    numr, numz, numphi, dr, isym, _ = grid
+    o, g = _pair(oracle_mod, bph, grid)
+    rho = smooth_density(numr, numz, numphi, dr, isym)
+    po, co, ro = o.solve_converged(rho, 20, True, 1e-13, 100)
+    pg, info = g.solve_converged(rho, 20, True, 1e-13, 100)
+    assert info.cycles == co
+    assert abs(info.residual - ro) <= 0.5 * ro + 1e-12
+    assert rel_l2(pg, po) <= POT_TOL
+    g.close()
+
+
+def test_device_api_matches_host_api(bph):
+    import torch
+
+    grid = SMALL_GRIDS[3]
+    numr, numz, numphi, dr, isym, mmax = grid
+    rho = smooth_density(numr, numz, numphi, dr, isym)
+    a = bph.PotentialSolver(*grid)
+    b = bph.PotentialSolver(*grid)
+    ph = a.potential_solver(rho, 0)
+    d_rho = torch.from_numpy(np.ascontiguousarray(rho.ravel(order="F"))).cuda()
+    d_pot = torch.empty_like(d_rho)
+    b.set_stream(torch.cuda.current_stream())
+    b.potential_solver_device(d_rho, d_pot, 0)
+    b.synchronize()
+    pd = d_pot.cpu().numpy().reshape(rho.shape, order="F")
+    assert np.array_equal(pd, ph)
+    a.close()
+    b.close()
+
+
+def test_nonfinite_density_is_reported(bph):
+    grid = SMALL_GRIDS[0]
+    numr, numz, numphi, dr, isym, mmax = grid
+    g = bph.PotentialSolver(*grid)
+    rho = smooth_density(numr, numz, numphi, dr, isym)
+    rho[3, 4, 5] = np.nan
+    with pytest.raises(bph.BphError) as ei:
+        g.potential_solver(rho, 0)
+    assert ei.value.code == bph.BPH_ERR_NONFINITE
+    # the context stays usable
+    rho[3, 4, 5] = 1.0
+    g.potential_solver(rho, 0)
+    g.close()
