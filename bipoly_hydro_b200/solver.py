@@ -44,7 +44,7 @@ EXPORTED_SYMBOLS = (
     "bph_setup", "bph_potential_solver", "bph_potential_solver_device", "bph_solve_nsteps",
     "bph_solve_converged", "bph_set_stream", "bph_synchronize", "bph_destroy", "bph_last_error",
     "bph_version", "bph_num_boundary_rows", "bph_copy_green", "bph_copy_moments", "bph_run_phase",
-    "bph_launch_count", "bph_device_bytes",
+    "bph_green_contract_noalloc", "bph_launch_count", "bph_device_bytes",
 )
 
 #: bph_run_phase phase ids.
@@ -101,6 +101,8 @@ def load_library(path: str | None = None):
     L.bph_copy_green.argtypes = [vp, dp, sz]
     L.bph_copy_moments.argtypes = [vp, dp, sz]
     L.bph_run_phase.argtypes = [vp, i, dp, dp, i]
+    L.bph_green_contract_noalloc.argtypes = [vp, dp, dp]
+    L.bph_green_contract_noalloc.restype = ctypes.c_int
     L.bph_launch_count.argtypes = [vp]
     L.bph_launch_count.restype = ctypes.c_longlong
     L.bph_device_bytes.argtypes = [vp]

@@ -119,6 +119,28 @@ int bph_copy_moments(bph_ctx_t *ctx, double *host_out, size_t n);
  * reproduce bph_solve_nsteps with on_device=1 and cold=0. */
 int bph_run_phase(bph_ctx_t *ctx, int phase, const double *d_rho, double *d_pot, int nsteps);
 
+/* Boundary contraction without any device allocation.  No counterpart in
+ * the reference (its bessel.F90:186-296 sums run on host memory).
+ *
+ * For callers that may not call cudaMalloc where they need the boundary
+ * moments (an application memory pool that must not grow, a real-time loop
+ * that cannot afford cudaMalloc's device synchronisation, code that only
+ * holds pointers its caller gave it).  Inputs: ctx (its Green tables, built
+ * earlier by bph_setup) and d_mom, the interior density moments on the
+ * device, layout mom[m][cos|sin][p], p = (J-2) + (numr-2)*(K-2), with
+ * mom = sum_l rho(J,K,l) (cos|sin)(f m (l-1/2) dphi), f = 2 for isym 3
+ * else 1.  Output: d_S on the device, S[m][b][cos|sin] (bph_copy_moments'
+ * layout).  Enqueued on the context's stream; allocates nothing.
+ *
+ * Scratch: an 8 MiB file-scope device array per GPU, held until the
+ * process exits.  Grids with mmax*nb*2 partial sums beyond its capacity
+ * are rejected with BPH_ERR_INVALID.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress): make that first call
+ * before any stream capture.  All calls on a device share the array and
+ * it keeps the last call's contents; calls that overlap on the GPU race
+ * and must be serialised by the caller. */
+int bph_green_contract_noalloc(bph_ctx_t *ctx, const double *d_mom, double *d_S);
+
 /* Number of kernels this context has launched so far. */
 long long bph_launch_count(const bph_ctx_t *ctx);
 
