@@ -148,3 +148,25 @@ def test_nonfinite_density_is_reported(bph):
     rho[3, 4, 5] = 1.0
     g.potential_solver(rho, 0)
     g.close()
+
+
+def _golden_files():
+    import os
+
+    d = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    return sorted(os.path.join(d, f) for f in os.listdir(d) if f.endswith(".npz"))
+
+
+@pytest.mark.parametrize("path", _golden_files(), ids=lambda p: p.rsplit("/", 1)[-1])
+def test_gpu_reproduces_golden_fixture(bph, path):
+    g = np.load(path)
+    numr, numz, numphi, isym, mmax = (int(v) for v in g["grid"])
+    s = bph.PotentialSolver(numr, numz, numphi, float(g["dr"]), isym, mmax)
+    rho = np.asfortranarray(g["rho"])
+    assert rel_l2(s.potential_solver(rho, 0), g["cold"]) <= POT_TOL
+    assert rel_l2(s.potential_solver(np.asfortranarray(np.roll(rho, 1, axis=2)), 2), g["warm"]) <= POT_TOL
+    assert rel_l2(s.moments_S(), g["S_warm"]) <= 1e-13
+    G = s.green()
+    assert rel_l2(G[0, :4], g["green_m0"]) <= 1e-13
+    assert rel_l2(G[-1, :4], g["green_mlast"]) <= 1e-13
+    s.close()
