@@ -19,6 +19,8 @@
 // once per schedule at setup (k_adi_factors).  The on-chip slab's row
 // stride is odd (in doubles) so that line-parallel accesses along r are
 // bank-conflict free.
+#include <cstdint>
+
 #include "bph_internal.cuh"
 
 namespace bph {
@@ -103,8 +105,8 @@ __global__ void __launch_bounds__(kAdiThreads) k_adi(AdiArgs a) {
     for (int it = 0; it < a.nsteps_run; ++it) {
         const int step = a.step0 + it;
         const double dtt = a.dt[step];
-        const double *rsrc = a.rad + ((long long)step * a.N + s) * 3 * nr;
-        const double *vsrc = a.ver + (long long)step * 3 * nz;
+        const double *rsrc = a.rad + ((long long)step * a.N + s) * kAdiFactors * nr;
+        const double *vsrc = a.ver + (long long)step * kAdiFactors * nz;
         for (int i = tid; i < 3 * nr; i += kAdiThreads) rf[i] = rsrc[i];
         for (int i = tid; i < 3 * nz; i += kAdiThreads) vf[i] = vsrc[i];
         // ---- radial half-sweep (helmadi.F90:203-260) ----
@@ -185,6 +187,366 @@ __global__ void __launch_bounds__(kAdiThreads) k_adi(AdiArgs a) {
 
 size_t smalls_bytes(const bph_ctx *c) { return sizeof(double) * (size_t)(9 * c->nr + 4 * c->nz); }
 
+// ---------------------------------------------------------------------------
+// Segmented on-chip ADI (the fast path).  The slot's potential P and its
+// right-hand side R = -4 pi rho_hat both stay in shared memory for all
+// steps.  Every line system is cut into kAdiSeg-long segments, one thread
+// per (line, segment):
+//   A. right-hand side and forward elimination with zero carry-in, kept in
+//      registers; the segment's last value goes to shared memory;
+//   B. carry-in y_{s-1} folded from the preceding segments' last values and
+//      forward carries, fix-up y = L + G y_{s-1}, backward elimination with
+//      zero carry-in; the segment's first value goes to shared memory;
+//   C. carry-in x_{e+1} folded from the following segments, x = M + K x_{e+1},
+//      stored to P.
+// The per-element arithmetic is the Thomas algorithm of tridagr/tridagz; the
+// carries only re-associate it (results agree to rounding).
+
+struct SegLayout {
+    int ps, Pr, Pz, xsz;
+    int fsz;                  // doubles of one direction's factor block
+    size_t doubles;
+};
+
+// Factor block of one direction, n = line length, in shared memory:
+//   ib[n]   1/bet_j
+//   dd[n]   a_j/bet_j
+//   GG[n]   double2 (G_j, gam_{j+1})   forward carry and next back-substitution factor
+//   K[n]    backward carry
+__host__ __device__ inline int factor_block(int n) { return 5 * n + 1; }  // +1: 16-byte alignment of GG
+
+__host__ __device__ inline SegLayout seg_layout(int nr, int nz) {
+    SegLayout L;
+    L.ps = nr | 1;
+    L.Pr = (nr + kAdiSeg - 1) / kAdiSeg;
+    L.Pz = (nz + kAdiSeg - 1) / kAdiSeg;
+    L.xsz = max(nz * L.Pr, nr * L.Pz);
+    L.fsz = factor_block(max(nr, nz));
+    L.doubles = 2 * (size_t)nz * L.ps + 2 * (size_t)L.fsz + 4 * (size_t)L.xsz + 5 * (size_t)nr + 2;
+    return L;
+}
+
+struct Fac {
+    const double *ib, *dd, *K;
+    const double2 *GG;
+};
+
+__device__ inline Fac fac_view(const double *base, int n) {
+    Fac f;
+    f.ib = base;
+    f.dd = base + n;
+    const double *g = base + 2 * n;
+    if ((reinterpret_cast<uintptr_t>(g) & 15) != 0) ++g;
+    f.GG = reinterpret_cast<const double2 *>(g);
+    f.K = g + 2 * n;
+    return f;
+}
+
+// Copies one direction's factors [ib, dd, gam, G, K] (global) into a block.
+__device__ inline void fac_load(double *base, int n, const double *src, int tid, int nthreads) {
+    double *ib = base, *dd = base + n;
+    double *g = base + 2 * n;
+    if ((reinterpret_cast<uintptr_t>(g) & 15) != 0) ++g;
+    double2 *GG = reinterpret_cast<double2 *>(g);
+    double *K = g + 2 * n;
+    for (int j = tid; j < n; j += nthreads) {
+        ib[j] = src[j];
+        dd[j] = src[n + j];
+        GG[j] = make_double2(src[3 * n + j], (j + 1 < n) ? src[2 * n + j + 1] : 0.0);
+        K[j] = src[4 * n + j];
+    }
+}
+
+// Shared-memory layout (doubles):
+//   Ww  nz x ps  the line systems' right-hand sides, pre-multiplied by the
+//                sweep's 1/bet: at the start of a step the radial one
+//                (step 0: the initial potential), after the radial sweep the
+//                vertical one, after the last sweep phi.
+//   Rw  nz x ps  -4 pi rho_hat plus every Dirichlet term, folded in once:
+//                +gamma*top (K = numz-1), -alphar(numr-1)*side (J = numr-1),
+//                +gamma*bottom (K = 2, isym 1).  Both sweeps add exactly these
+//                terms (helmadi.F90:252-256, 327-340, and the K+1 / J+1
+//                neighbours of :224-245 / :296-319), so the sweeps see a zero
+//                frame and need no boundary branches.
+//   Fr, Fz  radial / vertical factor blocks
+//   Xa, Xb, Ea, Eb  per (line, segment) exchange: forward ends, backward
+//                starts, first and last solution values
+//   el0 [nr], AB [nr] double2 (alphaz, betaz), zrow [nr]
+//
+// One half-sweep, threads = (line, segment), phases separated by barriers:
+//   A  forward elimination with zero carry-in, values kept in registers;
+//   B  carry-in folded from preceding segments, fix-up, backward elimination;
+//   C  carry-in folded from following segments: the line's solution, still
+//      in registers; segment edges published;
+//   D  the other direction's right-hand side (or phi after the last step)
+//      from the registers and the published edges, written to Ww.
+// The per-element arithmetic is the Thomas algorithm of tridagr/tridagz; the
+// segment carries only re-associate it (results agree to rounding).
+template <int kSegThreads, bool kFull>
+__global__ void __launch_bounds__(kSegThreads, 1) k_adi_seg(AdiArgs a) {
+    extern __shared__ double sm[];
+    const int s = blockIdx.x, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = kSegThreads / 32;
+    const int nr = a.nr, nz = a.nz, numr = a.numr, numz = a.numz;
+    const SegLayout Lo = seg_layout(nr, nz);
+    const int ps = Lo.ps, Pr = Lo.Pr, Pz = Lo.Pz;
+    double *Ww = sm;
+    double *Rw = Ww + (size_t)nz * ps;
+    double *Fr = Rw + (size_t)nz * ps;
+    double *Fz = Fr + Lo.fsz;
+    double *Xa = Fz + Lo.fsz;
+    double *Xb = Xa + Lo.xsz;
+    double *Ea = Xb + Lo.xsz;
+    double *Eb = Ea + Lo.xsz;
+    double *el0 = Eb + Lo.xsz;
+    double *abp = el0 + nr;
+    if ((reinterpret_cast<uintptr_t>(abp) & 15) != 0) ++abp;
+    double2 *AB = reinterpret_cast<double2 *>(abp);
+    double *zrow = abp + 2 * nr;
+    const long long nplane = (long long)numr * numz;
+    double *Pg = a.P + (long long)s * nplane;
+    const double *Rs = a.R + (long long)s * nr * nz;
+    const double gamma = a.gamma;
+    const double a_side = a.alphar[numr - 2];  // alphar(numr-1)
+    const bool sym_bottom = (a.isym != 1);
+    const double *rad = a.rad + (long long)s * kAdiFactors * nr;
+    const long long rad_step = (long long)a.N * kAdiFactors * nr;
+    const long long ver_step = (long long)kAdiFactors * nz;
+
+    for (int j = tid; j < nr; j += kSegThreads) {
+        AB[j] = make_double2(a.alphar[j + 1], a.betar[j + 1]);
+        el0[j] = a.elz[(long long)s * numr + j + 1];
+        zrow[j] = 0.0;
+    }
+    fac_load(Fr, nr, rad + a.step0 * rad_step, tid, kSegThreads);
+    fac_load(Fz, nz, a.ver + a.step0 * ver_step, tid, kSegThreads);
+    // Rw and the initial potential: 8 rows per warp pass, all loads in flight
+    // before the shared-memory stores.
+    {
+        const double top_g = gamma;
+        for (int k0 = warp * 8; k0 < nz; k0 += nwarps * 8) {
+            double rv[8][4], pv[8][4];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const int k = k0 + r;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const int j = lane + 32 * c;
+                    const bool ok = (k < nz) && (j < nr);
+                    rv[r][c] = ok ? Rs[(long long)nr * k + j] : 0.0;
+                    pv[r][c] = (ok && !a.cold) ? Pg[(long long)numr * (k + 1) + 1 + j] : 0.0;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const int k = k0 + r;
+                if (k >= nz) break;
+                const double side_v = Pg[(numr - 1) + (long long)numr * (k + 1)];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const int j = lane + 32 * c;
+                    if (j >= nr) break;
+                    double r0 = rv[r][c];
+                    if (k == nz - 1) r0 = r0 + top_g * Pg[(j + 1) + (long long)numr * (numz - 1)];
+                    if (!sym_bottom && k == 0) r0 = r0 + gamma * Pg[j + 1];
+                    if (j == nr - 1) r0 = r0 - a_side * side_v;
+                    Rw[k * ps + j] = r0;
+                    Ww[k * ps + j] = pv[r][c];
+                }
+            }
+        }
+        // lines longer than 128: the remaining columns
+        for (int k = warp; k < nz; k += nwarps)
+            for (int j = 128 + lane; j < nr; j += 32) {
+                double r0 = Rs[(long long)nr * k + j];
+                if (k == nz - 1) r0 = r0 + top_g * Pg[(j + 1) + (long long)numr * (numz - 1)];
+                if (!sym_bottom && k == 0) r0 = r0 + gamma * Pg[j + 1];
+                if (j == nr - 1) r0 = r0 - a_side * Pg[(numr - 1) + (long long)numr * (k + 1)];
+                Rw[k * ps + j] = r0;
+                Ww[k * ps + j] = a.cold ? 0.0 : Pg[(long long)numr * (k + 1) + 1 + j];
+            }
+    }
+    __syncthreads();
+
+    const int nitem_r = nz * Pr, nitem_z = nr * Pz;
+    for (int it = 0; it < a.nsteps_run; ++it) {
+        const int step = a.step0 + it;
+        const bool last_step = (it + 1 == a.nsteps_run);
+        const double dtt = a.dt[step];
+        const double dtn = last_step ? dtt : a.dt[step + 1];
+
+        // ================= radial half-sweep: lines k, segments along j =================
+        {
+            const Fac f = fac_view(Fr, nr);
+            double v[kAdiSeg];
+            const bool active = tid < nitem_r;
+            const int k = active ? tid % nz : 0, p = active ? tid / nz : 0;
+            const int j0 = p * kAdiSeg, len = kFull ? kAdiSeg : min(kAdiSeg, nr - j0);
+            double *wr = Ww + k * ps + j0;
+            const double *rr = Rw + k * ps + j0;
+            if (active) {
+                double L = 0.0;
+                if (it == 0) {
+                    // first step: the right-hand side from the initial potential
+                    const bool refl = (k == 0) && sym_bottom;
+                    const double cphi = refl ? dtt - gamma : dtt - 2.0 * gamma;
+                    const double cdn = refl ? 0.0 : 1.0;
+                    const double *pu = (k + 1 < nz) ? wr + ps : zrow + j0;
+                    const double *pd = (k > 0) ? wr - ps : zrow + j0;
+#pragma unroll
+                    for (int i = 0; i < kAdiSeg; ++i)
+                        if (kFull || i < len) {
+                            const double rhs = rr[i] + cphi * wr[i] + gamma * (pu[i] + cdn * pd[i]);
+                            L = rhs * f.ib[j0 + i] - f.dd[j0 + i] * L;
+                            v[i] = L;
+                        }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < kAdiSeg; ++i)
+                        if (kFull || i < len) {
+                            L = wr[i] - f.dd[j0 + i] * L;
+                            v[i] = L;
+                        }
+                }
+                Xa[k + nz * p] = L;
+            }
+            __syncthreads();
+            if (active) {
+                double yin = 0.0;
+                for (int q = 0; q < p; ++q) yin = Xa[k + nz * q] + f.GG[min((q + 1) * kAdiSeg, nr) - 1].x * yin;
+                double M = 0.0;
+#pragma unroll
+                for (int i = kAdiSeg - 1; i >= 0; --i)
+                    if (kFull || i < len) {
+                        const double2 gg = f.GG[j0 + i];
+                        M = (v[i] + gg.x * yin) - gg.y * M;
+                        v[i] = M;
+                    }
+                Xb[k + nz * p] = M;
+            }
+            __syncthreads();
+            if (active) {
+                double xin = 0.0;
+                for (int q = Pr - 1; q > p; --q) xin = Xb[k + nz * q] + f.K[q * kAdiSeg] * xin;
+#pragma unroll
+                for (int i = 0; i < kAdiSeg; ++i)
+                    if (kFull || i < len) v[i] = v[i] + f.K[j0 + i] * xin;
+                Ea[k + nz * p] = v[0];
+#pragma unroll
+                for (int i = 0; i < kAdiSeg; ++i)
+                    if (i == len - 1) Eb[k + nz * p] = v[i];
+            }
+            __syncthreads();
+            if (active) {
+                // vertical right-hand side of this step (helmadi.F90:276-340),
+                // times the vertical 1/bet of row k
+                const double ibz = fac_view(Fz, nz).ib[k];
+                const double left = (p > 0) ? Eb[k + nz * (p - 1)] : 0.0;
+                const double right = (p + 1 < Pr) ? Ea[k + nz * (p + 1)] : 0.0;
+#pragma unroll
+                for (int i = 0; i < kAdiSeg; ++i)
+                    if (kFull || i < len) {
+                        const int j = j0 + i;
+                        const double pl = (i > 0) ? v[i - 1] : left;
+                        const double pr = (kFull ? (i + 1 < kAdiSeg) : (i + 1 < len)) ? v[(i + 1) & (kAdiSeg - 1)]
+                                                                                         : right;
+                        const double2 ab = AB[j];
+                        wr[i] = (rr[i] + (el0[j] + dtt) * v[i] - ab.x * pr - ab.y * pl) * ibz;
+                    }
+            }
+            // the next step's radial factors (Fr is dead until then)
+            if (!last_step) {
+                __syncthreads();  // every reader of Fr is past phase D's ibz load
+                fac_load(Fr, nr, rad + (step + 1) * rad_step, tid, kSegThreads);
+            }
+            __syncthreads();
+        }
+        // ================= vertical half-sweep: lines j, segments along k =================
+        {
+            const Fac f = fac_view(Fz, nz);
+            double v[kAdiSeg];
+            const bool active = tid < nitem_z;
+            const int j = active ? tid % nr : 0, p = active ? tid / nr : 0;
+            const int k0 = p * kAdiSeg, len = kFull ? kAdiSeg : min(kAdiSeg, nz - k0);
+            double *wc = Ww + k0 * ps + j;
+            const double *rc = Rw + k0 * ps + j;
+            if (active) {
+                double L = 0.0;
+#pragma unroll
+                for (int i = 0; i < kAdiSeg; ++i)
+                    if (kFull || i < len) {
+                        L = wc[i * ps] - f.dd[k0 + i] * L;
+                        v[i] = L;
+                    }
+                Xa[j + nr * p] = L;
+            }
+            __syncthreads();
+            if (active) {
+                double yin = 0.0;
+                for (int q = 0; q < p; ++q) yin = Xa[j + nr * q] + f.GG[min((q + 1) * kAdiSeg, nz) - 1].x * yin;
+                double M = 0.0;
+#pragma unroll
+                for (int i = kAdiSeg - 1; i >= 0; --i)
+                    if (kFull || i < len) {
+                        const double2 gg = f.GG[k0 + i];
+                        M = (v[i] + gg.x * yin) - gg.y * M;
+                        v[i] = M;
+                    }
+                Xb[j + nr * p] = M;
+            }
+            __syncthreads();
+            if (active) {
+                double xin = 0.0;
+                for (int q = Pz - 1; q > p; --q) xin = Xb[j + nr * q] + f.K[q * kAdiSeg] * xin;
+#pragma unroll
+                for (int i = 0; i < kAdiSeg; ++i)
+                    if (kFull || i < len) v[i] = v[i] + f.K[k0 + i] * xin;
+                Ea[j + nr * p] = v[0];
+#pragma unroll
+                for (int i = 0; i < kAdiSeg; ++i)
+                    if (i == len - 1) Eb[j + nr * p] = v[i];
+            }
+            __syncthreads();
+            if (active) {
+                if (last_step) {
+#pragma unroll
+                    for (int i = 0; i < kAdiSeg; ++i)
+                        if (kFull || i < len) wc[i * ps] = v[i];
+                } else {
+                    // radial right-hand side of the next step (helmadi.F90:209-256),
+                    // times the next step's radial 1/bet of column j
+                    const double ibr = fac_view(Fr, nr).ib[j];
+                    const double dn_edge = (p > 0) ? Eb[j + nr * (p - 1)] : 0.0;
+                    const double up_edge = (p + 1 < Pz) ? Ea[j + nr * (p + 1)] : 0.0;
+#pragma unroll
+                    for (int i = 0; i < kAdiSeg; ++i)
+                        if (kFull || i < len) {
+                            const int k = k0 + i;
+                            const bool refl = (k == 0) && sym_bottom;
+                            const double up = (kFull ? (i + 1 < kAdiSeg) : (i + 1 < len)) ? v[(i + 1) & (kAdiSeg - 1)]
+                                                                                          : up_edge;
+                            const double dn = (i > 0) ? v[i - 1] : dn_edge;
+                            const double cphi = refl ? dtn - gamma : dtn - 2.0 * gamma;
+                            const double rhs = refl ? rc[i * ps] + cphi * v[i] + gamma * up
+                                                    : rc[i * ps] + cphi * v[i] + gamma * (up + dn);
+                            wc[i * ps] = rhs * ibr;
+                        }
+                }
+            }
+            if (!last_step) {
+                __syncthreads();  // every reader of Fz is past phase C
+                fac_load(Fz, nz, a.ver + (step + 1) * ver_step, tid, kSegThreads);
+            }
+            __syncthreads();
+        }
+    }
+    for (int k = warp; k < nz; k += nwarps) {
+        double *prow = Pg + (long long)numr * (k + 1) + 1;
+#pragma unroll 4
+        for (int j = lane; j < nr; j += 32) prow[j] = Ww[k * ps + j];
+    }
+}
+
 // Weighted (Parseval) squared norms over the interior of the slot array:
 // out[0] = sum w |P - prev|^2, out[1] = sum w |P|^2 (update test), or
 // out[0] = sum w |R - A P|^2, out[1] = sum w |R|^2 (residual).
@@ -240,17 +602,34 @@ k_slot_norms(const double *__restrict__ P, const double *__restrict__ Q, const d
 
 }  // namespace
 
+const void *seg_kernel(int threads, bool full) {
+    if (threads == 256) return full ? (const void *)k_adi_seg<256, true> : (const void *)k_adi_seg<256, false>;
+    if (threads == 384) return full ? (const void *)k_adi_seg<384, true> : (const void *)k_adi_seg<384, false>;
+    return full ? (const void *)k_adi_seg<512, true> : (const void *)k_adi_seg<512, false>;
+}
+
 int adi_configure(bph_ctx *c) {
     int dev_max = 0;
     cudaError_t e = cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
-    size_t onchip = sizeof(double) * 2 * (size_t)c->nz * (size_t)(c->nr | 1) + smalls_bytes(c);
-    if (onchip <= (size_t)dev_max) {
+    const SegLayout L = seg_layout(c->nr, c->nz);
+    const size_t seg_bytes = sizeof(double) * L.doubles;
+    const size_t onchip = sizeof(double) * 2 * (size_t)c->nz * (size_t)(c->nr | 1) + smalls_bytes(c);
+    c->adi_seg = 0;
+    c->adi_smem = 0;
+    const int items = max(c->nz * L.Pr, c->nr * L.Pz);
+    const int threads = (items <= 256) ? 256 : (items <= 384) ? 384 : 512;
+    if (seg_bytes <= (size_t)dev_max && items <= 512) {
+        c->adi_seg = threads;
+        c->adi_full = (c->nr % kAdiSeg == 0) && (c->nz % kAdiSeg == 0);
+        c->adi_smem = (int)seg_bytes;
+        const void *fn = seg_kernel(c->adi_seg, c->adi_full);
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, c->adi_smem);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_adi_seg)");
+    } else if (onchip <= (size_t)dev_max) {
         c->adi_smem = (int)onchip;
         e = cudaFuncSetAttribute(k_adi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, c->adi_smem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_adi)");
-    } else {
-        c->adi_smem = 0;
     }
     return BPH_OK;
 }
@@ -277,7 +656,11 @@ cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_ru
     a.cold = cold ? 1 : 0;
     a.gamma = c->gamma;
     ++c->launches;
-    if (c->adi_smem > 0)
+    if (c->adi_seg) {
+        void *args[] = {&a};
+        return cudaLaunchKernel(seg_kernel(c->adi_seg, c->adi_full), dim3(c->N), dim3(c->adi_seg), args,
+                                (size_t)c->adi_smem, c->stream);
+    } else if (c->adi_smem > 0)
         k_adi<true><<<c->N, kAdiThreads, c->adi_smem, c->stream>>>(a);
     else
         k_adi<false><<<c->N, kAdiThreads, smalls_bytes(c), c->stream>>>(a);

@@ -163,8 +163,8 @@ int get_schedule(bph_ctx *c, int nsteps, Schedule **out) {
     dt_schedule(h, c->g.numr, nsteps, s.h_dt);
     int rc;
     if ((rc = dev_alloc(c, &s.d_dt, nsteps))) return rc;
-    if ((rc = dev_alloc(c, &s.d_rad, (size_t)nsteps * c->N * 3 * c->nr))) return rc;
-    if ((rc = dev_alloc(c, &s.d_ver, (size_t)nsteps * 3 * c->nz))) return rc;
+    if ((rc = dev_alloc(c, &s.d_rad, (size_t)nsteps * c->N * kAdiFactors * c->nr))) return rc;
+    if ((rc = dev_alloc(c, &s.d_ver, (size_t)nsteps * kAdiFactors * c->nz))) return rc;
     BPH_CUDA(cudaMemcpyAsync(s.d_dt, s.h_dt, sizeof(double) * nsteps, cudaMemcpyHostToDevice, c->stream));
     s.nsteps = nsteps;
     BPH_CUDA(launch_adi_factors(c, s));
@@ -302,6 +302,13 @@ int setup_impl(bph_ctx *c) {
     BPH_CUDA(launch_green_tables(c));
     if ((rc = fft_configure(c))) return rc;
     if ((rc = adi_configure(c))) return rc;
+    if ((rc = contract_configure(c))) return rc;
+    {
+        const size_t groups = (size_t)(c->nb + 7) / 8;
+        if ((rc = dev_alloc(c, &c->d_ccnt, (size_t)g.mmax * groups))) return rc;
+        if ((rc = dev_alloc(c, &c->d_cpart, (size_t)c->contract_split * g.mmax * c->nb * 2))) return rc;
+        BPH_CUDA(cudaMemsetAsync(c->d_ccnt, 0, sizeof(unsigned int) * (size_t)g.mmax * groups, c->stream));
+    }
     if (c->adi_smem == 0) {
         if ((rc = dev_alloc(c, &c->d_W, (size_t)c->N * c->nplane))) return rc;
     }
@@ -416,6 +423,8 @@ int bph_destroy(bph_ctx_t *c) {
     dev_free(c->d_tw2);
     dev_free(c->d_ph);
     dev_free(c->d_status);
+    dev_free(c->d_ccnt);
+    dev_free(c->d_cpart);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return BPH_OK;

@@ -16,6 +16,8 @@
 // that transform is exact in closed form:
 //   F_0 = N factor S_C0,  F_k = e^{-i pi k/N} N factor (S_Cm + i S_Sm),
 // and zero at every other frequency, so the slots are written directly.
+#include <cmath>
+
 #include "bph_internal.cuh"
 
 namespace bph {
@@ -24,13 +26,23 @@ namespace {
 constexpr int kContractRows = 8;
 constexpr int kContractThreads = 256;
 
+// Grid (row groups, mmax, nsplit).  CTA (g, m, k) reduces table rows
+// b0..b0+7 of mode m over the k-th slice of the interior zones; the number
+// of slices is chosen at setup so that the launch fills whole waves of the
+// GPU.  Slices write partial sums, and the last CTA of each (m, group) to
+// arrive adds them in slice order (deterministic) and writes S; it also
+// resets its arrival counter for the next launch.
 template <bool kVec>
-__global__ void __launch_bounds__(kContractThreads)
+__global__ void __launch_bounds__(kContractThreads, 2)
 k_green_contract(const double *__restrict__ G, const double *__restrict__ mom, double *__restrict__ S,
-                 long long np, int nb) {
-    const int m = blockIdx.y;
+                 long long np, int nb, unsigned int *__restrict__ counters, double *__restrict__ partials) {
+    const int m = blockIdx.y, split = blockIdx.z, nsplit = gridDim.z;
     const int b0 = blockIdx.x * kContractRows;
     const int nrows = min(kContractRows, nb - b0);
+    // slice bounds in units of 2 doubles (16-byte loads) when vectorised
+    const long long unit = kVec ? 2 : 1, nu = np / unit;
+    const long long chunk = (nu + nsplit - 1) / nsplit;
+    const long long u0 = split * chunk, u1 = min(nu, u0 + chunk);
     const double *mc = mom + (2LL * m) * np;
     const double *ms = mom + (2LL * m + 1) * np;
     const double *g0 = G + ((long long)m * nb + b0) * np;
@@ -38,37 +50,37 @@ k_green_contract(const double *__restrict__ G, const double *__restrict__ mom, d
 #pragma unroll
     for (int r = 0; r < kContractRows; ++r) ac[r] = as[r] = 0.0;
     if (kVec) {
-        const long long n2 = np / 2;
         const double2 *mc2 = reinterpret_cast<const double2 *>(mc);
         const double2 *ms2 = reinterpret_cast<const double2 *>(ms);
-        for (long long i = threadIdx.x; i < n2; i += kContractThreads) {
-            double2 vc = __ldg(mc2 + i), vs = __ldg(ms2 + i);
+        for (long long i = u0 + threadIdx.x; i < u1; i += kContractThreads) {
+            double2 g[kContractRows];
+#pragma unroll
+            for (int r = 0; r < kContractRows; ++r)
+                g[r] = (r < nrows) ? __ldcs(reinterpret_cast<const double2 *>(g0 + r * np) + i) : make_double2(0.0, 0.0);
+            const double2 vc = __ldg(mc2 + i), vs = __ldg(ms2 + i);
 #pragma unroll
             for (int r = 0; r < kContractRows; ++r) {
-                if (r < nrows) {
-                    double2 g = __ldcs(reinterpret_cast<const double2 *>(g0 + r * np) + i);
-                    ac[r] = fma(g.x, vc.x, ac[r]);
-                    ac[r] = fma(g.y, vc.y, ac[r]);
-                    as[r] = fma(g.x, vs.x, as[r]);
-                    as[r] = fma(g.y, vs.y, as[r]);
-                }
+                ac[r] = fma(g[r].x, vc.x, ac[r]);
+                ac[r] = fma(g[r].y, vc.y, ac[r]);
+                as[r] = fma(g[r].x, vs.x, as[r]);
+                as[r] = fma(g[r].y, vs.y, as[r]);
             }
         }
     } else {
-        for (long long i = threadIdx.x; i < np; i += kContractThreads) {
-            double vc = __ldg(mc + i), vs = __ldg(ms + i);
+        for (long long i = u0 + threadIdx.x; i < u1; i += kContractThreads) {
+            const double vc = __ldg(mc + i), vs = __ldg(ms + i);
 #pragma unroll
             for (int r = 0; r < kContractRows; ++r) {
                 if (r < nrows) {
-                    double g = __ldcs(g0 + r * np + i);
+                    const double g = __ldcs(g0 + r * np + i);
                     ac[r] = fma(g, vc, ac[r]);
                     as[r] = fma(g, vs, as[r]);
                 }
             }
         }
     }
-    // Warp then CTA reduction in a fixed order.
     __shared__ double red[kContractThreads / 32][2 * kContractRows];
+    __shared__ bool last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int r = 0; r < kContractRows; ++r) {
@@ -86,13 +98,34 @@ k_green_contract(const double *__restrict__ G, const double *__restrict__ mom, d
         }
     }
     __syncthreads();
+    const long long slice_stride = (long long)gridDim.y * nb * 2;
+    double v = 0.0;
     if (threadIdx.x < 2 * nrows) {
-        double v = 0.0;
 #pragma unroll
         for (int w = 0; w < kContractThreads / 32; ++w) v += red[w][threadIdx.x];
-        int r = threadIdx.x >> 1, cs = threadIdx.x & 1;
-        S[((long long)m * nb + b0 + r) * 2 + cs] = (m == 0 && cs == 1) ? 0.0 : v;
     }
+    if (nsplit == 1) {
+        if (threadIdx.x < 2 * nrows) {
+            const int r = threadIdx.x >> 1, cs = threadIdx.x & 1;
+            S[((long long)m * nb + b0 + r) * 2 + cs] = (m == 0 && cs == 1) ? 0.0 : v;
+        }
+        return;
+    }
+    if (threadIdx.x < 2 * nrows) partials[split * slice_stride + ((long long)m * nb + b0) * 2 + threadIdx.x] = v;
+    __threadfence();
+    __syncthreads();
+    const int tile = m * gridDim.x + blockIdx.x;
+    if (threadIdx.x == 0) last = (atomicAdd(counters + tile, 1u) == (unsigned)(nsplit - 1));
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x < 2 * nrows) {
+        double t = 0.0;
+        for (int k = 0; k < nsplit; ++k) t += __ldcg(partials + k * slice_stride + ((long long)m * nb + b0) * 2 + threadIdx.x);
+        const int r = threadIdx.x >> 1, cs = threadIdx.x & 1;
+        S[((long long)m * nb + b0 + r) * 2 + cs] = (m == 0 && cs == 1) ? 0.0 : t;
+    }
+    if (threadIdx.x == 0) counters[tile] = 0u;
 }
 
 // One thread per (boundary row b, slot s); rows nb.. write the corner
@@ -136,13 +169,41 @@ __global__ void k_boundary_slots(const double *__restrict__ S, const double2 *__
 
 }  // namespace
 
+int contract_configure(bph_ctx *c) {
+    int sms = 0, per_sm = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_green_contract<true>, kContractThreads, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    const long long slots = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    const long long tiles = (long long)c->g.mmax * ((c->nb + kContractRows - 1) / kContractRows);
+    // smallest slice count whose last wave is >= 90% full, at least 2048 zones per slice
+    int best = 1;
+    double best_eff = 0.0;
+    for (int k = 1; k <= 16; ++k) {
+        if (k > 1 && c->np / k < 2048) break;
+        double waves = (double)(tiles * k) / (double)slots;
+        double eff = waves / std::ceil(waves);
+        if (eff > best_eff + 1e-9) {
+            best_eff = eff;
+            best = k;
+        }
+        if (eff >= 0.9) break;
+    }
+    c->contract_split = best;
+    return BPH_OK;
+}
+
 cudaError_t launch_green_contract(bph_ctx *c) {
-    dim3 grid((unsigned)((c->nb + kContractRows - 1) / kContractRows), (unsigned)c->g.mmax);
+    dim3 grid((unsigned)((c->nb + kContractRows - 1) / kContractRows), (unsigned)c->g.mmax,
+              (unsigned)c->contract_split);
     ++c->launches;
     if (c->np % 2 == 0)
-        k_green_contract<true><<<grid, kContractThreads, 0, c->stream>>>(c->d_green, c->d_mom, c->d_S, c->np, c->nb);
+        k_green_contract<true><<<grid, kContractThreads, 0, c->stream>>>(c->d_green, c->d_mom, c->d_S, c->np, c->nb,
+                                                                        c->d_ccnt, c->d_cpart);
     else
-        k_green_contract<false><<<grid, kContractThreads, 0, c->stream>>>(c->d_green, c->d_mom, c->d_S, c->np, c->nb);
+        k_green_contract<false><<<grid, kContractThreads, 0, c->stream>>>(c->d_green, c->d_mom, c->d_S, c->np, c->nb,
+                                                                         c->d_ccnt, c->d_cpart);
     return cudaGetLastError();
 }
 

@@ -1,8 +1,8 @@
 // bph_fft.cu -- azimuthal real FFTs (realft.F90 + the slot reorder of
 // helmadi.F90:132-183 and its inverse :357-411).
 //
-// A CTA takes a tile of 32 consecutive (J,K) columns and all numphi samples
-// of each: every row of the tile is a 256-byte coalesced segment of the
+// A CTA takes a tile of 16 consecutive (J,K) columns and all numphi samples
+// of each: every row of the tile is a 128-byte coalesced segment of the
 // Fortran array (J fastest).  The N real samples of a column are packed as
 // M = N/2 complex values in shared memory, transformed by in-place Stockham
 // radix-4 (and one radix-2) passes -- each pass loads its butterfly inputs
@@ -19,7 +19,7 @@
 namespace bph {
 namespace {
 
-constexpr int kTile = 32;  // columns per CTA
+constexpr int kTile = 16;  // columns per CTA (128-byte coalesced rows)
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -95,7 +95,7 @@ __device__ __forceinline__ void fft_tile(double2 *C, const double2 *tw) {
 
 template <int M>
 struct FftShape {
-    static constexpr int kThreads = (M >= 256) ? 512 : 256;
+    static constexpr int kThreads = (M >= 256) ? 256 : 128;
     static constexpr size_t kSmem = sizeof(double2) * ((size_t)M * kTile + M + (M + 1));
 };
 
@@ -121,20 +121,29 @@ k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__re
     const long long p0 = (long long)blockIdx.x * kTile;
     for (int i = tid; i < M; i += NT) tw[i] = g_tw[i];
     for (int i = tid; i <= M; i += NT) tw2[i] = g_tw2[i];
-    // Load: thread -> (column c, sample pair n).
+    // Load: thread -> (column c fixed, sample pairs n = n0, n0 + NT/kTile, ...);
+    // all global loads are issued before any shared-memory store.
+    static_assert(NT % kTile == 0, "threads must cover whole tile rows");
+    constexpr int kRowsPerPass = NT / kTile, kLoads = M / kRowsPerPass;
     bool bad = false;
-    for (int it = tid; it < kTile * M; it += NT) {
-        int c = it % kTile, n = it / kTile;
-        long long p = p0 + c;
-        double2 v = make_double2(0.0, 0.0);
-        if (p < np) {
-            int jz = (int)(p % nr) + 1, kz = (int)(p / nr) + 1;
-            const double *col = src + jz + (long long)numr * kz;
-            v.x = __ldg(col + nplane * (2 * n));
-            v.y = __ldg(col + nplane * (2 * n + 1));
-            if (kRho) bad |= !(isfinite(v.x) && isfinite(v.y));
+    {
+        const int c = tid % kTile, n0 = tid / kTile;
+        const long long p = p0 + c;
+        const bool valid = p < np;
+        const double *col = src;
+        if (valid) col = src + ((int)(p % nr) + 1) + (long long)numr * ((int)(p / nr) + 1);
+        double2 v[kLoads];
+#pragma unroll
+        for (int i = 0; i < kLoads; ++i) {
+            const int n = n0 + i * kRowsPerPass;
+            v[i] = valid ? make_double2(__ldg(col + nplane * (2 * n)), __ldg(col + nplane * (2 * n + 1)))
+                         : make_double2(0.0, 0.0);
         }
-        C[n * kTile + c] = v;
+#pragma unroll
+        for (int i = 0; i < kLoads; ++i) {
+            if (kRho) bad |= !(isfinite(v[i].x) && isfinite(v[i].y));
+            C[(n0 + i * kRowsPerPass) * kTile + c] = v[i];
+        }
     }
     if (kRho && bad) atomicOr(status, kStatusNonFinite);
     __syncthreads();
@@ -240,26 +249,41 @@ k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 
     const long long q0 = (long long)blockIdx.x * kTile;
     for (int i = tid; i < M; i += NT) tw[i] = g_tw[i];
     for (int i = tid; i <= M; i += NT) tw2[i] = g_tw2[i];
-    // Load slots: thread -> (column c, slot pair (k, M+k)).
-    for (int it = tid; it < kTile * M; it += NT) {
-        int c = it % kTile, k = it / kTile;
-        long long q = q0 + c;
-        double2 v = make_double2(0.0, 0.0);
-        if (q < nplane) {
-            int jz = (int)(q % numr), kz = (int)(q / numr);
-            bool flip = (jz == 0) && (isym != 3) && (k & 1);
-            int js = (jz == 0) ? 1 : jz;
-            int ks = (kz == 0 && isym != 1) ? 1 : kz;
-            const double *col = P + js + (long long)numr * ks;
-            double a = __ldg(col + nplane * k), b = __ldg(col + nplane * (M + k));
-            if (k == 0) {
-                v = make_double2(a, b);  // (F_0, F_M): both real
-            } else {
-                v = make_double2(a, -b);  // F_k = slot_k - i slot_{M+k}
-                if (flip) v = make_double2(-v.x, -v.y);
-            }
+    // Load slots: thread -> (column c fixed, slot pairs (k, M+k)); all global
+    // loads are issued before any shared-memory store.
+    constexpr int kRowsPerPass = NT / kTile, kLoads = M / kRowsPerPass;
+    {
+        const int c = tid % kTile, k0 = tid / kTile;
+        const long long q = q0 + c;
+        const bool valid = q < nplane;
+        int jz = 0, kz = 0;
+        if (valid) {
+            jz = (int)(q % numr);
+            kz = (int)(q / numr);
         }
-        C[k * kTile + c] = v;
+        const int js = (jz == 0) ? 1 : jz;
+        const int ks = (kz == 0 && isym != 1) ? 1 : kz;
+        const bool axis = valid && (jz == 0) && (isym != 3);
+        const double *col = P + js + (long long)numr * ks;
+        double a[kLoads], b[kLoads];
+#pragma unroll
+        for (int i = 0; i < kLoads; ++i) {
+            const int k = k0 + i * kRowsPerPass;
+            a[i] = valid ? __ldg(col + nplane * k) : 0.0;
+            b[i] = valid ? __ldg(col + nplane * (M + k)) : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < kLoads; ++i) {
+            const int k = k0 + i * kRowsPerPass;
+            double2 v;
+            if (k == 0) {
+                v = make_double2(a[i], b[i]);  // (F_0, F_M): both real
+            } else {
+                v = make_double2(a[i], -b[i]);  // F_k = slot_k - i slot_{M+k}
+                if (axis && (k & 1)) v = make_double2(-v.x, -v.y);
+            }
+            C[k * kTile + c] = v;
+        }
     }
     __syncthreads();
     // Pre-process into Z_k = E_k + i O_k.
@@ -283,13 +307,19 @@ k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 
     __syncthreads();
     fft_tile<M, -1, NT>(C, tw);
     const double scale = 1.0 / (double)M;
-    for (int it = tid; it < kTile * M; it += NT) {
-        int c = it % kTile, n = it / kTile;
-        long long q = q0 + c;
-        if (q >= nplane) continue;
-        double2 z = C[n * kTile + c];
-        pot[q + nplane * (2 * n)] = z.x * scale;
-        pot[q + nplane * (2 * n + 1)] = z.y * scale;
+    {
+        const int c = tid % kTile, n0 = tid / kTile;
+        const long long q = q0 + c;
+        if (q < nplane) {
+            double *col = pot + q;
+#pragma unroll
+            for (int i = 0; i < kLoads; ++i) {
+                const int n = n0 + i * kRowsPerPass;
+                const double2 z = C[n * kTile + c];
+                col[nplane * (2 * n)] = z.x * scale;
+                col[nplane * (2 * n + 1)] = z.y * scale;
+            }
+        }
     }
 }
 

@@ -34,11 +34,16 @@ constexpr int kNumSchedules = 3;       // 5 steps (warm), 20 steps (cold), one c
 // Deferred device status bits (d_status).
 constexpr int kStatusNonFinite = 1;
 
+// Segment length of the partitioned line solves in the on-chip ADI kernel.
+constexpr int kAdiSeg = 32;
+// Factor arrays per line system: 1/bet, a/bet, gam, forward carry, backward carry.
+constexpr int kAdiFactors = 5;
+
 struct Schedule {
     int nsteps = 0;
     double *d_dt = nullptr;   // [nsteps]
-    double *d_rad = nullptr;  // [nsteps][N][3][nr]: 1/bet, ar/bet, gam (radial Thomas)
-    double *d_ver = nullptr;  // [nsteps][3][nz]:    1/bet, az/bet, gam (vertical Thomas)
+    double *d_rad = nullptr;  // [nsteps][N][kAdiFactors][nr] radial Thomas factors
+    double *d_ver = nullptr;  // [nsteps][kAdiFactors][nz]    vertical Thomas factors
     double *h_dt = nullptr;   // host copy of the dt schedule
 };
 
@@ -81,8 +86,13 @@ struct bph_ctx {
     double *d_rho_stage = nullptr;
     double *d_pot_stage = nullptr;
     int *d_status = nullptr;
+    unsigned int *d_ccnt = nullptr;  // contraction arrival counters [mmax][row groups]
+    double *d_cpart = nullptr;       // contraction partial sums [split][mmax][nb][2]
+    int contract_split = 1;
 
     int adi_smem = 0;            // dynamic shared bytes of the on-chip ADI kernel (0: global variant)
+    int adi_seg = 0;             // threads of the segmented on-chip ADI kernel (0: not used)
+    bool adi_full = false;       // both line lengths are multiples of the segment length
     int adi_threads = 256;
     int fft_smem_fwd = 0, fft_smem_inv = 0;
     bool have_warm = false;
@@ -117,6 +127,7 @@ cudaError_t launch_update_norm(bph_ctx *c, double *d_out);
 cudaError_t launch_residual_norm(bph_ctx *c, double *d_out);
 
 int adi_configure(bph_ctx *c);
+int contract_configure(bph_ctx *c);
 int fft_configure(bph_ctx *c);
 
 }  // namespace bph

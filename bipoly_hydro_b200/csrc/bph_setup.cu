@@ -211,8 +211,32 @@ __global__ void k_green_tables(const double *__restrict__ grid, const double *__
 
 // Thomas factorisations for one ADI schedule (tridagr.F90:41-60,
 // tridagz.F90:115-132).  Radial: one thread per (step, slot); vertical: one
-// thread per step.  Stored as 1/bet, a/bet and gam so that the solve is
-//   y_j = w_j/bet_j - (a_j/bet_j) y_{j-1},  x_j = y_j - gam_{j+1} x_{j+1}.
+// thread per step.  For a line of n unknowns, five arrays of n:
+//   f[0] = 1/bet_j, f[1] = a_j/bet_j, f[2] = gam_j     (Thomas:
+//     y_j = w_j/bet_j - (a_j/bet_j) y_{j-1},  x_j = y_j - gam_{j+1} x_{j+1})
+//   f[3] = forward carry  G_j = prod_{i=s..j} (-a_i/bet_i)
+//   f[4] = backward carry K_j = prod_{i=j+1..e+1} (-gam_i), gam_n = 0
+// with [s, e] the kAdiSeg-long segment holding j: a segment solved with a
+// zero carry-in gives L (or M), and the true values are L + G y_{s-1}
+// (or M + K x_{e+1}).
+__device__ void line_carries(double *f, int n) {
+    double *dd = f + n, *gam = f + 2 * n, *G = f + 3 * n, *K = f + 4 * n;
+    for (int s0 = 0; s0 < n; s0 += kAdiSeg) {
+        int e0 = min(s0 + kAdiSeg, n) - 1;
+        double g = 1.0;
+        for (int j = s0; j <= e0; ++j) {
+            g = -dd[j] * g;
+            G[j] = g;
+        }
+        double k = 1.0;
+        for (int j = e0; j >= s0; --j) {
+            double gnext = (j + 1 < n) ? gam[j + 1] : 0.0;
+            k = -gnext * k;
+            K[j] = k;
+        }
+    }
+}
+
 __global__ void k_adi_factors(const double *__restrict__ dt, int nsteps, const double *__restrict__ brb,
                               const double *__restrict__ alphar, const double *__restrict__ betar,
                               const double *__restrict__ bzb, double gamma, double *__restrict__ rad,
@@ -223,7 +247,7 @@ __global__ void k_adi_factors(const double *__restrict__ dt, int nsteps, const d
         int step = t / N, s = t % N;
         double dtt = dt[step];
         const double *b = brb + (long long)s * numr;
-        double *o = rad + ((long long)step * N + s) * 3 * nr;
+        double *o = rad + ((long long)step * N + s) * kAdiFactors * nr;
         double bet = b[1] + dtt;  // J = 2
         o[0] = 1.0 / bet;
         o[nr] = 0.0;
@@ -237,11 +261,12 @@ __global__ void k_adi_factors(const double *__restrict__ dt, int nsteps, const d
             o[nr + j] = betar[J - 1] * ib;
             o[2 * nr + j] = gam;
         }
+        line_carries(o, nr);
     } else if (t < nsteps * N + nsteps) {
         int step = t - nsteps * N;
         double dtt = dt[step];
         const double az = -gamma, cz = -gamma;
-        double *o = ver + (long long)step * 3 * nz;
+        double *o = ver + (long long)step * kAdiFactors * nz;
         double bet = bzb[1] + dtt;  // K = 2
         o[0] = 1.0 / bet;
         o[nz] = 0.0;
@@ -255,6 +280,7 @@ __global__ void k_adi_factors(const double *__restrict__ dt, int nsteps, const d
             o[nz + k] = az * ib;
             o[2 * nz + k] = gam;
         }
+        line_carries(o, nz);
     }
 }
 
