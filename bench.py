@@ -158,14 +158,21 @@ def dist_setup():
 
 
 def max_over_ranks(x: float, world: int) -> float:
+    """Max of a per-rank value (device time of the timed region) over ranks."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(units_per_rank: int, world: int, ms_max: float) -> float:
+    """Whole-job throughput: units all ranks processed / the slowest rank's time."""
+    return world * units_per_rank / (ms_max / 1e3)
 
 
 def barrier(world: int):
@@ -298,7 +305,7 @@ def run_gpu(args, world, rank, local):
     solver.synchronize()
     ms_total = max_over_ranks(e0.elapsed_time(e1), world)
     ms_per_step = ms_total / args.steps
-    value = world * args.steps / (ms_total / 1e3)
+    value = job_rate(args.steps, world, ms_total)
     clocks = clk.summary()
 
     # ---- per-phase kernel times (CUDA events on the launch stream) ------
@@ -362,7 +369,7 @@ def run_gpu(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     ms_e2e = max_over_ranks(e2.elapsed_time(e3), world)
-    e2e_value = world * n_e2e / (ms_e2e / 1e3)
+    e2e_value = job_rate(n_e2e, world, ms_e2e)
 
     # ---- CPU baseline (rank 0, N = 1 only) ------------------------------
     cpu = None

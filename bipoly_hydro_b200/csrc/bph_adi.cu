@@ -38,6 +38,9 @@ struct AdiArgs {
     const double *elz;      // [N][numr]
     const double *alphar;   // [numr]
     const double *betar;    // [numr]
+    const double *brb;      // [N][numr] (defect form: residual)
+    const double *bzb;      // [numz]    (defect form: residual)
+    double *norms;          // [N][2]    (defect form: |delta|^2, |phi|^2 per slot)
     int numr, numz, nr, nz, N, isym;
     int step0, nsteps_run, cold;
     double gamma;
@@ -202,18 +205,31 @@ size_t smalls_bytes(const bph_ctx *c) { return sizeof(double) * (size_t)(9 * c->
 // The per-element arithmetic is the Thomas algorithm of tridagr/tridagz; the
 // carries only re-associate it (results agree to rounding).
 
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<double> {
+    using type = double2;
+    static __device__ __forceinline__ double2 make(double a, double b) { return make_double2(a, b); }
+};
+template <>
+struct Vec2<float> {
+    using type = float2;
+    static __device__ __forceinline__ float2 make(float a, float b) { return make_float2(a, b); }
+};
+
 struct SegLayout {
     int ps, Pr, Pz, xsz;
-    int fsz;                  // doubles of one direction's factor block
-    size_t doubles;
+    int fsz;                  // elements of one direction's factor block
+    size_t elems;             // elements of type T in the whole layout
 };
 
 // Factor block of one direction, n = line length, in shared memory:
 //   ib[n]   1/bet_j
 //   dd[n]   a_j/bet_j
-//   GG[n]   double2 (G_j, gam_{j+1})   forward carry and next back-substitution factor
+//   GG[n]   pairs (G_j, gam_{j+1})   forward carry and next back-substitution factor
 //   K[n]    backward carry
-__host__ __device__ inline int factor_block(int n) { return 5 * n + 1; }  // +1: 16-byte alignment of GG
+__host__ __device__ inline int factor_block(int n) { return 5 * n + 2; }  // +2: pair alignment
 
 __host__ __device__ inline SegLayout seg_layout(int nr, int nz) {
     SegLayout L;
@@ -222,91 +238,112 @@ __host__ __device__ inline SegLayout seg_layout(int nr, int nz) {
     L.Pz = (nz + kAdiSeg - 1) / kAdiSeg;
     L.xsz = max(nz * L.Pr, nr * L.Pz);
     L.fsz = factor_block(max(nr, nz));
-    L.doubles = 2 * (size_t)nz * L.ps + 2 * (size_t)L.fsz + 4 * (size_t)L.xsz + 5 * (size_t)nr + 2;
+    L.elems = 2 * (size_t)nz * L.ps + 2 * (size_t)L.fsz + 4 * (size_t)L.xsz + 5 * (size_t)nr + 4;
     return L;
 }
 
+template <typename T>
+__device__ inline T *align_pair(T *p) {
+    using P2 = typename Vec2<T>::type;
+    while ((reinterpret_cast<uintptr_t>(p) % sizeof(P2)) != 0) ++p;
+    return p;
+}
+
+template <typename T>
 struct Fac {
-    const double *ib, *dd, *K;
-    const double2 *GG;
+    const T *ib, *dd, *K;
+    const typename Vec2<T>::type *GG;
 };
 
-__device__ inline Fac fac_view(const double *base, int n) {
-    Fac f;
+template <typename T>
+__device__ inline Fac<T> fac_view(const T *base, int n) {
+    Fac<T> f;
     f.ib = base;
     f.dd = base + n;
-    const double *g = base + 2 * n;
-    if ((reinterpret_cast<uintptr_t>(g) & 15) != 0) ++g;
-    f.GG = reinterpret_cast<const double2 *>(g);
+    const T *g = align_pair(const_cast<T *>(base + 2 * n));
+    f.GG = reinterpret_cast<const typename Vec2<T>::type *>(g);
     f.K = g + 2 * n;
     return f;
 }
 
-// Copies one direction's factors [ib, dd, gam, G, K] (global) into a block.
-__device__ inline void fac_load(double *base, int n, const double *src, int tid, int nthreads) {
-    double *ib = base, *dd = base + n;
-    double *g = base + 2 * n;
-    if ((reinterpret_cast<uintptr_t>(g) & 15) != 0) ++g;
-    double2 *GG = reinterpret_cast<double2 *>(g);
-    double *K = g + 2 * n;
+// Copies one direction's factors [ib, dd, gam, G, K] (global FP64) into a block.
+template <typename T>
+__device__ inline void fac_load(T *base, int n, const double *src, int tid, int nthreads) {
+    T *ib = base, *dd = base + n;
+    T *g = align_pair(base + 2 * n);
+    auto *GG = reinterpret_cast<typename Vec2<T>::type *>(g);
+    T *K = g + 2 * n;
     for (int j = tid; j < n; j += nthreads) {
-        ib[j] = src[j];
-        dd[j] = src[n + j];
-        GG[j] = make_double2(src[3 * n + j], (j + 1 < n) ? src[2 * n + j + 1] : 0.0);
-        K[j] = src[4 * n + j];
+        ib[j] = (T)src[j];
+        dd[j] = (T)src[n + j];
+        GG[j] = Vec2<T>::make((T)src[3 * n + j], (T)((j + 1 < n) ? src[2 * n + j + 1] : 0.0));
+        K[j] = (T)src[4 * n + j];
     }
 }
 
-// Shared-memory layout (doubles):
+// The ADI of one Fourier slot per CTA, all steps on chip.
+//
+// kDefect = false (FP64 drop-in, T = double): nsteps Peaceman-Rachford steps
+//   on the potential itself, from the initial potential P (or zero).
+// kDefect = true (mixed precision, T = float): one refinement cycle.  The
+//   prologue forms the FP64 residual r = -4 pi rho_hat - A phi of the current
+//   potential (boundary columns included); the steps run in T on the defect
+//   equation A delta = r from delta = 0 with zero Dirichlet data; the
+//   epilogue adds delta to phi in FP64 and records |delta|^2, |phi|^2.
+//
+// Shared-memory layout (elements of T):
 //   Ww  nz x ps  the line systems' right-hand sides, pre-multiplied by the
 //                sweep's 1/bet: at the start of a step the radial one
-//                (step 0: the initial potential), after the radial sweep the
-//                vertical one, after the last sweep phi.
-//   Rw  nz x ps  -4 pi rho_hat plus every Dirichlet term, folded in once:
-//                +gamma*top (K = numz-1), -alphar(numr-1)*side (J = numr-1),
-//                +gamma*bottom (K = 2, isym 1).  Both sweeps add exactly these
-//                terms (helmadi.F90:252-256, 327-340, and the K+1 / J+1
-//                neighbours of :224-245 / :296-319), so the sweeps see a zero
-//                frame and need no boundary branches.
+//                (drop-in step 0: the initial potential), after the radial
+//                sweep the vertical one, after the last sweep the solution.
+//   Rw  nz x ps  the source: -4 pi rho_hat plus every Dirichlet term, folded
+//                in once (drop-in): +gamma*top (K = numz-1),
+//                -alphar(numr-1)*side (J = numr-1), +gamma*bottom (K = 2,
+//                isym 1) -- both sweeps add exactly these terms
+//                (helmadi.F90:252-256, 327-340 and the K+1 / J+1 neighbours
+//                of :224-245 / :296-319) -- or the residual r (defect form);
+//                either way the sweeps see a zero frame.
 //   Fr, Fz  radial / vertical factor blocks
 //   Xa, Xb, Ea, Eb  per (line, segment) exchange: forward ends, backward
 //                starts, first and last solution values
-//   el0 [nr], AB [nr] double2 (alphaz, betaz), zrow [nr]
+//   el0 [nr], AB [nr] pairs (alphaz, betaz), zrow [nr]
 //
 // One half-sweep, threads = (line, segment), phases separated by barriers:
 //   A  forward elimination with zero carry-in, values kept in registers;
 //   B  carry-in folded from preceding segments, fix-up, backward elimination;
 //   C  carry-in folded from following segments: the line's solution, still
 //      in registers; segment edges published;
-//   D  the other direction's right-hand side (or phi after the last step)
-//      from the registers and the published edges, written to Ww.
+//   D  the other direction's right-hand side (or the solution after the last
+//      step) from the registers and the published edges, written to Ww.
 // The per-element arithmetic is the Thomas algorithm of tridagr/tridagz; the
 // segment carries only re-associate it (results agree to rounding).
-template <int kSegThreads, bool kFull>
-__global__ void __launch_bounds__(kSegThreads, 1) k_adi_seg(AdiArgs a) {
-    extern __shared__ double sm[];
+template <typename T, int kSegThreads, bool kFull, bool kDefect>
+__global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArgs a) {
+    using T2 = typename Vec2<T>::type;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T *sm = reinterpret_cast<T *>(smraw);
     const int s = blockIdx.x, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = kSegThreads / 32;
     const int nr = a.nr, nz = a.nz, numr = a.numr, numz = a.numz;
     const SegLayout Lo = seg_layout(nr, nz);
     const int ps = Lo.ps, Pr = Lo.Pr, Pz = Lo.Pz;
-    double *Ww = sm;
-    double *Rw = Ww + (size_t)nz * ps;
-    double *Fr = Rw + (size_t)nz * ps;
-    double *Fz = Fr + Lo.fsz;
-    double *Xa = Fz + Lo.fsz;
-    double *Xb = Xa + Lo.xsz;
-    double *Ea = Xb + Lo.xsz;
-    double *Eb = Ea + Lo.xsz;
-    double *el0 = Eb + Lo.xsz;
-    double *abp = el0 + nr;
-    if ((reinterpret_cast<uintptr_t>(abp) & 15) != 0) ++abp;
-    double2 *AB = reinterpret_cast<double2 *>(abp);
-    double *zrow = abp + 2 * nr;
+    T *Ww = sm;
+    T *Rw = Ww + (size_t)nz * ps;
+    T *Fr = Rw + (size_t)nz * ps;
+    T *Fz = Fr + Lo.fsz;
+    T *Xa = Fz + Lo.fsz;
+    T *Xb = Xa + Lo.xsz;
+    T *Ea = Xb + Lo.xsz;
+    T *Eb = Ea + Lo.xsz;
+    T *el0 = Eb + Lo.xsz;
+    T *abp = align_pair(el0 + nr);
+    T2 *AB = reinterpret_cast<T2 *>(abp);
+    T *zrow = abp + 2 * nr;
     const long long nplane = (long long)numr * numz;
     double *Pg = a.P + (long long)s * nplane;
     const double *Rs = a.R + (long long)s * nr * nz;
     const double gamma = a.gamma;
+    const T gam_t = (T)gamma;
     const double a_side = a.alphar[numr - 2];  // alphar(numr-1)
     const bool sym_bottom = (a.isym != 1);
     const double *rad = a.rad + (long long)s * kAdiFactors * nr;
@@ -314,16 +351,15 @@ __global__ void __launch_bounds__(kSegThreads, 1) k_adi_seg(AdiArgs a) {
     const long long ver_step = (long long)kAdiFactors * nz;
 
     for (int j = tid; j < nr; j += kSegThreads) {
-        AB[j] = make_double2(a.alphar[j + 1], a.betar[j + 1]);
-        el0[j] = a.elz[(long long)s * numr + j + 1];
-        zrow[j] = 0.0;
+        AB[j] = Vec2<T>::make((T)a.alphar[j + 1], (T)a.betar[j + 1]);
+        el0[j] = (T)a.elz[(long long)s * numr + j + 1];
+        zrow[j] = (T)0;
     }
     fac_load(Fr, nr, rad + a.step0 * rad_step, tid, kSegThreads);
     fac_load(Fz, nz, a.ver + a.step0 * ver_step, tid, kSegThreads);
-    // Rw and the initial potential: 8 rows per warp pass, all loads in flight
-    // before the shared-memory stores.
-    {
-        const double top_g = gamma;
+    if (!kDefect) {
+        // Rw (source + folded Dirichlet terms) and the initial potential: 8 rows per
+        // warp pass, all loads in flight before the shared-memory stores.
         for (int k0 = warp * 8; k0 < nz; k0 += nwarps * 8) {
             double rv[8][4], pv[8][4];
 #pragma unroll
@@ -347,24 +383,45 @@ __global__ void __launch_bounds__(kSegThreads, 1) k_adi_seg(AdiArgs a) {
                     const int j = lane + 32 * c;
                     if (j >= nr) break;
                     double r0 = rv[r][c];
-                    if (k == nz - 1) r0 = r0 + top_g * Pg[(j + 1) + (long long)numr * (numz - 1)];
+                    if (k == nz - 1) r0 = r0 + gamma * Pg[(j + 1) + (long long)numr * (numz - 1)];
                     if (!sym_bottom && k == 0) r0 = r0 + gamma * Pg[j + 1];
                     if (j == nr - 1) r0 = r0 - a_side * side_v;
-                    Rw[k * ps + j] = r0;
-                    Ww[k * ps + j] = pv[r][c];
+                    Rw[k * ps + j] = (T)r0;
+                    Ww[k * ps + j] = (T)pv[r][c];
                 }
             }
         }
-        // lines longer than 128: the remaining columns
         for (int k = warp; k < nz; k += nwarps)
             for (int j = 128 + lane; j < nr; j += 32) {
                 double r0 = Rs[(long long)nr * k + j];
-                if (k == nz - 1) r0 = r0 + top_g * Pg[(j + 1) + (long long)numr * (numz - 1)];
+                if (k == nz - 1) r0 = r0 + gamma * Pg[(j + 1) + (long long)numr * (numz - 1)];
                 if (!sym_bottom && k == 0) r0 = r0 + gamma * Pg[j + 1];
                 if (j == nr - 1) r0 = r0 - a_side * Pg[(numr - 1) + (long long)numr * (k + 1)];
-                Rw[k * ps + j] = r0;
-                Ww[k * ps + j] = a.cold ? 0.0 : Pg[(long long)numr * (k + 1) + 1 + j];
+                Rw[k * ps + j] = (T)r0;
+                Ww[k * ps + j] = (T)(a.cold ? 0.0 : Pg[(long long)numr * (k + 1) + 1 + j]);
             }
+    } else {
+        // FP64 residual r = R - (Ar + Az) phi over the interior; the Dirichlet
+        // columns of phi (J = numr, K = numz, K = 1 for isym 1) enter through
+        // the stencil.  delta starts at zero, so the first radial right-hand
+        // side is r itself (times 1/bet).
+        __syncthreads();  // Fr is read below
+        const Fac<T> f = fac_view(Fr, nr);
+        const double *brb = a.brb + (long long)s * numr;
+        for (int k = warp; k < nz; k += nwarps) {
+            const double *pc = Pg + (long long)numr * (k + 1) + 1;
+#pragma unroll 2
+            for (int j = lane; j < nr; j += 32) {
+                const double c = pc[j], e = pc[j + 1], n = pc[j + numr];
+                const double w = (j > 0) ? pc[j - 1] : 0.0;
+                const double so = (k > 0 || !sym_bottom) ? pc[j - numr] : 0.0;
+                const double ar = brb[j + 1] * c + a.alphar[j + 1] * e + a.betar[j + 1] * w;
+                const double az = a.bzb[k + 1] * c - gamma * n - gamma * so;
+                const double r0 = Rs[(long long)nr * k + j] - ar - az;
+                Rw[k * ps + j] = (T)r0;
+                Ww[k * ps + j] = (T)r0 * f.ib[j];
+            }
+        }
     }
     __syncthreads();
 
@@ -372,31 +429,31 @@ __global__ void __launch_bounds__(kSegThreads, 1) k_adi_seg(AdiArgs a) {
     for (int it = 0; it < a.nsteps_run; ++it) {
         const int step = a.step0 + it;
         const bool last_step = (it + 1 == a.nsteps_run);
-        const double dtt = a.dt[step];
-        const double dtn = last_step ? dtt : a.dt[step + 1];
+        const T dtt = (T)a.dt[step];
+        const T dtn = last_step ? dtt : (T)a.dt[step + 1];
 
         // ================= radial half-sweep: lines k, segments along j =================
         {
-            const Fac f = fac_view(Fr, nr);
-            double v[kAdiSeg];
+            const Fac<T> f = fac_view(Fr, nr);
+            T v[kAdiSeg];
             const bool active = tid < nitem_r;
             const int k = active ? tid % nz : 0, p = active ? tid / nz : 0;
             const int j0 = p * kAdiSeg, len = kFull ? kAdiSeg : min(kAdiSeg, nr - j0);
-            double *wr = Ww + k * ps + j0;
-            const double *rr = Rw + k * ps + j0;
+            T *wr = Ww + k * ps + j0;
+            const T *rr = Rw + k * ps + j0;
             if (active) {
-                double L = 0.0;
-                if (it == 0) {
+                T L = (T)0;
+                if (!kDefect && it == 0) {
                     // first step: the right-hand side from the initial potential
                     const bool refl = (k == 0) && sym_bottom;
-                    const double cphi = refl ? dtt - gamma : dtt - 2.0 * gamma;
-                    const double cdn = refl ? 0.0 : 1.0;
-                    const double *pu = (k + 1 < nz) ? wr + ps : zrow + j0;
-                    const double *pd = (k > 0) ? wr - ps : zrow + j0;
+                    const T cphi = refl ? dtt - gam_t : dtt - (T)2 * gam_t;
+                    const T cdn = refl ? (T)0 : (T)1;
+                    const T *pu = (k + 1 < nz) ? wr + ps : zrow + j0;
+                    const T *pd = (k > 0) ? wr - ps : zrow + j0;
 #pragma unroll
                     for (int i = 0; i < kAdiSeg; ++i)
                         if (kFull || i < len) {
-                            const double rhs = rr[i] + cphi * wr[i] + gamma * (pu[i] + cdn * pd[i]);
+                            const T rhs = rr[i] + cphi * wr[i] + gam_t * (pu[i] + cdn * pd[i]);
                             L = rhs * f.ib[j0 + i] - f.dd[j0 + i] * L;
                             v[i] = L;
                         }
@@ -412,13 +469,13 @@ __global__ void __launch_bounds__(kSegThreads, 1) k_adi_seg(AdiArgs a) {
             }
             __syncthreads();
             if (active) {
-                double yin = 0.0;
+                T yin = (T)0;
                 for (int q = 0; q < p; ++q) yin = Xa[k + nz * q] + f.GG[min((q + 1) * kAdiSeg, nr) - 1].x * yin;
-                double M = 0.0;
+                T M = (T)0;
 #pragma unroll
                 for (int i = kAdiSeg - 1; i >= 0; --i)
                     if (kFull || i < len) {
-                        const double2 gg = f.GG[j0 + i];
+                        const T2 gg = f.GG[j0 + i];
                         M = (v[i] + gg.x * yin) - gg.y * M;
                         v[i] = M;
                     }
@@ -426,7 +483,7 @@ __global__ void __launch_bounds__(kSegThreads, 1) k_adi_seg(AdiArgs a) {
             }
             __syncthreads();
             if (active) {
-                double xin = 0.0;
+                T xin = (T)0;
                 for (int q = Pr - 1; q > p; --q) xin = Xb[k + nz * q] + f.K[q * kAdiSeg] * xin;
 #pragma unroll
                 for (int i = 0; i < kAdiSeg; ++i)
@@ -440,38 +497,36 @@ __global__ void __launch_bounds__(kSegThreads, 1) k_adi_seg(AdiArgs a) {
             if (active) {
                 // vertical right-hand side of this step (helmadi.F90:276-340),
                 // times the vertical 1/bet of row k
-                const double ibz = fac_view(Fz, nz).ib[k];
-                const double left = (p > 0) ? Eb[k + nz * (p - 1)] : 0.0;
-                const double right = (p + 1 < Pr) ? Ea[k + nz * (p + 1)] : 0.0;
+                const T ibz = fac_view(Fz, nz).ib[k];
+                const T left = (p > 0) ? Eb[k + nz * (p - 1)] : (T)0;
+                const T right = (p + 1 < Pr) ? Ea[k + nz * (p + 1)] : (T)0;
 #pragma unroll
                 for (int i = 0; i < kAdiSeg; ++i)
                     if (kFull || i < len) {
                         const int j = j0 + i;
-                        const double pl = (i > 0) ? v[i - 1] : left;
-                        const double pr = (kFull ? (i + 1 < kAdiSeg) : (i + 1 < len)) ? v[(i + 1) & (kAdiSeg - 1)]
-                                                                                         : right;
-                        const double2 ab = AB[j];
+                        const T pl = (i > 0) ? v[i - 1] : left;
+                        const T pr = (kFull ? (i + 1 < kAdiSeg) : (i + 1 < len)) ? v[(i + 1) & (kAdiSeg - 1)] : right;
+                        const T2 ab = AB[j];
                         wr[i] = (rr[i] + (el0[j] + dtt) * v[i] - ab.x * pr - ab.y * pl) * ibz;
                     }
             }
-            // the next step's radial factors (Fr is dead until then)
             if (!last_step) {
-                __syncthreads();  // every reader of Fr is past phase D's ibz load
+                __syncthreads();
                 fac_load(Fr, nr, rad + (step + 1) * rad_step, tid, kSegThreads);
             }
             __syncthreads();
         }
         // ================= vertical half-sweep: lines j, segments along k =================
         {
-            const Fac f = fac_view(Fz, nz);
-            double v[kAdiSeg];
+            const Fac<T> f = fac_view(Fz, nz);
+            T v[kAdiSeg];
             const bool active = tid < nitem_z;
             const int j = active ? tid % nr : 0, p = active ? tid / nr : 0;
             const int k0 = p * kAdiSeg, len = kFull ? kAdiSeg : min(kAdiSeg, nz - k0);
-            double *wc = Ww + k0 * ps + j;
-            const double *rc = Rw + k0 * ps + j;
+            T *wc = Ww + k0 * ps + j;
+            const T *rc = Rw + k0 * ps + j;
             if (active) {
-                double L = 0.0;
+                T L = (T)0;
 #pragma unroll
                 for (int i = 0; i < kAdiSeg; ++i)
                     if (kFull || i < len) {
@@ -482,13 +537,13 @@ __global__ void __launch_bounds__(kSegThreads, 1) k_adi_seg(AdiArgs a) {
             }
             __syncthreads();
             if (active) {
-                double yin = 0.0;
+                T yin = (T)0;
                 for (int q = 0; q < p; ++q) yin = Xa[j + nr * q] + f.GG[min((q + 1) * kAdiSeg, nz) - 1].x * yin;
-                double M = 0.0;
+                T M = (T)0;
 #pragma unroll
                 for (int i = kAdiSeg - 1; i >= 0; --i)
                     if (kFull || i < len) {
-                        const double2 gg = f.GG[k0 + i];
+                        const T2 gg = f.GG[k0 + i];
                         M = (v[i] + gg.x * yin) - gg.y * M;
                         v[i] = M;
                     }
@@ -496,7 +551,7 @@ __global__ void __launch_bounds__(kSegThreads, 1) k_adi_seg(AdiArgs a) {
             }
             __syncthreads();
             if (active) {
-                double xin = 0.0;
+                T xin = (T)0;
                 for (int q = Pz - 1; q > p; --q) xin = Xb[j + nr * q] + f.K[q * kAdiSeg] * xin;
 #pragma unroll
                 for (int i = 0; i < kAdiSeg; ++i)
@@ -515,35 +570,316 @@ __global__ void __launch_bounds__(kSegThreads, 1) k_adi_seg(AdiArgs a) {
                 } else {
                     // radial right-hand side of the next step (helmadi.F90:209-256),
                     // times the next step's radial 1/bet of column j
-                    const double ibr = fac_view(Fr, nr).ib[j];
-                    const double dn_edge = (p > 0) ? Eb[j + nr * (p - 1)] : 0.0;
-                    const double up_edge = (p + 1 < Pz) ? Ea[j + nr * (p + 1)] : 0.0;
+                    const T ibr = fac_view(Fr, nr).ib[j];
+                    const T dn_edge = (p > 0) ? Eb[j + nr * (p - 1)] : (T)0;
+                    const T up_edge = (p + 1 < Pz) ? Ea[j + nr * (p + 1)] : (T)0;
 #pragma unroll
                     for (int i = 0; i < kAdiSeg; ++i)
                         if (kFull || i < len) {
                             const int k = k0 + i;
                             const bool refl = (k == 0) && sym_bottom;
-                            const double up = (kFull ? (i + 1 < kAdiSeg) : (i + 1 < len)) ? v[(i + 1) & (kAdiSeg - 1)]
-                                                                                          : up_edge;
-                            const double dn = (i > 0) ? v[i - 1] : dn_edge;
-                            const double cphi = refl ? dtn - gamma : dtn - 2.0 * gamma;
-                            const double rhs = refl ? rc[i * ps] + cphi * v[i] + gamma * up
-                                                    : rc[i * ps] + cphi * v[i] + gamma * (up + dn);
+                            const T up = (kFull ? (i + 1 < kAdiSeg) : (i + 1 < len)) ? v[(i + 1) & (kAdiSeg - 1)] : up_edge;
+                            const T dn = (i > 0) ? v[i - 1] : dn_edge;
+                            const T cphi = refl ? dtn - gam_t : dtn - (T)2 * gam_t;
+                            const T rhs = refl ? rc[i * ps] + cphi * v[i] + gam_t * up
+                                               : rc[i * ps] + cphi * v[i] + gam_t * (up + dn);
                             wc[i * ps] = rhs * ibr;
                         }
                 }
             }
             if (!last_step) {
-                __syncthreads();  // every reader of Fz is past phase C
+                __syncthreads();
                 fac_load(Fz, nz, a.ver + (step + 1) * ver_step, tid, kSegThreads);
             }
             __syncthreads();
         }
     }
+    if (!kDefect) {
+        for (int k = warp; k < nz; k += nwarps) {
+            double *prow = Pg + (long long)numr * (k + 1) + 1;
+#pragma unroll 4
+            for (int j = lane; j < nr; j += 32) prow[j] = (double)Ww[k * ps + j];
+        }
+    } else {
+        // phi += delta in FP64; per-slot |delta|^2 and |phi|^2
+        double sd = 0.0, sp = 0.0;
+        for (int k = warp; k < nz; k += nwarps) {
+            double *prow = Pg + (long long)numr * (k + 1) + 1;
+#pragma unroll 2
+            for (int j = lane; j < nr; j += 32) {
+                const double d = (double)Ww[k * ps + j];
+                const double ph = prow[j] + d;
+                prow[j] = ph;
+                sd += d * d;
+                sp += ph * ph;
+            }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            sd += __shfl_down_sync(0xffffffffu, sd, off);
+            sp += __shfl_down_sync(0xffffffffu, sp, off);
+        }
+        __syncthreads();
+        double *red = reinterpret_cast<double *>(smraw);
+        if (lane == 0) {
+            red[2 * warp] = sd;
+            red[2 * warp + 1] = sp;
+        }
+        __syncthreads();
+        if (tid < 2) {
+            double t = 0.0;
+            for (int w = 0; w < nwarps; ++w) t += red[2 * w + tid];
+            const double wgt = (s == 0 || s == a.N / 2) ? 1.0 : 2.0;
+            a.norms[2 * s + tid] = wgt * t;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Mixed-precision refinement cycle (k_adi_delta, T = float).
+//
+// One CTA per slot, two CTAs per SM.  Prologue: the FP64 residual
+// r = -4 pi rho_hat - A phi of the current potential (its Dirichlet columns
+// enter through the stencil), rounded to T.  Body: nsteps ADI steps of the
+// defect equation A delta = r in increment form,
+//   (Ar + dt) D1 = r - A delta,  delta += D1,
+//   (Az + dt) D2 = r - A delta,  delta += D2,
+// which is the Peaceman-Rachford iteration of helmadi.F90 rewritten so that
+// every line solve sees a residual: in the plain form the intermediate
+// values of stiff near-axis components (A_r up to ~1e8 x dt) are amplified
+// thousands of times and T's rounding of them would not be recoverable.
+// Epilogue: phi += delta in FP64, per-slot |delta|^2 and |phi|^2.
+//
+// Shared memory (T): D = delta, Rv = r (both nz x ps), factor blocks Fr/Fz,
+// segment exchange Xa/Xb, C4 [nr] = (brb, alphar, betar, 0) of the slot,
+// bz [nz] = bzb.  Per line segment: A forms the residual with a sliding
+// window along the line and eliminates forward with zero carry-in; B folds
+// the carry-in and eliminates backward; C folds the carry-in and adds the
+// increment to D.
+struct DeltaLayout {
+    int ps, Pr, Pz, xsz, fsz;
+    size_t elems;
+};
+
+__host__ __device__ inline DeltaLayout delta_layout(int nr, int nz) {
+    DeltaLayout L;
+    L.ps = nr | 1;
+    L.Pr = (nr + kAdiSeg - 1) / kAdiSeg;
+    L.Pz = (nz + kAdiSeg - 1) / kAdiSeg;
+    L.xsz = max(nz * L.Pr, nr * L.Pz);
+    L.fsz = factor_block(max(nr, nz));
+    L.elems = 2 * (size_t)nz * L.ps + 2 * (size_t)L.fsz + 2 * (size_t)L.xsz + 4 * (size_t)nr + (size_t)nz + 8;
+    return L;
+}
+
+template <int kThreads, bool kFull>
+__global__ void __launch_bounds__(kThreads, 2) k_adi_delta(AdiArgs a) {
+    using T = float;
+    using T2 = float2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T *sm = reinterpret_cast<T *>(smraw);
+    const int s = blockIdx.x, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = kThreads / 32;
+    const int nr = a.nr, nz = a.nz, numr = a.numr, numz = a.numz;
+    const DeltaLayout Lo = delta_layout(nr, nz);
+    const int ps = Lo.ps, Pr = Lo.Pr, Pz = Lo.Pz;
+    T *D = sm;
+    T *Rv = D + (size_t)nz * ps;
+    T *Fr = Rv + (size_t)nz * ps;
+    T *Fz = Fr + Lo.fsz;
+    T *Xa = Fz + Lo.fsz;
+    T *Xb = Xa + Lo.xsz;
+    T *c4p = Xb + Lo.xsz;
+    while ((reinterpret_cast<uintptr_t>(c4p) & 15) != 0) ++c4p;
+    float4 *C4 = reinterpret_cast<float4 *>(c4p);
+    T *bz = c4p + 4 * nr;
+    const long long nplane = (long long)numr * numz;
+    double *Pg = a.P + (long long)s * nplane;
+    const double *Rs = a.R + (long long)s * nr * nz;
+    const double gamma = a.gamma;
+    const T g = (T)gamma;
+    const bool sym_bottom = (a.isym != 1);
+    const double *rad = a.rad + (long long)s * kAdiFactors * nr;
+    const long long rad_step = (long long)a.N * kAdiFactors * nr;
+    const long long ver_step = (long long)kAdiFactors * nz;
+    const double *brb = a.brb + (long long)s * numr;
+
+    for (int j = tid; j < nr; j += kThreads)
+        C4[j] = make_float4((T)brb[j + 1], (T)a.alphar[j + 1], (T)a.betar[j + 1], 0.f);
+    for (int k = tid; k < nz; k += kThreads) bz[k] = (T)a.bzb[k + 1];
+    fac_load(Fr, nr, rad + a.step0 * rad_step, tid, kThreads);
+    fac_load(Fz, nz, a.ver + a.step0 * ver_step, tid, kThreads);
+    // FP64 residual of the current potential; delta = 0
+    for (int k = warp; k < nz; k += nwarps) {
+        const double *pc = Pg + (long long)numr * (k + 1) + 1;
+#pragma unroll 2
+        for (int j = lane; j < nr; j += 32) {
+            const double c = pc[j], e = pc[j + 1], n = pc[j + numr];
+            const double w = (j > 0) ? pc[j - 1] : 0.0;
+            const double so = (k > 0 || !sym_bottom) ? pc[j - numr] : 0.0;
+            const double ar = brb[j + 1] * c + a.alphar[j + 1] * e + a.betar[j + 1] * w;
+            const double az = a.bzb[k + 1] * c - gamma * n - gamma * so;
+            Rv[k * ps + j] = (T)(Rs[(long long)nr * k + j] - ar - az);
+            D[k * ps + j] = 0.f;
+        }
+    }
+    __syncthreads();
+
+    const int nitem_r = nz * Pr, nitem_z = nr * Pz;
+    for (int it = 0; it < a.nsteps_run; ++it) {
+        const int step = a.step0 + it;
+        const bool last_step = (it + 1 == a.nsteps_run);
+        const T dtt = (T)a.dt[step];
+        // ================= radial: lines k, segments along j =================
+        {
+            const Fac<T> f = fac_view(Fr, nr);
+            T v[kAdiSeg];
+            const bool active = tid < nitem_r;
+            const int k = active ? tid % nz : 0, p = active ? tid / nz : 0;
+            const int j0 = p * kAdiSeg, len = kFull ? kAdiSeg : min(kAdiSeg, nr - j0);
+            const T *dc = D + k * ps;
+            const T *dn = (k > 0) ? dc - ps : nullptr;
+            const T *du = (k + 1 < nz) ? dc + ps : nullptr;
+            const T czn = (k > 0 || !sym_bottom) ? g : 0.f;  // K-1 neighbour weight
+            const T bzk = bz[k];
+            if (active) {
+                T L = 0.f;
+                T dl = (j0 > 0) ? dc[j0 - 1] : 0.f;
+                T dm = dc[j0];
+#pragma unroll
+                for (int i = 0; i < kAdiSeg; ++i)
+                    if (kFull || i < len) {
+                        const int j = j0 + i;
+                        const T dr_ = (j + 1 < nr) ? dc[j + 1] : 0.f;
+                        const T vd = (dn ? dn[j] : 0.f), vu = (du ? du[j] : 0.f);
+                        const float4 cc = C4[j];
+                        const T rhs = Rv[k * ps + j] - (cc.x * dm + cc.y * dr_ + cc.z * dl) -
+                                      (bzk * dm - g * vu - czn * vd);
+                        L = rhs * f.ib[j] - f.dd[j] * L;
+                        v[i] = L;
+                        dl = dm;
+                        dm = dr_;
+                    }
+                Xa[k + nz * p] = L;
+            }
+            __syncthreads();
+            if (active) {
+                T yin = 0.f;
+                for (int q = 0; q < p; ++q) yin = Xa[k + nz * q] + f.GG[min((q + 1) * kAdiSeg, nr) - 1].x * yin;
+                T M = 0.f;
+#pragma unroll
+                for (int i = kAdiSeg - 1; i >= 0; --i)
+                    if (kFull || i < len) {
+                        const T2 gg = f.GG[j0 + i];
+                        M = (v[i] + gg.x * yin) - gg.y * M;
+                        v[i] = M;
+                    }
+                Xb[k + nz * p] = M;
+            }
+            __syncthreads();
+            if (active) {
+                T xin = 0.f;
+                for (int q = Pr - 1; q > p; --q) xin = Xb[k + nz * q] + f.K[q * kAdiSeg] * xin;
+                T *dw = D + k * ps + j0;
+#pragma unroll
+                for (int i = 0; i < kAdiSeg; ++i)
+                    if (kFull || i < len) dw[i] = dw[i] + (v[i] + f.K[j0 + i] * xin);
+            }
+            if (!last_step) {
+                __syncthreads();
+                fac_load(Fr, nr, rad + (step + 1) * rad_step, tid, kThreads);
+            }
+            __syncthreads();
+        }
+        // ================= vertical: lines j, segments along k =================
+        {
+            const Fac<T> f = fac_view(Fz, nz);
+            T v[kAdiSeg];
+            const bool active = tid < nitem_z;
+            const int j = active ? tid % nr : 0, p = active ? tid / nr : 0;
+            const int k0 = p * kAdiSeg, len = kFull ? kAdiSeg : min(kAdiSeg, nz - k0);
+            const float4 cc = C4[j];
+            const bool has_l = j > 0, has_r = j + 1 < nr;
+            if (active) {
+                T L = 0.f;
+                T dd_ = (k0 > 0) ? D[(k0 - 1) * ps + j] : 0.f;
+                T dm = D[k0 * ps + j];
+#pragma unroll
+                for (int i = 0; i < kAdiSeg; ++i)
+                    if (kFull || i < len) {
+                        const int k = k0 + i;
+                        const T du_ = (k + 1 < nz) ? D[(k + 1) * ps + j] : 0.f;
+                        const T vl = has_l ? D[k * ps + j - 1] : 0.f, vr = has_r ? D[k * ps + j + 1] : 0.f;
+                        const T czn = (k > 0 || !sym_bottom) ? g : 0.f;
+                        const T rhs = Rv[k * ps + j] - (cc.x * dm + cc.y * vr + cc.z * vl) -
+                                      (bz[k] * dm - g * du_ - czn * dd_);
+                        L = rhs * f.ib[k] - f.dd[k] * L;
+                        v[i] = L;
+                        dd_ = dm;
+                        dm = du_;
+                    }
+                Xa[j + nr * p] = L;
+            }
+            __syncthreads();
+            if (active) {
+                T yin = 0.f;
+                for (int q = 0; q < p; ++q) yin = Xa[j + nr * q] + f.GG[min((q + 1) * kAdiSeg, nz) - 1].x * yin;
+                T M = 0.f;
+#pragma unroll
+                for (int i = kAdiSeg - 1; i >= 0; --i)
+                    if (kFull || i < len) {
+                        const T2 gg = f.GG[k0 + i];
+                        M = (v[i] + gg.x * yin) - gg.y * M;
+                        v[i] = M;
+                    }
+                Xb[j + nr * p] = M;
+            }
+            __syncthreads();
+            if (active) {
+                T xin = 0.f;
+                for (int q = Pz - 1; q > p; --q) xin = Xb[j + nr * q] + f.K[q * kAdiSeg] * xin;
+#pragma unroll
+                for (int i = 0; i < kAdiSeg; ++i)
+                    if (kFull || i < len) {
+                        T *dw = D + (k0 + i) * ps + j;
+                        *dw = *dw + (v[i] + f.K[k0 + i] * xin);
+                    }
+            }
+            if (!last_step) {
+                __syncthreads();
+                fac_load(Fz, nz, a.ver + (step + 1) * ver_step, tid, kThreads);
+            }
+            __syncthreads();
+        }
+    }
+    // phi += delta in FP64; per-slot |delta|^2 and |phi|^2
+    double sd = 0.0, sp = 0.0;
     for (int k = warp; k < nz; k += nwarps) {
         double *prow = Pg + (long long)numr * (k + 1) + 1;
-#pragma unroll 4
-        for (int j = lane; j < nr; j += 32) prow[j] = Ww[k * ps + j];
+#pragma unroll 2
+        for (int j = lane; j < nr; j += 32) {
+            const double d = (double)D[k * ps + j];
+            const double ph = prow[j] + d;
+            prow[j] = ph;
+            sd += d * d;
+            sp += ph * ph;
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        sd += __shfl_down_sync(0xffffffffu, sd, off);
+        sp += __shfl_down_sync(0xffffffffu, sp, off);
+    }
+    __syncthreads();
+    double *red = reinterpret_cast<double *>(smraw);
+    if (lane == 0) {
+        red[2 * warp] = sd;
+        red[2 * warp + 1] = sp;
+    }
+    __syncthreads();
+    if (tid < 2) {
+        double t = 0.0;
+        for (int w = 0; w < nwarps; ++w) t += red[2 * w + tid];
+        const double wgt = (s == 0 || s == a.N / 2) ? 1.0 : 2.0;
+        a.norms[2 * s + tid] = wgt * t;
     }
 }
 
@@ -602,10 +938,19 @@ k_slot_norms(const double *__restrict__ P, const double *__restrict__ Q, const d
 
 }  // namespace
 
+template <typename T, bool kDefect>
 const void *seg_kernel(int threads, bool full) {
-    if (threads == 256) return full ? (const void *)k_adi_seg<256, true> : (const void *)k_adi_seg<256, false>;
-    if (threads == 384) return full ? (const void *)k_adi_seg<384, true> : (const void *)k_adi_seg<384, false>;
-    return full ? (const void *)k_adi_seg<512, true> : (const void *)k_adi_seg<512, false>;
+    if (threads == 256)
+        return full ? (const void *)k_adi_seg<T, 256, true, kDefect> : (const void *)k_adi_seg<T, 256, false, kDefect>;
+    if (threads == 384)
+        return full ? (const void *)k_adi_seg<T, 384, true, kDefect> : (const void *)k_adi_seg<T, 384, false, kDefect>;
+    return full ? (const void *)k_adi_seg<T, 512, true, kDefect> : (const void *)k_adi_seg<T, 512, false, kDefect>;
+}
+
+const void *delta_kernel(int threads, bool full) {
+    if (threads == 256) return full ? (const void *)k_adi_delta<256, true> : (const void *)k_adi_delta<256, false>;
+    if (threads == 384) return full ? (const void *)k_adi_delta<384, true> : (const void *)k_adi_delta<384, false>;
+    return full ? (const void *)k_adi_delta<512, true> : (const void *)k_adi_delta<512, false>;
 }
 
 int adi_configure(bph_ctx *c) {
@@ -613,28 +958,43 @@ int adi_configure(bph_ctx *c) {
     cudaError_t e = cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
     const SegLayout L = seg_layout(c->nr, c->nz);
-    const size_t seg_bytes = sizeof(double) * L.doubles;
+    const size_t seg_bytes = sizeof(double) * L.elems + 16;
+    const size_t mixed_bytes = sizeof(float) * L.elems + 16;
     const size_t onchip = sizeof(double) * 2 * (size_t)c->nz * (size_t)(c->nr | 1) + smalls_bytes(c);
-    c->adi_seg = 0;
-    c->adi_smem = 0;
     const int items = max(c->nz * L.Pr, c->nr * L.Pz);
     const int threads = (items <= 256) ? 256 : (items <= 384) ? 384 : 512;
+    c->adi_seg = 0;
+    c->adi_smem = 0;
+    c->adi_mixed_smem = 0;
+    c->adi_full = (c->nr % kAdiSeg == 0) && (c->nz % kAdiSeg == 0);
     if (seg_bytes <= (size_t)dev_max && items <= 512) {
         c->adi_seg = threads;
-        c->adi_full = (c->nr % kAdiSeg == 0) && (c->nz % kAdiSeg == 0);
         c->adi_smem = (int)seg_bytes;
-        const void *fn = seg_kernel(c->adi_seg, c->adi_full);
-        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, c->adi_smem);
+        e = cudaFuncSetAttribute(seg_kernel<double, false>(c->adi_seg, c->adi_full),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, c->adi_smem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_adi_seg)");
     } else if (onchip <= (size_t)dev_max) {
         c->adi_smem = (int)onchip;
         e = cudaFuncSetAttribute(k_adi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, c->adi_smem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_adi)");
     }
+    const DeltaLayout DL = delta_layout(c->nr, c->nz);
+    const size_t delta_bytes = sizeof(float) * DL.elems + 16;
+    (void)mixed_bytes;
+    if (delta_bytes <= (size_t)dev_max && items <= 512) {
+        c->adi_mixed_threads = threads;
+        c->adi_mixed_smem = (int)delta_bytes;
+        const void *fn = delta_kernel(threads, c->adi_full);
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, c->adi_mixed_smem);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_adi_delta)");
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->adi_mixed_per_sm, fn, threads, c->adi_mixed_smem);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    }
     return BPH_OK;
 }
 
-cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bool cold) {
+AdiArgs make_args(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bool cold) {
     AdiArgs a;
     a.P = c->d_P;
     a.R = c->d_R;
@@ -645,6 +1005,9 @@ cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_ru
     a.elz = c->d_elz;
     a.alphar = c->d_alphar;
     a.betar = c->d_betar;
+    a.brb = c->d_brb;
+    a.bzb = c->d_bzb;
+    a.norms = c->d_red;
     a.numr = c->g.numr;
     a.numz = c->g.numz;
     a.nr = c->nr;
@@ -655,16 +1018,31 @@ cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_ru
     a.nsteps_run = nsteps_run;
     a.cold = cold ? 1 : 0;
     a.gamma = c->gamma;
+    return a;
+}
+
+cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bool cold) {
+    AdiArgs a = make_args(c, sch, step0, nsteps_run, cold);
     ++c->launches;
     if (c->adi_seg) {
         void *args[] = {&a};
-        return cudaLaunchKernel(seg_kernel(c->adi_seg, c->adi_full), dim3(c->N), dim3(c->adi_seg), args,
-                                (size_t)c->adi_smem, c->stream);
-    } else if (c->adi_smem > 0)
+        return cudaLaunchKernel(seg_kernel<double, false>(c->adi_seg, c->adi_full), dim3(c->N), dim3(c->adi_seg),
+                                args, (size_t)c->adi_smem, c->stream);
+    } else if (c->adi_smem > 0) {
         k_adi<true><<<c->N, kAdiThreads, c->adi_smem, c->stream>>>(a);
-    else
+    } else {
         k_adi<false><<<c->N, kAdiThreads, smalls_bytes(c), c->stream>>>(a);
+    }
     return cudaGetLastError();
+}
+
+cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {
+    if (!c->adi_mixed_smem) return cudaErrorNotSupported;
+    AdiArgs a = make_args(c, sch, 0, sch.nsteps, false);
+    ++c->launches;
+    void *args[] = {&a};
+    return cudaLaunchKernel(delta_kernel(c->adi_mixed_threads, c->adi_full), dim3(c->N),
+                            dim3(c->adi_mixed_threads), args, (size_t)c->adi_mixed_smem, c->stream);
 }
 
 cudaError_t launch_update_norm(bph_ctx *c, double *d_out) {

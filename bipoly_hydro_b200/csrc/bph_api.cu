@@ -545,6 +545,76 @@ int bph_solve_converged(bph_ctx_t *c, const double *rho, double *pot, int nsteps
     return read_status(c);
 }
 
+int bph_solve_converged_mixed(bph_ctx_t *c, const double *rho, double *pot, int nsteps, int cold, double tol,
+                              int max_cycles, int on_device, int *cycles_out, double *resid_out) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    if (!rho || !pot || nsteps < 1 || nsteps > 10000 || max_cycles < 1 || !(tol >= 0.0)) {
+        set_error("invalid arguments");
+        return BPH_ERR_INVALID;
+    }
+    if (!c->adi_mixed_smem) {
+        set_error("the mixed-precision ADI does not fit on chip for this grid");
+        return BPH_ERR_INVALID;
+    }
+    if ((rc = set_device_of(c))) return rc;
+    Schedule *s;
+    if ((rc = get_schedule(c, nsteps, &s))) return rc;
+    const size_t bytes = sizeof(double) * (size_t)c->ntot;
+    const double *d_rho = rho;
+    double *d_pot = pot;
+    if (!on_device) {
+        if ((rc = ensure_staging(c))) return rc;
+        BPH_CUDA(cudaMemcpyAsync(c->d_rho_stage, rho, bytes, cudaMemcpyHostToDevice, c->stream));
+        d_rho = c->d_rho_stage;
+        d_pot = c->d_pot_stage;
+    }
+    BPH_CUDA(launch_fft_fwd_rho(c, d_rho));
+    BPH_CUDA(launch_green_contract(c));
+    if (cold) BPH_CUDA(cudaMemsetAsync(c->d_P, 0, sizeof(double) * (size_t)c->N * c->nplane, c->stream));
+    BPH_CUDA(launch_boundary_slots(c));
+    std::vector<double> h(2 * (size_t)c->N);
+    int cyc = 0;
+    double prev_upd = INFINITY;
+    for (;;) {
+        BPH_CUDA(launch_adi_defect(c, *s));
+        ++cyc;
+        BPH_CUDA(cudaMemcpyAsync(h.data(), c->d_red, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+        BPH_CUDA(cudaStreamSynchronize(c->stream));
+        double num = 0.0, den = 0.0;
+        for (int i = 0; i < c->N; ++i) {
+            num += h[2 * i];
+            den += h[2 * i + 1];
+        }
+        double upd = den > 0.0 ? std::sqrt(num / den) : std::sqrt(num);
+        if (!(upd == upd)) {
+            set_error("mixed-precision refinement diverged");
+            return BPH_ERR_NONFINITE;
+        }
+        // Stop at the tolerance, or once a cycle no longer halves the update:
+        // the FP32 inner solves have then reached their accuracy, and more
+        // cycles only add FP32 rounding to stiff near-axis components.
+        if (upd <= tol || cyc >= max_cycles || upd > 0.5 * prev_upd) break;
+        prev_upd = upd;
+    }
+    if (resid_out) {
+        BPH_CUDA(launch_residual_norm(c, c->d_red));
+        BPH_CUDA(cudaMemcpyAsync(h.data(), c->d_red, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+        BPH_CUDA(cudaStreamSynchronize(c->stream));
+        double num = 0.0, den = 0.0;
+        for (int i = 0; i < c->N; ++i) {
+            num += h[2 * i];
+            den += h[2 * i + 1];
+        }
+        *resid_out = den > 0.0 ? std::sqrt(num / den) : std::sqrt(num);
+    }
+    if (cycles_out) *cycles_out = cyc;
+    BPH_CUDA(launch_fft_inv(c, d_pot));
+    c->have_warm = true;
+    if (!on_device) BPH_CUDA(cudaMemcpyAsync(pot, d_pot, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return read_status(c);
+}
+
 int bph_run_phase(bph_ctx_t *c, int phase, const double *d_rho, double *d_pot, int nsteps) {
     int rc;
     if ((rc = check_ctx(c))) return rc;
@@ -606,6 +676,19 @@ int bph_copy_moments(bph_ctx_t *c, double *out, size_t n) {
     BPH_CUDA(cudaMemcpyAsync(out, c->d_S, sizeof(double) * need, cudaMemcpyDeviceToHost, c->stream));
     BPH_CUDA(cudaStreamSynchronize(c->stream));
     return BPH_OK;
+}
+
+long long bph_info(const bph_ctx_t *c, int what) {
+    if (!c) return -1;
+    switch (what) {
+        case BPH_INFO_ADI_THREADS: return c->adi_seg;
+        case BPH_INFO_ADI_SMEM: return c->adi_smem;
+        case BPH_INFO_MIXED_THREADS: return c->adi_mixed_threads;
+        case BPH_INFO_MIXED_SMEM: return c->adi_mixed_smem;
+        case BPH_INFO_MIXED_CTAS_PER_SM: return c->adi_mixed_per_sm;
+        case BPH_INFO_CONTRACT_SPLIT: return c->contract_split;
+        default: return -1;
+    }
 }
 
 long long bph_launch_count(const bph_ctx_t *c) { return c ? c->launches : 0; }

@@ -93,6 +93,9 @@ struct bph_ctx {
     int adi_smem = 0;            // dynamic shared bytes of the on-chip ADI kernel (0: global variant)
     int adi_seg = 0;             // threads of the segmented on-chip ADI kernel (0: not used)
     bool adi_full = false;       // both line lengths are multiples of the segment length
+    int adi_mixed_threads = 0;   // threads of the FP32 defect-correction ADI kernel
+    int adi_mixed_smem = 0;      // its dynamic shared bytes (0: mixed form unavailable)
+    int adi_mixed_per_sm = 0;    // its resident CTAs per SM
     int adi_threads = 256;
     int fft_smem_fwd = 0, fft_smem_inv = 0;
     bool have_warm = false;
@@ -123,6 +126,7 @@ cudaError_t launch_fft_inv(bph_ctx *c, double *pot);
 cudaError_t launch_green_contract(bph_ctx *c);
 cudaError_t launch_boundary_slots(bph_ctx *c);
 cudaError_t launch_adi(bph_ctx *c, const Schedule &s, int step0, int nsteps_run, bool cold);
+cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &s);
 cudaError_t launch_update_norm(bph_ctx *c, double *d_out);
 cudaError_t launch_residual_norm(bph_ctx *c, double *d_out);
 

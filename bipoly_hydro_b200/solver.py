@@ -42,9 +42,9 @@ _ERR_NAMES = {
 #: Every symbol include/bph.h declares, in declaration order.
 EXPORTED_SYMBOLS = (
     "bph_setup", "bph_potential_solver", "bph_potential_solver_device", "bph_solve_nsteps",
-    "bph_solve_converged", "bph_set_stream", "bph_synchronize", "bph_destroy", "bph_last_error",
+    "bph_solve_converged", "bph_solve_converged_mixed", "bph_set_stream", "bph_synchronize", "bph_destroy", "bph_last_error",
     "bph_version", "bph_num_boundary_rows", "bph_copy_green", "bph_copy_moments", "bph_run_phase",
-    "bph_green_contract_noalloc", "bph_launch_count", "bph_device_bytes",
+    "bph_green_contract_noalloc", "bph_info", "bph_launch_count", "bph_device_bytes",
 )
 
 #: bph_run_phase phase ids.
@@ -92,6 +92,8 @@ def load_library(path: str | None = None):
     L.bph_solve_nsteps.argtypes = [vp, dp, dp, i, i, i]
     L.bph_solve_converged.argtypes = [vp, dp, dp, i, i, ctypes.c_double, i, i, ctypes.POINTER(i),
                                       ctypes.POINTER(ctypes.c_double)]
+    L.bph_solve_converged_mixed.argtypes = L.bph_solve_converged.argtypes
+    L.bph_solve_converged_mixed.restype = ctypes.c_int
     L.bph_set_stream.argtypes = [vp, vp]
     L.bph_synchronize.argtypes = [vp]
     L.bph_destroy.argtypes = [vp]
@@ -103,6 +105,8 @@ def load_library(path: str | None = None):
     L.bph_run_phase.argtypes = [vp, i, dp, dp, i]
     L.bph_green_contract_noalloc.argtypes = [vp, dp, dp]
     L.bph_green_contract_noalloc.restype = ctypes.c_int
+    L.bph_info.argtypes = [vp, i]
+    L.bph_info.restype = ctypes.c_longlong
     L.bph_launch_count.argtypes = [vp]
     L.bph_launch_count.restype = ctypes.c_longlong
     L.bph_device_bytes.argtypes = [vp]
@@ -209,6 +213,26 @@ class PotentialSolver:
                                              float(tol), int(max_cycles), 0, ctypes.byref(cyc), ctypes.byref(res)))
         return pot, ConvergedInfo(cyc.value, res.value)
 
+    def solve_converged_mixed(self, rho, nsteps: int = 20, cold: bool = True, tol: float = 1e-13,
+                              max_cycles: int = 200):
+        """FP32 ADI cycles with FP64 residual/update refinement to the converged solution."""
+        r = self._rho_host(rho)
+        pot = np.empty(self.shape, dtype=np.float64, order="F")
+        cyc, res = ctypes.c_int(0), ctypes.c_double(0.0)
+        _check(self._lib.bph_solve_converged_mixed(self._h, _host_ptr(r), _host_ptr(pot), int(nsteps),
+                                                   int(bool(cold)), float(tol), int(max_cycles), 0,
+                                                   ctypes.byref(cyc), ctypes.byref(res)))
+        return pot, ConvergedInfo(cyc.value, res.value)
+
+    def solve_converged_device(self, d_rho, d_pot, nsteps: int = 20, cold: bool = True, tol: float = 1e-13,
+                               max_cycles: int = 200, mixed: bool = False) -> ConvergedInfo:
+        """Converged solve on device arrays (synchronous: convergence is checked on the host)."""
+        fn = self._lib.bph_solve_converged_mixed if mixed else self._lib.bph_solve_converged
+        cyc = ctypes.c_int(0)
+        _check(fn(self._h, _dev_ptr(d_rho), _dev_ptr(d_pot), int(nsteps), int(bool(cold)), float(tol),
+                  int(max_cycles), 1, ctypes.byref(cyc), None))
+        return ConvergedInfo(cyc.value, float("nan"))
+
     # -- device-array API ---------------------------------------------------
     def set_stream(self, stream) -> None:
         """Run later work on a CUDA stream: an int handle or a torch.cuda.Stream
@@ -249,6 +273,11 @@ class PotentialSolver:
         """Enqueue one kernel of the solve (timing diagnostics)."""
         _check(self._lib.bph_run_phase(self._h, int(phase), _dev_ptr(d_rho) if d_rho is not None else None,
                                        _dev_ptr(d_pot) if d_pot is not None else None, int(nsteps)))
+
+    def info(self) -> dict:
+        """Launch-configuration facts (bph_info)."""
+        names = ("adi_threads", "adi_smem", "mixed_threads", "mixed_smem", "mixed_ctas_per_sm", "contract_split")
+        return {n: int(self._lib.bph_info(self._h, i)) for i, n in enumerate(names)}
 
     @property
     def launch_count(self) -> int:

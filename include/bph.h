@@ -76,6 +76,19 @@ int bph_solve_converged(bph_ctx_t *ctx, const double *rho, double *pot, int nste
                         double tol, int max_cycles, int on_device, int *cycles_out,
                         double *resid_out);
 
+/* Mixed-precision converged solve (no counterpart in the reference, which
+ * always runs a fixed 5 or 20 FP64 steps): iterative refinement in which
+ * every cycle forms the FP64 residual -4 pi rho_hat - A phi, runs the nsteps
+ * ADI schedule on the defect equation A delta = r in FP32 on chip, and adds
+ * delta to phi in FP64, until |delta|/|phi| <= tol or max_cycles.  The
+ * boundary potential, the FFTs and every residual/update stay FP64, so the
+ * result converges to the FP64 discrete solution (bph_solve_converged).
+ * It also stops once a cycle no longer halves the update (the FP32 inner
+ * solves have reached their accuracy).  Arguments as bph_solve_converged. */
+int bph_solve_converged_mixed(bph_ctx_t *ctx, const double *rho, double *pot, int nsteps, int cold,
+                              double tol, int max_cycles, int on_device, int *cycles_out,
+                              double *resid_out);
+
 /* Stream used for all later work of this context (a cudaStream_t; NULL is
  * CUDA's default stream).  Until the first call the context uses a
  * non-blocking stream of its own. */
@@ -140,6 +153,15 @@ int bph_run_phase(bph_ctx_t *ctx, int phase, const double *d_rho, double *d_pot,
  * it keeps the last call's contents; calls that overlap on the GPU race
  * and must be serialised by the caller. */
 int bph_green_contract_noalloc(bph_ctx_t *ctx, const double *d_mom, double *d_S);
+
+/* Launch-configuration facts of a context (diagnostics; -1 if unknown). */
+#define BPH_INFO_ADI_THREADS 0        /* threads of the FP64 on-chip ADI kernel (0: other variant) */
+#define BPH_INFO_ADI_SMEM 1           /* its dynamic shared bytes */
+#define BPH_INFO_MIXED_THREADS 2      /* threads of the FP32 refinement ADI kernel */
+#define BPH_INFO_MIXED_SMEM 3         /* its dynamic shared bytes */
+#define BPH_INFO_MIXED_CTAS_PER_SM 4  /* its resident CTAs per SM */
+#define BPH_INFO_CONTRACT_SPLIT 5     /* slices of the split-K Green contraction */
+long long bph_info(const bph_ctx_t *ctx, int what);
 
 /* Number of kernels this context has launched so far. */
 long long bph_launch_count(const bph_ctx_t *ctx);

@@ -170,3 +170,46 @@ def test_gpu_reproduces_golden_fixture(bph, path):
     assert rel_l2(G[0, :4], g["green_m0"]) <= 1e-13
     assert rel_l2(G[-1, :4], g["green_mlast"]) <= 1e-13
     s.close()
+
+
+@pytest.mark.parametrize("grid", [(34, 26, 64, 1.0 / 30.0, 2, 30), (66, 66, 64, 1.0 / 62.0, 2, 30),
+                                  (20, 14, 32, 1.0 / 18.0, 1, 8), (18, 16, 32, 1.0 / 16.0, 3, 6)],
+                         ids=["34x26x64", "66x66x64", "isym1", "isym3"])
+def test_mixed_converged_within_1e9_of_fp64(oracle_mod, bph, grid):
+    """FP32 ADI + FP64 residual/update refinement converges to the FP64 discrete
+    solution: relative L2 error <= 1e-9 against the GPU FP64 converged solve
+    and against the oracle's converged solve (north-star bound for the mixed form)."""
+    numr, numz, numphi, dr, isym, _ = grid
+    g = bph.PotentialSolver(*grid)
+    rho = smooth_density(numr, numz, numphi, dr, isym)
+    p64, i64 = g.solve_converged(rho, 20, True, 1e-13, 200)
+    pmx, imx = g.solve_converged_mixed(rho, 20, True, 1e-13, 200)
+    assert rel_l2(pmx, p64) <= 1e-9, (rel_l2(pmx, p64), imx.cycles, i64.cycles)
+    o = oracle_mod.Oracle(*grid)
+    po, _, _ = o.solve_converged(rho, 20, True, 1e-13, 200)
+    assert rel_l2(pmx, po) <= 1e-9
+    assert imx.residual <= 10 * max(i64.residual, 1e-12)
+    # warm start from the previous solution with a rotated density
+    rho2 = np.asfortranarray(np.roll(rho, 1, axis=2))
+    p64w, _ = g.solve_converged(rho2, 20, False, 1e-13, 200)
+    pmxw, imw = g.solve_converged_mixed(rho2, 20, False, 1e-13, 200)
+    assert rel_l2(pmxw, p64w) <= 1e-9
+    g.close()
+
+
+@pytest.mark.parametrize("nsteps", [10, 20])
+def test_mixed_converged_production_grid(bph, nsteps):
+    """130x98x256 bipolytrope pair: the mixed form stays within 1e-9 of the
+    FP64 converged potential (cold, then warm on the rotated density)."""
+    from bipoly_hydro_b200 import fields
+
+    g = bph.PotentialSolver(130, 98, 256, 1.0 / 126.0, 2, 30)
+    rho = fields.bipolytrope_pair()
+    p64, _ = g.solve_converged(rho, nsteps, True, 1e-13, 60)
+    pmx, imx = g.solve_converged_mixed(rho, nsteps, True, 1e-13, 60)
+    assert rel_l2(pmx, p64) <= 1e-9, (rel_l2(pmx, p64), imx.cycles)
+    rho2 = fields.rotate(rho)
+    p64w, _ = g.solve_converged(rho2, nsteps, False, 1e-13, 60)
+    pmxw, imw = g.solve_converged_mixed(rho2, nsteps, False, 1e-13, 60)
+    assert rel_l2(pmxw, p64w) <= 1e-9, (rel_l2(pmxw, p64w), imw.cycles)
+    g.close()
