@@ -13,6 +13,11 @@ larger than the 126 MB L2.
   e2e        solves/s through the host-array C ABI call: pinned rho copied in
              and pot copied out inside every step
   roofline   k_green_contract (the dominant kernel) against measured HBM
+  batched    warm solves of n independent instances per call (one pass over
+             the Green tables for all n): solves/s per batch size
+  converged  the same sequence solved to convergence in FP64 and in the
+             mixed form (FP32 ADI cycles, FP64 residual/update refinement):
+             solves/s, p50/p99 latency, and the mixed form's error vs FP64
   cpu_baseline  the CPU oracle (C restatement of the reference algorithm)
              on this host
 
@@ -267,7 +272,7 @@ def run_gpu(args, world, rank, local):
     base = fields.bipolytrope_pair(numr, numz, numphi, GRID["dr"], GRID["isym"], mass_ratio=0.5)
     base_t = torch.from_numpy(np.ascontiguousarray(base.ravel(order="F"))).to(dev)
     c_view = base_t.view(numphi, numz, numr)  # C view of the Fortran (numr, numz, numphi) array
-    nrot = numphi
+    nrot = args.rotations if args.rotations > 0 else numphi
     rhos = torch.empty((nrot, ntot), dtype=torch.float64, device=dev)
     for i in range(nrot):
         rhos[i].copy_(torch.roll(c_view, shifts=i + rank, dims=0).reshape(-1))
@@ -355,13 +360,13 @@ def run_gpu(args, world, rank, local):
     barrier(world)
     torch.cuda.synchronize()
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    lat = []
+    e2e_lat = []
     e2.record(stream)
     for i in range(n_e2e):
         t0 = time.perf_counter()
         rc = lib.bph_potential_solver(solver._h, ctypes.c_void_p(rho_np[i % npin].ctypes.data),
                                       ctypes.c_void_p(pot_np.ctypes.data), tstep)
-        lat.append(time.perf_counter() - t0)
+        e2e_lat.append(time.perf_counter() - t0)
         tstep += 1
         if rc != 0:
             raise RuntimeError(lib.bph_last_error().decode())
@@ -370,6 +375,65 @@ def run_gpu(args, world, rank, local):
     barrier(world)
     ms_e2e = max_over_ranks(e2.elapsed_time(e3), world)
     e2e_value = job_rate(n_e2e, world, ms_e2e)
+
+    # ---- batched solves: n instances per call, one table pass ----------
+    batched = None
+    if args.batch_sizes:
+        batched = {}
+        for nb_ in [int(x) for x in args.batch_sizes.split(",") if x]:
+            bt = B.Batch(solver, nb_)
+            ins = [rhos[(7 * i) % nrot] for i in range(nb_)]
+            outs = [torch.empty(ntot, dtype=torch.float64, device=dev) for _ in range(nb_)]
+            bt.solve_device(ins, outs, 0)
+            for w in range(3):
+                bt.solve_device(ins, outs, 2 + w)
+            calls = max(3, args.batch_calls)
+            ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            ea.record(stream)
+            for k in range(calls):
+                ins = [rhos[(7 * i + k + 1) % nrot] for i in range(nb_)]
+                bt.solve_device(ins, outs, 5 + k)
+            eb.record(stream)
+            torch.cuda.synchronize()
+            ms = ea.elapsed_time(eb)
+            batched[str(nb_)] = {"solves_per_s": nb_ * calls / (ms / 1e3), "ms_per_call": ms / calls}
+            del outs
+            bt.close()
+
+    # ---- converged solves: FP64 vs mixed (FP32 ADI + FP64 refinement) --
+    conv = None
+    if args.converged_steps > 0:
+        conv = {}
+        nconv = args.converged_steps
+        ref_pots = []
+        for mixed in (False, True):
+            # start both forms from the same converged potential of rhos[0]
+            solver.solve_converged_device(rhos[0], d_pot, args.conv_nsteps, True, 1e-13, 100, False)
+            lat, cycles, pots = [], [], []
+            for i in range(nconv):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                info = solver.solve_converged_device(rhos[(1 + i) % nrot], d_pot, args.conv_nsteps, False,
+                                                     args.conv_tol, 100, mixed)
+                torch.cuda.synchronize()
+                lat.append(time.perf_counter() - t0)
+                cycles.append(info.cycles)
+                pots.append(d_pot.clone())
+            key = "mixed" if mixed else "fp64"
+            if not mixed:
+                ref_pots = pots
+            err = None
+            if mixed:
+                err = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) for a, b in zip(pots, ref_pots))
+            conv[key] = {"solves_per_s": nconv / sum(lat), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+                         "p99_ms": 1e3 * float(np.percentile(lat, 99)), "mean_cycles": float(np.mean(cycles)),
+                         "max_rel_err_vs_fp64": err}
+            del pots
+        conv["nsteps_per_cycle"] = args.conv_nsteps
+        conv["tol_update"] = args.conv_tol
+        conv["speedup_mixed_vs_fp64"] = conv["mixed"]["solves_per_s"] / conv["fp64"]["solves_per_s"]
+        del ref_pots
 
     # ---- CPU baseline (rank 0, N = 1 only) ------------------------------
     cpu = None
@@ -382,6 +446,7 @@ def run_gpu(args, world, rank, local):
                "sample": f"{n} warm solves of the same sequence in {el:.1f} s after an untimed setup "
                          f"(C restatement of potential_solver, OpenMP)"}
 
+    solver_info = solver.info()
     solver.close()
     if rank == 0:
         line = {
@@ -394,12 +459,16 @@ def run_gpu(args, world, rank, local):
             "zone_updates_per_s": value * ntot * 5,
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 8 * ntot,
                     "d2h_bytes_per_step": 8 * ntot,
-                    "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99))},
+                    "p50_ms": 1e3 * float(np.percentile(e2e_lat, 50)),
+                    "p99_ms": 1e3 * float(np.percentile(e2e_lat, 99))},
             "roofline": {"bound": "hbm", "kernel": "k_green_contract", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "alg_bytes_per_launch": cb,
                          "solve_alg_bytes": b_alg, "solve_gbs": solve_gbs, "solve_frac": solve_gbs / peak},
             "phase_ms": phases,
+            "converged": conv,
+            "batched": batched,
+            "launch_config": solver_info,
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,
@@ -417,6 +486,14 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
+    ap.add_argument("--batch-sizes", default="4,16", help="batched warm solves timed per batch size (empty skips)")
+    ap.add_argument("--batch-calls", type=int, default=20)
+    ap.add_argument("--converged-steps", type=int, default=20,
+                    help="warm converged solves timed per form (FP64 and mixed); 0 skips")
+    ap.add_argument("--conv-nsteps", type=int, default=10, help="ADI steps per refinement cycle")
+    ap.add_argument("--conv-tol", type=float, default=1e-11, help="stop when |dphi|/|phi| <= tol")
+    ap.add_argument("--rotations", type=int, default=0,
+                    help="resident density rotations (0: numphi); small values make a small profiling case")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -16,12 +16,13 @@ from .solver import (  # noqa: F401
     BphError,
     Grid,
     PotentialSolver,
+    Batch,
     load_library,
     version,
 )
 
 __all__ = [
-    "PotentialSolver", "Grid", "BphError", "load_library", "version", "LIB_PATH", "EXPORTED_SYMBOLS",
+    "PotentialSolver", "Batch", "Grid", "BphError", "load_library", "version", "LIB_PATH", "EXPORTED_SYMBOLS",
     "BPH_OK", "BPH_ERR_INVALID", "BPH_ERR_NOMEM", "BPH_ERR_NONFINITE", "BPH_ERR_CUDA", "BPH_ERR_TIMEOUT",
     "BPH_ERR_STATE",
 ]

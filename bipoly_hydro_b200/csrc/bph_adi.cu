@@ -322,7 +322,10 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
     using T2 = typename Vec2<T>::type;
     extern __shared__ __align__(16) unsigned char smraw[];
     T *sm = reinterpret_cast<T *>(smraw);
-    const int s = blockIdx.x, tid = threadIdx.x;
+    // blockIdx.x = instance * N + slot: the slot picks the coefficients, the
+    // block index the slab (batches keep instances' slot arrays contiguous)
+    const int s = blockIdx.x % a.N, tid = threadIdx.x;
+    const long long blk = blockIdx.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = kSegThreads / 32;
     const int nr = a.nr, nz = a.nz, numr = a.numr, numz = a.numz;
     const SegLayout Lo = seg_layout(nr, nz);
@@ -340,8 +343,8 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
     T2 *AB = reinterpret_cast<T2 *>(abp);
     T *zrow = abp + 2 * nr;
     const long long nplane = (long long)numr * numz;
-    double *Pg = a.P + (long long)s * nplane;
-    const double *Rs = a.R + (long long)s * nr * nz;
+    double *Pg = a.P + blk * nplane;
+    const double *Rs = a.R + blk * nr * nz;
     const double gamma = a.gamma;
     const T gam_t = (T)gamma;
     const double a_side = a.alphar[numr - 2];  // alphar(numr-1)
@@ -629,7 +632,7 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
             double t = 0.0;
             for (int w = 0; w < nwarps; ++w) t += red[2 * w + tid];
             const double wgt = (s == 0 || s == a.N / 2) ? 1.0 : 2.0;
-            a.norms[2 * s + tid] = wgt * t;
+            a.norms[2 * blk + tid] = wgt * t;
         }
     }
 }
@@ -677,7 +680,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_adi_delta(AdiArgs a) {
     using T2 = float2;
     extern __shared__ __align__(16) unsigned char smraw[];
     T *sm = reinterpret_cast<T *>(smraw);
-    const int s = blockIdx.x, tid = threadIdx.x;
+    const int s = blockIdx.x % a.N, tid = threadIdx.x;
+    const long long blk = blockIdx.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = kThreads / 32;
     const int nr = a.nr, nz = a.nz, numr = a.numr, numz = a.numz;
     const DeltaLayout Lo = delta_layout(nr, nz);
@@ -693,8 +697,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_adi_delta(AdiArgs a) {
     float4 *C4 = reinterpret_cast<float4 *>(c4p);
     T *bz = c4p + 4 * nr;
     const long long nplane = (long long)numr * numz;
-    double *Pg = a.P + (long long)s * nplane;
-    const double *Rs = a.R + (long long)s * nr * nz;
+    double *Pg = a.P + blk * nplane;
+    const double *Rs = a.R + blk * nr * nz;
     const double gamma = a.gamma;
     const T g = (T)gamma;
     const bool sym_bottom = (a.isym != 1);
@@ -879,7 +883,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_adi_delta(AdiArgs a) {
         double t = 0.0;
         for (int w = 0; w < nwarps; ++w) t += red[2 * w + tid];
         const double wgt = (s == 0 || s == a.N / 2) ? 1.0 : 2.0;
-        a.norms[2 * s + tid] = wgt * t;
+        a.norms[2 * blk + tid] = wgt * t;
     }
 }
 
@@ -1021,19 +1025,31 @@ AdiArgs make_args(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bo
     return a;
 }
 
-cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bool cold) {
+cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bool cold, double *P,
+                       const double *R, int ninst) {
     AdiArgs a = make_args(c, sch, step0, nsteps_run, cold);
-    ++c->launches;
+    if (P) a.P = P;
+    if (R) a.R = R;
     if (c->adi_seg) {
+        ++c->launches;
         void *args[] = {&a};
-        return cudaLaunchKernel(seg_kernel<double, false>(c->adi_seg, c->adi_full), dim3(c->N), dim3(c->adi_seg),
-                                args, (size_t)c->adi_smem, c->stream);
-    } else if (c->adi_smem > 0) {
-        k_adi<true><<<c->N, kAdiThreads, c->adi_smem, c->stream>>>(a);
-    } else {
-        k_adi<false><<<c->N, kAdiThreads, smalls_bytes(c), c->stream>>>(a);
+        return cudaLaunchKernel(seg_kernel<double, false>(c->adi_seg, c->adi_full), dim3(c->N * ninst),
+                                dim3(c->adi_seg), args, (size_t)c->adi_smem, c->stream);
     }
-    return cudaGetLastError();
+    // other variants: one launch per instance
+    for (int i = 0; i < ninst; ++i) {
+        AdiArgs ai = a;
+        ai.P = a.P + (long long)i * c->N * c->nplane;
+        ai.R = a.R + (long long)i * c->N * c->np;
+        ++c->launches;
+        if (c->adi_smem > 0)
+            k_adi<true><<<c->N, kAdiThreads, c->adi_smem, c->stream>>>(ai);
+        else
+            k_adi<false><<<c->N, kAdiThreads, smalls_bytes(c), c->stream>>>(ai);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {

@@ -320,12 +320,13 @@ int setup_impl(bph_ctx *c) {
 }
 
 // The five-kernel solve on device arrays (see the file comment).
-int solve_device(bph_ctx *c, const double *d_rho, double *d_pot, const Schedule &s, bool cold) {
+int solve_device(bph_ctx *c, const double *d_rho, double *d_pot, const Schedule &s, bool cold,
+                 double *d_phieff = nullptr, double omega = 0.0) {
     BPH_CUDA(launch_fft_fwd_rho(c, d_rho));
     BPH_CUDA(launch_green_contract(c));
     BPH_CUDA(launch_boundary_slots(c));
     BPH_CUDA(launch_adi(c, s, 0, s.nsteps, cold));
-    BPH_CUDA(launch_fft_inv(c, d_pot));
+    BPH_CUDA(launch_fft_inv(c, d_pot, d_phieff, omega));
     c->have_warm = true;
     return BPH_OK;
 }
@@ -376,6 +377,9 @@ int set_device_of(bph_ctx *c) {
 }
 
 }  // namespace
+
+int batch_schedule(bph_ctx *c, int nsteps, Schedule **out) { return get_schedule(c, nsteps, out); }
+
 }  // namespace bph
 
 using namespace bph;
@@ -417,7 +421,8 @@ int bph_destroy(bph_ctx_t *c) {
     for (auto &s : c->sched) free_schedule(c, s);
     double *bufs[] = {c->d_green, c->d_brb,  c->d_elz, c->d_alphar, c->d_betar,     c->d_bzb,
                       c->d_qcoef, c->d_grid, c->d_R,   c->d_P,      c->d_prev,      c->d_mom,
-                      c->d_S,     c->d_W,    c->d_P2,  c->d_red,    c->d_rho_stage, c->d_pot_stage};
+                      c->d_S,     c->d_W,    c->d_P2,  c->d_red,    c->d_rho_stage, c->d_pot_stage,
+                      c->d_phieff_stage};
     for (double *p : bufs) dev_free(p);
     dev_free(c->d_tw);
     dev_free(c->d_tw2);
@@ -613,6 +618,50 @@ int bph_solve_converged_mixed(bph_ctx_t *c, const double *rho, double *pot, int 
     c->have_warm = true;
     if (!on_device) BPH_CUDA(cudaMemcpyAsync(pot, d_pot, bytes, cudaMemcpyDeviceToHost, c->stream));
     return read_status(c);
+}
+
+int bph_potential_solver_phieff(bph_ctx_t *c, const double *rho, double *pot, double *phieff, double omega_frame,
+                                int tstep, int on_device) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    if (!rho || !pot || !phieff || !std::isfinite(omega_frame)) {
+        set_error("rho, pot and phieff must be non-NULL and omega_frame finite");
+        return BPH_ERR_INVALID;
+    }
+    if ((rc = set_device_of(c))) return rc;
+    bool warm = tstep > 1;
+    Schedule *s;
+    if ((rc = get_schedule(c, warm ? 5 : 20, &s))) return rc;
+    if (on_device) return solve_device(c, rho, pot, *s, !warm, phieff, omega_frame);
+    if ((rc = ensure_staging(c))) return rc;
+    if (!c->d_phieff_stage && (rc = dev_alloc(c, &c->d_phieff_stage, (size_t)c->ntot))) return rc;
+    const size_t bytes = sizeof(double) * (size_t)c->ntot;
+    BPH_CUDA(cudaMemcpyAsync(c->d_rho_stage, rho, bytes, cudaMemcpyHostToDevice, c->stream));
+    if ((rc = solve_device(c, c->d_rho_stage, c->d_pot_stage, *s, !warm, c->d_phieff_stage, omega_frame))) return rc;
+    BPH_CUDA(cudaMemcpyAsync(pot, c->d_pot_stage, bytes, cudaMemcpyDeviceToHost, c->stream));
+    BPH_CUDA(cudaMemcpyAsync(phieff, c->d_phieff_stage, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return read_status(c);
+}
+
+int bph_set_potential(bph_ctx_t *c, const double *pot, int on_device) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    if (!pot) {
+        set_error("pot must be non-NULL");
+        return BPH_ERR_INVALID;
+    }
+    if ((rc = set_device_of(c))) return rc;
+    const double *d_pot = pot;
+    if (!on_device) {
+        if ((rc = ensure_staging(c))) return rc;
+        BPH_CUDA(cudaMemcpyAsync(c->d_pot_stage, pot, sizeof(double) * (size_t)c->ntot, cudaMemcpyHostToDevice,
+                                 c->stream));
+        d_pot = c->d_pot_stage;
+    }
+    BPH_CUDA(launch_fft_fwd_pot(c, d_pot));
+    c->have_warm = true;
+    if (!on_device) BPH_CUDA(cudaStreamSynchronize(c->stream));
+    return BPH_OK;
 }
 
 int bph_run_phase(bph_ctx_t *c, int phase, const double *d_rho, double *d_pot, int nsteps) {

@@ -1,0 +1,246 @@
+// bph_batch.cu -- many independent solves on one grid.
+//
+// A batch owns the per-instance state of n solves that share a context's
+// Green tables, trig data and ADI factors: the slot arrays P (each
+// instance's warm state, contiguous as [n][numphi][plane] so that the ADI
+// runs as one launch over n*numphi slots), -4 pi rho_hat and the moments.
+//
+// Per call (all instances at the same tstep):
+//   k_fft_fwd<rho>      per instance; moments in the layout mom[m][i][cos|sin][p]
+//   DGEMM, per mode m   C_m (nb x 2n) = G_m^T (nb x np) * M_m (np x 2n): every
+//                       instance's boundary moments from ONE pass over the
+//                       tables (the single-solve contraction is a GEMV that
+//                       reads the whole table per solve).  A plain strided-
+//                       batched library GEMM over the modes.
+//   k_boundary_slots_batch   Dirichlet slots of every instance from C
+//   k_adi_seg           one launch over n*numphi slots (no wave-quantisation
+//                       tail of a single 256-slot launch)
+//   k_fft_inv           per instance
+#include <cublas_v2.h>
+
+#include <cmath>
+#include <vector>
+
+#include "bph_internal.cuh"
+
+struct bph_batch {
+    bph_ctx *c = nullptr;
+    int cap = 0;
+    double *d_P = nullptr;     // [cap][N][nplane]
+    double *d_R = nullptr;     // [cap][N][np]
+    double *d_mom = nullptr;   // [mmax][cap][2][np]
+    double *d_C = nullptr;     // [mmax][2cap][nb] column-major per mode
+    double *d_rho_stage = nullptr, *d_pot_stage = nullptr;  // [cap][ntot] for host arrays
+    cublasHandle_t blas = nullptr;
+    size_t bytes = 0;
+};
+
+namespace bph {
+namespace {
+
+// One thread per (instance, boundary row or corner, slot), as k_boundary_slots.
+__global__ void k_boundary_slots_batch(const double *__restrict__ C, const double2 *__restrict__ ph,
+                                       double *__restrict__ P, int numr, int numz, int nr, int nz, int nb, int N,
+                                       int mmax, int fm, int isym, double nfactor, int n, int cap) {
+    const int M = N / 2;
+    const int ncorner = (isym == 1) ? 2 : 1;
+    const long long per = (long long)(nb + ncorner) * N;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= per * n) return;
+    const int inst = (int)(t / per);
+    t -= inst * per;
+    const int s = (int)(t % N), b = (int)(t / N);
+    const long long nplane = (long long)numr * numz;
+    double *Pi = P + (long long)inst * N * nplane;
+    int jz, kz;
+    if (b < nr) {
+        jz = b + 1;
+        kz = numz - 1;
+    } else if (b < nr + nz) {
+        jz = numr - 1;
+        kz = b - nr + 1;
+    } else if (b < nb) {
+        jz = b - nr - nz + 1;
+        kz = 0;
+    } else {
+        jz = numr - 1;
+        kz = (b == nb) ? numz - 1 : 0;
+        Pi[(long long)s * nplane + jz + (long long)numr * kz] = 0.0;
+        return;
+    }
+    const bool imag = s > M;
+    const int k = imag ? s - M : s;
+    double v = 0.0;
+    if (k < M && k % fm == 0 && k / fm < mmax) {
+        const int m = k / fm;
+        const double *Cm = C + (long long)m * (2LL * cap) * nb;
+        const double sc = Cm[(2LL * inst) * nb + b];
+        const double ss = (m == 0) ? 0.0 : Cm[(2LL * inst + 1) * nb + b];
+        const double2 w = ph[m];
+        v = imag ? nfactor * (w.y * sc - w.x * ss) : nfactor * (w.x * sc + w.y * ss);
+    }
+    Pi[(long long)s * nplane + jz + (long long)numr * kz] = v;
+}
+
+int batch_alloc(bph_batch *b, double **p, size_t count) {
+    cudaError_t e = cudaMalloc((void **)p, sizeof(double) * (count ? count : 1));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        set_error("batch allocation of %zu bytes failed: %s", sizeof(double) * count, cudaGetErrorString(e));
+        return BPH_ERR_NOMEM;
+    }
+    b->bytes += sizeof(double) * count;
+    return BPH_OK;
+}
+
+int blas_fail(cublasStatus_t st, const char *what) {
+    set_error("cuBLAS error %d in %s", (int)st, what);
+    return BPH_ERR_CUDA;
+}
+
+}  // namespace
+
+// Schedules are shared with the single-solve path (bph_api.cu).
+int batch_schedule(bph_ctx *c, int nsteps, Schedule **out);
+
+}  // namespace bph
+
+using namespace bph;
+
+extern "C" {
+
+int bph_batch_create(bph_ctx_t *c, int capacity, bph_batch_t **out) {
+    if (!out) {
+        set_error("out-pointer is NULL");
+        return BPH_ERR_INVALID;
+    }
+    *out = nullptr;
+    if (!c || capacity < 1 || capacity > 4096) {
+        set_error("invalid context or capacity (1..4096)");
+        return BPH_ERR_INVALID;
+    }
+    if (!c->adi_seg) {
+        set_error("batched solves need the on-chip ADI kernel (grid too large)");
+        return BPH_ERR_INVALID;
+    }
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    size_t need = sizeof(double) * (size_t)capacity *
+                  ((size_t)c->N * c->nplane + (size_t)c->N * c->np + 2ull * c->g.mmax * c->np + 2ull * c->g.mmax * c->nb);
+    size_t free_b = 0, total_b = 0;
+    e = cudaMemGetInfo(&free_b, &total_b);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemGetInfo");
+    if (need + (64ull << 20) > free_b) {
+        set_error("batch of %d needs %zu bytes of device memory, %zu free", capacity, need, free_b);
+        return BPH_ERR_NOMEM;
+    }
+    bph_batch *b = new bph_batch();
+    b->c = c;
+    b->cap = capacity;
+    int rc = BPH_OK;
+    if (!rc) rc = batch_alloc(b, &b->d_P, (size_t)capacity * c->N * c->nplane);
+    if (!rc) rc = batch_alloc(b, &b->d_R, (size_t)capacity * c->N * c->np);
+    if (!rc) rc = batch_alloc(b, &b->d_mom, (size_t)c->g.mmax * capacity * 2 * c->np);
+    if (!rc) rc = batch_alloc(b, &b->d_C, (size_t)c->g.mmax * 2 * capacity * c->nb);
+    if (!rc) {
+        e = cudaMemsetAsync(b->d_P, 0, sizeof(double) * (size_t)capacity * c->N * c->nplane, c->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(b->d_mom, 0, sizeof(double) * (size_t)c->g.mmax * capacity * 2 * c->np,
+                                                  c->stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemsetAsync");
+    }
+    if (!rc) {
+        cublasStatus_t st = cublasCreate(&b->blas);
+        if (st != CUBLAS_STATUS_SUCCESS) rc = blas_fail(st, "cublasCreate");
+    }
+    if (rc) {
+        bph_batch_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return BPH_OK;
+}
+
+int bph_batch_destroy(bph_batch_t *b) {
+    if (!b) return BPH_OK;
+    if (b->c) cudaSetDevice(b->c->device);
+    if (b->c && b->c->stream) cudaStreamSynchronize(b->c->stream);
+    if (b->blas) cublasDestroy(b->blas);
+    double *bufs[] = {b->d_P, b->d_R, b->d_mom, b->d_C, b->d_rho_stage, b->d_pot_stage};
+    for (double *p : bufs)
+        if (p) cudaFree(p);
+    delete b;
+    return BPH_OK;
+}
+
+int bph_batch_solve(bph_batch_t *b, int n, const double *const *rho, double *const *pot, int tstep, int on_device) {
+    if (!b || !rho || !pot || n < 1 || n > b->cap) {
+        set_error("invalid batch arguments (n must be in 1..capacity)");
+        return BPH_ERR_INVALID;
+    }
+    for (int i = 0; i < n; ++i)
+        if (!rho[i] || !pot[i]) {
+            set_error("instance %d has a NULL array", i);
+            return BPH_ERR_INVALID;
+        }
+    bph_ctx *c = b->c;
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    const bool warm = tstep > 1;  // potential_solver.F90:80
+    Schedule *s;
+    int rc = batch_schedule(c, warm ? 5 : 20, &s);
+    if (rc) return rc;
+    const size_t bytes = sizeof(double) * (size_t)c->ntot;
+    std::vector<const double *> d_rho(n);
+    std::vector<double *> d_pot(n);
+    if (on_device) {
+        for (int i = 0; i < n; ++i) {
+            d_rho[i] = rho[i];
+            d_pot[i] = pot[i];
+        }
+    } else {
+        if (!b->d_rho_stage && (rc = batch_alloc(b, &b->d_rho_stage, (size_t)b->cap * c->ntot))) return rc;
+        if (!b->d_pot_stage && (rc = batch_alloc(b, &b->d_pot_stage, (size_t)b->cap * c->ntot))) return rc;
+        for (int i = 0; i < n; ++i) {
+            d_rho[i] = b->d_rho_stage + (size_t)i * c->ntot;
+            d_pot[i] = b->d_pot_stage + (size_t)i * c->ntot;
+            BPH_CUDA(cudaMemcpyAsync((void *)d_rho[i], rho[i], bytes, cudaMemcpyHostToDevice, c->stream));
+        }
+    }
+    const long long np = c->np;
+    const long long mstride = 2LL * b->cap * np;
+    for (int i = 0; i < n; ++i)
+        BPH_CUDA(launch_fft_fwd_rho(c, d_rho[i], b->d_R + (size_t)i * c->N * np, b->d_mom + 2LL * i * np, mstride));
+    // C_m = G_m^T M_m for every mode in one strided-batched DGEMM
+    {
+        cublasStatus_t st = cublasSetStream(b->blas, c->stream);
+        if (st != CUBLAS_STATUS_SUCCESS) return blas_fail(st, "cublasSetStream");
+        const double one = 1.0, zero = 0.0;
+        st = cublasDgemmStridedBatched(b->blas, CUBLAS_OP_T, CUBLAS_OP_N, c->nb, 2 * n, (int)np, &one, c->d_green,
+                                       (int)np, (long long)c->nb * np, b->d_mom, (int)np, mstride, &zero, b->d_C,
+                                       c->nb, 2LL * b->cap * c->nb, c->g.mmax);
+        if (st != CUBLAS_STATUS_SUCCESS) return blas_fail(st, "cublasDgemmStridedBatched");
+    }
+    {
+        const int ncorner = (c->g.isym == 1) ? 2 : 1;
+        const long long total = (long long)(c->nb + ncorner) * c->N * n;
+        ++c->launches;
+        k_boundary_slots_batch<<<(unsigned)((total + 255) / 256), 256, 0, c->stream>>>(
+            b->d_C, c->d_ph, b->d_P, c->g.numr, c->g.numz, c->nr, c->nz, c->nb, c->N, c->g.mmax, c->fm, c->g.isym,
+            (double)c->N * c->factor, n, b->cap);
+        BPH_CUDA(cudaGetLastError());
+    }
+    BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, !warm, b->d_P, b->d_R, n));
+    for (int i = 0; i < n; ++i)
+        BPH_CUDA(launch_fft_inv(c, d_pot[i], nullptr, 0.0, b->d_P + (size_t)i * c->N * c->nplane));
+    if (!on_device) {
+        for (int i = 0; i < n; ++i)
+            BPH_CUDA(cudaMemcpyAsync(pot[i], d_pot[i], bytes, cudaMemcpyDeviceToHost, c->stream));
+        return bph_synchronize(c);
+    }
+    return BPH_OK;
+}
+
+size_t bph_batch_device_bytes(const bph_batch_t *b) { return b ? b->bytes : 0; }
+
+}  // extern "C"

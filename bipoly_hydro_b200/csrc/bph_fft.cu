@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(FftShape<M>::kThreads)
 k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__restrict__ mom,
           const double2 *__restrict__ g_tw, const double2 *__restrict__ g_tw2, const double2 *__restrict__ g_ph,
           int numr, int numz, int nr, int nz, int mmax, int fm, int isym, double four_pi,
-          int *__restrict__ status) {
+          int *__restrict__ status, long long mstride) {
     constexpr int NT = FftShape<M>::kThreads;
     extern __shared__ double2 smem[];
     double2 *C = smem;
@@ -209,8 +209,8 @@ k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__re
                     tc = ph.x * F.x - ph.y * F.y;
                     ts = ph.y * F.x + ph.x * F.y;
                 }
-                mom[(2LL * m) * np + p] = tc;
-                mom[(2LL * m + 1) * np + p] = ts;
+                mom[m * mstride + p] = tc;
+                mom[m * mstride + np + p] = ts;
             }
         } else {
             double *o = out + jz + (long long)numr * kz;
@@ -235,10 +235,14 @@ k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__re
 // phi(2,K,l+N/2) (isym 3: phi(2,K,l)) and the equator condition
 // phi(J,1,l) = phi(J,2,l) (isym 2,3) taken at the source: those columns
 // transform the source column's spectrum (shifted by N/2 = sign (-1)^k).
+// With phieff != nullptr the epilogue also writes the effective potential
+// phieff = pot - 0.5 omega^2 rhf(J)^2 that the hydro source step forms from
+// pot (source.F90:156, make_source_temp.F90:121), saving it a full pass.
 template <int M>
 __global__ void __launch_bounds__(FftShape<M>::kThreads)
 k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 *__restrict__ g_tw,
-          const double2 *__restrict__ g_tw2, int numr, int numz, int isym) {
+          const double2 *__restrict__ g_tw2, int numr, int numz, int isym, double *__restrict__ phieff,
+          const double *__restrict__ rhf, double omega) {
     constexpr int NT = FftShape<M>::kThreads;
     extern __shared__ double2 smem[];
     double2 *C = smem;
@@ -319,6 +323,18 @@ k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 
                 col[nplane * (2 * n)] = z.x * scale;
                 col[nplane * (2 * n + 1)] = z.y * scale;
             }
+            if (phieff) {
+                const double r = rhf[q % numr];
+                const double cen = 0.5 * omega * omega * r * r;
+                double *pe = phieff + q;
+#pragma unroll
+                for (int i = 0; i < kLoads; ++i) {
+                    const int n = n0 + i * kRowsPerPass;
+                    const double2 z = C[n * kTile + c];
+                    pe[nplane * (2 * n)] = z.x * scale - cen;
+                    pe[nplane * (2 * n + 1)] = z.y * scale - cen;
+                }
+            }
         }
     }
 }
@@ -336,11 +352,11 @@ cudaError_t set_fft_attrs(bph_ctx *c) {
 }
 
 template <int M>
-cudaError_t fwd_rho(bph_ctx *c, const double *rho) {
+cudaError_t fwd_rho(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride) {
     unsigned blocks = (unsigned)((c->np + kTile - 1) / kTile);
     k_fft_fwd<M, true><<<blocks, FftShape<M>::kThreads, FftShape<M>::kSmem, c->stream>>>(
-        rho, c->d_R, c->d_mom, c->d_tw, c->d_tw2, c->d_ph, c->g.numr, c->g.numz, c->nr, c->nz, c->g.mmax, c->fm,
-        c->g.isym, c->four_pi, c->d_status);
+        rho, R, mom, c->d_tw, c->d_tw2, c->d_ph, c->g.numr, c->g.numz, c->nr, c->nz, c->g.mmax, c->fm,
+        c->g.isym, c->four_pi, c->d_status, mstride);
     return cudaGetLastError();
 }
 
@@ -349,15 +365,15 @@ cudaError_t fwd_pot(bph_ctx *c, const double *pot) {
     unsigned blocks = (unsigned)((c->np + kTile - 1) / kTile);
     k_fft_fwd<M, false><<<blocks, FftShape<M>::kThreads, FftShape<M>::kSmem, c->stream>>>(
         pot, c->d_P, nullptr, c->d_tw, c->d_tw2, c->d_ph, c->g.numr, c->g.numz, c->nr, c->nz, c->g.mmax, c->fm,
-        c->g.isym, c->four_pi, c->d_status);
+        c->g.isym, c->four_pi, c->d_status, 0);
     return cudaGetLastError();
 }
 
 template <int M>
-cudaError_t inv(bph_ctx *c, double *pot) {
+cudaError_t inv(bph_ctx *c, double *pot, double *phieff, double omega, const double *P) {
     unsigned blocks = (unsigned)((c->nplane + kTile - 1) / kTile);
     k_fft_inv<M><<<blocks, FftShape<M>::kThreads, FftShape<M>::kSmem, c->stream>>>(
-        c->d_P, pot, c->d_tw, c->d_tw2, c->g.numr, c->g.numz, c->g.isym);
+        P, pot, c->d_tw, c->d_tw2, c->g.numr, c->g.numz, c->g.isym, phieff, c->d_grid, omega);
     return cudaGetLastError();
 }
 
@@ -373,9 +389,13 @@ cudaError_t inv(bph_ctx *c, double *pot) {
     }
 
 cudaError_t set_attrs_dispatch(bph_ctx *c) { BPH_FFT_DISPATCH(set_fft_attrs, c) }
-cudaError_t fwd_rho_dispatch(bph_ctx *c, const double *rho) { BPH_FFT_DISPATCH(fwd_rho, c, rho) }
+cudaError_t fwd_rho_dispatch(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride) {
+    BPH_FFT_DISPATCH(fwd_rho, c, rho, R, mom, mstride)
+}
 cudaError_t fwd_pot_dispatch(bph_ctx *c, const double *pot) { BPH_FFT_DISPATCH(fwd_pot, c, pot) }
-cudaError_t inv_dispatch(bph_ctx *c, double *pot) { BPH_FFT_DISPATCH(inv, c, pot) }
+cudaError_t inv_dispatch(bph_ctx *c, double *pot, double *phieff, double omega, const double *P) {
+    BPH_FFT_DISPATCH(inv, c, pot, phieff, omega, P)
+}
 
 }  // namespace
 
@@ -385,9 +405,9 @@ int fft_configure(bph_ctx *c) {
     return BPH_OK;
 }
 
-cudaError_t launch_fft_fwd_rho(bph_ctx *c, const double *rho) {
+cudaError_t launch_fft_fwd_rho(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride) {
     ++c->launches;
-    return fwd_rho_dispatch(c, rho);
+    return fwd_rho_dispatch(c, rho, R ? R : c->d_R, mom ? mom : c->d_mom, mstride ? mstride : 2 * c->np);
 }
 
 cudaError_t launch_fft_fwd_pot(bph_ctx *c, const double *pot) {
@@ -395,9 +415,9 @@ cudaError_t launch_fft_fwd_pot(bph_ctx *c, const double *pot) {
     return fwd_pot_dispatch(c, pot);
 }
 
-cudaError_t launch_fft_inv(bph_ctx *c, double *pot) {
+cudaError_t launch_fft_inv(bph_ctx *c, double *pot, double *phieff, double omega, const double *P) {
     ++c->launches;
-    return inv_dispatch(c, pot);
+    return inv_dispatch(c, pot, phieff, omega, P ? P : c->d_P);
 }
 
 }  // namespace bph

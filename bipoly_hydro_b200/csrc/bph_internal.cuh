@@ -85,6 +85,7 @@ struct bph_ctx {
     double *d_red = nullptr;     // reduction scratch
     double *d_rho_stage = nullptr;
     double *d_pot_stage = nullptr;
+    double *d_phieff_stage = nullptr;
     int *d_status = nullptr;
     unsigned int *d_ccnt = nullptr;  // contraction arrival counters [mmax][row groups]
     double *d_cpart = nullptr;       // contraction partial sums [split][mmax][nb][2]
@@ -120,12 +121,16 @@ int cuda_fail(cudaError_t e, const char *what);
 cudaError_t launch_qcoef(bph_ctx *c);
 cudaError_t launch_green_tables(bph_ctx *c);
 cudaError_t launch_adi_factors(bph_ctx *c, Schedule &s);
-cudaError_t launch_fft_fwd_rho(bph_ctx *c, const double *rho);
+// Optional arguments select batch buffers (R, moments with m-stride, P, instance count).
+cudaError_t launch_fft_fwd_rho(bph_ctx *c, const double *rho, double *R = nullptr, double *mom = nullptr,
+                               long long mstride = 0);
 cudaError_t launch_fft_fwd_pot(bph_ctx *c, const double *pot);
-cudaError_t launch_fft_inv(bph_ctx *c, double *pot);
+cudaError_t launch_fft_inv(bph_ctx *c, double *pot, double *phieff = nullptr, double omega = 0.0,
+                           const double *P = nullptr);
 cudaError_t launch_green_contract(bph_ctx *c);
 cudaError_t launch_boundary_slots(bph_ctx *c);
-cudaError_t launch_adi(bph_ctx *c, const Schedule &s, int step0, int nsteps_run, bool cold);
+cudaError_t launch_adi(bph_ctx *c, const Schedule &s, int step0, int nsteps_run, bool cold, double *P = nullptr,
+                       const double *R = nullptr, int ninst = 1);
 cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &s);
 cudaError_t launch_update_norm(bph_ctx *c, double *d_out);
 cudaError_t launch_residual_norm(bph_ctx *c, double *d_out);

@@ -42,9 +42,10 @@ _ERR_NAMES = {
 #: Every symbol include/bph.h declares, in declaration order.
 EXPORTED_SYMBOLS = (
     "bph_setup", "bph_potential_solver", "bph_potential_solver_device", "bph_solve_nsteps",
-    "bph_solve_converged", "bph_solve_converged_mixed", "bph_set_stream", "bph_synchronize", "bph_destroy", "bph_last_error",
+    "bph_solve_converged", "bph_potential_solver_phieff", "bph_set_potential", "bph_solve_converged_mixed", "bph_set_stream", "bph_synchronize", "bph_destroy", "bph_last_error",
     "bph_version", "bph_num_boundary_rows", "bph_copy_green", "bph_copy_moments", "bph_run_phase",
     "bph_green_contract_noalloc", "bph_info", "bph_launch_count", "bph_device_bytes",
+    "bph_batch_create", "bph_batch_solve", "bph_batch_destroy", "bph_batch_device_bytes",
 )
 
 #: bph_run_phase phase ids.
@@ -92,6 +93,10 @@ def load_library(path: str | None = None):
     L.bph_solve_nsteps.argtypes = [vp, dp, dp, i, i, i]
     L.bph_solve_converged.argtypes = [vp, dp, dp, i, i, ctypes.c_double, i, i, ctypes.POINTER(i),
                                       ctypes.POINTER(ctypes.c_double)]
+    L.bph_potential_solver_phieff.argtypes = [vp, dp, dp, dp, ctypes.c_double, i, i]
+    L.bph_potential_solver_phieff.restype = ctypes.c_int
+    L.bph_set_potential.argtypes = [vp, dp, i]
+    L.bph_set_potential.restype = ctypes.c_int
     L.bph_solve_converged_mixed.argtypes = L.bph_solve_converged.argtypes
     L.bph_solve_converged_mixed.restype = ctypes.c_int
     L.bph_set_stream.argtypes = [vp, vp]
@@ -105,6 +110,14 @@ def load_library(path: str | None = None):
     L.bph_run_phase.argtypes = [vp, i, dp, dp, i]
     L.bph_green_contract_noalloc.argtypes = [vp, dp, dp]
     L.bph_green_contract_noalloc.restype = ctypes.c_int
+    L.bph_batch_create.argtypes = [vp, i, ctypes.POINTER(vp)]
+    L.bph_batch_create.restype = ctypes.c_int
+    L.bph_batch_solve.argtypes = [vp, i, ctypes.POINTER(vp), ctypes.POINTER(vp), i, i]
+    L.bph_batch_solve.restype = ctypes.c_int
+    L.bph_batch_destroy.argtypes = [vp]
+    L.bph_batch_destroy.restype = ctypes.c_int
+    L.bph_batch_device_bytes.argtypes = [vp]
+    L.bph_batch_device_bytes.restype = ctypes.c_size_t
     L.bph_info.argtypes = [vp, i]
     L.bph_info.restype = ctypes.c_longlong
     L.bph_launch_count.argtypes = [vp]
@@ -198,6 +211,22 @@ class PotentialSolver:
         _check(self._lib.bph_potential_solver(self._h, _host_ptr(r), _host_ptr(pot), int(tstep)))
         return pot
 
+    def potential_solver_phieff(self, rho, tstep: int, omega_frame: float):
+        """potential_solver plus phieff = pot - 0.5 omega^2 rhf^2 (source.F90:156)."""
+        r = self._rho_host(rho)
+        pot = np.empty(self.shape, dtype=np.float64, order="F")
+        phieff = np.empty(self.shape, dtype=np.float64, order="F")
+        _check(self._lib.bph_potential_solver_phieff(self._h, _host_ptr(r), _host_ptr(pot), _host_ptr(phieff),
+                                                     float(omega_frame), int(tstep), 0))
+        return pot, phieff
+
+    def set_potential(self, pot) -> None:
+        """Warm state from a (checkpointed) potential for the next tstep > 1 solve."""
+        a = np.asfortranarray(np.asarray(pot, dtype=np.float64))
+        if a.shape != self.shape:
+            raise ValueError(f"pot has shape {a.shape}, expected {self.shape}")
+        _check(self._lib.bph_set_potential(self._h, _host_ptr(a), 0))
+
     def solve_nsteps(self, rho, nsteps: int, cold: bool) -> np.ndarray:
         r = self._rho_host(rho)
         pot = np.empty(self.shape, dtype=np.float64, order="F")
@@ -290,3 +319,51 @@ class PotentialSolver:
 
 def version() -> str:
     return load_library().bph_version().decode()
+
+
+class Batch:
+    """Up to ``capacity`` independent solves on one solver's grid (bph_batch_*).
+
+    Instance i keeps its own warm state; one call solves instances 0..n-1 at
+    the same ``tstep`` with a single pass over the shared Green tables.
+    """
+
+    def __init__(self, solver: PotentialSolver, capacity: int):
+        self.solver = solver
+        self._lib = solver._lib
+        self.capacity = int(capacity)
+        h = ctypes.c_void_p()
+        _check(self._lib.bph_batch_create(solver._h, self.capacity, ctypes.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.bph_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, rhos, tstep: int):
+        """Host arrays: list of (numr, numz, numphi) densities -> list of potentials."""
+        rs = [self.solver._rho_host(r) for r in rhos]
+        pots = [np.empty(self.solver.shape, dtype=np.float64, order="F") for _ in rs]
+        n = len(rs)
+        arr_r = (ctypes.c_void_p * n)(*[a.ctypes.data for a in rs])
+        arr_p = (ctypes.c_void_p * n)(*[a.ctypes.data for a in pots])
+        _check(self._lib.bph_batch_solve(self._h, n, arr_r, arr_p, int(tstep), 0))
+        return pots
+
+    def solve_device(self, d_rhos, d_pots, tstep: int) -> None:
+        """Device arrays (pointers or CUDA tensors), enqueued on the solver's stream."""
+        n = len(d_rhos)
+        arr_r = (ctypes.c_void_p * n)(*[_dev_ptr(x) for x in d_rhos])
+        arr_p = (ctypes.c_void_p * n)(*[_dev_ptr(x) for x in d_pots])
+        _check(self._lib.bph_batch_solve(self._h, n, arr_r, arr_p, int(tstep), 1))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self._lib.bph_batch_device_bytes(self._h))

@@ -76,6 +76,20 @@ int bph_solve_converged(bph_ctx_t *ctx, const double *rho, double *pot, int nste
                         double tol, int max_cycles, int on_device, int *cycles_out,
                         double *resid_out);
 
+/* potential_solver plus the effective potential the hydro source step
+ * builds from pot next (source.F90:156, make_source_temp.F90:121):
+ * phieff(J,K,L) = pot(J,K,L) - 0.5*omega_frame^2*rhf(J)^2, written by the
+ * same kernel that writes pot.  on_device selects device or host arrays. */
+int bph_potential_solver_phieff(bph_ctx_t *ctx, const double *rho, double *pot, double *phieff,
+                                double omega_frame, int tstep, int on_device);
+
+/* Warm state from a potential, e.g. one read back from a continuation file
+ * (ritecont_frac_new.F90:151-160 writes pot): the next tstep > 1 solve
+ * starts its 5 ADI steps from this potential, as potential_solver does from
+ * its kept potp (potential_solver.F90:80-87).  The reference instead starts
+ * cold after a restart (setup_frac.F90:690). */
+int bph_set_potential(bph_ctx_t *ctx, const double *pot, int on_device);
+
 /* Mixed-precision converged solve (no counterpart in the reference, which
  * always runs a fixed 5 or 20 FP64 steps): iterative refinement in which
  * every cycle forms the FP64 residual -4 pi rho_hat - A phi, runs the nsteps
@@ -88,6 +102,27 @@ int bph_solve_converged(bph_ctx_t *ctx, const double *rho, double *pot, int nste
 int bph_solve_converged_mixed(bph_ctx_t *ctx, const double *rho, double *pot, int nsteps, int cold,
                               double tol, int max_cycles, int on_device, int *cycles_out,
                               double *resid_out);
+
+/* ---- batches: many independent solves on one grid ----------------- */
+
+/* A batch holds the warm states of up to `capacity` independent solves on
+ * the context's grid (SCF sweeps over mass ratio and separation, ensembles,
+ * many clients).  No counterpart in the reference, which solves one density
+ * per call.  The instances share the context's Green tables: one pass over
+ * the tables serves every instance's boundary potential. */
+typedef struct bph_batch bph_batch_t;
+int bph_batch_create(bph_ctx_t *ctx, int capacity, bph_batch_t **batch);
+
+/* potential_solver for instances 0..n-1 (n <= capacity), all at the same
+ * tstep (warm 5 steps if tstep > 1, else cold 20); instance i keeps its own
+ * warm state between calls.  rho[i]/pot[i] are device arrays when
+ * on_device != 0 (asynchronous on the context's stream), else host arrays
+ * (synchronous).  Results equal n separate bph_potential_solver calls to
+ * rounding. */
+int bph_batch_solve(bph_batch_t *batch, int n, const double *const *rho, double *const *pot, int tstep,
+                    int on_device);
+int bph_batch_destroy(bph_batch_t *batch);
+size_t bph_batch_device_bytes(const bph_batch_t *batch);
 
 /* Stream used for all later work of this context (a cudaStream_t; NULL is
  * CUDA's default stream).  Until the first call the context uses a

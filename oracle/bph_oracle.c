@@ -975,6 +975,12 @@ int orc_solve_converged(orc_ctx *c, const double *rho, double *pot, int nsteps, 
     return solve_common(c, rho, pot, nsteps, cold, 1, tol, max_cycles, cycles_out, resid_out);
 }
 
+/* Replaces the kept potential potp (COMMON /potarrays/) with pot, as a
+ * continuation restart that restored potp would. */
+void orc_set_potential(orc_ctx *c, const double *pot) {
+    memcpy(c->potp, pot, sizeof(double) * (size_t)c->ntot);
+}
+
 double orc_residual(orc_ctx *c, const double *rho, const double *pot) {
     const long ntot = c->ntot;
     double *ffr = malloc(sizeof(double) * (size_t)ntot);

@@ -55,6 +55,9 @@ int orc_solve_converged(orc_ctx *c, const double *rho, double *pot, int nsteps,
                         int cold, double tol, int max_cycles,
                         int *cycles_out, double *resid_out);
 
+/* Sets the kept potential potp (warm-start state) to pot. */
+void orc_set_potential(orc_ctx *c, const double *pot);
+
 /* Relative residual of a physical-space potential (after a solve) in slot
  * space, the same measure orc_solve_converged uses. */
 double orc_residual(orc_ctx *c, const double *rho, const double *pot);

@@ -56,6 +56,7 @@ def lib():
         L.orc_solve_converged.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                           ctypes.c_int, ctypes.POINTER(ctypes.c_int), dp]
         L.orc_solve_converged.restype = ctypes.c_int
+        L.orc_set_potential.argtypes = [vp, dp]
         L.orc_residual.argtypes = [vp, dp, dp]
         L.orc_residual.restype = ctypes.c_double
         L.orc_num_boundary_rows.argtypes = [vp]
@@ -179,6 +180,10 @@ class Oracle:
         pot = self._call(lib().orc_solve_converged, rho, int(nsteps), int(bool(cold)), float(tol),
                          int(max_cycles), ctypes.byref(cyc), ctypes.byref(res))
         return pot, cyc.value, res.value
+
+    def set_potential(self, pot) -> None:
+        p = np.asfortranarray(pot, dtype=np.float64)
+        lib().orc_set_potential(self._h, _dp(p))
 
     def residual(self, rho, pot) -> float:
         rho = self._check(rho)

@@ -1,0 +1,96 @@
+"""Batched solves (bph_batch_*): n independent densities on one grid share one
+pass over the Green tables; each instance keeps its own warm state.  Every
+instance must equal its own single-solve sequence (and the oracle) to the
+FP64 drop-in bar."""
+import numpy as np
+import pytest
+
+from tests.helpers import rel_l2, smooth_density
+
+pytestmark = pytest.mark.gpu
+
+
+def _densities(grid, n):
+    numr, numz, numphi, dr, isym, _ = grid
+    return [np.asfortranarray(smooth_density(numr, numz, numphi, dr, isym, seed=100 + i) * (1.0 + 0.1 * i))
+            for i in range(n)]
+
+
+@pytest.mark.parametrize("grid", [(34, 26, 64, 1.0 / 30.0, 2, 30), (20, 14, 32, 1.0 / 18.0, 1, 8),
+                                  (35, 21, 64, 1.0 / 31.0, 2, 12)], ids=["34x26x64", "isym1", "odd"])
+def test_batch_equals_single_solves(oracle_mod, bph, grid):
+    n = 5
+    rhos = _densities(grid, n)
+    solver = bph.PotentialSolver(*grid)
+    batch = bph.Batch(solver, capacity=8)
+    singles = [bph.PotentialSolver(*grid) for _ in range(n)]
+    oracles = [oracle_mod.Oracle(*grid) for _ in range(2)]
+    for tstep in (0, 2, 3):
+        if tstep:
+            rhos = [np.asfortranarray(np.roll(r, 1, axis=2)) for r in rhos]
+        got = batch.solve(rhos, tstep)
+        for i in range(n):
+            want = singles[i].potential_solver(rhos[i], tstep)
+            assert rel_l2(got[i], want) <= 1e-12, (tstep, i)
+        for i in range(2):
+            assert rel_l2(got[i], oracles[i].potential_solver(rhos[i], tstep)) <= 1e-12, (tstep, i)
+    batch.close()
+    for s in singles:
+        s.close()
+    solver.close()
+
+
+def test_batch_subset_keeps_other_states(bph):
+    """Solving instances 0..1 of a batch leaves instance 2's warm state alone."""
+    grid = (34, 26, 64, 1.0 / 30.0, 2, 30)
+    rhos = _densities(grid, 3)
+    solver = bph.PotentialSolver(*grid)
+    batch = bph.Batch(solver, capacity=3)
+    ref = [bph.PotentialSolver(*grid) for _ in range(3)]
+    batch.solve(rhos, 0)
+    for i in range(3):
+        ref[i].potential_solver(rhos[i], 0)
+    batch.solve(rhos[:2], 2)
+    for i in range(2):
+        ref[i].potential_solver(rhos[i], 2)
+    got = batch.solve(rhos, 3)
+    for i in range(3):
+        assert rel_l2(got[i], ref[i].potential_solver(rhos[i], 3)) <= 1e-12, i
+    batch.close()
+    solver.close()
+
+
+def test_batch_production_grid_device_arrays(bph):
+    import torch
+
+    from bipoly_hydro_b200 import fields
+
+    grid = (130, 98, 256, 1.0 / 126.0, 2, 30)
+    n = 4
+    rhos = [fields.bipolytrope_pair(mass_ratio=q) for q in (0.3, 0.5, 0.7, 1.0)]
+    solver = bph.PotentialSolver(*grid)
+    solver.set_stream(torch.cuda.current_stream())
+    batch = bph.Batch(solver, capacity=n)
+    d_rho = [torch.from_numpy(np.ascontiguousarray(r.ravel(order="F"))).cuda() for r in rhos]
+    d_pot = [torch.empty_like(x) for x in d_rho]
+    singles = [bph.PotentialSolver(*grid) for _ in range(n)]
+    for tstep in (0, 2):
+        batch.solve_device(d_rho, d_pot, tstep)
+        solver.synchronize()
+        for i in range(n):
+            want = singles[i].potential_solver(rhos[i], tstep)
+            got = d_pot[i].cpu().numpy().reshape(rhos[i].shape, order="F")
+            assert rel_l2(got, want) <= 1e-12, (tstep, i)
+    batch.close()
+    solver.close()
+
+
+def test_batch_rejects_bad_sizes(bph):
+    grid = (18, 18, 16, 1.0 / 14.0, 2, 6)
+    solver = bph.PotentialSolver(*grid)
+    batch = bph.Batch(solver, capacity=2)
+    rhos = _densities(grid, 3)
+    with pytest.raises(bph.BphError):
+        batch.solve(rhos, 0)
+    batch.close()
+    solver.close()

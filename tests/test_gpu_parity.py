@@ -213,3 +213,36 @@ def test_mixed_converged_production_grid(bph, nsteps):
     pmxw, imw = g.solve_converged_mixed(rho2, nsteps, False, 1e-13, 60)
     assert rel_l2(pmxw, p64w) <= 1e-9, (rel_l2(pmxw, p64w), imw.cycles)
     g.close()
+
+
+def test_phieff_fused_output(oracle_mod, bph):
+    """phieff = pot - 0.5 omega^2 rhf(J)^2 (source.F90:156) written beside pot."""
+    grid = (34, 26, 64, 1.0 / 30.0, 2, 30)
+    numr, numz, numphi, dr, isym, _ = grid
+    o, g = _pair(oracle_mod, bph, grid)
+    rho = smooth_density(numr, numz, numphi, dr, isym)
+    omega = 1.37
+    for tstep in (0, 2):
+        po = o.potential_solver(rho, tstep)
+        pg, pe = g.potential_solver_phieff(rho, tstep, omega)
+        rhf = (np.arange(1, numr + 1) - 2.0) * dr + 0.5 * dr
+        expect = po - (0.5 * omega * omega * rhf * rhf)[:, None, None]
+        assert rel_l2(pg, po) <= POT_TOL
+        assert rel_l2(pe, expect) <= POT_TOL
+    g.close()
+
+
+def test_warm_start_from_checkpointed_potential(oracle_mod, bph):
+    """A potential restored from a continuation file becomes the warm state."""
+    grid = (34, 26, 64, 1.0 / 30.0, 2, 30)
+    numr, numz, numphi, dr, isym, _ = grid
+    o, g = _pair(oracle_mod, bph, grid)
+    rho = smooth_density(numr, numz, numphi, dr, isym)
+    checkpoint = o.solve_nsteps(rho, 20, True)          # a saved pot
+    rho2 = np.asfortranarray(np.roll(rho, 1, axis=2))
+    o2, g2 = _pair(oracle_mod, bph, grid)               # fresh contexts: a restarted run
+    o2.set_potential(checkpoint)
+    g2.set_potential(checkpoint)
+    assert rel_l2(g2.potential_solver(rho2, 5), o2.potential_solver(rho2, 5)) <= POT_TOL
+    g.close()
+    g2.close()
