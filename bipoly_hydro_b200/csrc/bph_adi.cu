@@ -643,13 +643,29 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
 // One CTA per slot, two CTAs per SM.  Prologue: the FP64 residual
 // r = -4 pi rho_hat - A phi of the current potential (its Dirichlet columns
 // enter through the stencil), rounded to T.  Body: nsteps ADI steps of the
-// defect equation A delta = r in increment form,
-//   (Ar + dt) D1 = r - A delta,  delta += D1,
-//   (Az + dt) D2 = r - A delta,  delta += D2,
+// defect equation A delta = r in increment form: one radial half-step at the
+// first step's dt, then for every step
+//   (Az + dt) D1 = r - A delta,  delta += D1,
+//   (Ar + dt) D2 = r - A delta,  delta += D2,
 // which is the Peaceman-Rachford iteration of helmadi.F90 rewritten so that
 // every line solve sees a residual: in the plain form the intermediate
 // values of stiff near-axis components (A_r up to ~1e8 x dt) are amplified
 // thousands of times and T's rounding of them would not be recoverable.
+// Why the cycle starts and ends on a radial half-step: where A_r is stiff
+// (A_r ~ 4 k^2 / dr^2 near the axis at high k) and A_z + dt is small, a
+// vertical half-step multiplies what it is given in those components by
+// A_r / (A_z + dt), up to ~1e8 at 130 x 98 x 256.  In exact arithmetic the
+// next radial half-step takes it back out, but T's rounding of the
+// amplified values (eps32 x 1e8 ~ 6) stays.  A vertical half-step first
+// would amplify the stiff part of r (the previous cycle's rounding) and a
+// vertical half-step last would leave its own rounding in delta; either way
+// the outer refinement grew ~5x per cycle in high-k slots.  Opening with a
+// radial half-step at the largest dt (dt >= A_z everywhere, so the extra
+// factor (dt - A_z)/(dt + A_r) is a contraction) resolves the stiff residual
+// before any vertical half-step sees it, and closing on a radial half-step
+// removes the last vertical one's rounding.  The outer FP64 defect
+// correction converges to the same discrete solution whatever the inner
+// order.
 // Epilogue: phi += delta in FP64, per-slot |delta|^2 and |phi|^2.
 //
 // Shared memory (T): D = delta, Rv = r (both nz x ps), factor blocks Fr/Fz,
@@ -729,12 +745,75 @@ __global__ void __launch_bounds__(kThreads, 2) k_adi_delta(AdiArgs a) {
     __syncthreads();
 
     const int nitem_r = nz * Pr, nitem_z = nr * Pz;
-    for (int it = 0; it < a.nsteps_run; ++it) {
+    // Half-steps: radial at the first step's dt, then vertical and radial at
+    // every step's dt (2 nsteps + 1 line solves).
+    for (int h = 0; h <= 2 * a.nsteps_run; ++h) {
+        const bool radial_half = (h % 2) == 0;
+        const int it = radial_half ? max(h / 2 - 1, 0) : (h - 1) / 2;
         const int step = a.step0 + it;
-        const bool last_step = (it + 1 == a.nsteps_run);
-        const T dtt = (T)a.dt[step];
+        const bool reload = (h > 0) && (it + 1 < a.nsteps_run);
+        // ================= vertical: lines j, segments along k =================
+        if (!radial_half) {
+            const Fac<T> f = fac_view(Fz, nz);
+            T v[kAdiSeg];
+            const bool active = tid < nitem_z;
+            const int j = active ? tid % nr : 0, p = active ? tid / nr : 0;
+            const int k0 = p * kAdiSeg, len = kFull ? kAdiSeg : min(kAdiSeg, nz - k0);
+            const float4 cc = C4[j];
+            const bool has_l = j > 0, has_r = j + 1 < nr;
+            if (active) {
+                T L = 0.f;
+                T dd_ = (k0 > 0) ? D[(k0 - 1) * ps + j] : 0.f;
+                T dm = D[k0 * ps + j];
+#pragma unroll
+                for (int i = 0; i < kAdiSeg; ++i)
+                    if (kFull || i < len) {
+                        const int k = k0 + i;
+                        const T du_ = (k + 1 < nz) ? D[(k + 1) * ps + j] : 0.f;
+                        const T vl = has_l ? D[k * ps + j - 1] : 0.f, vr = has_r ? D[k * ps + j + 1] : 0.f;
+                        const T czn = (k > 0 || !sym_bottom) ? g : 0.f;
+                        const T rhs = Rv[k * ps + j] - (cc.x * dm + cc.y * vr + cc.z * vl) -
+                                      (bz[k] * dm - g * du_ - czn * dd_);
+                        L = rhs * f.ib[k] - f.dd[k] * L;
+                        v[i] = L;
+                        dd_ = dm;
+                        dm = du_;
+                    }
+                Xa[j + nr * p] = L;
+            }
+            __syncthreads();
+            if (active) {
+                T yin = 0.f;
+                for (int q = 0; q < p; ++q) yin = Xa[j + nr * q] + f.GG[min((q + 1) * kAdiSeg, nz) - 1].x * yin;
+                T M = 0.f;
+#pragma unroll
+                for (int i = kAdiSeg - 1; i >= 0; --i)
+                    if (kFull || i < len) {
+                        const T2 gg = f.GG[k0 + i];
+                        M = (v[i] + gg.x * yin) - gg.y * M;
+                        v[i] = M;
+                    }
+                Xb[j + nr * p] = M;
+            }
+            __syncthreads();
+            if (active) {
+                T xin = 0.f;
+                for (int q = Pz - 1; q > p; --q) xin = Xb[j + nr * q] + f.K[q * kAdiSeg] * xin;
+#pragma unroll
+                for (int i = 0; i < kAdiSeg; ++i)
+                    if (kFull || i < len) {
+                        T *dw = D + (k0 + i) * ps + j;
+                        *dw = *dw + (v[i] + f.K[k0 + i] * xin);
+                    }
+            }
+            if (reload) {
+                __syncthreads();
+                fac_load(Fz, nz, a.ver + (step + 1) * ver_step, tid, kThreads);
+            }
+            __syncthreads();
+        }
         // ================= radial: lines k, segments along j =================
-        {
+        else {
             const Fac<T> f = fac_view(Fr, nr);
             T v[kAdiSeg];
             const bool active = tid < nitem_r;
@@ -788,69 +867,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_adi_delta(AdiArgs a) {
                 for (int i = 0; i < kAdiSeg; ++i)
                     if (kFull || i < len) dw[i] = dw[i] + (v[i] + f.K[j0 + i] * xin);
             }
-            if (!last_step) {
+            if (reload) {
                 __syncthreads();
                 fac_load(Fr, nr, rad + (step + 1) * rad_step, tid, kThreads);
-            }
-            __syncthreads();
-        }
-        // ================= vertical: lines j, segments along k =================
-        {
-            const Fac<T> f = fac_view(Fz, nz);
-            T v[kAdiSeg];
-            const bool active = tid < nitem_z;
-            const int j = active ? tid % nr : 0, p = active ? tid / nr : 0;
-            const int k0 = p * kAdiSeg, len = kFull ? kAdiSeg : min(kAdiSeg, nz - k0);
-            const float4 cc = C4[j];
-            const bool has_l = j > 0, has_r = j + 1 < nr;
-            if (active) {
-                T L = 0.f;
-                T dd_ = (k0 > 0) ? D[(k0 - 1) * ps + j] : 0.f;
-                T dm = D[k0 * ps + j];
-#pragma unroll
-                for (int i = 0; i < kAdiSeg; ++i)
-                    if (kFull || i < len) {
-                        const int k = k0 + i;
-                        const T du_ = (k + 1 < nz) ? D[(k + 1) * ps + j] : 0.f;
-                        const T vl = has_l ? D[k * ps + j - 1] : 0.f, vr = has_r ? D[k * ps + j + 1] : 0.f;
-                        const T czn = (k > 0 || !sym_bottom) ? g : 0.f;
-                        const T rhs = Rv[k * ps + j] - (cc.x * dm + cc.y * vr + cc.z * vl) -
-                                      (bz[k] * dm - g * du_ - czn * dd_);
-                        L = rhs * f.ib[k] - f.dd[k] * L;
-                        v[i] = L;
-                        dd_ = dm;
-                        dm = du_;
-                    }
-                Xa[j + nr * p] = L;
-            }
-            __syncthreads();
-            if (active) {
-                T yin = 0.f;
-                for (int q = 0; q < p; ++q) yin = Xa[j + nr * q] + f.GG[min((q + 1) * kAdiSeg, nz) - 1].x * yin;
-                T M = 0.f;
-#pragma unroll
-                for (int i = kAdiSeg - 1; i >= 0; --i)
-                    if (kFull || i < len) {
-                        const T2 gg = f.GG[k0 + i];
-                        M = (v[i] + gg.x * yin) - gg.y * M;
-                        v[i] = M;
-                    }
-                Xb[j + nr * p] = M;
-            }
-            __syncthreads();
-            if (active) {
-                T xin = 0.f;
-                for (int q = Pz - 1; q > p; --q) xin = Xb[j + nr * q] + f.K[q * kAdiSeg] * xin;
-#pragma unroll
-                for (int i = 0; i < kAdiSeg; ++i)
-                    if (kFull || i < len) {
-                        T *dw = D + (k0 + i) * ps + j;
-                        *dw = *dw + (v[i] + f.K[k0 + i] * xin);
-                    }
-            }
-            if (!last_step) {
-                __syncthreads();
-                fac_load(Fz, nz, a.ver + (step + 1) * ver_step, tid, kThreads);
             }
             __syncthreads();
         }

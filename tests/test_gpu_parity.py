@@ -215,6 +215,31 @@ def test_mixed_converged_production_grid(bph, nsteps):
     g.close()
 
 
+def test_mixed_warm_sequence_stays_converged(bph):
+    """A run of warm mixed solves (time-step sequence of a rotating pair at
+    130x98x256, update tolerance 1e-11) keeps its FP64 residual at the FP64
+    solve's level and every potential within 1e-9 of the FP64 sequence: no
+    component of the refinement grows from one solve to the next."""
+    from bipoly_hydro_b200 import fields
+
+    g = bph.PotentialSolver(130, 98, 256, 1.0 / 126.0, 2, 30)
+    base = fields.bipolytrope_pair()
+    rhos = [fields.rotate(base, i) for i in range(9)]
+    seqs = {}
+    for mixed in (False, True):
+        g.solve_converged(rhos[0], 10, True, 1e-13, 100)
+        out = []
+        for rho in rhos[1:]:
+            fn = g.solve_converged_mixed if mixed else g.solve_converged
+            out.append(fn(rho, 10, False, 1e-11, 100))
+        seqs[mixed] = out
+    floor = max(info.residual for _, info in seqs[False])
+    for (p64, i64), (pmx, imx) in zip(seqs[False], seqs[True]):
+        assert rel_l2(pmx, p64) <= 1e-9, (rel_l2(pmx, p64), imx.cycles, imx.residual)
+        assert imx.residual <= 100 * floor, (imx.residual, floor, imx.cycles)
+    g.close()
+
+
 def test_phieff_fused_output(oracle_mod, bph):
     """phieff = pot - 0.5 omega^2 rhf(J)^2 (source.F90:156) written beside pot."""
     grid = (34, 26, 64, 1.0 / 30.0, 2, 30)
