@@ -407,32 +407,40 @@ def run_gpu(args, world, rank, local):
         conv = {}
         nconv = args.converged_steps
         ref_pots = []
-        for mixed in (False, True):
-            # start both forms from the same converged potential of rhos[0]
+        tuned_kind = solver.info()["mixed_kind"]
+        variants = [("fp64", None), ("mixed_forward", B.solver.MIXED_ADI_FORWARD),
+                    ("mixed_increment", B.solver.MIXED_ADI_INCREMENT)]
+        for key, kind in variants:
+            if kind is not None:
+                solver.set_mixed_adi(kind)
+            # every form starts from the same converged potential of rhos[0]
             solver.solve_converged_device(rhos[0], d_pot, args.conv_nsteps, True, 1e-13, 100, False)
-            lat, cycles, pots = [], [], []
+            clat, cycles, pots = [], [], []
             for i in range(nconv):
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
                 info = solver.solve_converged_device(rhos[(1 + i) % nrot], d_pot, args.conv_nsteps, False,
-                                                     args.conv_tol, 100, mixed)
+                                                     args.conv_tol, 100, kind is not None)
                 torch.cuda.synchronize()
-                lat.append(time.perf_counter() - t0)
+                clat.append(time.perf_counter() - t0)
                 cycles.append(info.cycles)
                 pots.append(d_pot.clone())
-            key = "mixed" if mixed else "fp64"
-            if not mixed:
-                ref_pots = pots
             err = None
-            if mixed:
+            if kind is None:
+                ref_pots = pots
+            else:
                 err = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) for a, b in zip(pots, ref_pots))
-            conv[key] = {"solves_per_s": nconv / sum(lat), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
-                         "p99_ms": 1e3 * float(np.percentile(lat, 99)), "mean_cycles": float(np.mean(cycles)),
+            conv[key] = {"solves_per_s": nconv / sum(clat), "p50_ms": 1e3 * float(np.percentile(clat, 50)),
+                         "p99_ms": 1e3 * float(np.percentile(clat, 99)), "mean_cycles": float(np.mean(cycles)),
                          "max_rel_err_vs_fp64": err}
-            del pots
+            if kind is not None:
+                del pots
+        solver.set_mixed_adi(tuned_kind)
         conv["nsteps_per_cycle"] = args.conv_nsteps
         conv["tol_update"] = args.conv_tol
-        conv["speedup_mixed_vs_fp64"] = conv["mixed"]["solves_per_s"] / conv["fp64"]["solves_per_s"]
+        conv["autotuned_kind"] = "mixed_forward" if tuned_kind == B.solver.MIXED_ADI_FORWARD else "mixed_increment"
+        best = max(conv["mixed_forward"]["solves_per_s"], conv["mixed_increment"]["solves_per_s"])
+        conv["speedup_mixed_vs_fp64"] = best / conv["fp64"]["solves_per_s"]
         del ref_pots
 
     # ---- CPU baseline (rank 0, N = 1 only) ------------------------------

@@ -429,14 +429,25 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
     __syncthreads();
 
     const int nitem_r = nz * Pr, nitem_z = nr * Pz;
-    for (int it = 0; it < a.nsteps_run; ++it) {
+    // Half-step sequence.  Drop-in: radial(i), vertical(i) for i < nsteps
+    // (helmadi.F90:195-355).  Defect form: radial(0), then vertical(i),
+    // radial(i): the cycle opens and closes on a radial half-step (see
+    // k_adi_delta for why T = float needs that order).
+    const int nhalf = kDefect ? 2 * a.nsteps_run + 1 : 2 * a.nsteps_run;
+    for (int h = 0; h < nhalf; ++h) {
+        const bool radial_half = (h % 2) == 0;
+        const int it = kDefect ? (radial_half ? max(h / 2 - 1, 0) : (h - 1) / 2) : h / 2;
         const int step = a.step0 + it;
-        const bool last_step = (it + 1 == a.nsteps_run);
+        const bool last_half = (h + 1 == nhalf);
+        // step of the next half-step (whose right-hand side phase D writes)
+        const int it_next = kDefect ? (h + 1) / 2 - ((h + 1) % 2 == 0 ? 1 : 0) : (h + 1) / 2;
         const T dtt = (T)a.dt[step];
-        const T dtn = last_step ? dtt : (T)a.dt[step + 1];
+        const T dtn = last_half ? dtt : (T)a.dt[a.step0 + it_next];
+        // reload this direction's factors when its next half-step is at another step
+        const bool reload = kDefect ? (h > 0 && it + 1 < a.nsteps_run) : (it + 1 < a.nsteps_run);
 
         // ================= radial half-sweep: lines k, segments along j =================
-        {
+        if (radial_half) {
             const Fac<T> f = fac_view(Fr, nr);
             T v[kAdiSeg];
             const bool active = tid < nitem_r;
@@ -446,7 +457,7 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
             const T *rr = Rw + k * ps + j0;
             if (active) {
                 T L = (T)0;
-                if (!kDefect && it == 0) {
+                if (!kDefect && h == 0) {
                     // first step: the right-hand side from the initial potential
                     const bool refl = (k == 0) && sym_bottom;
                     const T cphi = refl ? dtt - gam_t : dtt - (T)2 * gam_t;
@@ -497,8 +508,12 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
                     if (i == len - 1) Eb[k + nz * p] = v[i];
             }
             __syncthreads();
-            if (active) {
-                // vertical right-hand side of this step (helmadi.F90:276-340),
+            if (active && last_half) {
+#pragma unroll
+                for (int i = 0; i < kAdiSeg; ++i)
+                    if (kFull || i < len) wr[i] = v[i];
+            } else if (active) {
+                // vertical right-hand side of the next half-step (helmadi.F90:276-340),
                 // times the vertical 1/bet of row k
                 const T ibz = fac_view(Fz, nz).ib[k];
                 const T left = (p > 0) ? Eb[k + nz * (p - 1)] : (T)0;
@@ -510,17 +525,17 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
                         const T pl = (i > 0) ? v[i - 1] : left;
                         const T pr = (kFull ? (i + 1 < kAdiSeg) : (i + 1 < len)) ? v[(i + 1) & (kAdiSeg - 1)] : right;
                         const T2 ab = AB[j];
-                        wr[i] = (rr[i] + (el0[j] + dtt) * v[i] - ab.x * pr - ab.y * pl) * ibz;
+                        wr[i] = (rr[i] + (el0[j] + dtn) * v[i] - ab.x * pr - ab.y * pl) * ibz;
                     }
             }
-            if (!last_step) {
+            if (reload) {
                 __syncthreads();
                 fac_load(Fr, nr, rad + (step + 1) * rad_step, tid, kSegThreads);
             }
             __syncthreads();
         }
         // ================= vertical half-sweep: lines j, segments along k =================
-        {
+        else {
             const Fac<T> f = fac_view(Fz, nz);
             T v[kAdiSeg];
             const bool active = tid < nitem_z;
@@ -566,13 +581,13 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
             }
             __syncthreads();
             if (active) {
-                if (last_step) {
+                if (last_half) {
 #pragma unroll
                     for (int i = 0; i < kAdiSeg; ++i)
                         if (kFull || i < len) wc[i * ps] = v[i];
                 } else {
-                    // radial right-hand side of the next step (helmadi.F90:209-256),
-                    // times the next step's radial 1/bet of column j
+                    // radial right-hand side of the next half-step (helmadi.F90:209-256),
+                    // times its radial 1/bet of column j
                     const T ibr = fac_view(Fr, nr).ib[j];
                     const T dn_edge = (p > 0) ? Eb[j + nr * (p - 1)] : (T)0;
                     const T up_edge = (p + 1 < Pz) ? Ea[j + nr * (p + 1)] : (T)0;
@@ -590,7 +605,7 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
                         }
                 }
             }
-            if (!last_step) {
+            if (it + 1 < a.nsteps_run) {
                 __syncthreads();
                 fac_load(Fz, nz, a.ver + (step + 1) * ver_step, tid, kSegThreads);
             }
@@ -982,7 +997,7 @@ int adi_configure(bph_ctx *c) {
     if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
     const SegLayout L = seg_layout(c->nr, c->nz);
     const size_t seg_bytes = sizeof(double) * L.elems + 16;
-    const size_t mixed_bytes = sizeof(float) * L.elems + 16;
+    const size_t mixed_bytes = sizeof(float) * L.elems + 16;  // forwarding form, T = float
     const size_t onchip = sizeof(double) * 2 * (size_t)c->nz * (size_t)(c->nr | 1) + smalls_bytes(c);
     const int items = max(c->nz * L.Pr, c->nr * L.Pz);
     const int threads = (items <= 256) ? 256 : (items <= 384) ? 384 : 512;
@@ -1001,19 +1016,40 @@ int adi_configure(bph_ctx *c) {
         e = cudaFuncSetAttribute(k_adi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, c->adi_smem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_adi)");
     }
+    // FP32 refinement kernels: the forwarding form (k_adi_seg<float>) and the
+    // increment form (k_adi_delta), both with the same thread count.
     const DeltaLayout DL = delta_layout(c->nr, c->nz);
     const size_t delta_bytes = sizeof(float) * DL.elems + 16;
-    (void)mixed_bytes;
-    if (delta_bytes <= (size_t)dev_max && items <= 512) {
-        c->adi_mixed_threads = threads;
-        c->adi_mixed_smem = (int)delta_bytes;
-        const void *fn = delta_kernel(threads, c->adi_full);
-        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, c->adi_mixed_smem);
+    c->adi_mixed_threads = 0;
+    c->mixed_kind = 0;
+    for (int kind = 1; kind <= 2; ++kind) {
+        c->mixed_smem_kind[kind] = 0;
+        c->mixed_per_sm_kind[kind] = 0;
+        const size_t bytes = (kind == BPH_MIXED_ADI_FORWARD) ? mixed_bytes : delta_bytes;
+        if (bytes > (size_t)dev_max || items > 512) continue;
+        const void *fn = (kind == BPH_MIXED_ADI_FORWARD) ? seg_kernel<float, true>(threads, c->adi_full)
+                                                         : delta_kernel(threads, c->adi_full);
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_adi_delta)");
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->adi_mixed_per_sm, fn, threads, c->adi_mixed_smem);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(refinement ADI)");
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->mixed_per_sm_kind[kind], fn, threads, (int)bytes);
         if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        c->mixed_smem_kind[kind] = (int)bytes;
+        c->adi_mixed_threads = threads;
+        if (!c->mixed_kind) c->mixed_kind = kind;
     }
+    return select_mixed_kind(c, c->mixed_kind);
+}
+
+int select_mixed_kind(bph_ctx *c, int kind) {
+    if (kind < 1 || kind > 2 || !c->mixed_smem_kind[kind]) {
+        c->adi_mixed_smem = 0;
+        c->adi_mixed_per_sm = 0;
+        return (kind == 0) ? BPH_OK : BPH_ERR_INVALID;
+    }
+    c->mixed_kind = kind;
+    c->adi_mixed_smem = c->mixed_smem_kind[kind];
+    c->adi_mixed_per_sm = c->mixed_per_sm_kind[kind];
     return BPH_OK;
 }
 
@@ -1076,8 +1112,11 @@ cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {
     AdiArgs a = make_args(c, sch, 0, sch.nsteps, false);
     ++c->launches;
     void *args[] = {&a};
-    return cudaLaunchKernel(delta_kernel(c->adi_mixed_threads, c->adi_full), dim3(c->N),
-                            dim3(c->adi_mixed_threads), args, (size_t)c->adi_mixed_smem, c->stream);
+    const void *fn = (c->mixed_kind == BPH_MIXED_ADI_FORWARD)
+                         ? seg_kernel<float, true>(c->adi_mixed_threads, c->adi_full)
+                         : delta_kernel(c->adi_mixed_threads, c->adi_full);
+    return cudaLaunchKernel(fn, dim3(c->N), dim3(c->adi_mixed_threads), args, (size_t)c->adi_mixed_smem,
+                            c->stream);
 }
 
 cudaError_t launch_update_norm(bph_ctx *c, double *d_out) {

@@ -210,6 +210,46 @@ int upload(bph_ctx *c, void *dst, const void *src, size_t bytes) {
     BPH_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
     return BPH_OK;
 }
+// Times each fitting refinement ADI kernel (one 5-step cycle over the
+// zeroed slot array: r = 0, so the state stays zero) and keeps the faster.
+int autotune_mixed(bph_ctx *c) {
+    int avail = 0;
+    for (int k = 1; k <= 2; ++k) avail += c->mixed_smem_kind[k] ? 1 : 0;
+    if (avail < 2) return BPH_OK;
+    Schedule *s;
+    int rc;
+    if ((rc = get_schedule(c, 5, &s))) return rc;
+    BPH_CUDA(cudaMemsetAsync(c->d_R, 0, sizeof(double) * (size_t)c->N * c->np, c->stream));
+    BPH_CUDA(cudaMemsetAsync(c->d_P, 0, sizeof(double) * (size_t)c->N * c->nplane, c->stream));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    int best = c->mixed_kind;
+    float best_ms = 0.f;
+    for (int k = 1; k <= 2 && e == cudaSuccess; ++k) {
+        select_mixed_kind(c, k);
+        e = launch_adi_defect(c, *s);
+        if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
+        for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = launch_adi_defect(c, *s);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess) break;
+        c->mixed_tuned_us[k] = 1e3f * ms / 3.f;
+        if (k == 1 || ms < best_ms) {
+            best = k;
+            best_ms = ms;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_fail(e, "refinement ADI autotune");
+    BPH_CUDA(cudaMemsetAsync(c->d_P, 0, sizeof(double) * (size_t)c->N * c->nplane, c->stream));
+    BPH_CUDA(cudaStreamSynchronize(c->stream));
+    return select_mixed_kind(c, best);
+}
+
 
 int setup_impl(bph_ctx *c) {
     const bph_grid_t &g = c->g;
@@ -316,6 +356,10 @@ int setup_impl(bph_ctx *c) {
     if ((rc = get_schedule(c, 5, &s))) return rc;
     if ((rc = get_schedule(c, 20, &s))) return rc;
     BPH_CUDA(cudaStreamSynchronize(c->stream));
+    const char *tune = std::getenv("BPH_AUTOTUNE");
+    if (!(tune && tune[0] == '0')) {
+        if ((rc = autotune_mixed(c))) return rc;
+    }
     return BPH_OK;
 }
 
@@ -736,8 +780,32 @@ long long bph_info(const bph_ctx_t *c, int what) {
         case BPH_INFO_MIXED_SMEM: return c->adi_mixed_smem;
         case BPH_INFO_MIXED_CTAS_PER_SM: return c->adi_mixed_per_sm;
         case BPH_INFO_CONTRACT_SPLIT: return c->contract_split;
+        case BPH_INFO_MIXED_KIND: return c->mixed_kind;
+        case BPH_INFO_MIXED_FORWARD_NS: return (long long)(1e3f * c->mixed_tuned_us[BPH_MIXED_ADI_FORWARD]);
+        case BPH_INFO_MIXED_INCREMENT_NS: return (long long)(1e3f * c->mixed_tuned_us[BPH_MIXED_ADI_INCREMENT]);
         default: return -1;
     }
+}
+
+int bph_configure(bph_ctx_t *c, int key, int value) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    if (key != BPH_CFG_MIXED_ADI) {
+        set_error("unknown configuration key %d", key);
+        return BPH_ERR_INVALID;
+    }
+    if ((rc = set_device_of(c))) return rc;
+    if (value == BPH_MIXED_ADI_AUTO) return autotune_mixed(c);
+    if (value != BPH_MIXED_ADI_FORWARD && value != BPH_MIXED_ADI_INCREMENT) {
+        set_error("unknown refinement ADI kind %d", value);
+        return BPH_ERR_INVALID;
+    }
+    BPH_CUDA(cudaStreamSynchronize(c->stream));
+    if (select_mixed_kind(c, value) != BPH_OK) {
+        set_error("refinement ADI kind %d does not fit this grid on chip", value);
+        return BPH_ERR_INVALID;
+    }
+    return BPH_OK;
 }
 
 long long bph_launch_count(const bph_ctx_t *c) { return c ? c->launches : 0; }

@@ -94,9 +94,13 @@ struct bph_ctx {
     int adi_smem = 0;            // dynamic shared bytes of the on-chip ADI kernel (0: global variant)
     int adi_seg = 0;             // threads of the segmented on-chip ADI kernel (0: not used)
     bool adi_full = false;       // both line lengths are multiples of the segment length
-    int adi_mixed_threads = 0;   // threads of the FP32 defect-correction ADI kernel
-    int adi_mixed_smem = 0;      // its dynamic shared bytes (0: mixed form unavailable)
+    int adi_mixed_threads = 0;   // threads of the FP32 defect-correction ADI kernels
+    int adi_mixed_smem = 0;      // dynamic shared bytes of the one in use (0: mixed form unavailable)
     int adi_mixed_per_sm = 0;    // its resident CTAs per SM
+    int mixed_kind = 0;          // refinement ADI in use: BPH_MIXED_ADI_FORWARD or _INCREMENT
+    int mixed_smem_kind[3] = {0, 0, 0};    // per kind: dynamic shared bytes (0: does not fit)
+    int mixed_per_sm_kind[3] = {0, 0, 0};  // per kind: resident CTAs per SM
+    float mixed_tuned_us[3] = {0.f, 0.f, 0.f};  // per kind: setup-time measurement (0: not timed)
     int adi_threads = 256;
     int fft_smem_fwd = 0, fft_smem_inv = 0;
     bool have_warm = false;
@@ -136,6 +140,8 @@ cudaError_t launch_update_norm(bph_ctx *c, double *d_out);
 cudaError_t launch_residual_norm(bph_ctx *c, double *d_out);
 
 int adi_configure(bph_ctx *c);
+// Makes kind (BPH_MIXED_ADI_FORWARD / _INCREMENT) the refinement ADI kernel.
+int select_mixed_kind(bph_ctx *c, int kind);
 int contract_configure(bph_ctx *c);
 int fft_configure(bph_ctx *c);
 

@@ -44,9 +44,13 @@ EXPORTED_SYMBOLS = (
     "bph_setup", "bph_potential_solver", "bph_potential_solver_device", "bph_solve_nsteps",
     "bph_solve_converged", "bph_potential_solver_phieff", "bph_set_potential", "bph_solve_converged_mixed", "bph_set_stream", "bph_synchronize", "bph_destroy", "bph_last_error",
     "bph_version", "bph_num_boundary_rows", "bph_copy_green", "bph_copy_moments", "bph_run_phase",
-    "bph_green_contract_noalloc", "bph_info", "bph_launch_count", "bph_device_bytes",
+    "bph_green_contract_noalloc", "bph_info", "bph_configure", "bph_launch_count", "bph_device_bytes",
     "bph_batch_create", "bph_batch_solve", "bph_batch_destroy", "bph_batch_device_bytes",
 )
+
+#: bph_configure keys and values.
+CFG_MIXED_ADI = 0
+MIXED_ADI_AUTO, MIXED_ADI_FORWARD, MIXED_ADI_INCREMENT = 0, 1, 2
 
 #: bph_run_phase phase ids.
 PHASE_FFT_RHO, PHASE_CONTRACT, PHASE_SLOTS, PHASE_ADI, PHASE_FFT_INV = range(5)
@@ -120,6 +124,8 @@ def load_library(path: str | None = None):
     L.bph_batch_device_bytes.restype = ctypes.c_size_t
     L.bph_info.argtypes = [vp, i]
     L.bph_info.restype = ctypes.c_longlong
+    L.bph_configure.argtypes = [vp, i, i]
+    L.bph_configure.restype = i
     L.bph_launch_count.argtypes = [vp]
     L.bph_launch_count.restype = ctypes.c_longlong
     L.bph_device_bytes.argtypes = [vp]
@@ -305,8 +311,14 @@ class PotentialSolver:
 
     def info(self) -> dict:
         """Launch-configuration facts (bph_info)."""
-        names = ("adi_threads", "adi_smem", "mixed_threads", "mixed_smem", "mixed_ctas_per_sm", "contract_split")
+        names = ("adi_threads", "adi_smem", "mixed_threads", "mixed_smem", "mixed_ctas_per_sm", "contract_split",
+                 "mixed_kind", "mixed_forward_ns", "mixed_increment_ns")
         return {n: int(self._lib.bph_info(self._h, i)) for i, n in enumerate(names)}
+
+    def set_mixed_adi(self, kind: int) -> None:
+        """Refinement ADI kernel of the mixed form: MIXED_ADI_AUTO (time both
+        and keep the faster), MIXED_ADI_FORWARD or MIXED_ADI_INCREMENT."""
+        _check(self._lib.bph_configure(self._h, CFG_MIXED_ADI, int(kind)))
 
     @property
     def launch_count(self) -> int:

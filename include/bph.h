@@ -196,7 +196,31 @@ int bph_green_contract_noalloc(bph_ctx_t *ctx, const double *d_mom, double *d_S)
 #define BPH_INFO_MIXED_SMEM 3         /* its dynamic shared bytes */
 #define BPH_INFO_MIXED_CTAS_PER_SM 4  /* its resident CTAs per SM */
 #define BPH_INFO_CONTRACT_SPLIT 5     /* slices of the split-K Green contraction */
+#define BPH_INFO_MIXED_KIND 6         /* refinement ADI kernel in use (BPH_MIXED_ADI_*) */
+#define BPH_INFO_MIXED_FORWARD_NS 7   /* setup-time duration of a 5-step forwarding-form launch, ns (0: not timed) */
+#define BPH_INFO_MIXED_INCREMENT_NS 8 /* the same for the increment form */
 long long bph_info(const bph_ctx_t *ctx, int what);
+
+/* Tuning knobs (no counterpart in the reference).
+ *
+ * BPH_CFG_MIXED_ADI selects the FP32 ADI kernel of the mixed-precision
+ * refinement (bph_solve_converged_mixed):
+ *   BPH_MIXED_ADI_AUTO       time both kernels on this grid and keep the faster
+ *                            (what bph_setup does unless the environment sets
+ *                            BPH_AUTOTUNE=0, which keeps the forwarding form);
+ *   BPH_MIXED_ADI_FORWARD    helmadi's right-hand-side form in FP32, the next
+ *                            half-step's right-hand side written by the
+ *                            current one (fewer instructions per step);
+ *   BPH_MIXED_ADI_INCREMENT  every half-step solves for an increment of the
+ *                            residual r - A delta (more instructions, smaller
+ *                            shared-memory footprint).
+ * Both converge to the same discrete solution.  Returns BPH_ERR_INVALID for
+ * a kind that does not fit this grid on chip. */
+#define BPH_CFG_MIXED_ADI 0
+#define BPH_MIXED_ADI_AUTO 0
+#define BPH_MIXED_ADI_FORWARD 1
+#define BPH_MIXED_ADI_INCREMENT 2
+int bph_configure(bph_ctx_t *ctx, int key, int value);
 
 /* Number of kernels this context has launched so far. */
 long long bph_launch_count(const bph_ctx_t *ctx);

@@ -175,12 +175,16 @@ def test_gpu_reproduces_golden_fixture(bph, path):
 @pytest.mark.parametrize("grid", [(34, 26, 64, 1.0 / 30.0, 2, 30), (66, 66, 64, 1.0 / 62.0, 2, 30),
                                   (20, 14, 32, 1.0 / 18.0, 1, 8), (18, 16, 32, 1.0 / 16.0, 3, 6)],
                          ids=["34x26x64", "66x66x64", "isym1", "isym3"])
-def test_mixed_converged_within_1e9_of_fp64(oracle_mod, bph, grid):
+@pytest.mark.parametrize("kind", [1, 2], ids=["forward", "increment"])
+def test_mixed_converged_within_1e9_of_fp64(oracle_mod, bph, grid, kind):
     """FP32 ADI + FP64 residual/update refinement converges to the FP64 discrete
     solution: relative L2 error <= 1e-9 against the GPU FP64 converged solve
-    and against the oracle's converged solve (north-star bound for the mixed form)."""
+    and against the oracle's converged solve (north-star bound for the mixed form),
+    with either refinement ADI kernel."""
     numr, numz, numphi, dr, isym, _ = grid
     g = bph.PotentialSolver(*grid)
+    g.set_mixed_adi(kind)
+    assert g.info()["mixed_kind"] == kind
     rho = smooth_density(numr, numz, numphi, dr, isym)
     p64, i64 = g.solve_converged(rho, 20, True, 1e-13, 200)
     pmx, imx = g.solve_converged_mixed(rho, 20, True, 1e-13, 200)
@@ -215,7 +219,8 @@ def test_mixed_converged_production_grid(bph, nsteps):
     g.close()
 
 
-def test_mixed_warm_sequence_stays_converged(bph):
+@pytest.mark.parametrize("kind", [1, 2], ids=["forward", "increment"])
+def test_mixed_warm_sequence_stays_converged(bph, kind):
     """A run of warm mixed solves (time-step sequence of a rotating pair at
     130x98x256, update tolerance 1e-11) keeps its FP64 residual at the FP64
     solve's level and every potential within 1e-9 of the FP64 sequence: no
@@ -223,6 +228,7 @@ def test_mixed_warm_sequence_stays_converged(bph):
     from bipoly_hydro_b200 import fields
 
     g = bph.PotentialSolver(130, 98, 256, 1.0 / 126.0, 2, 30)
+    g.set_mixed_adi(kind)
     base = fields.bipolytrope_pair()
     rhos = [fields.rotate(base, i) for i in range(9)]
     seqs = {}
@@ -271,3 +277,20 @@ def test_warm_start_from_checkpointed_potential(oracle_mod, bph):
     assert rel_l2(g2.potential_solver(rho2, 5), o2.potential_solver(rho2, 5)) <= POT_TOL
     g.close()
     g2.close()
+
+
+def test_mixed_adi_autotune_and_selection(bph):
+    """Setup times both refinement ADI kernels at 130x98x256 and keeps the
+    faster; an explicit choice sticks; an unknown kind is rejected."""
+    g = bph.PotentialSolver(130, 98, 256, 1.0 / 126.0, 2, 30)
+    info = g.info()
+    assert info["mixed_kind"] in (1, 2)
+    fwd, inc = info["mixed_forward_ns"], info["mixed_increment_ns"]
+    assert fwd > 0 and inc > 0
+    assert info["mixed_kind"] == (1 if fwd <= inc else 2)
+    g.set_mixed_adi(2)
+    assert g.info()["mixed_kind"] == 2
+    with pytest.raises(bph.BphError):
+        g.set_mixed_adi(7)
+    assert g.info()["mixed_kind"] == 2
+    g.close()
