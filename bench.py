@@ -328,7 +328,7 @@ def run_gpu(args, world, rank, local):
     phases = {
         "fft_fwd_rho": time_phase(B.solver.PHASE_FFT_RHO, 50, d_rho=rhos[0]),
         "green_contract": time_phase(B.solver.PHASE_CONTRACT, 50),
-        "boundary_slots": time_phase(B.solver.PHASE_SLOTS, 50),
+        "boundary_slots_standalone": time_phase(B.solver.PHASE_SLOTS, 50),
         "adi_5steps": time_phase(B.solver.PHASE_ADI, 50, nsteps=5),
         "fft_inv": time_phase(B.solver.PHASE_FFT_INV, 50, d_pot=d_pot),
     }

@@ -49,6 +49,7 @@ struct AdiArgs {
 template <bool kOnChip>
 __global__ void __launch_bounds__(kAdiThreads) k_adi(AdiArgs a) {
     extern __shared__ double sm[];
+    pdl_wait();
     const int s = blockIdx.x;
     const int tid = threadIdx.x;
     const int nr = a.nr, nz = a.nz, numr = a.numr;
@@ -360,6 +361,7 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
     }
     fac_load(Fr, nr, rad + a.step0 * rad_step, tid, kSegThreads);
     fac_load(Fz, nz, a.ver + a.step0 * ver_step, tid, kSegThreads);
+    pdl_wait();  // P and R come from the previous kernels of the solve
     if (!kDefect) {
         // Rw (source + folded Dirichlet terms) and the initial potential: 8 rows per
         // warp pass, all loads in flight before the shared-memory stores.
@@ -612,6 +614,7 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
             __syncthreads();
         }
     }
+    pdl_trigger();
     if (!kDefect) {
         for (int k = warp; k < nz; k += nwarps) {
             double *prow = Pg + (long long)numr * (k + 1) + 1;
@@ -743,6 +746,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_adi_delta(AdiArgs a) {
     for (int k = tid; k < nz; k += kThreads) bz[k] = (T)a.bzb[k + 1];
     fac_load(Fr, nr, rad + a.step0 * rad_step, tid, kThreads);
     fac_load(Fz, nz, a.ver + a.step0 * ver_step, tid, kThreads);
+    pdl_wait();
     // FP64 residual of the current potential; delta = 0
     for (int k = warp; k < nz; k += nwarps) {
         const double *pc = Pg + (long long)numr * (k + 1) + 1;
@@ -1088,8 +1092,9 @@ cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_ru
     if (c->adi_seg) {
         ++c->launches;
         void *args[] = {&a};
-        return cudaLaunchKernel(seg_kernel<double, false>(c->adi_seg, c->adi_full), dim3(c->N * ninst),
-                                dim3(c->adi_seg), args, (size_t)c->adi_smem, c->stream);
+        cudaLaunchAttribute attr[1];
+        cudaLaunchConfig_t cfg = launch_config(c, dim3(c->N * ninst), dim3(c->adi_seg), (size_t)c->adi_smem, attr);
+        return cudaLaunchKernelExC(&cfg, seg_kernel<double, false>(c->adi_seg, c->adi_full), args);
     }
     // other variants: one launch per instance
     for (int i = 0; i < ninst; ++i) {

@@ -338,6 +338,10 @@ int setup_impl(bph_ctx *c) {
     BPH_CUDA(cudaMemsetAsync(c->d_P, 0, sizeof(double) * (size_t)c->N * c->nplane, c->stream));
     BPH_CUDA(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
 
+    {
+        const char *pdl = std::getenv("BPH_PDL");
+        c->pdl = !(pdl && pdl[0] == '0');
+    }
     BPH_CUDA(launch_qcoef(c));
     BPH_CUDA(launch_green_tables(c));
     if ((rc = fft_configure(c))) return rc;
@@ -367,8 +371,7 @@ int setup_impl(bph_ctx *c) {
 int solve_device(bph_ctx *c, const double *d_rho, double *d_pot, const Schedule &s, bool cold,
                  double *d_phieff = nullptr, double omega = 0.0) {
     BPH_CUDA(launch_fft_fwd_rho(c, d_rho));
-    BPH_CUDA(launch_green_contract(c));
-    BPH_CUDA(launch_boundary_slots(c));
+    BPH_CUDA(launch_green_contract(c));  // also writes the Dirichlet slots
     BPH_CUDA(launch_adi(c, s, 0, s.nsteps, cold));
     BPH_CUDA(launch_fft_inv(c, d_pot, d_phieff, omega));
     c->have_warm = true;
@@ -557,8 +560,7 @@ int bph_solve_converged(bph_ctx_t *c, const double *rho, double *pot, int nsteps
         d_pot = c->d_pot_stage;
     }
     BPH_CUDA(launch_fft_fwd_rho(c, d_rho));
-    BPH_CUDA(launch_green_contract(c));
-    BPH_CUDA(launch_boundary_slots(c));
+    BPH_CUDA(launch_green_contract(c));  // also writes the Dirichlet slots
     std::vector<double> h(2 * (size_t)c->N);
     int cyc = 0;
     for (;;) {
@@ -618,10 +620,9 @@ int bph_solve_converged_mixed(bph_ctx_t *c, const double *rho, double *pot, int 
         d_rho = c->d_rho_stage;
         d_pot = c->d_pot_stage;
     }
-    BPH_CUDA(launch_fft_fwd_rho(c, d_rho));
-    BPH_CUDA(launch_green_contract(c));
     if (cold) BPH_CUDA(cudaMemsetAsync(c->d_P, 0, sizeof(double) * (size_t)c->N * c->nplane, c->stream));
-    BPH_CUDA(launch_boundary_slots(c));
+    BPH_CUDA(launch_fft_fwd_rho(c, d_rho));
+    BPH_CUDA(launch_green_contract(c));  // also writes the Dirichlet slots
     std::vector<double> h(2 * (size_t)c->N);
     int cyc = 0;
     double prev_upd = INFINITY;

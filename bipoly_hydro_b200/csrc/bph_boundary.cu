@@ -32,10 +32,22 @@ constexpr int kContractThreads = 256;
 // GPU.  Slices write partial sums, and the last CTA of each (m, group) to
 // arrive adds them in slice order (deterministic) and writes S; it also
 // resets its arrival counter for the next launch.
+// Dirichlet slots of one boundary row, written by the CTA that finishes the
+// row's moments (the closed form of k_boundary_slots below, fused so that
+// the solve needs no separate launch).  Slots of modes without boundary
+// data and the corner columns are zero from set-up and never written.
+struct SlotOut {
+    double *P;          // slot array [N][nplane], or nullptr: S only
+    const double2 *ph;  // (cos, sin) of pi fm m / N
+    int numr, numz, nr, nz, M, fm;
+    double nfactor;     // N * factor
+};
+
 template <bool kVec>
 __global__ void __launch_bounds__(kContractThreads, 2)
 k_green_contract(const double *__restrict__ G, const double *__restrict__ mom, double *__restrict__ S,
-                 long long np, int nb, unsigned int *__restrict__ counters, double *__restrict__ partials) {
+                 long long np, int nb, unsigned int *__restrict__ counters, double *__restrict__ partials,
+                 SlotOut so) {
     const int m = blockIdx.y, split = blockIdx.z, nsplit = gridDim.z;
     const int b0 = blockIdx.x * kContractRows;
     const int nrows = min(kContractRows, nb - b0);
@@ -49,6 +61,7 @@ k_green_contract(const double *__restrict__ G, const double *__restrict__ mom, d
     double ac[kContractRows], as[kContractRows];
 #pragma unroll
     for (int r = 0; r < kContractRows; ++r) ac[r] = as[r] = 0.0;
+    pdl_wait();
     if (kVec) {
         const double2 *mc2 = reinterpret_cast<const double2 *>(mc);
         const double2 *ms2 = reinterpret_cast<const double2 *>(ms);
@@ -79,6 +92,7 @@ k_green_contract(const double *__restrict__ G, const double *__restrict__ mom, d
             }
         }
     }
+    pdl_trigger();
     __shared__ double red[kContractThreads / 32][2 * kContractRows];
     __shared__ bool last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -104,11 +118,39 @@ k_green_contract(const double *__restrict__ G, const double *__restrict__ mom, d
 #pragma unroll
         for (int w = 0; w < kContractThreads / 32; ++w) v += red[w][threadIdx.x];
     }
-    if (nsplit == 1) {
-        if (threadIdx.x < 2 * nrows) {
-            const int r = threadIdx.x >> 1, cs = threadIdx.x & 1;
-            S[((long long)m * nb + b0 + r) * 2 + cs] = (m == 0 && cs == 1) ? 0.0 : v;
+    // Threads 2r, 2r+1 of warp 0 hold (S_C, S_S) of row b0 + r.
+    auto finish = [&](double val) {
+        const double other = __shfl_xor_sync(0xffffffffu, val, 1);
+        if (threadIdx.x >= 2 * nrows) return;
+        const int r = threadIdx.x >> 1, cs = threadIdx.x & 1;
+        const double mine = (m == 0 && cs == 1) ? 0.0 : val;
+        S[((long long)m * nb + b0 + r) * 2 + cs] = mine;
+        if (!so.P) return;
+        const double sc = cs ? other : mine;
+        const double ss = (m == 0) ? 0.0 : (cs ? mine : other);
+        const int b = b0 + r;
+        int jz, kz;
+        if (b < so.nr) {
+            jz = b + 1;
+            kz = so.numz - 1;
+        } else if (b < so.nr + so.nz) {
+            jz = so.numr - 1;
+            kz = b - so.nr + 1;
+        } else {
+            jz = b - so.nr - so.nz + 1;
+            kz = 0;
         }
+        const long long nplane = (long long)so.numr * so.numz;
+        const long long pos = jz + (long long)so.numr * kz;
+        const int k = so.fm * m;
+        const double2 w = so.ph[m];
+        if (cs == 0)
+            so.P[(long long)k * nplane + pos] = so.nfactor * (w.x * sc + w.y * ss);
+        else if (m > 0)
+            so.P[(long long)(so.M + k) * nplane + pos] = so.nfactor * (w.y * sc - w.x * ss);
+    };
+    if (nsplit == 1) {
+        if (threadIdx.x < 32) finish(v);
         return;
     }
     if (threadIdx.x < 2 * nrows) partials[split * slice_stride + ((long long)m * nb + b0) * 2 + threadIdx.x] = v;
@@ -119,11 +161,12 @@ k_green_contract(const double *__restrict__ G, const double *__restrict__ mom, d
     __syncthreads();
     if (!last) return;
     __threadfence();
-    if (threadIdx.x < 2 * nrows) {
+    if (threadIdx.x < 32) {
         double t = 0.0;
-        for (int k = 0; k < nsplit; ++k) t += __ldcg(partials + k * slice_stride + ((long long)m * nb + b0) * 2 + threadIdx.x);
-        const int r = threadIdx.x >> 1, cs = threadIdx.x & 1;
-        S[((long long)m * nb + b0 + r) * 2 + cs] = (m == 0 && cs == 1) ? 0.0 : t;
+        if (threadIdx.x < 2 * nrows)
+            for (int k = 0; k < nsplit; ++k)
+                t += __ldcg(partials + k * slice_stride + ((long long)m * nb + b0) * 2 + threadIdx.x);
+        finish(t);
     }
     if (threadIdx.x == 0) counters[tile] = 0u;
 }
@@ -135,6 +178,7 @@ __global__ void k_boundary_slots(const double *__restrict__ S, const double2 *__
                                  int mmax, int fm, int isym, double nfactor) {
     const int M = N / 2;
     const int ncorner = (isym == 1) ? 2 : 1;
+    pdl_wait();
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)(nb + ncorner) * N) return;
     const int s = (int)(t % N), b = (int)(t / N);
@@ -194,17 +238,27 @@ int contract_configure(bph_ctx *c) {
     return BPH_OK;
 }
 
-cudaError_t launch_green_contract(bph_ctx *c) {
+cudaError_t launch_green_contract(bph_ctx *c, bool write_slots) {
     dim3 grid((unsigned)((c->nb + kContractRows - 1) / kContractRows), (unsigned)c->g.mmax,
               (unsigned)c->contract_split);
+    SlotOut so;
+    so.P = write_slots ? c->d_P : nullptr;
+    so.ph = c->d_ph;
+    so.numr = c->g.numr;
+    so.numz = c->g.numz;
+    so.nr = c->nr;
+    so.nz = c->nz;
+    so.M = c->M;
+    so.fm = c->fm;
+    so.nfactor = (double)c->N * c->factor;
     ++c->launches;
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = launch_config(c, grid, dim3(kContractThreads), 0, attr);
+    const double *G = c->d_green, *mom = c->d_mom;
     if (c->np % 2 == 0)
-        k_green_contract<true><<<grid, kContractThreads, 0, c->stream>>>(c->d_green, c->d_mom, c->d_S, c->np, c->nb,
-                                                                        c->d_ccnt, c->d_cpart);
-    else
-        k_green_contract<false><<<grid, kContractThreads, 0, c->stream>>>(c->d_green, c->d_mom, c->d_S, c->np, c->nb,
-                                                                         c->d_ccnt, c->d_cpart);
-    return cudaGetLastError();
+        return cudaLaunchKernelEx(&cfg, k_green_contract<true>, G, mom, c->d_S, c->np, c->nb, c->d_ccnt, c->d_cpart,
+                                  so);
+    return cudaLaunchKernelEx(&cfg, k_green_contract<false>, G, mom, c->d_S, c->np, c->nb, c->d_ccnt, c->d_cpart, so);
 }
 
 cudaError_t launch_boundary_slots(bph_ctx *c) {

@@ -96,6 +96,10 @@ __device__ __forceinline__ void fft_tile(double2 *C, const double2 *tw) {
 template <int M>
 struct FftShape {
     static constexpr int kThreads = (M >= 256) ? 256 : 128;
+    // resident CTAs per SM the register budget is sized for (the loads of a
+    // tile are all in flight at once; more CTAs hide more of their latency)
+    static constexpr int kMinBlocksFwd = (M >= 256) ? 2 : 5;
+    static constexpr int kMinBlocksInv = (M >= 256) ? 1 : 4;
     static constexpr size_t kSmem = sizeof(double2) * ((size_t)M * kTile + M + (M + 1));
 };
 
@@ -105,7 +109,7 @@ struct FftShape {
 // from the same spectrum: sum_l rho_l e^{i k (l - 1/2) dphi} = e^{i pi k/N} F_k.
 // !kRho: write the warm-start potential into P's interior.
 template <int M, bool kRho>
-__global__ void __launch_bounds__(FftShape<M>::kThreads)
+__global__ void __launch_bounds__(FftShape<M>::kThreads, FftShape<M>::kMinBlocksFwd)
 k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__restrict__ mom,
           const double2 *__restrict__ g_tw, const double2 *__restrict__ g_tw2, const double2 *__restrict__ g_ph,
           int numr, int numz, int nr, int nz, int mmax, int fm, int isym, double four_pi,
@@ -121,6 +125,7 @@ k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__re
     const long long p0 = (long long)blockIdx.x * kTile;
     for (int i = tid; i < M; i += NT) tw[i] = g_tw[i];
     for (int i = tid; i <= M; i += NT) tw2[i] = g_tw2[i];
+    pdl_wait();
     // Load: thread -> (column c fixed, sample pairs n = n0, n0 + NT/kTile, ...);
     // all global loads are issued before any shared-memory store.
     static_assert(NT % kTile == 0, "threads must cover whole tile rows");
@@ -131,7 +136,7 @@ k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__re
         const long long p = p0 + c;
         const bool valid = p < np;
         const double *col = src;
-        if (valid) col = src + ((int)(p % nr) + 1) + (long long)numr * ((int)(p / nr) + 1);
+        if (valid) col = src + ((int)p % nr + 1) + (long long)numr * ((int)p / nr + 1);
         double2 v[kLoads];
 #pragma unroll
         for (int i = 0; i < kLoads; ++i) {
@@ -148,12 +153,16 @@ k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__re
     if (kRho && bad) atomicOr(status, kStatusNonFinite);
     __syncthreads();
     fft_tile<M, +1, NT>(C, tw);
-    // Post-process pairs (k, M-k) into F_k, F_{M-k}; write slots.
-    for (int it = tid; it < kTile * (M / 2 + 1); it += NT) {
-        int c = it % kTile, k = it / kTile;
-        long long p = p0 + c;
-        if (p >= np) continue;
-        int jz = (int)(p % nr) + 1, kz = (int)(p / nr) + 1;
+    pdl_trigger();
+    // Post-process pairs (k, M-k) into F_k, F_{M-k}; write slots.  The tile
+    // column of a thread is the same in every iteration (NT % kTile == 0).
+    const int c = tid % kTile;
+    const long long p = p0 + c;
+    if (p >= np) return;
+    const int pi = (int)p;
+    const int jz = pi % nr + 1, kz = pi / nr + 1;
+    const bool zeroed = (jz == numr - 2) || (kz == numz - 2) || (isym == 1 && kz == 1);
+    for (int k = tid / kTile; k <= M / 2; k += NT / kTile) {
         double2 Fk, Fm;  // F_k and F_{M-k} (for k = 0: F_0 and F_M, both real)
         if (k == 0) {
             double2 z = C[c];
@@ -177,7 +186,6 @@ k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__re
         const int ka = k, kb = M - k;
         double sa_re = Fk.x, sa_im = -Fk.y, sb_re = Fm.x, sb_im = -Fm.y;
         if (kRho) {
-            bool zeroed = (jz == numr - 2) || (kz == numz - 2) || (isym == 1 && kz == 1);
             double *o = out + p;
             if (k == 0) {
                 o[0] = zeroed ? 0.0 : -(four_pi * sa_re);
@@ -239,7 +247,7 @@ k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__re
 // phieff = pot - 0.5 omega^2 rhf(J)^2 that the hydro source step forms from
 // pot (source.F90:156, make_source_temp.F90:121), saving it a full pass.
 template <int M>
-__global__ void __launch_bounds__(FftShape<M>::kThreads)
+__global__ void __launch_bounds__(FftShape<M>::kThreads, FftShape<M>::kMinBlocksInv)
 k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 *__restrict__ g_tw,
           const double2 *__restrict__ g_tw2, int numr, int numz, int isym, double *__restrict__ phieff,
           const double *__restrict__ rhf, double omega) {
@@ -253,6 +261,7 @@ k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 
     const long long q0 = (long long)blockIdx.x * kTile;
     for (int i = tid; i < M; i += NT) tw[i] = g_tw[i];
     for (int i = tid; i <= M; i += NT) tw2[i] = g_tw2[i];
+    pdl_wait();
     // Load slots: thread -> (column c fixed, slot pairs (k, M+k)); all global
     // loads are issued before any shared-memory store.
     constexpr int kRowsPerPass = NT / kTile, kLoads = M / kRowsPerPass;
@@ -262,31 +271,36 @@ k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 
         const bool valid = q < nplane;
         int jz = 0, kz = 0;
         if (valid) {
-            jz = (int)(q % numr);
-            kz = (int)(q / numr);
+            jz = (int)q % numr;
+            kz = (int)q / numr;
         }
         const int js = (jz == 0) ? 1 : jz;
         const int ks = (kz == 0 && isym != 1) ? 1 : kz;
         const bool axis = valid && (jz == 0) && (isym != 3);
         const double *col = P + js + (long long)numr * ks;
-        double a[kLoads], b[kLoads];
+        // two batches of loads in flight (register budget of kMinBlocksInv CTAs per SM)
+        constexpr int kBatch = (kLoads >= 16) ? kLoads / 2 : kLoads;
 #pragma unroll
-        for (int i = 0; i < kLoads; ++i) {
-            const int k = k0 + i * kRowsPerPass;
-            a[i] = valid ? __ldg(col + nplane * k) : 0.0;
-            b[i] = valid ? __ldg(col + nplane * (M + k)) : 0.0;
-        }
+        for (int i0 = 0; i0 < kLoads; i0 += kBatch) {
+            double a[kBatch], b[kBatch];
 #pragma unroll
-        for (int i = 0; i < kLoads; ++i) {
-            const int k = k0 + i * kRowsPerPass;
-            double2 v;
-            if (k == 0) {
-                v = make_double2(a[i], b[i]);  // (F_0, F_M): both real
-            } else {
-                v = make_double2(a[i], -b[i]);  // F_k = slot_k - i slot_{M+k}
-                if (axis && (k & 1)) v = make_double2(-v.x, -v.y);
+            for (int i = 0; i < kBatch; ++i) {
+                const int k = k0 + (i0 + i) * kRowsPerPass;
+                a[i] = valid ? __ldg(col + nplane * k) : 0.0;
+                b[i] = valid ? __ldg(col + nplane * (M + k)) : 0.0;
             }
-            C[k * kTile + c] = v;
+#pragma unroll
+            for (int i = 0; i < kBatch; ++i) {
+                const int k = k0 + (i0 + i) * kRowsPerPass;
+                double2 v;
+                if (k == 0) {
+                    v = make_double2(a[i], b[i]);  // (F_0, F_M): both real
+                } else {
+                    v = make_double2(a[i], -b[i]);  // F_k = slot_k - i slot_{M+k}
+                    if (axis && (k & 1)) v = make_double2(-v.x, -v.y);
+                }
+                C[k * kTile + c] = v;
+            }
         }
     }
     __syncthreads();
@@ -310,6 +324,7 @@ k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 
     }
     __syncthreads();
     fft_tile<M, -1, NT>(C, tw);
+    pdl_trigger();
     const double scale = 1.0 / (double)M;
     {
         const int c = tid % kTile, n0 = tid / kTile;
@@ -324,7 +339,7 @@ k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 
                 col[nplane * (2 * n + 1)] = z.y * scale;
             }
             if (phieff) {
-                const double r = rhf[q % numr];
+                const double r = rhf[(int)q % numr];
                 const double cen = 0.5 * omega * omega * r * r;
                 double *pe = phieff + q;
 #pragma unroll
@@ -354,10 +369,11 @@ cudaError_t set_fft_attrs(bph_ctx *c) {
 template <int M>
 cudaError_t fwd_rho(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride) {
     unsigned blocks = (unsigned)((c->np + kTile - 1) / kTile);
-    k_fft_fwd<M, true><<<blocks, FftShape<M>::kThreads, FftShape<M>::kSmem, c->stream>>>(
-        rho, R, mom, c->d_tw, c->d_tw2, c->d_ph, c->g.numr, c->g.numz, c->nr, c->nz, c->g.mmax, c->fm,
-        c->g.isym, c->four_pi, c->d_status, mstride);
-    return cudaGetLastError();
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = launch_config(c, dim3(blocks), dim3(FftShape<M>::kThreads), FftShape<M>::kSmem, attr);
+    return cudaLaunchKernelEx(&cfg, k_fft_fwd<M, true>, rho, R, mom, (const double2 *)c->d_tw,
+                              (const double2 *)c->d_tw2, (const double2 *)c->d_ph, c->g.numr, c->g.numz, c->nr,
+                              c->nz, c->g.mmax, c->fm, c->g.isym, c->four_pi, c->d_status, mstride);
 }
 
 template <int M>
@@ -372,9 +388,10 @@ cudaError_t fwd_pot(bph_ctx *c, const double *pot) {
 template <int M>
 cudaError_t inv(bph_ctx *c, double *pot, double *phieff, double omega, const double *P) {
     unsigned blocks = (unsigned)((c->nplane + kTile - 1) / kTile);
-    k_fft_inv<M><<<blocks, FftShape<M>::kThreads, FftShape<M>::kSmem, c->stream>>>(
-        P, pot, c->d_tw, c->d_tw2, c->g.numr, c->g.numz, c->g.isym, phieff, c->d_grid, omega);
-    return cudaGetLastError();
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = launch_config(c, dim3(blocks), dim3(FftShape<M>::kThreads), FftShape<M>::kSmem, attr);
+    return cudaLaunchKernelEx(&cfg, k_fft_inv<M>, P, pot, (const double2 *)c->d_tw, (const double2 *)c->d_tw2,
+                              c->g.numr, c->g.numz, c->g.isym, phieff, (const double *)c->d_grid, omega);
 }
 
 #define BPH_FFT_DISPATCH(FN, ...)                  \

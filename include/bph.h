@@ -157,8 +157,8 @@ int bph_copy_moments(bph_ctx_t *ctx, double *host_out, size_t n);
 
 /* Phases of one solve, for timing a single kernel (bph_run_phase). */
 #define BPH_PHASE_FFT_RHO 0   /* k_fft_fwd: rho -> -4 pi rho_hat + moments */
-#define BPH_PHASE_CONTRACT 1  /* k_green_contract: tables x moments -> S */
-#define BPH_PHASE_SLOTS 2     /* k_boundary_slots: S -> Dirichlet slots */
+#define BPH_PHASE_CONTRACT 1  /* k_green_contract: tables x moments -> S and the Dirichlet slots */
+#define BPH_PHASE_SLOTS 2     /* k_boundary_slots: S -> Dirichlet slots (standalone form; solves write them in the contraction) */
 #define BPH_PHASE_ADI 3       /* k_adi: nsteps warm ADI steps */
 #define BPH_PHASE_FFT_INV 4   /* k_fft_inv: slots -> pot */
 
