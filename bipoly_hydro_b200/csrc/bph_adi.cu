@@ -41,6 +41,7 @@ struct AdiArgs {
     const double *brb;      // [N][numr] (defect form: residual)
     const double *bzb;      // [numz]    (defect form: residual)
     double *norms;          // [N][2]    (defect form: |delta|^2, |phi|^2 per slot)
+    const int *inst_map;    // batches: instance of each block row (nullptr: block row = instance)
     int numr, numz, nr, nz, N, isym;
     int step0, nsteps_run, cold;
     double gamma;
@@ -326,7 +327,8 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
     // blockIdx.x = instance * N + slot: the slot picks the coefficients, the
     // block index the slab (batches keep instances' slot arrays contiguous)
     const int s = blockIdx.x % a.N, tid = threadIdx.x;
-    const long long blk = blockIdx.x;
+    const int row = blockIdx.x / a.N;
+    const long long blk = (long long)(a.inst_map ? a.inst_map[row] : row) * a.N + s;
     const int lane = tid & 31, warp = tid >> 5, nwarps = kSegThreads / 32;
     const int nr = a.nr, nz = a.nz, numr = a.numr, numz = a.numz;
     const SegLayout Lo = seg_layout(nr, nz);
@@ -1071,6 +1073,7 @@ AdiArgs make_args(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bo
     a.brb = c->d_brb;
     a.bzb = c->d_bzb;
     a.norms = c->d_red;
+    a.inst_map = nullptr;
     a.numr = c->g.numr;
     a.numz = c->g.numz;
     a.nr = c->nr;
@@ -1085,10 +1088,11 @@ AdiArgs make_args(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bo
 }
 
 cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bool cold, double *P,
-                       const double *R, int ninst) {
+                       const double *R, int ninst, const int *d_inst_map) {
     AdiArgs a = make_args(c, sch, step0, nsteps_run, cold);
     if (P) a.P = P;
     if (R) a.R = R;
+    a.inst_map = d_inst_map;
     if (c->adi_seg) {
         ++c->launches;
         void *args[] = {&a};
@@ -1096,7 +1100,8 @@ cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_ru
         cudaLaunchConfig_t cfg = launch_config(c, dim3(c->N * ninst), dim3(c->adi_seg), (size_t)c->adi_smem, attr);
         return cudaLaunchKernelExC(&cfg, seg_kernel<double, false>(c->adi_seg, c->adi_full), args);
     }
-    // other variants: one launch per instance
+    // other variants: one launch per instance (batches need the on-chip kernel)
+    if (d_inst_map) return cudaErrorNotSupported;
     for (int i = 0; i < ninst; ++i) {
         AdiArgs ai = a;
         ai.P = a.P + (long long)i * c->N * c->nplane;

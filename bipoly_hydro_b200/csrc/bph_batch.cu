@@ -31,6 +31,11 @@ struct bph_batch {
     double *d_mom = nullptr;   // [mmax][cap][2][np]
     double *d_C = nullptr;     // [mmax][2cap][nb] column-major per mode
     double *d_rho_stage = nullptr, *d_pot_stage = nullptr;  // [cap][ntot] for host arrays
+    int *d_map = nullptr;      // [cap] instance of each batch position (device)
+    int *h_map = nullptr;      // [cap] pinned host copy
+    int *d_stat = nullptr;     // [cap] non-finite flag of each batch position (host-array calls)
+    int *h_stat = nullptr;     // [cap] pinned host copy
+    int stage_cap = 0;         // positions of the host-array staging buffers
     cublasHandle_t blas = nullptr;
     size_t bytes = 0;
 };
@@ -41,17 +46,18 @@ namespace {
 // One thread per (instance, boundary row or corner, slot), as k_boundary_slots.
 __global__ void k_boundary_slots_batch(const double *__restrict__ C, const double2 *__restrict__ ph,
                                        double *__restrict__ P, int numr, int numz, int nr, int nz, int nb, int N,
-                                       int mmax, int fm, int isym, double nfactor, int n, int cap) {
+                                       int mmax, int fm, int isym, double nfactor, int n, int cap,
+                                       const int *__restrict__ map) {
     const int M = N / 2;
     const int ncorner = (isym == 1) ? 2 : 1;
     const long long per = (long long)(nb + ncorner) * N;
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= per * n) return;
-    const int inst = (int)(t / per);
+    const int inst = (int)(t / per);  // batch position
     t -= inst * per;
     const int s = (int)(t % N), b = (int)(t / N);
     const long long nplane = (long long)numr * numz;
-    double *Pi = P + (long long)inst * N * nplane;
+    double *Pi = P + (long long)(map ? map[inst] : inst) * N * nplane;
     int jz, kz;
     if (b < nr) {
         jz = b + 1;
@@ -144,6 +150,17 @@ int bph_batch_create(bph_ctx_t *c, int capacity, bph_batch_t **out) {
     if (!rc) rc = batch_alloc(b, &b->d_mom, (size_t)c->g.mmax * capacity * 2 * c->np);
     if (!rc) rc = batch_alloc(b, &b->d_C, (size_t)c->g.mmax * 2 * capacity * c->nb);
     if (!rc) {
+        e = cudaMalloc((void **)&b->d_map, sizeof(int) * capacity);
+        if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_map, sizeof(int) * capacity);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_stat, sizeof(int) * capacity);
+        if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_stat, sizeof(int) * capacity);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            set_error("batch map allocation failed: %s", cudaGetErrorString(e));
+            rc = BPH_ERR_NOMEM;
+        }
+    }
+    if (!rc) {
         e = cudaMemsetAsync(b->d_P, 0, sizeof(double) * (size_t)capacity * c->N * c->nplane, c->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(b->d_mom, 0, sizeof(double) * (size_t)c->g.mmax * capacity * 2 * c->np,
                                                   c->stream);
@@ -169,28 +186,69 @@ int bph_batch_destroy(bph_batch_t *b) {
     double *bufs[] = {b->d_P, b->d_R, b->d_mom, b->d_C, b->d_rho_stage, b->d_pot_stage};
     for (double *p : bufs)
         if (p) cudaFree(p);
+    if (b->d_map) cudaFree(b->d_map);
+    if (b->h_map) cudaFreeHost(b->h_map);
+    if (b->d_stat) cudaFree(b->d_stat);
+    if (b->h_stat) cudaFreeHost(b->h_stat);
     delete b;
     return BPH_OK;
 }
 
 int bph_batch_solve(bph_batch_t *b, int n, const double *const *rho, double *const *pot, int tstep, int on_device) {
+    return bph_batch_solve_instances(b, n, nullptr, rho, pot, tstep, on_device);
+}
+
+int bph_batch_solve_instances(bph_batch_t *b, int n, const int *instances, const double *const *rho,
+                              double *const *pot, int tstep, int on_device) {
+    return bph::batch_solve_core(b, n, instances, rho, pot, tstep > 1, on_device != 0, nullptr);
+}
+
+}  // extern "C"
+
+namespace bph {
+
+// pos_status (host arrays only): per-position BPH_OK / BPH_ERR_NONFINITE
+// instead of one aggregated status.
+int batch_solve_core(bph_batch *b, int n, const int *instances, const double *const *rho, double *const *pot,
+                     bool warm, bool on_device, int *pos_status) {
     if (!b || !rho || !pot || n < 1 || n > b->cap) {
         set_error("invalid batch arguments (n must be in 1..capacity)");
         return BPH_ERR_INVALID;
     }
     for (int i = 0; i < n; ++i)
         if (!rho[i] || !pot[i]) {
-            set_error("instance %d has a NULL array", i);
+            set_error("batch position %d has a NULL array", i);
             return BPH_ERR_INVALID;
         }
+    if (instances) {
+        // distinct instances in range
+        std::vector<char> seen((size_t)b->cap, 0);
+        for (int i = 0; i < n; ++i) {
+            const int v = instances[i];
+            if (v < 0 || v >= b->cap || seen[(size_t)v]) {
+                set_error("instance %d at position %d is out of range or repeated", v, i);
+                return BPH_ERR_INVALID;
+            }
+            seen[(size_t)v] = 1;
+        }
+    }
     bph_ctx *c = b->c;
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
-    const bool warm = tstep > 1;  // potential_solver.F90:80
-    Schedule *s;
+    Schedule *s;  // warm: 5 steps, cold: 20 (potential_solver.F90:80-94)
     int rc = batch_schedule(c, warm ? 5 : 20, &s);
     if (rc) return rc;
     const size_t bytes = sizeof(double) * (size_t)c->ntot;
+    std::vector<int> inst(n);
+    for (int i = 0; i < n; ++i) inst[i] = instances ? instances[i] : i;
+    const int *d_map = nullptr;
+    if (instances) {
+        // the previous call's map may still be read by its kernels
+        BPH_CUDA(cudaStreamSynchronize(c->stream));
+        for (int i = 0; i < n; ++i) b->h_map[i] = inst[i];
+        BPH_CUDA(cudaMemcpyAsync(b->d_map, b->h_map, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+        d_map = b->d_map;
+    }
     std::vector<const double *> d_rho(n);
     std::vector<double *> d_pot(n);
     if (on_device) {
@@ -199,8 +257,25 @@ int bph_batch_solve(bph_batch_t *b, int n, const double *const *rho, double *con
             d_pot[i] = pot[i];
         }
     } else {
-        if (!b->d_rho_stage && (rc = batch_alloc(b, &b->d_rho_stage, (size_t)b->cap * c->ntot))) return rc;
-        if (!b->d_pot_stage && (rc = batch_alloc(b, &b->d_pot_stage, (size_t)b->cap * c->ntot))) return rc;
+        if (b->stage_cap < n) {
+            // staging grows to the largest batch seen
+            BPH_CUDA(cudaStreamSynchronize(c->stream));
+            if (b->d_rho_stage) {
+                cudaFree(b->d_rho_stage);
+                b->bytes -= sizeof(double) * (size_t)b->stage_cap * c->ntot;
+                b->d_rho_stage = nullptr;
+            }
+            if (b->d_pot_stage) {
+                cudaFree(b->d_pot_stage);
+                b->bytes -= sizeof(double) * (size_t)b->stage_cap * c->ntot;
+                b->d_pot_stage = nullptr;
+            }
+            b->stage_cap = 0;
+            if ((rc = batch_alloc(b, &b->d_rho_stage, (size_t)n * c->ntot))) return rc;
+            if ((rc = batch_alloc(b, &b->d_pot_stage, (size_t)n * c->ntot))) return rc;
+            b->stage_cap = n;
+        }
+        BPH_CUDA(cudaMemsetAsync(b->d_stat, 0, sizeof(int) * n, c->stream));
         for (int i = 0; i < n; ++i) {
             d_rho[i] = b->d_rho_stage + (size_t)i * c->ntot;
             d_pot[i] = b->d_pot_stage + (size_t)i * c->ntot;
@@ -210,8 +285,9 @@ int bph_batch_solve(bph_batch_t *b, int n, const double *const *rho, double *con
     const long long np = c->np;
     const long long mstride = 2LL * b->cap * np;
     for (int i = 0; i < n; ++i)
-        BPH_CUDA(launch_fft_fwd_rho(c, d_rho[i], b->d_R + (size_t)i * c->N * np, b->d_mom + 2LL * i * np, mstride));
-    // C_m = G_m^T M_m for every mode in one strided-batched DGEMM
+        BPH_CUDA(launch_fft_fwd_rho(c, d_rho[i], b->d_R + (size_t)inst[i] * c->N * np, b->d_mom + 2LL * i * np,
+                                    mstride, on_device ? nullptr : b->d_stat + i));
+    // C_m = G_m^T M_m for every mode in one strided-batched DGEMM (batch positions)
     {
         cublasStatus_t st = cublasSetStream(b->blas, c->stream);
         if (st != CUBLAS_STATUS_SUCCESS) return blas_fail(st, "cublasSetStream");
@@ -227,19 +303,35 @@ int bph_batch_solve(bph_batch_t *b, int n, const double *const *rho, double *con
         ++c->launches;
         k_boundary_slots_batch<<<(unsigned)((total + 255) / 256), 256, 0, c->stream>>>(
             b->d_C, c->d_ph, b->d_P, c->g.numr, c->g.numz, c->nr, c->nz, c->nb, c->N, c->g.mmax, c->fm, c->g.isym,
-            (double)c->N * c->factor, n, b->cap);
+            (double)c->N * c->factor, n, b->cap, d_map);
         BPH_CUDA(cudaGetLastError());
     }
-    BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, !warm, b->d_P, b->d_R, n));
+    BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, !warm, b->d_P, b->d_R, n, d_map));
     for (int i = 0; i < n; ++i)
-        BPH_CUDA(launch_fft_inv(c, d_pot[i], nullptr, 0.0, b->d_P + (size_t)i * c->N * c->nplane));
+        BPH_CUDA(launch_fft_inv(c, d_pot[i], nullptr, 0.0, b->d_P + (size_t)inst[i] * c->N * c->nplane));
     if (!on_device) {
         for (int i = 0; i < n; ++i)
             BPH_CUDA(cudaMemcpyAsync(pot[i], d_pot[i], bytes, cudaMemcpyDeviceToHost, c->stream));
-        return bph_synchronize(c);
+        BPH_CUDA(cudaMemcpyAsync(b->h_stat, b->d_stat, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream));
+        BPH_CUDA(cudaStreamSynchronize(c->stream));
+        int bad = -1;
+        for (int i = 0; i < n; ++i) {
+            const bool nf = (b->h_stat[i] & kStatusNonFinite) != 0;
+            if (pos_status) pos_status[i] = nf ? BPH_ERR_NONFINITE : BPH_OK;
+            if (nf && bad < 0) bad = i;
+        }
+        if (bad >= 0 && !pos_status) {
+            set_error("density of batch position %d contains NaN or Inf", bad);
+            return BPH_ERR_NONFINITE;
+        }
+        return BPH_OK;
     }
     return BPH_OK;
 }
+
+}  // namespace bph
+
+extern "C" {
 
 size_t bph_batch_device_bytes(const bph_batch_t *b) { return b ? b->bytes : 0; }
 

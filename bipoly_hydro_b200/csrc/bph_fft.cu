@@ -367,13 +367,13 @@ cudaError_t set_fft_attrs(bph_ctx *c) {
 }
 
 template <int M>
-cudaError_t fwd_rho(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride) {
+cudaError_t fwd_rho(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride, int *status) {
     unsigned blocks = (unsigned)((c->np + kTile - 1) / kTile);
     cudaLaunchAttribute attr[1];
     cudaLaunchConfig_t cfg = launch_config(c, dim3(blocks), dim3(FftShape<M>::kThreads), FftShape<M>::kSmem, attr);
     return cudaLaunchKernelEx(&cfg, k_fft_fwd<M, true>, rho, R, mom, (const double2 *)c->d_tw,
                               (const double2 *)c->d_tw2, (const double2 *)c->d_ph, c->g.numr, c->g.numz, c->nr,
-                              c->nz, c->g.mmax, c->fm, c->g.isym, c->four_pi, c->d_status, mstride);
+                              c->nz, c->g.mmax, c->fm, c->g.isym, c->four_pi, status, mstride);
 }
 
 template <int M>
@@ -406,8 +406,8 @@ cudaError_t inv(bph_ctx *c, double *pot, double *phieff, double omega, const dou
     }
 
 cudaError_t set_attrs_dispatch(bph_ctx *c) { BPH_FFT_DISPATCH(set_fft_attrs, c) }
-cudaError_t fwd_rho_dispatch(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride) {
-    BPH_FFT_DISPATCH(fwd_rho, c, rho, R, mom, mstride)
+cudaError_t fwd_rho_dispatch(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride, int *status) {
+    BPH_FFT_DISPATCH(fwd_rho, c, rho, R, mom, mstride, status)
 }
 cudaError_t fwd_pot_dispatch(bph_ctx *c, const double *pot) { BPH_FFT_DISPATCH(fwd_pot, c, pot) }
 cudaError_t inv_dispatch(bph_ctx *c, double *pot, double *phieff, double omega, const double *P) {
@@ -422,9 +422,11 @@ int fft_configure(bph_ctx *c) {
     return BPH_OK;
 }
 
-cudaError_t launch_fft_fwd_rho(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride) {
+cudaError_t launch_fft_fwd_rho(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride,
+                               int *status) {
     ++c->launches;
-    return fwd_rho_dispatch(c, rho, R ? R : c->d_R, mom ? mom : c->d_mom, mstride ? mstride : 2 * c->np);
+    return fwd_rho_dispatch(c, rho, R ? R : c->d_R, mom ? mom : c->d_mom, mstride ? mstride : 2 * c->np,
+                            status ? status : c->d_status);
 }
 
 cudaError_t launch_fft_fwd_pot(bph_ctx *c, const double *pot) {

@@ -159,8 +159,9 @@ cudaError_t launch_qcoef(bph_ctx *c);
 cudaError_t launch_green_tables(bph_ctx *c);
 cudaError_t launch_adi_factors(bph_ctx *c, Schedule &s);
 // Optional arguments select batch buffers (R, moments with m-stride, P, instance count).
+// status: where a non-finite density is flagged (nullptr: the context's status word).
 cudaError_t launch_fft_fwd_rho(bph_ctx *c, const double *rho, double *R = nullptr, double *mom = nullptr,
-                               long long mstride = 0);
+                               long long mstride = 0, int *status = nullptr);
 cudaError_t launch_fft_fwd_pot(bph_ctx *c, const double *pot);
 cudaError_t launch_fft_inv(bph_ctx *c, double *pot, double *phieff = nullptr, double omega = 0.0,
                            const double *P = nullptr);
@@ -168,13 +169,20 @@ cudaError_t launch_fft_inv(bph_ctx *c, double *pot, double *phieff = nullptr, do
 // fused form of launch_boundary_slots, which stays for phase timing).
 cudaError_t launch_green_contract(bph_ctx *c, bool write_slots = true);
 cudaError_t launch_boundary_slots(bph_ctx *c);
+// ninst instances of slot arrays P/R; block row i solves instance d_inst_map[i]
+// (nullptr: instance i).
 cudaError_t launch_adi(bph_ctx *c, const Schedule &s, int step0, int nsteps_run, bool cold, double *P = nullptr,
-                       const double *R = nullptr, int ninst = 1);
+                       const double *R = nullptr, int ninst = 1, const int *d_inst_map = nullptr);
 cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &s);
 cudaError_t launch_update_norm(bph_ctx *c, double *d_out);
 cudaError_t launch_residual_norm(bph_ctx *c, double *d_out);
 
 int adi_configure(bph_ctx *c);
+// Batched solve of batch positions 0..n-1 (bph_batch.cu); instances may be
+// nullptr (position i = instance i); pos_status: per-position result of a
+// host-array call.
+int batch_solve_core(bph_batch *b, int n, const int *instances, const double *const *rho, double *const *pot,
+                     bool warm, bool on_device, int *pos_status);
 // Makes kind (BPH_MIXED_ADI_FORWARD / _INCREMENT) the refinement ADI kernel.
 int select_mixed_kind(bph_ctx *c, int kind);
 int contract_configure(bph_ctx *c);

@@ -14,6 +14,7 @@ if the library or a CUDA device is missing, construction raises.
 from __future__ import annotations
 
 import ctypes
+import weakref
 import os
 from dataclasses import dataclass
 
@@ -45,7 +46,10 @@ EXPORTED_SYMBOLS = (
     "bph_solve_converged", "bph_potential_solver_phieff", "bph_set_potential", "bph_solve_converged_mixed", "bph_set_stream", "bph_synchronize", "bph_destroy", "bph_last_error",
     "bph_version", "bph_num_boundary_rows", "bph_copy_green", "bph_copy_moments", "bph_run_phase",
     "bph_green_contract_noalloc", "bph_info", "bph_configure", "bph_launch_count", "bph_device_bytes",
-    "bph_batch_create", "bph_batch_solve", "bph_batch_destroy", "bph_batch_device_bytes",
+    "bph_batch_create", "bph_batch_solve", "bph_batch_solve_instances", "bph_batch_destroy",
+    "bph_batch_device_bytes",
+    "bph_server_create", "bph_server_capacity", "bph_server_open_client", "bph_server_close_client",
+    "bph_server_submit", "bph_server_poll", "bph_server_wait", "bph_server_stats", "bph_server_destroy",
 )
 
 #: bph_configure keys and values.
@@ -118,8 +122,24 @@ def load_library(path: str | None = None):
     L.bph_batch_create.restype = ctypes.c_int
     L.bph_batch_solve.argtypes = [vp, i, ctypes.POINTER(vp), ctypes.POINTER(vp), i, i]
     L.bph_batch_solve.restype = ctypes.c_int
+    L.bph_batch_solve_instances.argtypes = [vp, i, ctypes.POINTER(i), ctypes.POINTER(vp), ctypes.POINTER(vp), i, i]
+    L.bph_batch_solve_instances.restype = ctypes.c_int
     L.bph_batch_destroy.argtypes = [vp]
     L.bph_batch_destroy.restype = ctypes.c_int
+    ll, dbl = ctypes.c_longlong, ctypes.c_double
+    L.bph_server_create.argtypes = [vp, i, sz, i, ctypes.POINTER(vp)]
+    L.bph_server_capacity.argtypes = [vp]
+    L.bph_server_open_client.argtypes = [vp, ctypes.POINTER(i)]
+    L.bph_server_close_client.argtypes = [vp, i]
+    L.bph_server_submit.argtypes = [vp, i, dp, dp, ctypes.POINTER(ll)]
+    L.bph_server_poll.argtypes = [vp, ll, ctypes.POINTER(dbl)]
+    L.bph_server_wait.argtypes = [vp, ll, dbl, ctypes.POINTER(dbl)]
+    L.bph_server_stats.argtypes = [vp, ctypes.POINTER(ll), ctypes.POINTER(ll)]
+    L.bph_server_destroy.argtypes = [vp]
+    for name in ("bph_server_create", "bph_server_capacity", "bph_server_open_client", "bph_server_close_client",
+                 "bph_server_submit", "bph_server_poll", "bph_server_wait", "bph_server_stats",
+                 "bph_server_destroy"):
+        getattr(L, name).restype = ctypes.c_int
     L.bph_batch_device_bytes.argtypes = [vp]
     L.bph_batch_device_bytes.restype = ctypes.c_size_t
     L.bph_info.argtypes = [vp, i]
@@ -172,6 +192,7 @@ class PotentialSolver:
 
     def __init__(self, numr: int, numz: int, numphi: int, dr: float, isym: int = 2, mmax: int = 30):
         self._lib = load_library()
+        self._dependents = weakref.WeakSet()
         self.grid = Grid(int(numr), int(numz), int(numphi), float(dr), int(isym), int(mmax))
         self.shape = (int(numr), int(numz), int(numphi))
         self.isym, self.mmax, self.dr = int(isym), int(mmax), float(dr)
@@ -181,6 +202,9 @@ class PotentialSolver:
 
     # -- lifetime -----------------------------------------------------------
     def close(self) -> None:
+        # batches and servers on this context go first (they hold its device state)
+        for dep in list(getattr(self, "_dependents", ())):
+            dep.close()
         if getattr(self, "_h", None):
             self._lib.bph_destroy(self._h)
             self._h = None
@@ -344,6 +368,7 @@ class Batch:
         self.solver = solver
         self._lib = solver._lib
         self.capacity = int(capacity)
+        solver._dependents.add(self)
         h = ctypes.c_void_p()
         _check(self._lib.bph_batch_create(solver._h, self.capacity, ctypes.byref(h)))
         self._h = h
@@ -376,6 +401,103 @@ class Batch:
         arr_p = (ctypes.c_void_p * n)(*[_dev_ptr(x) for x in d_pots])
         _check(self._lib.bph_batch_solve(self._h, n, arr_r, arr_p, int(tstep), 1))
 
+    def solve_instances(self, instances, rhos, tstep: int):
+        """Host arrays for the distinct ``instances``; the others keep their state."""
+        rs = [self.solver._rho_host(r) for r in rhos]
+        pots = [np.empty(self.solver.shape, dtype=np.float64, order="F") for _ in rs]
+        n = len(rs)
+        idx = (ctypes.c_int * n)(*[int(v) for v in instances])
+        arr_r = (ctypes.c_void_p * n)(*[a.ctypes.data for a in rs])
+        arr_p = (ctypes.c_void_p * n)(*[a.ctypes.data for a in pots])
+        _check(self._lib.bph_batch_solve_instances(self._h, n, idx, arr_r, arr_p, int(tstep), 0))
+        return pots
+
     @property
     def device_bytes(self) -> int:
         return int(self._lib.bph_batch_device_bytes(self._h))
+
+
+BPH_PENDING = 1
+
+
+class Server:
+    """Continuous batching of solve requests for resident clients (bph_server_*).
+
+    Each client keeps its density transform and last potential on the device;
+    its first request is cold, later ones warm-start from its previous
+    potential.  ``submit`` returns at once; ``poll``/``wait`` report completion.
+    The server drives the solver's context from a worker thread: make no other
+    call on that solver while the server is open.
+    """
+
+    def __init__(self, solver: PotentialSolver, max_clients: int, mem_cap_bytes: int = 0, max_batch: int = 0):
+        self.solver = solver
+        self._lib = solver._lib
+        h = ctypes.c_void_p()
+        _check(self._lib.bph_server_create(solver._h, int(max_clients), int(mem_cap_bytes), int(max_batch),
+                                           ctypes.byref(h)))
+        self._h = h
+        self._live = {}  # request id -> (rho, pot) kept alive until completion
+        solver._dependents.add(self)
+
+    @property
+    def capacity(self) -> int:
+        return int(self._lib.bph_server_capacity(self._h))
+
+    def open_client(self) -> int:
+        cid = ctypes.c_int(-1)
+        _check(self._lib.bph_server_open_client(self._h, ctypes.byref(cid)))
+        return cid.value
+
+    def close_client(self, client: int) -> None:
+        _check(self._lib.bph_server_close_client(self._h, int(client)))
+
+    def submit(self, client: int, rho, pot=None) -> int:
+        """Queue a solve; ``pot`` (Fortran-ordered float64, allocated if None) is
+        written when the request completes.  Returns the request id."""
+        r = self.solver._rho_host(rho)
+        if pot is None:
+            pot = np.empty(self.solver.shape, dtype=np.float64, order="F")
+        if not (pot.flags.f_contiguous and pot.dtype == np.float64 and pot.shape == self.solver.shape):
+            raise ValueError("pot must be a Fortran-ordered float64 array of the grid's shape")
+        rid = ctypes.c_longlong(0)
+        _check(self._lib.bph_server_submit(self._h, int(client), _host_ptr(r), _host_ptr(pot), ctypes.byref(rid)))
+        self._live[rid.value] = (r, pot)
+        return rid.value
+
+    def poll(self, request: int):
+        """None while pending, else (pot, latency_s); raises BphError if it failed."""
+        lat = ctypes.c_double(0.0)
+        rc = self._lib.bph_server_poll(self._h, int(request), ctypes.byref(lat))
+        if rc == BPH_PENDING:
+            return None
+        _, pot = self._live.pop(int(request), (None, None))
+        _check(rc)
+        return pot, lat.value
+
+    def wait(self, request: int, timeout: float = 0.0):
+        """(pot, latency_s) once the request completes; raises BphError if it failed or timed out."""
+        lat = ctypes.c_double(0.0)
+        rc = self._lib.bph_server_wait(self._h, int(request), float(timeout), ctypes.byref(lat))
+        if rc == -5:  # BPH_ERR_TIMEOUT: still pending, keep its arrays alive
+            _check(rc)
+        _, pot = self._live.pop(int(request), (None, None))
+        _check(rc)
+        return pot, lat.value
+
+    def stats(self):
+        b, n = ctypes.c_longlong(0), ctypes.c_longlong(0)
+        _check(self._lib.bph_server_stats(self._h, ctypes.byref(b), ctypes.byref(n)))
+        return {"batches": b.value, "solves": n.value}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.bph_server_destroy(self._h)
+            self._h = None
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

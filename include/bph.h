@@ -28,6 +28,7 @@ extern "C" {
 #define BPH_ERR_CUDA (-4)      /* CUDA runtime failure (text in bph_last_error) */
 #define BPH_ERR_TIMEOUT (-5)   /* a bounded wait expired */
 #define BPH_ERR_STATE (-6)     /* call made in the wrong state */
+#define BPH_PENDING 1          /* request not finished yet (bph_server_poll) */
 
 /* Grid and solver constants.  potsetup reads these from runhydro.h
  * (numr, numz, numphi), setup_frac.F90:374-376 (dr; dz = dr), the fort.7
@@ -121,8 +122,55 @@ int bph_batch_create(bph_ctx_t *ctx, int capacity, bph_batch_t **batch);
  * rounding. */
 int bph_batch_solve(bph_batch_t *batch, int n, const double *const *rho, double *const *pot, int tstep,
                     int on_device);
+
+/* As bph_batch_solve for the n distinct instances instances[0..n-1]
+ * (each in 0..capacity-1): position i of rho/pot belongs to instance
+ * instances[i]; the other instances keep their state untouched. */
+int bph_batch_solve_instances(bph_batch_t *batch, int n, const int *instances, const double *const *rho,
+                              double *const *pot, int tstep, int on_device);
 int bph_batch_destroy(bph_batch_t *batch);
 size_t bph_batch_device_bytes(const bph_batch_t *batch);
+
+/* ---- serving: continuous batching (no counterpart in the reference) ----
+ *
+ * A server drives one context from a worker thread (make no other call on
+ * that context until bph_server_destroy).  A client is a resident instance:
+ * its -4 pi rho_hat and its last potential stay on the device, its first
+ * request is a cold 20-step solve and every later one a warm 5-step solve
+ * from its previous potential (potential_solver.F90:80-94), as a sequence
+ * of potential_solver calls would be.  Requests queue in arrival order;
+ * whenever the GPU is free the worker takes the oldest pending request of
+ * every client that has one (at most max_batch; 0 = no limit) and solves
+ * them together (bph_batch_solve_instances: one pass over the tables),
+ * so requests that arrive while a batch runs join the next one.  Results
+ * equal the client's own sequence of single solves to rounding.
+ *
+ * Admission: the number of resident clients is fixed at creation by
+ * mem_cap_bytes (0 = no cap) and the free device memory, each client
+ * counting its slot arrays, moments and host staging; opening a client
+ * beyond that returns BPH_ERR_NOMEM.  rho/pot are host arrays of the grid's
+ * layout that the caller keeps valid until the request completes (pot is
+ * written then).  A request whose density holds NaN or Inf completes with
+ * BPH_ERR_NONFINITE and its client's next request runs cold; the other
+ * requests of its batch are unaffected. */
+typedef struct bph_server bph_server_t;
+int bph_server_create(bph_ctx_t *ctx, int max_clients, size_t mem_cap_bytes, int max_batch,
+                      bph_server_t **server);
+/* Resident clients this server admits. */
+int bph_server_capacity(const bph_server_t *server);
+int bph_server_open_client(bph_server_t *server, int *client);
+/* Queued requests of the client still complete; its slot is reused after. */
+int bph_server_close_client(bph_server_t *server, int client);
+int bph_server_submit(bph_server_t *server, int client, const double *rho, double *pot, long long *request);
+/* BPH_PENDING, or the request's final status (then forgotten); latency_s
+ * (may be NULL) receives submit-to-completion seconds. */
+int bph_server_poll(bph_server_t *server, long long request, double *latency_s);
+/* Blocks until the request completes (timeout_s <= 0: no limit; else
+ * BPH_ERR_TIMEOUT when it expires), then reports as bph_server_poll. */
+int bph_server_wait(bph_server_t *server, long long request, double timeout_s, double *latency_s);
+int bph_server_stats(const bph_server_t *server, long long *batches, long long *solves);
+/* Finishes the queued requests, stops the worker, frees the clients. */
+int bph_server_destroy(bph_server_t *server);
 
 /* Stream used for all later work of this context (a cudaStream_t; NULL is
  * CUDA's default stream).  Until the first call the context uses a
