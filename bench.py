@@ -254,6 +254,68 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def serve_bench(B, torch, dev, rhos, args):
+    """Continuous-batching server under Poisson arrivals (config-5 recipe).
+
+    serve_clients resident clients on the 130x98x256 grid, each running an
+    SCF-like sequence rho <- 0.9 rho + 0.1 rho (1 + 0.01 N(0,1)) renormalised
+    to its initial mass, densities kept on the device (two buffers per
+    client); the requests of all clients arrive as one Poisson process at the
+    offered rate.  Latency is submit-to-completion as the server records it.
+    """
+    nclients, iters = args.serve_clients, args.serve_iters
+    srv_solver = B.PotentialSolver(**GRID)
+    srv = B.Server(srv_solver, max_clients=nclients, mem_cap_bytes=150 * 10 ** 9, device_arrays=True)
+    nrot = rhos.shape[0]
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(20261203)
+    out = {"grid": "130x98x256", "clients": nclients, "requests_per_rate": nclients * iters,
+           "capacity": srv.capacity, "dtype": "f64", "mixed": None,
+           "mixed_note": "the batched/serving path is FP64 only (no mixed-precision batch kernel)",
+           "rates": []}
+    for rate in [float(x) for x in args.serve_rates.split(",") if x]:
+        ids = [srv.open_client() for _ in range(nclients)]
+        rho = [[rhos[(37 * c) % nrot] * (1.0 + 0.2 * c / nclients), torch.empty_like(rhos[0])] for c in range(nclients)]
+        mass = [float(r[0].sum()) for r in rho]
+        pot = [[torch.empty_like(rhos[0]), torch.empty_like(rhos[0])] for _ in range(nclients)]
+        rng = np.random.default_rng(int(rate))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=nclients * iters))
+        rid = {}
+        lat = []
+        st0 = srv.stats()
+        t0 = time.perf_counter()
+        for k in range(nclients * iters):
+            c, it = k % nclients, k // nclients
+            buf = it % 2
+            if it >= 2:
+                lat.append(srv.wait(rid.pop((c, it - 2)), timeout=120.0)[1])
+            src = rho[c][1 - buf] if it > 0 else rho[c][0]
+            if it > 0:
+                noise = torch.randn(src.shape, generator=gen, device=dev, dtype=torch.float64)
+                nxt = src * (1.0 + 0.001 * noise)
+                rho[c][buf].copy_(nxt * (mass[c] / float(nxt.sum())))
+            else:
+                rho[c][buf] = src.clone()
+            torch.cuda.current_stream().synchronize()
+            while time.perf_counter() - t0 < arrivals[k]:
+                pass
+            rid[(c, it)] = srv.submit(ids[c], rho[c][buf], pot[c][buf])
+        for key in list(rid):
+            lat.append(srv.wait(rid.pop(key), timeout=120.0)[1])
+        elapsed = time.perf_counter() - t0
+        st = srv.stats()
+        out["rates"].append({"offered_req_per_s": rate, "solves_per_s": nclients * iters / elapsed,
+                             "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+                             "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                             "mean_batch": (st["solves"] - st0["solves"]) / max(1, st["batches"] - st0["batches"])})
+        for cid in ids:
+            srv.close_client(cid)
+        del rho, pot
+    srv.close()
+    srv_solver.close()
+    return out
+
+
 def run_gpu(args, world, rank, local):
     import torch
 
@@ -401,6 +463,11 @@ def run_gpu(args, world, rank, local):
             del outs
             bt.close()
 
+    # ---- serving: Poisson arrivals of SCF-like client requests ----------
+    serving = None
+    if args.serve_rates:
+        serving = serve_bench(B, torch, dev, rhos, args)
+
     # ---- converged solves: FP64 vs mixed (FP32 ADI + FP64 refinement) --
     conv = None
     if args.converged_steps > 0:
@@ -476,6 +543,7 @@ def run_gpu(args, world, rank, local):
             "phase_ms": phases,
             "converged": conv,
             "batched": batched,
+            "serving": serving,
             "launch_config": solver_info,
             "gpu_launches": launches,
             "clocks": clocks,
@@ -496,6 +564,10 @@ def main():
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
     ap.add_argument("--batch-sizes", default="4,16", help="batched warm solves timed per batch size (empty skips)")
     ap.add_argument("--batch-calls", type=int, default=20)
+    ap.add_argument("--serve-rates", default="200,1000,4000",
+                    help="offered request rates (req/s) of the serving section (empty skips)")
+    ap.add_argument("--serve-clients", type=int, default=64)
+    ap.add_argument("--serve-iters", type=int, default=8, help="SCF-like requests per client per rate")
     ap.add_argument("--converged-steps", type=int, default=20,
                     help="warm converged solves timed per form (FP64 and mixed); 0 skips")
     ap.add_argument("--conv-nsteps", type=int, default=10, help="ADI steps per refinement cycle")

@@ -275,18 +275,20 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
             if ((rc = batch_alloc(b, &b->d_pot_stage, (size_t)n * c->ntot))) return rc;
             b->stage_cap = n;
         }
-        BPH_CUDA(cudaMemsetAsync(b->d_stat, 0, sizeof(int) * n, c->stream));
         for (int i = 0; i < n; ++i) {
             d_rho[i] = b->d_rho_stage + (size_t)i * c->ntot;
             d_pot[i] = b->d_pot_stage + (size_t)i * c->ntot;
             BPH_CUDA(cudaMemcpyAsync((void *)d_rho[i], rho[i], bytes, cudaMemcpyHostToDevice, c->stream));
         }
     }
+    // per-position non-finite flags: host-array calls and callers that want per-position status
+    const bool per_pos = !on_device || pos_status;
+    if (per_pos) BPH_CUDA(cudaMemsetAsync(b->d_stat, 0, sizeof(int) * n, c->stream));
     const long long np = c->np;
     const long long mstride = 2LL * b->cap * np;
     for (int i = 0; i < n; ++i)
         BPH_CUDA(launch_fft_fwd_rho(c, d_rho[i], b->d_R + (size_t)inst[i] * c->N * np, b->d_mom + 2LL * i * np,
-                                    mstride, on_device ? nullptr : b->d_stat + i));
+                                    mstride, per_pos ? b->d_stat + i : nullptr));
     // C_m = G_m^T M_m for every mode in one strided-batched DGEMM (batch positions)
     {
         cublasStatus_t st = cublasSetStream(b->blas, c->stream);
@@ -309,9 +311,10 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
     BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, !warm, b->d_P, b->d_R, n, d_map));
     for (int i = 0; i < n; ++i)
         BPH_CUDA(launch_fft_inv(c, d_pot[i], nullptr, 0.0, b->d_P + (size_t)inst[i] * c->N * c->nplane));
-    if (!on_device) {
-        for (int i = 0; i < n; ++i)
-            BPH_CUDA(cudaMemcpyAsync(pot[i], d_pot[i], bytes, cudaMemcpyDeviceToHost, c->stream));
+    if (per_pos) {
+        if (!on_device)
+            for (int i = 0; i < n; ++i)
+                BPH_CUDA(cudaMemcpyAsync(pot[i], d_pot[i], bytes, cudaMemcpyDeviceToHost, c->stream));
         BPH_CUDA(cudaMemcpyAsync(b->h_stat, b->d_stat, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream));
         BPH_CUDA(cudaStreamSynchronize(c->stream));
         int bad = -1;

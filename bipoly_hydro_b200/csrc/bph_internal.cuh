@@ -179,8 +179,8 @@ cudaError_t launch_residual_norm(bph_ctx *c, double *d_out);
 
 int adi_configure(bph_ctx *c);
 // Batched solve of batch positions 0..n-1 (bph_batch.cu); instances may be
-// nullptr (position i = instance i); pos_status: per-position result of a
-// host-array call.
+// nullptr (position i = instance i).  With pos_status (per-position
+// BPH_OK / BPH_ERR_NONFINITE) or host arrays the call is synchronous.
 int batch_solve_core(bph_batch *b, int n, const int *instances, const double *const *rho, double *const *pot,
                      bool warm, bool on_device, int *pos_status);
 // Makes kind (BPH_MIXED_ADI_FORWARD / _INCREMENT) the refinement ADI kernel.

@@ -30,6 +30,7 @@ struct bph_server {
     bph_batch *batch = nullptr;
     int capacity = 0;   // resident clients
     int max_batch = 0;  // requests per batched call
+    bool device_arrays = false;  // rho/pot are device arrays (else host arrays)
     size_t bytes_per_client = 0;
 
     struct Request {
@@ -114,7 +115,7 @@ void serve_loop(bph_server *s) {
             const int n = (int)group_ids.size();
             group_status.assign((size_t)n, BPH_OK);
             int rc = batch_solve_core(s->batch, n, group_inst.data(), group_rho.data(), group_pot.data(), warm_pass,
-                                      false, group_status.data());
+                                      s->device_arrays, group_status.data());
             const double t = now_s();
             {
                 std::lock_guard<std::mutex> lk(s->mu);
@@ -141,16 +142,18 @@ using namespace bph;
 
 extern "C" {
 
-int bph_server_create(bph_ctx_t *c, int max_clients, size_t mem_cap_bytes, int max_batch, bph_server_t **out) {
+int bph_server_create(bph_ctx_t *c, int max_clients, size_t mem_cap_bytes, int max_batch, int flags,
+                      bph_server_t **out) {
     if (!out) {
         set_error("out-pointer is NULL");
         return BPH_ERR_INVALID;
     }
     *out = nullptr;
-    if (!c || max_clients < 1 || max_clients > 4096 || max_batch < 0) {
-        set_error("invalid context, client count (1..4096) or batch size");
+    if (!c || max_clients < 1 || max_clients > 4096 || max_batch < 0 || (flags & ~BPH_SERVER_DEVICE_ARRAYS)) {
+        set_error("invalid context, client count (1..4096), batch size or flags");
         return BPH_ERR_INVALID;
     }
+    const bool dev = (flags & BPH_SERVER_DEVICE_ARRAYS) != 0;
     if (!c->adi_seg) {
         set_error("serving needs the on-chip ADI kernel (grid too large)");
         return BPH_ERR_INVALID;
@@ -160,7 +163,7 @@ int bph_server_create(bph_ctx_t *c, int max_clients, size_t mem_cap_bytes, int m
     // resident bytes of one client: slot array, -4 pi rho_hat, moments and
     // contraction output of its batch position, host-array staging (rho, pot)
     const size_t per = sizeof(double) * ((size_t)c->N * c->nplane + (size_t)c->N * c->np + 2ull * c->g.mmax * c->np +
-                                         2ull * c->g.mmax * c->nb + 2ull * c->ntot);
+                                         2ull * c->g.mmax * c->nb + (dev ? 0ull : 2ull * c->ntot));
     size_t free_b = 0, total_b = 0;
     e = cudaMemGetInfo(&free_b, &total_b);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemGetInfo");
@@ -178,6 +181,7 @@ int bph_server_create(bph_ctx_t *c, int max_clients, size_t mem_cap_bytes, int m
     s->capacity = cap;
     s->max_batch = (max_batch == 0 || max_batch > cap) ? cap : max_batch;
     s->bytes_per_client = per;
+    s->device_arrays = dev;
     s->open.assign((size_t)cap, 0);
     s->warm.assign((size_t)cap, 0);
     s->inflight.assign((size_t)cap, 0);

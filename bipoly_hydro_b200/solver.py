@@ -127,7 +127,7 @@ def load_library(path: str | None = None):
     L.bph_batch_destroy.argtypes = [vp]
     L.bph_batch_destroy.restype = ctypes.c_int
     ll, dbl = ctypes.c_longlong, ctypes.c_double
-    L.bph_server_create.argtypes = [vp, i, sz, i, ctypes.POINTER(vp)]
+    L.bph_server_create.argtypes = [vp, i, sz, i, i, ctypes.POINTER(vp)]
     L.bph_server_capacity.argtypes = [vp]
     L.bph_server_open_client.argtypes = [vp, ctypes.POINTER(i)]
     L.bph_server_close_client.argtypes = [vp, i]
@@ -430,12 +430,14 @@ class Server:
     call on that solver while the server is open.
     """
 
-    def __init__(self, solver: PotentialSolver, max_clients: int, mem_cap_bytes: int = 0, max_batch: int = 0):
+    def __init__(self, solver: PotentialSolver, max_clients: int, mem_cap_bytes: int = 0, max_batch: int = 0,
+                 device_arrays: bool = False):
         self.solver = solver
         self._lib = solver._lib
+        self.device_arrays = bool(device_arrays)
         h = ctypes.c_void_p()
         _check(self._lib.bph_server_create(solver._h, int(max_clients), int(mem_cap_bytes), int(max_batch),
-                                           ctypes.byref(h)))
+                                           1 if self.device_arrays else 0, ctypes.byref(h)))
         self._h = h
         self._live = {}  # request id -> (rho, pot) kept alive until completion
         solver._dependents.add(self)
@@ -453,15 +455,23 @@ class Server:
         _check(self._lib.bph_server_close_client(self._h, int(client)))
 
     def submit(self, client: int, rho, pot=None) -> int:
-        """Queue a solve; ``pot`` (Fortran-ordered float64, allocated if None) is
-        written when the request completes.  Returns the request id."""
-        r = self.solver._rho_host(rho)
-        if pot is None:
-            pot = np.empty(self.solver.shape, dtype=np.float64, order="F")
-        if not (pot.flags.f_contiguous and pot.dtype == np.float64 and pot.shape == self.solver.shape):
-            raise ValueError("pot must be a Fortran-ordered float64 array of the grid's shape")
+        """Queue a solve; ``pot`` is written when the request completes.  Host
+        mode: Fortran-ordered float64 arrays (pot allocated if None).  Device
+        mode: CUDA tensors or device pointers, rho's writes complete.  Returns
+        the request id."""
+        if self.device_arrays:
+            if pot is None:
+                raise ValueError("device mode needs a pot array")
+            r, p_ptr, r_ptr = rho, _dev_ptr(pot), _dev_ptr(rho)
+        else:
+            r = self.solver._rho_host(rho)
+            if pot is None:
+                pot = np.empty(self.solver.shape, dtype=np.float64, order="F")
+            if not (pot.flags.f_contiguous and pot.dtype == np.float64 and pot.shape == self.solver.shape):
+                raise ValueError("pot must be a Fortran-ordered float64 array of the grid's shape")
+            r_ptr, p_ptr = _host_ptr(r), _host_ptr(pot)
         rid = ctypes.c_longlong(0)
-        _check(self._lib.bph_server_submit(self._h, int(client), _host_ptr(r), _host_ptr(pot), ctypes.byref(rid)))
+        _check(self._lib.bph_server_submit(self._h, int(client), r_ptr, p_ptr, ctypes.byref(rid)))
         self._live[rid.value] = (r, pot)
         return rid.value
 

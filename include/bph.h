@@ -148,13 +148,17 @@ size_t bph_batch_device_bytes(const bph_batch_t *batch);
  * Admission: the number of resident clients is fixed at creation by
  * mem_cap_bytes (0 = no cap) and the free device memory, each client
  * counting its slot arrays, moments and host staging; opening a client
- * beyond that returns BPH_ERR_NOMEM.  rho/pot are host arrays of the grid's
+ * beyond that returns BPH_ERR_NOMEM.  rho/pot are arrays of the grid's
  * layout that the caller keeps valid until the request completes (pot is
  * written then).  A request whose density holds NaN or Inf completes with
  * BPH_ERR_NONFINITE and its client's next request runs cold; the other
  * requests of its batch are unaffected. */
 typedef struct bph_server bph_server_t;
-int bph_server_create(bph_ctx_t *ctx, int max_clients, size_t mem_cap_bytes, int max_batch,
+/* flags: BPH_SERVER_DEVICE_ARRAYS makes rho/pot device arrays of the
+ * context's GPU (their writes must be complete when submitted; pot is
+ * complete when the request is reported done); else host arrays. */
+#define BPH_SERVER_DEVICE_ARRAYS 1
+int bph_server_create(bph_ctx_t *ctx, int max_clients, size_t mem_cap_bytes, int max_batch, int flags,
                       bph_server_t **server);
 /* Resident clients this server admits. */
 int bph_server_capacity(const bph_server_t *server);

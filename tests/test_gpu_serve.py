@@ -169,3 +169,25 @@ def test_production_grid_batched_clients(bph):
             ref = ref_solver.potential_solver(seqs[c][t], 0 if t == 0 else t + 1)
             assert rel_l2(res[(c, t)], ref) <= POT_TOL, (c, t)
     ref_solver.close()
+
+
+def test_device_array_mode_matches_host_mode(bph):
+    import torch
+
+    seqs = _densities(3, 3, seed=40)
+    g = bph.PotentialSolver(*GRID)
+    srv = bph.Server(g, max_clients=3, device_arrays=True)
+    ids = [srv.open_client() for _ in seqs]
+    d_rho = [[torch.from_numpy(np.ascontiguousarray(r.ravel(order="F"))).cuda() for r in seq] for seq in seqs]
+    d_pot = [[torch.empty_like(x) for x in row] for row in d_rho]
+    torch.cuda.synchronize()
+    rids = {(c, t): srv.submit(c, d_rho[c][t], d_pot[c][t]) for t in range(3) for c in ids}
+    for k, r in rids.items():
+        srv.wait(r, timeout=60.0)
+    srv.close()
+    g.close()
+    for c in ids:
+        ref = _single_sequence(bph, seqs[c])
+        for t in range(3):
+            got = d_pot[c][t].cpu().numpy().reshape(ref[t].shape, order="F")
+            assert rel_l2(got, ref[t]) <= POT_TOL, (c, t)
