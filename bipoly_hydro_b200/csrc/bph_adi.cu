@@ -42,6 +42,8 @@ struct AdiArgs {
     const double *bzb;      // [numz]    (defect form: residual)
     double *norms;          // [N][2]    (defect form: |delta|^2, |phi|^2 per slot)
     const int *inst_map;    // batches: instance of each block row (nullptr: block row = instance)
+    const int *slot_map;    // slot of each block within a row (nullptr: block = slot)
+    int nslots;             // blocks per row (N without slot_map)
     int numr, numz, nr, nz, N, isym;
     int step0, nsteps_run, cold;
     double gamma;
@@ -326,8 +328,8 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
     T *sm = reinterpret_cast<T *>(smraw);
     // blockIdx.x = instance * N + slot: the slot picks the coefficients, the
     // block index the slab (batches keep instances' slot arrays contiguous)
-    const int s = blockIdx.x % a.N, tid = threadIdx.x;
-    const int row = blockIdx.x / a.N;
+    const int local = blockIdx.x % a.nslots, row = blockIdx.x / a.nslots, tid = threadIdx.x;
+    const int s = a.slot_map ? a.slot_map[local] : local;
     const long long blk = (long long)(a.inst_map ? a.inst_map[row] : row) * a.N + s;
     const int lane = tid & 31, warp = tid >> 5, nwarps = kSegThreads / 32;
     const int nr = a.nr, nz = a.nz, numr = a.numr, numz = a.numz;
@@ -1074,6 +1076,8 @@ AdiArgs make_args(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bo
     a.bzb = c->d_bzb;
     a.norms = c->d_red;
     a.inst_map = nullptr;
+    a.slot_map = nullptr;
+    a.nslots = c->N;
     a.numr = c->g.numr;
     a.numz = c->g.numz;
     a.nr = c->nr;
@@ -1115,6 +1119,21 @@ cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_ru
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+cudaError_t launch_adi_slots(bph_ctx *c, const Schedule &sch, bool cold, const int *d_slots, int nslots,
+                             cudaStream_t st, bool pdl) {
+    if (!c->adi_seg || nslots < 1) return cudaErrorNotSupported;
+    AdiArgs a = make_args(c, sch, 0, sch.nsteps, cold);
+    a.slot_map = d_slots;
+    a.nslots = nslots;
+    ++c->launches;
+    void *args[] = {&a};
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = launch_config(c, dim3(nslots), dim3(c->adi_seg), (size_t)c->adi_smem, attr);
+    cfg.stream = st;
+    if (!pdl) cfg.numAttrs = 0;
+    return cudaLaunchKernelExC(&cfg, seg_kernel<double, false>(c->adi_seg, c->adi_full), args);
 }
 
 cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {

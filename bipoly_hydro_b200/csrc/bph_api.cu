@@ -342,6 +342,32 @@ int setup_impl(bph_ctx *c) {
         const char *pdl = std::getenv("BPH_PDL");
         c->pdl = !(pdl && pdl[0] == '0');
     }
+    {
+        // slots that carry boundary data (the contraction writes them) last
+        std::vector<int> map, dep;
+        for (int sl = 0; sl < c->N; ++sl) {
+            const int k = (sl <= c->M) ? sl : sl - c->M;
+            const bool has_bc = (k < c->M) && (k % c->fm == 0) && (k / c->fm < g.mmax);
+            (has_bc ? dep : map).push_back(sl);
+        }
+        c->nfree = (int)map.size();
+        map.insert(map.end(), dep.begin(), dep.end());
+        BPH_CUDA(cudaMalloc((void **)&c->d_slot_map, sizeof(int) * c->N));
+        c->bytes += sizeof(int) * c->N;
+        BPH_CUDA(cudaMemcpy(c->d_slot_map, map.data(), sizeof(int) * c->N, cudaMemcpyHostToDevice));
+        int least = 0, greatest = 0;
+        BPH_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        // the lowest priority: the contraction's CTAs take the SMs first and
+        // the free slots' ADI fills SMs as its waves drain (a high-priority
+        // side stream starved the contraction: 304 against 266 us per solve
+        // at 130x98x256; this order gives 258)
+        (void)greatest;
+        BPH_CUDA(cudaStreamCreateWithPriority(&c->side_stream, cudaStreamNonBlocking, least));
+        BPH_CUDA(cudaEventCreateWithFlags(&c->ev_fft, cudaEventDisableTiming));
+        BPH_CUDA(cudaEventCreateWithFlags(&c->ev_free, cudaEventDisableTiming));
+        const char *ov = std::getenv("BPH_OVERLAP");
+        c->overlap = !(ov && ov[0] == '0');
+    }
     BPH_CUDA(launch_qcoef(c));
     BPH_CUDA(launch_green_tables(c));
     if ((rc = fft_configure(c))) return rc;
@@ -367,13 +393,39 @@ int setup_impl(bph_ctx *c) {
     return BPH_OK;
 }
 
-// The five-kernel solve on device arrays (see the file comment).
+// Programmatic dependent launch off for the launches in its scope (kernels
+// that follow a cross-stream event wait, or that must not become resident
+// before another stream's kernel).
+struct PdlOff {
+    bph_ctx *c;
+    bool keep;
+    explicit PdlOff(bph_ctx *cc) : c(cc), keep(cc->pdl) { c->pdl = false; }
+    ~PdlOff() { c->pdl = keep; }
+};
+
+// The solve on device arrays (see the file comment).  Overlapped form: the
+// ADI of the slots without boundary data runs on the low-priority side
+// stream from the end of the forward FFT, taking SMs as the contraction
+// (HBM-bound, main stream) drains; the dependent slots follow the
+// contraction; the inverse FFT joins both.
 int solve_device(bph_ctx *c, const double *d_rho, double *d_pot, const Schedule &s, bool cold,
                  double *d_phieff = nullptr, double omega = 0.0) {
     BPH_CUDA(launch_fft_fwd_rho(c, d_rho));
-    BPH_CUDA(launch_green_contract(c));  // also writes the Dirichlet slots
-    BPH_CUDA(launch_adi(c, s, 0, s.nsteps, cold));
-    BPH_CUDA(launch_fft_inv(c, d_pot, d_phieff, omega));
+    if (c->overlap && c->adi_seg && c->nfree > 0 && c->nfree < c->N) {
+        BPH_CUDA(cudaEventRecord(c->ev_fft, c->stream));
+        BPH_CUDA(cudaStreamWaitEvent(c->side_stream, c->ev_fft, 0));
+        BPH_CUDA(launch_adi_slots(c, s, cold, c->d_slot_map, c->nfree, c->side_stream, false));
+        BPH_CUDA(cudaEventRecord(c->ev_free, c->side_stream));
+        BPH_CUDA(launch_green_contract(c));  // also writes the Dirichlet slots
+        BPH_CUDA(launch_adi_slots(c, s, cold, c->d_slot_map + c->nfree, c->N - c->nfree, c->stream, c->pdl));
+        BPH_CUDA(cudaStreamWaitEvent(c->stream, c->ev_free, 0));
+        PdlOff off(c);
+        BPH_CUDA(launch_fft_inv(c, d_pot, d_phieff, omega));
+    } else {
+        BPH_CUDA(launch_green_contract(c));  // also writes the Dirichlet slots
+        BPH_CUDA(launch_adi(c, s, 0, s.nsteps, cold));
+        BPH_CUDA(launch_fft_inv(c, d_pot, d_phieff, omega));
+    }
     c->have_warm = true;
     return BPH_OK;
 }
@@ -477,6 +529,13 @@ int bph_destroy(bph_ctx_t *c) {
     dev_free(c->d_status);
     dev_free(c->d_ccnt);
     dev_free(c->d_cpart);
+    if (c->side_stream) {
+        cudaStreamSynchronize(c->side_stream);
+        cudaStreamDestroy(c->side_stream);
+    }
+    if (c->ev_fft) cudaEventDestroy(c->ev_fft);
+    if (c->ev_free) cudaEventDestroy(c->ev_free);
+    if (c->d_slot_map) cudaFree(c->d_slot_map);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return BPH_OK;

@@ -121,6 +121,14 @@ struct bph_ctx {
     int fft_smem_fwd = 0, fft_smem_inv = 0;
     bool have_warm = false;
     bool pdl = true;             // launch solve kernels with programmatic dependent launch
+    // Overlapped solve: slots whose mode carries no boundary data (k not a
+    // boundary mode fm*m, m < mmax) run their ADI on a low-priority side
+    // stream from the end of the forward FFT, beside the contraction.
+    bool overlap = false;
+    int nfree = 0;                     // slots without boundary data
+    int *d_slot_map = nullptr;         // [N]: the nfree free slots, then the dependent ones
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t ev_fft = nullptr, ev_free = nullptr;
     long long launches = 0;
     size_t bytes = 0;
 };
@@ -173,6 +181,10 @@ cudaError_t launch_boundary_slots(bph_ctx *c);
 // (nullptr: instance i).
 cudaError_t launch_adi(bph_ctx *c, const Schedule &s, int step0, int nsteps_run, bool cold, double *P = nullptr,
                        const double *R = nullptr, int ninst = 1, const int *d_inst_map = nullptr);
+// The slots d_slots[0..nslots) of the context's own arrays, on stream st
+// (pdl: with programmatic dependent launch on that stream).
+cudaError_t launch_adi_slots(bph_ctx *c, const Schedule &s, bool cold, const int *d_slots, int nslots,
+                             cudaStream_t st, bool pdl);
 cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &s);
 cudaError_t launch_update_norm(bph_ctx *c, double *d_out);
 cudaError_t launch_residual_norm(bph_ctx *c, double *d_out);
