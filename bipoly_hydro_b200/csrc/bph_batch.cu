@@ -19,6 +19,7 @@
 #include <cublas_v2.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "bph_internal.cuh"
@@ -36,12 +37,128 @@ struct bph_batch {
     int *d_stat = nullptr;     // [cap] non-finite flag of each batch position (host-array calls)
     int *h_stat = nullptr;     // [cap] pinned host copy
     int stage_cap = 0;         // positions of the host-array staging buffers
+    double *d_cpart = nullptr;        // split-K partial sums of k_contract_batch
+    unsigned int *d_ccnt = nullptr;   // its arrival counters [mmax][row groups]
+    bool own_contract = true;         // k_contract_batch for up to kBatchOwnMax positions
     cublasHandle_t blas = nullptr;
     size_t bytes = 0;
 };
 
 namespace bph {
 namespace {
+
+// ---------------------------------------------------------------------------
+// k_contract_batch: C_m = G_m^T M_m for a small batch (NC = 2n columns,
+// n <= 4), the multi-right-hand-side form of k_green_contract.  The tables
+// are streamed once from HBM (16-byte evict-first loads); the moment
+// columns of the CTA's slice of zones are read by every warp of the CTA and
+// stay in L1.  Each warp owns kRowsPerWarp table rows, its lanes stride over
+// the zones; split-K slices write partial sums and the last CTA of each
+// (mode, row group) adds them in slice order (deterministic).  The library
+// GEMM stays for larger batches, where the contraction becomes FP64
+// compute-bound.
+constexpr int kBatchOwnMax = 4;        // batch positions handled by k_contract_batch
+constexpr int kBatchSplitMax = 16;
+constexpr int kBatchContractThreads = 256;
+
+template <int NC>
+struct BcShape {
+    static constexpr int kRowsPerWarp = (NC <= 4) ? 4 : 2;
+    static constexpr int kRows = (kBatchContractThreads / 32) * kRowsPerWarp;
+};
+
+template <int NC>
+__global__ void __launch_bounds__(kBatchContractThreads, 2)
+k_contract_batch(const double *__restrict__ G, const double *__restrict__ mom, long long mstride, long long np,
+                 int nb, double *__restrict__ C, long long cstride, unsigned int *__restrict__ counters,
+                 double *__restrict__ partials) {
+    constexpr int RW = BcShape<NC>::kRowsPerWarp, RC = BcShape<NC>::kRows;
+    const int m = blockIdx.y, split = blockIdx.z, nsplit = gridDim.z;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int bc = blockIdx.x * RC, bw = bc + warp * RW;
+    const int nrows = max(0, min(RW, nb - bw));
+    const long long nu = np / 2;
+    const long long chunk = (nu + nsplit - 1) / nsplit;
+    const long long u0 = split * chunk, u1 = min(nu, u0 + chunk);
+    const double2 *g2[RW];
+#pragma unroll
+    for (int r = 0; r < RW; ++r)
+        g2[r] = reinterpret_cast<const double2 *>(G + ((long long)m * nb + (r < nrows ? bw + r : bc)) * np);
+    const double2 *m2 = reinterpret_cast<const double2 *>(mom + m * mstride);
+    double acc[RW][NC];
+#pragma unroll
+    for (int r = 0; r < RW; ++r)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) acc[r][c] = 0.0;
+    pdl_wait();
+#pragma unroll 2
+    for (long long i = u0 + lane; i < u1; i += 32) {
+        double2 g[RW];
+#pragma unroll
+        for (int r = 0; r < RW; ++r) g[r] = (r < nrows) ? __ldcs(g2[r] + i) : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const double2 v = __ldg(m2 + c * nu + i);
+#pragma unroll
+            for (int r = 0; r < RW; ++r) {
+                acc[r][c] = fma(g[r].x, v.x, acc[r][c]);
+                acc[r][c] = fma(g[r].y, v.y, acc[r][c]);
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RW; ++r)
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) acc[r][c] += __shfl_down_sync(0xffffffffu, acc[r][c], off);
+    const int mmax = gridDim.y;
+    if (nsplit == 1) {
+        if (lane == 0)
+            for (int r = 0; r < nrows; ++r)
+#pragma unroll
+                for (int c = 0; c < NC; ++c) C[m * cstride + (long long)c * nb + bw + r] = acc[r][c];
+        return;
+    }
+    // partial sums [split][m][b][c]
+    const long long pstride = (long long)mmax * nb * NC;
+    if (lane == 0)
+        for (int r = 0; r < nrows; ++r)
+#pragma unroll
+            for (int c = 0; c < NC; ++c) partials[split * pstride + ((long long)m * nb + bw + r) * NC + c] = acc[r][c];
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    const int tile = m * gridDim.x + blockIdx.x;
+    if (threadIdx.x == 0) last = (atomicAdd(counters + tile, 1u) == (unsigned)(nsplit - 1));
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const int nrc = min(RC, nb - bc);
+    for (int t = threadIdx.x; t < nrc * NC; t += kBatchContractThreads) {
+        const int r = t / NC, c = t % NC;
+        double sum = 0.0;
+        for (int k = 0; k < nsplit; ++k) sum += __ldcg(partials + k * pstride + ((long long)m * nb + bc + r) * NC + c);
+        C[m * cstride + (long long)c * nb + bc + r] = sum;
+    }
+    if (threadIdx.x == 0) counters[tile] = 0u;
+}
+
+template <int NC>
+cudaError_t contract_batch_launch(bph_ctx *c, bph_batch *b, long long mstride) {
+    const int groups = (c->nb + BcShape<NC>::kRows - 1) / BcShape<NC>::kRows;
+    const long long base = (long long)groups * c->g.mmax;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    // enough CTAs for two waves at two per SM, slices of at least 1024 zone pairs
+    int nsplit = 1;
+    while (nsplit < kBatchSplitMax && base * nsplit < 4LL * sms && (c->np / 2) / (nsplit + 1) >= 1024) ++nsplit;
+    dim3 grid((unsigned)groups, (unsigned)c->g.mmax, (unsigned)nsplit);
+    ++c->launches;
+    k_contract_batch<NC><<<grid, kBatchContractThreads, 0, c->stream>>>(
+        c->d_green, b->d_mom, mstride, c->np, c->nb, b->d_C, 2LL * b->cap * c->nb, b->d_ccnt, b->d_cpart);
+    return cudaGetLastError();
+}
 
 // One thread per (instance, boundary row or corner, slot), as k_boundary_slots.
 __global__ void k_boundary_slots_batch(const double *__restrict__ C, const double2 *__restrict__ ph,
@@ -149,6 +266,25 @@ int bph_batch_create(bph_ctx_t *c, int capacity, bph_batch_t **out) {
     if (!rc) rc = batch_alloc(b, &b->d_R, (size_t)capacity * c->N * c->np);
     if (!rc) rc = batch_alloc(b, &b->d_mom, (size_t)c->g.mmax * capacity * 2 * c->np);
     if (!rc) rc = batch_alloc(b, &b->d_C, (size_t)c->g.mmax * 2 * capacity * c->nb);
+    if (!rc && (c->np % 2 == 0)) {
+        // split-K scratch of k_contract_batch: partial sums for the widest case
+        // (8 columns) and arrival counters for the narrowest row groups (16 rows)
+        rc = batch_alloc(b, &b->d_cpart, (size_t)kBatchSplitMax * c->g.mmax * c->nb * 8);
+        if (!rc) {
+            const size_t ncnt = (size_t)c->g.mmax * ((c->nb + 15) / 16);
+            e = cudaMalloc((void **)&b->d_ccnt, sizeof(unsigned int) * ncnt);
+            if (e == cudaSuccess) e = cudaMemsetAsync(b->d_ccnt, 0, sizeof(unsigned int) * ncnt, c->stream);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                set_error("batch counter allocation failed: %s", cudaGetErrorString(e));
+                rc = BPH_ERR_NOMEM;
+            }
+        }
+    }
+    if (!rc) {
+        const char *g = std::getenv("BPH_BATCH_GEMM");
+        b->own_contract = (c->np % 2 == 0) && !(g && g[0] == 'l');  // "library": always the library GEMM
+    }
     if (!rc) {
         e = cudaMalloc((void **)&b->d_map, sizeof(int) * capacity);
         if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_map, sizeof(int) * capacity);
@@ -183,9 +319,10 @@ int bph_batch_destroy(bph_batch_t *b) {
     if (b->c) cudaSetDevice(b->c->device);
     if (b->c && b->c->stream) cudaStreamSynchronize(b->c->stream);
     if (b->blas) cublasDestroy(b->blas);
-    double *bufs[] = {b->d_P, b->d_R, b->d_mom, b->d_C, b->d_rho_stage, b->d_pot_stage};
+    double *bufs[] = {b->d_P, b->d_R, b->d_mom, b->d_C, b->d_rho_stage, b->d_pot_stage, b->d_cpart};
     for (double *p : bufs)
         if (p) cudaFree(p);
+    if (b->d_ccnt) cudaFree(b->d_ccnt);
     if (b->d_map) cudaFree(b->d_map);
     if (b->h_map) cudaFreeHost(b->h_map);
     if (b->d_stat) cudaFree(b->d_stat);
@@ -290,7 +427,16 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
         BPH_CUDA(launch_fft_fwd_rho(c, d_rho[i], b->d_R + (size_t)inst[i] * c->N * np, b->d_mom + 2LL * i * np,
                                     mstride, per_pos ? b->d_stat + i : nullptr));
     // C_m = G_m^T M_m for every mode in one strided-batched DGEMM (batch positions)
-    {
+    if (b->own_contract && n <= kBatchOwnMax) {
+        cudaError_t ce = cudaSuccess;
+        switch (n) {
+            case 1: ce = contract_batch_launch<2>(c, b, mstride); break;
+            case 2: ce = contract_batch_launch<4>(c, b, mstride); break;
+            case 3: ce = contract_batch_launch<6>(c, b, mstride); break;
+            default: ce = contract_batch_launch<8>(c, b, mstride); break;
+        }
+        BPH_CUDA(ce);
+    } else {
         cublasStatus_t st = cublasSetStream(b->blas, c->stream);
         if (st != CUBLAS_STATUS_SUCCESS) return blas_fail(st, "cublasSetStream");
         const double one = 1.0, zero = 0.0;
