@@ -32,8 +32,13 @@ struct bph_batch {
     double *d_mom = nullptr;   // [mmax][cap][2][np]
     double *d_C = nullptr;     // [mmax][2cap][nb] column-major per mode
     double *d_rho_stage = nullptr, *d_pot_stage = nullptr;  // [cap][ntot] for host arrays
-    int *d_map = nullptr;      // [cap] instance of each batch position (device)
-    int *h_map = nullptr;      // [cap] pinned host copy
+    // Per-call position tables, double-buffered (call k uses set k % 2, and
+    // waits for the event of the call two before it): caller input and output
+    // array of each position, then the instance of each position.
+    void *d_tab[2] = {nullptr, nullptr};
+    void *h_tab[2] = {nullptr, nullptr};  // pinned
+    cudaEvent_t tab_ev[2] = {nullptr, nullptr};
+    int tab_k = 0;
     int *d_stat = nullptr;     // [cap] non-finite flag of each batch position (host-array calls)
     int *h_stat = nullptr;     // [cap] pinned host copy
     int stage_cap = 0;         // positions of the host-array staging buffers
@@ -286,8 +291,12 @@ int bph_batch_create(bph_ctx_t *c, int capacity, bph_batch_t **out) {
         b->own_contract = (c->np % 2 == 0) && !(g && g[0] == 'l');  // "library": always the library GEMM
     }
     if (!rc) {
-        e = cudaMalloc((void **)&b->d_map, sizeof(int) * capacity);
-        if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_map, sizeof(int) * capacity);
+        const size_t tab_bytes = (2 * sizeof(void *) + sizeof(int)) * (size_t)capacity;
+        for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+            e = cudaMalloc(&b->d_tab[k], tab_bytes);
+            if (e == cudaSuccess) e = cudaMallocHost(&b->h_tab[k], tab_bytes);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->tab_ev[k], cudaEventDisableTiming);
+        }
         if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_stat, sizeof(int) * capacity);
         if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_stat, sizeof(int) * capacity);
         if (e != cudaSuccess) {
@@ -323,8 +332,11 @@ int bph_batch_destroy(bph_batch_t *b) {
     for (double *p : bufs)
         if (p) cudaFree(p);
     if (b->d_ccnt) cudaFree(b->d_ccnt);
-    if (b->d_map) cudaFree(b->d_map);
-    if (b->h_map) cudaFreeHost(b->h_map);
+    for (int k = 0; k < 2; ++k) {
+        if (b->d_tab[k]) cudaFree(b->d_tab[k]);
+        if (b->h_tab[k]) cudaFreeHost(b->h_tab[k]);
+        if (b->tab_ev[k]) cudaEventDestroy(b->tab_ev[k]);
+    }
     if (b->d_stat) cudaFree(b->d_stat);
     if (b->h_stat) cudaFreeHost(b->h_stat);
     delete b;
@@ -378,14 +390,7 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
     const size_t bytes = sizeof(double) * (size_t)c->ntot;
     std::vector<int> inst(n);
     for (int i = 0; i < n; ++i) inst[i] = instances ? instances[i] : i;
-    const int *d_map = nullptr;
-    if (instances) {
-        // the previous call's map may still be read by its kernels
-        BPH_CUDA(cudaStreamSynchronize(c->stream));
-        for (int i = 0; i < n; ++i) b->h_map[i] = inst[i];
-        BPH_CUDA(cudaMemcpyAsync(b->d_map, b->h_map, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
-        d_map = b->d_map;
-    }
+
     std::vector<const double *> d_rho(n);
     std::vector<double *> d_pot(n);
     if (on_device) {
@@ -418,14 +423,32 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
             BPH_CUDA(cudaMemcpyAsync((void *)d_rho[i], rho[i], bytes, cudaMemcpyHostToDevice, c->stream));
         }
     }
+    // position tables of this call (set tab_k, free once the call two before has consumed it)
+    const int tk = b->tab_k;
+    b->tab_k ^= 1;
+    BPH_CUDA(cudaEventSynchronize(b->tab_ev[tk]));
+    char *hb = static_cast<char *>(b->h_tab[tk]);
+    const double **h_in = reinterpret_cast<const double **>(hb);
+    double **h_out = reinterpret_cast<double **>(hb + sizeof(void *) * b->cap);
+    int *h_inst = reinterpret_cast<int *>(hb + 2 * sizeof(void *) * b->cap);
+    for (int i = 0; i < n; ++i) {
+        h_in[i] = d_rho[i];
+        h_out[i] = d_pot[i];
+        h_inst[i] = inst[i];
+    }
+    BPH_CUDA(cudaMemcpyAsync(b->d_tab[tk], b->h_tab[tk], (2 * sizeof(void *) + sizeof(int)) * (size_t)b->cap,
+                             cudaMemcpyHostToDevice, c->stream));
+    char *db = static_cast<char *>(b->d_tab[tk]);
+    const double *const *d_in = reinterpret_cast<const double *const *>(db);
+    double *const *d_out = reinterpret_cast<double *const *>(db + sizeof(void *) * b->cap);
+    const int *d_map = instances ? reinterpret_cast<const int *>(db + 2 * sizeof(void *) * b->cap) : nullptr;
     // per-position non-finite flags: host-array calls and callers that want per-position status
     const bool per_pos = !on_device || pos_status;
     if (per_pos) BPH_CUDA(cudaMemsetAsync(b->d_stat, 0, sizeof(int) * n, c->stream));
     const long long np = c->np;
     const long long mstride = 2LL * b->cap * np;
-    for (int i = 0; i < n; ++i)
-        BPH_CUDA(launch_fft_fwd_rho(c, d_rho[i], b->d_R + (size_t)inst[i] * c->N * np, b->d_mom + 2LL * i * np,
-                                    mstride, per_pos ? b->d_stat + i : nullptr));
+    BPH_CUDA(launch_fft_fwd_rho_batch(c, n, d_in, d_map, b->d_R, (long long)c->N * np, b->d_mom, mstride, 2LL * np,
+                                      per_pos ? b->d_stat : c->d_status, per_pos));
     // C_m = G_m^T M_m for every mode in one strided-batched DGEMM (batch positions)
     if (b->own_contract && n <= kBatchOwnMax) {
         cudaError_t ce = cudaSuccess;
@@ -455,8 +478,8 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
         BPH_CUDA(cudaGetLastError());
     }
     BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, !warm, b->d_P, b->d_R, n, d_map));
-    for (int i = 0; i < n; ++i)
-        BPH_CUDA(launch_fft_inv(c, d_pot[i], nullptr, 0.0, b->d_P + (size_t)inst[i] * c->N * c->nplane));
+    BPH_CUDA(launch_fft_inv_batch(c, n, d_out, d_map, b->d_P, (long long)c->N * c->nplane));
+    BPH_CUDA(cudaEventRecord(b->tab_ev[tk], c->stream));
     if (per_pos) {
         if (!on_device)
             for (int i = 0; i < n; ++i)

@@ -93,6 +93,19 @@ __device__ __forceinline__ void fft_tile(double2 *C, const double2 *tw) {
     }
 }
 
+// Batched launches: blockIdx.y is the batch position.  in / outp hold each
+// position's caller array (forward: rho; inverse: pot), inst its instance
+// (nullptr: position = instance); instance i's slot data sits at
+// i * inst_stride from the given base, position j's moments at
+// j * pos_stride, its non-finite flag at status[j].
+struct FftBatch {
+    const double *const *in = nullptr;
+    double *const *outp = nullptr;
+    const int *inst = nullptr;
+    long long inst_stride = 0, pos_stride = 0;
+    int status_stride = 0;  // 1: a flag per position, 0: one shared flag
+};
+
 template <int M>
 struct FftShape {
     static constexpr int kThreads = (M >= 256) ? 256 : 128;
@@ -113,7 +126,7 @@ __global__ void __launch_bounds__(FftShape<M>::kThreads, FftShape<M>::kMinBlocks
 k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__restrict__ mom,
           const double2 *__restrict__ g_tw, const double2 *__restrict__ g_tw2, const double2 *__restrict__ g_ph,
           int numr, int numz, int nr, int nz, int mmax, int fm, int isym, double four_pi,
-          int *__restrict__ status, long long mstride) {
+          int *__restrict__ status, long long mstride, FftBatch bt) {
     constexpr int NT = FftShape<M>::kThreads;
     extern __shared__ double2 smem[];
     double2 *C = smem;
@@ -126,6 +139,15 @@ k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__re
     for (int i = tid; i < M; i += NT) tw[i] = g_tw[i];
     for (int i = tid; i <= M; i += NT) tw2[i] = g_tw2[i];
     pdl_wait();
+    if (bt.in) {
+        const int pos = blockIdx.y;
+        src = bt.in[pos];
+        out += (long long)(bt.inst ? bt.inst[pos] : pos) * bt.inst_stride;
+        if (kRho) {
+            mom += pos * bt.pos_stride;
+            status += pos * bt.status_stride;
+        }
+    }
     // Load: thread -> (column c fixed, sample pairs n = n0, n0 + NT/kTile, ...);
     // all global loads are issued before any shared-memory store.
     static_assert(NT % kTile == 0, "threads must cover whole tile rows");
@@ -250,7 +272,7 @@ template <int M>
 __global__ void __launch_bounds__(FftShape<M>::kThreads, FftShape<M>::kMinBlocksInv)
 k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 *__restrict__ g_tw,
           const double2 *__restrict__ g_tw2, int numr, int numz, int isym, double *__restrict__ phieff,
-          const double *__restrict__ rhf, double omega) {
+          const double *__restrict__ rhf, double omega, FftBatch bt) {
     constexpr int NT = FftShape<M>::kThreads;
     extern __shared__ double2 smem[];
     double2 *C = smem;
@@ -262,6 +284,11 @@ k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 
     for (int i = tid; i < M; i += NT) tw[i] = g_tw[i];
     for (int i = tid; i <= M; i += NT) tw2[i] = g_tw2[i];
     pdl_wait();
+    if (bt.outp) {
+        const int pos = blockIdx.y;
+        P += (long long)(bt.inst ? bt.inst[pos] : pos) * bt.inst_stride;
+        pot = bt.outp[pos];
+    }
     // Load slots: thread -> (column c fixed, slot pairs (k, M+k)); all global
     // loads are issued before any shared-memory store.
     constexpr int kRowsPerPass = NT / kTile, kLoads = M / kRowsPerPass;
@@ -367,13 +394,15 @@ cudaError_t set_fft_attrs(bph_ctx *c) {
 }
 
 template <int M>
-cudaError_t fwd_rho(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride, int *status) {
+cudaError_t fwd_rho(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride, int *status,
+                    FftBatch bt, int npos) {
     unsigned blocks = (unsigned)((c->np + kTile - 1) / kTile);
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = launch_config(c, dim3(blocks), dim3(FftShape<M>::kThreads), FftShape<M>::kSmem, attr);
+    cudaLaunchConfig_t cfg =
+        launch_config(c, dim3(blocks, (unsigned)npos), dim3(FftShape<M>::kThreads), FftShape<M>::kSmem, attr);
     return cudaLaunchKernelEx(&cfg, k_fft_fwd<M, true>, rho, R, mom, (const double2 *)c->d_tw,
                               (const double2 *)c->d_tw2, (const double2 *)c->d_ph, c->g.numr, c->g.numz, c->nr,
-                              c->nz, c->g.mmax, c->fm, c->g.isym, c->four_pi, status, mstride);
+                              c->nz, c->g.mmax, c->fm, c->g.isym, c->four_pi, status, mstride, bt);
 }
 
 template <int M>
@@ -381,17 +410,18 @@ cudaError_t fwd_pot(bph_ctx *c, const double *pot) {
     unsigned blocks = (unsigned)((c->np + kTile - 1) / kTile);
     k_fft_fwd<M, false><<<blocks, FftShape<M>::kThreads, FftShape<M>::kSmem, c->stream>>>(
         pot, c->d_P, nullptr, c->d_tw, c->d_tw2, c->d_ph, c->g.numr, c->g.numz, c->nr, c->nz, c->g.mmax, c->fm,
-        c->g.isym, c->four_pi, c->d_status, 0);
+        c->g.isym, c->four_pi, c->d_status, 0, FftBatch());
     return cudaGetLastError();
 }
 
 template <int M>
-cudaError_t inv(bph_ctx *c, double *pot, double *phieff, double omega, const double *P) {
+cudaError_t inv(bph_ctx *c, double *pot, double *phieff, double omega, const double *P, FftBatch bt, int npos) {
     unsigned blocks = (unsigned)((c->nplane + kTile - 1) / kTile);
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = launch_config(c, dim3(blocks), dim3(FftShape<M>::kThreads), FftShape<M>::kSmem, attr);
+    cudaLaunchConfig_t cfg =
+        launch_config(c, dim3(blocks, (unsigned)npos), dim3(FftShape<M>::kThreads), FftShape<M>::kSmem, attr);
     return cudaLaunchKernelEx(&cfg, k_fft_inv<M>, P, pot, (const double2 *)c->d_tw, (const double2 *)c->d_tw2,
-                              c->g.numr, c->g.numz, c->g.isym, phieff, (const double *)c->d_grid, omega);
+                              c->g.numr, c->g.numz, c->g.isym, phieff, (const double *)c->d_grid, omega, bt);
 }
 
 #define BPH_FFT_DISPATCH(FN, ...)                  \
@@ -406,12 +436,14 @@ cudaError_t inv(bph_ctx *c, double *pot, double *phieff, double omega, const dou
     }
 
 cudaError_t set_attrs_dispatch(bph_ctx *c) { BPH_FFT_DISPATCH(set_fft_attrs, c) }
-cudaError_t fwd_rho_dispatch(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride, int *status) {
-    BPH_FFT_DISPATCH(fwd_rho, c, rho, R, mom, mstride, status)
+cudaError_t fwd_rho_dispatch(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride, int *status,
+                             FftBatch bt, int npos) {
+    BPH_FFT_DISPATCH(fwd_rho, c, rho, R, mom, mstride, status, bt, npos)
 }
 cudaError_t fwd_pot_dispatch(bph_ctx *c, const double *pot) { BPH_FFT_DISPATCH(fwd_pot, c, pot) }
-cudaError_t inv_dispatch(bph_ctx *c, double *pot, double *phieff, double omega, const double *P) {
-    BPH_FFT_DISPATCH(inv, c, pot, phieff, omega, P)
+cudaError_t inv_dispatch(bph_ctx *c, double *pot, double *phieff, double omega, const double *P, FftBatch bt,
+                         int npos) {
+    BPH_FFT_DISPATCH(inv, c, pot, phieff, omega, P, bt, npos)
 }
 
 }  // namespace
@@ -426,7 +458,7 @@ cudaError_t launch_fft_fwd_rho(bph_ctx *c, const double *rho, double *R, double 
                                int *status) {
     ++c->launches;
     return fwd_rho_dispatch(c, rho, R ? R : c->d_R, mom ? mom : c->d_mom, mstride ? mstride : 2 * c->np,
-                            status ? status : c->d_status);
+                            status ? status : c->d_status, FftBatch(), 1);
 }
 
 cudaError_t launch_fft_fwd_pot(bph_ctx *c, const double *pot) {
@@ -436,7 +468,30 @@ cudaError_t launch_fft_fwd_pot(bph_ctx *c, const double *pot) {
 
 cudaError_t launch_fft_inv(bph_ctx *c, double *pot, double *phieff, double omega, const double *P) {
     ++c->launches;
-    return inv_dispatch(c, pot, phieff, omega, P ? P : c->d_P);
+    return inv_dispatch(c, pot, phieff, omega, P ? P : c->d_P, FftBatch(), 1);
+}
+
+cudaError_t launch_fft_fwd_rho_batch(bph_ctx *c, int npos, const double *const *d_in, const int *d_inst, double *R,
+                                     long long inst_stride, double *mom, long long mstride, long long pos_stride,
+                                     int *status, bool status_per_pos) {
+    FftBatch bt;
+    bt.in = d_in;
+    bt.status_stride = status_per_pos ? 1 : 0;
+    bt.inst = d_inst;
+    bt.inst_stride = inst_stride;
+    bt.pos_stride = pos_stride;
+    ++c->launches;
+    return fwd_rho_dispatch(c, nullptr, R, mom, mstride, status, bt, npos);
+}
+
+cudaError_t launch_fft_inv_batch(bph_ctx *c, int npos, double *const *d_out, const int *d_inst, const double *P,
+                                 long long inst_stride) {
+    FftBatch bt;
+    bt.outp = d_out;
+    bt.inst = d_inst;
+    bt.inst_stride = inst_stride;
+    ++c->launches;
+    return inv_dispatch(c, nullptr, nullptr, 0.0, P, bt, npos);
 }
 
 }  // namespace bph

@@ -171,6 +171,16 @@ cudaError_t launch_adi_factors(bph_ctx *c, Schedule &s);
 cudaError_t launch_fft_fwd_rho(bph_ctx *c, const double *rho, double *R = nullptr, double *mom = nullptr,
                                long long mstride = 0, int *status = nullptr);
 cudaError_t launch_fft_fwd_pot(bph_ctx *c, const double *pot);
+// One launch over npos batch positions: position j reads d_in[j] (device
+// table) and writes instance d_inst[j]'s R (at inst * inst_stride from R),
+// its moments at mom + j * pos_stride and its non-finite flag at status[j]
+// (status_per_pos) or at *status.
+cudaError_t launch_fft_fwd_rho_batch(bph_ctx *c, int npos, const double *const *d_in, const int *d_inst, double *R,
+                                     long long inst_stride, double *mom, long long mstride, long long pos_stride,
+                                     int *status, bool status_per_pos);
+// One launch over npos positions: instance d_inst[j]'s slots -> d_out[j].
+cudaError_t launch_fft_inv_batch(bph_ctx *c, int npos, double *const *d_out, const int *d_inst, const double *P,
+                                 long long inst_stride);
 cudaError_t launch_fft_inv(bph_ctx *c, double *pot, double *phieff = nullptr, double omega = 0.0,
                            const double *P = nullptr);
 // write_slots: the contraction also writes the Dirichlet slots of P (the
