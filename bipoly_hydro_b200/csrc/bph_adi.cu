@@ -20,6 +20,7 @@
 // stride is odd (in doubles) so that line-parallel accesses along r are
 // bank-conflict free.
 #include <cstdint>
+#include <cstdlib>
 
 #include "bph_internal.cuh"
 
@@ -44,6 +45,10 @@ struct AdiArgs {
     const int *inst_map;    // batches: instance of each block row (nullptr: block row = instance)
     const int *slot_map;    // slot of each block within a row (nullptr: block = slot)
     int nslots;             // blocks per row (N without slot_map)
+    const void *rad_pk;     // packed radial factor blocks of the kernel's type [nsteps][N][pkr]
+    const void *ver_pk;     // packed vertical factor blocks [nsteps][pkz]
+    int pkr, pkz;           // their sizes in elements
+    int *status;            // deferred status word (bounded waits that expire)
     int numr, numz, nr, nz, N, isym;
     int step0, nsteps_run, cold;
     double gamma;
@@ -285,6 +290,95 @@ __device__ inline void fac_load(T *base, int n, const double *src, int tid, int 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Factor prefetch by bulk copy.  The segmented kernels read one factor block
+// per direction and step; with prefetch they hold two blocks per direction
+// in shared memory and fill the idle one with a bulk (TMA) copy of the next
+// step's packed block while the current half-steps run, completion tracked
+// by an mbarrier per block (one elected thread issues, every thread waits
+// before its first read).  Waits are bounded: an expired wait sets
+// kStatusTimeout and the kernel runs on (its results are then reported
+// invalid), so no CTA can hang on a copy.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// One thread: order this CTA's earlier generic-proxy accesses of dst before
+// the async-proxy write, then copy bytes (multiple of 16, both addresses
+// 16-byte aligned) from global src to shared dst, completing on bar.
+__device__ __forceinline__ void bulk_fill(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+constexpr int kWaitSpins = 1 << 20;  // try_wait rounds (each suspends at most a short hardware interval)
+
+__device__ __forceinline__ void mbar_wait(uint64_t *bar, uint32_t parity, int *status) {
+    for (int i = 0; i < kWaitSpins; ++i)
+        if (mbar_try_wait(bar, parity)) return;
+    atomicOr(status, kStatusTimeout);
+}
+
+// Shared-memory layout of the prefetching segmented kernel, byte offsets.
+struct PfLayout {
+    int ps, Pr, Pz, xsz, fpf;  // fpf: elements per factor block (both directions)
+    size_t o_rw, o_f, o_xa, o_xb, o_eb, o_el0, o_ab, o_zrow, o_mbar, bytes;
+};
+
+__host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+template <typename T>
+__host__ __device__ inline PfLayout pf_layout(int nr, int nz, bool with_zrow) {
+    PfLayout L;
+    L.ps = nr | 1;
+    L.Pr = (nr + kAdiSeg - 1) / kAdiSeg;
+    L.Pz = (nz + kAdiSeg - 1) / kAdiSeg;
+    L.xsz = max(nz * L.Pr, nr * L.Pz);
+    L.fpf = max(packed_block<T>(nr), packed_block<T>(nz));
+    const size_t e = sizeof(T);
+    size_t o = (size_t)nz * L.ps * e;
+    L.o_rw = o;
+    o = align_up(o + (size_t)nz * L.ps * e, 16);
+    L.o_f = o;  // Fr[0], Fr[1], Fz[0], Fz[1]
+    o += 4 * (size_t)L.fpf * e;
+    L.o_xa = o;  // the segment-edge values of phase C reuse it (dead after phase B)
+    o += (size_t)L.xsz * e;
+    L.o_xb = o;
+    o += (size_t)L.xsz * e;
+    L.o_eb = o;
+    o += (size_t)L.xsz * e;
+    L.o_el0 = o;
+    o = align_up(o + (size_t)nr * e, 2 * e);
+    L.o_ab = o;
+    o += 2 * (size_t)nr * e;
+    L.o_zrow = o;
+    if (with_zrow) o += (size_t)nr * e;
+    L.o_mbar = align_up(o, 8);
+    L.bytes = L.o_mbar + 4 * sizeof(uint64_t);
+    return L;
+}
+
 // The ADI of one Fourier slot per CTA, all steps on chip.
 //
 // kDefect = false (FP64 drop-in, T = double): nsteps Peaceman-Rachford steps
@@ -321,7 +415,7 @@ __device__ inline void fac_load(T *base, int n, const double *src, int tid, int 
 //      step) from the registers and the published edges, written to Ww.
 // The per-element arithmetic is the Thomas algorithm of tridagr/tridagz; the
 // segment carries only re-associate it (results agree to rounding).
-template <typename T, int kSegThreads, bool kFull, bool kDefect>
+template <typename T, int kSegThreads, bool kFull, bool kDefect, bool kPf>
 __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArgs a) {
     using T2 = typename Vec2<T>::type;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -336,17 +430,41 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
     const SegLayout Lo = seg_layout(nr, nz);
     const int ps = Lo.ps, Pr = Lo.Pr, Pz = Lo.Pz;
     T *Ww = sm;
-    T *Rw = Ww + (size_t)nz * ps;
-    T *Fr = Rw + (size_t)nz * ps;
-    T *Fz = Fr + Lo.fsz;
-    T *Xa = Fz + Lo.fsz;
-    T *Xb = Xa + Lo.xsz;
-    T *Ea = Xb + Lo.xsz;
-    T *Eb = Ea + Lo.xsz;
-    T *el0 = Eb + Lo.xsz;
-    T *abp = align_pair(el0 + nr);
+    T *Rw, *Fr0, *Fr1, *Fz0, *Fz1, *Xa, *Xb, *Ea, *Eb, *el0, *abp, *zrow;
+    uint64_t *mbar = nullptr;  // [4]: Fr[0], Fr[1], Fz[0], Fz[1]
+    if (kPf) {
+        const PfLayout P = pf_layout<T>(nr, nz, !kDefect);
+        Rw = reinterpret_cast<T *>(smraw + P.o_rw);
+        T *F = reinterpret_cast<T *>(smraw + P.o_f);
+        Fr0 = F;
+        Fr1 = F + P.fpf;
+        Fz0 = F + 2 * P.fpf;
+        Fz1 = F + 3 * P.fpf;
+        Xa = reinterpret_cast<T *>(smraw + P.o_xa);
+        Ea = Xa;
+        Xb = reinterpret_cast<T *>(smraw + P.o_xb);
+        Eb = reinterpret_cast<T *>(smraw + P.o_eb);
+        el0 = reinterpret_cast<T *>(smraw + P.o_el0);
+        abp = reinterpret_cast<T *>(smraw + P.o_ab);
+        zrow = kDefect ? nullptr : reinterpret_cast<T *>(smraw + P.o_zrow);
+        mbar = reinterpret_cast<uint64_t *>(smraw + P.o_mbar);
+    } else {
+        Rw = Ww + (size_t)nz * ps;
+        Fr0 = Fr1 = Rw + (size_t)nz * ps;
+        Fz0 = Fz1 = Fr0 + Lo.fsz;
+        Xa = Fz0 + Lo.fsz;
+        Xb = Xa + Lo.xsz;
+        Ea = Xb + Lo.xsz;
+        Eb = Ea + Lo.xsz;
+        el0 = Eb + Lo.xsz;
+        abp = align_pair(el0 + nr);
+        zrow = abp + 2 * nr;
+    }
+    T *Fr = Fr0, *Fz = Fz0;
+    // factor block of relative step j (the only block without prefetch)
+    auto frb = [&](int j) -> T * { return kPf ? ((j & 1) ? Fr1 : Fr0) : Fr0; };
+    auto fzb = [&](int j) -> T * { return kPf ? ((j & 1) ? Fz1 : Fz0) : Fz0; };
     T2 *AB = reinterpret_cast<T2 *>(abp);
-    T *zrow = abp + 2 * nr;
     const long long nplane = (long long)numr * numz;
     double *Pg = a.P + blk * nplane;
     const double *Rs = a.R + blk * nr * nz;
@@ -358,13 +476,45 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
     const long long rad_step = (long long)a.N * kAdiFactors * nr;
     const long long ver_step = (long long)kAdiFactors * nz;
 
+    const T *rad_pk = reinterpret_cast<const T *>(a.rad_pk) + (size_t)s * a.pkr;
+    const size_t rad_pk_step = (size_t)a.N * a.pkr;
+    const T *ver_pk = reinterpret_cast<const T *>(a.ver_pk);
+    // relative step j of a direction goes to block j % 2; its fill count there is j / 2
+    auto fill_r = [&](int j) {
+        bulk_fill(frb(j), rad_pk + (size_t)(a.step0 + j) * rad_pk_step, (uint32_t)(a.pkr * sizeof(T)),
+                  mbar + (j & 1));
+    };
+    auto fill_z = [&](int j) {
+        bulk_fill(fzb(j), ver_pk + (size_t)(a.step0 + j) * a.pkz, (uint32_t)(a.pkz * sizeof(T)),
+                  mbar + 2 + (j & 1));
+    };
+    auto wait_r = [&](int j) { mbar_wait(mbar + (j & 1), (uint32_t)((j >> 1) & 1), a.status); };
+    auto wait_z = [&](int j) { mbar_wait(mbar + 2 + (j & 1), (uint32_t)((j >> 1) & 1), a.status); };
+
+    if (kPf) {
+        if (tid == 0) {
+            for (int i = 0; i < 4; ++i) mbar_init(mbar + i, 1);
+            fence_mbar_init();
+        }
+        __syncthreads();
+        if (tid == 0) {  // set-up data: no dependence on the previous kernel
+            fill_r(0);
+            fill_z(0);
+            if (a.nsteps_run > 1) {
+                fill_r(1);
+                fill_z(1);
+            }
+        }
+    }
     for (int j = tid; j < nr; j += kSegThreads) {
         AB[j] = Vec2<T>::make((T)a.alphar[j + 1], (T)a.betar[j + 1]);
         el0[j] = (T)a.elz[(long long)s * numr + j + 1];
-        zrow[j] = (T)0;
+        if (zrow) zrow[j] = (T)0;
     }
-    fac_load(Fr, nr, rad + a.step0 * rad_step, tid, kSegThreads);
-    fac_load(Fz, nz, a.ver + a.step0 * ver_step, tid, kSegThreads);
+    if (!kPf) {
+        fac_load(Fr, nr, rad + a.step0 * rad_step, tid, kSegThreads);
+        fac_load(Fz, nz, a.ver + a.step0 * ver_step, tid, kSegThreads);
+    }
     pdl_wait();  // P and R come from the previous kernels of the solve
     if (!kDefect) {
         // Rw (source + folded Dirichlet terms) and the initial potential: 8 rows per
@@ -415,6 +565,7 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
         // the stencil.  delta starts at zero, so the first radial right-hand
         // side is r itself (times 1/bet).
         __syncthreads();  // Fr is read below
+        if (kPf) wait_r(0);
         const Fac<T> f = fac_view(Fr, nr);
         const double *brb = a.brb + (long long)s * numr;
         for (int k = warp; k < nz; k += nwarps) {
@@ -451,10 +602,32 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
         const T dtn = last_half ? dtt : (T)a.dt[a.step0 + it_next];
         // reload this direction's factors when its next half-step is at another step
         const bool reload = kDefect ? (h > 0 && it + 1 < a.nsteps_run) : (it + 1 < a.nsteps_run);
+        if (kPf) {
+            const int n = a.nsteps_run;
+            if (tid == 0) {
+                // refill the block whose step was used for the last time by the half-step before
+                if (!kDefect) {
+                    if (radial_half && it >= 1 && it + 1 < n) fill_z(it + 1);
+                    if (!radial_half && it + 2 < n) fill_r(it + 2);
+                } else {
+                    if (!radial_half && it >= 1 && it + 1 < n) fill_r(it + 1);
+                    if (radial_half && h >= 2 && it + 2 < n) fill_z(it + 2);
+                }
+            }
+            // the blocks this half-step reads: its own direction, and the
+            // other direction's 1/bet for the next right-hand side
+            if (radial_half) {
+                wait_r(it);
+                if (!last_half) wait_z(it_next);
+            } else {
+                wait_z(it);
+                if (!last_half) wait_r(it_next);
+            }
+        }
 
         // ================= radial half-sweep: lines k, segments along j =================
         if (radial_half) {
-            const Fac<T> f = fac_view(Fr, nr);
+            const Fac<T> f = fac_view(frb(it), nr);
             T v[kAdiSeg];
             const bool active = tid < nitem_r;
             const int k = active ? tid % nz : 0, p = active ? tid / nz : 0;
@@ -521,7 +694,7 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
             } else if (active) {
                 // vertical right-hand side of the next half-step (helmadi.F90:276-340),
                 // times the vertical 1/bet of row k
-                const T ibz = fac_view(Fz, nz).ib[k];
+                const T ibz = fac_view(fzb(it_next), nz).ib[k];
                 const T left = (p > 0) ? Eb[k + nz * (p - 1)] : (T)0;
                 const T right = (p + 1 < Pr) ? Ea[k + nz * (p + 1)] : (T)0;
 #pragma unroll
@@ -534,7 +707,7 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
                         wr[i] = (rr[i] + (el0[j] + dtn) * v[i] - ab.x * pr - ab.y * pl) * ibz;
                     }
             }
-            if (reload) {
+            if (!kPf && reload) {
                 __syncthreads();
                 fac_load(Fr, nr, rad + (step + 1) * rad_step, tid, kSegThreads);
             }
@@ -542,7 +715,7 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
         }
         // ================= vertical half-sweep: lines j, segments along k =================
         else {
-            const Fac<T> f = fac_view(Fz, nz);
+            const Fac<T> f = fac_view(fzb(it), nz);
             T v[kAdiSeg];
             const bool active = tid < nitem_z;
             const int j = active ? tid % nr : 0, p = active ? tid / nr : 0;
@@ -594,7 +767,7 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
                 } else {
                     // radial right-hand side of the next half-step (helmadi.F90:209-256),
                     // times its radial 1/bet of column j
-                    const T ibr = fac_view(Fr, nr).ib[j];
+                    const T ibr = fac_view(frb(it_next), nr).ib[j];
                     const T dn_edge = (p > 0) ? Eb[j + nr * (p - 1)] : (T)0;
                     const T up_edge = (p + 1 < Pz) ? Ea[j + nr * (p + 1)] : (T)0;
 #pragma unroll
@@ -611,7 +784,7 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
                         }
                 }
             }
-            if (it + 1 < a.nsteps_run) {
+            if (!kPf && it + 1 < a.nsteps_run) {
                 __syncthreads();
                 fac_load(Fz, nz, a.ver + (step + 1) * ver_step, tid, kSegThreads);
             }
@@ -984,13 +1157,21 @@ k_slot_norms(const double *__restrict__ P, const double *__restrict__ Q, const d
 
 }  // namespace
 
-template <typename T, bool kDefect>
-const void *seg_kernel(int threads, bool full) {
+template <typename T, bool kDefect, bool kPf>
+const void *seg_kernel_pf(int threads, bool full) {
     if (threads == 256)
-        return full ? (const void *)k_adi_seg<T, 256, true, kDefect> : (const void *)k_adi_seg<T, 256, false, kDefect>;
+        return full ? (const void *)k_adi_seg<T, 256, true, kDefect, kPf>
+                    : (const void *)k_adi_seg<T, 256, false, kDefect, kPf>;
     if (threads == 384)
-        return full ? (const void *)k_adi_seg<T, 384, true, kDefect> : (const void *)k_adi_seg<T, 384, false, kDefect>;
-    return full ? (const void *)k_adi_seg<T, 512, true, kDefect> : (const void *)k_adi_seg<T, 512, false, kDefect>;
+        return full ? (const void *)k_adi_seg<T, 384, true, kDefect, kPf>
+                    : (const void *)k_adi_seg<T, 384, false, kDefect, kPf>;
+    return full ? (const void *)k_adi_seg<T, 512, true, kDefect, kPf>
+                : (const void *)k_adi_seg<T, 512, false, kDefect, kPf>;
+}
+
+template <typename T, bool kDefect>
+const void *seg_kernel(int threads, bool full, bool pf) {
+    return pf ? seg_kernel_pf<T, kDefect, true>(threads, full) : seg_kernel_pf<T, kDefect, false>(threads, full);
 }
 
 const void *delta_kernel(int threads, bool full) {
@@ -1009,14 +1190,26 @@ int adi_configure(bph_ctx *c) {
     const size_t onchip = sizeof(double) * 2 * (size_t)c->nz * (size_t)(c->nr | 1) + smalls_bytes(c);
     const int items = max(c->nz * L.Pr, c->nr * L.Pz);
     const int threads = (items <= 256) ? 256 : (items <= 384) ? 384 : 512;
+    // Factor prefetch by bulk copy: on by default for the FP32 refinement
+    // kernel (74.8 against 85.3 us per 5-step cycle at 130x98x256 on B200),
+    // off for the FP64 drop-in, where it measured slower (101 against 95 us):
+    // the FP64 kernel's in-place reload costs ~5 us and the extra waits more.
+    // BPH_ADI_PREFETCH=0 turns it off everywhere, =1 on everywhere.
+    const char *pfenv = std::getenv("BPH_ADI_PREFETCH");
+    const bool pf_allowed = !(pfenv && pfenv[0] == '0');
+    const bool pf_fp64 = pfenv && pfenv[0] == '1';
     c->adi_seg = 0;
     c->adi_smem = 0;
     c->adi_mixed_smem = 0;
+    c->adi_pf = false;
+    c->mixed_pf = false;
     c->adi_full = (c->nr % kAdiSeg == 0) && (c->nz % kAdiSeg == 0);
-    if (seg_bytes <= (size_t)dev_max && items <= 512) {
+    const size_t seg_pf_bytes = pf_layout<double>(c->nr, c->nz, true).bytes;
+    if (items <= 512 && (seg_bytes <= (size_t)dev_max || (pf_fp64 && seg_pf_bytes <= (size_t)dev_max))) {
         c->adi_seg = threads;
-        c->adi_smem = (int)seg_bytes;
-        e = cudaFuncSetAttribute(seg_kernel<double, false>(c->adi_seg, c->adi_full),
+        c->adi_pf = pf_fp64 && seg_pf_bytes <= (size_t)dev_max;
+        c->adi_smem = (int)(c->adi_pf ? seg_pf_bytes : seg_bytes);
+        e = cudaFuncSetAttribute(seg_kernel<double, false>(c->adi_seg, c->adi_full, c->adi_pf),
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, c->adi_smem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_adi_seg)");
     } else if (onchip <= (size_t)dev_max) {
@@ -1030,12 +1223,32 @@ int adi_configure(bph_ctx *c) {
     const size_t delta_bytes = sizeof(float) * DL.elems + 16;
     c->adi_mixed_threads = 0;
     c->mixed_kind = 0;
+    // forwarding form: the prefetching variant when it keeps the resident CTAs per SM
+    if (pf_allowed && items <= 512) {
+        const size_t pf_bytes = pf_layout<float>(c->nr, c->nz, false).bytes;
+        if (pf_bytes <= (size_t)dev_max && mixed_bytes <= (size_t)dev_max) {
+            int occ_pf = 0, occ = 0;
+            const void *fpf = seg_kernel<float, true>(threads, c->adi_full, true);
+            const void *fno = seg_kernel<float, true>(threads, c->adi_full, false);
+            e = cudaFuncSetAttribute(fpf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pf_bytes);
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(fpf, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(fno, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mixed_bytes);
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(fno, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_pf, fpf, threads, (int)pf_bytes);
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fno, threads, (int)mixed_bytes);
+            if (e != cudaSuccess) return cuda_fail(e, "refinement ADI occupancy");
+            c->mixed_pf = occ_pf >= occ && occ_pf > 0;
+        } else if (pf_bytes <= (size_t)dev_max) {
+            c->mixed_pf = true;
+        }
+    }
+    const size_t fwd_bytes = c->mixed_pf ? pf_layout<float>(c->nr, c->nz, false).bytes : mixed_bytes;
     for (int kind = 1; kind <= 2; ++kind) {
         c->mixed_smem_kind[kind] = 0;
         c->mixed_per_sm_kind[kind] = 0;
-        const size_t bytes = (kind == BPH_MIXED_ADI_FORWARD) ? mixed_bytes : delta_bytes;
+        const size_t bytes = (kind == BPH_MIXED_ADI_FORWARD) ? fwd_bytes : delta_bytes;
         if (bytes > (size_t)dev_max || items > 512) continue;
-        const void *fn = (kind == BPH_MIXED_ADI_FORWARD) ? seg_kernel<float, true>(threads, c->adi_full)
+        const void *fn = (kind == BPH_MIXED_ADI_FORWARD) ? seg_kernel<float, true>(threads, c->adi_full, c->mixed_pf)
                                                          : delta_kernel(threads, c->adi_full);
         e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
@@ -1078,6 +1291,11 @@ AdiArgs make_args(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bo
     a.inst_map = nullptr;
     a.slot_map = nullptr;
     a.nslots = c->N;
+    a.rad_pk = sch.d_rad_pk[0];
+    a.ver_pk = sch.d_ver_pk[0];
+    a.pkr = packed_block<double>(c->nr);
+    a.pkz = packed_block<double>(c->nz);
+    a.status = c->d_status;
     a.numr = c->g.numr;
     a.numz = c->g.numz;
     a.nr = c->nr;
@@ -1102,7 +1320,7 @@ cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_ru
         void *args[] = {&a};
         cudaLaunchAttribute attr[1];
         cudaLaunchConfig_t cfg = launch_config(c, dim3(c->N * ninst), dim3(c->adi_seg), (size_t)c->adi_smem, attr);
-        return cudaLaunchKernelExC(&cfg, seg_kernel<double, false>(c->adi_seg, c->adi_full), args);
+        return cudaLaunchKernelExC(&cfg, seg_kernel<double, false>(c->adi_seg, c->adi_full, c->adi_pf), args);
     }
     // other variants: one launch per instance (batches need the on-chip kernel)
     if (d_inst_map) return cudaErrorNotSupported;
@@ -1133,16 +1351,20 @@ cudaError_t launch_adi_slots(bph_ctx *c, const Schedule &sch, bool cold, const i
     cudaLaunchConfig_t cfg = launch_config(c, dim3(nslots), dim3(c->adi_seg), (size_t)c->adi_smem, attr);
     cfg.stream = st;
     if (!pdl) cfg.numAttrs = 0;
-    return cudaLaunchKernelExC(&cfg, seg_kernel<double, false>(c->adi_seg, c->adi_full), args);
+    return cudaLaunchKernelExC(&cfg, seg_kernel<double, false>(c->adi_seg, c->adi_full, c->adi_pf), args);
 }
 
 cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {
     if (!c->adi_mixed_smem) return cudaErrorNotSupported;
     AdiArgs a = make_args(c, sch, 0, sch.nsteps, false);
+    a.rad_pk = sch.d_rad_pk[1];  // float blocks for the FP32 kernels
+    a.ver_pk = sch.d_ver_pk[1];
+    a.pkr = packed_block<float>(c->nr);
+    a.pkz = packed_block<float>(c->nz);
     ++c->launches;
     void *args[] = {&a};
     const void *fn = (c->mixed_kind == BPH_MIXED_ADI_FORWARD)
-                         ? seg_kernel<float, true>(c->adi_mixed_threads, c->adi_full)
+                         ? seg_kernel<float, true>(c->adi_mixed_threads, c->adi_full, c->mixed_pf)
                          : delta_kernel(c->adi_mixed_threads, c->adi_full);
     return cudaLaunchKernel(fn, dim3(c->N), dim3(c->adi_mixed_threads), args, (size_t)c->adi_mixed_smem,
                             c->stream);

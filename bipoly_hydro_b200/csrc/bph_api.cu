@@ -143,6 +143,10 @@ void free_schedule(bph_ctx *c, Schedule &s) {
     dev_free(s.d_dt);
     dev_free(s.d_rad);
     dev_free(s.d_ver);
+    for (int k = 0; k < 2; ++k) {
+        dev_free(s.d_rad_pk[k]);
+        dev_free(s.d_ver_pk[k]);
+    }
     free(s.h_dt);
     s = Schedule();
     (void)c;
@@ -168,6 +172,19 @@ int get_schedule(bph_ctx *c, int nsteps, Schedule **out) {
     BPH_CUDA(cudaMemcpyAsync(s.d_dt, s.h_dt, sizeof(double) * nsteps, cudaMemcpyHostToDevice, c->stream));
     s.nsteps = nsteps;
     BPH_CUDA(launch_adi_factors(c, s));
+    {
+        double *r64, *v64;
+        float *r32, *v32;
+        if ((rc = dev_alloc(c, &r64, (size_t)nsteps * c->N * packed_block<double>(c->nr)))) return rc;
+        s.d_rad_pk[0] = r64;
+        if ((rc = dev_alloc(c, &v64, (size_t)nsteps * packed_block<double>(c->nz)))) return rc;
+        s.d_ver_pk[0] = v64;
+        if ((rc = dev_alloc(c, &r32, (size_t)nsteps * c->N * packed_block<float>(c->nr)))) return rc;
+        s.d_rad_pk[1] = r32;
+        if ((rc = dev_alloc(c, &v32, (size_t)nsteps * packed_block<float>(c->nz)))) return rc;
+        s.d_ver_pk[1] = v32;
+    }
+    BPH_CUDA(launch_pack_factors(c, s));
     BPH_CUDA(cudaStreamSynchronize(c->stream));
     *out = &s;
     return BPH_OK;
@@ -445,6 +462,10 @@ int read_status(bph_ctx *c) {
     if (st & kStatusNonFinite) {
         set_error("density contains NaN or Inf");
         return BPH_ERR_NONFINITE;
+    }
+    if (st & kStatusTimeout) {
+        set_error("a bounded device wait expired (ADI factor bulk copy); results are not valid");
+        return BPH_ERR_TIMEOUT;
     }
     return BPH_OK;
 }
@@ -843,6 +864,7 @@ long long bph_info(const bph_ctx_t *c, int what) {
         case BPH_INFO_MIXED_KIND: return c->mixed_kind;
         case BPH_INFO_MIXED_FORWARD_NS: return (long long)(1e3f * c->mixed_tuned_us[BPH_MIXED_ADI_FORWARD]);
         case BPH_INFO_MIXED_INCREMENT_NS: return (long long)(1e3f * c->mixed_tuned_us[BPH_MIXED_ADI_INCREMENT]);
+        case BPH_INFO_ADI_PREFETCH: return (c->adi_pf ? 1 : 0) | (c->mixed_pf ? 2 : 0);
         default: return -1;
     }
 }

@@ -33,6 +33,7 @@ constexpr int kNumSchedules = 3;       // 5 steps (warm), 20 steps (cold), one c
 
 // Deferred device status bits (d_status).
 constexpr int kStatusNonFinite = 1;
+constexpr int kStatusTimeout = 2;  // a bounded device wait (bulk-copy barrier) expired
 
 // Segment length of the partitioned line solves in the on-chip ADI kernel.
 constexpr int kAdiSeg = 32;
@@ -55,12 +56,26 @@ constexpr int kAdiFactors = 5;
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// Packed factor block of one line system of length n in type T, the
+// shared-memory layout the segmented ADI kernels read: [1/bet n][a/bet n]
+// [(G_j, gam_{j+1}) pairs 2n][K n], padded to 16 bytes so that one bulk copy
+// moves it.
+template <typename T>
+__host__ __device__ inline int packed_block(int n) {
+    const int al = 16 / (int)sizeof(T);
+    return ((5 * n + al - 1) / al) * al;
+}
+
 struct Schedule {
     int nsteps = 0;
     double *d_dt = nullptr;   // [nsteps]
     double *d_rad = nullptr;  // [nsteps][N][kAdiFactors][nr] radial Thomas factors
     double *d_ver = nullptr;  // [nsteps][kAdiFactors][nz]    vertical Thomas factors
     double *h_dt = nullptr;   // host copy of the dt schedule
+    // packed blocks ([0]: double, [1]: float): radial [nsteps][N][packed_block(nr)],
+    // vertical [nsteps][packed_block(nz)]
+    void *d_rad_pk[2] = {nullptr, nullptr};
+    void *d_ver_pk[2] = {nullptr, nullptr};
 };
 
 }  // namespace bph
@@ -110,6 +125,8 @@ struct bph_ctx {
     int adi_smem = 0;            // dynamic shared bytes of the on-chip ADI kernel (0: global variant)
     int adi_seg = 0;             // threads of the segmented on-chip ADI kernel (0: not used)
     bool adi_full = false;       // both line lengths are multiples of the segment length
+    bool adi_pf = false;         // FP64 segmented ADI with bulk-copy factor prefetch
+    bool mixed_pf = false;       // the same for the FP32 forwarding-form refinement kernel
     int adi_mixed_threads = 0;   // threads of the FP32 defect-correction ADI kernels
     int adi_mixed_smem = 0;      // dynamic shared bytes of the one in use (0: mixed form unavailable)
     int adi_mixed_per_sm = 0;    // its resident CTAs per SM
@@ -166,6 +183,8 @@ inline cudaLaunchConfig_t launch_config(const bph_ctx *c, dim3 grid, dim3 block,
 cudaError_t launch_qcoef(bph_ctx *c);
 cudaError_t launch_green_tables(bph_ctx *c);
 cudaError_t launch_adi_factors(bph_ctx *c, Schedule &s);
+// Packed double and float factor blocks of a schedule (after launch_adi_factors).
+cudaError_t launch_pack_factors(bph_ctx *c, Schedule &s);
 // Optional arguments select batch buffers (R, moments with m-stride, P, instance count).
 // status: where a non-finite density is flagged (nullptr: the context's status word).
 cudaError_t launch_fft_fwd_rho(bph_ctx *c, const double *rho, double *R = nullptr, double *mom = nullptr,

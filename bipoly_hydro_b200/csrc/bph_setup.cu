@@ -304,6 +304,40 @@ cudaError_t launch_green_tables(bph_ctx *c) {
     return cudaGetLastError();
 }
 
+// One thread per (step, line system): the [ib, dd, gam, G, K] arrays of
+// k_adi_factors rearranged into packed_block<T> layout (pairs (G_j, gam_{j+1})).
+template <typename T>
+__global__ void k_pack_factors(const double *__restrict__ rad, const double *__restrict__ ver,
+                               T *__restrict__ rad_pk, T *__restrict__ ver_pk, int nsteps, int N, int nr, int nz) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nrad = (long long)nsteps * N;
+    if (t >= nrad + nsteps) return;
+    const bool radial = t < nrad;
+    const int n = radial ? nr : nz;
+    const double *src = radial ? rad + t * kAdiFactors * nr : ver + (t - nrad) * kAdiFactors * nz;
+    const int pb = packed_block<T>(n);
+    T *dst = radial ? rad_pk + t * pb : ver_pk + (t - nrad) * pb;
+    for (int j = 0; j < n; ++j) {
+        dst[j] = (T)src[j];
+        dst[n + j] = (T)src[n + j];
+        dst[2 * n + 2 * j] = (T)src[3 * n + j];
+        dst[2 * n + 2 * j + 1] = (T)((j + 1 < n) ? src[2 * n + j + 1] : 0.0);
+        dst[4 * n + j] = (T)src[4 * n + j];
+    }
+    for (int j = 5 * n; j < pb; ++j) dst[j] = (T)0;
+}
+
+cudaError_t launch_pack_factors(bph_ctx *c, Schedule &s) {
+    const long long n = (long long)s.nsteps * c->N + s.nsteps;
+    const unsigned blocks = (unsigned)((n + 127) / 128);
+    k_pack_factors<double><<<blocks, 128, 0, c->stream>>>(s.d_rad, s.d_ver, (double *)s.d_rad_pk[0],
+                                                          (double *)s.d_ver_pk[0], s.nsteps, c->N, c->nr, c->nz);
+    k_pack_factors<float><<<blocks, 128, 0, c->stream>>>(s.d_rad, s.d_ver, (float *)s.d_rad_pk[1],
+                                                         (float *)s.d_ver_pk[1], s.nsteps, c->N, c->nr, c->nz);
+    c->launches += 2;
+    return cudaGetLastError();
+}
+
 cudaError_t launch_adi_factors(bph_ctx *c, Schedule &s) {
     int n = s.nsteps * c->N + s.nsteps;
     k_adi_factors<<<(n + 127) / 128, 128, 0, c->stream>>>(s.d_dt, s.nsteps, c->d_brb, c->d_alphar, c->d_betar,

@@ -336,7 +336,7 @@ class PotentialSolver:
     def info(self) -> dict:
         """Launch-configuration facts (bph_info)."""
         names = ("adi_threads", "adi_smem", "mixed_threads", "mixed_smem", "mixed_ctas_per_sm", "contract_split",
-                 "mixed_kind", "mixed_forward_ns", "mixed_increment_ns")
+                 "mixed_kind", "mixed_forward_ns", "mixed_increment_ns", "adi_prefetch")
         return {n: int(self._lib.bph_info(self._h, i)) for i, n in enumerate(names)}
 
     def set_mixed_adi(self, kind: int) -> None:

@@ -251,6 +251,7 @@ int bph_green_contract_noalloc(bph_ctx_t *ctx, const double *d_mom, double *d_S)
 #define BPH_INFO_MIXED_KIND 6         /* refinement ADI kernel in use (BPH_MIXED_ADI_*) */
 #define BPH_INFO_MIXED_FORWARD_NS 7   /* setup-time duration of a 5-step forwarding-form launch, ns (0: not timed) */
 #define BPH_INFO_MIXED_INCREMENT_NS 8 /* the same for the increment form */
+#define BPH_INFO_ADI_PREFETCH 9       /* bulk-copy factor prefetch: bit 0 FP64 ADI, bit 1 FP32 refinement ADI */
 long long bph_info(const bph_ctx_t *ctx, int what);
 
 /* Tuning knobs (no counterpart in the reference).
