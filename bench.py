@@ -465,7 +465,7 @@ def run_gpu(args, world, rank, local):
 
     # ---- serving: Poisson arrivals of SCF-like client requests ----------
     serving = None
-    if args.serve_rates:
+    if args.serve_rates and not args.no_serving:
         serving = serve_bench(B, torch, dev, rhos, args)
 
     # ---- converged solves: FP64 vs mixed (FP32 ADI + FP64 refinement) --
@@ -567,6 +567,7 @@ def main():
     ap.add_argument("--serve-rates", default="200,1000,4000",
                     help="offered request rates (req/s) of the serving section (empty skips)")
     ap.add_argument("--serve-clients", type=int, default=64)
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
     ap.add_argument("--serve-iters", type=int, default=8, help="SCF-like requests per client per rate")
     ap.add_argument("--converged-steps", type=int, default=20,
                     help="warm converged solves timed per form (FP64 and mixed); 0 skips")
