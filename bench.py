@@ -375,6 +375,33 @@ def run_gpu(args, world, rank, local):
     value = job_rate(args.steps, world, ms_total)
     clocks = clk.summary()
 
+    # ---- the same warm solve captured once into a CUDA graph and replayed -
+    graph_replay = None
+    if not args.no_graph:
+        gbuf = rhos[1].clone()
+        gpot = torch.empty_like(d_pot)
+        cap = torch.cuda.Stream()
+        graph = torch.cuda.CUDAGraph()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(graph, stream=cap):
+            solver.set_stream(torch.cuda.current_stream())
+            solver.potential_solver_device(gbuf, gpot, tstep)
+        solver.set_stream(stream)
+        for _ in range(5):
+            graph.replay()
+        ga, gb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        nrep = max(50, args.steps // 2)
+        torch.cuda.synchronize()
+        ga.record(stream)
+        for _ in range(nrep):
+            graph.replay()
+        gb.record(stream)
+        torch.cuda.synchronize()
+        gms = ga.elapsed_time(gb) / nrep
+        graph_replay = {"solves_per_s": 1e3 / gms, "ms_per_solve": gms, "replays": nrep}
+        del graph
+        solver.synchronize()
+
     # ---- per-phase kernel times (CUDA events on the launch stream) ------
     def time_phase(phase, reps, **kw):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -544,6 +571,7 @@ def run_gpu(args, world, rank, local):
             "converged": conv,
             "batched": batched,
             "serving": serving,
+            "graph_replay": graph_replay,
             "launch_config": solver_info,
             "gpu_launches": launches,
             "clocks": clocks,
@@ -568,6 +596,7 @@ def main():
                     help="offered request rates (req/s) of the serving section (empty skips)")
     ap.add_argument("--serve-clients", type=int, default=64)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
+    ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay section")
     ap.add_argument("--serve-iters", type=int, default=8, help="SCF-like requests per client per rate")
     ap.add_argument("--converged-steps", type=int, default=20,
                     help="warm converged solves timed per form (FP64 and mixed); 0 skips")
