@@ -171,6 +171,8 @@ int get_schedule(bph_ctx *c, int nsteps, Schedule **out) {
     if ((rc = dev_alloc(c, &s.d_ver, (size_t)nsteps * kAdiFactors * c->nz))) return rc;
     BPH_CUDA(cudaMemcpyAsync(s.d_dt, s.h_dt, sizeof(double) * nsteps, cudaMemcpyHostToDevice, c->stream));
     s.nsteps = nsteps;
+    static long long next_build_id = 1;
+    s.build_id = next_build_id++;
     BPH_CUDA(launch_adi_factors(c, s));
     {
         double *r64, *v64;
@@ -382,6 +384,8 @@ int setup_impl(bph_ctx *c) {
         BPH_CUDA(cudaStreamCreateWithPriority(&c->side_stream, cudaStreamNonBlocking, least));
         BPH_CUDA(cudaEventCreateWithFlags(&c->ev_fft, cudaEventDisableTiming));
         BPH_CUDA(cudaEventCreateWithFlags(&c->ev_free, cudaEventDisableTiming));
+        const char *cg = std::getenv("BPH_CONV_GRAPH");
+        c->conv_graph = !(cg && cg[0] == '0');
         const char *ov = std::getenv("BPH_OVERLAP");
         c->overlap = !(ov && ov[0] == '0');
     }
@@ -550,6 +554,7 @@ int bph_destroy(bph_ctx_t *c) {
     dev_free(c->d_status);
     dev_free(c->d_ccnt);
     dev_free(c->d_cpart);
+    conv_graphs_free(c);
     if (c->side_stream) {
         cudaStreamSynchronize(c->side_stream);
         cudaStreamDestroy(c->side_stream);
@@ -618,79 +623,42 @@ int bph_solve_nsteps(bph_ctx_t *c, const double *rho, double *pot, int nsteps, i
     return solve_host(c, rho, pot, *s, cold != 0);
 }
 
-int bph_solve_converged(bph_ctx_t *c, const double *rho, double *pot, int nsteps, int cold, double tol,
-                        int max_cycles, int on_device, int *cycles_out, double *resid_out) {
-    int rc;
-    if ((rc = check_ctx(c))) return rc;
-    if (!rho || !pot || nsteps < 1 || nsteps > 10000 || max_cycles < 1 || !(tol >= 0.0)) {
-        set_error("invalid arguments");
-        return BPH_ERR_INVALID;
+}  // extern "C"
+
+namespace bph {
+
+// Sum of the per-slot (num, den) pairs a norm kernel left in c->d_red.
+static double host_ratio(const std::vector<double> &h, int N) {
+    double num = 0.0, den = 0.0;
+    for (int i = 0; i < N; ++i) {
+        num += h[2 * i];
+        den += h[2 * i + 1];
     }
-    if ((rc = set_device_of(c))) return rc;
-    Schedule *s;
-    if ((rc = get_schedule(c, nsteps, &s))) return rc;
-    if (!c->d_prev && (rc = dev_alloc(c, &c->d_prev, (size_t)c->N * c->nplane))) return rc;
-    const size_t bytes = sizeof(double) * (size_t)c->ntot;
-    const double *d_rho = rho;
-    double *d_pot = pot;
-    if (!on_device) {
-        if ((rc = ensure_staging(c))) return rc;
-        BPH_CUDA(cudaMemcpyAsync(c->d_rho_stage, rho, bytes, cudaMemcpyHostToDevice, c->stream));
-        d_rho = c->d_rho_stage;
-        d_pot = c->d_pot_stage;
-    }
-    BPH_CUDA(launch_fft_fwd_rho(c, d_rho));
-    BPH_CUDA(launch_green_contract(c));  // also writes the Dirichlet slots
-    std::vector<double> h(2 * (size_t)c->N);
-    int cyc = 0;
-    for (;;) {
-        BPH_CUDA(cudaMemcpyAsync(c->d_prev, c->d_P, bytes, cudaMemcpyDeviceToDevice, c->stream));
-        BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, cold != 0 && cyc == 0));
-        ++cyc;
-        BPH_CUDA(launch_update_norm(c, c->d_red));
-        BPH_CUDA(cudaMemcpyAsync(h.data(), c->d_red, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
-        BPH_CUDA(cudaStreamSynchronize(c->stream));
-        double num = 0.0, den = 0.0;
-        for (int i = 0; i < c->N; ++i) {
-            num += h[2 * i];
-            den += h[2 * i + 1];
-        }
-        double upd = den > 0.0 ? std::sqrt(num / den) : std::sqrt(num);
-        if (upd <= tol || cyc >= max_cycles) break;
-    }
-    if (resid_out) {
-        BPH_CUDA(launch_residual_norm(c, c->d_red));
-        BPH_CUDA(cudaMemcpyAsync(h.data(), c->d_red, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
-        BPH_CUDA(cudaStreamSynchronize(c->stream));
-        double num = 0.0, den = 0.0;
-        for (int i = 0; i < c->N; ++i) {
-            num += h[2 * i];
-            den += h[2 * i + 1];
-        }
-        *resid_out = den > 0.0 ? std::sqrt(num / den) : std::sqrt(num);
-    }
-    if (cycles_out) *cycles_out = cyc;
-    BPH_CUDA(launch_fft_inv(c, d_pot));
-    c->have_warm = true;
-    if (!on_device) BPH_CUDA(cudaMemcpyAsync(pot, d_pot, bytes, cudaMemcpyDeviceToHost, c->stream));
-    return read_status(c);
+    return den > 0.0 ? std::sqrt(num / den) : std::sqrt(num);
 }
 
-int bph_solve_converged_mixed(bph_ctx_t *c, const double *rho, double *pot, int nsteps, int cold, double tol,
-                              int max_cycles, int on_device, int *cycles_out, double *resid_out) {
+// Converged FP64 (mixed = false) or mixed-precision solve.  A cold start
+// zeroes the slot array before the contraction writes the Dirichlet slots,
+// as the reference's cold start zeroes potp.  The cycle loop runs on the
+// device as a graph while node (bph_converge.cu) unless BPH_CONV_GRAPH=0 or
+// the graph cannot be built, then on the host with one synchronisation per
+// cycle; both apply the same stopping rule.
+static int converged_impl(bph_ctx *c, const double *rho, double *pot, int nsteps, int cold, double tol, int max_cycles,
+                          int on_device, int *cycles_out, double *resid_out, bool mixed) {
     int rc;
     if ((rc = check_ctx(c))) return rc;
     if (!rho || !pot || nsteps < 1 || nsteps > 10000 || max_cycles < 1 || !(tol >= 0.0)) {
         set_error("invalid arguments");
         return BPH_ERR_INVALID;
     }
-    if (!c->adi_mixed_smem) {
+    if (mixed && !c->adi_mixed_smem) {
         set_error("the mixed-precision ADI does not fit on chip for this grid");
         return BPH_ERR_INVALID;
     }
     if ((rc = set_device_of(c))) return rc;
     Schedule *s;
     if ((rc = get_schedule(c, nsteps, &s))) return rc;
+    if (!mixed && !c->d_prev && (rc = dev_alloc(c, &c->d_prev, (size_t)c->N * c->nplane))) return rc;
     const size_t bytes = sizeof(double) * (size_t)c->ntot;
     const double *d_rho = rho;
     double *d_pot = pot;
@@ -705,44 +673,65 @@ int bph_solve_converged_mixed(bph_ctx_t *c, const double *rho, double *pot, int 
     BPH_CUDA(launch_green_contract(c));  // also writes the Dirichlet slots
     std::vector<double> h(2 * (size_t)c->N);
     int cyc = 0;
-    double prev_upd = INFINITY;
-    for (;;) {
-        BPH_CUDA(launch_adi_defect(c, *s));
-        ++cyc;
-        BPH_CUDA(cudaMemcpyAsync(h.data(), c->d_red, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
-        BPH_CUDA(cudaStreamSynchronize(c->stream));
-        double num = 0.0, den = 0.0;
-        for (int i = 0; i < c->N; ++i) {
-            num += h[2 * i];
-            den += h[2 * i + 1];
+    double upd = 0.0;
+    bool device_loop = c->conv_graph && conv_loop_device(c, *s, mixed, tol, max_cycles) == BPH_OK;
+    if (!device_loop) {
+        c->conv_graph = false;  // graphs unavailable: host loop from now on
+        double prev_upd = INFINITY;
+        for (;;) {
+            if (mixed) {
+                BPH_CUDA(launch_adi_defect(c, *s));
+            } else {
+                BPH_CUDA(cudaMemcpyAsync(c->d_prev, c->d_P, bytes, cudaMemcpyDeviceToDevice, c->stream));
+                BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, false));
+                BPH_CUDA(launch_update_norm(c, c->d_red));
+            }
+            ++cyc;
+            BPH_CUDA(cudaMemcpyAsync(h.data(), c->d_red, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
+                                     c->stream));
+            BPH_CUDA(cudaStreamSynchronize(c->stream));
+            upd = host_ratio(h, c->N);
+            bool stop = upd <= tol || cyc >= max_cycles;
+            if (mixed) stop = stop || !(upd == upd) || upd > 0.5 * prev_upd;
+            if (stop) break;
+            prev_upd = upd;
         }
-        double upd = den > 0.0 ? std::sqrt(num / den) : std::sqrt(num);
-        if (!(upd == upd)) {
-            set_error("mixed-precision refinement diverged");
-            return BPH_ERR_NONFINITE;
-        }
-        // Stop at the tolerance, or once a cycle no longer halves the update:
-        // the FP32 inner solves have then reached their accuracy, and more
-        // cycles only add FP32 rounding to stiff near-axis components.
-        if (upd <= tol || cyc >= max_cycles || upd > 0.5 * prev_upd) break;
-        prev_upd = upd;
     }
-    if (resid_out) {
-        BPH_CUDA(launch_residual_norm(c, c->d_red));
-        BPH_CUDA(cudaMemcpyAsync(h.data(), c->d_red, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
-        BPH_CUDA(cudaStreamSynchronize(c->stream));
-        double num = 0.0, den = 0.0;
-        for (int i = 0; i < c->N; ++i) {
-            num += h[2 * i];
-            den += h[2 * i + 1];
-        }
-        *resid_out = den > 0.0 ? std::sqrt(num / den) : std::sqrt(num);
-    }
-    if (cycles_out) *cycles_out = cyc;
+    if (resid_out) BPH_CUDA(launch_residual_norm(c, c->d_red));
     BPH_CUDA(launch_fft_inv(c, d_pot));
     c->have_warm = true;
     if (!on_device) BPH_CUDA(cudaMemcpyAsync(pot, d_pot, bytes, cudaMemcpyDeviceToHost, c->stream));
-    return read_status(c);
+    ConvState st = {};
+    if (device_loop)
+        BPH_CUDA(cudaMemcpyAsync(&st, c->d_conv, sizeof(ConvState), cudaMemcpyDeviceToHost, c->stream));
+    if (resid_out)
+        BPH_CUDA(cudaMemcpyAsync(h.data(), c->d_red, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = read_status(c))) return rc;  // synchronises
+    if (device_loop) {
+        cyc = st.cycles;
+        upd = st.upd;
+    }
+    if (mixed && !(upd == upd)) {
+        set_error("mixed-precision refinement diverged");
+        return BPH_ERR_NONFINITE;
+    }
+    if (resid_out) *resid_out = host_ratio(h, c->N);
+    if (cycles_out) *cycles_out = cyc;
+    return BPH_OK;
+}
+
+}  // namespace bph
+
+extern "C" {
+
+int bph_solve_converged(bph_ctx_t *c, const double *rho, double *pot, int nsteps, int cold, double tol,
+                        int max_cycles, int on_device, int *cycles_out, double *resid_out) {
+    return converged_impl(c, rho, pot, nsteps, cold, tol, max_cycles, on_device, cycles_out, resid_out, false);
+}
+
+int bph_solve_converged_mixed(bph_ctx_t *c, const double *rho, double *pot, int nsteps, int cold, double tol,
+                              int max_cycles, int on_device, int *cycles_out, double *resid_out) {
+    return converged_impl(c, rho, pot, nsteps, cold, tol, max_cycles, on_device, cycles_out, resid_out, true);
 }
 
 int bph_potential_solver_phieff(bph_ctx_t *c, const double *rho, double *pot, double *phieff, double omega_frame,

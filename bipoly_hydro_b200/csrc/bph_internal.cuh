@@ -76,6 +76,20 @@ struct Schedule {
     // vertical [nsteps][packed_block(nz)]
     void *d_rad_pk[2] = {nullptr, nullptr};
     void *d_ver_pk[2] = {nullptr, nullptr};
+    long long build_id = 0;  // distinct for every schedule built (graphs that captured it)
+};
+
+// Converged-loop state on the device (bph_converge.cu).
+struct ConvState {
+    double tol, prev, upd;
+    int max_cycles, cycles, mixed;
+};
+
+// Instantiated while-graph of a converged form and what it captured.
+struct ConvGraph {
+    cudaGraphExec_t exec = nullptr;
+    long long build_id = -1;
+    int kind = -1;
 };
 
 }  // namespace bph
@@ -141,6 +155,9 @@ struct bph_ctx {
     // Overlapped solve: slots whose mode carries no boundary data (k not a
     // boundary mode fm*m, m < mmax) run their ADI on a low-priority side
     // stream from the end of the forward FFT, beside the contraction.
+    bph::ConvState *d_conv = nullptr;  // converged-loop state
+    bph::ConvGraph conv[2];            // [0] FP64, [1] mixed converged loop graphs
+    bool conv_graph = true;            // run converged loops as device-side while graphs
     bool overlap = false;
     int nfree = 0;                     // slots without boundary data
     int *d_slot_map = nullptr;         // [N]: the nfree free slots, then the dependent ones
@@ -219,6 +236,11 @@ cudaError_t launch_update_norm(bph_ctx *c, double *d_out);
 cudaError_t launch_residual_norm(bph_ctx *c, double *d_out);
 
 int adi_configure(bph_ctx *c);
+// Converged-solve cycle loop as a CUDA graph while node (bph_converge.cu):
+// enqueues the loop on c->stream; the state (cycles, last update) is in
+// c->d_conv.  conv_graphs_free releases the graphs and the state.
+int conv_loop_device(bph_ctx *c, Schedule &s, bool mixed, double tol, int max_cycles);
+void conv_graphs_free(bph_ctx *c);
 // Batched solve of batch positions 0..n-1 (bph_batch.cu); instances may be
 // nullptr (position i = instance i).  With pos_status (per-position
 // BPH_OK / BPH_ERR_NONFINITE) or host arrays the call is synchronous.

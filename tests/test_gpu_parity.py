@@ -358,3 +358,26 @@ def test_factor_prefetch_variants_match_oracle(oracle_mod, bph, monkeypatch, pre
     pmx, imx = g.solve_converged_mixed(rho, 10, True, 1e-13, 100)
     assert rel_l2(pmx, p64) <= 1e-9, (rel_l2(pmx, p64), imx.cycles)
     g.close()
+
+
+def test_converged_loop_on_device_equals_host_loop(bph, monkeypatch):
+    """The converged solves' cycle loop as a CUDA graph while node (the
+    default) and as a host loop give the same potentials and cycle counts."""
+    grid = (34, 26, 64, 1.0 / 30.0, 2, 30)
+    numr, numz, numphi, dr, isym, _ = grid
+    rho = smooth_density(numr, numz, numphi, dr, isym)
+    rho2 = np.asfortranarray(np.roll(rho, 3, axis=2))
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("BPH_CONV_GRAPH", flag)
+        g = bph.PotentialSolver(*grid)
+        p1, i1 = g.solve_converged(rho, 10, True, 1e-12, 100)
+        p2, i2 = g.solve_converged(rho2, 10, False, 1e-12, 100)
+        m1, j1 = g.solve_converged_mixed(rho2, 10, False, 1e-12, 100)
+        out[flag] = (p1, i1, p2, i2, m1, j1)
+        g.close()
+    a, b = out["1"], out["0"]
+    for k in (0, 2, 4):
+        assert np.array_equal(a[k], b[k]), k
+        assert a[k + 1].cycles == b[k + 1].cycles, k
+        assert abs(a[k + 1].residual - b[k + 1].residual) <= 1e-12 * max(1.0, b[k + 1].residual)
