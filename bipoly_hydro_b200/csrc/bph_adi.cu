@@ -200,6 +200,154 @@ __global__ void __launch_bounds__(kAdiThreads) k_adi(AdiArgs a) {
 size_t smalls_bytes(const bph_ctx *c) { return sizeof(double) * (size_t)(9 * c->nr + 4 * c->nz); }
 
 // ---------------------------------------------------------------------------
+// FP32 refinement cycle for slots too large for shared memory (k_adi_gdefect).
+//
+// One CTA per slot; its defect r, increment delta and a right-hand-side
+// buffer live in a global work area (T, interior-packed [k][j]).  Prologue:
+// the FP64 residual r = -4 pi rho_hat - A phi of the current potential;
+// body: the defect equation A delta = r in helmadi's right-hand-side form
+// from delta = 0 with zero Dirichlet data, half-steps radial at the first
+// step's dt, then (vertical, radial) per step -- the order the on-chip FP32
+// kernels use, which keeps rounding of stiff near-axis components out of the
+// refinement; epilogue: phi += delta in FP64 and the per-slot norms.  Line
+// solves are the Thomas recurrences of tridagr/tridagz, one thread per line.
+template <typename T>
+__global__ void __launch_bounds__(kAdiThreads) k_adi_gdefect(AdiArgs a, T *__restrict__ work) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int s = blockIdx.x, tid = threadIdx.x;
+    const int nr = a.nr, nz = a.nz, numr = a.numr;
+    const long long np = (long long)nr * nz;
+    const long long nplane = (long long)numr * a.numz;
+    double *Pg = a.P + (long long)s * nplane;
+    const double *Rs = a.R + (long long)s * np;
+    T *rr = work + (long long)s * 3 * np, *dl = rr + np, *ww = dl + np;
+    T *rf = reinterpret_cast<T *>(smraw);  // [3][nr] radial ib, dd, gam of the current step
+    T *vf = rf + 3 * nr;                    // [3][nz] vertical
+    T *cb = vf + 3 * nz;                    // [nr] brb, [nr] alphar, [nr] betar of the slot
+    T *ca = cb + nr, *cbe = ca + nr;
+    const double gamma = a.gamma;
+    const T g = (T)gamma;
+    const bool sym_bottom = (a.isym != 1);
+    const double *brb = a.brb + (long long)s * numr;
+    for (int j = tid; j < nr; j += kAdiThreads) {
+        cb[j] = (T)brb[j + 1];
+        ca[j] = (T)a.alphar[j + 1];
+        cbe[j] = (T)a.betar[j + 1];
+    }
+    pdl_wait();
+    // FP64 residual; delta = 0
+    for (long long e = tid; e < np; e += kAdiThreads) {
+        const int j = (int)(e % nr), k = (int)(e / nr);
+        const double *pc = Pg + (long long)numr * (k + 1) + 1;
+        const double c = pc[j], east = pc[j + 1], n = pc[j + numr];
+        const double w = (j > 0) ? pc[j - 1] : 0.0;
+        const double so = (k > 0 || !sym_bottom) ? pc[j - numr] : 0.0;
+        const double ar = brb[j + 1] * c + a.alphar[j + 1] * east + a.betar[j + 1] * w;
+        const double az = a.bzb[k + 1] * c - gamma * n - gamma * so;
+        rr[e] = (T)(Rs[e] - ar - az);
+        dl[e] = (T)0;
+    }
+    __syncthreads();
+    const int nhalf = 2 * a.nsteps_run + 1;
+    for (int h = 0; h < nhalf; ++h) {
+        const bool radial = (h % 2) == 0;
+        const int it = radial ? max(h / 2 - 1, 0) : (h - 1) / 2;
+        const int step = a.step0 + it;
+        const T dtt = (T)a.dt[step];
+        if (radial) {
+            const double *src = a.rad + ((long long)step * a.N + s) * kAdiFactors * nr;
+            for (int i = tid; i < 3 * nr; i += kAdiThreads) rf[i] = (T)src[i];
+            // (Ar + dt) delta' = r + (dt - Az) delta
+            for (long long e = tid; e < np; e += kAdiThreads) {
+                const int k = (int)(e / nr);
+                const T d = dl[e];
+                const T up = (k + 1 < nz) ? dl[e + nr] : (T)0;
+                const T dn = (k > 0) ? dl[e - nr] : (T)0;
+                const T czn = (k > 0 || !sym_bottom) ? g : (T)0;
+                const T bz = (T)a.bzb[k + 1];
+                ww[e] = rr[e] + dtt * d - (bz * d - g * up - czn * dn);
+            }
+            __syncthreads();
+            const T *ib = rf, *dd = rf + nr, *gm = rf + 2 * nr;
+            for (int k = tid; k < nz; k += kAdiThreads) {
+                T *w = ww + (long long)k * nr;
+                T *x = dl + (long long)k * nr;
+                T y = w[0] * ib[0];
+                w[0] = y;
+                for (int j = 1; j < nr; ++j) {
+                    y = w[j] * ib[j] - dd[j] * y;
+                    w[j] = y;
+                }
+                T xv = y;
+                x[nr - 1] = xv;
+                for (int j = nr - 2; j >= 0; --j) {
+                    xv = w[j] - gm[j + 1] * xv;
+                    x[j] = xv;
+                }
+            }
+        } else {
+            const double *src = a.ver + (long long)step * kAdiFactors * nz;
+            for (int i = tid; i < 3 * nz; i += kAdiThreads) vf[i] = (T)src[i];
+            // (Az + dt) delta' = r + (dt - Ar) delta
+            for (long long e = tid; e < np; e += kAdiThreads) {
+                const int j = (int)(e % nr);
+                const T d = dl[e];
+                const T right = (j + 1 < nr) ? dl[e + 1] : (T)0;
+                const T left = (j > 0) ? dl[e - 1] : (T)0;
+                ww[e] = rr[e] + dtt * d - (cb[j] * d + ca[j] * right + cbe[j] * left);
+            }
+            __syncthreads();
+            const T *ib = vf, *dd = vf + nz, *gm = vf + 2 * nz;
+            for (int j = tid; j < nr; j += kAdiThreads) {
+                T y = ww[j] * ib[0];
+                ww[j] = y;
+                for (int k = 1; k < nz; ++k) {
+                    y = ww[(long long)k * nr + j] * ib[k] - dd[k] * y;
+                    ww[(long long)k * nr + j] = y;
+                }
+                T xv = y;
+                dl[(long long)(nz - 1) * nr + j] = xv;
+                for (int k = nz - 2; k >= 0; --k) {
+                    xv = ww[(long long)k * nr + j] - gm[k + 1] * xv;
+                    dl[(long long)k * nr + j] = xv;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // phi += delta in FP64; per-slot |delta|^2 and |phi|^2
+    double sd = 0.0, sp = 0.0;
+    for (long long e = tid; e < np; e += kAdiThreads) {
+        const int j = (int)(e % nr), k = (int)(e / nr);
+        double *pp = Pg + (long long)numr * (k + 1) + 1 + j;
+        const double d = (double)dl[e];
+        const double ph = *pp + d;
+        *pp = ph;
+        sd += d * d;
+        sp += ph * ph;
+    }
+    const int lane = tid & 31, warp = tid >> 5;
+    for (int off = 16; off > 0; off >>= 1) {
+        sd += __shfl_down_sync(0xffffffffu, sd, off);
+        sp += __shfl_down_sync(0xffffffffu, sp, off);
+    }
+    __shared__ double red[2 * (kAdiThreads / 32)];
+    if (lane == 0) {
+        red[2 * warp] = sd;
+        red[2 * warp + 1] = sp;
+    }
+    __syncthreads();
+    if (tid < 2) {
+        double t = 0.0;
+        for (int w = 0; w < kAdiThreads / 32; ++w) t += red[2 * w + tid];
+        const double wgt = (s == 0 || s == a.N / 2) ? 1.0 : 2.0;
+        a.norms[2 * s + tid] = wgt * t;
+    }
+}
+
+size_t gdefect_smem(const bph_ctx *c) { return sizeof(float) * (size_t)(6 * c->nr + 3 * c->nz) + 16; }
+
+// ---------------------------------------------------------------------------
 // Segmented on-chip ADI (the fast path).  The slot's potential P and its
 // right-hand side R = -4 pi rho_hat both stay in shared memory for all
 // steps.  Every line system is cut into kAdiSeg-long segments, one thread
@@ -1259,11 +1407,16 @@ int adi_configure(bph_ctx *c) {
         c->adi_mixed_threads = threads;
         if (!c->mixed_kind) c->mixed_kind = kind;
     }
+    // the global-memory kernel fits every grid: the default when neither on-chip kernel does
+    c->mixed_smem_kind[BPH_MIXED_ADI_GLOBAL] = (int)gdefect_smem(c);
+    c->mixed_per_sm_kind[BPH_MIXED_ADI_GLOBAL] = 0;
+    if (!c->mixed_kind) c->mixed_kind = BPH_MIXED_ADI_GLOBAL;
+    if (!c->adi_mixed_threads) c->adi_mixed_threads = kAdiThreads;
     return select_mixed_kind(c, c->mixed_kind);
 }
 
 int select_mixed_kind(bph_ctx *c, int kind) {
-    if (kind < 1 || kind > 2 || !c->mixed_smem_kind[kind]) {
+    if (kind < 1 || kind > 3 || !c->mixed_smem_kind[kind]) {
         c->adi_mixed_smem = 0;
         c->adi_mixed_per_sm = 0;
         return (kind == 0) ? BPH_OK : BPH_ERR_INVALID;
@@ -1363,6 +1516,11 @@ cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {
     a.pkz = packed_block<float>(c->nz);
     ++c->launches;
     void *args[] = {&a};
+    if (c->mixed_kind == BPH_MIXED_ADI_GLOBAL) {
+        if (!c->d_work32) return cudaErrorNotReady;  // ensure_mixed_work first
+        k_adi_gdefect<float><<<c->N, kAdiThreads, gdefect_smem(c), c->stream>>>(a, c->d_work32);
+        return cudaGetLastError();
+    }
     const void *fn = (c->mixed_kind == BPH_MIXED_ADI_FORWARD)
                          ? seg_kernel<float, true>(c->adi_mixed_threads, c->adi_full, c->mixed_pf)
                          : delta_kernel(c->adi_mixed_threads, c->adi_full);

@@ -555,6 +555,7 @@ int bph_destroy(bph_ctx_t *c) {
     dev_free(c->d_ccnt);
     dev_free(c->d_cpart);
     conv_graphs_free(c);
+    dev_free(c->d_work32);
     if (c->side_stream) {
         cudaStreamSynchronize(c->side_stream);
         cudaStreamDestroy(c->side_stream);
@@ -628,6 +629,11 @@ int bph_solve_nsteps(bph_ctx_t *c, const double *rho, double *pot, int nsteps, i
 namespace bph {
 
 // Sum of the per-slot (num, den) pairs a norm kernel left in c->d_red.
+int ensure_mixed_work(bph_ctx *c) {
+    if (c->d_work32) return BPH_OK;
+    return dev_alloc(c, &c->d_work32, (size_t)c->N * 3 * (size_t)c->np);
+}
+
 static double host_ratio(const std::vector<double> &h, int N) {
     double num = 0.0, den = 0.0;
     for (int i = 0; i < N; ++i) {
@@ -652,12 +658,13 @@ static int converged_impl(bph_ctx *c, const double *rho, double *pot, int nsteps
         return BPH_ERR_INVALID;
     }
     if (mixed && !c->adi_mixed_smem) {
-        set_error("the mixed-precision ADI does not fit on chip for this grid");
+        set_error("no mixed-precision ADI kernel is configured for this grid");
         return BPH_ERR_INVALID;
     }
     if ((rc = set_device_of(c))) return rc;
     Schedule *s;
     if ((rc = get_schedule(c, nsteps, &s))) return rc;
+    if (mixed && c->mixed_kind == BPH_MIXED_ADI_GLOBAL && (rc = ensure_mixed_work(c))) return rc;
     if (!mixed && !c->d_prev && (rc = dev_alloc(c, &c->d_prev, (size_t)c->N * c->nplane))) return rc;
     const size_t bytes = sizeof(double) * (size_t)c->ntot;
     const double *d_rho = rho;
@@ -867,7 +874,7 @@ int bph_configure(bph_ctx_t *c, int key, int value) {
     }
     if ((rc = set_device_of(c))) return rc;
     if (value == BPH_MIXED_ADI_AUTO) return autotune_mixed(c);
-    if (value != BPH_MIXED_ADI_FORWARD && value != BPH_MIXED_ADI_INCREMENT) {
+    if (value != BPH_MIXED_ADI_FORWARD && value != BPH_MIXED_ADI_INCREMENT && value != BPH_MIXED_ADI_GLOBAL) {
         set_error("unknown refinement ADI kind %d", value);
         return BPH_ERR_INVALID;
     }

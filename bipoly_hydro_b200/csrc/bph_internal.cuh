@@ -145,9 +145,10 @@ struct bph_ctx {
     int adi_mixed_smem = 0;      // dynamic shared bytes of the one in use (0: mixed form unavailable)
     int adi_mixed_per_sm = 0;    // its resident CTAs per SM
     int mixed_kind = 0;          // refinement ADI in use: BPH_MIXED_ADI_FORWARD or _INCREMENT
-    int mixed_smem_kind[3] = {0, 0, 0};    // per kind: dynamic shared bytes (0: does not fit)
-    int mixed_per_sm_kind[3] = {0, 0, 0};  // per kind: resident CTAs per SM
-    float mixed_tuned_us[3] = {0.f, 0.f, 0.f};  // per kind: setup-time measurement (0: not timed)
+    int mixed_smem_kind[4] = {0, 0, 0, 0};    // per kind: dynamic shared bytes (0: does not fit)
+    int mixed_per_sm_kind[4] = {0, 0, 0, 0};  // per kind: resident CTAs per SM
+    float mixed_tuned_us[4] = {0.f, 0.f, 0.f, 0.f};  // per kind: setup-time measurement (0: not timed)
+    float *d_work32 = nullptr;                // global-memory refinement kernel: [N][3][np] (lazy)
     int adi_threads = 256;
     int fft_smem_fwd = 0, fft_smem_inv = 0;
     bool have_warm = false;
@@ -248,6 +249,8 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
                      bool warm, bool on_device, int *pos_status);
 // Makes kind (BPH_MIXED_ADI_FORWARD / _INCREMENT) the refinement ADI kernel.
 int select_mixed_kind(bph_ctx *c, int kind);
+// Work area of the global-memory refinement kernel (allocated on first use).
+int ensure_mixed_work(bph_ctx *c);
 int contract_configure(bph_ctx *c);
 int fft_configure(bph_ctx *c);
 

@@ -267,12 +267,17 @@ long long bph_info(const bph_ctx_t *ctx, int what);
  *   BPH_MIXED_ADI_INCREMENT  every half-step solves for an increment of the
  *                            residual r - A delta (more instructions, smaller
  *                            shared-memory footprint).
- * Both converge to the same discrete solution.  Returns BPH_ERR_INVALID for
- * a kind that does not fit this grid on chip. */
+ *   BPH_MIXED_ADI_GLOBAL     the same cycle with the slot's arrays in global
+ *                            memory, for grids whose slots exceed shared memory.
+ * All converge to the same discrete solution.  Returns BPH_ERR_INVALID for
+ * an on-chip kind that does not fit this grid. */
 #define BPH_CFG_MIXED_ADI 0
 #define BPH_MIXED_ADI_AUTO 0
 #define BPH_MIXED_ADI_FORWARD 1
 #define BPH_MIXED_ADI_INCREMENT 2
+/* the forwarding form with its slot in global memory: any grid size, the
+ * choice when neither on-chip kernel fits (e.g. 258x194x512) */
+#define BPH_MIXED_ADI_GLOBAL 3
 int bph_configure(bph_ctx_t *ctx, int key, int value);
 
 /* Number of kernels this context has launched so far. */

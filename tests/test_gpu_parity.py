@@ -175,7 +175,7 @@ def test_gpu_reproduces_golden_fixture(bph, path):
 @pytest.mark.parametrize("grid", [(34, 26, 64, 1.0 / 30.0, 2, 30), (66, 66, 64, 1.0 / 62.0, 2, 30),
                                   (20, 14, 32, 1.0 / 18.0, 1, 8), (18, 16, 32, 1.0 / 16.0, 3, 6)],
                          ids=["34x26x64", "66x66x64", "isym1", "isym3"])
-@pytest.mark.parametrize("kind", [1, 2], ids=["forward", "increment"])
+@pytest.mark.parametrize("kind", [1, 2, 3], ids=["forward", "increment", "global"])
 def test_mixed_converged_within_1e9_of_fp64(oracle_mod, bph, grid, kind):
     """FP32 ADI + FP64 residual/update refinement converges to the FP64 discrete
     solution: relative L2 error <= 1e-9 against the GPU FP64 converged solve
@@ -334,6 +334,11 @@ def test_config3_large_grid_gaussian_sphere(bph):
     err = rel_l2(pot[sl], exact[sl])
     # the 66x66 grid (dr = 1/62) reaches ~1e-3; dr is 4x smaller here
     assert err < 2e-4, err
+    # mixed precision (config 3): the slots exceed shared memory, so the
+    # global-memory FP32 refinement kernel is chosen; within 1e-9 of FP64
+    assert g.info()["mixed_kind"] == 3
+    pmx, imx = g.solve_converged_mixed(rho, 20, True, 1e-12, 60)
+    assert rel_l2(pmx, pot) <= 1e-9, (rel_l2(pmx, pot), imx.cycles)
     # the time-step solves are near the converged potential
     assert rel_l2(cold, pot) < 0.1 and rel_l2(warm, pot) < 0.1
     g.close()
