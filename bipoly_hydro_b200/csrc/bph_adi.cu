@@ -200,6 +200,162 @@ __global__ void __launch_bounds__(kAdiThreads) k_adi(AdiArgs a) {
 size_t smalls_bytes(const bph_ctx *c) { return sizeof(double) * (size_t)(9 * c->nr + 4 * c->nz); }
 
 // ---------------------------------------------------------------------------
+// ADI for slots too large for shared memory (k_adi_tiled).
+//
+// One CTA per slot; the potential stays in the slot array (layout A,
+// [k][j], j contiguous) and the radial half-sweep works on a transposed copy
+// (layout B, [j][k]) so that every line solve reads and writes coalesced:
+// radial lines run along j with the threads of a warp on consecutive k
+// (layout B), vertical lines along k with the threads on consecutive j
+// (layout A).  Each half-sweep's right-hand side is formed tile by tile
+// (32 x 32) through shared memory, which is where the layout changes: the
+// tile is computed reading one layout and written out in the other.  The
+// arithmetic is that of k_adi (helmadi.F90:203-343).
+constexpr int kTileT = 32;
+
+__global__ void __launch_bounds__(kAdiThreads) k_adi_tiled(AdiArgs a, double *__restrict__ Wb,
+                                                           double *__restrict__ Qb) {
+    __shared__ double tile[kTileT][kTileT + 1];
+    extern __shared__ double sm[];
+    const int s = blockIdx.x, tid = threadIdx.x;
+    const int nr = a.nr, nz = a.nz, numr = a.numr;
+    const long long np = (long long)nr * nz;
+    const long long nplane = (long long)numr * a.numz;
+    double *Pg = a.P + (long long)s * nplane;
+    const double *Rs = a.R + (long long)s * np;
+    double *W = Wb + (long long)s * np;  // right-hand sides: layout B (radial) or A (vertical)
+    double *Q = Qb + (long long)s * np;  // radial half-sweep result, layout B
+    double *rf = sm;                     // [3][nr]
+    double *vf = rf + 3 * nr;            // [3][nz]
+    double *top = vf + 3 * nz;           // [nr] phi(J, numz)
+    double *side = top + nr;             // [nz] phi(numr, K)
+    double *bot = side + nz;             // [nr] phi(J, 1) (isym 1)
+    double *alz = bot + nr, *bez = alz + nr, *elz = bez + nr;
+    const double gamma = a.gamma;
+    const double a_side = a.alphar[numr - 2];  // alphar(numr-1)
+    const bool sym_bottom = (a.isym != 1);
+    for (int j = tid; j < nr; j += kAdiThreads) {
+        alz[j] = a.alphar[j + 1];
+        bez[j] = a.betar[j + 1];
+        elz[j] = a.elz[(long long)s * numr + j + 1];
+    }
+    pdl_wait();
+    for (int j = tid; j < nr; j += kAdiThreads) {
+        top[j] = Pg[(j + 1) + (long long)numr * (a.numz - 1)];
+        bot[j] = (a.isym == 1) ? Pg[j + 1] : 0.0;
+    }
+    for (int k = tid; k < nz; k += kAdiThreads) side[k] = Pg[(numr - 1) + (long long)numr * (k + 1)];
+    if (a.cold)
+        for (long long e = tid; e < np; e += kAdiThreads)
+            Pg[(e % nr + 1) + (long long)numr * (e / nr + 1)] = 0.0;
+    __syncthreads();
+    const int tk = (nz + kTileT - 1) / kTileT, tj = (nr + kTileT - 1) / kTileT;
+    for (int it = 0; it < a.nsteps_run; ++it) {
+        const int step = a.step0 + it;
+        const double dtt = a.dt[step];
+        const double *rsrc = a.rad + ((long long)step * a.N + s) * kAdiFactors * nr;
+        const double *vsrc = a.ver + (long long)step * kAdiFactors * nz;
+        for (int i = tid; i < 3 * nr; i += kAdiThreads) rf[i] = rsrc[i];
+        for (int i = tid; i < 3 * nz; i += kAdiThreads) vf[i] = vsrc[i];
+        // ---- radial right-hand side (helmadi.F90:203-256), A -> B ----
+        for (int t = 0; t < tk * tj; ++t) {
+            const int k0 = (t / tj) * kTileT, j0 = (t % tj) * kTileT;
+            for (int e = tid; e < kTileT * kTileT; e += kAdiThreads) {
+                const int kl = e / kTileT, jl = e % kTileT, k = k0 + kl, j = j0 + jl;
+                if (k < nz && j < nr) {
+                    const double *pc = Pg + (j + 1) + (long long)numr * (k + 1);
+                    const double phi = pc[0], up = pc[numr];  // row numz-1 above the last interior row
+                    double v;
+                    if (k == 0 && sym_bottom) {
+                        v = Rs[(long long)nr * k + j] + (dtt - gamma) * phi + gamma * up;
+                    } else {
+                        v = Rs[(long long)nr * k + j] + (dtt - 2.0 * gamma) * phi + gamma * (up + pc[-numr]);
+                    }
+                    if (j == nr - 1) v = v - a_side * side[k];
+                    tile[kl][jl] = v;
+                }
+            }
+            __syncthreads();
+            for (int e = tid; e < kTileT * kTileT; e += kAdiThreads) {
+                const int jl = e / kTileT, kl = e % kTileT, k = k0 + kl, j = j0 + jl;
+                if (k < nz && j < nr) W[(long long)j * nz + k] = tile[kl][jl];
+            }
+            __syncthreads();
+        }
+        // ---- radial line solves (tridagr): line k, threads on consecutive k ----
+        {
+            const double *ib = rf, *dd = rf + nr, *gm = rf + 2 * nr;
+            for (int k = tid; k < nz; k += kAdiThreads) {
+                double y = W[k] * ib[0];
+                W[k] = y;
+#pragma unroll 4
+                for (int j = 1; j < nr; ++j) {
+                    y = W[(long long)j * nz + k] * ib[j] - dd[j] * y;
+                    W[(long long)j * nz + k] = y;
+                }
+                double x = y;
+                Q[(long long)(nr - 1) * nz + k] = x;
+#pragma unroll 4
+                for (int j = nr - 2; j >= 0; --j) {
+                    x = W[(long long)j * nz + k] - gm[j + 1] * x;
+                    Q[(long long)j * nz + k] = x;
+                }
+            }
+        }
+        __syncthreads();
+        // ---- vertical right-hand side (helmadi.F90:272-340), B -> A ----
+        for (int t = 0; t < tk * tj; ++t) {
+            const int k0 = (t / tj) * kTileT, j0 = (t % tj) * kTileT;
+            for (int e = tid; e < kTileT * kTileT; e += kAdiThreads) {
+                const int jl = e / kTileT, kl = e % kTileT, k = k0 + kl, j = j0 + jl;
+                if (k < nz && j < nr) {
+                    const double *qc = Q + (long long)j * nz + k;
+                    const double phi = qc[0];
+                    const double right = (j + 1 < nr) ? qc[nz] : side[k];
+                    double v = (elz[j] + dtt) * phi - alz[j] * right;
+                    if (j > 0) v = v - bez[j] * qc[-nz];
+                    tile[jl][kl] = v;
+                }
+            }
+            __syncthreads();
+            for (int e = tid; e < kTileT * kTileT; e += kAdiThreads) {
+                const int kl = e / kTileT, jl = e % kTileT, k = k0 + kl, j = j0 + jl;
+                if (k < nz && j < nr) {
+                    double v = Rs[(long long)nr * k + j] + tile[jl][kl];
+                    if (k == nz - 1) v = v + gamma * top[j];
+                    if (!sym_bottom && k == 0) v = v + gamma * bot[j];
+                    W[(long long)k * nr + j] = v;
+                }
+            }
+            __syncthreads();
+        }
+        // ---- vertical line solves (tridagz): line j, threads on consecutive j ----
+        {
+            const double *ib = vf, *dd = vf + nz, *gm = vf + 2 * nz;
+            for (int j = tid; j < nr; j += kAdiThreads) {
+                double y = W[j] * ib[0];
+                W[j] = y;
+#pragma unroll 4
+                for (int k = 1; k < nz; ++k) {
+                    y = W[(long long)k * nr + j] * ib[k] - dd[k] * y;
+                    W[(long long)k * nr + j] = y;
+                }
+                double x = y;
+                Pg[(j + 1) + (long long)numr * nz] = x;
+#pragma unroll 4
+                for (int k = nz - 2; k >= 0; --k) {
+                    x = W[(long long)k * nr + j] - gm[k + 1] * x;
+                    Pg[(j + 1) + (long long)numr * (k + 1)] = x;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+size_t tiled_smem(const bph_ctx *c) { return sizeof(double) * (size_t)(3 * c->nr + 3 * c->nz + 5 * c->nr + c->nz); }
+
+// ---------------------------------------------------------------------------
 // FP32 refinement cycle for slots too large for shared memory (k_adi_gdefect).
 //
 // One CTA per slot; its defect r, increment delta and a right-hand-side
@@ -1485,7 +1641,7 @@ cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_ru
         if (c->adi_smem > 0)
             k_adi<true><<<c->N, kAdiThreads, c->adi_smem, c->stream>>>(ai);
         else
-            k_adi<false><<<c->N, kAdiThreads, smalls_bytes(c), c->stream>>>(ai);
+            k_adi_tiled<<<c->N, kAdiThreads, tiled_smem(c), c->stream>>>(ai, c->d_W, c->d_W2);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }

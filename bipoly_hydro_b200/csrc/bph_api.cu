@@ -402,6 +402,7 @@ int setup_impl(bph_ctx *c) {
     }
     if (c->adi_smem == 0) {
         if ((rc = dev_alloc(c, &c->d_W, (size_t)c->N * c->nplane))) return rc;
+        if ((rc = dev_alloc(c, &c->d_W2, (size_t)c->N * c->np))) return rc;
     }
     Schedule *s;
     if ((rc = get_schedule(c, 5, &s))) return rc;
@@ -545,7 +546,7 @@ int bph_destroy(bph_ctx_t *c) {
     for (auto &s : c->sched) free_schedule(c, s);
     double *bufs[] = {c->d_green, c->d_brb,  c->d_elz, c->d_alphar, c->d_betar,     c->d_bzb,
                       c->d_qcoef, c->d_grid, c->d_R,   c->d_P,      c->d_prev,      c->d_mom,
-                      c->d_S,     c->d_W,    c->d_P2,  c->d_red,    c->d_rho_stage, c->d_pot_stage,
+                      c->d_S,     c->d_W,    c->d_W2,  c->d_P2,     c->d_red,       c->d_rho_stage, c->d_pot_stage,
                       c->d_phieff_stage};
     for (double *p : bufs) dev_free(p);
     dev_free(c->d_tw);

@@ -126,6 +126,7 @@ struct bph_ctx {
     double *d_mom = nullptr;     // [mmax][2][np]
     double *d_S = nullptr;       // [mmax][nb][2]
     double *d_W = nullptr;       // ADI work slabs when they do not fit on chip
+    double *d_W2 = nullptr;      // tiled large-grid ADI: the radial half-sweep result [N][np], transposed
     double *d_P2 = nullptr;      // ADI potential slabs when they do not fit on chip
     double *d_red = nullptr;     // reduction scratch
     double *d_rho_stage = nullptr;
