@@ -199,309 +199,9 @@ __global__ void __launch_bounds__(kAdiThreads) k_adi(AdiArgs a) {
 
 size_t smalls_bytes(const bph_ctx *c) { return sizeof(double) * (size_t)(9 * c->nr + 4 * c->nz); }
 
-// ---------------------------------------------------------------------------
-// ADI for slots too large for shared memory (k_adi_tiled).
-//
-// One CTA per slot; the potential stays in the slot array (layout A,
-// [k][j], j contiguous) and the radial half-sweep works on a transposed copy
-// (layout B, [j][k]) so that every line solve reads and writes coalesced:
-// radial lines run along j with the threads of a warp on consecutive k
-// (layout B), vertical lines along k with the threads on consecutive j
-// (layout A).  Each half-sweep's right-hand side is formed tile by tile
-// (32 x 32) through shared memory, which is where the layout changes: the
-// tile is computed reading one layout and written out in the other.  The
-// arithmetic is that of k_adi (helmadi.F90:203-343).
-constexpr int kTileT = 32;
 
-__global__ void __launch_bounds__(kAdiThreads) k_adi_tiled(AdiArgs a, double *__restrict__ Wb,
-                                                           double *__restrict__ Qb) {
-    __shared__ double tile[kTileT][kTileT + 1];
-    extern __shared__ double sm[];
-    const int s = blockIdx.x, tid = threadIdx.x;
-    const int nr = a.nr, nz = a.nz, numr = a.numr;
-    const long long np = (long long)nr * nz;
-    const long long nplane = (long long)numr * a.numz;
-    double *Pg = a.P + (long long)s * nplane;
-    const double *Rs = a.R + (long long)s * np;
-    double *W = Wb + (long long)s * np;  // right-hand sides: layout B (radial) or A (vertical)
-    double *Q = Qb + (long long)s * np;  // radial half-sweep result, layout B
-    double *rf = sm;                     // [3][nr]
-    double *vf = rf + 3 * nr;            // [3][nz]
-    double *top = vf + 3 * nz;           // [nr] phi(J, numz)
-    double *side = top + nr;             // [nz] phi(numr, K)
-    double *bot = side + nz;             // [nr] phi(J, 1) (isym 1)
-    double *alz = bot + nr, *bez = alz + nr, *elz = bez + nr;
-    const double gamma = a.gamma;
-    const double a_side = a.alphar[numr - 2];  // alphar(numr-1)
-    const bool sym_bottom = (a.isym != 1);
-    for (int j = tid; j < nr; j += kAdiThreads) {
-        alz[j] = a.alphar[j + 1];
-        bez[j] = a.betar[j + 1];
-        elz[j] = a.elz[(long long)s * numr + j + 1];
-    }
-    pdl_wait();
-    for (int j = tid; j < nr; j += kAdiThreads) {
-        top[j] = Pg[(j + 1) + (long long)numr * (a.numz - 1)];
-        bot[j] = (a.isym == 1) ? Pg[j + 1] : 0.0;
-    }
-    for (int k = tid; k < nz; k += kAdiThreads) side[k] = Pg[(numr - 1) + (long long)numr * (k + 1)];
-    if (a.cold)
-        for (long long e = tid; e < np; e += kAdiThreads)
-            Pg[(e % nr + 1) + (long long)numr * (e / nr + 1)] = 0.0;
-    __syncthreads();
-    const int tk = (nz + kTileT - 1) / kTileT, tj = (nr + kTileT - 1) / kTileT;
-    for (int it = 0; it < a.nsteps_run; ++it) {
-        const int step = a.step0 + it;
-        const double dtt = a.dt[step];
-        const double *rsrc = a.rad + ((long long)step * a.N + s) * kAdiFactors * nr;
-        const double *vsrc = a.ver + (long long)step * kAdiFactors * nz;
-        for (int i = tid; i < 3 * nr; i += kAdiThreads) rf[i] = rsrc[i];
-        for (int i = tid; i < 3 * nz; i += kAdiThreads) vf[i] = vsrc[i];
-        // ---- radial right-hand side (helmadi.F90:203-256), A -> B ----
-        for (int t = 0; t < tk * tj; ++t) {
-            const int k0 = (t / tj) * kTileT, j0 = (t % tj) * kTileT;
-            for (int e = tid; e < kTileT * kTileT; e += kAdiThreads) {
-                const int kl = e / kTileT, jl = e % kTileT, k = k0 + kl, j = j0 + jl;
-                if (k < nz && j < nr) {
-                    const double *pc = Pg + (j + 1) + (long long)numr * (k + 1);
-                    const double phi = pc[0], up = pc[numr];  // row numz-1 above the last interior row
-                    double v;
-                    if (k == 0 && sym_bottom) {
-                        v = Rs[(long long)nr * k + j] + (dtt - gamma) * phi + gamma * up;
-                    } else {
-                        v = Rs[(long long)nr * k + j] + (dtt - 2.0 * gamma) * phi + gamma * (up + pc[-numr]);
-                    }
-                    if (j == nr - 1) v = v - a_side * side[k];
-                    tile[kl][jl] = v;
-                }
-            }
-            __syncthreads();
-            for (int e = tid; e < kTileT * kTileT; e += kAdiThreads) {
-                const int jl = e / kTileT, kl = e % kTileT, k = k0 + kl, j = j0 + jl;
-                if (k < nz && j < nr) W[(long long)j * nz + k] = tile[kl][jl];
-            }
-            __syncthreads();
-        }
-        // ---- radial line solves (tridagr): line k, threads on consecutive k ----
-        {
-            const double *ib = rf, *dd = rf + nr, *gm = rf + 2 * nr;
-            for (int k = tid; k < nz; k += kAdiThreads) {
-                double y = W[k] * ib[0];
-                W[k] = y;
-#pragma unroll 4
-                for (int j = 1; j < nr; ++j) {
-                    y = W[(long long)j * nz + k] * ib[j] - dd[j] * y;
-                    W[(long long)j * nz + k] = y;
-                }
-                double x = y;
-                Q[(long long)(nr - 1) * nz + k] = x;
-#pragma unroll 4
-                for (int j = nr - 2; j >= 0; --j) {
-                    x = W[(long long)j * nz + k] - gm[j + 1] * x;
-                    Q[(long long)j * nz + k] = x;
-                }
-            }
-        }
-        __syncthreads();
-        // ---- vertical right-hand side (helmadi.F90:272-340), B -> A ----
-        for (int t = 0; t < tk * tj; ++t) {
-            const int k0 = (t / tj) * kTileT, j0 = (t % tj) * kTileT;
-            for (int e = tid; e < kTileT * kTileT; e += kAdiThreads) {
-                const int jl = e / kTileT, kl = e % kTileT, k = k0 + kl, j = j0 + jl;
-                if (k < nz && j < nr) {
-                    const double *qc = Q + (long long)j * nz + k;
-                    const double phi = qc[0];
-                    const double right = (j + 1 < nr) ? qc[nz] : side[k];
-                    double v = (elz[j] + dtt) * phi - alz[j] * right;
-                    if (j > 0) v = v - bez[j] * qc[-nz];
-                    tile[jl][kl] = v;
-                }
-            }
-            __syncthreads();
-            for (int e = tid; e < kTileT * kTileT; e += kAdiThreads) {
-                const int kl = e / kTileT, jl = e % kTileT, k = k0 + kl, j = j0 + jl;
-                if (k < nz && j < nr) {
-                    double v = Rs[(long long)nr * k + j] + tile[jl][kl];
-                    if (k == nz - 1) v = v + gamma * top[j];
-                    if (!sym_bottom && k == 0) v = v + gamma * bot[j];
-                    W[(long long)k * nr + j] = v;
-                }
-            }
-            __syncthreads();
-        }
-        // ---- vertical line solves (tridagz): line j, threads on consecutive j ----
-        {
-            const double *ib = vf, *dd = vf + nz, *gm = vf + 2 * nz;
-            for (int j = tid; j < nr; j += kAdiThreads) {
-                double y = W[j] * ib[0];
-                W[j] = y;
-#pragma unroll 4
-                for (int k = 1; k < nz; ++k) {
-                    y = W[(long long)k * nr + j] * ib[k] - dd[k] * y;
-                    W[(long long)k * nr + j] = y;
-                }
-                double x = y;
-                Pg[(j + 1) + (long long)numr * nz] = x;
-#pragma unroll 4
-                for (int k = nz - 2; k >= 0; --k) {
-                    x = W[(long long)k * nr + j] - gm[k + 1] * x;
-                    Pg[(j + 1) + (long long)numr * (k + 1)] = x;
-                }
-            }
-        }
-        __syncthreads();
-    }
-}
 
-size_t tiled_smem(const bph_ctx *c) { return sizeof(double) * (size_t)(3 * c->nr + 3 * c->nz + 5 * c->nr + c->nz); }
 
-// ---------------------------------------------------------------------------
-// FP32 refinement cycle for slots too large for shared memory (k_adi_gdefect).
-//
-// One CTA per slot; its defect r, increment delta and a right-hand-side
-// buffer live in a global work area (T, interior-packed [k][j]).  Prologue:
-// the FP64 residual r = -4 pi rho_hat - A phi of the current potential;
-// body: the defect equation A delta = r in helmadi's right-hand-side form
-// from delta = 0 with zero Dirichlet data, half-steps radial at the first
-// step's dt, then (vertical, radial) per step -- the order the on-chip FP32
-// kernels use, which keeps rounding of stiff near-axis components out of the
-// refinement; epilogue: phi += delta in FP64 and the per-slot norms.  Line
-// solves are the Thomas recurrences of tridagr/tridagz, one thread per line.
-template <typename T>
-__global__ void __launch_bounds__(kAdiThreads) k_adi_gdefect(AdiArgs a, T *__restrict__ work) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    const int s = blockIdx.x, tid = threadIdx.x;
-    const int nr = a.nr, nz = a.nz, numr = a.numr;
-    const long long np = (long long)nr * nz;
-    const long long nplane = (long long)numr * a.numz;
-    double *Pg = a.P + (long long)s * nplane;
-    const double *Rs = a.R + (long long)s * np;
-    T *rr = work + (long long)s * 3 * np, *dl = rr + np, *ww = dl + np;
-    T *rf = reinterpret_cast<T *>(smraw);  // [3][nr] radial ib, dd, gam of the current step
-    T *vf = rf + 3 * nr;                    // [3][nz] vertical
-    T *cb = vf + 3 * nz;                    // [nr] brb, [nr] alphar, [nr] betar of the slot
-    T *ca = cb + nr, *cbe = ca + nr;
-    const double gamma = a.gamma;
-    const T g = (T)gamma;
-    const bool sym_bottom = (a.isym != 1);
-    const double *brb = a.brb + (long long)s * numr;
-    for (int j = tid; j < nr; j += kAdiThreads) {
-        cb[j] = (T)brb[j + 1];
-        ca[j] = (T)a.alphar[j + 1];
-        cbe[j] = (T)a.betar[j + 1];
-    }
-    pdl_wait();
-    // FP64 residual; delta = 0
-    for (long long e = tid; e < np; e += kAdiThreads) {
-        const int j = (int)(e % nr), k = (int)(e / nr);
-        const double *pc = Pg + (long long)numr * (k + 1) + 1;
-        const double c = pc[j], east = pc[j + 1], n = pc[j + numr];
-        const double w = (j > 0) ? pc[j - 1] : 0.0;
-        const double so = (k > 0 || !sym_bottom) ? pc[j - numr] : 0.0;
-        const double ar = brb[j + 1] * c + a.alphar[j + 1] * east + a.betar[j + 1] * w;
-        const double az = a.bzb[k + 1] * c - gamma * n - gamma * so;
-        rr[e] = (T)(Rs[e] - ar - az);
-        dl[e] = (T)0;
-    }
-    __syncthreads();
-    const int nhalf = 2 * a.nsteps_run + 1;
-    for (int h = 0; h < nhalf; ++h) {
-        const bool radial = (h % 2) == 0;
-        const int it = radial ? max(h / 2 - 1, 0) : (h - 1) / 2;
-        const int step = a.step0 + it;
-        const T dtt = (T)a.dt[step];
-        if (radial) {
-            const double *src = a.rad + ((long long)step * a.N + s) * kAdiFactors * nr;
-            for (int i = tid; i < 3 * nr; i += kAdiThreads) rf[i] = (T)src[i];
-            // (Ar + dt) delta' = r + (dt - Az) delta
-            for (long long e = tid; e < np; e += kAdiThreads) {
-                const int k = (int)(e / nr);
-                const T d = dl[e];
-                const T up = (k + 1 < nz) ? dl[e + nr] : (T)0;
-                const T dn = (k > 0) ? dl[e - nr] : (T)0;
-                const T czn = (k > 0 || !sym_bottom) ? g : (T)0;
-                const T bz = (T)a.bzb[k + 1];
-                ww[e] = rr[e] + dtt * d - (bz * d - g * up - czn * dn);
-            }
-            __syncthreads();
-            const T *ib = rf, *dd = rf + nr, *gm = rf + 2 * nr;
-            for (int k = tid; k < nz; k += kAdiThreads) {
-                T *w = ww + (long long)k * nr;
-                T *x = dl + (long long)k * nr;
-                T y = w[0] * ib[0];
-                w[0] = y;
-                for (int j = 1; j < nr; ++j) {
-                    y = w[j] * ib[j] - dd[j] * y;
-                    w[j] = y;
-                }
-                T xv = y;
-                x[nr - 1] = xv;
-                for (int j = nr - 2; j >= 0; --j) {
-                    xv = w[j] - gm[j + 1] * xv;
-                    x[j] = xv;
-                }
-            }
-        } else {
-            const double *src = a.ver + (long long)step * kAdiFactors * nz;
-            for (int i = tid; i < 3 * nz; i += kAdiThreads) vf[i] = (T)src[i];
-            // (Az + dt) delta' = r + (dt - Ar) delta
-            for (long long e = tid; e < np; e += kAdiThreads) {
-                const int j = (int)(e % nr);
-                const T d = dl[e];
-                const T right = (j + 1 < nr) ? dl[e + 1] : (T)0;
-                const T left = (j > 0) ? dl[e - 1] : (T)0;
-                ww[e] = rr[e] + dtt * d - (cb[j] * d + ca[j] * right + cbe[j] * left);
-            }
-            __syncthreads();
-            const T *ib = vf, *dd = vf + nz, *gm = vf + 2 * nz;
-            for (int j = tid; j < nr; j += kAdiThreads) {
-                T y = ww[j] * ib[0];
-                ww[j] = y;
-                for (int k = 1; k < nz; ++k) {
-                    y = ww[(long long)k * nr + j] * ib[k] - dd[k] * y;
-                    ww[(long long)k * nr + j] = y;
-                }
-                T xv = y;
-                dl[(long long)(nz - 1) * nr + j] = xv;
-                for (int k = nz - 2; k >= 0; --k) {
-                    xv = ww[(long long)k * nr + j] - gm[k + 1] * xv;
-                    dl[(long long)k * nr + j] = xv;
-                }
-            }
-        }
-        __syncthreads();
-    }
-    // phi += delta in FP64; per-slot |delta|^2 and |phi|^2
-    double sd = 0.0, sp = 0.0;
-    for (long long e = tid; e < np; e += kAdiThreads) {
-        const int j = (int)(e % nr), k = (int)(e / nr);
-        double *pp = Pg + (long long)numr * (k + 1) + 1 + j;
-        const double d = (double)dl[e];
-        const double ph = *pp + d;
-        *pp = ph;
-        sd += d * d;
-        sp += ph * ph;
-    }
-    const int lane = tid & 31, warp = tid >> 5;
-    for (int off = 16; off > 0; off >>= 1) {
-        sd += __shfl_down_sync(0xffffffffu, sd, off);
-        sp += __shfl_down_sync(0xffffffffu, sp, off);
-    }
-    __shared__ double red[2 * (kAdiThreads / 32)];
-    if (lane == 0) {
-        red[2 * warp] = sd;
-        red[2 * warp + 1] = sp;
-    }
-    __syncthreads();
-    if (tid < 2) {
-        double t = 0.0;
-        for (int w = 0; w < kAdiThreads / 32; ++w) t += red[2 * w + tid];
-        const double wgt = (s == 0 || s == a.N / 2) ? 1.0 : 2.0;
-        a.norms[2 * s + tid] = wgt * t;
-    }
-}
-
-size_t gdefect_smem(const bph_ctx *c) { return sizeof(float) * (size_t)(6 * c->nr + 3 * c->nz) + 16; }
 
 // ---------------------------------------------------------------------------
 // Segmented on-chip ADI (the fast path).  The slot's potential P and its
@@ -1564,7 +1264,7 @@ int adi_configure(bph_ctx *c) {
         if (!c->mixed_kind) c->mixed_kind = kind;
     }
     // the global-memory kernel fits every grid: the default when neither on-chip kernel does
-    c->mixed_smem_kind[BPH_MIXED_ADI_GLOBAL] = (int)gdefect_smem(c);
+    c->mixed_smem_kind[BPH_MIXED_ADI_GLOBAL] = 1;  // no shared memory: always available
     c->mixed_per_sm_kind[BPH_MIXED_ADI_GLOBAL] = 0;
     if (!c->mixed_kind) c->mixed_kind = BPH_MIXED_ADI_GLOBAL;
     if (!c->adi_mixed_threads) c->adi_mixed_threads = kAdiThreads;
@@ -1637,12 +1337,14 @@ cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_ru
         AdiArgs ai = a;
         ai.P = a.P + (long long)i * c->N * c->nplane;
         ai.R = a.R + (long long)i * c->N * c->np;
-        ++c->launches;
-        if (c->adi_smem > 0)
+        cudaError_t e;
+        if (c->adi_smem > 0) {
+            ++c->launches;
             k_adi<true><<<c->N, kAdiThreads, c->adi_smem, c->stream>>>(ai);
-        else
-            k_adi_tiled<<<c->N, kAdiThreads, tiled_smem(c), c->stream>>>(ai, c->d_W, c->d_W2);
-        cudaError_t e = cudaGetLastError();
+            e = cudaGetLastError();
+        } else {
+            e = launch_adi_large(c, sch, step0, nsteps_run, cold, ai.P, ai.R);
+        }
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -1674,8 +1376,8 @@ cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {
     void *args[] = {&a};
     if (c->mixed_kind == BPH_MIXED_ADI_GLOBAL) {
         if (!c->d_work32) return cudaErrorNotReady;  // ensure_mixed_work first
-        k_adi_gdefect<float><<<c->N, kAdiThreads, gdefect_smem(c), c->stream>>>(a, c->d_work32);
-        return cudaGetLastError();
+        --c->launches;  // counted per kernel there
+        return launch_adi_defect_large(c, sch);
     }
     const void *fn = (c->mixed_kind == BPH_MIXED_ADI_FORWARD)
                          ? seg_kernel<float, true>(c->adi_mixed_threads, c->adi_full, c->mixed_pf)

@@ -632,7 +632,7 @@ namespace bph {
 // Sum of the per-slot (num, den) pairs a norm kernel left in c->d_red.
 int ensure_mixed_work(bph_ctx *c) {
     if (c->d_work32) return BPH_OK;
-    return dev_alloc(c, &c->d_work32, (size_t)c->N * 3 * (size_t)c->np);
+    return dev_alloc(c, &c->d_work32, (size_t)c->N * 4 * (size_t)c->np);
 }
 
 static double host_ratio(const std::vector<double> &h, int N) {

@@ -149,7 +149,7 @@ struct bph_ctx {
     int mixed_smem_kind[4] = {0, 0, 0, 0};    // per kind: dynamic shared bytes (0: does not fit)
     int mixed_per_sm_kind[4] = {0, 0, 0, 0};  // per kind: resident CTAs per SM
     float mixed_tuned_us[4] = {0.f, 0.f, 0.f, 0.f};  // per kind: setup-time measurement (0: not timed)
-    float *d_work32 = nullptr;                // global-memory refinement kernel: [N][3][np] (lazy)
+    float *d_work32 = nullptr;                // global-memory refinement kernels: [4][N][np] (lazy)
     int adi_threads = 256;
     int fft_smem_fwd = 0, fft_smem_inv = 0;
     bool have_warm = false;
@@ -234,6 +234,12 @@ cudaError_t launch_adi(bph_ctx *c, const Schedule &s, int step0, int nsteps_run,
 cudaError_t launch_adi_slots(bph_ctx *c, const Schedule &s, bool cold, const int *d_slots, int nslots,
                              cudaStream_t st, bool pdl);
 cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &s);
+// Slots too large for shared memory (bph_adi_large.cu): the drop-in ADI on
+// the slot array P with source R, and one FP32 refinement cycle (work area
+// c->d_work32: r, delta and two [N][np] buffers).
+cudaError_t launch_adi_large(bph_ctx *c, const Schedule &s, int step0, int nsteps_run, bool cold, double *P,
+                             const double *R);
+cudaError_t launch_adi_defect_large(bph_ctx *c, const Schedule &s);
 cudaError_t launch_update_norm(bph_ctx *c, double *d_out);
 cudaError_t launch_residual_norm(bph_ctx *c, double *d_out);
 
