@@ -316,6 +316,97 @@ def serve_bench(B, torch, dev, rhos, args):
     return out
 
 
+MIXED_GRIDS = [(66, 66, 64, 1.0 / 62.0), (130, 98, 128, 1.0 / 126.0), (130, 98, 256, 1.0 / 126.0),
+               (258, 194, 256, 1.0 / 250.0)]
+
+
+def mixed_grid_bench(B, torch, dev, args, stream):
+    """Independent warm solves on a mix of grids: instances drawn uniformly over
+    MIXED_GRIDS with mass ratio U(0.2,1), separation U(0.6,1) and core jump
+    U(1.5,3).  One batch per grid, all recorded as one plan (one graph launch,
+    the grids' branches concurrent), against the same batches called one after
+    another on one stream."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from bipoly_hydro_b200 import fields
+
+    rng = np.random.default_rng(20261203)
+    n = args.mixed_grid_instances
+    shape_of = rng.integers(0, len(MIXED_GRIDS), n)
+    params = [(int(g), float(rng.uniform(0.2, 1.0)), float(rng.uniform(0.6, 1.0)), float(rng.uniform(1.5, 3.0)))
+              for g in shape_of]
+
+    def make(p):
+        g, q, a, cj = p
+        numr, numz, numphi, dr = MIXED_GRIDS[g]
+        return fields.bipolytrope_pair(numr, numz, numphi, dr, 2, mass_ratio=q, separation=a, core_jump=cj)
+
+    with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        fields_ = list(ex.map(make, params))
+    solvers, batches, parts, counts = [], [], [], []
+    t0 = time.perf_counter()
+    for g, (numr, numz, numphi, dr) in enumerate(MIXED_GRIDS):
+        idx = [i for i in range(n) if shape_of[i] == g]
+        if not idx:
+            continue
+        sv = B.PotentialSolver(numr, numz, numphi, dr, 2, 30)
+        sv.set_stream(stream)
+        bt = B.Batch(sv, len(idx))
+        d_rho = [torch.from_numpy(np.ascontiguousarray(fields_[i].ravel(order="F"))).to(dev) for i in idx]
+        d_pot = [torch.empty_like(x) for x in d_rho]
+        solvers.append(sv)
+        batches.append(bt)
+        parts.append((bt, d_rho, d_pot))
+        counts.append(len(idx))
+    setup_s = time.perf_counter() - t0
+    del fields_
+    calls = max(3, args.mixed_grid_calls)
+    ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    # the same batches called in turn on one stream
+    for bt, r, p in parts:
+        bt.solve_device(r, p, 0)
+    for w in range(3):
+        for bt, r, p in parts:
+            bt.solve_device(r, p, 2 + w)
+    torch.cuda.synchronize()
+    ea.record(stream)
+    for k in range(calls):
+        for bt, r, p in parts:
+            bt.solve_device(r, p, 5 + k)
+    eb.record(stream)
+    torch.cuda.synchronize()
+    ms_serial = ea.elapsed_time(eb) / calls
+
+    plan = B.Plan(parts)
+    plan.launch(0, stream)
+    for w in range(3):
+        plan.launch(2 + w, stream)
+    plan.synchronize(stream)
+    torch.cuda.synchronize()
+    ea.record(stream)
+    for k in range(calls):
+        plan.launch(5 + k, stream)
+    eb.record(stream)
+    plan.synchronize(stream)
+    ms_plan = ea.elapsed_time(eb) / calls
+    launches = plan.launches
+    plan.close()
+    for bt in batches:
+        bt.close()
+    for sv in solvers:
+        sv.close()
+    del parts
+    torch.cuda.empty_cache()
+    return {"instances": n, "per_grid": {f"{a}x{b}x{c}": k for (a, b, c, _), k in
+                                         zip([MIXED_GRIDS[g] for g in range(len(MIXED_GRIDS))
+                                              if any(shape_of == g)], counts)},
+            "plan_solves_per_s": n / (ms_plan / 1e3), "plan_ms_per_launch": ms_plan,
+            "plan_kernel_launches": launches,
+            "serial_batches_solves_per_s": n / (ms_serial / 1e3), "serial_ms_per_round": ms_serial,
+            "setup_s": setup_s, "precision": "f64 drop-in (5 warm ADI steps)", "calls": calls}
+
+
 def run_gpu(args, world, rank, local):
     import torch
 
@@ -490,6 +581,11 @@ def run_gpu(args, world, rank, local):
             del outs
             bt.close()
 
+    # ---- batches over a mix of grids, one plan launch ------------------
+    mixed_grid = None
+    if args.mixed_grid_instances > 0:
+        mixed_grid = mixed_grid_bench(B, torch, dev, args, stream)
+
     # ---- serving: Poisson arrivals of SCF-like client requests ----------
     serving = None
     if args.serve_rates and not args.no_serving:
@@ -570,6 +666,7 @@ def run_gpu(args, world, rank, local):
             "phase_ms": phases,
             "converged": conv,
             "batched": batched,
+            "mixed_grid_batches": mixed_grid,
             "serving": serving,
             "graph_replay": graph_replay,
             "launch_config": solver_info,
@@ -592,6 +689,9 @@ def main():
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
     ap.add_argument("--batch-sizes", default="4,16", help="batched warm solves timed per batch size (empty skips)")
     ap.add_argument("--batch-calls", type=int, default=20)
+    ap.add_argument("--mixed-grid-instances", type=int, default=96,
+                    help="instances of the mixed-grid plan section (0 skips)")
+    ap.add_argument("--mixed-grid-calls", type=int, default=10)
     ap.add_argument("--serve-rates", default="200,1000,4000",
                     help="offered request rates (req/s) of the serving section (empty skips)")
     ap.add_argument("--serve-clients", type=int, default=64)

@@ -17,13 +17,14 @@ from .solver import (  # noqa: F401
     Grid,
     PotentialSolver,
     Batch,
+    Plan,
     Server,
     load_library,
     version,
 )
 
 __all__ = [
-    "PotentialSolver", "Batch", "Server", "Grid", "BphError", "load_library", "version", "LIB_PATH", "EXPORTED_SYMBOLS",
+    "PotentialSolver", "Batch", "Plan", "Server", "Grid", "BphError", "load_library", "version", "LIB_PATH", "EXPORTED_SYMBOLS",
     "BPH_OK", "BPH_ERR_INVALID", "BPH_ERR_NOMEM", "BPH_ERR_NONFINITE", "BPH_ERR_CUDA", "BPH_ERR_TIMEOUT",
     "BPH_ERR_STATE",
 ]

@@ -21,6 +21,9 @@
 // bank-conflict free.
 #include <cstdint>
 #include <cstdlib>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "bph_internal.cuh"
 
@@ -1184,6 +1187,20 @@ const void *delta_kernel(int threads, bool full) {
     return full ? (const void *)k_adi_delta<512, true> : (const void *)k_adi_delta<512, false>;
 }
 
+cudaError_t raise_smem_limit(const void *fn, int bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, int> limit;  // (device, kernel) -> bytes set
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    int &cur = limit[{dev, fn}];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
 int adi_configure(bph_ctx *c) {
     int dev_max = 0;
     cudaError_t e = cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
@@ -1213,12 +1230,11 @@ int adi_configure(bph_ctx *c) {
         c->adi_seg = threads;
         c->adi_pf = pf_fp64 && seg_pf_bytes <= (size_t)dev_max;
         c->adi_smem = (int)(c->adi_pf ? seg_pf_bytes : seg_bytes);
-        e = cudaFuncSetAttribute(seg_kernel<double, false>(c->adi_seg, c->adi_full, c->adi_pf),
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, c->adi_smem);
+        e = raise_smem_limit(seg_kernel<double, false>(c->adi_seg, c->adi_full, c->adi_pf), c->adi_smem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_adi_seg)");
     } else if (onchip <= (size_t)dev_max) {
         c->adi_smem = (int)onchip;
-        e = cudaFuncSetAttribute(k_adi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, c->adi_smem);
+        e = raise_smem_limit((const void *)k_adi<true>, c->adi_smem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_adi)");
     }
     // FP32 refinement kernels: the forwarding form (k_adi_seg<float>) and the
@@ -1234,9 +1250,9 @@ int adi_configure(bph_ctx *c) {
             int occ_pf = 0, occ = 0;
             const void *fpf = seg_kernel<float, true>(threads, c->adi_full, true);
             const void *fno = seg_kernel<float, true>(threads, c->adi_full, false);
-            e = cudaFuncSetAttribute(fpf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pf_bytes);
+            e = raise_smem_limit(fpf, (int)pf_bytes);
             if (e == cudaSuccess) e = cudaFuncSetAttribute(fpf, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-            if (e == cudaSuccess) e = cudaFuncSetAttribute(fno, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mixed_bytes);
+            if (e == cudaSuccess) e = raise_smem_limit(fno, (int)mixed_bytes);
             if (e == cudaSuccess) e = cudaFuncSetAttribute(fno, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
             if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_pf, fpf, threads, (int)pf_bytes);
             if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fno, threads, (int)mixed_bytes);
@@ -1254,7 +1270,7 @@ int adi_configure(bph_ctx *c) {
         if (bytes > (size_t)dev_max || items > 512) continue;
         const void *fn = (kind == BPH_MIXED_ADI_FORWARD) ? seg_kernel<float, true>(threads, c->adi_full, c->mixed_pf)
                                                          : delta_kernel(threads, c->adi_full);
-        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        e = raise_smem_limit(fn, (int)bytes);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(refinement ADI)");
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->mixed_per_sm_kind[kind], fn, threads, (int)bytes);

@@ -37,13 +37,32 @@ struct Large {
     const double *P;        // slot array for the Dirichlet frame; nullptr: zero frame
     const double *rad, *ver;
     const double *elz, *alphar, *betar;
+    const int *inst_map;    // batches: instance of each row of N slots (nullptr: row = instance)
     int numr, numz, nr, nz, N, isym;
     double gamma, dt;
     int step, cold;
 };
 
+// blockIdx.y = row * N + slot; the slot picks coefficients and factors,
+// the instance (through the map) the data, the row the scratch W/Q.
+struct Where {
+    int sl;             // slot within its instance
+    long long sg;       // slot index of the data arrays (instance * N + slot)
+    long long sw;       // slot index of the scratch arrays
+};
+
 template <typename T>
-__device__ __forceinline__ T phi_at(const Large<T> &a, int s, int k, int j) {
+__device__ __forceinline__ Where where(const Large<T> &a) {
+    Where w;
+    const int row = blockIdx.y / a.N;
+    w.sl = blockIdx.y % a.N;
+    w.sg = (long long)(a.inst_map ? a.inst_map[row] : row) * a.N + w.sl;
+    w.sw = blockIdx.y;
+    return w;
+}
+
+template <typename T>
+__device__ __forceinline__ T phi_at(const Large<T> &a, long long s, int k, int j) {
     return a.phi[s * a.phi_slot + a.phi_off + (long long)k * a.phi_row + j];
 }
 
@@ -51,7 +70,9 @@ __device__ __forceinline__ T phi_at(const Large<T> &a, int s, int k, int j) {
 template <typename T>
 __global__ void __launch_bounds__(kTileThreads) k_large_rhs_r(Large<T> a) {
     __shared__ T tile[kT][kT + 1];
-    const int s = blockIdx.y, tj = (a.nr + kT - 1) / kT;
+    const Where wh = where(a);
+    const long long s = wh.sg;
+    const int tj = (a.nr + kT - 1) / kT;
     const int k0 = (blockIdx.x / tj) * kT, j0 = (blockIdx.x % tj) * kT;
     const long long np = (long long)a.nr * a.nz, nplane = (long long)a.numr * a.numz;
     const double *Pg = a.P ? a.P + s * nplane : nullptr;
@@ -75,20 +96,21 @@ __global__ void __launch_bounds__(kTileThreads) k_large_rhs_r(Large<T> a) {
     __syncthreads();
     for (int e = threadIdx.x; e < kT * kT; e += kTileThreads) {
         const int jl = e / kT, kl = e % kT, k = k0 + kl, j = j0 + jl;
-        if (k < a.nz && j < a.nr) a.W[s * np + (long long)j * a.nz + k] = tile[kl][jl];
+        if (k < a.nz && j < a.nr) a.W[wh.sw * np + (long long)j * a.nz + k] = tile[kl][jl];
     }
 }
 
 // radial lines: thread (slot, k), W (layout B) -> Q (layout B)
 template <typename T>
 __global__ void __launch_bounds__(kLineThreads) k_large_lines_r(Large<T> a) {
-    const int s = blockIdx.y, k = blockIdx.x * kLineThreads + threadIdx.x;
+    const Where wh = where(a);
+    const int k = blockIdx.x * kLineThreads + threadIdx.x;
     if (k >= a.nz) return;
     const int nr = a.nr, nz = a.nz;
     const long long np = (long long)nr * nz;
-    const double *f = a.rad + ((long long)a.step * a.N + s) * kAdiFactors * nr;
+    const double *f = a.rad + ((long long)a.step * a.N + wh.sl) * kAdiFactors * nr;
     const double *ib = f, *dd = f + nr, *gm = f + 2 * nr;
-    T *w = a.W + s * np + k, *q = a.Q + s * np + k;
+    T *w = a.W + wh.sw * np + k, *q = a.Q + wh.sw * np + k;
     T y = w[0] * (T)ib[0];
     w[0] = y;
 #pragma unroll 4
@@ -109,13 +131,15 @@ __global__ void __launch_bounds__(kLineThreads) k_large_lines_r(Large<T> a) {
 template <typename T>
 __global__ void __launch_bounds__(kTileThreads) k_large_rhs_z(Large<T> a) {
     __shared__ T tile[kT][kT + 1];
-    const int s = blockIdx.y, tj = (a.nr + kT - 1) / kT;
+    const Where wh = where(a);
+    const long long s = wh.sg;
+    const int tj = (a.nr + kT - 1) / kT;
     const int k0 = (blockIdx.x / tj) * kT, j0 = (blockIdx.x % tj) * kT;
     const long long np = (long long)a.nr * a.nz, nplane = (long long)a.numr * a.numz;
     const double *Pg = a.P ? a.P + s * nplane : nullptr;
     const bool sym_bottom = (a.isym != 1);
     const T dt = (T)a.dt, g = (T)a.gamma;
-    const T *Q = a.Q + s * np;
+    const T *Q = a.Q + wh.sw * np;
     for (int e = threadIdx.x; e < kT * kT; e += kTileThreads) {
         const int jl = e / kT, kl = e % kT, k = k0 + kl, j = j0 + jl;
         if (k >= a.nz || j >= a.nr) continue;
@@ -123,7 +147,7 @@ __global__ void __launch_bounds__(kTileThreads) k_large_rhs_z(Large<T> a) {
         T right;
         if (j + 1 < a.nr) right = qc[a.nz];
         else right = Pg ? (T)Pg[(a.numr - 1) + (long long)a.numr * (k + 1)] : (T)0;
-        T v = ((T)a.elz[(long long)s * a.numr + j + 1] + dt) * qc[0] - (T)a.alphar[j + 1] * right;
+        T v = ((T)a.elz[(long long)wh.sl * a.numr + j + 1] + dt) * qc[0] - (T)a.alphar[j + 1] * right;
         if (j > 0) v = v - (T)a.betar[j + 1] * qc[-a.nz];
         tile[jl][kl] = v;
     }
@@ -134,21 +158,22 @@ __global__ void __launch_bounds__(kTileThreads) k_large_rhs_z(Large<T> a) {
         T v = a.src[s * np + (long long)k * a.nr + j] + tile[jl][kl];
         if (Pg && k == a.nz - 1) v = v + g * (T)Pg[(j + 1) + (long long)a.numr * (a.numz - 1)];
         if (Pg && !sym_bottom && k == 0) v = v + g * (T)Pg[j + 1];
-        a.W[s * np + (long long)k * a.nr + j] = v;
+        a.W[wh.sw * np + (long long)k * a.nr + j] = v;
     }
 }
 
 // vertical lines: thread (slot, j), W (layout A) -> phi (layout A)
 template <typename T>
 __global__ void __launch_bounds__(kLineThreads) k_large_lines_z(Large<T> a) {
-    const int s = blockIdx.y, j = blockIdx.x * kLineThreads + threadIdx.x;
+    const Where wh = where(a);
+    const int j = blockIdx.x * kLineThreads + threadIdx.x;
     if (j >= a.nr) return;
     const int nr = a.nr, nz = a.nz;
     const long long np = (long long)nr * nz;
     const double *f = a.ver + (long long)a.step * kAdiFactors * nz;
     const double *ib = f, *dd = f + nz, *gm = f + 2 * nz;
-    T *w = a.W + s * np + j;
-    T *p = a.phi + s * a.phi_slot + a.phi_off + j;
+    T *w = a.W + wh.sw * np + j;
+    T *p = a.phi + wh.sg * a.phi_slot + a.phi_off + j;
     T y = w[0] * (T)ib[0];
     w[0] = y;
 #pragma unroll 4
@@ -170,12 +195,14 @@ __global__ void __launch_bounds__(kLineThreads) k_large_lines_z(Large<T> a) {
 template <typename T>
 __global__ void __launch_bounds__(kTileThreads) k_large_b_to_a(Large<T> a) {
     __shared__ T tile[kT][kT + 1];
-    const int s = blockIdx.y, tj = (a.nr + kT - 1) / kT;
+    const Where wh = where(a);
+    const long long s = wh.sg;
+    const int tj = (a.nr + kT - 1) / kT;
     const int k0 = (blockIdx.x / tj) * kT, j0 = (blockIdx.x % tj) * kT;
     const long long np = (long long)a.nr * a.nz;
     for (int e = threadIdx.x; e < kT * kT; e += kTileThreads) {
         const int jl = e / kT, kl = e % kT, k = k0 + kl, j = j0 + jl;
-        if (k < a.nz && j < a.nr) tile[jl][kl] = a.Q[s * np + (long long)j * a.nz + k];
+        if (k < a.nz && j < a.nr) tile[jl][kl] = a.Q[wh.sw * np + (long long)j * a.nz + k];
     }
     __syncthreads();
     for (int e = threadIdx.x; e < kT * kT; e += kTileThreads) {
@@ -249,17 +276,18 @@ __global__ void __launch_bounds__(256) k_large_defect_epilogue(double *__restric
 }
 
 template <typename T>
-cudaError_t half_step(bph_ctx *c, Large<T> a, bool radial) {
+cudaError_t half_step(bph_ctx *c, Large<T> a, bool radial, int ninst) {
     const int tiles = ((c->nr + kT - 1) / kT) * ((c->nz + kT - 1) / kT);
+    const unsigned rows = (unsigned)(c->N * ninst);
     c->launches += 2;
     if (radial) {
-        k_large_rhs_r<T><<<dim3((unsigned)tiles, (unsigned)c->N), kTileThreads, 0, c->stream>>>(a);
-        k_large_lines_r<T><<<dim3((unsigned)((c->nz + kLineThreads - 1) / kLineThreads), (unsigned)c->N),
-                             kLineThreads, 0, c->stream>>>(a);
+        k_large_rhs_r<T><<<dim3((unsigned)tiles, rows), kTileThreads, 0, c->stream>>>(a);
+        k_large_lines_r<T><<<dim3((unsigned)((c->nz + kLineThreads - 1) / kLineThreads), rows), kLineThreads, 0,
+                             c->stream>>>(a);
     } else {
-        k_large_rhs_z<T><<<dim3((unsigned)tiles, (unsigned)c->N), kTileThreads, 0, c->stream>>>(a);
-        k_large_lines_z<T><<<dim3((unsigned)((c->nr + kLineThreads - 1) / kLineThreads), (unsigned)c->N),
-                             kLineThreads, 0, c->stream>>>(a);
+        k_large_rhs_z<T><<<dim3((unsigned)tiles, rows), kTileThreads, 0, c->stream>>>(a);
+        k_large_lines_z<T><<<dim3((unsigned)((c->nr + kLineThreads - 1) / kLineThreads), rows), kLineThreads, 0,
+                             c->stream>>>(a);
     }
     return cudaGetLastError();
 }
@@ -285,24 +313,26 @@ Large<T> base_args(bph_ctx *c, const Schedule &sch) {
 }  // namespace
 
 cudaError_t launch_adi_large(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bool cold, double *P,
-                             const double *R) {
+                             const double *R, int ninst, const int *d_inst_map, double *W, double *Q) {
     Large<double> a = base_args<double>(c, sch);
     a.phi = P;
     a.phi_slot = c->nplane;
     a.phi_off = c->g.numr + 1;
     a.phi_row = c->g.numr;
     a.src = R;
-    a.W = c->d_W;
-    a.Q = c->d_W2;
+    a.W = W ? W : c->d_W;
+    a.Q = Q ? Q : c->d_W2;
     a.P = P;
+    a.inst_map = d_inst_map;
+    if (ninst < 1 || (long long)ninst * c->N > 65535) return cudaErrorInvalidConfiguration;  // grid.y limit
     cudaError_t e = cudaSuccess;
     for (int it = 0; it < nsteps_run && e == cudaSuccess; ++it) {
         a.step = step0 + it;
         a.dt = sch.h_dt[a.step];
         a.cold = (cold && it == 0) ? 1 : 0;
-        e = half_step(c, a, true);
+        e = half_step(c, a, true, ninst);
         a.cold = 0;
-        if (e == cudaSuccess) e = half_step(c, a, false);
+        if (e == cudaSuccess) e = half_step(c, a, false, ninst);
     }
     return e;
 }
@@ -333,7 +363,7 @@ cudaError_t launch_adi_defect_large(bph_ctx *c, const Schedule &sch) {
         const int it = radial ? (h / 2 - 1 > 0 ? h / 2 - 1 : 0) : (h - 1) / 2;
         a.step = it;
         a.dt = sch.h_dt[it];
-        e = half_step(c, a, radial);
+        e = half_step(c, a, radial, 1);
     }
     if (e == cudaSuccess) {
         const int tiles = ((c->nr + kT - 1) / kT) * ((c->nz + kT - 1) / kT);

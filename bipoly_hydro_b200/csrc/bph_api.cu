@@ -504,6 +504,7 @@ int set_device_of(bph_ctx *c) {
 }  // namespace
 
 int batch_schedule(bph_ctx *c, int nsteps, Schedule **out) { return get_schedule(c, nsteps, out); }
+int context_status(bph_ctx *c) { return read_status(c); }
 
 }  // namespace bph
 

@@ -42,6 +42,7 @@ struct bph_batch {
     int *d_stat = nullptr;     // [cap] non-finite flag of each batch position (host-array calls)
     int *h_stat = nullptr;     // [cap] pinned host copy
     int stage_cap = 0;         // positions of the host-array staging buffers
+    double *d_LW = nullptr, *d_LQ = nullptr;  // grid-wide ADI scratch [cap][N][np] (large slots)
     double *d_cpart = nullptr;        // split-K partial sums of k_contract_batch
     unsigned int *d_ccnt = nullptr;   // its arrival counters [mmax][row groups]
     bool own_contract = true;         // k_contract_batch for up to kBatchOwnMax positions
@@ -231,6 +232,8 @@ int blas_fail(cublasStatus_t st, const char *what) {
 
 // Schedules are shared with the single-solve path (bph_api.cu).
 int batch_schedule(bph_ctx *c, int nsteps, Schedule **out);
+int batch_enqueue(bph_batch *b, int n, const double *const *d_in, double *const *d_out, const int *d_map,
+                  Schedule &sch, bool warm, bool per_pos);
 
 }  // namespace bph
 
@@ -248,14 +251,20 @@ int bph_batch_create(bph_ctx_t *c, int capacity, bph_batch_t **out) {
         set_error("invalid context or capacity (1..4096)");
         return BPH_ERR_INVALID;
     }
-    if (!c->adi_seg) {
-        set_error("batched solves need the on-chip ADI kernel (grid too large)");
+    const bool large = !c->adi_seg;  // slots beyond shared memory: the grid-wide kernels
+    if (large && c->adi_smem) {
+        set_error("batched solves need the segmented or the grid-wide ADI kernels for this grid");
+        return BPH_ERR_INVALID;
+    }
+    if (large && (long long)capacity * c->N > 65535) {
+        set_error("batch capacity %d too large for the grid-wide ADI kernels (capacity * numphi <= 65535)", capacity);
         return BPH_ERR_INVALID;
     }
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
     size_t need = sizeof(double) * (size_t)capacity *
-                  ((size_t)c->N * c->nplane + (size_t)c->N * c->np + 2ull * c->g.mmax * c->np + 2ull * c->g.mmax * c->nb);
+                  ((size_t)c->N * c->nplane + (size_t)c->N * c->np * (large ? 3 : 1) + 2ull * c->g.mmax * c->np +
+                   2ull * c->g.mmax * c->nb);
     size_t free_b = 0, total_b = 0;
     e = cudaMemGetInfo(&free_b, &total_b);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemGetInfo");
@@ -271,6 +280,8 @@ int bph_batch_create(bph_ctx_t *c, int capacity, bph_batch_t **out) {
     if (!rc) rc = batch_alloc(b, &b->d_R, (size_t)capacity * c->N * c->np);
     if (!rc) rc = batch_alloc(b, &b->d_mom, (size_t)c->g.mmax * capacity * 2 * c->np);
     if (!rc) rc = batch_alloc(b, &b->d_C, (size_t)c->g.mmax * 2 * capacity * c->nb);
+    if (!rc && large) rc = batch_alloc(b, &b->d_LW, (size_t)capacity * c->N * c->np);
+    if (!rc && large) rc = batch_alloc(b, &b->d_LQ, (size_t)capacity * c->N * c->np);
     if (!rc && (c->np % 2 == 0)) {
         // split-K scratch of k_contract_batch: partial sums for the widest case
         // (8 columns) and arrival counters for the narrowest row groups (16 rows)
@@ -328,7 +339,7 @@ int bph_batch_destroy(bph_batch_t *b) {
     if (b->c) cudaSetDevice(b->c->device);
     if (b->c && b->c->stream) cudaStreamSynchronize(b->c->stream);
     if (b->blas) cublasDestroy(b->blas);
-    double *bufs[] = {b->d_P, b->d_R, b->d_mom, b->d_C, b->d_rho_stage, b->d_pot_stage, b->d_cpart};
+    double *bufs[] = {b->d_P, b->d_R, b->d_mom, b->d_C, b->d_rho_stage, b->d_pot_stage, b->d_cpart, b->d_LW, b->d_LQ};
     for (double *p : bufs)
         if (p) cudaFree(p);
     if (b->d_ccnt) cudaFree(b->d_ccnt);
@@ -444,6 +455,38 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
     const int *d_map = instances ? reinterpret_cast<const int *>(db + 2 * sizeof(void *) * b->cap) : nullptr;
     // per-position non-finite flags: host-array calls and callers that want per-position status
     const bool per_pos = !on_device || pos_status;
+    if ((rc = batch_enqueue(b, n, d_in, d_out, d_map, *s, warm, per_pos))) return rc;
+    BPH_CUDA(cudaEventRecord(b->tab_ev[tk], c->stream));
+    if (per_pos) {
+        if (!on_device)
+            for (int i = 0; i < n; ++i)
+                BPH_CUDA(cudaMemcpyAsync(pot[i], d_pot[i], bytes, cudaMemcpyDeviceToHost, c->stream));
+        BPH_CUDA(cudaMemcpyAsync(b->h_stat, b->d_stat, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream));
+        BPH_CUDA(cudaStreamSynchronize(c->stream));
+        int bad = -1;
+        for (int i = 0; i < n; ++i) {
+            const bool nf = (b->h_stat[i] & kStatusNonFinite) != 0;
+            if (pos_status) pos_status[i] = nf ? BPH_ERR_NONFINITE : BPH_OK;
+            if (nf && bad < 0) bad = i;
+        }
+        if (bad >= 0 && !pos_status) {
+            set_error("density of batch position %d contains NaN or Inf", bad);
+            return BPH_ERR_NONFINITE;
+        }
+        return BPH_OK;
+    }
+    return BPH_OK;
+}
+
+// The device work of one batched call on c->stream: n positions whose input
+// and output arrays (and instances, d_map; nullptr: position = instance) are
+// read from device tables.  per_pos: non-finite flags per position in d_stat
+// (else the context's aggregated status).  Host-synchronisation free, so that
+// it can be captured into a graph.
+int batch_enqueue(bph_batch *b, int n, const double *const *d_in, double *const *d_out, const int *d_map,
+                  Schedule &sch, bool warm, bool per_pos) {
+    bph_ctx *c = b->c;
+    Schedule *s = &sch;
     if (per_pos) BPH_CUDA(cudaMemsetAsync(b->d_stat, 0, sizeof(int) * n, c->stream));
     const long long np = c->np;
     const long long mstride = 2LL * b->cap * np;
@@ -477,27 +520,11 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
             (double)c->N * c->factor, n, b->cap, d_map);
         BPH_CUDA(cudaGetLastError());
     }
-    BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, !warm, b->d_P, b->d_R, n, d_map));
+    if (c->adi_seg)
+        BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, !warm, b->d_P, b->d_R, n, d_map));
+    else
+        BPH_CUDA(launch_adi_large(c, *s, 0, s->nsteps, !warm, b->d_P, b->d_R, n, d_map, b->d_LW, b->d_LQ));
     BPH_CUDA(launch_fft_inv_batch(c, n, d_out, d_map, b->d_P, (long long)c->N * c->nplane));
-    BPH_CUDA(cudaEventRecord(b->tab_ev[tk], c->stream));
-    if (per_pos) {
-        if (!on_device)
-            for (int i = 0; i < n; ++i)
-                BPH_CUDA(cudaMemcpyAsync(pot[i], d_pot[i], bytes, cudaMemcpyDeviceToHost, c->stream));
-        BPH_CUDA(cudaMemcpyAsync(b->h_stat, b->d_stat, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream));
-        BPH_CUDA(cudaStreamSynchronize(c->stream));
-        int bad = -1;
-        for (int i = 0; i < n; ++i) {
-            const bool nf = (b->h_stat[i] & kStatusNonFinite) != 0;
-            if (pos_status) pos_status[i] = nf ? BPH_ERR_NONFINITE : BPH_OK;
-            if (nf && bad < 0) bad = i;
-        }
-        if (bad >= 0 && !pos_status) {
-            set_error("density of batch position %d contains NaN or Inf", bad);
-            return BPH_ERR_NONFINITE;
-        }
-        return BPH_OK;
-    }
     return BPH_OK;
 }
 
@@ -506,5 +533,221 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
 extern "C" {
 
 size_t bph_batch_device_bytes(const bph_batch_t *b) { return b ? b->bytes : 0; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Plans: the device work of several batches (one per grid shape) recorded as
+// one CUDA graph.  Capture forks from a private stream into one stream per
+// part (each part's work is batch_enqueue on its context, unchanged), joins
+// back, and instantiates; a launch replays the graph on the caller's stream.
+// The position tables are written once at creation (the arrays are fixed).
+struct bph_plan {
+    int device = 0;
+    std::vector<bph_batch *> parts;
+    std::vector<int> counts;
+    std::vector<void *> d_tab;          // per part: [in counts[p]][out counts[p]] device pointers
+    std::vector<cudaStream_t> streams;  // per part (capture only)
+    std::vector<cudaEvent_t> joins;     // per part
+    cudaEvent_t fork = nullptr;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};  // cold, warm
+    std::vector<long long> build_id[2];            // schedules captured, per kind and part
+    std::vector<long long> launches_part;          // kernel launches of each part per replay
+    int launches = 0;
+};
+
+namespace bph {
+
+static int plan_record(bph_plan *pl, bool warm) {
+    const int np_ = (int)pl->parts.size();
+    // schedules first: building one synchronises, which capture forbids
+    std::vector<Schedule *> sch((size_t)np_);
+    for (int p = 0; p < np_; ++p) {
+        int rc = batch_schedule(pl->parts[(size_t)p]->c, warm ? 5 : 20, &sch[(size_t)p]);
+        if (rc) return rc;
+    }
+    cudaStream_t cs = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate(plan capture)");
+    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) e = cudaEventRecord(pl->fork, cs);
+    int rc = BPH_OK;
+    std::vector<long long> counted((size_t)np_, 0);
+    for (int p = 0; p < np_ && e == cudaSuccess && rc == BPH_OK; ++p) {
+        bph_batch *b = pl->parts[(size_t)p];
+        bph_ctx *c = b->c;
+        cudaStream_t sp = pl->streams[(size_t)p];
+        e = cudaStreamWaitEvent(sp, pl->fork, 0);
+        if (e != cudaSuccess) break;
+        cudaStream_t keep = c->stream;
+        const bool keep_pdl = c->pdl;
+        const long long before = c->launches;
+        c->stream = sp;
+        c->pdl = false;  // plain edges: each branch starts after an event node
+        const char *db = static_cast<const char *>(pl->d_tab[(size_t)p]);
+        const int n = pl->counts[(size_t)p];
+        rc = batch_enqueue(b, n, reinterpret_cast<const double *const *>(db),
+                           reinterpret_cast<double *const *>(db + sizeof(void *) * (size_t)n), nullptr,
+                           *sch[(size_t)p], warm, false);
+        counted[(size_t)p] = c->launches - before;
+        c->launches = before;
+        c->stream = keep;
+        c->pdl = keep_pdl;
+        if (rc == BPH_OK) e = cudaEventRecord(pl->joins[(size_t)p], sp);
+        if (e == cudaSuccess && rc == BPH_OK) e = cudaStreamWaitEvent(cs, pl->joins[(size_t)p], 0);
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(cs, &g);
+    if (e == cudaSuccess) e = ee;
+    cudaGraphExec_t exec = nullptr;
+    if (e == cudaSuccess && rc == BPH_OK) e = cudaGraphInstantiate(&exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    cudaStreamDestroy(cs);
+    if (rc != BPH_OK) {
+        cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        return rc;
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        return cuda_fail(e, "plan graph capture");
+    }
+    const int k = warm ? 1 : 0;
+    if (pl->exec[k]) cudaGraphExecDestroy(pl->exec[k]);
+    pl->exec[k] = exec;
+    pl->build_id[k].clear();
+    for (Schedule *x : sch) pl->build_id[k].push_back(x->build_id);
+    pl->launches_part = counted;
+    long long tot = 0;
+    for (long long v : counted) tot += v;
+    pl->launches = (int)tot;
+    return BPH_OK;
+}
+
+}  // namespace bph
+
+extern "C" {
+
+int bph_plan_destroy(bph_plan_t *pl) {
+    if (!pl) return BPH_OK;
+    cudaSetDevice(pl->device);
+    for (cudaGraphExec_t &x : pl->exec)
+        if (x) cudaGraphExecDestroy(x);
+    for (void *t : pl->d_tab)
+        if (t) cudaFree(t);
+    for (cudaStream_t s : pl->streams)
+        if (s) cudaStreamDestroy(s);
+    for (cudaEvent_t ev : pl->joins)
+        if (ev) cudaEventDestroy(ev);
+    if (pl->fork) cudaEventDestroy(pl->fork);
+    delete pl;
+    return BPH_OK;
+}
+
+int bph_plan_create(int nparts, bph_batch_t *const *batches, const int *counts, const double *const *const *rho,
+                    double *const *const *pot, bph_plan_t **out) {
+    if (!out) {
+        set_error("out-pointer is NULL");
+        return BPH_ERR_INVALID;
+    }
+    *out = nullptr;
+    if (nparts < 1 || nparts > 256 || !batches || !counts || !rho || !pot) {
+        set_error("invalid plan arguments (1..256 parts, non-NULL arrays)");
+        return BPH_ERR_INVALID;
+    }
+    for (int p = 0; p < nparts; ++p) {
+        const bph_batch *b = batches[p];
+        if (!b || counts[p] < 1 || counts[p] > b->cap || !rho[p] || !pot[p]) {
+            set_error("plan part %d: NULL batch or arrays, or count outside 1..capacity", p);
+            return BPH_ERR_INVALID;
+        }
+        if (b->c->device != batches[0]->c->device) {
+            set_error("plan part %d lives on device %d, part 0 on %d", p, b->c->device, batches[0]->c->device);
+            return BPH_ERR_INVALID;
+        }
+        for (int q = 0; q < p; ++q)
+            if (batches[q] == b || batches[q]->c == b->c) {
+                set_error("plan parts %d and %d share a batch or a context", q, p);
+                return BPH_ERR_INVALID;
+            }
+        for (int i = 0; i < counts[p]; ++i)
+            if (!rho[p][i] || !pot[p][i]) {
+                set_error("plan part %d position %d has a NULL array", p, i);
+                return BPH_ERR_INVALID;
+            }
+    }
+    bph_plan *pl = new bph_plan();
+    pl->device = batches[0]->c->device;
+    cudaError_t e = cudaSetDevice(pl->device);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pl->fork, cudaEventDisableTiming);
+    for (int p = 0; p < nparts && e == cudaSuccess; ++p) {
+        pl->parts.push_back(batches[p]);
+        pl->counts.push_back(counts[p]);
+        const int n = counts[p];
+        std::vector<const void *> h((size_t)2 * n);
+        for (int i = 0; i < n; ++i) {
+            h[(size_t)i] = rho[p][i];
+            h[(size_t)(n + i)] = pot[p][i];
+        }
+        void *d = nullptr;
+        e = cudaMalloc(&d, sizeof(void *) * h.size());
+        pl->d_tab.push_back(d);
+        if (e == cudaSuccess) e = cudaMemcpy(d, h.data(), sizeof(void *) * h.size(), cudaMemcpyHostToDevice);
+        cudaStream_t s = nullptr;
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        pl->streams.push_back(s);
+        cudaEvent_t ev = nullptr;
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        pl->joins.push_back(ev);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        bph_plan_destroy(pl);
+        return cuda_fail(e, "plan creation");
+    }
+    *out = pl;
+    return BPH_OK;
+}
+
+int bph_plan_launch(bph_plan_t *pl, int tstep, void *stream) {
+    if (!pl) {
+        set_error("plan is NULL");
+        return BPH_ERR_INVALID;
+    }
+    BPH_CUDA(cudaSetDevice(pl->device));
+    const bool warm = tstep > 1;
+    const int k = warm ? 1 : 0;
+    // a schedule rebuilt since the recording invalidates the graph
+    bool stale = !pl->exec[k];
+    for (size_t p = 0; p < pl->parts.size() && !stale; ++p) {
+        Schedule *x = nullptr;
+        const int rc = batch_schedule(pl->parts[p]->c, warm ? 5 : 20, &x);
+        if (rc) return rc;
+        stale = x->build_id != pl->build_id[k][p];
+    }
+    int rc;
+    if (stale && (rc = plan_record(pl, warm))) return rc;
+    BPH_CUDA(cudaGraphLaunch(pl->exec[k], (cudaStream_t)stream));
+    for (size_t p = 0; p < pl->parts.size(); ++p) pl->parts[p]->c->launches += pl->launches_part[p];
+    return BPH_OK;
+}
+
+int bph_plan_synchronize(bph_plan_t *pl, void *stream) {
+    if (!pl) {
+        set_error("plan is NULL");
+        return BPH_ERR_INVALID;
+    }
+    BPH_CUDA(cudaSetDevice(pl->device));
+    BPH_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    int worst = BPH_OK;
+    for (bph_batch *b : pl->parts) {
+        const int rc = context_status(b->c);
+        if (rc && !worst) worst = rc;
+    }
+    return worst;
+}
+
+int bph_plan_launches(const bph_plan_t *pl) { return pl ? pl->launches : 0; }
 
 }  // extern "C"

@@ -237,8 +237,11 @@ cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &s);
 // Slots too large for shared memory (bph_adi_large.cu): the drop-in ADI on
 // the slot array P with source R, and one FP32 refinement cycle (work area
 // c->d_work32: r, delta and two [N][np] buffers).
+// ninst instances (row i -> instance d_inst_map[i]); W, Q: scratch of
+// ninst * N * np doubles each (nullptr: the context's, one instance).
 cudaError_t launch_adi_large(bph_ctx *c, const Schedule &s, int step0, int nsteps_run, bool cold, double *P,
-                             const double *R);
+                             const double *R, int ninst = 1, const int *d_inst_map = nullptr, double *W = nullptr,
+                             double *Q = nullptr);
 cudaError_t launch_adi_defect_large(bph_ctx *c, const Schedule &s);
 cudaError_t launch_update_norm(bph_ctx *c, double *d_out);
 cudaError_t launch_residual_norm(bph_ctx *c, double *d_out);
@@ -254,6 +257,13 @@ void conv_graphs_free(bph_ctx *c);
 // BPH_OK / BPH_ERR_NONFINITE) or host arrays the call is synchronous.
 int batch_solve_core(bph_batch *b, int n, const int *instances, const double *const *rho, double *const *pot,
                      bool warm, bool on_device, int *pos_status);
+// Raises the dynamic shared memory limit of kernel fn on the current device
+// to at least bytes.  The limit is a process-wide property of the kernel
+// while contexts of different grids share kernels, so it only ever grows
+// (a context set up later with a smaller need must not lower it).
+cudaError_t raise_smem_limit(const void *fn, int bytes);
+// Reads and clears the context's device status word (synchronises its stream).
+int context_status(bph_ctx *c);
 // Makes kind (BPH_MIXED_ADI_FORWARD / _INCREMENT) the refinement ADI kernel.
 int select_mixed_kind(bph_ctx *c, int kind);
 // Work area of the global-memory refinement kernel (allocated on first use).

@@ -154,16 +154,17 @@ int bph_server_create(bph_ctx_t *c, int max_clients, size_t mem_cap_bytes, int m
         return BPH_ERR_INVALID;
     }
     const bool dev = (flags & BPH_SERVER_DEVICE_ARRAYS) != 0;
-    if (!c->adi_seg) {
-        set_error("serving needs the on-chip ADI kernel (grid too large)");
+    if (!c->adi_seg && c->adi_smem) {
+        set_error("serving needs the segmented or the grid-wide ADI kernels for this grid");
         return BPH_ERR_INVALID;
     }
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
     // resident bytes of one client: slot array, -4 pi rho_hat, moments and
     // contraction output of its batch position, host-array staging (rho, pot)
-    const size_t per = sizeof(double) * ((size_t)c->N * c->nplane + (size_t)c->N * c->np + 2ull * c->g.mmax * c->np +
-                                         2ull * c->g.mmax * c->nb + (dev ? 0ull : 2ull * c->ntot));
+    const size_t per = sizeof(double) * ((size_t)c->N * c->nplane + (size_t)c->N * c->np * (c->adi_seg ? 1 : 3) +
+                                         2ull * c->g.mmax * c->np + 2ull * c->g.mmax * c->nb +
+                                         (dev ? 0ull : 2ull * c->ntot));
     size_t free_b = 0, total_b = 0;
     e = cudaMemGetInfo(&free_b, &total_b);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemGetInfo");
@@ -171,6 +172,7 @@ int bph_server_create(bph_ctx_t *c, int max_clients, size_t mem_cap_bytes, int m
     size_t budget = free_b > margin ? free_b - margin : 0;
     if (mem_cap_bytes && mem_cap_bytes < budget) budget = mem_cap_bytes;
     long long fit = (long long)(budget / per);
+    if (!c->adi_seg && fit > 65535 / c->N) fit = 65535 / c->N;  // grid-wide ADI: capacity * numphi <= 65535
     const int cap = (int)(fit < max_clients ? fit : max_clients);
     if (cap < 1) {
         set_error("no client fits: %zu bytes per client, budget %zu", per, budget);

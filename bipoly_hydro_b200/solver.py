@@ -47,7 +47,8 @@ EXPORTED_SYMBOLS = (
     "bph_version", "bph_num_boundary_rows", "bph_copy_green", "bph_copy_moments", "bph_run_phase",
     "bph_green_contract_noalloc", "bph_info", "bph_configure", "bph_launch_count", "bph_device_bytes",
     "bph_batch_create", "bph_batch_solve", "bph_batch_solve_instances", "bph_batch_destroy",
-    "bph_batch_device_bytes",
+    "bph_batch_device_bytes", "bph_plan_create", "bph_plan_launch", "bph_plan_synchronize", "bph_plan_launches",
+    "bph_plan_destroy",
     "bph_server_create", "bph_server_capacity", "bph_server_open_client", "bph_server_close_client",
     "bph_server_submit", "bph_server_poll", "bph_server_wait", "bph_server_stats", "bph_server_destroy",
 )
@@ -139,6 +140,15 @@ def load_library(path: str | None = None):
     for name in ("bph_server_create", "bph_server_capacity", "bph_server_open_client", "bph_server_close_client",
                  "bph_server_submit", "bph_server_poll", "bph_server_wait", "bph_server_stats",
                  "bph_server_destroy"):
+        getattr(L, name).restype = ctypes.c_int
+    L.bph_plan_create.argtypes = [i, ctypes.POINTER(vp), ctypes.POINTER(i), ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                  ctypes.POINTER(vp)]
+    L.bph_plan_launch.argtypes = [vp, i, vp]
+    L.bph_plan_synchronize.argtypes = [vp, vp]
+    L.bph_plan_launches.argtypes = [vp]
+    L.bph_plan_destroy.argtypes = [vp]
+    for name in ("bph_plan_create", "bph_plan_launch", "bph_plan_synchronize", "bph_plan_launches",
+                 "bph_plan_destroy"):
         getattr(L, name).restype = ctypes.c_int
     L.bph_batch_device_bytes.argtypes = [vp]
     L.bph_batch_device_bytes.restype = ctypes.c_size_t
@@ -368,12 +378,15 @@ class Batch:
         self.solver = solver
         self._lib = solver._lib
         self.capacity = int(capacity)
+        self._dependents = weakref.WeakSet()  # plans recording this batch
         solver._dependents.add(self)
         h = ctypes.c_void_p()
         _check(self._lib.bph_batch_create(solver._h, self.capacity, ctypes.byref(h)))
         self._h = h
 
     def close(self) -> None:
+        for dep in list(getattr(self, "_dependents", ())):
+            dep.close()
         if getattr(self, "_h", None):
             self._lib.bph_batch_destroy(self._h)
             self._h = None
@@ -415,6 +428,62 @@ class Batch:
     @property
     def device_bytes(self) -> int:
         return int(self._lib.bph_batch_device_bytes(self._h))
+
+
+class Plan:
+    """Batches on several grids recorded as one CUDA graph (bph_plan_*).
+
+    ``parts`` is a list of ``(batch, d_rhos, d_pots)``: each batch on its own
+    solver (grid), with device arrays (CUDA tensors or pointers) that stay
+    fixed; refill the densities between launches.  ``launch`` replays every
+    part's solves concurrently on ``stream`` (None: the default stream).
+    """
+
+    def __init__(self, parts):
+        self._lib = parts[0][0]._lib
+        self._keep = [(b, list(r), list(p)) for b, r, p in parts]  # arrays stay alive with the plan
+        n = len(parts)
+        batches = (ctypes.c_void_p * n)(*[b._h.value for b, _, _ in parts])
+        counts = (ctypes.c_int * n)(*[len(r) for _, r, _ in parts])
+        self._rows = [((ctypes.c_void_p * len(r))(*[_dev_ptr(x) for x in r]),
+                       (ctypes.c_void_p * len(pp))(*[_dev_ptr(x) for x in pp])) for _, r, pp in parts]
+        if any(len(r) != len(pp) for _, r, pp in parts):
+            raise ValueError("every part needs as many potentials as densities")
+        rho = (ctypes.c_void_p * n)(*[ctypes.cast(a, ctypes.c_void_p).value for a, _ in self._rows])
+        pot = (ctypes.c_void_p * n)(*[ctypes.cast(b, ctypes.c_void_p).value for _, b in self._rows])
+        h = ctypes.c_void_p()
+        _check(self._lib.bph_plan_create(n, batches, counts, rho, pot, ctypes.byref(h)))
+        self._h = h
+        for b, _, _ in parts:
+            b._dependents.add(self)
+
+    @staticmethod
+    def _stream(stream):
+        if stream is None:
+            return None
+        return ctypes.c_void_p(getattr(stream, "cuda_stream", stream))
+
+    def launch(self, tstep: int, stream=None) -> None:
+        _check(self._lib.bph_plan_launch(self._h, int(tstep), self._stream(stream)))
+
+    def synchronize(self, stream=None) -> None:
+        _check(self._lib.bph_plan_synchronize(self._h, self._stream(stream)))
+
+    @property
+    def launches(self) -> int:
+        """Kernel launches in one replay."""
+        return int(self._lib.bph_plan_launches(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.bph_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 BPH_PENDING = 1

@@ -131,6 +131,29 @@ int bph_batch_solve_instances(bph_batch_t *batch, int n, const int *instances, c
 int bph_batch_destroy(bph_batch_t *batch);
 size_t bph_batch_device_bytes(const bph_batch_t *batch);
 
+/* ---- plans: batches on several grids as one graph launch -------------
+ *
+ * No counterpart in the reference.  A plan records the device work of
+ * several batches (typically one per grid shape, each batch on its own
+ * context) into one CUDA graph whose branches run concurrently, so that a
+ * mixed set of small and large grids fills the GPU and costs one launch.
+ * Part p solves instances 0..counts[p]-1 of batches[p], reading
+ * rho[p][i] and writing pot[p][i]: DEVICE arrays fixed at creation (refill
+ * them between launches).  The contexts must live on one device and must
+ * not be used by other calls while a launch of the plan runs. */
+typedef struct bph_plan bph_plan_t;
+int bph_plan_create(int nparts, bph_batch_t *const *batches, const int *counts, const double *const *const *rho,
+                    double *const *const *pot, bph_plan_t **plan);
+/* Asynchronous replay on `stream` (a cudaStream_t, NULL = default stream):
+ * every instance of every part at this tstep (warm 5 steps if tstep > 1,
+ * else cold 20; one graph per kind, recorded on first use). */
+int bph_plan_launch(bph_plan_t *plan, int tstep, void *stream);
+/* Waits for the launches on `stream` and reports non-finite densities. */
+int bph_plan_synchronize(bph_plan_t *plan, void *stream);
+/* Kernel launches one replay makes (both kinds record the same count). */
+int bph_plan_launches(const bph_plan_t *plan);
+int bph_plan_destroy(bph_plan_t *plan);
+
 /* ---- serving: continuous batching (no counterpart in the reference) ----
  *
  * A server drives one context from a worker thread (make no other call on
