@@ -1279,8 +1279,10 @@ int adi_configure(bph_ctx *c) {
         c->adi_mixed_threads = threads;
         if (!c->mixed_kind) c->mixed_kind = kind;
     }
-    // the global-memory kernel fits every grid: the default when neither on-chip kernel does
-    c->mixed_smem_kind[BPH_MIXED_ADI_GLOBAL] = 1;  // no shared memory: always available
+    int rc = large_configure(c);
+    if (rc) return rc;
+    // the grid-wide kernels fit every practical grid: the default when neither on-chip kernel does
+    c->mixed_smem_kind[BPH_MIXED_ADI_GLOBAL] = c->large_kb[1] ? 1 : 0;
     c->mixed_per_sm_kind[BPH_MIXED_ADI_GLOBAL] = 0;
     if (!c->mixed_kind) c->mixed_kind = BPH_MIXED_ADI_GLOBAL;
     if (!c->adi_mixed_threads) c->adi_mixed_threads = kAdiThreads;

@@ -1,18 +1,23 @@
 // bph_adi_large.cu -- ADI for slots too large for shared memory.
 //
 // When a slot's slabs exceed an SM's shared memory (e.g. 258 x 194 x 512),
-// each half-sweep is two grid-wide kernels over every slot at once instead
-// of one CTA per slot:
-//   k_large_rhs_r / k_large_rhs_z  the half-sweep's right-hand side, tile by
-//       tile (32 x 32) through shared memory; reading one layout and writing
-//       the other is where the data changes layout;
-//   k_large_lines_r / k_large_lines_z  the line solves (tridagr / tridagz),
-//       one thread per line over all slots.
-// The potential stays in layout A ([k][j], j contiguous: the slot array);
-// the radial half-sweep works in layout B ([j][k]) so that consecutive
-// threads always read consecutive addresses: radial lines run along j with
-// the threads on consecutive k, vertical lines along k with the threads on
-// consecutive j.
+// the slots are cut into panels instead of one CTA per slot.  Every array
+// stays in layout A ([k][j], j contiguous), and each half-sweep is ONE
+// grid-wide kernel that also produces the next half-sweep's right-hand side:
+//   k_large_radial    CTA = (slot, kKB consecutive rows k): loads the radial
+//       right-hand side rows (contiguous), solves the r-lines in shared
+//       memory (tridagr, a thread per line), then writes the vertical
+//       right-hand side of the same rows (it needs q at j-1, j, j+1, all in
+//       the CTA) -- or the result, after the last half-sweep;
+//   k_large_vertical  CTA = (slot, kJB consecutive columns j): loads the
+//       vertical right-hand side (row segments of kJB), solves the z-lines
+//       (tridagz), then writes the next step's radial right-hand side (it
+//       needs phi at k-1, k, k+1 of the same column) -- or the potential.
+//   k_large_rhs0      the first radial right-hand side, from the warm
+//       potential (zero when cold).
+// Per step and zone: 8 bytes in, the source term and 8 bytes out per
+// kernel (48 bytes per step), against 112 for separate right-hand-side and
+// line kernels.
 //
 // The same kernels, in FP32 and with a zero Dirichlet frame, run the
 // mixed-precision refinement cycle on the defect equation (prologue: the
@@ -23,9 +28,10 @@
 namespace bph {
 namespace {
 
-constexpr int kT = 32;              // tile edge
-constexpr int kTileThreads = 256;
-constexpr int kLineThreads = 128;
+constexpr int kPanelThreads = 128;
+constexpr int kJB = 32;             // columns of a vertical panel
+constexpr int kEmit = 8;            // source loads a thread keeps in flight while emitting
+static_assert(kPanelThreads == 4 * 32, "a panel solves 32 lines in four segments, a warp each");
 
 template <typename T>
 struct Large {
@@ -33,14 +39,15 @@ struct Large {
     long long phi_slot, phi_off;
     int phi_row;
     const T *src;           // -4 pi rho_hat (drop-in) or the defect r, packed [N][nz][nr]
-    T *W, *Q;               // right-hand sides and the radial result, [N][np]
+    T *W, *Q;               // radial and vertical right-hand sides, [rows][nz][nr]
     const double *P;        // slot array for the Dirichlet frame; nullptr: zero frame
     const double *rad, *ver;
     const double *elz, *alphar, *betar;
     const int *inst_map;    // batches: instance of each row of N slots (nullptr: row = instance)
     int numr, numz, nr, nz, N, isym;
-    double gamma, dt;
-    int step, cold;
+    double gamma;
+    int kb;                 // rows of a radial panel
+    int ustride;            // shared-memory row stride of a radial panel (odd: no bank conflicts)
 };
 
 // blockIdx.y = row * N + slot; the slot picks coefficients and factors,
@@ -61,153 +68,273 @@ __device__ __forceinline__ Where where(const Large<T> &a) {
     return w;
 }
 
+// Asynchronous element copy global -> shared (no register round trip, so a
+// thread keeps all of its panel loads in flight at once).
 template <typename T>
-__device__ __forceinline__ T phi_at(const Large<T> &a, long long s, int k, int j) {
-    return a.phi[s * a.phi_slot + a.phi_off + (long long)k * a.phi_row + j];
+__device__ __forceinline__ void async_copy(T *dst, const T *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
 }
 
-// radial right-hand side (helmadi.F90:203-256): A -> B
+__device__ __forceinline__ void async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+}
+
+// Partitioned Thomas sweep with precomputed factors (tridagr.F90 /
+// tridagz.F90) on 32 lines x[0], x[st], ..., x[(n-1) st] in shared memory,
+// in place:  forward  y_i = x_i ib_i - dd_i y_{i-1},  backward  x_i = y_i -
+// gm_{i+1} x_{i+1}.  Lane l of warp w owns segment w of line l: every
+// segment solves its recurrence from a zero start while tracking the
+// product of its coefficients (the affine map of its incoming value), the
+// maps are composed across the four warps through shared memory, and a
+// second pass adds the incoming value times the running product.  Lanes of
+// a warp address one segment of 32 different lines (no bank conflicts for
+// an odd line stride).  Every thread of the CTA calls it (barriers inside);
+// lanes with active == false own empty segments.
 template <typename T>
-__global__ void __launch_bounds__(kTileThreads) k_large_rhs_r(Large<T> a) {
-    __shared__ T tile[kT][kT + 1];
-    const Where wh = where(a);
-    const long long s = wh.sg;
-    const int tj = (a.nr + kT - 1) / kT;
-    const int k0 = (blockIdx.x / tj) * kT, j0 = (blockIdx.x % tj) * kT;
-    const long long np = (long long)a.nr * a.nz, nplane = (long long)a.numr * a.numz;
-    const double *Pg = a.P ? a.P + s * nplane : nullptr;
-    const bool sym_bottom = (a.isym != 1);
-    const T dt = (T)a.dt, g = (T)a.gamma;
-    for (int e = threadIdx.x; e < kT * kT; e += kTileThreads) {
-        const int kl = e / kT, jl = e % kT, k = k0 + kl, j = j0 + jl;
-        if (k >= a.nz || j >= a.nr) continue;
-        const T phi = a.cold ? (T)0 : phi_at(a, s, k, j);
-        T up, dn;
-        if (k + 1 < a.nz) up = a.cold ? (T)0 : phi_at(a, s, k + 1, j);
-        else up = Pg ? (T)Pg[(j + 1) + (long long)a.numr * (a.numz - 1)] : (T)0;
-        if (k > 0) dn = a.cold ? (T)0 : phi_at(a, s, k - 1, j);
-        else dn = (Pg && !sym_bottom) ? (T)Pg[j + 1] : (T)0;
-        const T r = a.src[s * np + (long long)k * a.nr + j];
-        T v = (k == 0 && sym_bottom) ? r + (dt - g) * phi + g * up : r + (dt - (T)2 * g) * phi + g * (up + dn);
-        if (j == a.nr - 1 && Pg)
-            v = v - (T)a.alphar[a.numr - 2] * (T)Pg[(a.numr - 1) + (long long)a.numr * (k + 1)];
-        tile[kl][jl] = v;
+__device__ __forceinline__ void thomas4(T *x, int st, int n, const T *ib, const T *dd, const T *gm, bool active,
+                                        T (*sY)[32], T (*sP)[32]) {
+    const int seg = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int L = (n + 3) >> 2;
+    const int a = active ? min(n, seg * L) : 0, b = active ? min(n, a + L) : 0;
+    // forward, local: y from zero, p = product of -dd (0 once row 0 is in)
+    T y = 0, p = 1;
+#pragma unroll 4
+    for (int i = a; i < b; ++i) {
+        const T t = x[i * st] * ib[i];
+        if (i == 0) {
+            y = t;
+            p = 0;
+        } else {
+            y = t - dd[i] * y;
+            p = -dd[i] * p;
+        }
+        x[i * st] = y;
+    }
+    sY[seg][lane] = y;
+    sP[seg][lane] = p;
+    __syncthreads();
+    if (seg > 0 && a < b) {
+        T cin = 0;  // true y just below the segment: maps of segments 0..seg-1
+        for (int s = 0; s < seg; ++s) cin = sY[s][lane] + sP[s][lane] * cin;
+        T q = 1;
+#pragma unroll 4
+        for (int i = a; i < b; ++i) {
+            q = -dd[i] * q;
+            x[i * st] += q * cin;
+        }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < kT * kT; e += kTileThreads) {
-        const int jl = e / kT, kl = e % kT, k = k0 + kl, j = j0 + jl;
-        if (k < a.nz && j < a.nr) a.W[wh.sw * np + (long long)j * a.nz + k] = tile[kl][jl];
-    }
-}
-
-// radial lines: thread (slot, k), W (layout B) -> Q (layout B)
-template <typename T>
-__global__ void __launch_bounds__(kLineThreads) k_large_lines_r(Large<T> a) {
-    const Where wh = where(a);
-    const int k = blockIdx.x * kLineThreads + threadIdx.x;
-    if (k >= a.nz) return;
-    const int nr = a.nr, nz = a.nz;
-    const long long np = (long long)nr * nz;
-    const double *f = a.rad + ((long long)a.step * a.N + wh.sl) * kAdiFactors * nr;
-    const double *ib = f, *dd = f + nr, *gm = f + 2 * nr;
-    T *w = a.W + wh.sw * np + k, *q = a.Q + wh.sw * np + k;
-    T y = w[0] * (T)ib[0];
-    w[0] = y;
+    // backward, local: x from zero above the segment, q = product of -gm
+    T xl = 0, q = 1;
 #pragma unroll 4
-    for (int j = 1; j < nr; ++j) {
-        y = w[(long long)j * nz] * (T)ib[j] - (T)dd[j] * y;
-        w[(long long)j * nz] = y;
+    for (int i = b - 1; i >= a; --i) {
+        if (i == n - 1) {
+            xl = x[i * st];
+            q = 0;
+        } else {
+            xl = x[i * st] - gm[i + 1] * xl;
+            q = -gm[i + 1] * q;
+        }
+        x[i * st] = xl;
     }
-    T x = y;
-    q[(long long)(nr - 1) * nz] = x;
-#pragma unroll 4
-    for (int j = nr - 2; j >= 0; --j) {
-        x = w[(long long)j * nz] - (T)gm[j + 1] * x;
-        q[(long long)j * nz] = x;
-    }
-}
-
-// vertical right-hand side (helmadi.F90:272-340): B -> A
-template <typename T>
-__global__ void __launch_bounds__(kTileThreads) k_large_rhs_z(Large<T> a) {
-    __shared__ T tile[kT][kT + 1];
-    const Where wh = where(a);
-    const long long s = wh.sg;
-    const int tj = (a.nr + kT - 1) / kT;
-    const int k0 = (blockIdx.x / tj) * kT, j0 = (blockIdx.x % tj) * kT;
-    const long long np = (long long)a.nr * a.nz, nplane = (long long)a.numr * a.numz;
-    const double *Pg = a.P ? a.P + s * nplane : nullptr;
-    const bool sym_bottom = (a.isym != 1);
-    const T dt = (T)a.dt, g = (T)a.gamma;
-    const T *Q = a.Q + wh.sw * np;
-    for (int e = threadIdx.x; e < kT * kT; e += kTileThreads) {
-        const int jl = e / kT, kl = e % kT, k = k0 + kl, j = j0 + jl;
-        if (k >= a.nz || j >= a.nr) continue;
-        const T *qc = Q + (long long)j * a.nz + k;
-        T right;
-        if (j + 1 < a.nr) right = qc[a.nz];
-        else right = Pg ? (T)Pg[(a.numr - 1) + (long long)a.numr * (k + 1)] : (T)0;
-        T v = ((T)a.elz[(long long)wh.sl * a.numr + j + 1] + dt) * qc[0] - (T)a.alphar[j + 1] * right;
-        if (j > 0) v = v - (T)a.betar[j + 1] * qc[-a.nz];
-        tile[jl][kl] = v;
-    }
+    sY[seg][lane] = xl;
+    sP[seg][lane] = q;
     __syncthreads();
-    for (int e = threadIdx.x; e < kT * kT; e += kTileThreads) {
-        const int kl = e / kT, jl = e % kT, k = k0 + kl, j = j0 + jl;
-        if (k >= a.nz || j >= a.nr) continue;
-        T v = a.src[s * np + (long long)k * a.nr + j] + tile[jl][kl];
-        if (Pg && k == a.nz - 1) v = v + g * (T)Pg[(j + 1) + (long long)a.numr * (a.numz - 1)];
-        if (Pg && !sym_bottom && k == 0) v = v + g * (T)Pg[j + 1];
-        a.W[wh.sw * np + (long long)k * a.nr + j] = v;
+    if (seg < 3 && a < b) {
+        T cin = 0;  // true x just above the segment: maps of segments 3..seg+1
+        for (int s = 3; s > seg; --s) cin = sY[s][lane] + sP[s][lane] * cin;
+        T r = 1;
+#pragma unroll 4
+        for (int i = b - 1; i >= a; --i) {
+            r = (i == n - 1) ? (T)0 : -gm[i + 1] * r;
+            x[i * st] += r * cin;
+        }
     }
 }
 
-// vertical lines: thread (slot, j), W (layout A) -> phi (layout A)
+// Radial right-hand side at (k, j) (helmadi.F90:203-256) from phi at
+// (k-1, j), (k, j), (k+1, j) in the interior; the frame values come from P.
 template <typename T>
-__global__ void __launch_bounds__(kLineThreads) k_large_lines_z(Large<T> a) {
-    const Where wh = where(a);
-    const int j = blockIdx.x * kLineThreads + threadIdx.x;
-    if (j >= a.nr) return;
-    const int nr = a.nr, nz = a.nz;
-    const long long np = (long long)nr * nz;
-    const double *f = a.ver + (long long)a.step * kAdiFactors * nz;
-    const double *ib = f, *dd = f + nz, *gm = f + 2 * nz;
-    T *w = a.W + wh.sw * np + j;
-    T *p = a.phi + wh.sg * a.phi_slot + a.phi_off + j;
-    T y = w[0] * (T)ib[0];
-    w[0] = y;
-#pragma unroll 4
-    for (int k = 1; k < nz; ++k) {
-        y = w[(long long)k * nr] * (T)ib[k] - (T)dd[k] * y;
-        w[(long long)k * nr] = y;
-    }
-    T x = y;
-    p[(long long)(nz - 1) * a.phi_row] = x;
-#pragma unroll 4
-    for (int k = nz - 2; k >= 0; --k) {
-        x = w[(long long)k * nr] - (T)gm[k + 1] * x;
-        p[(long long)k * a.phi_row] = x;
-    }
+__device__ __forceinline__ T rhs_radial(const Large<T> &a, const double *Pg, T r, T phi, T up, T dn, int k, int j,
+                                        T dt) {
+    const bool sym_bottom = (a.isym != 1);
+    const T g = (T)a.gamma;
+    if (k + 1 >= a.nz) up = Pg ? (T)Pg[(j + 1) + (long long)a.numr * (a.numz - 1)] : (T)0;
+    if (k == 0) dn = (Pg && !sym_bottom) ? (T)Pg[j + 1] : (T)0;
+    T v = (k == 0 && sym_bottom) ? r + (dt - g) * phi + g * up : r + (dt - (T)2 * g) * phi + g * (up + dn);
+    if (j == a.nr - 1 && Pg) v = v - (T)a.alphar[a.numr - 2] * (T)Pg[(a.numr - 1) + (long long)a.numr * (k + 1)];
+    return v;
 }
 
-// Layout B -> A copy of the radial result (the refinement cycle ends on a
-// radial half-sweep, whose result is in Q).
+// First radial right-hand side of a sweep: from the potential in phi (or
+// zero when cold), element-wise.
 template <typename T>
-__global__ void __launch_bounds__(kTileThreads) k_large_b_to_a(Large<T> a) {
-    __shared__ T tile[kT][kT + 1];
+__global__ void __launch_bounds__(256) k_large_rhs0(Large<T> a, T dt, int cold) {
     const Where wh = where(a);
-    const long long s = wh.sg;
-    const int tj = (a.nr + kT - 1) / kT;
-    const int k0 = (blockIdx.x / tj) * kT, j0 = (blockIdx.x % tj) * kT;
     const long long np = (long long)a.nr * a.nz;
-    for (int e = threadIdx.x; e < kT * kT; e += kTileThreads) {
-        const int jl = e / kT, kl = e % kT, k = k0 + kl, j = j0 + jl;
-        if (k < a.nz && j < a.nr) tile[jl][kl] = a.Q[wh.sw * np + (long long)j * a.nz + k];
+    const long long e = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (e >= np) return;
+    const int k = (int)(e / a.nr), j = (int)(e % a.nr);
+    const double *Pg = a.P ? a.P + wh.sg * (long long)a.numr * a.numz : nullptr;
+    const T *ph = a.phi + wh.sg * a.phi_slot + a.phi_off + (long long)k * a.phi_row + j;
+    T phi = 0, up = 0, dn = 0;
+    if (!cold) {
+        phi = ph[0];
+        if (k + 1 < a.nz) up = ph[a.phi_row];
+        if (k > 0) dn = ph[-a.phi_row];
+    }
+    a.W[wh.sw * np + e] = rhs_radial(a, Pg, a.src[wh.sg * np + e], phi, up, dn, k, j, dt);
+}
+
+// Radial half-sweep on a panel of kb rows: W -> (r-lines) -> Q = vertical
+// right-hand side at dt_next, or -> phi when last.
+template <typename T>
+__global__ void __launch_bounds__(kPanelThreads) k_large_radial(Large<T> a, int step, T dt_next, int last) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *U = reinterpret_cast<T *>(smem_raw);
+    const Where wh = where(a);
+    const int nr = a.nr, nz = a.nz, us = a.ustride;
+    const int k0 = blockIdx.x * a.kb, kb = min(a.kb, nz - k0);
+    T *fib = U + (long long)a.kb * us, *fdd = fib + nr, *fgm = fdd + nr;
+    const long long np = (long long)nr * nz;
+    const T *Wg = a.W + wh.sw * np + (long long)k0 * nr;
+    for (int e = threadIdx.x; e < kb * nr; e += kPanelThreads) {
+        const int kl = e / nr, j = e - kl * nr;
+        async_copy(U + kl * us + j, Wg + e);
+    }
+    const double *f = a.rad + ((long long)step * a.N + wh.sl) * kAdiFactors * nr;
+    for (int j = threadIdx.x; j < nr; j += kPanelThreads) {
+        fib[j] = (T)f[j];
+        fdd[j] = (T)f[nr + j];
+        fgm[j] = (T)f[2 * nr + j];
+    }
+    async_wait_all();
+    __syncthreads();
+    {  // tridagr.F90: an r-line per lane, four segments (warps)
+        __shared__ T sY[4][32], sP[4][32];
+        const int line = threadIdx.x & 31;
+        thomas4(U + min(line, kb - 1) * us, 1, nr, fib, fdd, fgm, line < kb, sY, sP);
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < kT * kT; e += kTileThreads) {
-        const int kl = e / kT, jl = e % kT, k = k0 + kl, j = j0 + jl;
-        if (k < a.nz && j < a.nr) a.phi[s * a.phi_slot + a.phi_off + (long long)k * a.phi_row + j] = tile[jl][kl];
+    if (last) {
+        T *ph = a.phi + wh.sg * a.phi_slot + a.phi_off + (long long)k0 * a.phi_row;
+        for (int j = threadIdx.x; j < nr; j += kPanelThreads)
+            for (int kl = 0; kl < kb; ++kl) ph[(long long)kl * a.phi_row + j] = U[kl * us + j];
+        return;
+    }
+    // vertical right-hand side (helmadi.F90:272-340) of the panel's rows:
+    // a thread per column, its coefficients in registers, kEmit source rows
+    // in flight at a time
+    const double *Pg = a.P ? a.P + wh.sg * (long long)a.numr * a.numz : nullptr;
+    const bool sym_bottom = (a.isym != 1);
+    const T g = (T)a.gamma;
+    const T *sgp = a.src + wh.sg * np + (long long)k0 * nr;
+    T *Qg = a.Q + wh.sw * np + (long long)k0 * nr;
+    const double *elz = a.elz + (long long)wh.sl * a.numr;
+    for (int j = threadIdx.x; j < nr; j += kPanelThreads) {
+        const T cz = (T)elz[j + 1] + dt_next, al = (T)a.alphar[j + 1], be = (T)a.betar[j + 1];
+        const T top = Pg ? g * (T)Pg[(j + 1) + (long long)a.numr * (a.numz - 1)] : (T)0;
+        const T bot = (Pg && !sym_bottom) ? g * (T)Pg[j + 1] : (T)0;
+        for (int kl0 = 0; kl0 < kb; kl0 += kEmit) {
+            T sv[kEmit];
+#pragma unroll
+            for (int m = 0; m < kEmit; ++m) sv[m] = (kl0 + m < kb) ? sgp[(long long)(kl0 + m) * nr + j] : (T)0;
+#pragma unroll
+            for (int m = 0; m < kEmit; ++m) {
+                const int kl = kl0 + m, k = k0 + kl;
+                if (kl >= kb) break;
+                const T *qc = U + kl * us + j;
+                T right;
+                if (j + 1 < nr) right = qc[1];
+                else right = Pg ? (T)Pg[(a.numr - 1) + (long long)a.numr * (k + 1)] : (T)0;
+                T v = cz * qc[0] - al * right;
+                if (j > 0) v = v - be * qc[-1];
+                v = sv[m] + v;
+                if (k == nz - 1) v = v + top;
+                if (k == 0) v = v + bot;
+                Qg[(long long)kl * nr + j] = v;
+            }
+        }
+    }
+}
+
+// Vertical half-sweep on a panel of kJB columns: Q -> (z-lines) -> W =
+// radial right-hand side at dt_next, or -> phi when last.
+template <typename T>
+__global__ void __launch_bounds__(kPanelThreads) k_large_vertical(Large<T> a, int step, T dt_next, int last) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *V = reinterpret_cast<T *>(smem_raw);
+    constexpr int vs = kJB + 1;
+    const Where wh = where(a);
+    const int nr = a.nr, nz = a.nz;
+    const int j0 = blockIdx.x * kJB, jb = min(kJB, nr - j0);
+    T *fib = V + (long long)nz * vs, *fdd = fib + nz, *fgm = fdd + nz;
+    const long long np = (long long)nr * nz;
+    const T *Qg = a.Q + wh.sw * np + j0;
+    for (int e = threadIdx.x; e < nz * kJB; e += kPanelThreads) {
+        const int k = e / kJB, jl = e - k * kJB;
+        if (jl < jb) async_copy(V + k * vs + jl, Qg + (long long)k * nr + jl);
+    }
+    const double *f = a.ver + (long long)step * kAdiFactors * nz;
+    for (int k = threadIdx.x; k < nz; k += kPanelThreads) {
+        fib[k] = (T)f[k];
+        fdd[k] = (T)f[nz + k];
+        fgm[k] = (T)f[2 * nz + k];
+    }
+    async_wait_all();
+    __syncthreads();
+    {  // tridagz.F90: a z-line per lane, four segments (warps)
+        __shared__ T sY[4][32], sP[4][32];
+        const int line = threadIdx.x & 31;
+        thomas4(V + min(line, jb - 1), vs, nz, fib, fdd, fgm, line < jb, sY, sP);
+    }
+    __syncthreads();
+    const int jl = threadIdx.x & (kJB - 1), kg = threadIdx.x / kJB;
+    constexpr int kRowGroups = kPanelThreads / kJB;
+    if (last) {
+        if (jl < jb) {
+            T *ph = a.phi + wh.sg * a.phi_slot + a.phi_off + j0 + jl;
+            for (int k = kg; k < nz; k += kRowGroups) ph[(long long)k * a.phi_row] = V[k * vs + jl];
+        }
+        return;
+    }
+    if (jl >= jb) return;
+    // next radial right-hand side (helmadi.F90:203-256): a thread per
+    // (column, row group), kEmit source rows in flight at a time
+    const double *Pg = a.P ? a.P + wh.sg * (long long)a.numr * a.numz : nullptr;
+    const bool sym_bottom = (a.isym != 1);
+    const int j = j0 + jl;
+    const T g = (T)a.gamma, dt = dt_next;
+    const T top = Pg ? (T)Pg[(j + 1) + (long long)a.numr * (a.numz - 1)] : (T)0;
+    const T bot = (Pg && !sym_bottom) ? (T)Pg[j + 1] : (T)0;
+    const bool edge = (j == nr - 1) && Pg;
+    const T aedge = edge ? (T)a.alphar[a.numr - 2] : (T)0;
+    const T *sgp = a.src + wh.sg * np + j;
+    T *Wg = a.W + wh.sw * np + j;
+    for (int k0r = kg; k0r < nz; k0r += kEmit * kRowGroups) {
+        T sv[kEmit];
+#pragma unroll
+        for (int m = 0; m < kEmit; ++m) {
+            const int k = k0r + m * kRowGroups;
+            sv[m] = (k < nz) ? sgp[(long long)k * nr] : (T)0;
+        }
+#pragma unroll
+        for (int m = 0; m < kEmit; ++m) {
+            const int k = k0r + m * kRowGroups;
+            if (k >= nz) break;
+            const T *vc = V + k * vs + jl;
+            const T phi = vc[0];
+            const T up = (k + 1 < nz) ? vc[vs] : top;
+            const T dn = (k > 0) ? vc[-vs] : bot;
+            T v = (k == 0 && sym_bottom) ? sv[m] + (dt - g) * phi + g * up
+                                         : sv[m] + (dt - (T)2 * g) * phi + g * (up + dn);
+            if (edge) v = v - aedge * (T)Pg[(a.numr - 1) + (long long)a.numr * (k + 1)];
+            Wg[(long long)k * nr] = v;
+        }
     }
 }
 
@@ -276,20 +403,13 @@ __global__ void __launch_bounds__(256) k_large_defect_epilogue(double *__restric
 }
 
 template <typename T>
-cudaError_t half_step(bph_ctx *c, Large<T> a, bool radial, int ninst) {
-    const int tiles = ((c->nr + kT - 1) / kT) * ((c->nz + kT - 1) / kT);
-    const unsigned rows = (unsigned)(c->N * ninst);
-    c->launches += 2;
-    if (radial) {
-        k_large_rhs_r<T><<<dim3((unsigned)tiles, rows), kTileThreads, 0, c->stream>>>(a);
-        k_large_lines_r<T><<<dim3((unsigned)((c->nz + kLineThreads - 1) / kLineThreads), rows), kLineThreads, 0,
-                             c->stream>>>(a);
-    } else {
-        k_large_rhs_z<T><<<dim3((unsigned)tiles, rows), kTileThreads, 0, c->stream>>>(a);
-        k_large_lines_z<T><<<dim3((unsigned)((c->nr + kLineThreads - 1) / kLineThreads), rows), kLineThreads, 0,
-                             c->stream>>>(a);
-    }
-    return cudaGetLastError();
+size_t radial_bytes(int kb, int us, int nr) {
+    return sizeof(T) * ((size_t)kb * us + 3 * (size_t)nr);
+}
+
+template <typename T>
+size_t vertical_bytes(int nz) {
+    return sizeof(T) * ((size_t)nz * (kJB + 1) + 3 * (size_t)nz);
 }
 
 template <typename T>
@@ -307,13 +427,69 @@ Large<T> base_args(bph_ctx *c, const Schedule &sch) {
     a.N = c->N;
     a.isym = c->g.isym;
     a.gamma = c->gamma;
+    const int t = (sizeof(T) == 8) ? 0 : 1;
+    a.kb = c->large_kb[t];
+    a.ustride = c->nr | 1;
     return a;
+}
+
+// One half-sweep: radial or vertical panels over rows * N slots.
+template <typename T>
+cudaError_t panel_launch(bph_ctx *c, const Large<T> &a, bool radial, int rows, int step, double dt_next, bool last) {
+    ++c->launches;
+    if (radial) {
+        const dim3 grid((unsigned)((c->nz + a.kb - 1) / a.kb), (unsigned)rows);
+        k_large_radial<T><<<grid, kPanelThreads, radial_bytes<T>(a.kb, a.ustride, c->nr), c->stream>>>(
+            a, step, (T)dt_next, last ? 1 : 0);
+    } else {
+        const dim3 grid((unsigned)((c->nr + kJB - 1) / kJB), (unsigned)rows);
+        k_large_vertical<T><<<grid, kPanelThreads, vertical_bytes<T>(c->nz), c->stream>>>(a, step, (T)dt_next,
+                                                                                         last ? 1 : 0);
+    }
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t rhs0_launch(bph_ctx *c, const Large<T> &a, int rows, double dt, bool cold) {
+    ++c->launches;
+    const long long np = c->np;
+    k_large_rhs0<T><<<dim3((unsigned)((np + 255) / 256), (unsigned)rows), 256, 0, c->stream>>>(a, (T)dt,
+                                                                                            cold ? 1 : 0);
+    return cudaGetLastError();
+}
+
+template <typename T>
+int configure_type(bph_ctx *c, int dev_max) {
+    dev_max -= 4096;  // the kernels' static scan arrays
+    const int t = (sizeof(T) == 8) ? 0 : 1;
+    const int us = c->nr | 1;
+    int kb = 32;
+    while (kb > 1 && radial_bytes<T>(kb, us, c->nr) > (size_t)dev_max) kb /= 2;
+    if (radial_bytes<T>(kb, us, c->nr) > (size_t)dev_max || vertical_bytes<T>(c->nz) > (size_t)dev_max) {
+        c->large_kb[t] = 0;
+        return BPH_OK;
+    }
+    cudaError_t e = raise_smem_limit((const void *)k_large_radial<T>, (int)radial_bytes<T>(kb, us, c->nr));
+    if (e == cudaSuccess) e = raise_smem_limit((const void *)k_large_vertical<T>, (int)vertical_bytes<T>(c->nz));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(grid-wide ADI panels)");
+    c->large_kb[t] = kb;
+    return BPH_OK;
 }
 
 }  // namespace
 
+int large_configure(bph_ctx *c) {
+    int dev_max = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+    int rc = configure_type<double>(c, dev_max);
+    if (!rc) rc = configure_type<float>(c, dev_max);
+    return rc;
+}
+
 cudaError_t launch_adi_large(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bool cold, double *P,
                              const double *R, int ninst, const int *d_inst_map, double *W, double *Q) {
+    if (!c->large_kb[0]) return cudaErrorNotSupported;
     Large<double> a = base_args<double>(c, sch);
     a.phi = P;
     a.phi_slot = c->nplane;
@@ -325,19 +501,21 @@ cudaError_t launch_adi_large(bph_ctx *c, const Schedule &sch, int step0, int nst
     a.P = P;
     a.inst_map = d_inst_map;
     if (ninst < 1 || (long long)ninst * c->N > 65535) return cudaErrorInvalidConfiguration;  // grid.y limit
-    cudaError_t e = cudaSuccess;
+    const int rows = ninst * c->N;
+    if (nsteps_run < 1) return cudaSuccess;
+    // step i: radial (dt_i), vertical (dt_i); each emits the next right-hand side
+    cudaError_t e = rhs0_launch(c, a, rows, sch.h_dt[step0], cold);
     for (int it = 0; it < nsteps_run && e == cudaSuccess; ++it) {
-        a.step = step0 + it;
-        a.dt = sch.h_dt[a.step];
-        a.cold = (cold && it == 0) ? 1 : 0;
-        e = half_step(c, a, true, ninst);
-        a.cold = 0;
-        if (e == cudaSuccess) e = half_step(c, a, false, ninst);
+        const int st = step0 + it;
+        const bool last = (it == nsteps_run - 1);
+        e = panel_launch(c, a, true, rows, st, sch.h_dt[st], false);
+        if (e == cudaSuccess) e = panel_launch(c, a, false, rows, st, last ? 0.0 : sch.h_dt[st + 1], last);
     }
     return e;
 }
 
 cudaError_t launch_adi_defect_large(bph_ctx *c, const Schedule &sch) {
+    if (!c->large_kb[1]) return cudaErrorNotSupported;
     const long long np = c->np;
     float *r = c->d_work32, *delta = r + (long long)c->N * np, *W = delta + (long long)c->N * np,
           *Q = W + (long long)c->N * np;
@@ -356,20 +534,15 @@ cudaError_t launch_adi_defect_large(bph_ctx *c, const Schedule &sch) {
     a.W = W;
     a.Q = Q;
     a.P = nullptr;  // zero frame
-    // radial at the first step's dt, then (vertical, radial) per step
+    // half-sweeps h = 0..2n: radial at step 0, then (vertical, radial) at
+    // steps 0..n-1; each emits the next one's right-hand side at its dt
     const int nhalf = 2 * sch.nsteps + 1;
+    auto step_of = [](int h) { return (h % 2 == 0) ? (h / 2 - 1 > 0 ? h / 2 - 1 : 0) : (h - 1) / 2; };
+    if (e == cudaSuccess) e = rhs0_launch(c, a, c->N, sch.h_dt[0], true);  // delta = 0
     for (int h = 0; h < nhalf && e == cudaSuccess; ++h) {
-        const bool radial = (h % 2) == 0;
-        const int it = radial ? (h / 2 - 1 > 0 ? h / 2 - 1 : 0) : (h - 1) / 2;
-        a.step = it;
-        a.dt = sch.h_dt[it];
-        e = half_step(c, a, radial, 1);
-    }
-    if (e == cudaSuccess) {
-        const int tiles = ((c->nr + kT - 1) / kT) * ((c->nz + kT - 1) / kT);
-        ++c->launches;
-        k_large_b_to_a<float><<<dim3((unsigned)tiles, (unsigned)c->N), kTileThreads, 0, c->stream>>>(a);
-        e = cudaGetLastError();
+        const bool last = (h == nhalf - 1);
+        const double dt_next = last ? 0.0 : sch.h_dt[step_of(h + 1)];
+        e = panel_launch(c, a, (h % 2) == 0, c->N, step_of(h), dt_next, last);
     }
     if (e == cudaSuccess) {
         ++c->launches;

@@ -401,6 +401,10 @@ int setup_impl(bph_ctx *c) {
         BPH_CUDA(cudaMemsetAsync(c->d_ccnt, 0, sizeof(unsigned int) * (size_t)g.mmax * groups, c->stream));
     }
     if (c->adi_smem == 0) {
+        if (!c->large_kb[0]) {
+            set_error("grid too large: an ADI panel of one row exceeds shared memory");
+            return BPH_ERR_INVALID;
+        }
         if ((rc = dev_alloc(c, &c->d_W, (size_t)c->N * c->nplane))) return rc;
         if ((rc = dev_alloc(c, &c->d_W2, (size_t)c->N * c->np))) return rc;
     }

@@ -139,6 +139,7 @@ struct bph_ctx {
 
     int adi_smem = 0;            // dynamic shared bytes of the on-chip ADI kernel (0: global variant)
     int adi_seg = 0;             // threads of the segmented on-chip ADI kernel (0: not used)
+    int large_kb[2] = {0, 0};    // rows of a grid-wide radial ADI panel, FP64 / FP32 (0: does not fit)
     bool adi_full = false;       // both line lengths are multiples of the segment length
     bool adi_pf = false;         // FP64 segmented ADI with bulk-copy factor prefetch
     bool mixed_pf = false;       // the same for the FP32 forwarding-form refinement kernel
@@ -243,6 +244,8 @@ cudaError_t launch_adi_large(bph_ctx *c, const Schedule &s, int step0, int nstep
                              const double *R, int ninst = 1, const int *d_inst_map = nullptr, double *W = nullptr,
                              double *Q = nullptr);
 cudaError_t launch_adi_defect_large(bph_ctx *c, const Schedule &s);
+// Panel sizes and shared-memory limits of the grid-wide ADI kernels.
+int large_configure(bph_ctx *c);
 cudaError_t launch_update_norm(bph_ctx *c, double *d_out);
 cudaError_t launch_residual_norm(bph_ctx *c, double *d_out);
 
