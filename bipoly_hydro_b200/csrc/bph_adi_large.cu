@@ -79,6 +79,12 @@ __device__ __forceinline__ void async_copy(T *dst, const T *src) {
         asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
 }
 
+// Warms L2 with the 128-byte line holding p (the source rows that a panel
+// reads after its line solves: their loads then wait on L2, not DRAM).
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 __device__ __forceinline__ void async_wait_all() {
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
 }
@@ -206,6 +212,11 @@ __global__ void __launch_bounds__(kPanelThreads) k_large_radial(Large<T> a, int 
         const int kl = e / nr, j = e - kl * nr;
         async_copy(U + kl * us + j, Wg + e);
     }
+    if (!last) {
+        const char *sp = reinterpret_cast<const char *>(a.src + wh.sg * np + (long long)k0 * nr);
+        const int lines = (int)((sizeof(T) * (size_t)kb * nr + 127) / 128);
+        for (int l = threadIdx.x; l < lines; l += kPanelThreads) prefetch_l2(sp + 128 * (size_t)l);
+    }
     const double *f = a.rad + ((long long)step * a.N + wh.sl) * kAdiFactors * nr;
     for (int j = threadIdx.x; j < nr; j += kPanelThreads) {
         fib[j] = (T)f[j];
@@ -278,6 +289,16 @@ __global__ void __launch_bounds__(kPanelThreads) k_large_vertical(Large<T> a, in
     for (int e = threadIdx.x; e < nz * kJB; e += kPanelThreads) {
         const int k = e / kJB, jl = e - k * kJB;
         if (jl < jb) async_copy(V + k * vs + jl, Qg + (long long)k * nr + jl);
+    }
+    if (!last) {
+        const T *sp = a.src + wh.sg * np + j0;
+        const int per_row = (int)((sizeof(T) * (size_t)jb + 127) / 128) + 1;  // the rows need not start on a line
+        for (int l = threadIdx.x; l < nz * per_row; l += kPanelThreads) {
+            const int k = l / per_row, c = l - k * per_row;
+            const size_t start = reinterpret_cast<size_t>(sp + (long long)k * nr), end = start + sizeof(T) * jb;
+            const size_t at = c ? (start & ~(size_t)127) + 128 * (size_t)c : start;  // stays inside the row's block
+            if (at < end) prefetch_l2(reinterpret_cast<const void *>(at));
+        }
     }
     const double *f = a.ver + (long long)step * kAdiFactors * nz;
     for (int k = threadIdx.x; k < nz; k += kPanelThreads) {
