@@ -407,6 +407,64 @@ def mixed_grid_bench(B, torch, dev, args, stream):
             "setup_s": setup_s, "precision": "f64 drop-in (5 warm ADI steps)", "calls": calls}
 
 
+def large_grid_bench(B, torch, dev, args, stream):
+    """Mixed precision against FP64 on the 258x194x512 grid (dr = 1/250,
+    the bipolytrope-pair recipe of the production grid) and on the 66x66x64
+    field of two n=1 polytropes: warm drop-in rate, then converged solves
+    (FP64, and the FP32 refinement with FP64 residuals) with their error."""
+    from bipoly_hydro_b200 import fields
+
+    out = {}
+    cases = [("258x194x512", (258, 194, 512, 1.0 / 250.0),
+              lambda: fields.bipolytrope_pair(258, 194, 512, 1.0 / 250.0, 2, mass_ratio=0.5)),
+             ("66x66x64", (66, 66, 64, 1.0 / 62.0), lambda: fields.two_polytropes())]
+    for name, (numr, numz, numphi, dr), make in cases:
+        sv = B.PotentialSolver(numr, numz, numphi, dr, 2, 30)
+        sv.set_stream(stream)
+        base = make()
+        d = [torch.from_numpy(np.ascontiguousarray(fields.rotate(base, i).ravel(order="F"))).to(dev)
+             for i in range(2)]
+        pot = torch.empty_like(d[0])
+        sv.potential_solver_device(d[0], pot, 0)
+        for i in range(3):
+            sv.potential_solver_device(d[i % 2], pot, 2 + i)
+        n = 10
+        ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ea.record(stream)
+        for i in range(n):
+            sv.potential_solver_device(d[i % 2], pot, 5 + i)
+        eb.record(stream)
+        torch.cuda.synchronize()
+        ms = ea.elapsed_time(eb) / n
+        res = {"dropin_ms": ms, "dropin_solves_per_s": 1e3 / ms}
+        ref = None
+        for key, mixed in (("fp64", False), ("mixed", True)):
+            ts = []
+            for rep in range(4):  # the first builds the loop graph: untimed
+                sv.solve_converged_device(d[0], pot, args.conv_nsteps, True, 1e-13, 100, False)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                info = sv.solve_converged_device(d[1], pot, args.conv_nsteps, False, args.conv_tol, 100, mixed)
+                torch.cuda.synchronize()
+                if rep:
+                    ts.append(time.perf_counter() - t0)
+            r = {"ms": 1e3 * float(np.median(ts)), "solves_per_s": 1.0 / float(np.median(ts)),
+                 "cycles": info.cycles}
+            if mixed:
+                r["rel_err_vs_fp64"] = float(torch.linalg.norm(pot - ref) / torch.linalg.norm(ref))
+            else:
+                ref = pot.clone()
+            res[key] = r
+        res["speedup_mixed_vs_fp64"] = res["mixed"]["solves_per_s"] / res["fp64"]["solves_per_s"]
+        res["mixed_kind"] = sv.info()["mixed_kind"]
+        out[name] = res
+        sv.close()
+        del d, pot, ref
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_gpu(args, world, rank, local):
     import torch
 
@@ -581,6 +639,11 @@ def run_gpu(args, world, rank, local):
             del outs
             bt.close()
 
+    # ---- mixed precision on the large grid and the small field --------
+    large_grid = None
+    if not args.no_large_grid:
+        large_grid = large_grid_bench(B, torch, dev, args, stream)
+
     # ---- batches over a mix of grids, one plan launch ------------------
     mixed_grid = None
     if args.mixed_grid_instances > 0:
@@ -667,6 +730,7 @@ def run_gpu(args, world, rank, local):
             "converged": conv,
             "batched": batched,
             "mixed_grid_batches": mixed_grid,
+            "large_grid": large_grid,
             "serving": serving,
             "graph_replay": graph_replay,
             "launch_config": solver_info,
@@ -692,6 +756,8 @@ def main():
     ap.add_argument("--mixed-grid-instances", type=int, default=96,
                     help="instances of the mixed-grid plan section (0 skips)")
     ap.add_argument("--mixed-grid-calls", type=int, default=10)
+    ap.add_argument("--no-large-grid", action="store_true",
+                    help="skip the 258x194x512 / 66x66x64 mixed-vs-FP64 section")
     ap.add_argument("--serve-rates", default="200,1000,4000",
                     help="offered request rates (req/s) of the serving section (empty skips)")
     ap.add_argument("--serve-clients", type=int, default=64)

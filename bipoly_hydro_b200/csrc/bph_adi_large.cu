@@ -4,13 +4,14 @@
 // the slots are cut into panels instead of one CTA per slot.  Every array
 // stays in layout A ([k][j], j contiguous), and each half-sweep is ONE
 // grid-wide kernel that also produces the next half-sweep's right-hand side:
-//   k_large_radial    CTA = (slot, kKB consecutive rows k): loads the radial
-//       right-hand side rows (contiguous), solves the r-lines in shared
-//       memory (tridagr, a thread per line), then writes the vertical
+//   k_large_radial    CTA = (slot, kb consecutive rows k): loads the radial
+//       right-hand side rows (contiguous, by asynchronous copies), solves
+//       the r-lines in shared memory (tridagr, each line partitioned over
+//       several threads), then writes the vertical
 //       right-hand side of the same rows (it needs q at j-1, j, j+1, all in
 //       the CTA) -- or the result, after the last half-sweep;
-//   k_large_vertical  CTA = (slot, kJB consecutive columns j): loads the
-//       vertical right-hand side (row segments of kJB), solves the z-lines
+//   k_large_vertical  CTA = (slot, NL consecutive columns j): loads the
+//       vertical right-hand side (row segments of NL), solves the z-lines
 //       (tridagz), then writes the next step's radial right-hand side (it
 //       needs phi at k-1, k, k+1 of the same column) -- or the potential.
 //   k_large_rhs0      the first radial right-hand side, from the warm
@@ -23,15 +24,22 @@
 // mixed-precision refinement cycle on the defect equation (prologue: the
 // FP64 residual; body: radial at the first step's dt, then vertical and
 // radial per step; epilogue: phi += delta in FP64 and the per-slot norms).
+#include <cstdlib>
+
 #include "bph_internal.cuh"
 
 namespace bph {
 namespace {
 
 constexpr int kPanelThreads = 128;
-constexpr int kJB = 32;             // columns of a vertical panel
+// Lines of a panel (columns of a vertical panel, at most the rows of a
+// radial one): 16 for FP64, 32 for FP32, so that the lanes sharing a sweep
+// segment fill the shared-memory banks once.
+template <typename T>
+constexpr int panel_lines() {
+    return sizeof(T) == 8 ? 16 : 32;
+}
 constexpr int kEmit = 8;            // source loads a thread keeps in flight while emitting
-static_assert(kPanelThreads == 4 * 32, "a panel solves 32 lines in four segments, a warp each");
 
 template <typename T>
 struct Large {
@@ -90,21 +98,23 @@ __device__ __forceinline__ void async_wait_all() {
 }
 
 // Partitioned Thomas sweep with precomputed factors (tridagr.F90 /
-// tridagz.F90) on 32 lines x[0], x[st], ..., x[(n-1) st] in shared memory,
+// tridagz.F90) on NL lines x[0], x[st], ..., x[(n-1) st] in shared memory,
 // in place:  forward  y_i = x_i ib_i - dd_i y_{i-1},  backward  x_i = y_i -
-// gm_{i+1} x_{i+1}.  Lane l of warp w owns segment w of line l: every
+// gm_{i+1} x_{i+1}.  Thread t owns segment t / NL of line t % NL: every
 // segment solves its recurrence from a zero start while tracking the
 // product of its coefficients (the affine map of its incoming value), the
-// maps are composed across the four warps through shared memory, and a
-// second pass adds the incoming value times the running product.  Lanes of
-// a warp address one segment of 32 different lines (no bank conflicts for
-// an odd line stride).  Every thread of the CTA calls it (barriers inside);
-// lanes with active == false own empty segments.
-template <typename T>
-__device__ __forceinline__ void thomas4(T *x, int st, int n, const T *ib, const T *dd, const T *gm, bool active,
-                                        T (*sY)[32], T (*sP)[32]) {
-    const int seg = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int L = (n + 3) >> 2;
+// maps are composed across segments through shared memory, and a second
+// pass adds the incoming value times the running product.  The lanes that
+// share a segment address NL different lines (no bank conflicts for an odd
+// line stride: NL = 32 for 4-byte, 16 for 8-byte elements).  Every thread
+// of the CTA calls it (barriers inside); lanes with active == false own
+// empty segments.
+template <typename T, int NL>
+__device__ __forceinline__ void thomas_panel(T *x, int st, int n, const T *ib, const T *dd, const T *gm, bool active,
+                                             T (*sY)[NL], T (*sP)[NL]) {
+    constexpr int NS = kPanelThreads / NL;  // segments per line
+    const int seg = threadIdx.x / NL, lane = threadIdx.x % NL;
+    const int L = (n + NS - 1) / NS;
     const int a = active ? min(n, seg * L) : 0, b = active ? min(n, a + L) : 0;
     // forward, local: y from zero, p = product of -dd (0 once row 0 is in)
     T y = 0, p = 1;
@@ -150,9 +160,9 @@ __device__ __forceinline__ void thomas4(T *x, int st, int n, const T *ib, const 
     sY[seg][lane] = xl;
     sP[seg][lane] = q;
     __syncthreads();
-    if (seg < 3 && a < b) {
-        T cin = 0;  // true x just above the segment: maps of segments 3..seg+1
-        for (int s = 3; s > seg; --s) cin = sY[s][lane] + sP[s][lane] * cin;
+    if (seg < NS - 1 && a < b) {
+        T cin = 0;  // true x just above the segment: maps of the segments above
+        for (int s = NS - 1; s > seg; --s) cin = sY[s][lane] + sP[s][lane] * cin;
         T r = 1;
 #pragma unroll 4
         for (int i = b - 1; i >= a; --i) {
@@ -177,28 +187,28 @@ __device__ __forceinline__ T rhs_radial(const Large<T> &a, const double *Pg, T r
 }
 
 // First radial right-hand side of a sweep: from the potential in phi (or
-// zero when cold), element-wise.
+// zero when cold), element-wise; grid (j blocks, k, rows * N slots).
 template <typename T>
-__global__ void __launch_bounds__(256) k_large_rhs0(Large<T> a, T dt, int cold) {
-    const Where wh = where(a);
-    const long long np = (long long)a.nr * a.nz;
-    const long long e = (long long)blockIdx.x * 256 + threadIdx.x;
-    if (e >= np) return;
-    const int k = (int)(e / a.nr), j = (int)(e % a.nr);
-    const double *Pg = a.P ? a.P + wh.sg * (long long)a.numr * a.numz : nullptr;
-    const T *ph = a.phi + wh.sg * a.phi_slot + a.phi_off + (long long)k * a.phi_row + j;
+__global__ void __launch_bounds__(128) k_large_rhs0(Large<T> a, T dt, int cold) {
+    const int j = blockIdx.x * 128 + threadIdx.x, k = blockIdx.y;
+    if (j >= a.nr) return;
+    const int row = blockIdx.z / a.N, sl = blockIdx.z - row * a.N;
+    const long long sg = (long long)(a.inst_map ? a.inst_map[row] : row) * a.N + sl;
+    const long long np = (long long)a.nr * a.nz, e = (long long)k * a.nr + j;
+    const double *Pg = a.P ? a.P + sg * (long long)a.numr * a.numz : nullptr;
+    const T *ph = a.phi + sg * a.phi_slot + a.phi_off + (long long)k * a.phi_row + j;
     T phi = 0, up = 0, dn = 0;
     if (!cold) {
         phi = ph[0];
         if (k + 1 < a.nz) up = ph[a.phi_row];
         if (k > 0) dn = ph[-a.phi_row];
     }
-    a.W[wh.sw * np + e] = rhs_radial(a, Pg, a.src[wh.sg * np + e], phi, up, dn, k, j, dt);
+    a.W[(long long)blockIdx.z * np + e] = rhs_radial(a, Pg, a.src[sg * np + e], phi, up, dn, k, j, dt);
 }
 
 // Radial half-sweep on a panel of kb rows: W -> (r-lines) -> Q = vertical
 // right-hand side at dt_next, or -> phi when last.
-template <typename T>
+template <typename T, int NL>
 __global__ void __launch_bounds__(kPanelThreads) k_large_radial(Large<T> a, int step, T dt_next, int last) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *U = reinterpret_cast<T *>(smem_raw);
@@ -226,9 +236,9 @@ __global__ void __launch_bounds__(kPanelThreads) k_large_radial(Large<T> a, int 
     async_wait_all();
     __syncthreads();
     {  // tridagr.F90: an r-line per lane, four segments (warps)
-        __shared__ T sY[4][32], sP[4][32];
-        const int line = threadIdx.x & 31;
-        thomas4(U + min(line, kb - 1) * us, 1, nr, fib, fdd, fgm, line < kb, sY, sP);
+        __shared__ T sY[kPanelThreads / NL][NL], sP[kPanelThreads / NL][NL];
+        const int line = threadIdx.x % NL;
+        thomas_panel<T, NL>(U + min(line, kb - 1) * us, 1, nr, fib, fdd, fgm, line < kb, sY, sP);
     }
     __syncthreads();
     if (last) {
@@ -273,21 +283,21 @@ __global__ void __launch_bounds__(kPanelThreads) k_large_radial(Large<T> a, int 
     }
 }
 
-// Vertical half-sweep on a panel of kJB columns: Q -> (z-lines) -> W =
+// Vertical half-sweep on a panel of NL columns: Q -> (z-lines) -> W =
 // radial right-hand side at dt_next, or -> phi when last.
-template <typename T>
+template <typename T, int NL>
 __global__ void __launch_bounds__(kPanelThreads) k_large_vertical(Large<T> a, int step, T dt_next, int last) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *V = reinterpret_cast<T *>(smem_raw);
-    constexpr int vs = kJB + 1;
+    constexpr int vs = NL + 1;
     const Where wh = where(a);
     const int nr = a.nr, nz = a.nz;
-    const int j0 = blockIdx.x * kJB, jb = min(kJB, nr - j0);
+    const int j0 = blockIdx.x * NL, jb = min(NL, nr - j0);
     T *fib = V + (long long)nz * vs, *fdd = fib + nz, *fgm = fdd + nz;
     const long long np = (long long)nr * nz;
     const T *Qg = a.Q + wh.sw * np + j0;
-    for (int e = threadIdx.x; e < nz * kJB; e += kPanelThreads) {
-        const int k = e / kJB, jl = e - k * kJB;
+    for (int e = threadIdx.x; e < nz * NL; e += kPanelThreads) {
+        const int k = e / NL, jl = e - k * NL;
         if (jl < jb) async_copy(V + k * vs + jl, Qg + (long long)k * nr + jl);
     }
     if (!last) {
@@ -309,13 +319,13 @@ __global__ void __launch_bounds__(kPanelThreads) k_large_vertical(Large<T> a, in
     async_wait_all();
     __syncthreads();
     {  // tridagz.F90: a z-line per lane, four segments (warps)
-        __shared__ T sY[4][32], sP[4][32];
-        const int line = threadIdx.x & 31;
-        thomas4(V + min(line, jb - 1), vs, nz, fib, fdd, fgm, line < jb, sY, sP);
+        __shared__ T sY[kPanelThreads / NL][NL], sP[kPanelThreads / NL][NL];
+        const int line = threadIdx.x % NL;
+        thomas_panel<T, NL>(V + min(line, jb - 1), vs, nz, fib, fdd, fgm, line < jb, sY, sP);
     }
     __syncthreads();
-    const int jl = threadIdx.x & (kJB - 1), kg = threadIdx.x / kJB;
-    constexpr int kRowGroups = kPanelThreads / kJB;
+    const int jl = threadIdx.x % NL, kg = threadIdx.x / NL;
+    constexpr int kRowGroups = kPanelThreads / NL;
     if (last) {
         if (jl < jb) {
             T *ph = a.phi + wh.sg * a.phi_slot + a.phi_off + j0 + jl;
@@ -430,7 +440,7 @@ size_t radial_bytes(int kb, int us, int nr) {
 
 template <typename T>
 size_t vertical_bytes(int nz) {
-    return sizeof(T) * ((size_t)nz * (kJB + 1) + 3 * (size_t)nz);
+    return sizeof(T) * ((size_t)nz * (panel_lines<T>() + 1) + 3 * (size_t)nz);
 }
 
 template <typename T>
@@ -460,11 +470,12 @@ cudaError_t panel_launch(bph_ctx *c, const Large<T> &a, bool radial, int rows, i
     ++c->launches;
     if (radial) {
         const dim3 grid((unsigned)((c->nz + a.kb - 1) / a.kb), (unsigned)rows);
-        k_large_radial<T><<<grid, kPanelThreads, radial_bytes<T>(a.kb, a.ustride, c->nr), c->stream>>>(
+        k_large_radial<T, panel_lines<T>()><<<grid, kPanelThreads, radial_bytes<T>(a.kb, a.ustride, c->nr),
+                                              c->stream>>>(
             a, step, (T)dt_next, last ? 1 : 0);
     } else {
-        const dim3 grid((unsigned)((c->nr + kJB - 1) / kJB), (unsigned)rows);
-        k_large_vertical<T><<<grid, kPanelThreads, vertical_bytes<T>(c->nz), c->stream>>>(a, step, (T)dt_next,
+        const dim3 grid((unsigned)((c->nr + panel_lines<T>() - 1) / panel_lines<T>()), (unsigned)rows);
+        k_large_vertical<T, panel_lines<T>()><<<grid, kPanelThreads, vertical_bytes<T>(c->nz), c->stream>>>(a, step, (T)dt_next,
                                                                                          last ? 1 : 0);
     }
     return cudaGetLastError();
@@ -473,9 +484,8 @@ cudaError_t panel_launch(bph_ctx *c, const Large<T> &a, bool radial, int rows, i
 template <typename T>
 cudaError_t rhs0_launch(bph_ctx *c, const Large<T> &a, int rows, double dt, bool cold) {
     ++c->launches;
-    const long long np = c->np;
-    k_large_rhs0<T><<<dim3((unsigned)((np + 255) / 256), (unsigned)rows), 256, 0, c->stream>>>(a, (T)dt,
-                                                                                            cold ? 1 : 0);
+    k_large_rhs0<T><<<dim3((unsigned)((c->nr + 127) / 128), (unsigned)c->nz, (unsigned)rows), 128, 0, c->stream>>>(
+        a, (T)dt, cold ? 1 : 0);
     return cudaGetLastError();
 }
 
@@ -484,14 +494,18 @@ int configure_type(bph_ctx *c, int dev_max) {
     dev_max -= 4096;  // the kernels' static scan arrays
     const int t = (sizeof(T) == 8) ? 0 : 1;
     const int us = c->nr | 1;
-    int kb = 32;
+    int kb = panel_lines<T>();  // BPH_LARGE_ROWS=1..lines overrides (rows of a radial panel)
+    if (const char *env = std::getenv("BPH_LARGE_ROWS")) {
+        const int v = std::atoi(env);
+        if (v >= 1 && v <= panel_lines<T>()) kb = v;
+    }
     while (kb > 1 && radial_bytes<T>(kb, us, c->nr) > (size_t)dev_max) kb /= 2;
     if (radial_bytes<T>(kb, us, c->nr) > (size_t)dev_max || vertical_bytes<T>(c->nz) > (size_t)dev_max) {
         c->large_kb[t] = 0;
         return BPH_OK;
     }
-    cudaError_t e = raise_smem_limit((const void *)k_large_radial<T>, (int)radial_bytes<T>(kb, us, c->nr));
-    if (e == cudaSuccess) e = raise_smem_limit((const void *)k_large_vertical<T>, (int)vertical_bytes<T>(c->nz));
+    cudaError_t e = raise_smem_limit((const void *)k_large_radial<T, panel_lines<T>()>, (int)radial_bytes<T>(kb, us, c->nr));
+    if (e == cudaSuccess) e = raise_smem_limit((const void *)k_large_vertical<T, panel_lines<T>()>, (int)vertical_bytes<T>(c->nz));
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(grid-wide ADI panels)");
     c->large_kb[t] = kb;
     return BPH_OK;
