@@ -320,6 +320,86 @@ MIXED_GRIDS = [(66, 66, 64, 1.0 / 62.0), (130, 98, 128, 1.0 / 126.0), (130, 98, 
                (258, 194, 256, 1.0 / 250.0)]
 
 
+def serve_mixed_bench(B, torch, dev, args):
+    """Serving with the clients' grids drawn uniformly over MIXED_GRIDS: one
+    server (continuous batching, resident clients) per grid, each on its own
+    stream, the admission cap split evenly; the requests of all clients
+    arrive as one Poisson process; SCF-like sequences as in serve_bench.
+    Each grid gets two base densities (drawn q, a, core jump), scaled per
+    client."""
+    from bipoly_hydro_b200 import fields
+
+    nclients, iters = args.serve_clients, args.serve_iters
+    rng = np.random.default_rng(20261204)
+    shape_of = [int(g) for g in rng.integers(0, len(MIXED_GRIDS), nclients)]
+    servers, solvers, streams, bases = [], [], [], []
+    for g, (numr, numz, numphi, dr) in enumerate(MIXED_GRIDS):
+        sv = B.PotentialSolver(numr, numz, numphi, dr, 2, 30)
+        st = torch.cuda.Stream()
+        sv.set_stream(st)
+        n_g = max(1, shape_of.count(g))
+        servers.append(B.Server(sv, max_clients=n_g, mem_cap_bytes=150 * 10 ** 9 // len(MIXED_GRIDS),
+                                device_arrays=True))
+        solvers.append(sv)
+        streams.append(st)
+        bases.append([torch.from_numpy(np.ascontiguousarray(fields.bipolytrope_pair(
+            numr, numz, numphi, dr, 2, mass_ratio=float(rng.uniform(0.2, 1.0)),
+            separation=float(rng.uniform(0.6, 1.0)), core_jump=float(rng.uniform(1.5, 3.0))).ravel(order="F"))).to(dev)
+            for _ in range(2)])
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(20261204)
+    out = {"grids": {f"{a}x{b}x{c}": shape_of.count(g) for g, (a, b, c, _) in enumerate(MIXED_GRIDS)},
+           "clients": nclients, "requests_per_rate": nclients * iters, "dtype": "f64", "rates": []}
+    for rate in [float(x) for x in args.serve_mixed_rates.split(",") if x]:
+        ids = [servers[shape_of[c]].open_client() for c in range(nclients)]
+        rho = [[bases[shape_of[c]][c % 2] * (1.0 + 0.2 * c / nclients), None] for c in range(nclients)]
+        for r in rho:
+            r[1] = torch.empty_like(r[0])
+        mass = [float(r[0].sum()) for r in rho]
+        pot = [[torch.empty_like(r[0]), torch.empty_like(r[0])] for r in rho]
+        arrivals = np.cumsum(np.random.default_rng(int(rate)).exponential(1.0 / rate, size=nclients * iters))
+        rid, lat, lat_g = {}, [], [[] for _ in MIXED_GRIDS]
+        t0 = time.perf_counter()
+        for k in range(nclients * iters):
+            c, it = k % nclients, k // nclients
+            srv, buf = servers[shape_of[c]], it % 2
+            if it >= 2:
+                v = srv.wait(rid.pop((c, it - 2)), timeout=120.0)[1]
+                lat.append(v)
+                lat_g[shape_of[c]].append(v)
+            src = rho[c][1 - buf] if it > 0 else rho[c][0]
+            if it > 0:
+                noise = torch.randn(src.shape, generator=gen, device=dev, dtype=torch.float64)
+                nxt = src * (1.0 + 0.001 * noise)
+                rho[c][buf].copy_(nxt * (mass[c] / float(nxt.sum())))
+            else:
+                rho[c][buf] = src.clone()
+            torch.cuda.current_stream().synchronize()
+            while time.perf_counter() - t0 < arrivals[k]:
+                pass
+            rid[(c, it)] = srv.submit(ids[c], rho[c][buf], pot[c][buf])
+        for (c, it) in list(rid):
+            v = servers[shape_of[c]].wait(rid.pop((c, it)), timeout=120.0)[1]
+            lat.append(v)
+            lat_g[shape_of[c]].append(v)
+        elapsed = time.perf_counter() - t0
+        out["rates"].append({
+            "offered_req_per_s": rate, "solves_per_s": nclients * iters / elapsed,
+            "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+            "p50_ms_per_grid": {f"{a}x{b}x{c2}": (1e3 * float(np.percentile(lg, 50)) if lg else None)
+                                for (a, b, c2, _), lg in zip(MIXED_GRIDS, lat_g)}})
+        for c in range(nclients):
+            servers[shape_of[c]].close_client(ids[c])
+        del rho, pot
+    for srv in servers:
+        srv.close()
+    for sv in solvers:
+        sv.close()
+    del bases
+    torch.cuda.empty_cache()
+    return out
+
+
 def mixed_grid_bench(B, torch, dev, args, stream):
     """Independent warm solves on a mix of grids: instances drawn uniformly over
     MIXED_GRIDS with mass ratio U(0.2,1), separation U(0.6,1) and core jump
@@ -654,6 +734,10 @@ def run_gpu(args, world, rank, local):
     if args.serve_rates and not args.no_serving:
         serving = serve_bench(B, torch, dev, rhos, args)
 
+    serving_mixed = None
+    if args.serve_mixed_rates and not args.no_serving:
+        serving_mixed = serve_mixed_bench(B, torch, dev, args)
+
     # ---- converged solves: FP64 vs mixed (FP32 ADI + FP64 refinement) --
     conv = None
     if args.converged_steps > 0:
@@ -732,6 +816,7 @@ def run_gpu(args, world, rank, local):
             "mixed_grid_batches": mixed_grid,
             "large_grid": large_grid,
             "serving": serving,
+            "serving_mixed_grids": serving_mixed,
             "graph_replay": graph_replay,
             "launch_config": solver_info,
             "gpu_launches": launches,
@@ -761,6 +846,8 @@ def main():
     ap.add_argument("--serve-rates", default="200,1000,4000",
                     help="offered request rates (req/s) of the serving section (empty skips)")
     ap.add_argument("--serve-clients", type=int, default=64)
+    ap.add_argument("--serve-mixed-rates", default="100,400,1600",
+                    help="offered rates of the mixed-grid serving section (empty skips)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
     ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay section")
     ap.add_argument("--serve-iters", type=int, default=8, help="SCF-like requests per client per rate")

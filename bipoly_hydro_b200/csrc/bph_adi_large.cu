@@ -114,7 +114,9 @@ __device__ __forceinline__ void thomas_panel(T *x, int st, int n, const T *ib, c
                                              T (*sY)[NL], T (*sP)[NL]) {
     constexpr int NS = kPanelThreads / NL;  // segments per line
     const int seg = threadIdx.x / NL, lane = threadIdx.x % NL;
-    const int L = (n + NS - 1) / NS;
+    // odd segment length: the lanes of neighbouring segments read their
+    // factors (and, for a line stride of 1, their elements) from different banks
+    const int L = ((n + NS - 1) / NS) | 1;
     const int a = active ? min(n, seg * L) : 0, b = active ? min(n, a + L) : 0;
     // forward, local: y from zero, p = product of -dd (0 once row 0 is in)
     T y = 0, p = 1;
