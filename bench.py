@@ -724,6 +724,39 @@ def run_gpu(args, world, rank, local):
     if not args.no_large_grid:
         large_grid = large_grid_bench(B, torch, dev, args, stream)
 
+    # ---- converged batched solves: FP64 vs mixed ------------------------
+    batched_conv = None
+    if args.batch_sizes and args.converged_steps > 0:
+        nb_ = max(int(x) for x in args.batch_sizes.split(",") if x)
+        ins = [rhos[(7 * i) % nrot] for i in range(nb_)]
+        batched_conv = {"instances": nb_, "nsteps_per_cycle": args.conv_nsteps, "tol_update": args.conv_tol}
+        ref_outs = None
+        for key, mixed in (("fp64", False), ("mixed", True)):
+            bt = B.Batch(solver, nb_)
+            outs = [torch.empty(ntot, dtype=torch.float64, device=dev) for _ in range(nb_)]
+            bt.solve_converged_device(ins, outs, args.conv_nsteps, True, 1e-13, 100, mixed)
+            ts, cyc = [], []
+            for k in range(4):
+                ins_k = [rhos[(7 * i + k + 1) % nrot] for i in range(nb_)]
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                info = bt.solve_converged_device(ins_k, outs, args.conv_nsteps, False, args.conv_tol, 100, mixed)
+                torch.cuda.synchronize()
+                ts.append(time.perf_counter() - t0)
+                cyc.append(info.cycles)
+            r = {"solves_per_s": nb_ / float(np.median(ts)), "ms_per_call": 1e3 * float(np.median(ts)),
+                 "mean_cycles": float(np.mean(cyc))}
+            if mixed:
+                r["max_rel_err_vs_fp64"] = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+                                               for a, b in zip(outs, ref_outs))
+            else:
+                ref_outs = [o.clone() for o in outs]
+            batched_conv[key] = r
+            bt.close()
+            del outs
+        batched_conv["speedup_mixed_vs_fp64"] = batched_conv["mixed"]["solves_per_s"] / batched_conv["fp64"]["solves_per_s"]
+        del ref_outs
+
     # ---- batches over a mix of grids, one plan launch ------------------
     mixed_grid = None
     if args.mixed_grid_instances > 0:
@@ -813,6 +846,7 @@ def run_gpu(args, world, rank, local):
             "phase_ms": phases,
             "converged": conv,
             "batched": batched,
+            "batched_converged": batched_conv,
             "mixed_grid_batches": mixed_grid,
             "large_grid": large_grid,
             "serving": serving,

@@ -1120,7 +1120,8 @@ k_slot_norms(const double *__restrict__ P, const double *__restrict__ Q, const d
              const double *__restrict__ brb, const double *__restrict__ alphar, const double *__restrict__ betar,
              const double *__restrict__ bzb, double gamma, int numr, int numz, int nr, int nz, int N, int isym,
              double *__restrict__ out) {
-    const int s = blockIdx.x;
+    // blockIdx.x = instance * N + slot (instances contiguous, as in a batch)
+    const int s = blockIdx.x, sl = s % N;
     const long long nplane = (long long)numr * numz, np = (long long)nr * nz;
     const double *Ps = P + (long long)s * nplane;
     double a0 = 0.0, a1 = 0.0;
@@ -1128,7 +1129,7 @@ k_slot_norms(const double *__restrict__ P, const double *__restrict__ Q, const d
         int j = (int)(e % nr), k = (int)(e / nr);
         long long q = (j + 1) + (long long)numr * (k + 1);
         if (kResidual) {
-            const double *b = brb + (long long)s * numr;
+            const double *b = brb + (long long)sl * numr;
             double ar = b[j + 1] * Ps[q] + alphar[j + 1] * Ps[q + 1];
             if (j > 0) ar += betar[j + 1] * Ps[q - 1];
             double az = bzb[k + 1] * Ps[q] - gamma * Ps[q + numr];
@@ -1157,7 +1158,7 @@ k_slot_norms(const double *__restrict__ P, const double *__restrict__ Q, const d
     if (threadIdx.x < 2) {
         double v = 0.0;
         for (int w = 0; w < kNormThreads / 32; ++w) v += red[threadIdx.x][w];
-        double wgt = (s == 0 || s == N / 2) ? 1.0 : 2.0;
+        double wgt = (sl == 0 || sl == N / 2) ? 1.0 : 2.0;
         out[2 * s + threadIdx.x] = wgt * v;
     }
 }
@@ -1402,6 +1403,39 @@ cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {
                          : delta_kernel(c->adi_mixed_threads, c->adi_full);
     return cudaLaunchKernel(fn, dim3(c->N), dim3(c->adi_mixed_threads), args, (size_t)c->adi_mixed_smem,
                             c->stream);
+}
+
+cudaError_t launch_defect_batch(bph_ctx *c, const Schedule &sch, double *P, const double *R, int n, double *norms) {
+    if (!c->adi_mixed_smem || c->mixed_kind == BPH_MIXED_ADI_GLOBAL) return cudaErrorNotSupported;
+    AdiArgs a = make_args(c, sch, 0, sch.nsteps, false);
+    a.P = P;
+    a.R = R;
+    a.norms = norms;
+    a.rad_pk = sch.d_rad_pk[1];
+    a.ver_pk = sch.d_ver_pk[1];
+    a.pkr = packed_block<float>(c->nr);
+    a.pkz = packed_block<float>(c->nz);
+    ++c->launches;
+    void *args[] = {&a};
+    const void *fn = (c->mixed_kind == BPH_MIXED_ADI_FORWARD)
+                         ? seg_kernel<float, true>(c->adi_mixed_threads, c->adi_full, c->mixed_pf)
+                         : delta_kernel(c->adi_mixed_threads, c->adi_full);
+    return cudaLaunchKernel(fn, dim3((unsigned)(c->N * n)), dim3(c->adi_mixed_threads), args,
+                            (size_t)c->adi_mixed_smem, c->stream);
+}
+
+cudaError_t launch_norms_batch(bph_ctx *c, bool residual, const double *P, const double *prev, const double *R, int n,
+                               double *d_out) {
+    ++c->launches;
+    if (residual)
+        k_slot_norms<true><<<c->N * n, kNormThreads, 0, c->stream>>>(
+            P, prev, R, c->d_brb, c->d_alphar, c->d_betar, c->d_bzb, c->gamma, c->g.numr, c->g.numz, c->nr, c->nz,
+            c->N, c->g.isym, d_out);
+    else
+        k_slot_norms<false><<<c->N * n, kNormThreads, 0, c->stream>>>(
+            P, prev, R, c->d_brb, c->d_alphar, c->d_betar, c->d_bzb, c->gamma, c->g.numr, c->g.numz, c->nr, c->nz,
+            c->N, c->g.isym, d_out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_update_norm(bph_ctx *c, double *d_out) {

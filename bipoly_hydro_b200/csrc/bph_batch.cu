@@ -18,6 +18,7 @@
 //   k_fft_inv           per instance
 #include <cublas_v2.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <vector>
@@ -43,6 +44,9 @@ struct bph_batch {
     int *h_stat = nullptr;     // [cap] pinned host copy
     int stage_cap = 0;         // positions of the host-array staging buffers
     double *d_LW = nullptr, *d_LQ = nullptr;  // grid-wide ADI scratch [cap][N][np] (large slots)
+    double *d_prev = nullptr;         // converged FP64 solves: slot arrays of the previous cycle (on first use)
+    double *d_cnorm = nullptr;        // converged solves: per (instance, slot) norm pairs [cap][N][2]
+    double *h_cnorm = nullptr;        // its pinned host copy
     double *d_cpart = nullptr;        // split-K partial sums of k_contract_batch
     unsigned int *d_ccnt = nullptr;   // its arrival counters [mmax][row groups]
     bool own_contract = true;         // k_contract_batch for up to kBatchOwnMax positions
@@ -235,6 +239,18 @@ int batch_schedule(bph_ctx *c, int nsteps, Schedule **out);
 int batch_enqueue(bph_batch *b, int n, const double *const *d_in, double *const *d_out, const int *d_map,
                   Schedule &sch, bool warm, bool per_pos);
 
+// A converged batched call (bph_batch_solve_converged).
+struct BatchConv {
+    int nsteps = 0, max_cycles = 0;
+    bool cold = false, mixed = false;
+    double tol = 0.0;
+    int cycles = 0;           // out: cycles run
+    double resid = 0.0;       // out: largest relative FP64 residual over the instances
+    bool want_resid = false;
+};
+int batch_converged_run(bph_batch *b, int n, const double *const *d_in, double *const *d_out, BatchConv &cv,
+                        bool per_pos);
+
 }  // namespace bph
 
 using namespace bph;
@@ -339,7 +355,8 @@ int bph_batch_destroy(bph_batch_t *b) {
     if (b->c) cudaSetDevice(b->c->device);
     if (b->c && b->c->stream) cudaStreamSynchronize(b->c->stream);
     if (b->blas) cublasDestroy(b->blas);
-    double *bufs[] = {b->d_P, b->d_R, b->d_mom, b->d_C, b->d_rho_stage, b->d_pot_stage, b->d_cpart, b->d_LW, b->d_LQ};
+    double *bufs[] = {b->d_P,     b->d_R,     b->d_mom, b->d_C,    b->d_rho_stage, b->d_pot_stage,
+                      b->d_cpart, b->d_LW,    b->d_LQ,  b->d_prev, b->d_cnorm};
     for (double *p : bufs)
         if (p) cudaFree(p);
     if (b->d_ccnt) cudaFree(b->d_ccnt);
@@ -350,6 +367,7 @@ int bph_batch_destroy(bph_batch_t *b) {
     }
     if (b->d_stat) cudaFree(b->d_stat);
     if (b->h_stat) cudaFreeHost(b->h_stat);
+    if (b->h_cnorm) cudaFreeHost(b->h_cnorm);
     delete b;
     return BPH_OK;
 }
@@ -363,6 +381,31 @@ int bph_batch_solve_instances(bph_batch_t *b, int n, const int *instances, const
     return bph::batch_solve_core(b, n, instances, rho, pot, tstep > 1, on_device != 0, nullptr);
 }
 
+int bph_batch_solve_converged(bph_batch_t *b, int n, const double *const *rho, double *const *pot, int nsteps,
+                              int cold, double tol, int max_cycles, int mixed, int on_device, int *cycles_out,
+                              double *resid_out) {
+    if (!b || nsteps < 1 || nsteps > 10000 || max_cycles < 1 || !(tol >= 0.0)) {
+        set_error("invalid arguments");
+        return BPH_ERR_INVALID;
+    }
+    bph_ctx *c = b->c;
+    if (mixed && (!c->adi_mixed_smem || c->mixed_kind == BPH_MIXED_ADI_GLOBAL)) {
+        set_error("mixed batched solves need an on-chip refinement kernel (this grid's slots exceed shared memory)");
+        return BPH_ERR_INVALID;
+    }
+    BatchConv cv;
+    cv.nsteps = nsteps;
+    cv.max_cycles = max_cycles;
+    cv.cold = cold != 0;
+    cv.mixed = mixed != 0;
+    cv.tol = tol;
+    cv.want_resid = resid_out != nullptr;
+    const int rc = bph::batch_solve_core(b, n, nullptr, rho, pot, !cold, on_device != 0, nullptr, &cv);
+    if (cycles_out) *cycles_out = cv.cycles;
+    if (resid_out) *resid_out = cv.resid;
+    return rc;
+}
+
 }  // extern "C"
 
 namespace bph {
@@ -370,7 +413,7 @@ namespace bph {
 // pos_status (host arrays only): per-position BPH_OK / BPH_ERR_NONFINITE
 // instead of one aggregated status.
 int batch_solve_core(bph_batch *b, int n, const int *instances, const double *const *rho, double *const *pot,
-                     bool warm, bool on_device, int *pos_status) {
+                     bool warm, bool on_device, int *pos_status, BatchConv *conv) {
     if (!b || !rho || !pot || n < 1 || n > b->cap) {
         set_error("invalid batch arguments (n must be in 1..capacity)");
         return BPH_ERR_INVALID;
@@ -395,8 +438,12 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
     bph_ctx *c = b->c;
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
-    Schedule *s;  // warm: 5 steps, cold: 20 (potential_solver.F90:80-94)
-    int rc = batch_schedule(c, warm ? 5 : 20, &s);
+    if (conv && instances) {
+        set_error("converged batched solves take instances 0..n-1");
+        return BPH_ERR_INVALID;
+    }
+    Schedule *s;  // warm: 5 steps, cold: 20 (potential_solver.F90:80-94); converged: its cycle length
+    int rc = batch_schedule(c, conv ? conv->nsteps : (warm ? 5 : 20), &s);
     if (rc) return rc;
     const size_t bytes = sizeof(double) * (size_t)c->ntot;
     std::vector<int> inst(n);
@@ -455,7 +502,11 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
     const int *d_map = instances ? reinterpret_cast<const int *>(db + 2 * sizeof(void *) * b->cap) : nullptr;
     // per-position non-finite flags: host-array calls and callers that want per-position status
     const bool per_pos = !on_device || pos_status;
-    if ((rc = batch_enqueue(b, n, d_in, d_out, d_map, *s, warm, per_pos))) return rc;
+    if (conv)
+        rc = batch_converged_run(b, n, d_in, d_out, *conv, per_pos);
+    else
+        rc = batch_enqueue(b, n, d_in, d_out, d_map, *s, warm, per_pos);
+    if (rc) return rc;
     BPH_CUDA(cudaEventRecord(b->tab_ev[tk], c->stream));
     if (per_pos) {
         if (!on_device)
@@ -483,10 +534,10 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
 // read from device tables.  per_pos: non-finite flags per position in d_stat
 // (else the context's aggregated status).  Host-synchronisation free, so that
 // it can be captured into a graph.
-int batch_enqueue(bph_batch *b, int n, const double *const *d_in, double *const *d_out, const int *d_map,
-                  Schedule &sch, bool warm, bool per_pos) {
+// Forward transforms, boundary contraction and Dirichlet slots of a
+// batched call (the part before the ADI).
+static int batch_prologue(bph_batch *b, int n, const double *const *d_in, const int *d_map, bool per_pos) {
     bph_ctx *c = b->c;
-    Schedule *s = &sch;
     if (per_pos) BPH_CUDA(cudaMemsetAsync(b->d_stat, 0, sizeof(int) * n, c->stream));
     const long long np = c->np;
     const long long mstride = 2LL * b->cap * np;
@@ -520,11 +571,98 @@ int batch_enqueue(bph_batch *b, int n, const double *const *d_in, double *const 
             (double)c->N * c->factor, n, b->cap, d_map);
         BPH_CUDA(cudaGetLastError());
     }
+    return BPH_OK;
+}
+
+int batch_enqueue(bph_batch *b, int n, const double *const *d_in, double *const *d_out, const int *d_map,
+                  Schedule &sch, bool warm, bool per_pos) {
+    bph_ctx *c = b->c;
+    Schedule *s = &sch;
+    int rc = batch_prologue(b, n, d_in, d_map, per_pos);
+    if (rc) return rc;
     if (c->adi_seg)
         BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, !warm, b->d_P, b->d_R, n, d_map));
     else
         BPH_CUDA(launch_adi_large(c, *s, 0, s->nsteps, !warm, b->d_P, b->d_R, n, d_map, b->d_LW, b->d_LQ));
     BPH_CUDA(launch_fft_inv_batch(c, n, d_out, d_map, b->d_P, (long long)c->N * c->nplane));
+    return BPH_OK;
+}
+
+// Sums the per-slot norm pairs of instance i: sqrt(sum |a|^2 / sum |b|^2).
+static double instance_ratio(const double *h, int N, int i) {
+    double num = 0.0, den = 0.0;
+    for (int sl = 0; sl < N; ++sl) {
+        num += h[2 * ((size_t)i * N + sl)];
+        den += h[2 * ((size_t)i * N + sl) + 1];
+    }
+    return den > 0.0 ? std::sqrt(num / den) : std::sqrt(num);
+}
+
+// Converged solves of the contiguous instances 0..n-1: the transforms and
+// boundary once, then cycles of nsteps ADI steps (FP64: update measured
+// against the previous cycle's slot arrays) or FP32 refinement cycles on
+// the FP64 defect (the update is the cycle's own correction), until every
+// instance's relative update is at most tol (mixed: or no longer halves)
+// or max_cycles.  One host synchronisation per cycle.
+int batch_converged_run(bph_batch *b, int n, const double *const *d_in, double *const *d_out, BatchConv &cv,
+                        bool per_pos) {
+    bph_ctx *c = b->c;
+    Schedule *s;
+    int rc = batch_schedule(c, cv.nsteps, &s);
+    if (rc) return rc;
+    const size_t pbytes = sizeof(double) * (size_t)n * c->N * c->nplane;
+    if (!b->d_cnorm && (rc = batch_alloc(b, &b->d_cnorm, 2ull * b->cap * c->N))) return rc;
+    if (!b->h_cnorm) BPH_CUDA(cudaMallocHost((void **)&b->h_cnorm, sizeof(double) * 2 * (size_t)b->cap * c->N));
+    if (!cv.mixed && !b->d_prev && (rc = batch_alloc(b, &b->d_prev, (size_t)b->cap * c->N * c->nplane))) return rc;
+    if (cv.cold) BPH_CUDA(cudaMemsetAsync(b->d_P, 0, pbytes, c->stream));  // before the Dirichlet slots
+    if ((rc = batch_prologue(b, n, d_in, nullptr, per_pos))) return rc;
+    std::vector<double> prev_upd((size_t)n, INFINITY);
+    std::vector<char> done((size_t)n, 0);
+    const size_t hbytes = sizeof(double) * 2 * (size_t)n * c->N;
+    int cyc = 0;
+    bool diverged = false;
+    for (;;) {
+        if (cv.mixed) {
+            BPH_CUDA(launch_defect_batch(c, *s, b->d_P, b->d_R, n, b->d_cnorm));
+        } else {
+            BPH_CUDA(cudaMemcpyAsync(b->d_prev, b->d_P, pbytes, cudaMemcpyDeviceToDevice, c->stream));
+            if (c->adi_seg)
+                BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, false, b->d_P, b->d_R, n, nullptr));
+            else
+                BPH_CUDA(launch_adi_large(c, *s, 0, s->nsteps, false, b->d_P, b->d_R, n, nullptr, b->d_LW, b->d_LQ));
+            BPH_CUDA(launch_norms_batch(c, false, b->d_P, b->d_prev, nullptr, n, b->d_cnorm));
+        }
+        ++cyc;
+        BPH_CUDA(cudaMemcpyAsync(b->h_cnorm, b->d_cnorm, hbytes, cudaMemcpyDeviceToHost, c->stream));
+        BPH_CUDA(cudaStreamSynchronize(c->stream));
+        bool all = true;
+        for (int i = 0; i < n; ++i) {
+            if (done[(size_t)i]) continue;  // converged instances keep cycling with the rest (harmless)
+            const double upd = instance_ratio(b->h_cnorm, c->N, i);
+            bool stop = upd <= cv.tol;
+            if (cv.mixed) {
+                if (!(upd == upd)) diverged = true;
+                stop = stop || !(upd == upd) || upd > 0.5 * prev_upd[(size_t)i];
+            }
+            prev_upd[(size_t)i] = upd;
+            done[(size_t)i] = stop;
+            all = all && stop;
+        }
+        if (all || diverged || cyc >= cv.max_cycles) break;
+    }
+    cv.cycles = cyc;
+    if (cv.want_resid) {
+        BPH_CUDA(launch_norms_batch(c, true, b->d_P, nullptr, b->d_R, n, b->d_cnorm));
+        BPH_CUDA(cudaMemcpyAsync(b->h_cnorm, b->d_cnorm, hbytes, cudaMemcpyDeviceToHost, c->stream));
+        BPH_CUDA(cudaStreamSynchronize(c->stream));
+        cv.resid = 0.0;
+        for (int i = 0; i < n; ++i) cv.resid = std::max(cv.resid, instance_ratio(b->h_cnorm, c->N, i));
+    }
+    BPH_CUDA(launch_fft_inv_batch(c, n, d_out, nullptr, b->d_P, (long long)c->N * c->nplane));
+    if (diverged) {
+        set_error("mixed-precision refinement diverged in a batch instance");
+        return BPH_ERR_NONFINITE;
+    }
     return BPH_OK;
 }
 

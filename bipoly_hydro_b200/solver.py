@@ -46,7 +46,8 @@ EXPORTED_SYMBOLS = (
     "bph_solve_converged", "bph_potential_solver_phieff", "bph_set_potential", "bph_solve_converged_mixed", "bph_set_stream", "bph_synchronize", "bph_destroy", "bph_last_error",
     "bph_version", "bph_num_boundary_rows", "bph_copy_green", "bph_copy_moments", "bph_run_phase",
     "bph_green_contract_noalloc", "bph_info", "bph_configure", "bph_launch_count", "bph_device_bytes",
-    "bph_batch_create", "bph_batch_solve", "bph_batch_solve_instances", "bph_batch_destroy",
+    "bph_batch_create", "bph_batch_solve", "bph_batch_solve_instances", "bph_batch_solve_converged",
+    "bph_batch_destroy",
     "bph_batch_device_bytes", "bph_plan_create", "bph_plan_launch", "bph_plan_synchronize", "bph_plan_launches",
     "bph_plan_destroy",
     "bph_server_create", "bph_server_capacity", "bph_server_open_client", "bph_server_close_client",
@@ -125,6 +126,9 @@ def load_library(path: str | None = None):
     L.bph_batch_solve.restype = ctypes.c_int
     L.bph_batch_solve_instances.argtypes = [vp, i, ctypes.POINTER(i), ctypes.POINTER(vp), ctypes.POINTER(vp), i, i]
     L.bph_batch_solve_instances.restype = ctypes.c_int
+    L.bph_batch_solve_converged.argtypes = [vp, i, ctypes.POINTER(vp), ctypes.POINTER(vp), i, i, ctypes.c_double, i,
+                                            i, i, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_double)]
+    L.bph_batch_solve_converged.restype = ctypes.c_int
     L.bph_batch_destroy.argtypes = [vp]
     L.bph_batch_destroy.restype = ctypes.c_int
     ll, dbl = ctypes.c_longlong, ctypes.c_double
@@ -424,6 +428,32 @@ class Batch:
         arr_p = (ctypes.c_void_p * n)(*[a.ctypes.data for a in pots])
         _check(self._lib.bph_batch_solve_instances(self._h, n, idx, arr_r, arr_p, int(tstep), 0))
         return pots
+
+    def _converged(self, arr_r, arr_p, n, nsteps, cold, tol, max_cycles, mixed, on_device):
+        cyc, res = ctypes.c_int(0), ctypes.c_double(0.0)
+        _check(self._lib.bph_batch_solve_converged(self._h, n, arr_r, arr_p, int(nsteps), int(bool(cold)), float(tol),
+                                                   int(max_cycles), int(bool(mixed)), int(on_device),
+                                                   ctypes.byref(cyc), ctypes.byref(res)))
+        return ConvergedInfo(cyc.value, res.value)
+
+    def solve_converged(self, rhos, nsteps: int = 10, cold: bool = False, tol: float = 1e-11, max_cycles: int = 100,
+                        mixed: bool = False):
+        """Host arrays: converged solves of instances 0..n-1 -> (potentials, ConvergedInfo)."""
+        rs = [self.solver._rho_host(r) for r in rhos]
+        pots = [np.empty(self.solver.shape, dtype=np.float64, order="F") for _ in rs]
+        n = len(rs)
+        arr_r = (ctypes.c_void_p * n)(*[a.ctypes.data for a in rs])
+        arr_p = (ctypes.c_void_p * n)(*[a.ctypes.data for a in pots])
+        info = self._converged(arr_r, arr_p, n, nsteps, cold, tol, max_cycles, mixed, 0)
+        return pots, info
+
+    def solve_converged_device(self, d_rhos, d_pots, nsteps: int = 10, cold: bool = False, tol: float = 1e-11,
+                               max_cycles: int = 100, mixed: bool = False):
+        """Device arrays: as solve_converged, results enqueued on the solver's stream."""
+        n = len(d_rhos)
+        arr_r = (ctypes.c_void_p * n)(*[_dev_ptr(x) for x in d_rhos])
+        arr_p = (ctypes.c_void_p * n)(*[_dev_ptr(x) for x in d_pots])
+        return self._converged(arr_r, arr_p, n, nsteps, cold, tol, max_cycles, mixed, 1)
 
     @property
     def device_bytes(self) -> int:

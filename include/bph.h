@@ -128,6 +128,19 @@ int bph_batch_solve(bph_batch_t *batch, int n, const double *const *rho, double 
  * instances[i]; the other instances keep their state untouched. */
 int bph_batch_solve_instances(bph_batch_t *batch, int n, const int *instances, const double *const *rho,
                               double *const *pot, int tstep, int on_device);
+/* Converged solves of instances 0..n-1 (the bph_solve_converged /
+ * bph_solve_converged_mixed forms for a batch): the transforms and the
+ * boundary once per call, then cycles of nsteps ADI steps from each
+ * instance's warm state (cold != 0: from zero) until every instance's
+ * relative update is at most tol (mixed != 0: FP32 refinement cycles on the
+ * FP64 defect, which also stop once a cycle no longer halves the update) or
+ * max_cycles.  cycles_out: cycles run; resid_out: the largest relative FP64
+ * residual over the instances (NULL skips it).  One host synchronisation
+ * per cycle.  Mixed needs an on-chip refinement kernel (slots that fit
+ * shared memory). */
+int bph_batch_solve_converged(bph_batch_t *batch, int n, const double *const *rho, double *const *pot, int nsteps,
+                              int cold, double tol, int max_cycles, int mixed, int on_device, int *cycles_out,
+                              double *resid_out);
 int bph_batch_destroy(bph_batch_t *batch);
 size_t bph_batch_device_bytes(const bph_batch_t *batch);
 
