@@ -270,10 +270,10 @@ def serve_bench(B, torch, dev, rhos, args):
     gen = torch.Generator(device=dev)
     gen.manual_seed(20261203)
     out = {"grid": "130x98x256", "clients": nclients, "requests_per_rate": nclients * iters,
-           "capacity": srv.capacity, "dtype": "f64", "mixed": None,
-           "mixed_note": "the batched/serving path is FP64 only (no mixed-precision batch kernel)",
+           "capacity": srv.capacity, "dtype": "f64 drop-in (rates); converged FP64 vs mixed (converged)",
            "rates": []}
-    for rate in [float(x) for x in args.serve_rates.split(",") if x]:
+
+    def run_rate(rate):
         ids = [srv.open_client() for _ in range(nclients)]
         rho = [[rhos[(37 * c) % nrot] * (1.0 + 0.2 * c / nclients), torch.empty_like(rhos[0])] for c in range(nclients)]
         mass = [float(r[0].sum()) for r in rho]
@@ -304,13 +304,22 @@ def serve_bench(B, torch, dev, rhos, args):
             lat.append(srv.wait(rid.pop(key), timeout=120.0)[1])
         elapsed = time.perf_counter() - t0
         st = srv.stats()
-        out["rates"].append({"offered_req_per_s": rate, "solves_per_s": nclients * iters / elapsed,
-                             "p50_ms": 1e3 * float(np.percentile(lat, 50)),
-                             "p99_ms": 1e3 * float(np.percentile(lat, 99)),
-                             "mean_batch": (st["solves"] - st0["solves"]) / max(1, st["batches"] - st0["batches"])})
         for cid in ids:
             srv.close_client(cid)
-        del rho, pot
+        return {"offered_req_per_s": rate, "solves_per_s": nclients * iters / elapsed,
+                "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                "mean_batch": (st["solves"] - st0["solves"]) / max(1, st["batches"] - st0["batches"])}
+
+    for rate in [float(x) for x in args.serve_rates.split(",") if x]:
+        out["rates"].append(run_rate(rate))
+    # converged serving, FP64 against mixed precision (same clients and arrivals)
+    conv_rates = [float(x) for x in args.serve_conv_rates.split(",") if x]
+    if conv_rates:
+        out["converged"] = {"nsteps_per_cycle": args.conv_nsteps, "tol_update": args.conv_tol}
+        for key, mixed in (("fp64", False), ("mixed", True)):
+            srv.set_converged(args.conv_nsteps, args.conv_tol, 100, mixed)
+            out["converged"][key] = [run_rate(r) for r in conv_rates]
+        srv.set_converged(0)
     srv.close()
     srv_solver.close()
     return out
@@ -880,6 +889,8 @@ def main():
     ap.add_argument("--serve-rates", default="200,1000,4000",
                     help="offered request rates (req/s) of the serving section (empty skips)")
     ap.add_argument("--serve-clients", type=int, default=64)
+    ap.add_argument("--serve-conv-rates", default="300,1500",
+                    help="offered rates of converged serving, FP64 and mixed (empty skips)")
     ap.add_argument("--serve-mixed-rates", default="100,400,1600",
                     help="offered rates of the mixed-grid serving section (empty skips)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section")

@@ -898,8 +898,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_adi_delta(AdiArgs a) {
     using T2 = float2;
     extern __shared__ __align__(16) unsigned char smraw[];
     T *sm = reinterpret_cast<T *>(smraw);
-    const int s = blockIdx.x % a.N, tid = threadIdx.x;
-    const long long blk = blockIdx.x;
+    // blockIdx.x = position * N + slot; the instance of a position through the map
+    const int s = blockIdx.x % a.N, row = blockIdx.x / a.N, tid = threadIdx.x;
+    const long long blk = (long long)(a.inst_map ? a.inst_map[row] : row) * a.N + s;
     const int lane = tid & 31, warp = tid >> 5, nwarps = kThreads / 32;
     const int nr = a.nr, nz = a.nz, numr = a.numr, numz = a.numz;
     const DeltaLayout Lo = delta_layout(nr, nz);
@@ -1119,9 +1120,11 @@ __global__ void __launch_bounds__(kNormThreads)
 k_slot_norms(const double *__restrict__ P, const double *__restrict__ Q, const double *__restrict__ R,
              const double *__restrict__ brb, const double *__restrict__ alphar, const double *__restrict__ betar,
              const double *__restrict__ bzb, double gamma, int numr, int numz, int nr, int nz, int N, int isym,
-             double *__restrict__ out) {
-    // blockIdx.x = instance * N + slot (instances contiguous, as in a batch)
-    const int s = blockIdx.x, sl = s % N;
+             double *__restrict__ out, const int *__restrict__ map) {
+    // blockIdx.x = position * N + slot; s = instance * N + slot (batch
+    // instances are contiguous; map: instance of each position)
+    const int row = blockIdx.x / N, sl = blockIdx.x % N;
+    const int s = (map ? map[row] : row) * N + sl;
     const long long nplane = (long long)numr * numz, np = (long long)nr * nz;
     const double *Ps = P + (long long)s * nplane;
     double a0 = 0.0, a1 = 0.0;
@@ -1405,12 +1408,14 @@ cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {
                             c->stream);
 }
 
-cudaError_t launch_defect_batch(bph_ctx *c, const Schedule &sch, double *P, const double *R, int n, double *norms) {
+cudaError_t launch_defect_batch(bph_ctx *c, const Schedule &sch, double *P, const double *R, int n, const int *d_map,
+                                double *norms) {
     if (!c->adi_mixed_smem || c->mixed_kind == BPH_MIXED_ADI_GLOBAL) return cudaErrorNotSupported;
     AdiArgs a = make_args(c, sch, 0, sch.nsteps, false);
     a.P = P;
     a.R = R;
     a.norms = norms;
+    a.inst_map = d_map;
     a.rad_pk = sch.d_rad_pk[1];
     a.ver_pk = sch.d_ver_pk[1];
     a.pkr = packed_block<float>(c->nr);
@@ -1425,16 +1430,16 @@ cudaError_t launch_defect_batch(bph_ctx *c, const Schedule &sch, double *P, cons
 }
 
 cudaError_t launch_norms_batch(bph_ctx *c, bool residual, const double *P, const double *prev, const double *R, int n,
-                               double *d_out) {
+                               const int *d_map, double *d_out) {
     ++c->launches;
     if (residual)
         k_slot_norms<true><<<c->N * n, kNormThreads, 0, c->stream>>>(
             P, prev, R, c->d_brb, c->d_alphar, c->d_betar, c->d_bzb, c->gamma, c->g.numr, c->g.numz, c->nr, c->nz,
-            c->N, c->g.isym, d_out);
+            c->N, c->g.isym, d_out, d_map);
     else
         k_slot_norms<false><<<c->N * n, kNormThreads, 0, c->stream>>>(
             P, prev, R, c->d_brb, c->d_alphar, c->d_betar, c->d_bzb, c->gamma, c->g.numr, c->g.numz, c->nr, c->nz,
-            c->N, c->g.isym, d_out);
+            c->N, c->g.isym, d_out, d_map);
     return cudaGetLastError();
 }
 
@@ -1442,7 +1447,7 @@ cudaError_t launch_update_norm(bph_ctx *c, double *d_out) {
     ++c->launches;
     k_slot_norms<false><<<c->N, kNormThreads, 0, c->stream>>>(
         c->d_P, c->d_prev, c->d_R, c->d_brb, c->d_alphar, c->d_betar, c->d_bzb, c->gamma, c->g.numr, c->g.numz,
-        c->nr, c->nz, c->N, c->g.isym, d_out);
+        c->nr, c->nz, c->N, c->g.isym, d_out, nullptr);
     return cudaGetLastError();
 }
 
@@ -1450,7 +1455,7 @@ cudaError_t launch_residual_norm(bph_ctx *c, double *d_out) {
     ++c->launches;
     k_slot_norms<true><<<c->N, kNormThreads, 0, c->stream>>>(
         c->d_P, c->d_prev, c->d_R, c->d_brb, c->d_alphar, c->d_betar, c->d_bzb, c->gamma, c->g.numr, c->g.numz,
-        c->nr, c->nz, c->N, c->g.isym, d_out);
+        c->nr, c->nz, c->N, c->g.isym, d_out, nullptr);
     return cudaGetLastError();
 }
 

@@ -239,17 +239,8 @@ int batch_schedule(bph_ctx *c, int nsteps, Schedule **out);
 int batch_enqueue(bph_batch *b, int n, const double *const *d_in, double *const *d_out, const int *d_map,
                   Schedule &sch, bool warm, bool per_pos);
 
-// A converged batched call (bph_batch_solve_converged).
-struct BatchConv {
-    int nsteps = 0, max_cycles = 0;
-    bool cold = false, mixed = false;
-    double tol = 0.0;
-    int cycles = 0;           // out: cycles run
-    double resid = 0.0;       // out: largest relative FP64 residual over the instances
-    bool want_resid = false;
-};
-int batch_converged_run(bph_batch *b, int n, const double *const *d_in, double *const *d_out, BatchConv &cv,
-                        bool per_pos);
+int batch_converged_run(bph_batch *b, int n, const int *inst, const int *d_map, const double *const *d_in,
+                        double *const *d_out, BatchConv &cv, bool per_pos);
 
 }  // namespace bph
 
@@ -438,10 +429,6 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
     bph_ctx *c = b->c;
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
-    if (conv && instances) {
-        set_error("converged batched solves take instances 0..n-1");
-        return BPH_ERR_INVALID;
-    }
     Schedule *s;  // warm: 5 steps, cold: 20 (potential_solver.F90:80-94); converged: its cycle length
     int rc = batch_schedule(c, conv ? conv->nsteps : (warm ? 5 : 20), &s);
     if (rc) return rc;
@@ -502,8 +489,10 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
     const int *d_map = instances ? reinterpret_cast<const int *>(db + 2 * sizeof(void *) * b->cap) : nullptr;
     // per-position non-finite flags: host-array calls and callers that want per-position status
     const bool per_pos = !on_device || pos_status;
-    if (conv)
-        rc = batch_converged_run(b, n, d_in, d_out, *conv, per_pos);
+    if (conv) {
+        conv->report_divergence = (pos_status == nullptr);
+        rc = batch_converged_run(b, n, inst.data(), d_map, d_in, d_out, *conv, per_pos);
+    }
     else
         rc = batch_enqueue(b, n, d_in, d_out, d_map, *s, warm, per_pos);
     if (rc) return rc;
@@ -588,6 +577,15 @@ int batch_enqueue(bph_batch *b, int n, const double *const *d_in, double *const 
     return BPH_OK;
 }
 
+int batch_reserve_converged(bph_batch *b, bool fp64) {
+    bph_ctx *c = b->c;
+    int rc;
+    if (!b->d_cnorm && (rc = batch_alloc(b, &b->d_cnorm, 2ull * b->cap * c->N))) return rc;
+    if (!b->h_cnorm) BPH_CUDA(cudaMallocHost((void **)&b->h_cnorm, sizeof(double) * 2 * (size_t)b->cap * c->N));
+    if (fp64 && !b->d_prev && (rc = batch_alloc(b, &b->d_prev, (size_t)b->cap * c->N * c->nplane))) return rc;
+    return BPH_OK;
+}
+
 // Sums the per-slot norm pairs of instance i: sqrt(sum |a|^2 / sum |b|^2).
 static double instance_ratio(const double *h, int N, int i) {
     double num = 0.0, den = 0.0;
@@ -598,39 +596,51 @@ static double instance_ratio(const double *h, int N, int i) {
     return den > 0.0 ? std::sqrt(num / den) : std::sqrt(num);
 }
 
-// Converged solves of the contiguous instances 0..n-1: the transforms and
-// boundary once, then cycles of nsteps ADI steps (FP64: update measured
+// Converged solves of n batch positions (instance inst[i] on the host,
+// d_map on the device; d_map nullptr: position = instance): the transforms
+// and boundary once, then cycles of nsteps ADI steps (FP64: update measured
 // against the previous cycle's slot arrays) or FP32 refinement cycles on
 // the FP64 defect (the update is the cycle's own correction), until every
 // instance's relative update is at most tol (mixed: or no longer halves)
-// or max_cycles.  One host synchronisation per cycle.
-int batch_converged_run(bph_batch *b, int n, const double *const *d_in, double *const *d_out, BatchConv &cv,
-                        bool per_pos) {
+// or max_cycles.  Norms are indexed by instance.  One host synchronisation
+// per cycle.
+int batch_converged_run(bph_batch *b, int n, const int *inst, const int *d_map, const double *const *d_in,
+                        double *const *d_out, BatchConv &cv, bool per_pos) {
     bph_ctx *c = b->c;
     Schedule *s;
     int rc = batch_schedule(c, cv.nsteps, &s);
     if (rc) return rc;
-    const size_t pbytes = sizeof(double) * (size_t)n * c->N * c->nplane;
-    if (!b->d_cnorm && (rc = batch_alloc(b, &b->d_cnorm, 2ull * b->cap * c->N))) return rc;
-    if (!b->h_cnorm) BPH_CUDA(cudaMallocHost((void **)&b->h_cnorm, sizeof(double) * 2 * (size_t)b->cap * c->N));
-    if (!cv.mixed && !b->d_prev && (rc = batch_alloc(b, &b->d_prev, (size_t)b->cap * c->N * c->nplane))) return rc;
-    if (cv.cold) BPH_CUDA(cudaMemsetAsync(b->d_P, 0, pbytes, c->stream));  // before the Dirichlet slots
-    if ((rc = batch_prologue(b, n, d_in, nullptr, per_pos))) return rc;
+    const size_t ibytes = sizeof(double) * (size_t)c->N * c->nplane;  // one instance's slot arrays
+    int top = 0;  // instances 0..top-1 hold every position's norms
+    for (int i = 0; i < n; ++i) top = std::max(top, inst[i] + 1);
+    if ((rc = batch_reserve_converged(b, !cv.mixed))) return rc;
+    if (cv.cold)  // before the Dirichlet slots
+        for (int i = 0; i < n; ++i)
+            BPH_CUDA(cudaMemsetAsync(b->d_P + (size_t)inst[i] * c->N * c->nplane, 0, ibytes, c->stream));
+    if ((rc = batch_prologue(b, n, d_in, d_map, per_pos))) return rc;
     std::vector<double> prev_upd((size_t)n, INFINITY);
     std::vector<char> done((size_t)n, 0);
-    const size_t hbytes = sizeof(double) * 2 * (size_t)n * c->N;
+    const size_t hbytes = sizeof(double) * 2 * (size_t)top * c->N;
     int cyc = 0;
     bool diverged = false;
     for (;;) {
         if (cv.mixed) {
-            BPH_CUDA(launch_defect_batch(c, *s, b->d_P, b->d_R, n, b->d_cnorm));
+            BPH_CUDA(launch_defect_batch(c, *s, b->d_P, b->d_R, n, d_map, b->d_cnorm));
         } else {
-            BPH_CUDA(cudaMemcpyAsync(b->d_prev, b->d_P, pbytes, cudaMemcpyDeviceToDevice, c->stream));
+            if (d_map) {
+                for (int i = 0; i < n; ++i) {
+                    const size_t off = (size_t)inst[i] * c->N * c->nplane;
+                    BPH_CUDA(cudaMemcpyAsync(b->d_prev + off, b->d_P + off, ibytes, cudaMemcpyDeviceToDevice,
+                                             c->stream));
+                }
+            } else {
+                BPH_CUDA(cudaMemcpyAsync(b->d_prev, b->d_P, ibytes * n, cudaMemcpyDeviceToDevice, c->stream));
+            }
             if (c->adi_seg)
-                BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, false, b->d_P, b->d_R, n, nullptr));
+                BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, false, b->d_P, b->d_R, n, d_map));
             else
-                BPH_CUDA(launch_adi_large(c, *s, 0, s->nsteps, false, b->d_P, b->d_R, n, nullptr, b->d_LW, b->d_LQ));
-            BPH_CUDA(launch_norms_batch(c, false, b->d_P, b->d_prev, nullptr, n, b->d_cnorm));
+                BPH_CUDA(launch_adi_large(c, *s, 0, s->nsteps, false, b->d_P, b->d_R, n, d_map, b->d_LW, b->d_LQ));
+            BPH_CUDA(launch_norms_batch(c, false, b->d_P, b->d_prev, nullptr, n, d_map, b->d_cnorm));
         }
         ++cyc;
         BPH_CUDA(cudaMemcpyAsync(b->h_cnorm, b->d_cnorm, hbytes, cudaMemcpyDeviceToHost, c->stream));
@@ -638,12 +648,12 @@ int batch_converged_run(bph_batch *b, int n, const double *const *d_in, double *
         bool all = true;
         for (int i = 0; i < n; ++i) {
             if (done[(size_t)i]) continue;  // converged instances keep cycling with the rest (harmless)
-            const double upd = instance_ratio(b->h_cnorm, c->N, i);
-            bool stop = upd <= cv.tol;
-            if (cv.mixed) {
-                if (!(upd == upd)) diverged = true;
-                stop = stop || !(upd == upd) || upd > 0.5 * prev_upd[(size_t)i];
-            }
+            const double upd = instance_ratio(b->h_cnorm, c->N, inst[i]);
+            // a non-finite update ends the instance (a non-finite density is
+            // also flagged per position by the forward transform)
+            bool stop = upd <= cv.tol || !(upd == upd);
+            if (!(upd == upd) && cv.mixed) diverged = true;
+            if (cv.mixed) stop = stop || upd > 0.5 * prev_upd[(size_t)i];
             prev_upd[(size_t)i] = upd;
             done[(size_t)i] = stop;
             all = all && stop;
@@ -652,15 +662,15 @@ int batch_converged_run(bph_batch *b, int n, const double *const *d_in, double *
     }
     cv.cycles = cyc;
     if (cv.want_resid) {
-        BPH_CUDA(launch_norms_batch(c, true, b->d_P, nullptr, b->d_R, n, b->d_cnorm));
+        BPH_CUDA(launch_norms_batch(c, true, b->d_P, nullptr, b->d_R, n, d_map, b->d_cnorm));
         BPH_CUDA(cudaMemcpyAsync(b->h_cnorm, b->d_cnorm, hbytes, cudaMemcpyDeviceToHost, c->stream));
         BPH_CUDA(cudaStreamSynchronize(c->stream));
         cv.resid = 0.0;
-        for (int i = 0; i < n; ++i) cv.resid = std::max(cv.resid, instance_ratio(b->h_cnorm, c->N, i));
+        for (int i = 0; i < n; ++i) cv.resid = std::max(cv.resid, instance_ratio(b->h_cnorm, c->N, inst[i]));
     }
-    BPH_CUDA(launch_fft_inv_batch(c, n, d_out, nullptr, b->d_P, (long long)c->N * c->nplane));
-    if (diverged) {
-        set_error("mixed-precision refinement diverged in a batch instance");
+    BPH_CUDA(launch_fft_inv_batch(c, n, d_out, d_map, b->d_P, (long long)c->N * c->nplane));
+    if (diverged && cv.report_divergence) {
+        set_error("mixed-precision refinement diverged (or a density is non-finite) in a batch instance");
         return BPH_ERR_NONFINITE;
     }
     return BPH_OK;

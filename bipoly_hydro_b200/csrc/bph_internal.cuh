@@ -258,7 +258,20 @@ void conv_graphs_free(bph_ctx *c);
 // Batched solve of batch positions 0..n-1 (bph_batch.cu); instances may be
 // nullptr (position i = instance i).  With pos_status (per-position
 // BPH_OK / BPH_ERR_NONFINITE) or host arrays the call is synchronous.
-struct BatchConv;
+// A converged batched call (bph_batch_solve_converged; servers in
+// converged mode).
+struct BatchConv {
+    int nsteps = 0, max_cycles = 0;
+    bool cold = false, mixed = false;
+    double tol = 0.0;
+    int cycles = 0;           // out: cycles run
+    double resid = 0.0;       // out: largest relative FP64 residual over the instances
+    bool want_resid = false;
+    bool report_divergence = true;  // false: per-position status reports bad densities
+};
+// Norm buffers (and, for FP64, the previous-cycle slot arrays) of converged
+// batched calls, allocated ahead of the first one.
+int batch_reserve_converged(bph_batch *b, bool fp64);
 int batch_solve_core(bph_batch *b, int n, const int *instances, const double *const *rho, double *const *pot,
                      bool warm, bool on_device, int *pos_status, BatchConv *conv = nullptr);
 // Raises the dynamic shared memory limit of kernel fn on the current device
@@ -266,13 +279,15 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
 // while contexts of different grids share kernels, so it only ever grows
 // (a context set up later with a smaller need must not lower it).
 cudaError_t raise_smem_limit(const void *fn, int bytes);
-// FP32 refinement cycle (on-chip kinds) over the contiguous instances
-// 0..n-1 of batch arrays P/R; per (instance, slot) norms into norms[2 (i N + s) + 0/1].
-cudaError_t launch_defect_batch(bph_ctx *c, const Schedule &sch, double *P, const double *R, int n, double *norms);
+// FP32 refinement cycle (on-chip kinds) over n batch positions of the
+// batch arrays P/R (d_map: instance of each position, nullptr: position =
+// instance); per (instance, slot) norms into norms[2 (i N + s) + 0/1].
+cudaError_t launch_defect_batch(bph_ctx *c, const Schedule &sch, double *P, const double *R, int n, const int *d_map,
+                                double *norms);
 // Per (instance, slot) update (|P - prev|^2, |P|^2) or residual (|R - A P|^2,
-// |R|^2) norms of the contiguous instances 0..n-1.
+// |R|^2) norms of n batch positions, indexed as above.
 cudaError_t launch_norms_batch(bph_ctx *c, bool residual, const double *P, const double *prev, const double *R, int n,
-                               double *d_out);
+                               const int *d_map, double *d_out);
 // Reads and clears the context's device status word (synchronises its stream).
 int context_status(bph_ctx *c);
 // Makes kind (BPH_MIXED_ADI_FORWARD / _INCREMENT) the refinement ADI kernel.

@@ -49,6 +49,10 @@ struct bph_server {
     std::vector<int> inflight;                   // requests queued or running per client
     long long next_id = 1;
     long long batches = 0, solves = 0;
+    int conv_nsteps = 0;  // converged mode: ADI steps per cycle (0: the drop-in solve)
+    double conv_tol = 0.0;
+    int conv_max_cycles = 0;
+    bool conv_mixed = false;
     bool stop = false;
     std::thread worker;
 };
@@ -74,10 +78,17 @@ void serve_loop(bph_server *s) {
     for (;;) {
         take.clear();
         take_warm.clear();
+        BatchConv conv;
+        bool converged = false;
         {
             std::unique_lock<std::mutex> lk(s->mu);
             s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
             if (s->queue.empty()) return;  // stop requested and nothing left
+            converged = s->conv_nsteps > 0;
+            conv.nsteps = s->conv_nsteps;
+            conv.tol = s->conv_tol;
+            conv.max_cycles = s->conv_max_cycles;
+            conv.mixed = s->conv_mixed;
             // oldest request of every client with one pending, in arrival order
             std::vector<char> seen((size_t)s->capacity, 0);
             for (auto it = s->queue.begin(); it != s->queue.end() && (int)take.size() < s->max_batch;) {
@@ -114,8 +125,9 @@ void serve_loop(bph_server *s) {
             if (group_ids.empty()) continue;
             const int n = (int)group_ids.size();
             group_status.assign((size_t)n, BPH_OK);
+            conv.cold = !warm_pass;
             int rc = batch_solve_core(s->batch, n, group_inst.data(), group_rho.data(), group_pot.data(), warm_pass,
-                                      s->device_arrays, group_status.data());
+                                      s->device_arrays, group_status.data(), converged ? &conv : nullptr);
             const double t = now_s();
             {
                 std::lock_guard<std::mutex> lk(s->mu);
@@ -194,6 +206,29 @@ int bph_server_create(bph_ctx_t *c, int max_clients, size_t mem_cap_bytes, int m
     }
     s->worker = std::thread(serve_loop, s);
     *out = s;
+    return BPH_OK;
+}
+
+int bph_server_set_converged(bph_server_t *s, int nsteps, double tol, int max_cycles, int mixed) {
+    if (!s || nsteps < 0 || nsteps > 10000 || (nsteps > 0 && (max_cycles < 1 || !(tol >= 0.0)))) {
+        set_error("invalid server or converged-mode arguments");
+        return BPH_ERR_INVALID;
+    }
+    bph_ctx *c = s->c;
+    if (nsteps > 0 && mixed && (!c->adi_mixed_smem || c->mixed_kind == BPH_MIXED_ADI_GLOBAL)) {
+        set_error("mixed converged serving needs an on-chip refinement kernel (slots that fit shared memory)");
+        return BPH_ERR_INVALID;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (nsteps > 0) {
+        // buffers first: a batch the worker takes after the mode changes finds them
+        const int rc = batch_reserve_converged(s->batch, !mixed);
+        if (rc) return rc;
+    }
+    s->conv_nsteps = nsteps;
+    s->conv_tol = tol;
+    s->conv_max_cycles = max_cycles;
+    s->conv_mixed = mixed != 0;
     return BPH_OK;
 }
 

@@ -50,7 +50,8 @@ EXPORTED_SYMBOLS = (
     "bph_batch_destroy",
     "bph_batch_device_bytes", "bph_plan_create", "bph_plan_launch", "bph_plan_synchronize", "bph_plan_launches",
     "bph_plan_destroy",
-    "bph_server_create", "bph_server_capacity", "bph_server_open_client", "bph_server_close_client",
+    "bph_server_create", "bph_server_set_converged", "bph_server_capacity", "bph_server_open_client",
+    "bph_server_close_client",
     "bph_server_submit", "bph_server_poll", "bph_server_wait", "bph_server_stats", "bph_server_destroy",
 )
 
@@ -133,6 +134,7 @@ def load_library(path: str | None = None):
     L.bph_batch_destroy.restype = ctypes.c_int
     ll, dbl = ctypes.c_longlong, ctypes.c_double
     L.bph_server_create.argtypes = [vp, i, sz, i, i, ctypes.POINTER(vp)]
+    L.bph_server_set_converged.argtypes = [vp, i, dbl, i, i]
     L.bph_server_capacity.argtypes = [vp]
     L.bph_server_open_client.argtypes = [vp, ctypes.POINTER(i)]
     L.bph_server_close_client.argtypes = [vp, i]
@@ -141,8 +143,8 @@ def load_library(path: str | None = None):
     L.bph_server_wait.argtypes = [vp, ll, dbl, ctypes.POINTER(dbl)]
     L.bph_server_stats.argtypes = [vp, ctypes.POINTER(ll), ctypes.POINTER(ll)]
     L.bph_server_destroy.argtypes = [vp]
-    for name in ("bph_server_create", "bph_server_capacity", "bph_server_open_client", "bph_server_close_client",
-                 "bph_server_submit", "bph_server_poll", "bph_server_wait", "bph_server_stats",
+    for name in ("bph_server_create", "bph_server_set_converged", "bph_server_capacity", "bph_server_open_client",
+                 "bph_server_close_client", "bph_server_submit", "bph_server_poll", "bph_server_wait", "bph_server_stats",
                  "bph_server_destroy"):
         getattr(L, name).restype = ctypes.c_int
     L.bph_plan_create.argtypes = [i, ctypes.POINTER(vp), ctypes.POINTER(i), ctypes.POINTER(vp), ctypes.POINTER(vp),
@@ -540,6 +542,10 @@ class Server:
         self._h = h
         self._live = {}  # request id -> (rho, pot) kept alive until completion
         solver._dependents.add(self)
+
+    def set_converged(self, nsteps: int = 10, tol: float = 1e-11, max_cycles: int = 100, mixed: bool = False) -> None:
+        """Serve converged solves (FP64, or mixed precision) from the next batch on; nsteps=0: drop-in."""
+        _check(self._lib.bph_server_set_converged(self._h, int(nsteps), float(tol), int(max_cycles), int(bool(mixed))))
 
     @property
     def capacity(self) -> int:

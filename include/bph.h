@@ -196,6 +196,13 @@ typedef struct bph_server bph_server_t;
 #define BPH_SERVER_DEVICE_ARRAYS 1
 int bph_server_create(bph_ctx_t *ctx, int max_clients, size_t mem_cap_bytes, int max_batch, int flags,
                       bph_server_t **server);
+/* Converged mode: from the next batch on, every request is a converged
+ * solve (bph_batch_solve_converged with nsteps, tol, max_cycles; mixed != 0:
+ * FP32 refinement on the FP64 defect; first requests of a client cold, later
+ * ones from its last potential).  nsteps = 0 returns to the drop-in solve.
+ * Best called before submitting; FP64 mode reserves one more slot array per
+ * resident client. */
+int bph_server_set_converged(bph_server_t *server, int nsteps, double tol, int max_cycles, int mixed);
 /* Resident clients this server admits. */
 int bph_server_capacity(const bph_server_t *server);
 int bph_server_open_client(bph_server_t *server, int *client);

@@ -191,3 +191,31 @@ def test_device_array_mode_matches_host_mode(bph):
         for t in range(3):
             got = d_pot[c][t].cpu().numpy().reshape(ref[t].shape, order="F")
             assert rel_l2(got, ref[t]) <= POT_TOL, (c, t)
+
+
+@pytest.mark.parametrize("mixed", [False, True], ids=["fp64", "mixed"])
+def test_converged_mode_serves_converged_solutions(bph, mixed):
+    """In converged mode (FP64 or FP32 refinement) every request's potential
+    is the converged discrete solution of its density: equal to a single
+    converged FP64 solve to 1e-9, first requests cold and later ones warm."""
+    seqs = _densities(3, 3, seed=40)
+    g = bph.PotentialSolver(*GRID)
+    srv = bph.Server(g, max_clients=3)
+    srv.set_converged(nsteps=10, tol=1e-12, max_cycles=80, mixed=mixed)
+    clients = [srv.open_client() for _ in seqs]
+    rids = {}
+    for t in range(3):
+        for c, seq in zip(clients, seqs):
+            rids[(c, t)] = srv.submit(c, seq[t])
+    ref = bph.PotentialSolver(*GRID)
+    for c, seq in zip(clients, seqs):
+        for t in range(3):
+            pot, _ = srv.wait(rids[(c, t)], timeout=60.0)
+            want, _ = ref.solve_converged(seq[t], 10, True, 1e-13, 200)
+            assert rel_l2(pot, want) <= 1e-9, (c, t)
+    srv.set_converged(0)  # back to the drop-in solve
+    rid = srv.submit(clients[0], seqs[0][0])
+    assert srv.wait(rid, timeout=60.0)[0].shape == seqs[0][0].shape
+    srv.close()
+    ref.close()
+    g.close()
