@@ -19,7 +19,13 @@
 namespace bph {
 namespace {
 
-constexpr int kTile = 16;  // columns per CTA (128-byte coalesced rows)
+// Columns per CTA: 8 (64-byte rows) for the 64- and 128-point transforms, so
+// that a grid is several short waves instead of one long one with a tail;
+// 16 (128-byte rows) otherwise.
+template <int M>
+constexpr int tile_cols() {
+    return (M >= 64 && M <= 128) ? 8 : 16;
+}
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -35,6 +41,7 @@ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_doub
 // SIGN = +1 forward (e^{+i}), -1 inverse.
 template <int M, int R, int SIGN, int NT>
 __device__ __forceinline__ void stockham_pass(double2 *C, const double2 *tw, int Ns) {
+    constexpr int kTile = tile_cols<M>();
     constexpr int kTotal = kTile * (M / R);
     constexpr int kItems = (kTotal + NT - 1) / NT;  // butterflies per thread
     double2 v[kItems][R];
@@ -113,7 +120,7 @@ struct FftShape {
     // tile are all in flight at once; more CTAs hide more of their latency)
     static constexpr int kMinBlocksFwd = (M >= 256) ? 2 : 5;
     static constexpr int kMinBlocksInv = (M >= 256) ? 1 : 4;
-    static constexpr size_t kSmem = sizeof(double2) * ((size_t)M * kTile + M + (M + 1));
+    static constexpr size_t kSmem = sizeof(double2) * ((size_t)M * tile_cols<M>() + M + (M + 1));
 };
 
 // Forward transform of interior columns.  kRho: write R = -4 pi rho_hat
@@ -127,6 +134,7 @@ k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__re
           const double2 *__restrict__ g_tw, const double2 *__restrict__ g_tw2, const double2 *__restrict__ g_ph,
           int numr, int numz, int nr, int nz, int mmax, int fm, int isym, double four_pi,
           int *__restrict__ status, long long mstride, FftBatch bt) {
+    constexpr int kTile = tile_cols<M>();
     constexpr int NT = FftShape<M>::kThreads;
     extern __shared__ double2 smem[];
     double2 *C = smem;
@@ -273,6 +281,7 @@ __global__ void __launch_bounds__(FftShape<M>::kThreads, FftShape<M>::kMinBlocks
 k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 *__restrict__ g_tw,
           const double2 *__restrict__ g_tw2, int numr, int numz, int isym, double *__restrict__ phieff,
           const double *__restrict__ rhf, double omega, FftBatch bt) {
+    constexpr int kTile = tile_cols<M>();
     constexpr int NT = FftShape<M>::kThreads;
     extern __shared__ double2 smem[];
     double2 *C = smem;
@@ -396,6 +405,7 @@ cudaError_t set_fft_attrs(bph_ctx *c) {
 template <int M>
 cudaError_t fwd_rho(bph_ctx *c, const double *rho, double *R, double *mom, long long mstride, int *status,
                     FftBatch bt, int npos) {
+    constexpr int kTile = tile_cols<M>();
     unsigned blocks = (unsigned)((c->np + kTile - 1) / kTile);
     cudaLaunchAttribute attr[1];
     cudaLaunchConfig_t cfg =
@@ -407,6 +417,7 @@ cudaError_t fwd_rho(bph_ctx *c, const double *rho, double *R, double *mom, long 
 
 template <int M>
 cudaError_t fwd_pot(bph_ctx *c, const double *pot) {
+    constexpr int kTile = tile_cols<M>();
     unsigned blocks = (unsigned)((c->np + kTile - 1) / kTile);
     k_fft_fwd<M, false><<<blocks, FftShape<M>::kThreads, FftShape<M>::kSmem, c->stream>>>(
         pot, c->d_P, nullptr, c->d_tw, c->d_tw2, c->d_ph, c->g.numr, c->g.numz, c->nr, c->nz, c->g.mmax, c->fm,
@@ -416,6 +427,7 @@ cudaError_t fwd_pot(bph_ctx *c, const double *pot) {
 
 template <int M>
 cudaError_t inv(bph_ctx *c, double *pot, double *phieff, double omega, const double *P, FftBatch bt, int npos) {
+    constexpr int kTile = tile_cols<M>();
     unsigned blocks = (unsigned)((c->nplane + kTile - 1) / kTile);
     cudaLaunchAttribute attr[1];
     cudaLaunchConfig_t cfg =
