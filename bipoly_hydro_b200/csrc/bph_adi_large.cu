@@ -372,40 +372,47 @@ __global__ void __launch_bounds__(kPanelThreads) k_large_vertical(Large<T> a, in
 }
 
 // FP64 residual r = -4 pi rho_hat - A phi of the current potential (its
-// Dirichlet columns through the stencil), stored in T; delta = 0.
+// Dirichlet columns through the stencil), stored in T; delta = 0.  Thread
+// per (position, slot, zone); P and R of instance map[position] (map
+// nullptr: position = instance), r and delta by position.
 template <typename T>
 __global__ void k_large_defect_prologue(const double *__restrict__ P, const double *__restrict__ R,
                                         const double *__restrict__ brb, const double *__restrict__ alphar,
                                         const double *__restrict__ betar, const double *__restrict__ bzb,
-                                        double gamma, int numr, int numz, int nr, int nz, int N, int isym,
-                                        T *__restrict__ r, T *__restrict__ delta) {
+                                        double gamma, int numr, int numz, int nr, int nz, int N, int isym, int npos,
+                                        const int *__restrict__ map, T *__restrict__ r, T *__restrict__ delta) {
     const long long np = (long long)nr * nz, nplane = (long long)numr * numz;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= np * N) return;
-    const int s = (int)(t / np);
-    const long long e = t - s * np;
+    if (t >= np * N * npos) return;
+    const long long sp = t / np;  // position * N + slot
+    const int row = (int)(sp / N), s = (int)(sp % N);
+    const long long si = (long long)(map ? map[row] : row) * N + s;
+    const long long e = t - sp * np;
     const int j = (int)(e % nr), k = (int)(e / nr);
     const bool sym_bottom = (isym != 1);
-    const double *pc = P + s * nplane + (long long)numr * (k + 1) + 1;
+    const double *pc = P + si * nplane + (long long)numr * (k + 1) + 1;
     const double c = pc[j], east = pc[j + 1], n = pc[j + numr];
     const double w = (j > 0) ? pc[j - 1] : 0.0;
     const double so = (k > 0 || !sym_bottom) ? pc[j - numr] : 0.0;
     const double *b = brb + (long long)s * numr;
     const double ar = b[j + 1] * c + alphar[j + 1] * east + betar[j + 1] * w;
     const double az = bzb[k + 1] * c - gamma * n - gamma * so;
-    r[t] = (T)(R[t] - ar - az);
+    r[t] = (T)(R[si * np + e] - ar - az);
     delta[t] = (T)0;
 }
 
-// phi += delta in FP64 and the per-slot |delta|^2, |phi|^2 (one CTA per slot)
+// phi += delta in FP64 and the per-slot |delta|^2, |phi|^2 (one CTA per
+// position and slot; norms indexed by instance * N + slot)
 template <typename T>
 __global__ void __launch_bounds__(256) k_large_defect_epilogue(double *__restrict__ P, const T *__restrict__ delta,
                                                                int numr, int numz, int nr, int nz, int N,
+                                                               const int *__restrict__ map,
                                                                double *__restrict__ norms) {
-    const int s = blockIdx.x;
+    const int row = blockIdx.x / N, s = blockIdx.x % N;
+    const long long si = (long long)(map ? map[row] : row) * N + s;
     const long long np = (long long)nr * nz, nplane = (long long)numr * numz;
-    double *Pg = P + s * nplane;
-    const T *d = delta + s * np;
+    double *Pg = P + si * nplane;
+    const T *d = delta + (long long)blockIdx.x * np;
     double sd = 0.0, sp = 0.0;
     for (long long e = threadIdx.x; e < np; e += 256) {
         const int j = (int)(e % nr), k = (int)(e / nr);
@@ -431,7 +438,7 @@ __global__ void __launch_bounds__(256) k_large_defect_epilogue(double *__restric
         double t = 0.0;
         for (int w = 0; w < 8; ++w) t += red[2 * w + threadIdx.x];
         const double wgt = (s == 0 || s == N / 2) ? 1.0 : 2.0;
-        norms[2 * s + threadIdx.x] = wgt * t;
+        norms[2 * si + threadIdx.x] = wgt * t;
     }
 }
 
@@ -551,18 +558,19 @@ cudaError_t launch_adi_large(bph_ctx *c, const Schedule &sch, int step0, int nst
     return e;
 }
 
-cudaError_t launch_adi_defect_large(bph_ctx *c, const Schedule &sch) {
+cudaError_t launch_adi_defect_large_batch(bph_ctx *c, const Schedule &sch, double *P, const double *R, int npos,
+                                         const int *d_map, float *work, double *norms) {
     if (!c->large_kb[1]) return cudaErrorNotSupported;
-    const long long np = c->np;
-    float *r = c->d_work32, *delta = r + (long long)c->N * np, *W = delta + (long long)c->N * np,
-          *Q = W + (long long)c->N * np;
-    const long long total = np * c->N;
+    if (npos < 1 || (long long)npos * c->N > 65535) return cudaErrorInvalidConfiguration;  // grid.y limit
+    const long long np = c->np, span = (long long)npos * c->N * np;
+    float *r = work, *delta = r + span, *W = delta + span, *Q = W + span;
+    const int rows = npos * c->N;
     ++c->launches;
-    k_large_defect_prologue<float><<<(unsigned)((total + 255) / 256), 256, 0, c->stream>>>(
-        c->d_P, c->d_R, c->d_brb, c->d_alphar, c->d_betar, c->d_bzb, c->gamma, c->g.numr, c->g.numz, c->nr, c->nz,
-        c->N, c->g.isym, r, delta);
+    k_large_defect_prologue<float><<<(unsigned)((span + 255) / 256), 256, 0, c->stream>>>(
+        P, R, c->d_brb, c->d_alphar, c->d_betar, c->d_bzb, c->gamma, c->g.numr, c->g.numz, c->nr, c->nz, c->N,
+        c->g.isym, npos, d_map, r, delta);
     cudaError_t e = cudaGetLastError();
-    Large<float> a = base_args<float>(c, sch);
+    Large<float> a = base_args<float>(c, sch);  // work arrays by position: no map
     a.phi = delta;
     a.phi_slot = np;
     a.phi_off = 0;
@@ -575,19 +583,23 @@ cudaError_t launch_adi_defect_large(bph_ctx *c, const Schedule &sch) {
     // steps 0..n-1; each emits the next one's right-hand side at its dt
     const int nhalf = 2 * sch.nsteps + 1;
     auto step_of = [](int h) { return (h % 2 == 0) ? (h / 2 - 1 > 0 ? h / 2 - 1 : 0) : (h - 1) / 2; };
-    if (e == cudaSuccess) e = rhs0_launch(c, a, c->N, sch.h_dt[0], true);  // delta = 0
+    if (e == cudaSuccess) e = rhs0_launch(c, a, rows, sch.h_dt[0], true);  // delta = 0
     for (int h = 0; h < nhalf && e == cudaSuccess; ++h) {
         const bool last = (h == nhalf - 1);
         const double dt_next = last ? 0.0 : sch.h_dt[step_of(h + 1)];
-        e = panel_launch(c, a, (h % 2) == 0, c->N, step_of(h), dt_next, last);
+        e = panel_launch(c, a, (h % 2) == 0, rows, step_of(h), dt_next, last);
     }
     if (e == cudaSuccess) {
         ++c->launches;
-        k_large_defect_epilogue<float><<<c->N, 256, 0, c->stream>>>(c->d_P, delta, c->g.numr, c->g.numz, c->nr, c->nz,
-                                                                    c->N, c->d_red);
+        k_large_defect_epilogue<float><<<(unsigned)rows, 256, 0, c->stream>>>(P, delta, c->g.numr, c->g.numz, c->nr,
+                                                                             c->nz, c->N, d_map, norms);
         e = cudaGetLastError();
     }
     return e;
+}
+
+cudaError_t launch_adi_defect_large(bph_ctx *c, const Schedule &sch) {
+    return launch_adi_defect_large_batch(c, sch, c->d_P, c->d_R, 1, nullptr, c->d_work32, c->d_red);
 }
 
 }  // namespace bph

@@ -45,6 +45,7 @@ struct bph_batch {
     int stage_cap = 0;         // positions of the host-array staging buffers
     double *d_LW = nullptr, *d_LQ = nullptr;  // grid-wide ADI scratch [cap][N][np] (large slots)
     double *d_prev = nullptr;         // converged FP64 solves: slot arrays of the previous cycle (on first use)
+    double *d_work32 = nullptr;       // mixed converged on grid-wide kernels: 4 * cap * N * np floats
     double *d_cnorm = nullptr;        // converged solves: per (instance, slot) norm pairs [cap][N][2]
     double *h_cnorm = nullptr;        // its pinned host copy
     double *d_cpart = nullptr;        // split-K partial sums of k_contract_batch
@@ -347,7 +348,7 @@ int bph_batch_destroy(bph_batch_t *b) {
     if (b->c && b->c->stream) cudaStreamSynchronize(b->c->stream);
     if (b->blas) cublasDestroy(b->blas);
     double *bufs[] = {b->d_P,     b->d_R,     b->d_mom, b->d_C,    b->d_rho_stage, b->d_pot_stage,
-                      b->d_cpart, b->d_LW,    b->d_LQ,  b->d_prev, b->d_cnorm};
+                      b->d_cpart, b->d_LW,    b->d_LQ,  b->d_prev, b->d_cnorm, b->d_work32};
     for (double *p : bufs)
         if (p) cudaFree(p);
     if (b->d_ccnt) cudaFree(b->d_ccnt);
@@ -380,8 +381,8 @@ int bph_batch_solve_converged(bph_batch_t *b, int n, const double *const *rho, d
         return BPH_ERR_INVALID;
     }
     bph_ctx *c = b->c;
-    if (mixed && (!c->adi_mixed_smem || c->mixed_kind == BPH_MIXED_ADI_GLOBAL)) {
-        set_error("mixed batched solves need an on-chip refinement kernel (this grid's slots exceed shared memory)");
+    if (mixed && !c->adi_mixed_smem) {
+        set_error("no mixed-precision ADI kernel is configured for this grid");
         return BPH_ERR_INVALID;
     }
     BatchConv cv;
@@ -577,12 +578,16 @@ int batch_enqueue(bph_batch *b, int n, const double *const *d_in, double *const 
     return BPH_OK;
 }
 
-int batch_reserve_converged(bph_batch *b, bool fp64) {
+int batch_reserve_converged(bph_batch *b, bool mixed) {
     bph_ctx *c = b->c;
     int rc;
     if (!b->d_cnorm && (rc = batch_alloc(b, &b->d_cnorm, 2ull * b->cap * c->N))) return rc;
     if (!b->h_cnorm) BPH_CUDA(cudaMallocHost((void **)&b->h_cnorm, sizeof(double) * 2 * (size_t)b->cap * c->N));
-    if (fp64 && !b->d_prev && (rc = batch_alloc(b, &b->d_prev, (size_t)b->cap * c->N * c->nplane))) return rc;
+    if (!mixed && !b->d_prev && (rc = batch_alloc(b, &b->d_prev, (size_t)b->cap * c->N * c->nplane))) return rc;
+    // the grid-wide refinement cycle keeps r, delta and two right-hand sides per position (FP32)
+    if (mixed && c->mixed_kind == BPH_MIXED_ADI_GLOBAL && !b->d_work32 &&
+        (rc = batch_alloc(b, &b->d_work32, 2ull * b->cap * c->N * c->np)))
+        return rc;
     return BPH_OK;
 }
 
@@ -613,7 +618,7 @@ int batch_converged_run(bph_batch *b, int n, const int *inst, const int *d_map, 
     const size_t ibytes = sizeof(double) * (size_t)c->N * c->nplane;  // one instance's slot arrays
     int top = 0;  // instances 0..top-1 hold every position's norms
     for (int i = 0; i < n; ++i) top = std::max(top, inst[i] + 1);
-    if ((rc = batch_reserve_converged(b, !cv.mixed))) return rc;
+    if ((rc = batch_reserve_converged(b, cv.mixed))) return rc;
     if (cv.cold)  // before the Dirichlet slots
         for (int i = 0; i < n; ++i)
             BPH_CUDA(cudaMemsetAsync(b->d_P + (size_t)inst[i] * c->N * c->nplane, 0, ibytes, c->stream));
@@ -625,7 +630,11 @@ int batch_converged_run(bph_batch *b, int n, const int *inst, const int *d_map, 
     bool diverged = false;
     for (;;) {
         if (cv.mixed) {
-            BPH_CUDA(launch_defect_batch(c, *s, b->d_P, b->d_R, n, d_map, b->d_cnorm));
+            if (c->mixed_kind == BPH_MIXED_ADI_GLOBAL)
+                BPH_CUDA(launch_adi_defect_large_batch(c, *s, b->d_P, b->d_R, n, d_map,
+                                                       reinterpret_cast<float *>(b->d_work32), b->d_cnorm));
+            else
+                BPH_CUDA(launch_defect_batch(c, *s, b->d_P, b->d_R, n, d_map, b->d_cnorm));
         } else {
             if (d_map) {
                 for (int i = 0; i < n; ++i) {

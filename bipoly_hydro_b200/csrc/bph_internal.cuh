@@ -244,6 +244,11 @@ cudaError_t launch_adi_large(bph_ctx *c, const Schedule &s, int step0, int nstep
                              const double *R, int ninst = 1, const int *d_inst_map = nullptr, double *W = nullptr,
                              double *Q = nullptr);
 cudaError_t launch_adi_defect_large(bph_ctx *c, const Schedule &s);
+// The same FP32 refinement cycle for npos batch positions (instance
+// d_map[i], nullptr: position = instance) of batch arrays P/R; work: 4 *
+// npos * N * np floats; norms by instance * N + slot.
+cudaError_t launch_adi_defect_large_batch(bph_ctx *c, const Schedule &s, double *P, const double *R, int npos,
+                                         const int *d_map, float *work, double *norms);
 // Panel sizes and shared-memory limits of the grid-wide ADI kernels.
 int large_configure(bph_ctx *c);
 cudaError_t launch_update_norm(bph_ctx *c, double *d_out);
@@ -269,9 +274,10 @@ struct BatchConv {
     bool want_resid = false;
     bool report_divergence = true;  // false: per-position status reports bad densities
 };
-// Norm buffers (and, for FP64, the previous-cycle slot arrays) of converged
-// batched calls, allocated ahead of the first one.
-int batch_reserve_converged(bph_batch *b, bool fp64);
+// Norm buffers (FP64: the previous-cycle slot arrays; mixed on grid-wide
+// kernels: the FP32 work arrays) of converged batched calls, allocated ahead
+// of the first one.
+int batch_reserve_converged(bph_batch *b, bool mixed);
 int batch_solve_core(bph_batch *b, int n, const int *instances, const double *const *rho, double *const *pot,
                      bool warm, bool on_device, int *pos_status, BatchConv *conv = nullptr);
 // Raises the dynamic shared memory limit of kernel fn on the current device

@@ -215,14 +215,14 @@ int bph_server_set_converged(bph_server_t *s, int nsteps, double tol, int max_cy
         return BPH_ERR_INVALID;
     }
     bph_ctx *c = s->c;
-    if (nsteps > 0 && mixed && (!c->adi_mixed_smem || c->mixed_kind == BPH_MIXED_ADI_GLOBAL)) {
-        set_error("mixed converged serving needs an on-chip refinement kernel (slots that fit shared memory)");
+    if (nsteps > 0 && mixed && !c->adi_mixed_smem) {
+        set_error("no mixed-precision ADI kernel is configured for this grid");
         return BPH_ERR_INVALID;
     }
     std::lock_guard<std::mutex> lk(s->mu);
     if (nsteps > 0) {
         // buffers first: a batch the worker takes after the mode changes finds them
-        const int rc = batch_reserve_converged(s->batch, !mixed);
+        const int rc = batch_reserve_converged(s->batch, mixed != 0);
         if (rc) return rc;
     }
     s->conv_nsteps = nsteps;

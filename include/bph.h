@@ -136,8 +136,8 @@ int bph_batch_solve_instances(bph_batch_t *batch, int n, const int *instances, c
  * FP64 defect, which also stop once a cycle no longer halves the update) or
  * max_cycles.  cycles_out: cycles run; resid_out: the largest relative FP64
  * residual over the instances (NULL skips it).  One host synchronisation
- * per cycle.  Mixed needs an on-chip refinement kernel (slots that fit
- * shared memory). */
+ * per cycle.  Mixed runs the context's refinement kernel (on-chip, or the
+ * grid-wide one for slots beyond shared memory). */
 int bph_batch_solve_converged(bph_batch_t *batch, int n, const double *const *rho, double *const *pot, int nsteps,
                               int cold, double tol, int max_cycles, int mixed, int on_device, int *cycles_out,
                               double *resid_out);

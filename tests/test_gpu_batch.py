@@ -99,15 +99,15 @@ def test_batch_rejects_bad_sizes(bph):
 @pytest.mark.parametrize("grid", [(66, 66, 64, 1.0 / 62.0, 2, 30), (202, 152, 16, 1.0 / 200.0, 2, 4)],
                          ids=["66x66x64", "grid-wide-adi"])
 def test_batch_converged_equals_single_converged(bph, grid):
-    """Converged batched solves (FP64, and the FP32 refinement where the grid
-    has an on-chip refinement kernel) against single converged FP64 solves of
-    each instance: cold, then warm after the densities move."""
+    """Converged batched solves (FP64, and the FP32 refinement: on-chip kernels
+    or, for slots beyond shared memory, the grid-wide ones) against single
+    converged FP64 solves of each instance: cold, then warm after the
+    densities move."""
     n = 3
     rhos = _densities(grid, n)
     solver = bph.PotentialSolver(*grid)
-    on_chip = solver.info()["adi_threads"] > 0
     batch = bph.Batch(solver, capacity=n)
-    mixed_batch = bph.Batch(solver, capacity=n) if on_chip else None  # its own warm states
+    mixed_batch = bph.Batch(solver, capacity=n)  # its own warm states
     singles = [bph.PotentialSolver(*grid) for _ in range(n)]
     for cold in (True, False):
         if not cold:
@@ -117,15 +117,10 @@ def test_batch_converged_equals_single_converged(bph, grid):
         assert 1 <= info.cycles <= 80 and info.residual < 1e-8
         for i in range(n):
             assert rel_l2(got[i], want[i]) <= 1e-10, (cold, i)
-        if mixed_batch is not None:
-            gm, _ = mixed_batch.solve_converged(rhos, nsteps=10, cold=cold, tol=1e-12, max_cycles=80, mixed=True)
-            for i in range(n):
-                assert rel_l2(gm[i], want[i]) <= 1e-9, ("mixed", cold, i)
-    if mixed_batch is None:
-        with pytest.raises(bph.BphError):
-            batch.solve_converged(rhos, mixed=True)
-    else:
-        mixed_batch.close()
+        gm, _ = mixed_batch.solve_converged(rhos, nsteps=10, cold=cold, tol=1e-12, max_cycles=80, mixed=True)
+        for i in range(n):
+            assert rel_l2(gm[i], want[i]) <= 1e-9, ("mixed", cold, i)
+    mixed_batch.close()
     for s in singles:
         s.close()
     batch.close()

@@ -138,3 +138,25 @@ def test_contexts_set_up_largest_first_keep_working(bph):
     for s in smaller:
         s.close()
     a.close()
+
+
+def test_large_grid_server_mixed_converged(bph):
+    """Serving on a grid whose slots exceed shared memory, in mixed converged
+    mode: the grid-wide FP32 refinement runs on client slots through the
+    instance map; every result is the converged FP64 solution to 1e-9."""
+    rhos = _densities(LARGE, 3, seed=500)
+    g = bph.PotentialSolver(*LARGE)
+    srv = bph.Server(g, max_clients=3)
+    srv.set_converged(nsteps=10, tol=1e-12, max_cycles=80, mixed=True)
+    clients = [srv.open_client() for _ in range(3)]
+    rids = [srv.submit(clients[2], rhos[2]), srv.submit(clients[0], rhos[0])]
+    rhos2 = [np.asfortranarray(np.roll(r, 1, axis=2)) for r in rhos]
+    rids.append(srv.submit(clients[0], rhos2[0]))  # warm, after the first request of client 0
+    ref = bph.PotentialSolver(*LARGE)
+    for rid, rho in zip(rids, [rhos[2], rhos[0], rhos2[0]]):
+        pot, _ = srv.wait(rid, timeout=120.0)
+        want, _ = ref.solve_converged(rho, 10, True, 1e-13, 200)
+        assert rel_l2(pot, want) <= 1e-9
+    srv.close()
+    ref.close()
+    g.close()
