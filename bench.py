@@ -467,6 +467,29 @@ def mixed_grid_bench(B, torch, dev, args, stream):
     torch.cuda.synchronize()
     ms_serial = ea.elapsed_time(eb) / calls
 
+    # converged solves of every instance, FP64 against mixed precision (cold starts, so both
+    # forms run their full cycle count; one batched call per grid, grids in turn)
+    conv = {}
+    for key, mixed in (("fp64", False), ("mixed", True)):
+        for bt, r, p in parts:  # untimed: builds schedules and work arrays
+            bt.solve_converged_device(r, p, args.conv_nsteps, True, args.conv_tol, 100, mixed)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cyc = []
+        for bt, r, p in parts:
+            cyc.append(bt.solve_converged_device(r, p, args.conv_nsteps, True, args.conv_tol, 100, mixed).cycles)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        conv[key] = {"ms": 1e3 * el, "solves_per_s": n / el, "cycles_per_grid": cyc}
+        if not mixed:
+            ref = [[x.clone() for x in p] for _, _, p in parts]
+        else:
+            conv[key]["max_rel_err_vs_fp64"] = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+                                                   for (_, _, p), rp in zip(parts, ref) for a, b in zip(p, rp))
+            del ref
+    conv["speedup_mixed_vs_fp64"] = conv["mixed"]["solves_per_s"] / conv["fp64"]["solves_per_s"]
+    conv["nsteps_per_cycle"], conv["tol_update"] = args.conv_nsteps, args.conv_tol
+
     plan = B.Plan(parts)
     plan.launch(0, stream)
     for w in range(3):
@@ -493,7 +516,8 @@ def mixed_grid_bench(B, torch, dev, args, stream):
             "plan_solves_per_s": n / (ms_plan / 1e3), "plan_ms_per_launch": ms_plan,
             "plan_kernel_launches": launches,
             "serial_batches_solves_per_s": n / (ms_serial / 1e3), "serial_ms_per_round": ms_serial,
-            "setup_s": setup_s, "precision": "f64 drop-in (5 warm ADI steps)", "calls": calls}
+            "setup_s": setup_s, "precision": "f64 drop-in (5 warm ADI steps)", "calls": calls,
+            "converged": conv}
 
 
 def large_grid_bench(B, torch, dev, args, stream):
