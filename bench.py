@@ -359,7 +359,7 @@ def serve_mixed_bench(B, torch, dev, args):
     gen.manual_seed(20261204)
     out = {"grids": {f"{a}x{b}x{c}": shape_of.count(g) for g, (a, b, c, _) in enumerate(MIXED_GRIDS)},
            "clients": nclients, "requests_per_rate": nclients * iters, "dtype": "f64", "rates": []}
-    for rate in [float(x) for x in args.serve_mixed_rates.split(",") if x]:
+    def run_rate(rate):
         ids = [servers[shape_of[c]].open_client() for c in range(nclients)]
         rho = [[bases[shape_of[c]][c % 2] * (1.0 + 0.2 * c / nclients), None] for c in range(nclients)]
         for r in rho:
@@ -392,14 +392,27 @@ def serve_mixed_bench(B, torch, dev, args):
             lat.append(v)
             lat_g[shape_of[c]].append(v)
         elapsed = time.perf_counter() - t0
-        out["rates"].append({
+        res = {
             "offered_req_per_s": rate, "solves_per_s": nclients * iters / elapsed,
             "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
             "p50_ms_per_grid": {f"{a}x{b}x{c2}": (1e3 * float(np.percentile(lg, 50)) if lg else None)
-                                for (a, b, c2, _), lg in zip(MIXED_GRIDS, lat_g)}})
+                                for (a, b, c2, _), lg in zip(MIXED_GRIDS, lat_g)}}
         for c in range(nclients):
             servers[shape_of[c]].close_client(ids[c])
-        del rho, pot
+        return res
+
+    for rate in [float(x) for x in args.serve_mixed_rates.split(",") if x]:
+        out["rates"].append(run_rate(rate))
+    # converged serving over the grid mix, FP64 against mixed precision
+    conv_rates = [float(x) for x in args.serve_conv_rates.split(",") if x][:1]
+    if conv_rates:
+        out["converged"] = {"nsteps_per_cycle": args.conv_nsteps, "tol_update": args.conv_tol}
+        for key, mixed in (("fp64", False), ("mixed", True)):
+            for srv in servers:
+                srv.set_converged(args.conv_nsteps, args.conv_tol, 100, mixed)
+            out["converged"][key] = [run_rate(r) for r in conv_rates]
+        for srv in servers:
+            srv.set_converged(0)
     for srv in servers:
         srv.close()
     for sv in solvers:
