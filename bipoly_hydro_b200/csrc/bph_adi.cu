@@ -800,10 +800,44 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
     }
     pdl_trigger();
     if (!kDefect) {
-        for (int k = warp; k < nz; k += nwarps) {
-            double *prow = Pg + (long long)numr * (k + 1) + 1;
+        if (!a.norms) {
+            for (int k = warp; k < nz; k += nwarps) {
+                double *prow = Pg + (long long)numr * (k + 1) + 1;
 #pragma unroll 4
-            for (int j = lane; j < nr; j += 32) prow[j] = (double)Ww[k * ps + j];
+                for (int j = lane; j < nr; j += 32) prow[j] = (double)Ww[k * ps + j];
+            }
+        } else {
+            // converged cycles: the update against the potential being
+            // overwritten, |new - old|^2 and |new|^2 per slot, in the write-back
+            double sd = 0.0, sp = 0.0;
+            for (int k = warp; k < nz; k += nwarps) {
+                double *prow = Pg + (long long)numr * (k + 1) + 1;
+#pragma unroll 2
+                for (int j = lane; j < nr; j += 32) {
+                    const double v = (double)Ww[k * ps + j];
+                    const double d = v - prow[j];
+                    prow[j] = v;
+                    sd += d * d;
+                    sp += v * v;
+                }
+            }
+            for (int off = 16; off > 0; off >>= 1) {
+                sd += __shfl_down_sync(0xffffffffu, sd, off);
+                sp += __shfl_down_sync(0xffffffffu, sp, off);
+            }
+            __syncthreads();
+            double *red = reinterpret_cast<double *>(smraw);
+            if (lane == 0) {
+                red[2 * warp] = sd;
+                red[2 * warp + 1] = sp;
+            }
+            __syncthreads();
+            if (tid < 2) {
+                double t = 0.0;
+                for (int w = 0; w < nwarps; ++w) t += red[2 * w + tid];
+                const double wgt = (s == 0 || s == a.N / 2) ? 1.0 : 2.0;
+                a.norms[2 * blk + tid] = wgt * t;
+            }
         }
     } else {
         // phi += delta in FP64; per-slot |delta|^2 and |phi|^2
@@ -1318,7 +1352,7 @@ AdiArgs make_args(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bo
     a.betar = c->d_betar;
     a.brb = c->d_brb;
     a.bzb = c->d_bzb;
-    a.norms = c->d_red;
+    a.norms = nullptr;  // FP64 sweeps: set to get update norms from the write-back
     a.inst_map = nullptr;
     a.slot_map = nullptr;
     a.nslots = c->N;
@@ -1341,11 +1375,13 @@ AdiArgs make_args(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bo
 }
 
 cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_run, bool cold, double *P,
-                       const double *R, int ninst, const int *d_inst_map) {
+                       const double *R, int ninst, const int *d_inst_map, double *norms) {
     AdiArgs a = make_args(c, sch, step0, nsteps_run, cold);
     if (P) a.P = P;
     if (R) a.R = R;
     a.inst_map = d_inst_map;
+    if (norms && !c->adi_seg) return cudaErrorNotSupported;  // only the segmented kernel reports them
+    a.norms = norms;
     if (c->adi_seg) {
         ++c->launches;
         void *args[] = {&a};
@@ -1390,6 +1426,7 @@ cudaError_t launch_adi_slots(bph_ctx *c, const Schedule &sch, bool cold, const i
 cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {
     if (!c->adi_mixed_smem) return cudaErrorNotSupported;
     AdiArgs a = make_args(c, sch, 0, sch.nsteps, false);
+    a.norms = c->d_red;
     a.rad_pk = sch.d_rad_pk[1];  // float blocks for the FP32 kernels
     a.ver_pk = sch.d_ver_pk[1];
     a.pkr = packed_block<float>(c->nr);

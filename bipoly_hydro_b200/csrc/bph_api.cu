@@ -694,6 +694,8 @@ static int converged_impl(bph_ctx *c, const double *rho, double *pot, int nsteps
         for (;;) {
             if (mixed) {
                 BPH_CUDA(launch_adi_defect(c, *s));
+            } else if (c->adi_seg) {  // update norms from the sweep's write-back
+                BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, false, nullptr, nullptr, 1, nullptr, c->d_red));
             } else {
                 BPH_CUDA(cudaMemcpyAsync(c->d_prev, c->d_P, bytes, cudaMemcpyDeviceToDevice, c->stream));
                 BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, false));

@@ -583,7 +583,11 @@ int batch_reserve_converged(bph_batch *b, bool mixed) {
     int rc;
     if (!b->d_cnorm && (rc = batch_alloc(b, &b->d_cnorm, 2ull * b->cap * c->N))) return rc;
     if (!b->h_cnorm) BPH_CUDA(cudaMallocHost((void **)&b->h_cnorm, sizeof(double) * 2 * (size_t)b->cap * c->N));
-    if (!mixed && !b->d_prev && (rc = batch_alloc(b, &b->d_prev, (size_t)b->cap * c->N * c->nplane))) return rc;
+    // FP64 on the grid-wide kernels: the previous cycle's slot arrays (the segmented kernel
+    // forms the update while writing back)
+    if (!mixed && !c->adi_seg && !b->d_prev &&
+        (rc = batch_alloc(b, &b->d_prev, (size_t)b->cap * c->N * c->nplane)))
+        return rc;
     // the grid-wide refinement cycle keeps r, delta and two right-hand sides per position (FP32)
     if (mixed && c->mixed_kind == BPH_MIXED_ADI_GLOBAL && !b->d_work32 &&
         (rc = batch_alloc(b, &b->d_work32, 2ull * b->cap * c->N * c->np)))
@@ -635,6 +639,8 @@ int batch_converged_run(bph_batch *b, int n, const int *inst, const int *d_map, 
                                                        reinterpret_cast<float *>(b->d_work32), b->d_cnorm));
             else
                 BPH_CUDA(launch_defect_batch(c, *s, b->d_P, b->d_R, n, d_map, b->d_cnorm));
+        } else if (c->adi_seg) {  // update norms from the sweep's write-back
+            BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, false, b->d_P, b->d_R, n, d_map, b->d_cnorm));
         } else {
             if (d_map) {
                 for (int i = 0; i < n; ++i) {
@@ -645,10 +651,7 @@ int batch_converged_run(bph_batch *b, int n, const int *inst, const int *d_map, 
             } else {
                 BPH_CUDA(cudaMemcpyAsync(b->d_prev, b->d_P, ibytes * n, cudaMemcpyDeviceToDevice, c->stream));
             }
-            if (c->adi_seg)
-                BPH_CUDA(launch_adi(c, *s, 0, s->nsteps, false, b->d_P, b->d_R, n, d_map));
-            else
-                BPH_CUDA(launch_adi_large(c, *s, 0, s->nsteps, false, b->d_P, b->d_R, n, d_map, b->d_LW, b->d_LQ));
+            BPH_CUDA(launch_adi_large(c, *s, 0, s->nsteps, false, b->d_P, b->d_R, n, d_map, b->d_LW, b->d_LQ));
             BPH_CUDA(launch_norms_batch(c, false, b->d_P, b->d_prev, nullptr, n, d_map, b->d_cnorm));
         }
         ++cyc;

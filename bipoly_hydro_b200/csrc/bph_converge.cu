@@ -97,6 +97,8 @@ static int build_conv_graph(bph_ctx *c, Schedule &s, bool mixed, cudaGraphExec_t
         cudaError_t ce = cudaSuccess;
         if (mixed) {
             ce = launch_adi_defect(c, s);
+        } else if (c->adi_seg) {  // the update norms come from the sweep's write-back
+            ce = launch_adi(c, s, 0, s.nsteps, false, nullptr, nullptr, 1, nullptr, c->d_red);
         } else {
             ce = cudaMemcpyAsync(c->d_prev, c->d_P, sizeof(double) * (size_t)c->N * c->nplane,
                                  cudaMemcpyDeviceToDevice, cs);

@@ -228,8 +228,11 @@ cudaError_t launch_green_contract(bph_ctx *c, bool write_slots = true);
 cudaError_t launch_boundary_slots(bph_ctx *c);
 // ninst instances of slot arrays P/R; block row i solves instance d_inst_map[i]
 // (nullptr: instance i).
+// norms (segmented kernel only): per (instance, slot) |P_new - P_old|^2 and
+// |P_new|^2, formed while the result is written back.
 cudaError_t launch_adi(bph_ctx *c, const Schedule &s, int step0, int nsteps_run, bool cold, double *P = nullptr,
-                       const double *R = nullptr, int ninst = 1, const int *d_inst_map = nullptr);
+                       const double *R = nullptr, int ninst = 1, const int *d_inst_map = nullptr,
+                       double *norms = nullptr);
 // The slots d_slots[0..nslots) of the context's own arrays, on stream st
 // (pdl: with programmatic dependent launch on that stream).
 cudaError_t launch_adi_slots(bph_ctx *c, const Schedule &s, bool cold, const int *d_slots, int nslots,
