@@ -809,16 +809,39 @@ __global__ void __launch_bounds__(kSegThreads, kDefect ? 2 : 1) k_adi_seg(AdiArg
         } else {
             // converged cycles: the update against the potential being
             // overwritten, |new - old|^2 and |new|^2 per slot, in the write-back
+            // the old values of two rows x 4 columns per lane are loaded before any store
+            // (eight global loads in flight instead of one)
             double sd = 0.0, sp = 0.0;
-            for (int k = warp; k < nz; k += nwarps) {
-                double *prow = Pg + (long long)numr * (k + 1) + 1;
-#pragma unroll 2
-                for (int j = lane; j < nr; j += 32) {
-                    const double v = (double)Ww[k * ps + j];
-                    const double d = v - prow[j];
-                    prow[j] = v;
-                    sd += d * d;
-                    sp += v * v;
+            constexpr int kQ = 4;
+            for (int k0 = warp; k0 < nz; k0 += 2 * nwarps) {
+                for (int j0 = lane; j0 < nr; j0 += 32 * kQ) {
+                    double o[2][kQ];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int k = k0 + h * nwarps;
+                        const double *prow = Pg + (long long)numr * (k + 1) + 1;
+#pragma unroll
+                        for (int q = 0; q < kQ; ++q) {
+                            const int j = j0 + 32 * q;
+                            o[h][q] = (k < nz && j < nr) ? prow[j] : 0.0;
+                        }
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int k = k0 + h * nwarps;
+                        if (k >= nz) continue;
+                        double *prow = Pg + (long long)numr * (k + 1) + 1;
+#pragma unroll
+                        for (int q = 0; q < kQ; ++q) {
+                            const int j = j0 + 32 * q;
+                            if (j >= nr) continue;
+                            const double v = (double)Ww[k * ps + j];
+                            const double d = v - o[h][q];
+                            prow[j] = v;
+                            sd += d * d;
+                            sp += v * v;
+                        }
+                    }
                 }
             }
             for (int off = 16; off > 0; off >>= 1) {
