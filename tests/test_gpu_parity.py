@@ -1,8 +1,7 @@
 """CUDA solver vs the CPU oracle through the C ABI (FP64 drop-in parity).
 
-The bar is the one the north star sets for the FP64 form: relative L2 error of
-the potential <= 1e-12 against the reference algorithm with the same ADI step
-count.  Tables and boundary moments are compared on their own as well.
+The bar for the FP64 form: relative L2 error of the potential <= 1e-12 against
+the reference algorithm with the same ADI step count.  Tables and boundary moments are compared on their own as well.
 """
 import numpy as np
 import pytest
@@ -179,7 +178,7 @@ def test_gpu_reproduces_golden_fixture(bph, path):
 def test_mixed_converged_within_1e9_of_fp64(oracle_mod, bph, grid, kind):
     """FP32 ADI + FP64 residual/update refinement converges to the FP64 discrete
     solution: relative L2 error <= 1e-9 against the GPU FP64 converged solve
-    and against the oracle's converged solve (north-star bound for the mixed form),
+    and against the oracle's converged solve (the accuracy bound of the mixed form),
     with either refinement ADI kernel."""
     numr, numz, numphi, dr, isym, _ = grid
     g = bph.PotentialSolver(*grid)
