@@ -255,7 +255,7 @@ def run_reference(args, world, rank):
 
 
 def serve_bench(B, torch, dev, rhos, args):
-    """Continuous-batching server under Poisson arrivals (config-5 recipe).
+    """Continuous-batching server under Poisson arrivals of SCF-like client requests.
 
     serve_clients resident clients on the 130x98x256 grid, each running an
     SCF-like sequence rho <- 0.9 rho + 0.1 rho (1 + 0.01 N(0,1)) renormalised

@@ -76,7 +76,7 @@ def test_tstep_one_is_cold(oracle_mod, bph):
     g.close()
 
 
-def test_config1_drop_in_sequence(oracle_mod, bph):
+def test_two_polytropes_66x66x64_drop_in_sequence(oracle_mod, bph):
     """66x66x64, dr=1/62, isym 2, mmax 30: cold start then warm rotated steps."""
     from bipoly_hydro_b200 import fields
 
@@ -309,7 +309,7 @@ def test_global_memory_adi_variant_matches_oracle(oracle_mod, bph):
     g.close()
 
 
-def test_config3_large_grid_gaussian_sphere(bph):
+def test_258x194x512_gaussian_sphere(bph):
     """258x194x512 (dr = 1/250): the drop-in runs (global-memory ADI) and the
     converged FP64 solve of a spherical Gaussian matches its closed-form
     potential -M erf(s/(sqrt2 sigma))/s to second order in dr."""
@@ -333,7 +333,7 @@ def test_config3_large_grid_gaussian_sphere(bph):
     err = rel_l2(pot[sl], exact[sl])
     # the 66x66 grid (dr = 1/62) reaches ~1e-3; dr is 4x smaller here
     assert err < 2e-4, err
-    # mixed precision (config 3): the slots exceed shared memory, so the
+    # mixed precision: the slots exceed shared memory, so the
     # global-memory FP32 refinement kernel is chosen; within 1e-9 of FP64
     assert g.info()["mixed_kind"] == 3
     pmx, imx = g.solve_converged_mixed(rho, 20, True, 1e-12, 60)
