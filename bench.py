@@ -740,9 +740,14 @@ def run_gpu(args, world, rank, local):
     ms_e2e = max_over_ranks(e2.elapsed_time(e3), world)
     e2e_value = job_rate(n_e2e, world, ms_e2e)
 
+    # The sections below are reported by rank 0 only; with several ranks the
+    # others skip them (no collective follows, and the host is not shared by
+    # eight copies of the serving loops).
+    side = rank == 0
+
     # ---- batched solves: n instances per call, one table pass ----------
     batched = None
-    if args.batch_sizes:
+    if side and args.batch_sizes:
         batched = {}
         for nb_ in [int(x) for x in args.batch_sizes.split(",") if x]:
             bt = B.Batch(solver, nb_)
@@ -767,12 +772,12 @@ def run_gpu(args, world, rank, local):
 
     # ---- mixed precision on the large grid and the small field --------
     large_grid = None
-    if not args.no_large_grid:
+    if side and not args.no_large_grid:
         large_grid = large_grid_bench(B, torch, dev, args, stream)
 
     # ---- converged batched solves: FP64 vs mixed ------------------------
     batched_conv = None
-    if args.batch_sizes and args.converged_steps > 0:
+    if side and args.batch_sizes and args.converged_steps > 0:
         nb_ = max(int(x) for x in args.batch_sizes.split(",") if x)
         ins = [rhos[(7 * i) % nrot] for i in range(nb_)]
         batched_conv = {"instances": nb_, "nsteps_per_cycle": args.conv_nsteps, "tol_update": args.conv_tol}
@@ -805,21 +810,21 @@ def run_gpu(args, world, rank, local):
 
     # ---- batches over a mix of grids, one plan launch ------------------
     mixed_grid = None
-    if args.mixed_grid_instances > 0:
+    if side and args.mixed_grid_instances > 0:
         mixed_grid = mixed_grid_bench(B, torch, dev, args, stream)
 
     # ---- serving: Poisson arrivals of SCF-like client requests ----------
     serving = None
-    if args.serve_rates and not args.no_serving:
+    if side and args.serve_rates and not args.no_serving:
         serving = serve_bench(B, torch, dev, rhos, args)
 
     serving_mixed = None
-    if args.serve_mixed_rates and not args.no_serving:
+    if side and args.serve_mixed_rates and not args.no_serving:
         serving_mixed = serve_mixed_bench(B, torch, dev, args)
 
     # ---- converged solves: FP64 vs mixed (FP32 ADI + FP64 refinement) --
     conv = None
-    if args.converged_steps > 0:
+    if side and args.converged_steps > 0:
         conv = {}
         nconv = args.converged_steps
         ref_pots = []
