@@ -31,7 +31,7 @@
 namespace bph {
 namespace {
 
-constexpr int kPanelThreads = 128;
+constexpr int kPanelThreads = 256;
 // Lines of a panel (columns of a vertical panel, at most the rows of a
 // radial one): 16 for FP64, 32 for FP32, so that the lanes sharing a sweep
 // segment fill the shared-memory banks once.
