@@ -63,3 +63,24 @@ def test_product_does_not_import_the_oracle():
             if f.endswith((".py", ".cu", ".cuh", ".h", ".cpp", "Makefile")):
                 src = open(os.path.join(dirpath, f)).read()
                 assert not bad.search(src), f
+
+
+def test_null_handles_of_batches_plans_and_servers_are_errors(bph):
+    """The batch, plan and server entry points reject NULL handles and bad
+    counts before any device work."""
+    import ctypes
+
+    lib = bph.load_library()
+    inv = bph.BPH_ERR_INVALID
+    assert lib.bph_batch_solve(None, 1, None, None, 0, 0) == inv
+    assert lib.bph_batch_solve_converged(None, 1, None, None, 10, 1, 1e-11, 10, 0, 0, None, None) == inv
+    assert lib.bph_batch_destroy(None) == bph.BPH_OK
+    out = ctypes.c_void_p(123)
+    assert lib.bph_plan_create(0, None, None, None, None, ctypes.byref(out)) == inv
+    assert out.value is None  # cleared on failure
+    assert lib.bph_plan_launch(None, 2, None) == inv
+    assert lib.bph_plan_synchronize(None, None) == inv
+    assert lib.bph_plan_launches(None) == 0
+    assert lib.bph_plan_destroy(None) == bph.BPH_OK
+    assert lib.bph_server_set_converged(None, 10, 1e-11, 10, 0) == inv
+    assert lib.bph_server_destroy(None) in (bph.BPH_OK, inv)
