@@ -189,23 +189,38 @@ __device__ __forceinline__ T rhs_radial(const Large<T> &a, const double *Pg, T r
 }
 
 // First radial right-hand side of a sweep: from the potential in phi (or
-// zero when cold), element-wise; grid (j blocks, k, rows * N slots).
+// zero when cold); grid (j blocks, k blocks of kRhs0Rows, rows * N slots).
+// A thread walks kRhs0Rows rows of one column, so each phi value is loaded
+// once and all of its loads are in flight together.
+constexpr int kRhs0Rows = 8;
+
 template <typename T>
 __global__ void __launch_bounds__(128) k_large_rhs0(Large<T> a, T dt, int cold) {
-    const int j = blockIdx.x * 128 + threadIdx.x, k = blockIdx.y;
+    const int j = blockIdx.x * 128 + threadIdx.x, k0 = blockIdx.y * kRhs0Rows;
     if (j >= a.nr) return;
     const int row = blockIdx.z / a.N, sl = blockIdx.z - row * a.N;
     const long long sg = (long long)(a.inst_map ? a.inst_map[row] : row) * a.N + sl;
-    const long long np = (long long)a.nr * a.nz, e = (long long)k * a.nr + j;
+    const long long np = (long long)a.nr * a.nz;
     const double *Pg = a.P ? a.P + sg * (long long)a.numr * a.numz : nullptr;
-    const T *ph = a.phi + sg * a.phi_slot + a.phi_off + (long long)k * a.phi_row + j;
-    T phi = 0, up = 0, dn = 0;
-    if (!cold) {
-        phi = ph[0];
-        if (k + 1 < a.nz) up = ph[a.phi_row];
-        if (k > 0) dn = ph[-a.phi_row];
+    const T *ph = a.phi + sg * a.phi_slot + a.phi_off + j;
+    const T *src = a.src + sg * np + j;
+    T *W = a.W + (long long)blockIdx.z * np + j;
+    T v[kRhs0Rows + 2], r[kRhs0Rows];  // v[m] = phi at row k0 - 1 + m
+#pragma unroll
+    for (int m = 0; m < kRhs0Rows + 2; ++m) {
+        const int k = k0 - 1 + m;
+        v[m] = (!cold && k >= 0 && k < a.nz) ? ph[(long long)k * a.phi_row] : (T)0;
     }
-    a.W[(long long)blockIdx.z * np + e] = rhs_radial(a, Pg, a.src[sg * np + e], phi, up, dn, k, j, dt);
+#pragma unroll
+    for (int m = 0; m < kRhs0Rows; ++m) {
+        const int k = k0 + m;
+        r[m] = (k < a.nz) ? src[(long long)k * a.nr] : (T)0;
+    }
+#pragma unroll
+    for (int m = 0; m < kRhs0Rows; ++m) {
+        const int k = k0 + m;
+        if (k < a.nz) W[(long long)k * a.nr] = rhs_radial(a, Pg, r[m], v[m + 1], v[m + 2], v[m], k, j, dt);
+    }
 }
 
 // Radial half-sweep on a panel of kb rows: W -> (r-lines) -> Q = vertical
@@ -493,8 +508,9 @@ cudaError_t panel_launch(bph_ctx *c, const Large<T> &a, bool radial, int rows, i
 template <typename T>
 cudaError_t rhs0_launch(bph_ctx *c, const Large<T> &a, int rows, double dt, bool cold) {
     ++c->launches;
-    k_large_rhs0<T><<<dim3((unsigned)((c->nr + 127) / 128), (unsigned)c->nz, (unsigned)rows), 128, 0, c->stream>>>(
-        a, (T)dt, cold ? 1 : 0);
+    k_large_rhs0<T><<<dim3((unsigned)((c->nr + 127) / 128), (unsigned)((c->nz + kRhs0Rows - 1) / kRhs0Rows),
+                        (unsigned)rows),
+                       128, 0, c->stream>>>(a, (T)dt, cold ? 1 : 0);
     return cudaGetLastError();
 }
 
