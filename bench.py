@@ -187,25 +187,73 @@ def barrier(world: int):
         dist.barrier()
 
 
-def cpu_oracle_rate(rho_seq, seconds: float, threads: int | None, max_solves: int):
-    """Warm solves/s of the CPU oracle on this host over a bounded sample."""
+def shard_instances(n: int, world: int, rank: int) -> range:
+    """The contiguous block of instance ids 0..n-1 that rank owns; block sizes
+    differ by at most one and the blocks of ranks 0..world-1 cover 0..n-1
+    once.  Independent solves need no exchange between ranks."""
+    q, r = divmod(n, world)
+    start = rank * q + min(rank, r)
+    return range(start, start + q + (1 if rank < r else 0))
+
+
+def rel_l2(a, b) -> float:
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def oracle_section(B, solver, base, last, args, want_cpu):
+    """Parity of the timed workload with the CPU oracle, and the CPU baseline.
+
+    * last_timed_rel_l2: the oracle's warm state is set from the potential
+      of the second-to-last timed solve, and its warm solve of the last timed
+      density is compared with the last timed potential;
+    * sequence: a cold solve and four warm rotated solves through the
+      host-array drop-in call on the GPU and on the oracle, max rel L2;
+    * cpu_baseline: warm solves/s of the oracle on this host's cores.
+    """
+    from bipoly_hydro_b200 import fields
     from oracle import oracle as O
 
     O.build()
-    if threads:
-        O.set_num_threads(threads)
+    O.set_num_threads(os.cpu_count() or 1)
+    t0 = time.perf_counter()
     o = O.Oracle(GRID["numr"], GRID["numz"], GRID["numphi"], GRID["dr"], GRID["isym"], GRID["mmax"])
-    o.potential_solver(rho_seq(0), 0)  # cold start, untimed
-    o.potential_solver(rho_seq(1), 2)  # one warm solve, untimed
-    n, t0 = 0, time.perf_counter()
-    while True:
-        o.potential_solver(rho_seq(2 + n), 3 + n)
-        n += 1
-        el = time.perf_counter() - t0
-        if el >= seconds or n >= max_solves:
-            break
+    setup_s = time.perf_counter() - t0
+    shape = (GRID["numr"], GRID["numz"], GRID["numphi"])
+
+    def fortran(v):
+        return np.asfortranarray(np.asarray(v).reshape(shape, order="F"))
+
+    parity = {"tolerance": 1e-12, "oracle_setup_s": setup_s}
+    if last["prev"] is not None:
+        o.set_potential(fortran(last["prev"]))
+        po = o.potential_solver(fortran(last["rho"]), last["tstep"])
+        parity["last_timed_rel_l2"] = rel_l2(fortran(last["pot"]), po)
+    else:
+        parity["last_timed_rel_l2"] = None
+    seq = []
+    for k in range(5):
+        rho = fields.rotate(base, k)
+        seq.append(rel_l2(solver.potential_solver(rho, 0 if k == 0 else k + 1),
+                          o.potential_solver(rho, 0 if k == 0 else k + 1)))
+    parity["sequence_rel_l2"] = seq
+    parity["sequence"] = "cold + 4 warm rotated solves through bph_potential_solver (host arrays)"
+    parity["pass"] = max(seq + [parity["last_timed_rel_l2"] or 0.0]) <= 1e-12
+    cpu = None
+    if want_cpu:
+        n, t0 = 0, time.perf_counter()
+        while True:
+            o.potential_solver(fields.rotate(base, 5 + n), 6 + n)
+            n += 1
+            el = time.perf_counter() - t0
+            if el >= args.cpu_seconds or n >= 200:
+                break
+        cpu = {"value": n / el, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+               "sample": f"{n} warm solves of the same sequence in {el:.1f} s after an untimed setup "
+                         f"(C restatement of potential_solver, OpenMP)"}
     o.close()
-    return n / el, n, el, O.num_threads()
+    return parity, cpu
 
 
 def run_reference(args, world, rank):
@@ -605,15 +653,22 @@ def run_gpu(args, world, rank, local):
     stream = torch.cuda.current_stream()
     solver.set_stream(stream)
 
-    # Density sequence: rank-dependent seed/phase, all numphi rotations resident.
+    # Density sequence: the numphi rotations of the pair are sharded over the
+    # ranks (shard_instances); each rank keeps its shard resident and cycles
+    # through it (one zone of rotation per solve within the shard).
     base = fields.bipolytrope_pair(numr, numz, numphi, GRID["dr"], GRID["isym"], mass_ratio=0.5)
     base_t = torch.from_numpy(np.ascontiguousarray(base.ravel(order="F"))).to(dev)
     c_view = base_t.view(numphi, numz, numr)  # C view of the Fortran (numr, numz, numphi) array
-    nrot = args.rotations if args.rotations > 0 else numphi
+    total_rot = args.rotations if args.rotations > 0 else numphi
+    shard = shard_instances(max(total_rot, world), world, rank)
+    nrot = len(shard)
     rhos = torch.empty((nrot, ntot), dtype=torch.float64, device=dev)
-    for i in range(nrot):
-        rhos[i].copy_(torch.roll(c_view, shifts=i + rank, dims=0).reshape(-1))
-    d_pot = torch.empty(ntot, dtype=torch.float64, device=dev)
+    for i, rot in enumerate(shard):
+        rhos[i].copy_(torch.roll(c_view, shifts=rot % numphi, dims=0).reshape(-1))
+    # two output buffers, alternated by the timed solves: the last two
+    # potentials stay on the device for the parity check after the timing
+    d_pots = [torch.empty(ntot, dtype=torch.float64, device=dev) for _ in range(2)]
+    d_pot = d_pots[0]
 
     # cold start, then warm-up solves
     solver.potential_solver_device(rhos[0], d_pot, 0)
@@ -638,13 +693,18 @@ def run_gpu(args, world, rank, local):
     with ClockSampler(uuid) as clk:
         e0.record(stream)
         for i in range(args.steps):
-            solver.potential_solver_device(rhos[(1 + args.warmup + i) % nrot], d_pot, tstep)
+            solver.potential_solver_device(rhos[(1 + args.warmup + i) % nrot], d_pots[i % 2], tstep)
             tstep += 1
         e1.record(stream)
         torch.cuda.synchronize()
     barrier(world)
     launches = solver.launch_count - l0
     solver.synchronize()
+    # the last timed solve (its density, the potential before it, its result)
+    last_i = args.steps - 1
+    last = {"rho": rhos[(1 + args.warmup + last_i) % nrot].cpu().numpy(),
+            "prev": d_pots[(last_i - 1) % 2].cpu().numpy() if args.steps >= 2 else None,
+            "pot": d_pots[last_i % 2].cpu().numpy(), "tstep": tstep - 1}
     ms_total = max_over_ranks(e0.elapsed_time(e1), world)
     ms_per_step = ms_total / args.steps
     value = job_rate(args.steps, world, ms_total)
@@ -739,6 +799,52 @@ def run_gpu(args, world, rank, local):
     barrier(world)
     ms_e2e = max_over_ranks(e2.elapsed_time(e3), world)
     e2e_value = job_rate(n_e2e, world, ms_e2e)
+
+    # ---- e2e on pageable host arrays, then the same arrays registered ----
+    # (a Fortran caller passes its COMMON arrays: pageable unless the shim
+    # registers them, which it does once in potsetup)
+    def host_rate(rho_list, pot_arr, n):
+        nonlocal tstep
+        lat = []
+        for i in range(3):
+            rc = lib.bph_potential_solver(solver._h, ctypes.c_void_p(rho_list[i % len(rho_list)].ctypes.data),
+                                          ctypes.c_void_p(pot_arr.ctypes.data), tstep)
+            tstep += 1
+            assert rc == 0, lib.bph_last_error()
+        barrier(world)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for i in range(n):
+            t0 = time.perf_counter()
+            rc = lib.bph_potential_solver(solver._h, ctypes.c_void_p(rho_list[i % len(rho_list)].ctypes.data),
+                                          ctypes.c_void_p(pot_arr.ctypes.data), tstep)
+            lat.append(time.perf_counter() - t0)
+            tstep += 1
+            if rc != 0:
+                raise RuntimeError(lib.bph_last_error().decode())
+        b.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        ms = max_over_ranks(a.elapsed_time(b), world)
+        return {"value": job_rate(n, world, ms), "unit": "solves/s",
+                "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99))}
+
+    n_pg = min(n_e2e, args.e2e_pageable_steps)
+    rho_pg = [np.array(rho_np[i % npin]) for i in range(min(npin, 4))]  # plain (pageable) numpy copies
+    pot_pg = np.empty(ntot)
+    e2e_pageable = host_rate(rho_pg, pot_pg, n_pg)
+    for arr in rho_pg + [pot_pg]:
+        B.register_host(arr)
+    e2e_registered = host_rate(rho_pg, pot_pg, n_pg)
+    for arr in rho_pg + [pot_pg]:
+        B.unregister_host(arr)
+    del rho_pg, pot_pg
+
+    # ---- parity with the oracle and the CPU baseline (rank 0) ----------
+    parity, cpu = None, None
+    if rank == 0 and not args.no_parity:
+        parity, cpu = oracle_section(B, solver, base, last, args, want_cpu=(world == 1 and not args.no_cpu_baseline))
 
     # The sections below are reported by rank 0 only; with several ranks the
     # others skip them (no collective follows, and the host is not shared by
@@ -864,17 +970,6 @@ def run_gpu(args, world, rank, local):
         conv["speedup_mixed_vs_fp64"] = best / conv["fp64"]["solves_per_s"]
         del ref_pots
 
-    # ---- CPU baseline (rank 0, N = 1 only) ------------------------------
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        def rho_seq(i):
-            return fields.rotate(base, i)
-
-        rate, n, el, cores = cpu_oracle_rate(rho_seq, args.cpu_seconds, os.cpu_count(), 200)
-        cpu = {"value": rate, "unit": "solves/s", "cores": cores, "kind": "port",
-               "sample": f"{n} warm solves of the same sequence in {el:.1f} s after an untimed setup "
-                         f"(C restatement of potential_solver, OpenMP)"}
-
     solver_info = solver.info()
     solver.close()
     if rank == 0:
@@ -883,13 +978,19 @@ def run_gpu(args, world, rank, local):
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "130x98x256 warm time-step solves, bipolytrope pair rotated 1 zone/solve",
-                       **GRID, "nsteps_adi": 5, "parallelism": f"independent sequence per GPU x{world}",
-                       "l2": "per-solve working set (660 MB Green tables) > 126 MB L2"},
+                       **GRID, "nsteps_adi": 5},
+            "parallelism": f"independent sequence per GPU x{world}",
+            "l2": "per-solve working set (660 MB Green tables) > 126 MB L2, no flush needed",
             "zone_updates_per_s": value * ntot * 5,
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 8 * ntot,
-                    "d2h_bytes_per_step": 8 * ntot,
+                    "d2h_bytes_per_step": 8 * ntot, "host_memory": "pinned (torch pin_memory)",
                     "p50_ms": 1e3 * float(np.percentile(e2e_lat, 50)),
-                    "p99_ms": 1e3 * float(np.percentile(e2e_lat, 99))},
+                    "p99_ms": 1e3 * float(np.percentile(e2e_lat, 99)),
+                    "pageable": e2e_pageable, "registered": e2e_registered,
+                    "pageable_vs_pinned": e2e_pageable["value"] / e2e_value,
+                    "registered_vs_pinned": e2e_registered["value"] / e2e_value},
+            "parity": parity,
+            "parity_rel_l2": parity["last_timed_rel_l2"] if parity else None,
             "roofline": {"bound": "hbm", "kernel": "k_green_contract", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "alg_bytes_per_launch": cb,
@@ -920,6 +1021,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=500)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle parity section")
+    ap.add_argument("--e2e-pageable-steps", type=int, default=100,
+                    help="host-array solves timed on pageable and on registered arrays")
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
     ap.add_argument("--batch-sizes", default="4,16", help="batched warm solves timed per batch size (empty skips)")
     ap.add_argument("--batch-calls", type=int, default=20)

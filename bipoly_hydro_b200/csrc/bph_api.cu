@@ -394,6 +394,7 @@ int setup_impl(bph_ctx *c) {
     if ((rc = fft_configure(c))) return rc;
     if ((rc = adi_configure(c))) return rc;
     if ((rc = contract_configure(c))) return rc;
+    if ((rc = noalloc_setup(c))) return rc;
     {
         const size_t groups = (size_t)(c->nb + 7) / 8;
         if ((rc = dev_alloc(c, &c->d_ccnt, (size_t)g.mmax * groups))) return rc;
@@ -498,12 +499,6 @@ int check_ctx(const bph_ctx *c) {
     return BPH_OK;
 }
 
-int set_device_of(bph_ctx *c) {
-    int cur = -1;
-    BPH_CUDA(cudaGetDevice(&cur));
-    if (cur != c->device) BPH_CUDA(cudaSetDevice(c->device));
-    return BPH_OK;
-}
 
 }  // namespace
 
@@ -545,7 +540,7 @@ int bph_setup(const bph_grid_t *grid, bph_ctx_t **ctx) {
 
 int bph_destroy(bph_ctx_t *c) {
     if (!c) return BPH_OK;
-    set_device_of(c);
+    ::bph::DeviceScope scope_(c->device);
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->stream && c->stream != c->own_stream) cudaStreamSynchronize(c->stream);
     for (auto &s : c->sched) free_schedule(c, s);
@@ -574,6 +569,35 @@ int bph_destroy(bph_ctx_t *c) {
     return BPH_OK;
 }
 
+int bph_register_host(void *ptr, size_t bytes) {
+    if (!ptr || bytes == 0) {
+        set_error("ptr must be non-NULL and bytes > 0");
+        return BPH_ERR_INVALID;
+    }
+    cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterPortable);
+    if (e == cudaErrorHostMemoryAlreadyRegistered) {
+        (void)cudaGetLastError();  // already pinned: nothing to do
+        return BPH_OK;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaHostRegister");
+    return BPH_OK;
+}
+
+int bph_unregister_host(void *ptr) {
+    if (!ptr) {
+        set_error("ptr is NULL");
+        return BPH_ERR_INVALID;
+    }
+    cudaError_t e = cudaHostUnregister(ptr);
+    if (e == cudaErrorHostMemoryNotRegistered) {
+        (void)cudaGetLastError();
+        set_error("pointer was not registered with bph_register_host");
+        return BPH_ERR_INVALID;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaHostUnregister");
+    return BPH_OK;
+}
+
 int bph_set_stream(bph_ctx_t *c, void *stream) {
     int rc;
     if ((rc = check_ctx(c))) return rc;
@@ -584,7 +608,7 @@ int bph_set_stream(bph_ctx_t *c, void *stream) {
 int bph_synchronize(bph_ctx_t *c) {
     int rc;
     if ((rc = check_ctx(c))) return rc;
-    if ((rc = set_device_of(c))) return rc;
+    BPH_DEVICE_SCOPE(c);
     return read_status(c);
 }
 
@@ -595,7 +619,7 @@ int bph_potential_solver(bph_ctx_t *c, const double *rho, double *pot, int tstep
         set_error("rho and pot must be non-NULL");
         return BPH_ERR_INVALID;
     }
-    if ((rc = set_device_of(c))) return rc;
+    BPH_DEVICE_SCOPE(c);
     bool warm = tstep > 1;  // potential_solver.F90:80
     Schedule *s;
     if ((rc = get_schedule(c, warm ? 5 : 20, &s))) return rc;
@@ -609,7 +633,7 @@ int bph_potential_solver_device(bph_ctx_t *c, const double *d_rho, double *d_pot
         set_error("rho and pot must be non-NULL");
         return BPH_ERR_INVALID;
     }
-    if ((rc = set_device_of(c))) return rc;
+    BPH_DEVICE_SCOPE(c);
     bool warm = tstep > 1;
     Schedule *s;
     if ((rc = get_schedule(c, warm ? 5 : 20, &s))) return rc;
@@ -623,7 +647,7 @@ int bph_solve_nsteps(bph_ctx_t *c, const double *rho, double *pot, int nsteps, i
         set_error("invalid arguments (nsteps must be in [1, 10000])");
         return BPH_ERR_INVALID;
     }
-    if ((rc = set_device_of(c))) return rc;
+    BPH_DEVICE_SCOPE(c);
     Schedule *s;
     if ((rc = get_schedule(c, nsteps, &s))) return rc;
     if (on_device) return solve_device(c, rho, pot, *s, cold != 0);
@@ -667,7 +691,7 @@ static int converged_impl(bph_ctx *c, const double *rho, double *pot, int nsteps
         set_error("no mixed-precision ADI kernel is configured for this grid");
         return BPH_ERR_INVALID;
     }
-    if ((rc = set_device_of(c))) return rc;
+    BPH_DEVICE_SCOPE(c);
     Schedule *s;
     if ((rc = get_schedule(c, nsteps, &s))) return rc;
     if (mixed && c->mixed_kind == BPH_MIXED_ADI_GLOBAL && (rc = ensure_mixed_work(c))) return rc;
@@ -757,7 +781,7 @@ int bph_potential_solver_phieff(bph_ctx_t *c, const double *rho, double *pot, do
         set_error("rho, pot and phieff must be non-NULL and omega_frame finite");
         return BPH_ERR_INVALID;
     }
-    if ((rc = set_device_of(c))) return rc;
+    BPH_DEVICE_SCOPE(c);
     bool warm = tstep > 1;
     Schedule *s;
     if ((rc = get_schedule(c, warm ? 5 : 20, &s))) return rc;
@@ -779,7 +803,7 @@ int bph_set_potential(bph_ctx_t *c, const double *pot, int on_device) {
         set_error("pot must be non-NULL");
         return BPH_ERR_INVALID;
     }
-    if ((rc = set_device_of(c))) return rc;
+    BPH_DEVICE_SCOPE(c);
     const double *d_pot = pot;
     if (!on_device) {
         if ((rc = ensure_staging(c))) return rc;
@@ -796,7 +820,7 @@ int bph_set_potential(bph_ctx_t *c, const double *pot, int on_device) {
 int bph_run_phase(bph_ctx_t *c, int phase, const double *d_rho, double *d_pot, int nsteps) {
     int rc;
     if ((rc = check_ctx(c))) return rc;
-    if ((rc = set_device_of(c))) return rc;
+    BPH_DEVICE_SCOPE(c);
     switch (phase) {
         case BPH_PHASE_FFT_RHO:
             if (!d_rho) break;
@@ -836,7 +860,7 @@ int bph_copy_green(bph_ctx_t *c, double *out, size_t n) {
         set_error("output buffer too small (%zu < %zu)", n, need);
         return BPH_ERR_INVALID;
     }
-    if ((rc = set_device_of(c))) return rc;
+    BPH_DEVICE_SCOPE(c);
     BPH_CUDA(cudaMemcpyAsync(out, c->d_green, sizeof(double) * need, cudaMemcpyDeviceToHost, c->stream));
     BPH_CUDA(cudaStreamSynchronize(c->stream));
     return BPH_OK;
@@ -850,7 +874,7 @@ int bph_copy_moments(bph_ctx_t *c, double *out, size_t n) {
         set_error("output buffer too small (%zu < %zu)", n, need);
         return BPH_ERR_INVALID;
     }
-    if ((rc = set_device_of(c))) return rc;
+    BPH_DEVICE_SCOPE(c);
     BPH_CUDA(cudaMemcpyAsync(out, c->d_S, sizeof(double) * need, cudaMemcpyDeviceToHost, c->stream));
     BPH_CUDA(cudaStreamSynchronize(c->stream));
     return BPH_OK;
@@ -880,7 +904,7 @@ int bph_configure(bph_ctx_t *c, int key, int value) {
         set_error("unknown configuration key %d", key);
         return BPH_ERR_INVALID;
     }
-    if ((rc = set_device_of(c))) return rc;
+    BPH_DEVICE_SCOPE(c);
     if (value == BPH_MIXED_ADI_AUTO) return autotune_mixed(c);
     if (value != BPH_MIXED_ADI_FORWARD && value != BPH_MIXED_ADI_INCREMENT && value != BPH_MIXED_ADI_GLOBAL) {
         set_error("unknown refinement ADI kind %d", value);

@@ -268,8 +268,8 @@ int bph_batch_create(bph_ctx_t *c, int capacity, bph_batch_t **out) {
         set_error("batch capacity %d too large for the grid-wide ADI kernels (capacity * numphi <= 65535)", capacity);
         return BPH_ERR_INVALID;
     }
-    cudaError_t e = cudaSetDevice(c->device);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    BPH_DEVICE_SCOPE(c);
+    cudaError_t e;
     size_t need = sizeof(double) * (size_t)capacity *
                   ((size_t)c->N * c->nplane + (size_t)c->N * c->np * (large ? 3 : 1) + 2ull * c->g.mmax * c->np +
                    2ull * c->g.mmax * c->nb);
@@ -344,7 +344,7 @@ int bph_batch_create(bph_ctx_t *c, int capacity, bph_batch_t **out) {
 
 int bph_batch_destroy(bph_batch_t *b) {
     if (!b) return BPH_OK;
-    if (b->c) cudaSetDevice(b->c->device);
+    ::bph::DeviceScope scope_(b->c ? b->c->device : 0);
     if (b->c && b->c->stream) cudaStreamSynchronize(b->c->stream);
     if (b->blas) cublasDestroy(b->blas);
     double *bufs[] = {b->d_P,     b->d_R,     b->d_mom, b->d_C,    b->d_rho_stage, b->d_pot_stage,
@@ -428,8 +428,7 @@ int batch_solve_core(bph_batch *b, int n, const int *instances, const double *co
         }
     }
     bph_ctx *c = b->c;
-    cudaError_t e = cudaSetDevice(c->device);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    BPH_DEVICE_SCOPE(c);
     Schedule *s;  // warm: 5 steps, cold: 20 (potential_solver.F90:80-94); converged: its cycle length
     int rc = batch_schedule(c, conv ? conv->nsteps : (warm ? 5 : 20), &s);
     if (rc) return rc;
@@ -791,7 +790,7 @@ extern "C" {
 
 int bph_plan_destroy(bph_plan_t *pl) {
     if (!pl) return BPH_OK;
-    cudaSetDevice(pl->device);
+    ::bph::DeviceScope scope_(pl->device);
     for (cudaGraphExec_t &x : pl->exec)
         if (x) cudaGraphExecDestroy(x);
     for (void *t : pl->d_tab)
@@ -839,7 +838,8 @@ int bph_plan_create(int nparts, bph_batch_t *const *batches, const int *counts, 
     }
     bph_plan *pl = new bph_plan();
     pl->device = batches[0]->c->device;
-    cudaError_t e = cudaSetDevice(pl->device);
+    ::bph::DeviceScope scope_(pl->device);
+    cudaError_t e = scope_.status();
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pl->fork, cudaEventDisableTiming);
     for (int p = 0; p < nparts && e == cudaSuccess; ++p) {
         pl->parts.push_back(batches[p]);
@@ -875,7 +875,7 @@ int bph_plan_launch(bph_plan_t *pl, int tstep, void *stream) {
         set_error("plan is NULL");
         return BPH_ERR_INVALID;
     }
-    BPH_CUDA(cudaSetDevice(pl->device));
+    BPH_DEVICE_SCOPE(pl);
     const bool warm = tstep > 1;
     const int k = warm ? 1 : 0;
     // a schedule rebuilt since the recording invalidates the graph
@@ -898,7 +898,7 @@ int bph_plan_synchronize(bph_plan_t *pl, void *stream) {
         set_error("plan is NULL");
         return BPH_ERR_INVALID;
     }
-    BPH_CUDA(cudaSetDevice(pl->device));
+    BPH_DEVICE_SCOPE(pl);
     BPH_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
     int worst = BPH_OK;
     for (bph_batch *b : pl->parts) {

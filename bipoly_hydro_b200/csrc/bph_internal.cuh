@@ -166,6 +166,7 @@ struct bph_ctx {
     int *d_slot_map = nullptr;         // [N]: the nfree free slots, then the dependent ones
     cudaStream_t side_stream = nullptr;
     cudaEvent_t ev_fft = nullptr, ev_free = nullptr;
+    void *noalloc_scratch = nullptr;   // device address of the allocation-free contraction's scratch array
     long long launches = 0;
     size_t bytes = 0;
 };
@@ -181,6 +182,12 @@ int cuda_fail(cudaError_t e, const char *what);
         cudaError_t _e = (call);                                \
         if (_e != cudaSuccess) return ::bph::cuda_fail(_e, #call); \
     } while (0)
+
+}  // namespace bph
+
+#include "bph_device_scope.h"
+
+namespace bph {
 
 // Launch configuration with the programmatic-serialisation attribute when
 // the context uses it (attrs must outlive the launch call).
@@ -304,6 +311,9 @@ int select_mixed_kind(bph_ctx *c, int kind);
 // Work area of the global-memory refinement kernel (allocated on first use).
 int ensure_mixed_work(bph_ctx *c);
 int contract_configure(bph_ctx *c);
+// Device address of the allocation-free contraction's file-scope scratch
+// array for a context being set up (bph_noalloc.cu).
+int noalloc_setup(bph_ctx *c);
 int fft_configure(bph_ctx *c);
 
 }  // namespace bph

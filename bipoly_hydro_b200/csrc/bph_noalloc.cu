@@ -17,42 +17,23 @@
 // Calls whose work overlaps on the GPU (different streams, or different
 // host threads on one device) race on the scratch and must be serialised by
 // the caller.
-#include <mutex>
-
+//
+// In host code the name bph_noalloc_scratch is a host-side stand-in, not a
+// device address: bph_setup resolves the array's device address once for
+// its context (noalloc_setup, with the context's device current) and the
+// entry point passes that address to the kernel, so the call path itself
+// makes no runtime lookup.
 #include "bph_internal.cuh"
+#include "bph_noalloc_plan.h"
 
 namespace bph {
 namespace {
 
-// 8 MiB of scratch per device: counters first, partial sums after.
-constexpr size_t kNoallocScratchBytes = size_t(8) << 20;
-constexpr size_t kCounterBytes = 64 * 1024;  // up to 16384 (mode, row-group) tiles
-constexpr int kRows = 8;
+using noalloc::kCounterBytes;
+using noalloc::kRows;
 constexpr int kThreads = 256;
-constexpr int kMaxSplits = 16;
 
-static __device__ __align__(256) unsigned char bph_noalloc_scratch[kNoallocScratchBytes];
-
-std::mutex g_mu;
-void *g_scratch_addr[64] = {nullptr};
-
-// The device address of the scratch array on the current device (host code
-// cannot use the symbol itself: it is a host-side stand-in).
-int scratch_address(int device, void **out) {
-    if (device < 0 || device >= 64) {
-        set_error("device ordinal %d out of range", device);
-        return BPH_ERR_INVALID;
-    }
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[device]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, bph_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(bph_noalloc_scratch)");
-        g_scratch_addr[device] = p;
-    }
-    *out = g_scratch_addr[device];
-    return BPH_OK;
-}
+static __device__ __align__(256) unsigned char bph_noalloc_scratch[noalloc::kScratchBytes];
 
 // Grid (row groups, mmax, splits).  Each CTA reduces its p-range for kRows
 // boundary rows of one mode into partials[split][m][b][2]; the last CTA of a
@@ -125,6 +106,19 @@ k_green_contract_splitk(const double *__restrict__ G, const double *__restrict__
 }
 
 }  // namespace
+
+// Resolves the device address of the scratch array for a context being set
+// up (its device is current).  Every context holds its own copy, so a
+// context created after a device reset sees the array where the reloaded
+// module put it.
+int noalloc_setup(bph_ctx *c) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, bph_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(bph_noalloc_scratch)");
+    c->noalloc_scratch = p;
+    return BPH_OK;
+}
+
 }  // namespace bph
 
 extern "C" int bph_green_contract_noalloc(bph_ctx_t *c, const double *d_mom, double *d_S) {
@@ -137,37 +131,27 @@ extern "C" int bph_green_contract_noalloc(bph_ctx_t *c, const double *d_mom, dou
         set_error("d_mom and d_S must be device arrays");
         return BPH_ERR_INVALID;
     }
-    int cur = -1;
-    cudaError_t e = cudaGetDevice(&cur);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    if (cur != c->device) {
-        e = cudaSetDevice(c->device);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
-    }
     const int mmax = c->g.mmax, nb = c->nb;
-    const int groups = (nb + kRows - 1) / kRows;
-    const size_t tiles = (size_t)mmax * groups;
-    const size_t tile_doubles = (size_t)mmax * nb * 2;
-    const size_t avail = (kNoallocScratchBytes - kCounterBytes) / sizeof(double);
-    if (tiles * sizeof(unsigned int) > kCounterBytes || tile_doubles > avail) {
+    noalloc::Plan plan;
+    if (!noalloc::plan(mmax, nb, c->np, &plan)) {
         set_error("grid too large for the %zu-byte no-allocation scratch (mmax*nb = %d; limit %zu tiles, "
                   "%zu partial doubles per split)",
-                  kNoallocScratchBytes, mmax * nb, kCounterBytes / sizeof(unsigned int), avail);
+                  noalloc::kScratchBytes, mmax * nb, kCounterBytes / sizeof(unsigned int),
+                  noalloc::partial_capacity());
         return BPH_ERR_INVALID;
     }
-    int nsplit = (int)(avail / tile_doubles);
-    if (nsplit > kMaxSplits) nsplit = kMaxSplits;
-    if ((long long)nsplit > c->np) nsplit = (int)c->np;
-    void *base = nullptr;
-    int rc = scratch_address(c->device, &base);
-    if (rc) return rc;
-    unsigned int *counters = reinterpret_cast<unsigned int *>(base);
-    double *partials = reinterpret_cast<double *>(static_cast<unsigned char *>(base) + kCounterBytes);
-    e = cudaMemsetAsync(counters, 0, tiles * sizeof(unsigned int), c->stream);
+    if (!c->noalloc_scratch) {
+        set_error("the context has no scratch address (bph_setup did not complete)");
+        return BPH_ERR_STATE;
+    }
+    BPH_DEVICE_SCOPE(c);
+    unsigned int *counters = reinterpret_cast<unsigned int *>(c->noalloc_scratch);
+    double *partials = reinterpret_cast<double *>(static_cast<unsigned char *>(c->noalloc_scratch) + kCounterBytes);
+    cudaError_t e = cudaMemsetAsync(counters, 0, plan.tiles * sizeof(unsigned int), c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(counters)");
-    dim3 grid((unsigned)groups, (unsigned)mmax, (unsigned)nsplit);
-    k_green_contract_splitk<<<grid, kThreads, 0, c->stream>>>(c->d_green, d_mom, d_S, c->np, nb, nsplit, counters,
-                                                             partials);
+    dim3 grid((unsigned)plan.groups, (unsigned)mmax, (unsigned)plan.nsplit);
+    k_green_contract_splitk<<<grid, kThreads, 0, c->stream>>>(c->d_green, d_mom, d_S, c->np, nb, plan.nsplit,
+                                                             counters, partials);
     ++c->launches;
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "k_green_contract_splitk");

@@ -170,8 +170,8 @@ int bph_server_create(bph_ctx_t *c, int max_clients, size_t mem_cap_bytes, int m
         set_error("serving needs the segmented or the grid-wide ADI kernels for this grid");
         return BPH_ERR_INVALID;
     }
-    cudaError_t e = cudaSetDevice(c->device);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    BPH_DEVICE_SCOPE(c);
+    cudaError_t e;
     // resident bytes of one client: slot array, -4 pi rho_hat, moments and
     // contraction output of its batch position, host-array staging (rho, pot)
     const size_t per = sizeof(double) * ((size_t)c->N * c->nplane + (size_t)c->N * c->np * (c->adi_seg ? 1 : 3) +

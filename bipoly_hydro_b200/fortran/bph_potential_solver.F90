@@ -31,6 +31,11 @@ module bph_c
          real(c_double), intent(out) :: pot(*)
          integer(c_int), value :: tstep
       end function bph_potential_solver
+      integer(c_int) function bph_register_host(a, bytes) bind(c, name="bph_register_host")
+         import :: c_int, c_double, c_size_t
+         real(c_double), intent(in) :: a(*)
+         integer(c_size_t), value :: bytes
+      end function bph_register_host
       type(c_ptr) function bph_last_error() bind(c, name="bph_last_error")
          import :: c_ptr
       end function bph_last_error
@@ -48,12 +53,24 @@ subroutine potsetup
    integer :: isym
    integer, dimension(3) :: boundary_condition
    common /boundary_conditions/ isym, boundary_condition
+   real, dimension(numr_dd,numz_dd,numphi) :: pot, rho
+   common /poisson/ pot, rho
    type(bph_grid_t) :: grid
    integer(c_int) :: rc
+   integer(c_size_t) :: nbytes
    grid = bph_grid_t(numr, numz, numphi, real(dr, c_double), isym, mmax)
    rc = bph_setup(grid, bph_context)
    if (rc /= 0) then
       write(6,*) 'bph_setup failed with status ', rc
+      error stop
+   endif
+   ! COMMON /poisson/ lives at a fixed address for the whole run: pin it once
+   ! so that every potential_solver call copies at pinned-memory speed
+   nbytes = int(8, c_size_t) * int(numr_dd, c_size_t) * int(numz_dd, c_size_t) * int(numphi, c_size_t)
+   rc = bph_register_host(rho, nbytes)
+   if (rc == 0) rc = bph_register_host(pot, nbytes)
+   if (rc /= 0) then
+      write(6,*) 'bph_register_host failed with status ', rc
       error stop
    endif
 end subroutine potsetup

@@ -53,6 +53,7 @@ EXPORTED_SYMBOLS = (
     "bph_server_create", "bph_server_set_converged", "bph_server_capacity", "bph_server_open_client",
     "bph_server_close_client",
     "bph_server_submit", "bph_server_poll", "bph_server_wait", "bph_server_stats", "bph_server_destroy",
+    "bph_register_host", "bph_unregister_host",
 )
 
 #: bph_configure keys and values.
@@ -166,6 +167,10 @@ def load_library(path: str | None = None):
     L.bph_launch_count.restype = ctypes.c_longlong
     L.bph_device_bytes.argtypes = [vp]
     L.bph_device_bytes.restype = ctypes.c_size_t
+    L.bph_register_host.argtypes = [vp, sz]
+    L.bph_register_host.restype = i
+    L.bph_unregister_host.argtypes = [vp]
+    L.bph_unregister_host.restype = i
     for name in ("bph_setup", "bph_potential_solver", "bph_potential_solver_device", "bph_solve_nsteps",
                  "bph_solve_converged", "bph_set_stream", "bph_synchronize", "bph_destroy",
                  "bph_num_boundary_rows", "bph_copy_green", "bph_copy_moments", "bph_run_phase"):
@@ -367,6 +372,18 @@ class PotentialSolver:
     @property
     def device_bytes(self) -> int:
         return int(self._lib.bph_device_bytes(self._h))
+
+
+def register_host(a: np.ndarray) -> None:
+    """Pin a host array for fast host-array solves (bph_register_host).  Call
+    :func:`unregister_host` on the same array before it is freed."""
+    if not isinstance(a, np.ndarray) or a.nbytes == 0:
+        raise ValueError("expected a non-empty numpy array")
+    _check(load_library().bph_register_host(ctypes.c_void_p(a.ctypes.data), a.nbytes))
+
+
+def unregister_host(a: np.ndarray) -> None:
+    _check(load_library().bph_unregister_host(ctypes.c_void_p(a.ctypes.data)))
 
 
 def version() -> str:

@@ -219,6 +219,17 @@ int bph_server_stats(const bph_server_t *server, long long *batches, long long *
 /* Finishes the queued requests, stops the worker, frees the clients. */
 int bph_server_destroy(bph_server_t *server);
 
+/* Pins a host array for the life of the run (cudaHostRegister, portable to
+ * every device) so that bph_potential_solver and the other host-array calls
+ * copy it at pinned-memory speed instead of through the driver's pageable
+ * staging.  Meant for arrays at fixed addresses such as the reference's
+ * COMMON /poisson/ rho and pot (potential_solver.F90:18-19): the Fortran
+ * shim registers both once in potsetup.  No counterpart in the reference.
+ * Registering an already registered range is not an error.  Unregister
+ * (bph_unregister_host, same pointer) before freeing the memory. */
+int bph_register_host(void *ptr, size_t bytes);
+int bph_unregister_host(void *ptr);
+
 /* Stream used for all later work of this context (a cudaStream_t; NULL is
  * CUDA's default stream).  Until the first call the context uses a
  * non-blocking stream of its own. */
@@ -276,10 +287,11 @@ int bph_run_phase(bph_ctx_t *ctx, int phase, const double *d_rho, double *d_pot,
  * layout).  Enqueued on the context's stream; allocates nothing.
  *
  * Scratch: an 8 MiB file-scope device array per GPU, held until the
- * process exits.  Grids with mmax*nb*2 partial sums beyond its capacity
- * are rejected with BPH_ERR_INVALID.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress): make that first call
- * before any stream capture.  All calls on a device share the array and
+ * process exits.  Grids whose 64 KiB of arrival counters (mmax * ceil(nb/8)
+ * tiles) or whose mmax*nb*2 partial sums per split exceed it are rejected
+ * with BPH_ERR_INVALID before any device work.  bph_setup looks up the
+ * array's device address for its context (cudaGetSymbolAddress), so this
+ * call makes no runtime lookup.  All calls on a device share the array and
  * it keeps the last call's contents; calls that overlap on the GPU race
  * and must be serialised by the caller. */
 int bph_green_contract_noalloc(bph_ctx_t *ctx, const double *d_mom, double *d_S);

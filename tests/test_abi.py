@@ -54,6 +54,14 @@ def test_null_context_is_an_error(bph):
     assert lib.bph_destroy(None) == bph.BPH_OK
 
 
+def test_host_registration_rejects_bad_arguments_before_device_work(bph):
+    lib = bph.load_library()
+    assert lib.bph_register_host(None, 1024) == bph.BPH_ERR_INVALID
+    buf = ctypes.create_string_buffer(64)
+    assert lib.bph_register_host(ctypes.cast(buf, ctypes.c_void_p), 0) == bph.BPH_ERR_INVALID
+    assert lib.bph_unregister_host(None) == bph.BPH_ERR_INVALID
+
+
 def test_product_does_not_import_the_oracle():
     """The product package never imports, links or loads the CPU oracle."""
     pkg = os.path.join(ROOT, "bipoly_hydro_b200")

@@ -1,0 +1,132 @@
+"""Oracle parity at the production grids the benchmark measures.
+
+130x98x256 (dr = 1/126, isym 2, mmax 30) is the time-step workload: the
+bipolytrope pair, a cold solve and then warm solves with the density rotated
+by one azimuthal zone per call (potential_solver.F90:80-94 with
+main.F90:396).  These tests run it through the same calls and the same
+launch configuration as the benchmark (384-thread on-chip ADI, the side
+stream for the slots without boundary data, programmatic dependent launch,
+8-column FFT tiles) and compare every potential with the oracle at the FP64
+bar: relative L2 error <= 1e-12 with the same ADI step count.
+
+258x194x64 has the production slot size of the 258x194 grids (256 x 192
+interior zones per slot): its slots exceed shared memory, so the drop-in
+takes the grid-wide panel ADI kernels.
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+POT_TOL = 1e-12
+GRID_130 = (130, 98, 256, 1.0 / 126.0, 2, 30)
+
+
+@pytest.fixture(scope="module")
+def oracle_130(oracle_mod):
+    o = oracle_mod.Oracle(*GRID_130)
+    yield o
+    o.close()
+
+
+@pytest.fixture(scope="module")
+def pair_rho():
+    from bipoly_hydro_b200 import fields
+
+    return fields.bipolytrope_pair()
+
+
+def test_time_step_sequence_host_arrays(oracle_130, pair_rho, bph):
+    """bph_potential_solver (host arrays): cold, then four warm rotated solves."""
+    from bipoly_hydro_b200 import fields
+
+    g = bph.PotentialSolver(*GRID_130)
+    info = g.info()
+    assert info["adi_threads"] == 384, info
+    rho = pair_rho
+    for tstep in range(0, 5):
+        po = oracle_130.potential_solver(rho, tstep)
+        pg = g.potential_solver(rho, tstep)
+        err = rel_l2(pg, po)
+        assert err <= POT_TOL, (tstep, err)
+        if tstep == 0:
+            assert rel_l2(g.moments_S(), oracle_130.moments_S()) <= 1e-13
+        rho = fields.rotate(rho)
+    g.close()
+
+
+def test_time_step_sequence_device_arrays(oracle_130, pair_rho, bph):
+    """bph_potential_solver_device on the caller's torch stream: the benchmark's
+    call, with the free-slot ADI on the low-priority side stream and
+    programmatic dependent launch; several solves are enqueued back to back
+    before the host waits."""
+    import torch
+
+    from bipoly_hydro_b200 import fields
+
+    torch.cuda.set_device(0)
+    g = bph.PotentialSolver(*GRID_130)
+    stream = torch.cuda.Stream()
+    g.set_stream(stream)
+    rhos = [fields.rotate(pair_rho, i) for i in range(5)]
+    d_rho = [torch.from_numpy(np.ascontiguousarray(r.ravel(order="F"))).cuda() for r in rhos]
+    d_pot = [torch.empty_like(d_rho[0]) for _ in rhos]
+    torch.cuda.synchronize()
+    for i in range(5):
+        g.potential_solver_device(d_rho[i], d_pot[i], 0 if i == 0 else i + 1)
+    g.synchronize()
+    for i in range(5):
+        po = oracle_130.potential_solver(rhos[i], 0 if i == 0 else i + 1)
+        pg = d_pot[i].cpu().numpy().reshape(rhos[i].shape, order="F")
+        err = rel_l2(pg, po)
+        assert err <= POT_TOL, (i, err)
+    g.close()
+
+
+def test_warm_state_restored_from_previous_potential(oracle_130, pair_rho, bph):
+    """The benchmark's parity check: the oracle's warm state set from the GPU's
+    previous potential reproduces the GPU's next warm solve."""
+    from bipoly_hydro_b200 import fields
+
+    g = bph.PotentialSolver(*GRID_130)
+    p0 = g.potential_solver(pair_rho, 0)
+    rho1 = fields.rotate(pair_rho)
+    p1 = g.potential_solver(rho1, 2)
+    oracle_130.set_potential(p0)
+    po = oracle_130.potential_solver(rho1, 2)
+    assert rel_l2(p1, po) <= POT_TOL
+    g.close()
+
+
+def test_converged_fp64_and_mixed_match_oracle(oracle_130, pair_rho, bph):
+    """bph_solve_converged against orc_solve_converged with the same cycle
+    count, and the mixed-precision form within 1e-9 of the oracle."""
+    g = bph.PotentialSolver(*GRID_130)
+    po, co, ro = oracle_130.solve_converged(pair_rho, 10, True, 1e-11, 60)
+    pg, info = g.solve_converged(pair_rho, 10, True, 1e-11, 60)
+    assert info.cycles == co, (info.cycles, co)
+    assert rel_l2(pg, po) <= POT_TOL
+    assert abs(info.residual - ro) <= 0.5 * ro + 1e-12
+    pm, im = g.solve_converged_mixed(pair_rho, 10, True, 1e-11, 60)
+    assert rel_l2(pm, po) <= 1e-9, (rel_l2(pm, po), im.cycles)
+    g.close()
+
+
+def test_grid_wide_adi_at_production_slot_size(oracle_mod, bph):
+    """258x194x64, dr = 1/250, mmax 30: slots of 256 x 192 zones take the
+    grid-wide panel ADI; cold and warm solves at the FP64 bar."""
+    from bipoly_hydro_b200 import fields
+
+    grid = (258, 194, 64, 1.0 / 250.0, 2, 30)
+    g = bph.PotentialSolver(*grid)
+    assert g.info()["adi_threads"] == 0
+    o = oracle_mod.Oracle(*grid)
+    rho = fields.bipolytrope_pair(258, 194, 64, 1.0 / 250.0)
+    for tstep in (0, 2, 3):
+        err = rel_l2(g.potential_solver(rho, tstep), o.potential_solver(rho, tstep))
+        assert err <= POT_TOL, (tstep, err)
+        rho = fields.rotate(rho)
+    o.close()
+    g.close()

@@ -134,6 +134,31 @@ def test_device_api_matches_host_api(bph):
     b.close()
 
 
+def test_registered_host_arrays_give_the_same_potential(bph):
+    """bph_register_host pins the caller's arrays in place (the Fortran shim
+    does this for COMMON /poisson/); solves on them equal solves on pageable
+    copies bit for bit, and unregistering restores plain pageable arrays."""
+    grid = SMALL_GRIDS[3]
+    numr, numz, numphi, dr, isym, _ = grid
+    rho = smooth_density(numr, numz, numphi, dr, isym)
+    a, b = bph.PotentialSolver(*grid), bph.PotentialSolver(*grid)
+    pinned_rho = np.asfortranarray(rho.copy())
+    pinned_pot = np.zeros(rho.shape, order="F")
+    bph.register_host(pinned_rho)
+    bph.register_host(pinned_rho)  # a second registration is not an error
+    bph.register_host(pinned_pot)
+    for tstep in (0, 2):
+        ref = a.potential_solver(rho, tstep)
+        b.potential_solver(pinned_rho, tstep, out=pinned_pot)
+        assert np.array_equal(pinned_pot, ref), tstep
+    bph.unregister_host(pinned_rho)
+    bph.unregister_host(pinned_pot)
+    with pytest.raises(bph.BphError):
+        bph.unregister_host(pinned_pot)
+    a.close()
+    b.close()
+
+
 def test_nonfinite_density_is_reported(bph):
     grid = SMALL_GRIDS[0]
     numr, numz, numphi, dr, isym, mmax = grid

@@ -1,0 +1,49 @@
+"""Host-side logic of the library compiled with g++ and run on the CPU.
+
+* bph_device_scope.h: every entry point makes its context's device current
+  and puts the caller's current device back (a Fortran host that drives
+  other work on another GPU from the same thread must not find its device
+  switched).  The guard's logic runs here against a fake runtime.
+* bph_noalloc_plan.h: the scratch sizing of the allocation-free contraction
+  (rejection beyond the 8 MiB array, split-count clamps), including limits
+  no constructible context on one GPU reaches.
+"""
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CSRC = os.path.join(ROOT, "bipoly_hydro_b200", "csrc")
+CPP = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cpp")
+
+
+def _run(tmp_path, name):
+    exe = tmp_path / name
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Werror", "-I", CSRC, os.path.join(CPP, name + ".cpp"),
+                    "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    return out.stdout
+
+
+def test_device_scope_restores_callers_device(tmp_path):
+    assert "all checks passed" in _run(tmp_path, "device_scope_check")
+
+
+def test_noalloc_plan_limits_and_clamps(tmp_path):
+    assert "all checks passed" in _run(tmp_path, "noalloc_plan_check")
+
+
+def test_library_selects_devices_only_through_the_scope():
+    """No source file of the library calls cudaSetDevice except the scope
+    header, so no entry point can leave the caller on another device."""
+    offenders = []
+    for name in sorted(os.listdir(CSRC)):
+        if not name.endswith((".cu", ".cuh", ".h")) or name == "bph_device_scope.h":
+            continue
+        text = open(os.path.join(CSRC, name)).read()
+        for m in re.finditer(r"cudaSetDevice\s*\(", text):
+            offenders.append(f"{name}:{text[:m.start()].count(chr(10)) + 1}")
+    assert not offenders, offenders

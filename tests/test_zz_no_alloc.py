@@ -2,8 +2,10 @@
 cannot allocate device memory (its scratch is a file-scope device array).
 
 Its boundary moments S must equal those the regular solve computes for the
-same density (bph_copy_moments after a solve), on two calls in a row (the
-second call reuses the scratch the first one left behind).  This file is
+same density (bph_copy_moments after a solve) and the CPU oracle's, on two
+calls in a row (the second call reuses the scratch the first one left
+behind); a 3x3 interior (9 zones, fewer than the 16 splits) exercises the
+clamp of the split count to the zone count.  This file is
 collected last so that a run stopping at the first failure has already run
 every other test.
 """
@@ -33,9 +35,10 @@ def _moments(torch, rho, numphi, mmax, fm):
 
 
 @pytest.mark.parametrize("grid", [(34, 26, 64, 1.0 / 30.0, 2, 30), (130, 98, 256, 1.0 / 126.0, 2, 30),
-                                  (20, 14, 32, 1.0 / 18.0, 1, 8), (18, 16, 32, 1.0 / 16.0, 3, 6)],
-                         ids=["34x26x64", "130x98x256", "isym1", "isym3"])
-def test_noalloc_contraction_matches_solve(bph, grid):
+                                  (20, 14, 32, 1.0 / 18.0, 1, 8), (18, 16, 32, 1.0 / 16.0, 3, 6),
+                                  (5, 5, 16, 1.0 / 3.0, 2, 2), (21, 13, 16, 1.0 / 19.0, 2, 4)],
+                         ids=["34x26x64", "130x98x256", "isym1", "isym3", "np9-split-clamp", "odd-np"])
+def test_noalloc_contraction_matches_solve(bph, oracle_mod, grid):
     import torch
 
     numr, numz, numphi, dr, isym, mmax = grid
@@ -43,6 +46,10 @@ def test_noalloc_contraction_matches_solve(bph, grid):
     rho = smooth_density(numr, numz, numphi, dr, isym)
     solver.potential_solver(rho, 0)          # the existing entry point
     s_ref = solver.moments_S()
+    o = oracle_mod.Oracle(*grid)             # the same moments from the CPU oracle
+    o.potential_solver(rho, 0)
+    s_orc = o.moments_S()
+    o.close()
     mom = _moments(torch, rho, numphi, mmax, 2 if isym == 3 else 1)
     lib = bph.load_library()
     torch.cuda.synchronize()
@@ -56,6 +63,7 @@ def test_noalloc_contraction_matches_solve(bph, grid):
         s_new = d_s.cpu().numpy().reshape(mmax, solver.nb, 2)
         assert np.all(np.isfinite(s_new)), f"call {call}"
         assert rel_l2(s_new, s_ref) <= S_TOL, f"call {call}: {rel_l2(s_new, s_ref):.3e}"
+        assert rel_l2(s_new, s_orc) <= S_TOL, f"call {call} vs oracle: {rel_l2(s_new, s_orc):.3e}"
     solver.close()
 
 
