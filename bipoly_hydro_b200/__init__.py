@@ -20,13 +20,14 @@ from .solver import (  # noqa: F401
     Plan,
     Server,
     load_library,
+    read_continuation,
     register_host,
     unregister_host,
     version,
 )
 
 __all__ = [
-    "PotentialSolver", "Batch", "Plan", "Server", "Grid", "BphError", "load_library", "register_host",
+    "PotentialSolver", "Batch", "Plan", "Server", "Grid", "BphError", "load_library", "read_continuation", "register_host",
     "unregister_host", "version", "LIB_PATH", "EXPORTED_SYMBOLS",
     "BPH_OK", "BPH_ERR_INVALID", "BPH_ERR_NOMEM", "BPH_ERR_NONFINITE", "BPH_ERR_CUDA", "BPH_ERR_TIMEOUT",
     "BPH_ERR_STATE",

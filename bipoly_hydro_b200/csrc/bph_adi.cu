@@ -1403,8 +1403,11 @@ cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_ru
     if (P) a.P = P;
     if (R) a.R = R;
     a.inst_map = d_inst_map;
-    if (norms && !c->adi_seg) return cudaErrorNotSupported;  // only the segmented kernel reports them
+    if (norms && !c->adi_seg) return cudaErrorNotSupported;  // only the on-chip kernels report them
     a.norms = norms;
+    if (c->adi_warp)
+        return launch_adi_warp(c, sch, step0, nsteps_run, cold, a.P, a.R, ninst, d_inst_map, nullptr, c->N, norms,
+                               c->stream, c->pdl);
     if (c->adi_seg) {
         ++c->launches;
         void *args[] = {&a};
@@ -1434,6 +1437,9 @@ cudaError_t launch_adi(bph_ctx *c, const Schedule &sch, int step0, int nsteps_ru
 cudaError_t launch_adi_slots(bph_ctx *c, const Schedule &sch, bool cold, const int *d_slots, int nslots,
                              cudaStream_t st, bool pdl) {
     if (!c->adi_seg || nslots < 1) return cudaErrorNotSupported;
+    if (c->adi_warp)
+        return launch_adi_warp(c, sch, 0, sch.nsteps, cold, c->d_P, c->d_R, 1, nullptr, d_slots, nslots, nullptr, st,
+                               pdl);
     AdiArgs a = make_args(c, sch, 0, sch.nsteps, cold);
     a.slot_map = d_slots;
     a.nslots = nslots;

@@ -147,6 +147,8 @@ void free_schedule(bph_ctx *c, Schedule &s) {
         dev_free(s.d_rad_pk[k]);
         dev_free(s.d_ver_pk[k]);
     }
+    dev_free(s.d_warp_rad);
+    dev_free(s.d_warp_ver);
     free(s.h_dt);
     s = Schedule();
     (void)c;
@@ -187,6 +189,11 @@ int get_schedule(bph_ctx *c, int nsteps, Schedule **out) {
         s.d_ver_pk[1] = v32;
     }
     BPH_CUDA(launch_pack_factors(c, s));
+    if (c->adi_warp) {
+        if ((rc = dev_alloc(c, &s.d_warp_rad, (size_t)nsteps * c->N * warp_block_doubles(c->nr)))) return rc;
+        if ((rc = dev_alloc(c, &s.d_warp_ver, (size_t)nsteps * warp_block_doubles(c->nz)))) return rc;
+        BPH_CUDA(launch_pack_warp(c, s));
+    }
     BPH_CUDA(cudaStreamSynchronize(c->stream));
     *out = &s;
     return BPH_OK;
@@ -344,6 +351,7 @@ int setup_impl(bph_ctx *c) {
     if ((rc = dev_alloc(c, &c->d_ph, (size_t)g.mmax))) return rc;
     if ((rc = dev_alloc(c, &c->d_red, (size_t)2 * c->N))) return rc;
     if ((rc = dev_alloc(c, &c->d_status, 1))) return rc;
+    if ((rc = dev_alloc(c, &c->d_scf, scf_scratch_doubles()))) return rc;
 
     if ((rc = upload(c, c->d_brb, h.brb.data(), sizeof(double) * h.brb.size()))) return rc;
     if ((rc = upload(c, c->d_elz, h.elz.data(), sizeof(double) * h.elz.size()))) return rc;
@@ -393,6 +401,7 @@ int setup_impl(bph_ctx *c) {
     BPH_CUDA(launch_green_tables(c));
     if ((rc = fft_configure(c))) return rc;
     if ((rc = adi_configure(c))) return rc;
+    if ((rc = warp_configure(c))) return rc;
     if ((rc = contract_configure(c))) return rc;
     if ((rc = noalloc_setup(c))) return rc;
     {
@@ -557,6 +566,8 @@ int bph_destroy(bph_ctx_t *c) {
     dev_free(c->d_cpart);
     conv_graphs_free(c);
     dev_free(c->d_work32);
+    dev_free(c->d_warp_coef);
+    dev_free(c->d_scf);
     if (c->side_stream) {
         cudaStreamSynchronize(c->side_stream);
         cudaStreamDestroy(c->side_stream);
@@ -638,6 +649,34 @@ int bph_potential_solver_device(bph_ctx_t *c, const double *d_rho, double *d_pot
     Schedule *s;
     if ((rc = get_schedule(c, warm ? 5 : 20, &s))) return rc;
     return solve_device(c, d_rho, d_pot, *s, !warm);
+}
+
+int bph_scf_step(bph_ctx_t *c, double *d_rho, double *d_pot, double eps, double mass, unsigned long long seed,
+                 int iteration, int tstep) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    if (!d_rho || !d_pot || !(eps >= 0.0) || !std::isfinite(eps) || !std::isfinite(mass) || iteration < 0) {
+        set_error("invalid arguments (device arrays, eps >= 0, finite mass, iteration >= 0)");
+        return BPH_ERR_INVALID;
+    }
+    BPH_DEVICE_SCOPE(c);
+    BPH_CUDA(launch_scf_update(c, d_rho, eps, mass, seed, iteration, c->d_scf));
+    const bool warm = tstep > 1;  // potential_solver.F90:80
+    Schedule *s;
+    if ((rc = get_schedule(c, warm ? 5 : 20, &s))) return rc;
+    return solve_device(c, d_rho, d_pot, *s, !warm);
+}
+
+int bph_scf_mass(bph_ctx_t *c, double *mass_out, double *scale_out) {
+    int rc;
+    if ((rc = check_ctx(c))) return rc;
+    BPH_DEVICE_SCOPE(c);
+    double h[2] = {0.0, 0.0};
+    BPH_CUDA(cudaMemcpyAsync(h, c->d_scf + scf_scratch_doubles() - 2, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    BPH_CUDA(cudaStreamSynchronize(c->stream));
+    if (scale_out) *scale_out = h[0];
+    if (mass_out) *mass_out = h[1];
+    return BPH_OK;
 }
 
 int bph_solve_nsteps(bph_ctx_t *c, const double *rho, double *pot, int nsteps, int cold, int on_device) {
@@ -893,6 +932,11 @@ long long bph_info(const bph_ctx_t *c, int what) {
         case BPH_INFO_MIXED_FORWARD_NS: return (long long)(1e3f * c->mixed_tuned_us[BPH_MIXED_ADI_FORWARD]);
         case BPH_INFO_MIXED_INCREMENT_NS: return (long long)(1e3f * c->mixed_tuned_us[BPH_MIXED_ADI_INCREMENT]);
         case BPH_INFO_ADI_PREFETCH: return (c->adi_pf ? 1 : 0) | (c->mixed_pf ? 2 : 0);
+        case BPH_INFO_ADI_KERNEL:
+            return c->adi_warp ? BPH_ADI_KERNEL_WARP
+                               : c->adi_seg ? BPH_ADI_KERNEL_SEGMENTED
+                                            : c->adi_smem ? BPH_ADI_KERNEL_ONCHIP : BPH_ADI_KERNEL_GRID_WIDE;
+        case BPH_INFO_ADI_WARP_SMEM: return c->adi_warp_smem;
         default: return -1;
     }
 }

@@ -16,7 +16,6 @@
 //   k_adi_seg           one launch over n*numphi slots (no wave-quantisation
 //                       tail of a single 256-slot launch)
 //   k_fft_inv           per instance
-#include <cublas_v2.h>
 
 #include <algorithm>
 #include <cmath>
@@ -48,10 +47,9 @@ struct bph_batch {
     double *d_work32 = nullptr;       // mixed converged on grid-wide kernels: 4 * cap * N * np floats
     double *d_cnorm = nullptr;        // converged solves: per (instance, slot) norm pairs [cap][N][2]
     double *h_cnorm = nullptr;        // its pinned host copy
-    double *d_cpart = nullptr;        // split-K partial sums of k_contract_batch
+    double *d_cpart = nullptr;        // split-K partial sums of the batched contraction
     unsigned int *d_ccnt = nullptr;   // its arrival counters [mmax][row groups]
-    bool own_contract = true;         // k_contract_batch for up to kBatchOwnMax positions
-    cublasHandle_t blas = nullptr;
+    bool own_contract = false;        // the CUDA-core k_contract_batch for up to kBatchOwnMax positions
     size_t bytes = 0;
 };
 
@@ -171,6 +169,194 @@ cudaError_t contract_batch_launch(bph_ctx *c, bph_batch *b, long long mstride) {
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// k_contract_dmma: C_m = G_m^T M_m on the FP64 tensor cores (DMMA,
+// mma.sync m16n8k8 .f64), the batched boundary contraction for every batch
+// size.  Warp w of a CTA owns a 16-row tile of boundary rows b and all
+// 8 NT columns c of the launch's column block; the CTA's 8 warps share one
+// (mode, slice of zones).  Per 8-zone step a warp streams its 16 x 8 table
+// tile (four 8-byte evict-first loads per thread, prefetched kDmmaStages
+// steps ahead so that ~64 KB of table bytes per SM are in flight) and reads
+// the moment fragments (L1: every warp of the CTA reads the same ones).
+// Slices write partial sums; the last CTA of each (mode, row group) to
+// arrive adds them in slice order (deterministic) and writes C.
+//   A (16 x 8, row major) = G[m][b0 + r][k0 + q]      (table rows)
+//   B (8 x 8, column major) = M[m][c0 + n][k0 + q]     (moment columns)
+//   fragment layout of m16n8k8 .f64 (lane = 4 group + t):
+//     a0 (group, t), a1 (group + 8, t), a2 (group, t + 4), a3 (group + 8, t + 4)
+//     b0 (k = t, n = group), b1 (k = t + 4, n = group)
+//     d0 (group, 2t), d1 (group, 2t + 1), d2 (group + 8, 2t), d3 (group + 8, 2t + 1)
+constexpr int kDmmaWarps = 8;
+constexpr int kDmmaStages = 4;
+constexpr int kDmmaMaxTiles = 8;  // column tiles of 8 per launch (64 columns)
+
+__device__ __forceinline__ void dmma16x8x8(double (&d)[4], const double (&a)[4], double b0, double b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b0), "d"(b1));
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kDmmaWarps * 32, 2)
+k_contract_dmma(const double *__restrict__ G, const double *__restrict__ mom, long long mstride, long long np, int nb,
+                int c0, int ncol, double *__restrict__ C, long long cstride, unsigned int *__restrict__ counters,
+                double *__restrict__ partials) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane >> 2, t = lane & 3;
+    const int m = blockIdx.y, split = blockIdx.z, nsplit = gridDim.z;
+    const int b0 = (blockIdx.x * kDmmaWarps + warp) * 16;
+    // table rows of this thread's fragments (clamped: rows beyond nb read row 0 and are never stored)
+    const int ra = b0 + grp, rb = b0 + grp + 8;
+    const double *ga = G + ((long long)m * nb + (ra < nb ? ra : 0)) * np;
+    const double *gb = G + ((long long)m * nb + (rb < nb ? rb : 0)) * np;
+    const bool live = b0 < nb;
+    // moment column c0 + 8 j + grp of this thread's B fragments (columns beyond ncol are zero)
+    const double *mcol = mom + m * mstride + (long long)(c0 + grp) * np;
+    const int ncols_here = ncol - c0 - grp;  // tile j is live when 8 j < ncols_here
+    const long long nk = (np + 7) / 8;  // 8-zone steps (the last one may be partial)
+    const long long per = (nk + nsplit - 1) / nsplit;
+    const long long k_begin = split * per, k_end = min(nk, k_begin + per);
+    double acc[NT][4];
+#pragma unroll
+    for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
+    auto load_a = [&](long long k, double (&a)[4]) {
+        const long long z0 = 8 * k + t, z1 = z0 + 4;
+        if (live && k < k_end) {
+            a[0] = z0 < np ? __ldcs(ga + z0) : 0.0;
+            a[1] = z0 < np ? __ldcs(gb + z0) : 0.0;
+            a[2] = z1 < np ? __ldcs(ga + z1) : 0.0;
+            a[3] = z1 < np ? __ldcs(gb + z1) : 0.0;
+        } else {
+            a[0] = a[1] = a[2] = a[3] = 0.0;
+        }
+    };
+    // the tables are set-up data: the first steps load before the moments are ready
+    double ab[kDmmaStages][4];
+#pragma unroll
+    for (int st = 0; st < kDmmaStages; ++st) load_a(k_begin + st, ab[st]);
+    pdl_wait();
+    for (long long k = k_begin; k < k_end; k += kDmmaStages) {
+#pragma unroll
+        for (int st = 0; st < kDmmaStages; ++st) {
+            const long long kk = k + st;
+            if (kk < k_end) {
+                const long long z0 = 8 * kk + t, z1 = z0 + 4;
+                double a[4] = {ab[st][0], ab[st][1], ab[st][2], ab[st][3]};
+                load_a(kk + kDmmaStages, ab[st]);  // the step kDmmaStages ahead
+#pragma unroll
+                for (int j = 0; j < NT; ++j) {
+                    const bool cl = 8 * j < ncols_here;
+                    const double bv0 = (cl && z0 < np) ? __ldg(mcol + 8LL * j * np + z0) : 0.0;
+                    const double bv1 = (cl && z1 < np) ? __ldg(mcol + 8LL * j * np + z1) : 0.0;
+                    dmma16x8x8(acc[j], a, bv0, bv1);
+                }
+            }
+        }
+    }
+    pdl_trigger();
+    constexpr int NCP = 8 * NT;  // columns of a partial-sum row
+    const int rows0 = blockIdx.x * kDmmaWarps * 16;
+    const int nrows = min(kDmmaWarps * 16, nb - rows0);
+    auto put = [&](double *dst, long long rstride, long long cstr) {
+        // d0 (grp, 2t), d1 (grp, 2t+1), d2 (grp+8, 2t), d3 (grp+8, 2t+1) of every column tile
+#pragma unroll
+        for (int j = 0; j < NT; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int r = b0 + grp + ((e & 2) ? 8 : 0);
+                const int cc = 8 * j + 2 * t + (e & 1);
+                if (live && r < nb) dst[(long long)r * rstride + (long long)cc * cstr] = acc[j][e];
+            }
+    };
+    if (nsplit == 1) {
+        // C[m][c0 + cc][r], columns within ncol only
+#pragma unroll
+        for (int j = 0; j < NT; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int r = b0 + grp + ((e & 2) ? 8 : 0);
+                const int col = c0 + 8 * j + 2 * t + (e & 1);
+                if (live && r < nb && col < ncol) C[m * cstride + (long long)col * nb + r] = acc[j][e];
+            }
+        return;
+    }
+    // partials [split][m][b][NCP]
+    const long long pstride = (long long)gridDim.y * nb * NCP;
+    put(partials + split * pstride + (long long)m * nb * NCP, NCP, 1);
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    const int tile = m * gridDim.x + blockIdx.x;
+    if (threadIdx.x == 0) last = (atomicAdd(counters + tile, 1u) == (unsigned)(nsplit - 1));
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int q = threadIdx.x; q < nrows * NCP; q += kDmmaWarps * 32) {
+        const int r = rows0 + q / NCP, cc = q % NCP;
+        const int col = c0 + cc;
+        if (col >= ncol) continue;
+        double sum = 0.0;
+        for (int sp = 0; sp < nsplit; ++sp) sum += __ldcg(partials + sp * pstride + ((long long)m * nb + r) * NCP + cc);
+        C[m * cstride + (long long)col * nb + r] = sum;
+    }
+    if (threadIdx.x == 0) counters[tile] = 0u;
+}
+
+template <int NT>
+cudaError_t contract_dmma_launch_nt(bph_ctx *c, bph_batch *b, long long mstride, int c0, int ncol, int nsplit) {
+    const int groups = (c->nb + kDmmaWarps * 16 - 1) / (kDmmaWarps * 16);
+    dim3 grid((unsigned)groups, (unsigned)c->g.mmax, (unsigned)nsplit);
+    ++c->launches;
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = launch_config(c, grid, dim3(kDmmaWarps * 32), 0, attr);
+    const double *G = c->d_green;
+    const double *mom = b->d_mom;
+    long long np = c->np, cstride = 2LL * b->cap * c->nb;
+    int nb = c->nb;
+    double *C = b->d_C;
+    unsigned int *cnt = b->d_ccnt;
+    double *part = b->d_cpart;
+    void *args[] = {(void *)&G, (void *)&mom, (void *)&mstride, (void *)&np, (void *)&nb, (void *)&c0,
+                    (void *)&ncol, (void *)&C, (void *)&cstride, (void *)&cnt, (void *)&part};
+    return cudaLaunchKernelExC(&cfg, (const void *)k_contract_dmma<NT>, args);
+}
+
+// Slices of the zone range: about four CTAs per SM over the launch, at least
+// 64 steps of 8 zones per slice, at most kBatchSplitMax.
+int dmma_splits(const bph_ctx *c) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    const long long groups = (c->nb + kDmmaWarps * 16 - 1) / (kDmmaWarps * 16);
+    const long long base = groups * c->g.mmax;
+    const long long nk = (c->np + 7) / 8;
+    int nsplit = 1;
+    while (nsplit < kBatchSplitMax && base * (nsplit + 1) <= 4LL * sms && nk / (nsplit + 1) >= 64) ++nsplit;
+    return nsplit;
+}
+
+// C for the 2n columns of n batch positions: one launch per block of 64 columns.
+cudaError_t contract_dmma_launch(bph_ctx *c, bph_batch *b, long long mstride, int n) {
+    const int ncol = 2 * n;
+    const int nsplit = dmma_splits(c);
+    for (int c0 = 0; c0 < ncol; c0 += 8 * kDmmaMaxTiles) {
+        const int tiles = min(kDmmaMaxTiles, (ncol - c0 + 7) / 8);
+        cudaError_t e;
+        switch (tiles) {
+            case 1: e = contract_dmma_launch_nt<1>(c, b, mstride, c0, ncol, nsplit); break;
+            case 2: e = contract_dmma_launch_nt<2>(c, b, mstride, c0, ncol, nsplit); break;
+            case 3: e = contract_dmma_launch_nt<3>(c, b, mstride, c0, ncol, nsplit); break;
+            case 4: e = contract_dmma_launch_nt<4>(c, b, mstride, c0, ncol, nsplit); break;
+            case 5: e = contract_dmma_launch_nt<5>(c, b, mstride, c0, ncol, nsplit); break;
+            case 6: e = contract_dmma_launch_nt<6>(c, b, mstride, c0, ncol, nsplit); break;
+            case 7: e = contract_dmma_launch_nt<7>(c, b, mstride, c0, ncol, nsplit); break;
+            default: e = contract_dmma_launch_nt<8>(c, b, mstride, c0, ncol, nsplit); break;
+        }
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 // One thread per (instance, boundary row or corner, slot), as k_boundary_slots.
 __global__ void k_boundary_slots_batch(const double *__restrict__ C, const double2 *__restrict__ ph,
                                        double *__restrict__ P, int numr, int numz, int nr, int nz, int nb, int N,
@@ -226,11 +412,6 @@ int batch_alloc(bph_batch *b, double **p, size_t count) {
     }
     b->bytes += sizeof(double) * count;
     return BPH_OK;
-}
-
-int blas_fail(cublasStatus_t st, const char *what) {
-    set_error("cuBLAS error %d in %s", (int)st, what);
-    return BPH_ERR_CUDA;
 }
 
 }  // namespace
@@ -290,10 +471,12 @@ int bph_batch_create(bph_ctx_t *c, int capacity, bph_batch_t **out) {
     if (!rc) rc = batch_alloc(b, &b->d_C, (size_t)c->g.mmax * 2 * capacity * c->nb);
     if (!rc && large) rc = batch_alloc(b, &b->d_LW, (size_t)capacity * c->N * c->np);
     if (!rc && large) rc = batch_alloc(b, &b->d_LQ, (size_t)capacity * c->N * c->np);
-    if (!rc && (c->np % 2 == 0)) {
-        // split-K scratch of k_contract_batch: partial sums for the widest case
-        // (8 columns) and arrival counters for the narrowest row groups (16 rows)
-        rc = batch_alloc(b, &b->d_cpart, (size_t)kBatchSplitMax * c->g.mmax * c->nb * 8);
+    if (!rc) {
+        // split-K scratch of the contraction: partial sums for the widest
+        // column block (8 per CUDA-core launch, up to 64 per tensor-core
+        // launch) and arrival counters for the narrowest row groups (16 rows)
+        const size_t cols = std::max<size_t>(8, std::min<size_t>(8 * kDmmaMaxTiles, 8 * ((2 * (size_t)capacity + 7) / 8)));
+        rc = batch_alloc(b, &b->d_cpart, (size_t)kBatchSplitMax * c->g.mmax * c->nb * cols);
         if (!rc) {
             const size_t ncnt = (size_t)c->g.mmax * ((c->nb + 15) / 16);
             e = cudaMalloc((void **)&b->d_ccnt, sizeof(unsigned int) * ncnt);
@@ -306,8 +489,10 @@ int bph_batch_create(bph_ctx_t *c, int capacity, bph_batch_t **out) {
         }
     }
     if (!rc) {
-        const char *g = std::getenv("BPH_BATCH_GEMM");
-        b->own_contract = (c->np % 2 == 0) && !(g && g[0] == 'l');  // "library": always the library GEMM
+        // BPH_BATCH_CONTRACT=simt: the CUDA-core kernel for up to kBatchOwnMax
+        // positions (comparison only; the tensor-core kernel is the default)
+        const char *g = std::getenv("BPH_BATCH_CONTRACT");
+        b->own_contract = (c->np % 2 == 0) && g && g[0] == 's';
     }
     if (!rc) {
         const size_t tab_bytes = (2 * sizeof(void *) + sizeof(int)) * (size_t)capacity;
@@ -330,10 +515,6 @@ int bph_batch_create(bph_ctx_t *c, int capacity, bph_batch_t **out) {
                                                   c->stream);
         if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemsetAsync");
     }
-    if (!rc) {
-        cublasStatus_t st = cublasCreate(&b->blas);
-        if (st != CUBLAS_STATUS_SUCCESS) rc = blas_fail(st, "cublasCreate");
-    }
     if (rc) {
         bph_batch_destroy(b);
         return rc;
@@ -346,7 +527,6 @@ int bph_batch_destroy(bph_batch_t *b) {
     if (!b) return BPH_OK;
     ::bph::DeviceScope scope_(b->c ? b->c->device : 0);
     if (b->c && b->c->stream) cudaStreamSynchronize(b->c->stream);
-    if (b->blas) cublasDestroy(b->blas);
     double *bufs[] = {b->d_P,     b->d_R,     b->d_mom, b->d_C,    b->d_rho_stage, b->d_pot_stage,
                       b->d_cpart, b->d_LW,    b->d_LQ,  b->d_prev, b->d_cnorm, b->d_work32};
     for (double *p : bufs)
@@ -532,8 +712,11 @@ static int batch_prologue(bph_batch *b, int n, const double *const *d_in, const 
     const long long mstride = 2LL * b->cap * np;
     BPH_CUDA(launch_fft_fwd_rho_batch(c, n, d_in, d_map, b->d_R, (long long)c->N * np, b->d_mom, mstride, 2LL * np,
                                       per_pos ? b->d_stat : c->d_status, per_pos));
-    // C_m = G_m^T M_m for every mode in one strided-batched DGEMM (batch positions)
-    if (b->own_contract && n <= kBatchOwnMax) {
+    // C_m = G_m^T M_m for every mode: FP64 tensor-core contraction (or, on
+    // request, the CUDA-core kernel for up to kBatchOwnMax positions)
+    if (!b->own_contract || n > kBatchOwnMax) {
+        BPH_CUDA(contract_dmma_launch(c, b, mstride, n));
+    } else {
         cudaError_t ce = cudaSuccess;
         switch (n) {
             case 1: ce = contract_batch_launch<2>(c, b, mstride); break;
@@ -542,14 +725,6 @@ static int batch_prologue(bph_batch *b, int n, const double *const *d_in, const 
             default: ce = contract_batch_launch<8>(c, b, mstride); break;
         }
         BPH_CUDA(ce);
-    } else {
-        cublasStatus_t st = cublasSetStream(b->blas, c->stream);
-        if (st != CUBLAS_STATUS_SUCCESS) return blas_fail(st, "cublasSetStream");
-        const double one = 1.0, zero = 0.0;
-        st = cublasDgemmStridedBatched(b->blas, CUBLAS_OP_T, CUBLAS_OP_N, c->nb, 2 * n, (int)np, &one, c->d_green,
-                                       (int)np, (long long)c->nb * np, b->d_mom, (int)np, mstride, &zero, b->d_C,
-                                       c->nb, 2LL * b->cap * c->nb, c->g.mmax);
-        if (st != CUBLAS_STATUS_SUCCESS) return blas_fail(st, "cublasDgemmStridedBatched");
     }
     {
         const int ncorner = (c->g.isym == 1) ? 2 : 1;
@@ -692,6 +867,33 @@ int batch_converged_run(bph_batch *b, int n, const int *inst, const int *d_map, 
 extern "C" {
 
 size_t bph_batch_device_bytes(const bph_batch_t *b) { return b ? b->bytes : 0; }
+
+int bph_batch_copy_moments(bph_batch_t *b, int n, double *out, size_t count) {
+    if (!b || !out || n < 1 || n > b->cap) {
+        set_error("invalid batch, position count or output");
+        return BPH_ERR_INVALID;
+    }
+    bph_ctx *c = b->c;
+    const size_t per = (size_t)c->g.mmax * c->nb * 2;
+    if (count < per * (size_t)n) {
+        set_error("output holds %zu doubles, %zu needed", count, per * (size_t)n);
+        return BPH_ERR_INVALID;
+    }
+    BPH_DEVICE_SCOPE(c);
+    // C[m][2 pos + cs][b] -> out[pos][m][b][cs]
+    const size_t cn = (size_t)c->g.mmax * 2 * b->cap * c->nb;
+    std::vector<double> h(cn);
+    BPH_CUDA(cudaMemcpyAsync(h.data(), b->d_C, sizeof(double) * cn, cudaMemcpyDeviceToHost, c->stream));
+    BPH_CUDA(cudaStreamSynchronize(c->stream));
+    for (int pos = 0; pos < n; ++pos)
+        for (int m = 0; m < c->g.mmax; ++m)
+            for (int r = 0; r < c->nb; ++r)
+                for (int cs = 0; cs < 2; ++cs) {
+                    const double v = h[((size_t)m * 2 * b->cap + 2 * pos + cs) * c->nb + r];
+                    out[(((size_t)pos * c->g.mmax + m) * c->nb + r) * 2 + cs] = (m == 0 && cs == 1) ? 0.0 : v;
+                }
+    return BPH_OK;
+}
 
 }  // extern "C"
 

@@ -77,6 +77,10 @@ struct Schedule {
     void *d_rad_pk[2] = {nullptr, nullptr};
     void *d_ver_pk[2] = {nullptr, nullptr};
     long long build_id = 0;  // distinct for every schedule built (graphs that captured it)
+    // warp-cooperative ADI (bph_adi_warp.cu): segment-interleaved FP64 blocks,
+    // radial [nsteps][N][40 nr/8 + 48], vertical [nsteps][40 nz/8 + 48]
+    double *d_warp_rad = nullptr;
+    double *d_warp_ver = nullptr;
 };
 
 // Converged-loop state on the device (bph_converge.cu).
@@ -166,6 +170,10 @@ struct bph_ctx {
     int *d_slot_map = nullptr;         // [N]: the nfree free slots, then the dependent ones
     cudaStream_t side_stream = nullptr;
     cudaEvent_t ev_fft = nullptr, ev_free = nullptr;
+    int adi_warp = 0;                  // warp-cooperative FP64 ADI shape (0: not used; bph_adi_warp.cu)
+    int adi_warp_smem = 0;             // its dynamic shared bytes
+    double *d_warp_coef = nullptr;     // its per-slot (elambdazb, alphaz, betaz) blocks
+    double *d_scf = nullptr;           // SCF-step mass partials and scale (bph_scf.cu)
     void *noalloc_scratch = nullptr;   // device address of the allocation-free contraction's scratch array
     long long launches = 0;
     size_t bytes = 0;
@@ -311,6 +319,22 @@ int select_mixed_kind(bph_ctx *c, int kind);
 // Work area of the global-memory refinement kernel (allocated on first use).
 int ensure_mixed_work(bph_ctx *c);
 int contract_configure(bph_ctx *c);
+// Warp-cooperative FP64 ADI (bph_adi_warp.cu).  warp_configure selects it
+// for the grids it covers (c->adi_warp != 0) and packs the per-slot
+// coefficients; launch_pack_warp fills a schedule's factor blocks;
+// launch_adi_warp runs nsteps_run steps of nslots * nrows slots (block row
+// r solves instance inst_map[r], slot slot_map[b] of the row).
+int warp_configure(bph_ctx *c);
+// SCF-like density update and renormalisation in place (bph_scf.cu);
+// d_part: scf_scratch_doubles() of scratch (partials, then scale and mass).
+cudaError_t launch_scf_update(bph_ctx *c, double *d_rho, double eps, double mass, unsigned long long seed,
+                              int iteration, double *d_part);
+size_t scf_scratch_doubles();
+size_t warp_block_doubles(int n);
+cudaError_t launch_pack_warp(bph_ctx *c, Schedule &s);
+cudaError_t launch_adi_warp(bph_ctx *c, const Schedule &s, int step0, int nsteps_run, bool cold, double *P,
+                            const double *R, int nrows, const int *inst_map, const int *slot_map, int nslots,
+                            double *norms, cudaStream_t st, bool pdl);
 // Device address of the allocation-free contraction's file-scope scratch
 // array for a context being set up (bph_noalloc.cu).
 int noalloc_setup(bph_ctx *c);

@@ -53,12 +53,16 @@ EXPORTED_SYMBOLS = (
     "bph_server_create", "bph_server_set_converged", "bph_server_capacity", "bph_server_open_client",
     "bph_server_close_client",
     "bph_server_submit", "bph_server_poll", "bph_server_wait", "bph_server_stats", "bph_server_destroy",
-    "bph_register_host", "bph_unregister_host",
+    "bph_register_host", "bph_unregister_host", "bph_read_continuation", "bph_restore_continuation",
+    "bph_scf_step", "bph_scf_mass", "bph_batch_copy_moments",
 )
 
 #: bph_configure keys and values.
 CFG_MIXED_ADI = 0
 MIXED_ADI_AUTO, MIXED_ADI_FORWARD, MIXED_ADI_INCREMENT = 0, 1, 2
+
+#: bph_info(BPH_INFO_ADI_KERNEL) values.
+ADI_KERNEL_WARP, ADI_KERNEL_SEGMENTED, ADI_KERNEL_ONCHIP, ADI_KERNEL_GRID_WIDE = 1, 2, 3, 4
 
 #: bph_run_phase phase ids.
 PHASE_FFT_RHO, PHASE_CONTRACT, PHASE_SLOTS, PHASE_ADI, PHASE_FFT_INV = range(5)
@@ -131,6 +135,8 @@ def load_library(path: str | None = None):
     L.bph_batch_solve_converged.argtypes = [vp, i, ctypes.POINTER(vp), ctypes.POINTER(vp), i, i, ctypes.c_double, i,
                                             i, i, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_double)]
     L.bph_batch_solve_converged.restype = ctypes.c_int
+    L.bph_batch_copy_moments.argtypes = [vp, i, dp, sz]
+    L.bph_batch_copy_moments.restype = ctypes.c_int
     L.bph_batch_destroy.argtypes = [vp]
     L.bph_batch_destroy.restype = ctypes.c_int
     ll, dbl = ctypes.c_longlong, ctypes.c_double
@@ -167,6 +173,14 @@ def load_library(path: str | None = None):
     L.bph_launch_count.restype = ctypes.c_longlong
     L.bph_device_bytes.argtypes = [vp]
     L.bph_device_bytes.restype = ctypes.c_size_t
+    L.bph_scf_step.argtypes = [vp, dp, dp, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong, i, i]
+    L.bph_scf_step.restype = i
+    L.bph_scf_mass.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    L.bph_scf_mass.restype = i
+    L.bph_read_continuation.argtypes = [ctypes.c_char_p, ctypes.POINTER(Grid), dp, dp]
+    L.bph_read_continuation.restype = i
+    L.bph_restore_continuation.argtypes = [vp, ctypes.c_char_p, dp]
+    L.bph_restore_continuation.restype = i
     L.bph_register_host.argtypes = [vp, sz]
     L.bph_register_host.restype = i
     L.bph_unregister_host.argtypes = [vp]
@@ -278,6 +292,13 @@ class PotentialSolver:
             raise ValueError(f"pot has shape {a.shape}, expected {self.shape}")
         _check(self._lib.bph_set_potential(self._h, _host_ptr(a), 0))
 
+    def restore_continuation(self, path: str) -> np.ndarray:
+        """Warm state from the reference's continuation record (fort.12.<tstep>.<rank>,
+        ritecont_frac_new.F90:151-160); returns the density stored beside it."""
+        rho = np.empty(self.shape, dtype=np.float64, order="F")
+        _check(self._lib.bph_restore_continuation(self._h, os.fsencode(path), _host_ptr(rho)))
+        return rho
+
     def solve_nsteps(self, rho, nsteps: int, cold: bool) -> np.ndarray:
         r = self._rho_host(rho)
         pot = np.empty(self.shape, dtype=np.float64, order="F")
@@ -326,6 +347,20 @@ class PotentialSolver:
         """Enqueue one solve on device arrays (pointers or CUDA tensors)."""
         _check(self._lib.bph_potential_solver_device(self._h, _dev_ptr(d_rho), _dev_ptr(d_pot), int(tstep)))
 
+    def scf_step(self, d_rho, d_pot, eps: float = 0.01, mass: float = 0.0, seed: int = 20261203,
+                 iteration: int = 0, tstep: int = 2) -> None:
+        """One SCF-like iteration on device arrays (bph_scf_step): the seeded
+        density update rho <- 0.9 rho + 0.1 rho (1 + eps xi), renormalised to
+        `mass` (<= 0: its mass before the update), then potential_solver."""
+        _check(self._lib.bph_scf_step(self._h, _dev_ptr(d_rho), _dev_ptr(d_pot), float(eps), float(mass),
+                                      int(seed) & 0xFFFFFFFFFFFFFFFF, int(iteration), int(tstep)))
+
+    def scf_mass(self):
+        """(target mass, renormalisation factor) of the last scf_step."""
+        m, sc = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        _check(self._lib.bph_scf_mass(self._h, ctypes.byref(m), ctypes.byref(sc)))
+        return m.value, sc.value
+
     def solve_nsteps_device(self, d_rho, d_pot, nsteps: int, cold: bool) -> None:
         _check(self._lib.bph_solve_nsteps(self._h, _dev_ptr(d_rho), _dev_ptr(d_pot), int(nsteps),
                                           int(bool(cold)), 1))
@@ -357,7 +392,8 @@ class PotentialSolver:
     def info(self) -> dict:
         """Launch-configuration facts (bph_info)."""
         names = ("adi_threads", "adi_smem", "mixed_threads", "mixed_smem", "mixed_ctas_per_sm", "contract_split",
-                 "mixed_kind", "mixed_forward_ns", "mixed_increment_ns", "adi_prefetch")
+                 "mixed_kind", "mixed_forward_ns", "mixed_increment_ns", "adi_prefetch", "adi_kernel",
+                 "adi_warp_smem")
         return {n: int(self._lib.bph_info(self._h, i)) for i, n in enumerate(names)}
 
     def set_mixed_adi(self, kind: int) -> None:
@@ -372,6 +408,16 @@ class PotentialSolver:
     @property
     def device_bytes(self) -> int:
         return int(self._lib.bph_device_bytes(self._h))
+
+
+def read_continuation(path: str, numr: int, numz: int, numphi: int):
+    """(rho, pot) of the reference's continuation record (bph_read_continuation),
+    Fortran-ordered (numr, numz, numphi) arrays."""
+    g = Grid(int(numr), int(numz), int(numphi), 1.0, 2, 2)
+    rho = np.empty((numr, numz, numphi), dtype=np.float64, order="F")
+    pot = np.empty_like(rho)
+    _check(load_library().bph_read_continuation(os.fsencode(path), ctypes.byref(g), _host_ptr(rho), _host_ptr(pot)))
+    return rho, pot
 
 
 def register_host(a: np.ndarray) -> None:
@@ -477,6 +523,13 @@ class Batch:
     @property
     def device_bytes(self) -> int:
         return int(self._lib.bph_batch_device_bytes(self._h))
+
+    def moments_S(self, n: int) -> np.ndarray:
+        """Boundary moments S[pos][m][b][cos|sin] of positions 0..n-1 of the last call."""
+        mmax, nb = self.solver.mmax, self.solver.nb
+        out = np.empty(n * mmax * nb * 2, dtype=np.float64)
+        _check(self._lib.bph_batch_copy_moments(self._h, int(n), _host_ptr(out), out.size))
+        return out.reshape(n, mmax, nb, 2)
 
 
 class Plan:

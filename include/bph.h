@@ -61,6 +61,24 @@ int bph_potential_solver(bph_ctx_t *ctx, const double *rho, double *pot, int tst
  * without waiting.  A non-finite density is reported by bph_synchronize. */
 int bph_potential_solver_device(bph_ctx_t *ctx, const double *d_rho, double *d_pot, int tstep);
 
+/* One SCF-like iteration on DEVICE arrays in one call (no counterpart in
+ * the reference, whose SCF code produced the models scfin_frac.F90:105-125
+ * reads from disk): the density is mixed with a seeded perturbation of
+ * itself, rho <- 0.9 rho + 0.1 rho (1 + eps xi), xi ~ N(0,1) per zone
+ * from a counter-based generator keyed by (seed, iteration, zone), so a
+ * sequence is reproducible; renormalised so that its interior mass
+ * sum_{J=2..numr-1, K=2..numz-1, L} rho rhf(J) dr dz dphi equals `mass`
+ * (mass <= 0 keeps the mass it had before the update); then solved as
+ * potential_solver (tstep > 1 warm from the kept potential, else cold).
+ * d_rho is updated in place, d_pot receives the potential.  Enqueued on
+ * the context's stream; a non-finite density is reported by
+ * bph_synchronize. */
+int bph_scf_step(bph_ctx_t *ctx, double *d_rho, double *d_pot, double eps, double mass, unsigned long long seed,
+                 int iteration, int tstep);
+/* Target mass and renormalisation factor of the last bph_scf_step
+ * (synchronises the context's stream); either pointer may be NULL. */
+int bph_scf_mass(bph_ctx_t *ctx, double *mass_out, double *scale_out);
+
 /* Explicit step count (helmadi(nsteps)); cold != 0 starts from zero.
  * on_device != 0 means rho/pot are device arrays (asynchronous). */
 int bph_solve_nsteps(bph_ctx_t *ctx, const double *rho, double *pot, int nsteps, int cold,
@@ -90,6 +108,23 @@ int bph_potential_solver_phieff(bph_ctx_t *ctx, const double *rho, double *pot, 
  * its kept potp (potential_solver.F90:80-87).  The reference instead starts
  * cold after a restart (setup_frac.F90:690). */
 int bph_set_potential(bph_ctx_t *ctx, const double *pot, int on_device);
+
+/* Reads the reference's continuation record: the fort.12.<tstep>.<rank>
+ * file that ritecont_frac_new.F90:151-160 writes with
+ *     write(12) s, t, a, rho, tau, pot, tempa, frac1, frac2
+ * (one Fortran unformatted sequential record of nine real(8) arrays of
+ * the grid's shape, 4-byte record markers; subrecords with negative
+ * leading markers and big-endian files are recognised) and that
+ * setup_frac.F90:647-648 reads for a continued run.  rho_out / pot_out
+ * (host arrays of numr*numz*numphi doubles, either may be NULL) receive
+ * the density and the potential.  BPH_ERR_INVALID when the file is
+ * missing or its record does not hold nine arrays of the grid's shape. */
+int bph_read_continuation(const char *path, const bph_grid_t *grid, double *rho_out, double *pot_out);
+
+/* bph_read_continuation on the context's grid, then bph_set_potential
+ * with the stored potential: the next tstep > 1 solve continues warm from
+ * the potential of the run that wrote the file.  rho_out may be NULL. */
+int bph_restore_continuation(bph_ctx_t *ctx, const char *path, double *rho_out);
 
 /* Mixed-precision converged solve (no counterpart in the reference, which
  * always runs a fixed 5 or 20 FP64 steps): iterative refinement in which
@@ -143,6 +178,10 @@ int bph_batch_solve_converged(bph_batch_t *batch, int n, const double *const *rh
                               double *resid_out);
 int bph_batch_destroy(bph_batch_t *batch);
 size_t bph_batch_device_bytes(const bph_batch_t *batch);
+/* Boundary moments of batch positions 0..n-1 from the last batched call
+ * (inspection): out[pos][m][b][cos|sin], the bph_copy_moments layout per
+ * position; count >= n*mmax*nb*2. */
+int bph_batch_copy_moments(bph_batch_t *batch, int n, double *out, size_t count);
 
 /* ---- plans: batches on several grids as one graph launch -------------
  *
@@ -307,6 +346,12 @@ int bph_green_contract_noalloc(bph_ctx_t *ctx, const double *d_mom, double *d_S)
 #define BPH_INFO_MIXED_FORWARD_NS 7   /* setup-time duration of a 5-step forwarding-form launch, ns (0: not timed) */
 #define BPH_INFO_MIXED_INCREMENT_NS 8 /* the same for the increment form */
 #define BPH_INFO_ADI_PREFETCH 9       /* bulk-copy factor prefetch: bit 0 FP64 ADI, bit 1 FP32 refinement ADI */
+#define BPH_INFO_ADI_KERNEL 10        /* FP64 drop-in ADI kernel in use (BPH_ADI_KERNEL_*) */
+#define BPH_INFO_ADI_WARP_SMEM 11     /* dynamic shared bytes of the warp-cooperative kernel (0: not used) */
+#define BPH_ADI_KERNEL_WARP 1         /* warp-cooperative line solves, shuffle carries (128x96, 64x64 interiors) */
+#define BPH_ADI_KERNEL_SEGMENTED 2    /* CTA-wide segmented line solves (other grids whose slot fits on chip) */
+#define BPH_ADI_KERNEL_ONCHIP 3       /* one thread per line, slot on chip */
+#define BPH_ADI_KERNEL_GRID_WIDE 4    /* slots beyond shared memory: grid-wide panel kernels */
 long long bph_info(const bph_ctx_t *ctx, int what);
 
 /* Tuning knobs (no counterpart in the reference).

@@ -125,3 +125,43 @@ def test_batch_converged_equals_single_converged(bph, grid):
         s.close()
     batch.close()
     solver.close()
+
+
+@pytest.mark.parametrize("n", [1, 4, 5, 16, 33], ids=lambda n: f"n{n}")
+def test_tensor_core_contraction_matches_single_solve_moments(bph, n):
+    """The batched boundary contraction (FP64 tensor cores, DMMA) gives every
+    position the boundary moments S of its own single solve to 1e-13, at
+    every batch size (33 positions: two column blocks of the kernel)."""
+    grid = (34, 26, 64, 1.0 / 30.0, 2, 30)
+    rhos = _densities(grid, n)
+    solver = bph.PotentialSolver(*grid)
+    batch = bph.Batch(solver, capacity=n)
+    batch.solve(rhos, 0)
+    got = batch.moments_S(n)
+    single = bph.PotentialSolver(*grid)
+    for i in range(n):
+        single.potential_solver(rhos[i], 0)
+        assert rel_l2(got[i], single.moments_S()) <= 1e-13, i
+    single.close()
+    batch.close()
+    solver.close()
+
+
+def test_tensor_core_contraction_production_grid(bph):
+    """130x98x256, 16 positions: S per position against its single solve."""
+    from bipoly_hydro_b200 import fields
+
+    grid = (130, 98, 256, 1.0 / 126.0, 2, 30)
+    n = 16
+    rhos = [fields.bipolytrope_pair(mass_ratio=0.2 + 0.05 * i) for i in range(n)]
+    solver = bph.PotentialSolver(*grid)
+    batch = bph.Batch(solver, capacity=n)
+    batch.solve(rhos, 0)
+    got = batch.moments_S(n)
+    single = bph.PotentialSolver(*grid)
+    for i in range(0, n, 5):
+        single.potential_solver(rhos[i], 0)
+        assert rel_l2(got[i], single.moments_S()) <= 1e-13, i
+    single.close()
+    batch.close()
+    solver.close()

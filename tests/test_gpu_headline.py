@@ -4,9 +4,9 @@
 bipolytrope pair, a cold solve and then warm solves with the density rotated
 by one azimuthal zone per call (potential_solver.F90:80-94 with
 main.F90:396).  These tests run it through the same calls and the same
-launch configuration as the benchmark (384-thread on-chip ADI, the side
-stream for the slots without boundary data, programmatic dependent launch,
-8-column FFT tiles) and compare every potential with the oracle at the FP64
+launch configuration as the benchmark (the warp-cooperative on-chip ADI,
+the side stream for the slots without boundary data, programmatic
+dependent launch, 8-column FFT tiles) and compare every potential with the oracle at the FP64
 bar: relative L2 error <= 1e-12 with the same ADI step count.
 
 258x194x64 has the production slot size of the 258x194 grids (256 x 192
@@ -44,7 +44,7 @@ def test_time_step_sequence_host_arrays(oracle_130, pair_rho, bph):
 
     g = bph.PotentialSolver(*GRID_130)
     info = g.info()
-    assert info["adi_threads"] == 384, info
+    assert info["adi_kernel"] == bph.solver.ADI_KERNEL_WARP, info
     rho = pair_rho
     for tstep in range(0, 5):
         po = oracle_130.potential_solver(rho, tstep)
@@ -129,4 +129,26 @@ def test_grid_wide_adi_at_production_slot_size(oracle_mod, bph):
         assert err <= POT_TOL, (tstep, err)
         rho = fields.rotate(rho)
     o.close()
+    g.close()
+
+
+@pytest.mark.parametrize("kernel", ["warp", "segmented"])
+def test_both_on_chip_adi_kernels_match_oracle(oracle_130, pair_rho, bph, monkeypatch, kernel):
+    """The warp-cooperative ADI (default on this grid) and the CTA-wide
+    segmented one (BPH_ADI_WARP=0 at set-up) both meet the bar, cold and warm,
+    including the converged form whose cycles report update norms."""
+    from bipoly_hydro_b200 import fields
+
+    monkeypatch.setenv("BPH_ADI_WARP", "1" if kernel == "warp" else "0")
+    g = bph.PotentialSolver(*GRID_130)
+    want = bph.solver.ADI_KERNEL_WARP if kernel == "warp" else bph.solver.ADI_KERNEL_SEGMENTED
+    assert g.info()["adi_kernel"] == want
+    rho = pair_rho
+    for tstep in (0, 2):
+        err = rel_l2(g.potential_solver(rho, tstep), oracle_130.potential_solver(rho, tstep))
+        assert err <= POT_TOL, (kernel, tstep, err)
+        rho = fields.rotate(rho)
+    po, co, _ = oracle_130.solve_converged(pair_rho, 10, True, 1e-11, 60)
+    pg, info = g.solve_converged(pair_rho, 10, True, 1e-11, 60)
+    assert info.cycles == co and rel_l2(pg, po) <= POT_TOL
     g.close()
