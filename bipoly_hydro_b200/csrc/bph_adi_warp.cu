@@ -87,9 +87,28 @@ __device__ __forceinline__ void cp16(void *dst, const void *src) {
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// n doubles (even), 16-byte aligned at both ends, copied by the whole CTA.
-__device__ __forceinline__ void copy_block(double *dst, const double *src, int n, int tid) {
-    for (int c = tid; c < n / 2; c += kWThreads) cp16(dst + 2 * c, src + 2 * c);
+// n elements of T (a whole number of 16-byte chunks), 16-byte aligned at
+// both ends, copied by the whole CTA.
+template <typename T>
+__device__ __forceinline__ void copy_block(T *dst, const T *src, int n, int tid) {
+    constexpr int E = 16 / (int)sizeof(T);
+    for (int c = tid; c < n / E; c += kWThreads) cp16(dst + E * c, src + E * c);
+}
+
+template <typename T>
+struct Pair;
+template <>
+struct Pair<double> {
+    using type = double2;
+};
+template <>
+struct Pair<float> {
+    using type = float2;
+};
+// Two consecutive elements (8- or 16-byte aligned).
+template <typename T>
+__device__ __forceinline__ typename Pair<T>::type ldp(const T *p) {
+    return *reinterpret_cast<const typename Pair<T>::type *>(p);
 }
 
 __device__ __forceinline__ double2 lds2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
@@ -108,51 +127,51 @@ __device__ __forceinline__ int swz(int k, int j) {
 
 // Forward carry scan over the 8 lanes of a group: in a = L_end(g), out the
 // carry into segment g, y_end(g-1) (0 for g = 0).
-template <int NL>
-__device__ __forceinline__ void scan_forward(double (&a)[NL], const double *scan, int g) {
-    const double p1 = scan[g], p2 = scan[8 + g], p4 = scan[16 + g];
+template <typename T, int NL>
+__device__ __forceinline__ void scan_forward(T (&a)[NL], const T *scan, int g) {
+    const T p1 = scan[g], p2 = scan[8 + g], p4 = scan[16 + g];
 #pragma unroll
     for (int l = 0; l < NL; ++l) {
-        double t = __shfl_up_sync(kFull, a[l], 1, 8);
+        T t = __shfl_up_sync(kFull, a[l], 1, 8);
         if (g >= 1) a[l] = fma(p1, t, a[l]);
         t = __shfl_up_sync(kFull, a[l], 2, 8);
         if (g >= 2) a[l] = fma(p2, t, a[l]);
         t = __shfl_up_sync(kFull, a[l], 4, 8);
         if (g >= 4) a[l] = fma(p4, t, a[l]);
         t = __shfl_up_sync(kFull, a[l], 1, 8);
-        a[l] = (g >= 1) ? t : 0.0;
+        a[l] = (g >= 1) ? t : (T)0;
     }
 }
 
 // Backward carry scan: in b = M_start(g), out the carry into segment g from
 // above, x_start(g+1) (0 for g = 7).
-template <int NL>
-__device__ __forceinline__ void scan_backward(double (&b)[NL], const double *scan, int g) {
-    const double q1 = scan[24 + g], q2 = scan[32 + g], q4 = scan[40 + g];
+template <typename T, int NL>
+__device__ __forceinline__ void scan_backward(T (&b)[NL], const T *scan, int g) {
+    const T q1 = scan[24 + g], q2 = scan[32 + g], q4 = scan[40 + g];
 #pragma unroll
     for (int l = 0; l < NL; ++l) {
-        double t = __shfl_down_sync(kFull, b[l], 1, 8);
+        T t = __shfl_down_sync(kFull, b[l], 1, 8);
         if (g <= 6) b[l] = fma(q1, t, b[l]);
         t = __shfl_down_sync(kFull, b[l], 2, 8);
         if (g <= 5) b[l] = fma(q2, t, b[l]);
         t = __shfl_down_sync(kFull, b[l], 4, 8);
         if (g <= 3) b[l] = fma(q4, t, b[l]);
         t = __shfl_down_sync(kFull, b[l], 1, 8);
-        b[l] = (g <= 6) ? t : 0.0;
+        b[l] = (g <= 6) ? t : (T)0;
     }
 }
 
 // Phases A, scan, B, scan, C of NL lines of segment length L held in v,
 // with the factor block f (segment-interleaved layout).
-template <int NL, int L>
-__device__ __forceinline__ void solve_lines(double (&v)[NL][L], const double *f, int g) {
-    double c[NL];
+template <typename T, int NL, int L>
+__device__ __forceinline__ void solve_lines(T (&v)[NL][L], const T *f, int g) {
+    T c[NL];
 #pragma unroll
-    for (int l = 0; l < NL; ++l) c[l] = 0.0;
+    for (int l = 0; l < NL; ++l) c[l] = (T)0;
     // A: forward elimination, zero carry-in
 #pragma unroll
     for (int t = 0; t < L / 2; ++t) {
-        const double2 dd = lds2(f + fo_dd(L) + (t * 8 + g) * 2);
+        const auto dd = ldp(f + fo_dd(L) + (t * 8 + g) * 2);
 #pragma unroll
         for (int l = 0; l < NL; ++l) {
             c[l] = v[l][2 * t] - dd.x * c[l];
@@ -161,25 +180,25 @@ __device__ __forceinline__ void solve_lines(double (&v)[NL][L], const double *f,
             v[l][2 * t + 1] = c[l];
         }
     }
-    scan_forward<NL>(c, f + fo_scan(L), g);
+    scan_forward<T, NL>(c, f + fo_scan(L), g);
     // B: y = L + G y_in, backward substitution with zero carry-in
-    double m[NL];
+    T m[NL];
 #pragma unroll
-    for (int l = 0; l < NL; ++l) m[l] = 0.0;
+    for (int l = 0; l < NL; ++l) m[l] = (T)0;
 #pragma unroll
     for (int i = L - 1; i >= 0; --i) {
-        const double2 gg = lds2(f + fo_gg(L) + (i * 8 + g) * 2);
+        const auto gg = ldp(f + fo_gg(L) + (i * 8 + g) * 2);
 #pragma unroll
         for (int l = 0; l < NL; ++l) {
             m[l] = (v[l][i] + gg.x * c[l]) - gg.y * m[l];
             v[l][i] = m[l];
         }
     }
-    scan_backward<NL>(m, f + fo_scan(L), g);
+    scan_backward<T, NL>(m, f + fo_scan(L), g);
     // C: x = M + K x_in
 #pragma unroll
     for (int t = 0; t < L / 2; ++t) {
-        const double2 kk = lds2(f + fo_k(L) + (t * 8 + g) * 2);
+        const auto kk = ldp(f + fo_k(L) + (t * 8 + g) * 2);
 #pragma unroll
         for (int l = 0; l < NL; ++l) {
             v[l][2 * t] = v[l][2 * t] + kk.x * m[l];
@@ -342,7 +361,7 @@ __global__ void __launch_bounds__(kWThreads, 1) k_adi_warp(WarpArgs a) {
                     v[l][2 * t + 1] = q.y;
                 }
             }
-            solve_lines<NLR, LR>(v, rb, g);
+            solve_lines<double, NLR, LR>(v, rb, g);
             // vertical right-hand side of this step (helmadi.F90:276-340) times the vertical 1/bet
             double le[NLR], re[NLR], ibz[NLR];
 #pragma unroll
@@ -388,7 +407,7 @@ __global__ void __launch_bounds__(kWThreads, 1) k_adi_warp(WarpArgs a) {
                     v[2 * m + 1][i] = q.y;
                 }
             }
-            solve_lines<NLZ, LZ>(v, vb, g);
+            solve_lines<double, NLZ, LZ>(v, vb, g);
             if (it + 1 < n) {
                 cp_wait_all();    // the next step's blocks (this thread's copies)
                 __syncthreads();  // every lane has read W; every copy has landed

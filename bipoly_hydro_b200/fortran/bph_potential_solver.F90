@@ -36,6 +36,13 @@ module bph_c
          real(c_double), intent(in) :: a(*)
          integer(c_size_t), value :: bytes
       end function bph_register_host
+      integer(c_int) function bph_restore_continuation(ctx, path, rho) &
+            bind(c, name="bph_restore_continuation")
+         import :: c_int, c_ptr, c_char
+         type(c_ptr), value :: ctx
+         character(kind=c_char), intent(in) :: path(*)
+         type(c_ptr), value :: rho
+      end function bph_restore_continuation
       type(c_ptr) function bph_last_error() bind(c, name="bph_last_error")
          import :: c_ptr
       end function bph_last_error
