@@ -737,6 +737,38 @@ def run_gpu(args, world, rank, local):
         del graph
         solver.synchronize()
 
+    # ---- the same solve with the GPU split into two SM partitions --------
+    # (green contexts: the contraction on one, the free-slot ADI on the other)
+    green = None
+    if rank == 0 and not args.no_green:
+        green = []
+        for sms in [int(x) for x in args.green_sms.split(",") if x]:
+            os.environ["BPH_GREEN"], os.environ["BPH_GREEN_SMS"] = "1", str(sms)
+            try:
+                gs = B.PotentialSolver(**GRID)
+            finally:
+                os.environ.pop("BPH_GREEN", None)
+                os.environ.pop("BPH_GREEN_SMS", None)
+            gs.set_stream(stream)
+            got = gs.info()["green_sms"]
+            gp = torch.empty_like(d_pot)
+            gs.potential_solver_device(rhos[0], gp, 0)
+            for w in range(3):
+                gs.potential_solver_device(rhos[(1 + w) % nrot], gp, 2 + w)
+            ga, gb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            nrep = max(50, min(args.steps, 500))
+            torch.cuda.synchronize()
+            ga.record(stream)
+            for i in range(nrep):
+                gs.potential_solver_device(rhos[(4 + i) % nrot], gp, 5 + i)
+            gb.record(stream)
+            torch.cuda.synchronize()
+            gms = ga.elapsed_time(gb) / nrep
+            green.append({"requested_sms": sms, "contraction_sms": got, "solves_per_s": 1e3 / gms,
+                          "ms_per_solve": gms})
+            gs.close()
+            del gp
+
     # ---- per-phase kernel times (CUDA events on the launch stream) ------
     def time_phase(phase, reps, **kw):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1004,6 +1036,7 @@ def run_gpu(args, world, rank, local):
             "serving": serving,
             "serving_mixed_grids": serving_mixed,
             "graph_replay": graph_replay,
+            "sm_partitions": green,
             "launch_config": solver_info,
             "gpu_launches": launches,
             "clocks": clocks,
@@ -1041,6 +1074,9 @@ def main():
                     help="offered rates of the mixed-grid serving section (empty skips)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
     ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay section")
+    ap.add_argument("--no-green", action="store_true", help="skip the SM-partition section")
+    ap.add_argument("--green-sms", default="48,64,80,96",
+                    help="contraction SMs of the SM-partition section (green contexts)")
     ap.add_argument("--serve-iters", type=int, default=8, help="SCF-like requests per client per rate")
     ap.add_argument("--converged-steps", type=int, default=20,
                     help="warm converged solves timed per form (FP64 and mixed); 0 skips")

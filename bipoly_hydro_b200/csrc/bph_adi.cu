@@ -1351,7 +1351,7 @@ int adi_configure(bph_ctx *c) {
 }
 
 int select_mixed_kind(bph_ctx *c, int kind) {
-    if (kind < 1 || kind > 3 || !c->mixed_smem_kind[kind]) {
+    if (kind < 1 || kind > 4 || !c->mixed_smem_kind[kind]) {
         c->adi_mixed_smem = 0;
         c->adi_mixed_per_sm = 0;
         return (kind == 0) ? BPH_OK : BPH_ERR_INVALID;
@@ -1460,6 +1460,7 @@ cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {
     a.ver_pk = sch.d_ver_pk[1];
     a.pkr = packed_block<float>(c->nr);
     a.pkz = packed_block<float>(c->nz);
+    if (c->mixed_kind == BPH_MIXED_ADI_WARP) return launch_defect_warp(c, sch, c->d_P, c->d_R, 1, nullptr, c->d_red);
     ++c->launches;
     void *args[] = {&a};
     if (c->mixed_kind == BPH_MIXED_ADI_GLOBAL) {
@@ -1477,6 +1478,7 @@ cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {
 cudaError_t launch_defect_batch(bph_ctx *c, const Schedule &sch, double *P, const double *R, int n, const int *d_map,
                                 double *norms) {
     if (!c->adi_mixed_smem || c->mixed_kind == BPH_MIXED_ADI_GLOBAL) return cudaErrorNotSupported;
+    if (c->mixed_kind == BPH_MIXED_ADI_WARP) return launch_defect_warp(c, sch, P, R, n, d_map, norms);
     AdiArgs a = make_args(c, sch, 0, sch.nsteps, false);
     a.P = P;
     a.R = R;

@@ -84,6 +84,9 @@ __device__ __forceinline__ uint32_t saddr(const void *p) { return (uint32_t)__cv
 __device__ __forceinline__ void cp16(void *dst, const void *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr(dst)), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp8(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(saddr(dst)), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
@@ -256,30 +259,53 @@ __global__ void __launch_bounds__(kWThreads, 1) k_adi_warp(WarpArgs a) {
     const double a_side = a.alphar[numr - 2];  // alphar(numr-1)
     pdl_wait();
 
-    // R -> shared (swizzled), 8 loads in flight per thread
+    // R -> shared, 16-byte chunks straight into their swizzled places, and
+    // (warm start) the initial potential's interior into W, element by
+    // element: every copy of the prologue is in flight at once.
     constexpr int kTot = NR * NZ;
-    static_assert(kTot % (kWThreads * 8) == 0, "whole load batches");
-#pragma unroll 1
-    for (int e0 = tid; e0 < kTot; e0 += kWThreads * 8) {
-        double r[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) r[u] = __ldg(Rg + e0 + u * kWThreads);
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int e = e0 + u * kWThreads;
-            Rsh[swz<NLR, NLZ>(e / NR, e % NR)] = r[u];
+    for (int q = tid; q < kTot / 2; q += kWThreads) {
+        const int e = 2 * q;
+        cp16(Rsh + swz<NLR, NLZ>(e / NR, e % NR), Rg + e);
+    }
+    if (!a.cold) {
+        for (int e = tid; e < kTot; e += kWThreads) {
+            const int k = e / NR, j = e % NR;
+            cp8(W + swz<NLR, NLZ>(k, j), Pg + (j + 1) + (long long)numr * (k + 1));
         }
     }
-    __syncthreads();
-    // Dirichlet terms: top row (K = numz-1), side column (J = numr-1), bottom row (isym 1)
-    for (int j = tid; j < NR; j += kWThreads) {
-        Rsh[swz<NLR, NLZ>(NZ - 1, j)] += gamma * Pg[(j + 1) + (long long)numr * (numz - 1)];
-        if (!sym_bottom) Rsh[swz<NLR, NLZ>(0, j)] += gamma * Pg[j + 1];
+    cp_commit();
+    // Dirichlet terms (helmadi.F90:252-256, 327-340): thread t folds the top
+    // (and, isym 1, bottom) zone of column t, and the side zone of row t;
+    // the corners take the top/bottom term first, then the side term.
+    double top_v = 0.0, bot_v = 0.0, side_top = 0.0, side_bot = 0.0, side_v = 0.0;
+    if (tid < NR) {
+        top_v = Pg[(tid + 1) + (long long)numr * (numz - 1)];
+        if (!sym_bottom) bot_v = Pg[tid + 1];
+        if (tid == NR - 1) {
+            side_top = Pg[(numr - 1) + (long long)numr * NZ];
+            side_bot = Pg[(numr - 1) + (long long)numr];
+        }
     }
-    __syncthreads();
-    for (int k = tid; k < NZ; k += kWThreads)
-        Rsh[swz<NLR, NLZ>(k, NR - 1)] -= a_side * Pg[(numr - 1) + (long long)numr * (k + 1)];
+    const bool side_row = tid < NZ && tid != NZ - 1 && !(tid == 0 && !sym_bottom);
+    if (side_row) side_v = Pg[(numr - 1) + (long long)numr * (tid + 1)];
     cp_wait_all();
+    __syncthreads();
+    if (tid < NR) {
+        double *t = Rsh + swz<NLR, NLZ>(NZ - 1, tid);
+        double v = *t + gamma * top_v;
+        if (tid == NR - 1) v = v - a_side * side_top;
+        *t = v;
+        if (!sym_bottom) {
+            double *b = Rsh + swz<NLR, NLZ>(0, tid);
+            double u = *b + gamma * bot_v;
+            if (tid == NR - 1) u = u - a_side * side_bot;
+            *b = u;
+        }
+    }
+    if (side_row) {
+        double *sd = Rsh + swz<NLR, NLZ>(tid, NR - 1);
+        *sd = *sd - a_side * side_v;
+    }
     __syncthreads();
 
     // Radial right-hand side of step `st` from a potential held in vertical
@@ -324,15 +350,21 @@ __global__ void __launch_bounds__(kWThreads, 1) k_adi_warp(WarpArgs a) {
         }
     };
 
-    // first radial right-hand side, from the initial potential
+    // first radial right-hand side, from the initial potential (in W)
     {
         double v[NLZ][LZ];
 #pragma unroll
-        for (int i = 0; i < LZ; ++i)
+        for (int i = 0; i < LZ; ++i) {
+            const int k = LZ * g + i;
 #pragma unroll
-            for (int l = 0; l < NLZ; ++l)
-                v[l][i] = a.cold ? 0.0
-                                 : Pg[(NLZ * p + l + 1) + (long long)numr * (LZ * g + i + 1)];
+            for (int m = 0; m < NLZ / 2; ++m) {
+                const double2 q = a.cold ? make_double2(0.0, 0.0)
+                                         : lds2(W + k * NR + 2 * (((NLZ / 2) * p + m) ^ x));
+                v[2 * m][i] = q.x;
+                v[2 * m + 1][i] = q.y;
+            }
+        }
+        __syncthreads();  // every lane has read the initial potential
         store_radial_rhs(v, radb + fo_ib(LR), a.dt[a.step0]);
     }
     __syncthreads();
@@ -453,11 +485,298 @@ __global__ void __launch_bounds__(kWThreads, 1) k_adi_warp(WarpArgs a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Mixed-precision refinement cycle, warp-cooperative, T = float (the FP32
+// counterpart of k_adi_warp for the converged mixed form).  One CTA per
+// slot, two CTAs per SM.
+//   prologue  FP64 residual r = -4 pi rho_hat - A phi of the current
+//             potential (its Dirichlet columns enter through the stencil),
+//             rounded to float into Rv; delta = 0, so the first radial
+//             right-hand side is r (1/bet);
+//   body      2 nsteps + 1 half-steps on the defect equation A delta = r
+//             with zero Dirichlet data: radial at step 0, then (vertical,
+//             radial) at every step -- the cycle opens and closes on a
+//             radial half-step, the order that keeps FP32 rounding of the
+//             stiff near-axis components out of the result (see the
+//             segmented refinement kernels in bph_adi.cu);
+//   epilogue  phi += delta in FP64; per-slot |delta|^2 and |phi|^2.
+// Shared memory (floats): W, Rv (NZ x NR, the 16-byte-chunk swizzle of
+// k_adi_warp: 4 floats per chunk), two radial and two vertical factor
+// blocks (float), the slot's (elambdazb, alphaz, betaz).
+template <int NLR, int NLZ>
+struct WSF {
+    using S = WS<NLR, NLZ>;
+    static constexpr int NR = S::NR, NZ = S::NZ, LR = S::LR, LZ = S::LZ;
+    static constexpr int RAD = S::RAD, VER = S::VER, COEF = S::COEF;  // in floats
+    static constexpr int O_R = NZ * NR;
+    static constexpr int O_RAD = 2 * NZ * NR;
+    static constexpr int O_VER = O_RAD + 2 * RAD;
+    static constexpr int O_COEF = O_VER + 2 * VER;
+    static constexpr int TOTAL = O_COEF + COEF;
+    static_assert(RAD % 4 == 0 && VER % 4 == 0 && COEF % 4 == 0, "blocks must be whole 16-byte chunks");
+    static_assert(LR % 4 == 0 && NLZ == 4, "radial segments and vertical line sets in whole float4 chunks");
+};
+
+template <int NLR, int NLZ>
+__device__ __forceinline__ int swzf(int k, int j) {
+    using S = WS<NLR, NLZ>;
+    const int c = j >> 2;
+    const int x = ((j / S::LR) ^ (k / S::LZ)) & 7;
+    return k * S::NR + 4 * (c ^ x) + (j & 3);
+}
+
+struct WarpDefArgs {
+    double *P;             // slot arrays [inst][N][numr*numz] (FP64, updated in place)
+    const double *R;       // [inst][N][nr*nz]
+    const float *rad;      // radial blocks [nsteps][N][RAD]
+    const float *ver;      // vertical blocks [nsteps][VER]
+    const float *coef;     // [N][COEF]
+    const double *dt;      // [nsteps]
+    const double *brb;     // [N][numr] radial diagonal without dt
+    const double *alphar, *betar, *bzb;
+    double *norms;         // per (instance, slot) |delta|^2, |phi|^2
+    const int *inst_map;   // instance of each block row (nullptr: row)
+    int N, numr, numz, isym, nsteps;
+    double gamma;
+};
+
+template <int NLR, int NLZ>
+__global__ void __launch_bounds__(kWThreads, 2) k_adi_warp_defect(WarpDefArgs a) {
+    using F = WSF<NLR, NLZ>;
+    constexpr int LR = F::LR, LZ = F::LZ, NR = F::NR, NZ = F::NZ;
+    extern __shared__ __align__(16) float smf[];
+    float *W = smf;
+    float *Rv = smf + F::O_R;
+    float *radb = smf + F::O_RAD;
+    float *verb = smf + F::O_VER;
+    const float *coefb = smf + F::O_COEF;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, g = lane & 7;
+    const int p = 4 * w + (lane >> 3);
+    const int x = (g ^ w) & 7;
+    const int s = blockIdx.x % a.N, row = blockIdx.x / a.N;
+    const long long blk = (long long)(a.inst_map ? a.inst_map[row] : row) * a.N + s;
+    const int numr = a.numr, numz = a.numz;
+    double *Pg = a.P + blk * (long long)numr * numz;
+    const double *Rg = a.R + blk * (long long)NR * NZ;
+    const size_t rad_step = (size_t)a.N * F::RAD;
+    const float *rad_src = a.rad + (size_t)s * F::RAD;
+    const double gamma = a.gamma;
+    const float gf = (float)gamma;
+    const bool sym_bottom = (a.isym != 1);
+    const int n = a.nsteps;
+    const double *brb = a.brb + (long long)s * numr;
+
+    copy_block(radb, rad_src, F::RAD, tid);
+    copy_block(verb, a.ver, F::VER, tid);
+    copy_block(const_cast<float *>(coefb), a.coef + (size_t)s * F::COEF, F::COEF, tid);
+    cp_commit();
+    pdl_wait();
+    cp_wait_all();
+    __syncthreads();
+    // FP64 residual of the current potential, 8 zones per thread in flight
+    {
+        const float *ibr = radb + fo_ib(LR);
+        constexpr int kTot = NR * NZ;
+#pragma unroll 1
+        for (int e0 = tid; e0 < kTot; e0 += kWThreads * 8) {
+            double rr[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int e = e0 + u * kWThreads;
+                const int k = e / NR, j = e % NR;
+                const double *pc = Pg + (long long)numr * (k + 1) + 1 + j;
+                const double c = pc[0], ea = pc[1], no = pc[numr];
+                const double we = (j > 0) ? pc[-1] : 0.0;
+                const double so = (k > 0 || !sym_bottom) ? pc[-numr] : 0.0;
+                const double ar = brb[j + 1] * c + a.alphar[j + 1] * ea + a.betar[j + 1] * we;
+                const double az = a.bzb[k + 1] * c - gamma * no - gamma * so;
+                rr[u] = Rg[e] - ar - az;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int e = e0 + u * kWThreads;
+                const int k = e / NR, j = e % NR;
+                const int off = swzf<NLR, NLZ>(k, j);
+                const float r32 = (float)rr[u];
+                Rv[off] = r32;
+                W[off] = r32 * ibr[j];
+            }
+        }
+    }
+    __syncthreads();
+
+#pragma unroll 1
+    for (int h = 0; h <= 2 * n; ++h) {
+        const bool radial = (h & 1) == 0;
+        // prefetch: radial step i at the start of half-step 2i, vertical step i at 2i - 1
+        if (radial && h >= 2 && h / 2 < n) {
+            const int i = h / 2;
+            copy_block(radb + (i & 1) * F::RAD, rad_src + (size_t)i * rad_step, F::RAD, tid);
+            cp_commit();
+        }
+        if (!radial && (h + 1) / 2 < n) {
+            const int i = (h + 1) / 2;
+            copy_block(verb + (i & 1) * F::VER, a.ver + (size_t)i * F::VER, F::VER, tid);
+            cp_commit();
+        }
+        if (radial) {
+            const int st = (h == 0) ? 0 : h / 2 - 1;
+            float v[NLR][LR];
+#pragma unroll
+            for (int l = 0; l < NLR; ++l) {
+                const int k = NLR * p + l;
+#pragma unroll
+                for (int t = 0; t < LR / 4; ++t) {
+                    const float4 q = *reinterpret_cast<const float4 *>(W + k * NR + 4 * (((LR / 4) * g + t) ^ x));
+                    v[l][4 * t] = q.x;
+                    v[l][4 * t + 1] = q.y;
+                    v[l][4 * t + 2] = q.z;
+                    v[l][4 * t + 3] = q.w;
+                }
+            }
+            solve_lines<float, NLR, LR>(v, radb + (st & 1) * F::RAD, g);
+            if (h == 2 * n) {
+                // phi += delta in FP64, per-slot norms
+                pdl_trigger();
+                double sd = 0.0, sp = 0.0;
+#pragma unroll
+                for (int l = 0; l < NLR; ++l) {
+                    double *prow = Pg + (long long)numr * (NLR * p + l + 1) + 1 + LR * g;
+#pragma unroll
+                    for (int i = 0; i < LR; ++i) {
+                        const double d = (double)v[l][i];
+                        const double ph = prow[i] + d;
+                        prow[i] = ph;
+                        sd += d * d;
+                        sp += ph * ph;
+                    }
+                }
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    sd += __shfl_down_sync(kFull, sd, off);
+                    sp += __shfl_down_sync(kFull, sp, off);
+                }
+                __syncthreads();
+                double *red = reinterpret_cast<double *>(W);
+                if (lane == 0) {
+                    red[2 * w] = sd;
+                    red[2 * w + 1] = sp;
+                }
+                __syncthreads();
+                if (tid < 2) {
+                    double tsum = 0.0;
+                    for (int q = 0; q < kWThreads / 32; ++q) tsum += red[2 * q + tid];
+                    const double wgt = (s == 0 || s == a.N / 2) ? 1.0 : 2.0;
+                    a.norms[2 * blk + tid] = wgt * tsum;
+                }
+                break;
+            }
+            // vertical right-hand side of the next half-step (step h / 2)
+            const int sv = h / 2;
+            const float *vb = verb + (sv & 1) * F::VER;
+            float le[NLR], re[NLR], ibz[NLR];
+            const float dtn = (float)a.dt[sv];
+#pragma unroll
+            for (int l = 0; l < NLR; ++l) {
+                le[l] = __shfl_up_sync(kFull, v[l][LR - 1], 1, 8);
+                re[l] = __shfl_down_sync(kFull, v[l][0], 1, 8);
+                if (g == 0) le[l] = 0.f;
+                if (g == 7) re[l] = 0.f;
+            }
+            cp_wait_all();
+            __syncthreads();  // every lane has read W; the next blocks have landed
+#pragma unroll
+            for (int l = 0; l < NLR; ++l) ibz[l] = vb[fo_ib(LZ) + NLR * p + l];
+#pragma unroll
+            for (int t = 0; t < LR / 4; ++t) {
+                float el[4], al[4], be[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int i = 4 * t + e;
+                    el[e] = coefb[((i / 2) * 8 + g) * 2 + (i & 1)];
+                    const float2 ab = ldp(coefb + 8 * LR + (i * 8 + g) * 2);
+                    al[e] = ab.x;
+                    be[e] = ab.y;
+                }
+#pragma unroll
+                for (int l = 0; l < NLR; ++l) {
+                    const int k = NLR * p + l;
+                    const int off = k * NR + 4 * (((LR / 4) * g + t) ^ x);
+                    const float4 r = *reinterpret_cast<const float4 *>(Rv + off);
+                    const float rr[4] = {r.x, r.y, r.z, r.w};
+                    float o[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const int i = 4 * t + e;
+                        const float pl = (i > 0) ? v[l][(i - 1) & (LR - 1)] : le[l];
+                        const float pr = (i + 1 < LR) ? v[l][(i + 1) & (LR - 1)] : re[l];
+                        o[e] = (rr[e] + (el[e] + dtn) * v[l][i] - al[e] * pr - be[e] * pl) * ibz[l];
+                    }
+                    *reinterpret_cast<float4 *>(W + off) = make_float4(o[0], o[1], o[2], o[3]);
+                }
+            }
+            __syncthreads();
+        } else {
+            const int st = (h - 1) / 2;
+            float v[NLZ][LZ];
+#pragma unroll
+            for (int i = 0; i < LZ; ++i) {
+                const int k = LZ * g + i;
+                const float4 q = *reinterpret_cast<const float4 *>(W + k * NR + 4 * (p ^ x));
+                v[0][i] = q.x;
+                v[1][i] = q.y;
+                v[2][i] = q.z;
+                v[3][i] = q.w;
+            }
+            solve_lines<float, NLZ, LZ>(v, verb + (st & 1) * F::VER, g);
+            // radial right-hand side of the next half-step (the radial one of the same step)
+            float dn_e[NLZ], up_e[NLZ], ib[NLZ];
+#pragma unroll
+            for (int l = 0; l < NLZ; ++l) {
+                dn_e[l] = __shfl_up_sync(kFull, v[l][LZ - 1], 1, 8);
+                up_e[l] = __shfl_down_sync(kFull, v[l][0], 1, 8);
+                if (g == 0) dn_e[l] = 0.f;
+                if (g == 7) up_e[l] = 0.f;
+            }
+            cp_wait_all();
+            __syncthreads();
+            {
+                const float4 t4 = *reinterpret_cast<const float4 *>(radb + (st & 1) * F::RAD + fo_ib(LR) + 4 * p);
+                ib[0] = t4.x;
+                ib[1] = t4.y;
+                ib[2] = t4.z;
+                ib[3] = t4.w;
+            }
+            const float dtn = (float)a.dt[st];
+            const float c2 = dtn - 2.f * gf, c1 = dtn - gf;
+#pragma unroll
+            for (int i = 0; i < LZ; ++i) {
+                const int k = LZ * g + i;
+                const bool refl = (k == 0) && sym_bottom;
+                const int off = k * NR + 4 * (p ^ x);
+                const float4 r = *reinterpret_cast<const float4 *>(Rv + off);
+                const float rr[4] = {r.x, r.y, r.z, r.w};
+                float o[4];
+#pragma unroll
+                for (int l = 0; l < NLZ; ++l) {
+                    const float up = (i + 1 < LZ) ? v[l][i + 1] : up_e[l];
+                    const float dn = (i > 0) ? v[l][i - 1] : dn_e[l];
+                    const float rhs = refl ? rr[l] + c1 * v[l][i] + gf * up : rr[l] + c2 * v[l][i] + gf * (up + dn);
+                    o[l] = rhs * ib[l];
+                }
+                *reinterpret_cast<float4 *>(W + off) = make_float4(o[0], o[1], o[2], o[3]);
+            }
+            __syncthreads();
+        }
+    }
+}
+
 // Factor blocks of one schedule in the segment-interleaved layout, from the
 // Thomas factors [1/bet, a/bet, gam, ...] of k_adi_factors: one thread per
 // (step, line system) and segment length L = n / 8.
-__global__ void k_pack_warp(const double *__restrict__ rad, const double *__restrict__ ver, double *__restrict__ rad_w,
-                            double *__restrict__ ver_w, int nsteps, int N, int nr, int nz) {
+template <typename T>
+__global__ void k_pack_warp(const double *__restrict__ rad, const double *__restrict__ ver, T *__restrict__ rad_w,
+                            T *__restrict__ ver_w, int nsteps, int N, int nr, int nz) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long nrad = (long long)nsteps * N;
     if (t >= nrad + nsteps) return;
@@ -465,7 +784,7 @@ __global__ void k_pack_warp(const double *__restrict__ rad, const double *__rest
     const int n = radial ? nr : nz, L = n / 8;
     const double *src = radial ? rad + t * kAdiFactors * nr : ver + (t - nrad) * kAdiFactors * nz;
     const int bsz = 40 * L + 48;
-    double *dst = radial ? rad_w + t * bsz : ver_w + (t - nrad) * bsz;
+    T *dst = radial ? rad_w + t * bsz : ver_w + (t - nrad) * bsz;
     const double *ib = src, *dd = src + n, *gam = src + 2 * n;
     double gend[8], kst[8];
     for (int g = 0; g < 8; ++g) {
@@ -475,9 +794,9 @@ __global__ void k_pack_warp(const double *__restrict__ rad, const double *__rest
             const int j = j0 + i;
             gp = -dd[j] * gp;
             const double gnext = (j + 1 < n) ? gam[j + 1] : 0.0;
-            dst[fo_dd(L) + ((i / 2) * 8 + g) * 2 + (i & 1)] = dd[j];
-            dst[fo_gg(L) + (i * 8 + g) * 2] = gp;
-            dst[fo_gg(L) + (i * 8 + g) * 2 + 1] = gnext;
+            dst[fo_dd(L) + ((i / 2) * 8 + g) * 2 + (i & 1)] = (T)dd[j];
+            dst[fo_gg(L) + (i * 8 + g) * 2] = (T)gp;
+            dst[fo_gg(L) + (i * 8 + g) * 2 + 1] = (T)gnext;
         }
         gend[g] = gp;
         double kp = 1.0;
@@ -485,34 +804,34 @@ __global__ void k_pack_warp(const double *__restrict__ rad, const double *__rest
             const int j = j0 + i;
             const double gnext = (j + 1 < n) ? gam[j + 1] : 0.0;
             kp = -gnext * kp;
-            dst[fo_k(L) + ((i / 2) * 8 + g) * 2 + (i & 1)] = kp;
+            dst[fo_k(L) + ((i / 2) * 8 + g) * 2 + (i & 1)] = (T)kp;
         }
         kst[g] = kp;
     }
-    double *sc = dst + fo_scan(L);
+    T *sc = dst + fo_scan(L);
     for (int g = 0; g < 8; ++g) {
-        sc[g] = gend[g];
-        sc[8 + g] = (g >= 1) ? gend[g] * gend[g - 1] : 0.0;
-        sc[16 + g] = (g >= 3) ? gend[g] * gend[g - 1] * gend[g - 2] * gend[g - 3] : 0.0;
-        sc[24 + g] = kst[g];
-        sc[32 + g] = (g <= 6) ? kst[g] * kst[g + 1] : 0.0;
-        sc[40 + g] = (g <= 4) ? kst[g] * kst[g + 1] * kst[g + 2] * kst[g + 3] : 0.0;
+        sc[g] = (T)gend[g];
+        sc[8 + g] = (T)((g >= 1) ? gend[g] * gend[g - 1] : 0.0);
+        sc[16 + g] = (T)((g >= 3) ? gend[g] * gend[g - 1] * gend[g - 2] * gend[g - 3] : 0.0);
+        sc[24 + g] = (T)kst[g];
+        sc[32 + g] = (T)((g <= 6) ? kst[g] * kst[g + 1] : 0.0);
+        sc[40 + g] = (T)((g <= 4) ? kst[g] * kst[g + 1] * kst[g + 2] * kst[g + 3] : 0.0);
     }
-    for (int j = 0; j < n; ++j) dst[fo_ib(L) + j] = ib[j];
+    for (int j = 0; j < n; ++j) dst[fo_ib(L) + j] = (T)ib[j];
 }
 
 // (elambdazb, alphaz, betaz) of every slot in the segment-interleaved layout.
+template <typename T>
 __global__ void k_pack_warp_coef(const double *__restrict__ elz, const double *__restrict__ alphar,
-                                 const double *__restrict__ betar, double *__restrict__ out, int N, int numr,
-                                 int nr) {
+                                 const double *__restrict__ betar, T *__restrict__ out, int N, int numr, int nr) {
     const int s = blockIdx.x;
     const int LR = nr / 8;
-    double *o = out + (size_t)s * 24 * LR;
+    T *o = out + (size_t)s * 24 * LR;
     for (int j = threadIdx.x; j < nr; j += blockDim.x) {
         const int g = j / LR, i = j % LR;
-        o[((i / 2) * 8 + g) * 2 + (i & 1)] = elz[(size_t)s * numr + j + 1];
-        o[8 * LR + (i * 8 + g) * 2] = alphar[j + 1];
-        o[8 * LR + (i * 8 + g) * 2 + 1] = betar[j + 1];
+        o[((i / 2) * 8 + g) * 2 + (i & 1)] = (T)elz[(size_t)s * numr + j + 1];
+        o[8 * LR + (i * 8 + g) * 2] = (T)alphar[j + 1];
+        o[8 * LR + (i * 8 + g) * 2 + 1] = (T)betar[j + 1];
     }
 }
 
@@ -524,6 +843,10 @@ const void *warp_kernel() {
 const void *warp_kernel_for(int shape) {
     return shape == 1 ? warp_kernel<3, 4>() : warp_kernel<2, 2>();
 }
+
+const void *warp_defect_kernel() { return (const void *)k_adi_warp_defect<3, 4>; }
+
+int warp_defect_smem() { return (int)sizeof(float) * WSF<3, 4>::TOTAL; }
 
 int warp_smem(int shape) {
     return shape == 1 ? (int)sizeof(double) * WS<3, 4>::TOTAL : (int)sizeof(double) * WS<2, 2>::TOTAL;
@@ -558,21 +881,76 @@ int warp_configure(bph_ctx *c) {
     e = cudaMalloc((void **)&c->d_warp_coef, sizeof(double) * coef);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(warp coefficients)");
     c->bytes += sizeof(double) * coef;
-    k_pack_warp_coef<<<c->N, 128, 0, c->stream>>>(c->d_elz, c->d_alphar, c->d_betar, c->d_warp_coef, c->N,
-                                                    c->g.numr, c->nr);
+    k_pack_warp_coef<double><<<c->N, 128, 0, c->stream>>>(c->d_elz, c->d_alphar, c->d_betar, c->d_warp_coef, c->N,
+                                                            c->g.numr, c->nr);
     ++c->launches;
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "k_pack_warp_coef");
     c->adi_warp = shape;
     c->adi_warp_smem = smem;
+    // FP32 refinement form of the same kernel (128 x 96 interiors)
+    c->mixed_warp = 0;
+    if (shape == 1 && warp_defect_smem() <= dev_max) {
+        const int sm32 = warp_defect_smem();
+        e = raise_smem_limit(warp_defect_kernel(), sm32);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(warp_defect_kernel(), cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        int per_sm = 0;
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, warp_defect_kernel(), kWThreads, sm32);
+        if (e != cudaSuccess) return cuda_fail(e, "k_adi_warp_defect attributes");
+        e = cudaMalloc((void **)&c->d_warp_coef32, sizeof(float) * coef);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(warp coefficients, float)");
+        c->bytes += sizeof(float) * coef;
+        k_pack_warp_coef<float><<<c->N, 128, 0, c->stream>>>(c->d_elz, c->d_alphar, c->d_betar, c->d_warp_coef32, c->N,
+                                                               c->g.numr, c->nr);
+        ++c->launches;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "k_pack_warp_coef<float>");
+        c->mixed_warp = 1;
+        c->mixed_smem_kind[BPH_MIXED_ADI_WARP] = sm32;
+        c->mixed_per_sm_kind[BPH_MIXED_ADI_WARP] = per_sm;
+    }
     return BPH_OK;
+}
+
+cudaError_t launch_defect_warp(bph_ctx *c, const Schedule &s, double *P, const double *R, int nrows,
+                               const int *inst_map, double *norms) {
+    if (!c->mixed_warp || !s.d_warp_rad32 || !norms) return cudaErrorNotSupported;
+    WarpDefArgs a;
+    a.P = P;
+    a.R = R;
+    a.rad = s.d_warp_rad32;
+    a.ver = s.d_warp_ver32;
+    a.coef = c->d_warp_coef32;
+    a.dt = s.d_dt;
+    a.brb = c->d_brb;
+    a.alphar = c->d_alphar;
+    a.betar = c->d_betar;
+    a.bzb = c->d_bzb;
+    a.norms = norms;
+    a.inst_map = inst_map;
+    a.N = c->N;
+    a.numr = c->g.numr;
+    a.numz = c->g.numz;
+    a.isym = c->g.isym;
+    a.nsteps = s.nsteps;
+    a.gamma = c->gamma;
+    ++c->launches;
+    void *args[] = {&a};
+    return cudaLaunchKernel(warp_defect_kernel(), dim3((unsigned)(c->N * nrows)), dim3(kWThreads), args,
+                            (size_t)warp_defect_smem(), c->stream);
 }
 
 cudaError_t launch_pack_warp(bph_ctx *c, Schedule &s) {
     const long long n = (long long)s.nsteps * c->N + s.nsteps;
-    k_pack_warp<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(s.d_rad, s.d_ver, s.d_warp_rad, s.d_warp_ver,
-                                                                    s.nsteps, c->N, c->nr, c->nz);
+    k_pack_warp<double><<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(s.d_rad, s.d_ver, s.d_warp_rad,
+                                                                            s.d_warp_ver, s.nsteps, c->N, c->nr, c->nz);
     ++c->launches;
+    if (c->mixed_warp) {
+        k_pack_warp<float><<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(s.d_rad, s.d_ver, s.d_warp_rad32,
+                                                                               s.d_warp_ver32, s.nsteps, c->N, c->nr,
+                                                                               c->nz);
+        ++c->launches;
+    }
     return cudaGetLastError();
 }
 

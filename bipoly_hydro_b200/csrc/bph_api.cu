@@ -149,6 +149,8 @@ void free_schedule(bph_ctx *c, Schedule &s) {
     }
     dev_free(s.d_warp_rad);
     dev_free(s.d_warp_ver);
+    dev_free(s.d_warp_rad32);
+    dev_free(s.d_warp_ver32);
     free(s.h_dt);
     s = Schedule();
     (void)c;
@@ -192,6 +194,10 @@ int get_schedule(bph_ctx *c, int nsteps, Schedule **out) {
     if (c->adi_warp) {
         if ((rc = dev_alloc(c, &s.d_warp_rad, (size_t)nsteps * c->N * warp_block_doubles(c->nr)))) return rc;
         if ((rc = dev_alloc(c, &s.d_warp_ver, (size_t)nsteps * warp_block_doubles(c->nz)))) return rc;
+        if (c->mixed_warp) {
+            if ((rc = dev_alloc(c, &s.d_warp_rad32, (size_t)nsteps * c->N * warp_block_doubles(c->nr)))) return rc;
+            if ((rc = dev_alloc(c, &s.d_warp_ver32, (size_t)nsteps * warp_block_doubles(c->nz)))) return rc;
+        }
         BPH_CUDA(launch_pack_warp(c, s));
     }
     BPH_CUDA(cudaStreamSynchronize(c->stream));
@@ -239,8 +245,9 @@ int upload(bph_ctx *c, void *dst, const void *src, size_t bytes) {
 // Times each fitting refinement ADI kernel (one 5-step cycle over the
 // zeroed slot array: r = 0, so the state stays zero) and keeps the faster.
 int autotune_mixed(bph_ctx *c) {
+    const int kinds[3] = {BPH_MIXED_ADI_FORWARD, BPH_MIXED_ADI_INCREMENT, BPH_MIXED_ADI_WARP};
     int avail = 0;
-    for (int k = 1; k <= 2; ++k) avail += c->mixed_smem_kind[k] ? 1 : 0;
+    for (int k : kinds) avail += c->mixed_smem_kind[k] ? 1 : 0;
     if (avail < 2) return BPH_OK;
     Schedule *s;
     int rc;
@@ -252,7 +259,10 @@ int autotune_mixed(bph_ctx *c) {
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
     int best = c->mixed_kind;
     float best_ms = 0.f;
-    for (int k = 1; k <= 2 && e == cudaSuccess; ++k) {
+    bool first = true;
+    for (int k : kinds) {
+        if (e != cudaSuccess) break;
+        if (!c->mixed_smem_kind[k]) continue;
         select_mixed_kind(c, k);
         e = launch_adi_defect(c, *s);
         if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
@@ -263,9 +273,10 @@ int autotune_mixed(bph_ctx *c) {
         if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
         if (e != cudaSuccess) break;
         c->mixed_tuned_us[k] = 1e3f * ms / 3.f;
-        if (k == 1 || ms < best_ms) {
+        if (first || ms < best_ms) {
             best = k;
             best_ms = ms;
+            first = false;
         }
     }
     if (e0) cudaEventDestroy(e0);
@@ -392,6 +403,7 @@ int setup_impl(bph_ctx *c) {
         BPH_CUDA(cudaStreamCreateWithPriority(&c->side_stream, cudaStreamNonBlocking, least));
         BPH_CUDA(cudaEventCreateWithFlags(&c->ev_fft, cudaEventDisableTiming));
         BPH_CUDA(cudaEventCreateWithFlags(&c->ev_free, cudaEventDisableTiming));
+        BPH_CUDA(cudaEventCreateWithFlags(&c->ev_contract, cudaEventDisableTiming));
         const char *cg = std::getenv("BPH_CONV_GRAPH");
         c->conv_graph = !(cg && cg[0] == '0');
         const char *ov = std::getenv("BPH_OVERLAP");
@@ -404,6 +416,16 @@ int setup_impl(bph_ctx *c) {
     if ((rc = warp_configure(c))) return rc;
     if ((rc = contract_configure(c))) return rc;
     if ((rc = noalloc_setup(c))) return rc;
+    {
+        // SM partitions for the overlapped solve: BPH_GREEN=1 turns them on,
+        // BPH_GREEN_SMS sets the contraction's share (default 72 of 148)
+        const char *gr = std::getenv("BPH_GREEN");
+        if (gr && gr[0] == '1') {
+            const char *gs = std::getenv("BPH_GREEN_SMS");
+            const int sms = gs ? std::atoi(gs) : 72;
+            if ((rc = green_setup(c, sms > 0 ? sms : 72))) return rc;
+        }
+    }
     {
         const size_t groups = (size_t)(c->nb + 7) / 8;
         if ((rc = dev_alloc(c, &c->d_ccnt, (size_t)g.mmax * groups))) return rc;
@@ -444,10 +466,39 @@ struct PdlOff {
 // stream from the end of the forward FFT, taking SMs as the contraction
 // (HBM-bound, main stream) drains; the dependent slots follow the
 // contraction; the inverse FFT joins both.
+// Launches of its scope go to stream st (the launch wrappers use c->stream).
+struct StreamSwap {
+    bph_ctx *c;
+    cudaStream_t keep;
+    StreamSwap(bph_ctx *cc, cudaStream_t st) : c(cc), keep(cc->stream) { c->stream = st; }
+    ~StreamSwap() { c->stream = keep; }
+};
+
 int solve_device(bph_ctx *c, const double *d_rho, double *d_pot, const Schedule &s, bool cold,
                  double *d_phieff = nullptr, double omega = 0.0) {
     BPH_CUDA(launch_fft_fwd_rho(c, d_rho));
-    if (c->overlap && c->adi_seg && c->nfree > 0 && c->nfree < c->N) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (c->green) BPH_CUDA(cudaStreamIsCapturing(c->stream, &cap));
+    if (c->green && cap == cudaStreamCaptureStatusNone && c->overlap && c->adi_seg && c->nfree > 0 &&
+        c->nfree < c->N) {
+        // contraction on partition 0, free-slot ADI on partition 1, both from the forward FFT
+        BPH_CUDA(cudaEventRecord(c->ev_fft, c->stream));
+        {
+            PdlOff off(c);
+            StreamSwap sw(c, c->green_stream[0]);
+            BPH_CUDA(cudaStreamWaitEvent(c->stream, c->ev_fft, 0));
+            BPH_CUDA(launch_green_contract(c));  // also writes the Dirichlet slots
+            BPH_CUDA(cudaEventRecord(c->ev_contract, c->stream));
+        }
+        BPH_CUDA(cudaStreamWaitEvent(c->green_stream[1], c->ev_fft, 0));
+        BPH_CUDA(launch_adi_slots(c, s, cold, c->d_slot_map, c->nfree, c->green_stream[1], false));
+        BPH_CUDA(cudaEventRecord(c->ev_free, c->green_stream[1]));
+        BPH_CUDA(cudaStreamWaitEvent(c->stream, c->ev_contract, 0));
+        BPH_CUDA(launch_adi_slots(c, s, cold, c->d_slot_map + c->nfree, c->N - c->nfree, c->stream, false));
+        BPH_CUDA(cudaStreamWaitEvent(c->stream, c->ev_free, 0));
+        PdlOff off(c);
+        BPH_CUDA(launch_fft_inv(c, d_pot, d_phieff, omega));
+    } else if (c->overlap && c->adi_seg && c->nfree > 0 && c->nfree < c->N) {
         BPH_CUDA(cudaEventRecord(c->ev_fft, c->stream));
         BPH_CUDA(cudaStreamWaitEvent(c->side_stream, c->ev_fft, 0));
         BPH_CUDA(launch_adi_slots(c, s, cold, c->d_slot_map, c->nfree, c->side_stream, false));
@@ -567,6 +618,7 @@ int bph_destroy(bph_ctx_t *c) {
     conv_graphs_free(c);
     dev_free(c->d_work32);
     dev_free(c->d_warp_coef);
+    dev_free(c->d_warp_coef32);
     dev_free(c->d_scf);
     if (c->side_stream) {
         cudaStreamSynchronize(c->side_stream);
@@ -574,6 +626,8 @@ int bph_destroy(bph_ctx_t *c) {
     }
     if (c->ev_fft) cudaEventDestroy(c->ev_fft);
     if (c->ev_free) cudaEventDestroy(c->ev_free);
+    if (c->ev_contract) cudaEventDestroy(c->ev_contract);
+    green_free(c);
     if (c->d_slot_map) cudaFree(c->d_slot_map);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
@@ -937,6 +991,8 @@ long long bph_info(const bph_ctx_t *c, int what) {
                                : c->adi_seg ? BPH_ADI_KERNEL_SEGMENTED
                                             : c->adi_smem ? BPH_ADI_KERNEL_ONCHIP : BPH_ADI_KERNEL_GRID_WIDE;
         case BPH_INFO_ADI_WARP_SMEM: return c->adi_warp_smem;
+        case BPH_INFO_MIXED_WARP_NS: return (long long)(1e3f * c->mixed_tuned_us[BPH_MIXED_ADI_WARP]);
+        case BPH_INFO_GREEN_SMS: return c->green ? c->green_sms[0] : 0;
         default: return -1;
     }
 }
@@ -950,7 +1006,8 @@ int bph_configure(bph_ctx_t *c, int key, int value) {
     }
     BPH_DEVICE_SCOPE(c);
     if (value == BPH_MIXED_ADI_AUTO) return autotune_mixed(c);
-    if (value != BPH_MIXED_ADI_FORWARD && value != BPH_MIXED_ADI_INCREMENT && value != BPH_MIXED_ADI_GLOBAL) {
+    if (value != BPH_MIXED_ADI_FORWARD && value != BPH_MIXED_ADI_INCREMENT && value != BPH_MIXED_ADI_GLOBAL &&
+        value != BPH_MIXED_ADI_WARP) {
         set_error("unknown refinement ADI kind %d", value);
         return BPH_ERR_INVALID;
     }

@@ -81,6 +81,8 @@ struct Schedule {
     // radial [nsteps][N][40 nr/8 + 48], vertical [nsteps][40 nz/8 + 48]
     double *d_warp_rad = nullptr;
     double *d_warp_ver = nullptr;
+    float *d_warp_rad32 = nullptr;  // the same blocks in float (warp-cooperative refinement kernel)
+    float *d_warp_ver32 = nullptr;
 };
 
 // Converged-loop state on the device (bph_converge.cu).
@@ -151,9 +153,9 @@ struct bph_ctx {
     int adi_mixed_smem = 0;      // dynamic shared bytes of the one in use (0: mixed form unavailable)
     int adi_mixed_per_sm = 0;    // its resident CTAs per SM
     int mixed_kind = 0;          // refinement ADI in use: BPH_MIXED_ADI_FORWARD or _INCREMENT
-    int mixed_smem_kind[4] = {0, 0, 0, 0};    // per kind: dynamic shared bytes (0: does not fit)
-    int mixed_per_sm_kind[4] = {0, 0, 0, 0};  // per kind: resident CTAs per SM
-    float mixed_tuned_us[4] = {0.f, 0.f, 0.f, 0.f};  // per kind: setup-time measurement (0: not timed)
+    int mixed_smem_kind[5] = {0, 0, 0, 0, 0};    // per kind: dynamic shared bytes (0: does not fit)
+    int mixed_per_sm_kind[5] = {0, 0, 0, 0, 0};  // per kind: resident CTAs per SM
+    float mixed_tuned_us[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // per kind: setup-time measurement (0: not timed)
     float *d_work32 = nullptr;                // global-memory refinement kernels: [4][N][np] (lazy)
     int adi_threads = 256;
     int fft_smem_fwd = 0, fft_smem_inv = 0;
@@ -169,10 +171,18 @@ struct bph_ctx {
     int nfree = 0;                     // slots without boundary data
     int *d_slot_map = nullptr;         // [N]: the nfree free slots, then the dependent ones
     cudaStream_t side_stream = nullptr;
-    cudaEvent_t ev_fft = nullptr, ev_free = nullptr;
+    cudaEvent_t ev_fft = nullptr, ev_free = nullptr, ev_contract = nullptr;
+    // SM partitions (green contexts, bph_green.cu): [0] the contraction's,
+    // [1] the free-slot ADI's; used by the overlapped solve when set
+    bool green = false;
+    void *green_ctx[2] = {nullptr, nullptr};
+    cudaStream_t green_stream[2] = {nullptr, nullptr};
+    int green_sms[2] = {0, 0};
     int adi_warp = 0;                  // warp-cooperative FP64 ADI shape (0: not used; bph_adi_warp.cu)
     int adi_warp_smem = 0;             // its dynamic shared bytes
     double *d_warp_coef = nullptr;     // its per-slot (elambdazb, alphaz, betaz) blocks
+    int mixed_warp = 0;                // FP32 warp-cooperative refinement kernel available
+    float *d_warp_coef32 = nullptr;    // its coefficient blocks
     double *d_scf = nullptr;           // SCF-step mass partials and scale (bph_scf.cu)
     void *noalloc_scratch = nullptr;   // device address of the allocation-free contraction's scratch array
     long long launches = 0;
@@ -325,6 +335,11 @@ int contract_configure(bph_ctx *c);
 // launch_adi_warp runs nsteps_run steps of nslots * nrows slots (block row
 // r solves instance inst_map[r], slot slot_map[b] of the row).
 int warp_configure(bph_ctx *c);
+// SM partitions for the overlapped solve (bph_green.cu): contract_sms SMs
+// for the contraction, the rest for the free-slot ADI; leaves c->green
+// false when the driver offers no partitions.
+int green_setup(bph_ctx *c, int contract_sms);
+void green_free(bph_ctx *c);
 // SCF-like density update and renormalisation in place (bph_scf.cu);
 // d_part: scf_scratch_doubles() of scratch (partials, then scale and mass).
 cudaError_t launch_scf_update(bph_ctx *c, double *d_rho, double eps, double mass, unsigned long long seed,
@@ -332,6 +347,11 @@ cudaError_t launch_scf_update(bph_ctx *c, double *d_rho, double eps, double mass
 size_t scf_scratch_doubles();
 size_t warp_block_doubles(int n);
 cudaError_t launch_pack_warp(bph_ctx *c, Schedule &s);
+// One FP32 refinement cycle of the warp-cooperative kind on nrows instance
+// rows of the slot arrays P/R (row r: instance inst_map[r]); per (instance,
+// slot) norms into norms[2 (i N + s) + 0/1].
+cudaError_t launch_defect_warp(bph_ctx *c, const Schedule &s, double *P, const double *R, int nrows,
+                               const int *inst_map, double *norms);
 cudaError_t launch_adi_warp(bph_ctx *c, const Schedule &s, int step0, int nsteps_run, bool cold, double *P,
                             const double *R, int nrows, const int *inst_map, const int *slot_map, int nslots,
                             double *norms, cudaStream_t st, bool pdl);

@@ -59,7 +59,7 @@ EXPORTED_SYMBOLS = (
 
 #: bph_configure keys and values.
 CFG_MIXED_ADI = 0
-MIXED_ADI_AUTO, MIXED_ADI_FORWARD, MIXED_ADI_INCREMENT = 0, 1, 2
+MIXED_ADI_AUTO, MIXED_ADI_FORWARD, MIXED_ADI_INCREMENT, MIXED_ADI_GLOBAL, MIXED_ADI_WARP = 0, 1, 2, 3, 4
 
 #: bph_info(BPH_INFO_ADI_KERNEL) values.
 ADI_KERNEL_WARP, ADI_KERNEL_SEGMENTED, ADI_KERNEL_ONCHIP, ADI_KERNEL_GRID_WIDE = 1, 2, 3, 4
@@ -393,7 +393,7 @@ class PotentialSolver:
         """Launch-configuration facts (bph_info)."""
         names = ("adi_threads", "adi_smem", "mixed_threads", "mixed_smem", "mixed_ctas_per_sm", "contract_split",
                  "mixed_kind", "mixed_forward_ns", "mixed_increment_ns", "adi_prefetch", "adi_kernel",
-                 "adi_warp_smem")
+                 "adi_warp_smem", "mixed_warp_ns", "green_sms")
         return {n: int(self._lib.bph_info(self._h, i)) for i, n in enumerate(names)}
 
     def set_mixed_adi(self, kind: int) -> None:

@@ -348,6 +348,8 @@ int bph_green_contract_noalloc(bph_ctx_t *ctx, const double *d_mom, double *d_S)
 #define BPH_INFO_ADI_PREFETCH 9       /* bulk-copy factor prefetch: bit 0 FP64 ADI, bit 1 FP32 refinement ADI */
 #define BPH_INFO_ADI_KERNEL 10        /* FP64 drop-in ADI kernel in use (BPH_ADI_KERNEL_*) */
 #define BPH_INFO_ADI_WARP_SMEM 11     /* dynamic shared bytes of the warp-cooperative kernel (0: not used) */
+#define BPH_INFO_MIXED_WARP_NS 12     /* setup-time duration of a 5-step warp-cooperative refinement launch, ns */
+#define BPH_INFO_GREEN_SMS 13         /* SMs of the contraction's partition in the overlapped solve (0: no partitions) */
 #define BPH_ADI_KERNEL_WARP 1         /* warp-cooperative line solves, shuffle carries (128x96, 64x64 interiors) */
 #define BPH_ADI_KERNEL_SEGMENTED 2    /* CTA-wide segmented line solves (other grids whose slot fits on chip) */
 #define BPH_ADI_KERNEL_ONCHIP 3       /* one thread per line, slot on chip */
@@ -358,7 +360,7 @@ long long bph_info(const bph_ctx_t *ctx, int what);
  *
  * BPH_CFG_MIXED_ADI selects the FP32 ADI kernel of the mixed-precision
  * refinement (bph_solve_converged_mixed):
- *   BPH_MIXED_ADI_AUTO       time both kernels on this grid and keep the faster
+ *   BPH_MIXED_ADI_AUTO       time the on-chip kernels that fit this grid and keep the fastest
  *                            (what bph_setup does unless the environment sets
  *                            BPH_AUTOTUNE=0, which keeps the forwarding form);
  *   BPH_MIXED_ADI_FORWARD    helmadi's right-hand-side form in FP32, the next
@@ -378,6 +380,9 @@ long long bph_info(const bph_ctx_t *ctx, int what);
 /* the forwarding form with its slot in global memory: any grid size, the
  * choice when neither on-chip kernel fits (e.g. 258x194x512) */
 #define BPH_MIXED_ADI_GLOBAL 3
+/* the forwarding form with warp-cooperative line solves (shuffle carries,
+ * two CTAs per SM), for 128 x 96 interiors (130x98 grids) */
+#define BPH_MIXED_ADI_WARP 4
 int bph_configure(bph_ctx_t *ctx, int key, int value);
 
 /* Number of kernels this context has launched so far. */

@@ -152,3 +152,54 @@ def test_both_on_chip_adi_kernels_match_oracle(oracle_130, pair_rho, bph, monkey
     pg, info = g.solve_converged(pair_rho, 10, True, 1e-11, 60)
     assert info.cycles == co and rel_l2(pg, po) <= POT_TOL
     g.close()
+
+
+def test_warp_refinement_kernel_matches_oracle(oracle_130, pair_rho, bph):
+    """The FP32 warp-cooperative refinement kernel (mixed kind 4): cold and
+    warm converged mixed solves within 1e-9 of the oracle's converged FP64
+    potential, single and batched."""
+    from bipoly_hydro_b200 import fields
+
+    g = bph.PotentialSolver(*GRID_130)
+    g.set_mixed_adi(bph.solver.MIXED_ADI_WARP)
+    po, _, _ = oracle_130.solve_converged(pair_rho, 10, True, 1e-12, 60)
+    pm, im = g.solve_converged_mixed(pair_rho, 10, True, 1e-12, 60)
+    assert rel_l2(pm, po) <= 1e-9, (rel_l2(pm, po), im.cycles)
+    rho2 = fields.rotate(pair_rho)
+    po2, _, _ = oracle_130.solve_converged(rho2, 10, False, 1e-12, 60)
+    pm2, im2 = g.solve_converged_mixed(rho2, 10, False, 1e-12, 60)
+    assert rel_l2(pm2, po2) <= 1e-9, (rel_l2(pm2, po2), im2.cycles)
+    batch = bph.Batch(g, capacity=3)
+    rhos = [fields.rotate(pair_rho, i) for i in range(3)]
+    pots, info = batch.solve_converged(rhos, 10, True, 1e-12, 60, mixed=True)
+    ref = oracle_130.solve_converged(rhos[2], 10, True, 1e-12, 60)[0]
+    assert rel_l2(pots[2], ref) <= 1e-9, rel_l2(pots[2], ref)
+    batch.close()
+    g.close()
+
+
+def test_sm_partitioned_solve_matches_oracle(oracle_130, pair_rho, bph, monkeypatch):
+    """BPH_GREEN=1: the overlapped solve with the contraction and the
+    free-slot ADI on disjoint SM partitions (green contexts) gives the same
+    potentials: cold and warm solves at the FP64 bar, device arrays."""
+    import torch
+
+    from bipoly_hydro_b200 import fields
+
+    monkeypatch.setenv("BPH_GREEN", "1")
+    monkeypatch.setenv("BPH_GREEN_SMS", "64")
+    g = bph.PotentialSolver(*GRID_130)
+    if g.info()["green_sms"] == 0:
+        g.close()
+        pytest.skip("the driver offers no SM partitions on this device")
+    assert g.info()["green_sms"] >= 64
+    rhos = [fields.rotate(pair_rho, i) for i in range(3)]
+    d_rho = [torch.from_numpy(np.ascontiguousarray(r.ravel(order="F"))).cuda() for r in rhos]
+    d_pot = [torch.empty_like(d_rho[0]) for _ in rhos]
+    for i in range(3):
+        g.potential_solver_device(d_rho[i], d_pot[i], 0 if i == 0 else i + 1)
+    g.synchronize()
+    for i in range(3):
+        po = oracle_130.potential_solver(rhos[i], 0 if i == 0 else i + 1)
+        assert rel_l2(d_pot[i].cpu().numpy().reshape(rhos[i].shape, order="F"), po) <= POT_TOL, i
+    g.close()

@@ -243,7 +243,7 @@ def test_mixed_converged_production_grid(bph, nsteps):
     g.close()
 
 
-@pytest.mark.parametrize("kind", [1, 2], ids=["forward", "increment"])
+@pytest.mark.parametrize("kind", [1, 2, 4], ids=["forward", "increment", "warp"])
 def test_mixed_warm_sequence_stays_converged(bph, kind):
     """A run of warm mixed solves (time-step sequence of a rotating pair at
     130x98x256, update tolerance 1e-11) keeps its FP64 residual at the FP64
@@ -304,18 +304,22 @@ def test_warm_start_from_checkpointed_potential(oracle_mod, bph):
 
 
 def test_mixed_adi_autotune_and_selection(bph):
-    """Setup times both refinement ADI kernels at 130x98x256 and keeps the
-    faster; an explicit choice sticks; an unknown kind is rejected."""
+    """Setup times the on-chip refinement ADI kernels at 130x98x256 (forwarding,
+    increment, warp-cooperative) and keeps the fastest; an explicit choice
+    sticks; an unknown kind is rejected."""
     g = bph.PotentialSolver(130, 98, 256, 1.0 / 126.0, 2, 30)
     info = g.info()
-    assert info["mixed_kind"] in (1, 2)
-    fwd, inc = info["mixed_forward_ns"], info["mixed_increment_ns"]
-    assert fwd > 0 and inc > 0
-    assert info["mixed_kind"] == (1 if fwd <= inc else 2)
+    assert info["mixed_kind"] in (1, 2, 4)
+    times = {1: info["mixed_forward_ns"], 2: info["mixed_increment_ns"], 4: info["mixed_warp_ns"]}
+    assert all(t > 0 for t in times.values()), times
+    assert info["mixed_kind"] == min(times, key=times.get)
     g.set_mixed_adi(2)
     assert g.info()["mixed_kind"] == 2
     with pytest.raises(bph.BphError):
         g.set_mixed_adi(7)
+    g.set_mixed_adi(4)
+    assert g.info()["mixed_kind"] == 4
+    g.set_mixed_adi(2)
     assert g.info()["mixed_kind"] == 2
     g.close()
 
