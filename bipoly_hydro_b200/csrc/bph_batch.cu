@@ -211,9 +211,6 @@ k_contract_dmma(const double *__restrict__ G, const double *__restrict__ mom, lo
     const double *ga = G + ((long long)m * nb + (ra < nb ? ra : 0)) * np;
     const double *gb = G + ((long long)m * nb + (rb < nb ? rb : 0)) * np;
     const bool live = b0 < nb;
-    // moment column c0 + 8 j + grp of this thread's B fragments (columns beyond ncol are zero)
-    const double *mcol = mom + m * mstride + (long long)(c0 + grp) * np;
-    const int ncols_here = ncol - c0 - grp;  // tile j is live when 8 j < ncols_here
     const long long nk = (np + 7) / 8;  // 8-zone steps (the last one may be partial)
     const long long per = (nk + nsplit - 1) / nsplit;
     const long long k_begin = split * per, k_end = min(nk, k_begin + per);
@@ -235,27 +232,72 @@ k_contract_dmma(const double *__restrict__ G, const double *__restrict__ mom, lo
     double ab[kDmmaStages][4];
 #pragma unroll
     for (int st = 0; st < kDmmaStages; ++st) load_a(k_begin + st, ab[st]);
+    // Moment columns staged per chunk of kDmmaStages steps (32 zones) in
+    // shared memory by cp.async, double-buffered: Ms[buf][column][zone],
+    // rows padded to 36 doubles (the B-fragment reads of a half-warp hit 16
+    // different banks); columns beyond ncol and zones beyond np read zero.
+    constexpr int NCP = 8 * NT;
+    constexpr int KC = 8 * kDmmaStages, KS = KC + 4;
+    __shared__ __align__(16) double Ms[2][NCP][KS];
+    const double *mbase = mom + m * mstride;
+    const long long nchunk = (k_end - k_begin + kDmmaStages - 1) / kDmmaStages;
+    const bool even_np = (np & 1) == 0;
+    auto issue_chunk = [&](long long ch, int buf) {
+        const long long zc = 8 * (k_begin + ch * kDmmaStages);
+        if (even_np) {
+            for (int q = threadIdx.x; q < NCP * (KC / 2); q += kDmmaWarps * 32) {
+                const int cc = q / (KC / 2), zz = 2 * (q % (KC / 2));
+                const int col = c0 + cc;
+                const long long z = zc + zz;
+                const int bytes = (col < ncol && z < np) ? 16 : 0;
+                const double *src = (bytes ? mbase + (long long)col * np + z : mbase);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                                 (uint32_t)__cvta_generic_to_shared(&Ms[buf][cc][zz])),
+                             "l"(src), "r"(bytes)
+                             : "memory");
+            }
+        } else {
+            for (int q = threadIdx.x; q < NCP * KC; q += kDmmaWarps * 32) {
+                const int cc = q / KC, zz = q % KC;
+                const int col = c0 + cc;
+                const long long z = zc + zz;
+                const int bytes = (col < ncol && z < np) ? 8 : 0;
+                const double *src = (bytes ? mbase + (long long)col * np + z : mbase);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(
+                                 (uint32_t)__cvta_generic_to_shared(&Ms[buf][cc][zz])),
+                             "l"(src), "r"(bytes)
+                             : "memory");
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
     pdl_wait();
-    for (long long k = k_begin; k < k_end; k += kDmmaStages) {
+    if (nchunk > 0) issue_chunk(0, 0);
+    for (long long ch = 0; ch < nchunk; ++ch) {
+        const int buf = (int)(ch & 1);
+        if (ch + 1 < nchunk) {
+            issue_chunk(ch + 1, buf ^ 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        __syncthreads();
 #pragma unroll
         for (int st = 0; st < kDmmaStages; ++st) {
-            const long long kk = k + st;
+            const long long kk = k_begin + ch * kDmmaStages + st;
             if (kk < k_end) {
-                const long long z0 = 8 * kk + t, z1 = z0 + 4;
                 double a[4] = {ab[st][0], ab[st][1], ab[st][2], ab[st][3]};
                 load_a(kk + kDmmaStages, ab[st]);  // the step kDmmaStages ahead
 #pragma unroll
                 for (int j = 0; j < NT; ++j) {
-                    const bool cl = 8 * j < ncols_here;
-                    const double bv0 = (cl && z0 < np) ? __ldg(mcol + 8LL * j * np + z0) : 0.0;
-                    const double bv1 = (cl && z1 < np) ? __ldg(mcol + 8LL * j * np + z1) : 0.0;
-                    dmma16x8x8(acc[j], a, bv0, bv1);
+                    const double *mj = &Ms[buf][8 * j + grp][8 * st + t];
+                    dmma16x8x8(acc[j], a, mj[0], mj[4]);
                 }
             }
         }
+        __syncthreads();  // the buffer is refilled two chunks later
     }
     pdl_trigger();
-    constexpr int NCP = 8 * NT;  // columns of a partial-sum row
     const int rows0 = blockIdx.x * kDmmaWarps * 16;
     const int nrows = min(kDmmaWarps * 16, nb - rows0);
     auto put = [&](double *dst, long long rstride, long long cstr) {
