@@ -63,6 +63,7 @@ struct orc_ctx {
     double az, cz;
     double *green;                                     /* [mmax][nb][nr*nz] */
     double *S;                                         /* [mmax][nb][2] */
+    const double *S_override;                          /* test hook: boundary moments to use instead */
     double *potp, *rhop;                               /* [numphi][numz][numr] */
 };
 
@@ -624,6 +625,7 @@ static void bessel(orc_ctx *c, const double *rho) {
         }
     }
     free(tmp);
+    if (c->S_override) memcpy(c->S, c->S_override, sizeof(double) * (size_t)mmax * nb * 2);
     /* synthesis over m (bessel.F90:399-488) */
     double *line = malloc(sizeof(double) * (size_t)N);
     /* top, K = numz */
@@ -974,6 +976,12 @@ int orc_solve_converged(orc_ctx *c, const double *rho, double *pot, int nsteps, 
     if (max_cycles < 1) max_cycles = 1;
     return solve_common(c, rho, pot, nsteps, cold, 1, tol, max_cycles, cycles_out, resid_out);
 }
+
+/* Test hook (not part of the reference algorithm): later solves use the
+ * given boundary moments S[m][b][cos|sin] in place of the contraction's,
+ * so that a test can measure how an error in S moves the potential.  NULL
+ * restores the contraction.  The array must outlive the solves. */
+void orc_set_moments_override(orc_ctx *c, const double *S) { c->S_override = S; }
 
 /* Replaces the kept potential potp (COMMON /potarrays/) with pot, as a
  * continuation restart that restored potp would. */

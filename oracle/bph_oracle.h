@@ -57,6 +57,9 @@ int orc_solve_converged(orc_ctx *c, const double *rho, double *pot, int nsteps,
 
 /* Sets the kept potential potp (warm-start state) to pot. */
 void orc_set_potential(orc_ctx *c, const double *pot);
+/* Test hook: boundary moments S[m][b][2] used by later solves instead of the
+ * contraction's (NULL: the contraction again). */
+void orc_set_moments_override(orc_ctx *c, const double *S);
 
 /* Relative residual of a physical-space potential (after a solve) in slot
  * space, the same measure orc_solve_converged uses. */

@@ -57,6 +57,7 @@ def lib():
                                           ctypes.c_int, ctypes.POINTER(ctypes.c_int), dp]
         L.orc_solve_converged.restype = ctypes.c_int
         L.orc_set_potential.argtypes = [vp, dp]
+        L.orc_set_moments_override.argtypes = [vp, ctypes.c_void_p]
         L.orc_residual.argtypes = [vp, dp, dp]
         L.orc_residual.restype = ctypes.c_double
         L.orc_num_boundary_rows.argtypes = [vp]
@@ -184,6 +185,16 @@ class Oracle:
     def set_potential(self, pot) -> None:
         p = np.asfortranarray(pot, dtype=np.float64)
         lib().orc_set_potential(self._h, _dp(p))
+
+    def set_moments_override(self, S) -> None:
+        """Test hook: later solves use these boundary moments S[m][b][2]
+        (None: the contraction's own)."""
+        if S is None:
+            self._S_keep = None
+            lib().orc_set_moments_override(self._h, None)
+            return
+        self._S_keep = np.ascontiguousarray(S, dtype=np.float64).copy()
+        lib().orc_set_moments_override(self._h, self._S_keep.ctypes.data)
 
     def residual(self, rho, pot) -> float:
         rho = self._check(rho)
