@@ -969,6 +969,8 @@ def run_gpu(args, world, rank, local):
         tuned_kind = solver.info()["mixed_kind"]
         variants = [("fp64", None), ("mixed_forward", B.solver.MIXED_ADI_FORWARD),
                     ("mixed_increment", B.solver.MIXED_ADI_INCREMENT)]
+        if solver.info()["mixed_warp_ns"] > 0:
+            variants.append(("mixed_warp", B.solver.MIXED_ADI_WARP))
         for key, kind in variants:
             if kind is not None:
                 solver.set_mixed_adi(kind)
@@ -997,8 +999,10 @@ def run_gpu(args, world, rank, local):
         solver.set_mixed_adi(tuned_kind)
         conv["nsteps_per_cycle"] = args.conv_nsteps
         conv["tol_update"] = args.conv_tol
-        conv["autotuned_kind"] = "mixed_forward" if tuned_kind == B.solver.MIXED_ADI_FORWARD else "mixed_increment"
-        best = max(conv["mixed_forward"]["solves_per_s"], conv["mixed_increment"]["solves_per_s"])
+        names = {B.solver.MIXED_ADI_FORWARD: "mixed_forward", B.solver.MIXED_ADI_INCREMENT: "mixed_increment",
+                 B.solver.MIXED_ADI_WARP: "mixed_warp"}
+        conv["autotuned_kind"] = names.get(tuned_kind, str(tuned_kind))
+        best = max(conv[k]["solves_per_s"] for k, kind in variants if kind is not None)
         conv["speedup_mixed_vs_fp64"] = best / conv["fp64"]["solves_per_s"]
         del ref_pots
 

@@ -992,7 +992,7 @@ long long bph_info(const bph_ctx_t *c, int what) {
                                             : c->adi_smem ? BPH_ADI_KERNEL_ONCHIP : BPH_ADI_KERNEL_GRID_WIDE;
         case BPH_INFO_ADI_WARP_SMEM: return c->adi_warp_smem;
         case BPH_INFO_MIXED_WARP_NS: return (long long)(1e3f * c->mixed_tuned_us[BPH_MIXED_ADI_WARP]);
-        case BPH_INFO_GREEN_SMS: return c->green ? c->green_sms[0] : 0;
+        case BPH_INFO_GREEN_SMS: return c->green ? c->green_sms[0] : -c->green_fail;
         default: return -1;
     }
 }

@@ -35,7 +35,7 @@ template <typename F>
 bool entry(const char *name, F *out) {
     void *fn = nullptr;
     cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPointByVersion(name, &fn, 12040, cudaEnableDefault, &q) != cudaSuccess ||
+    if (cudaGetDriverEntryPointByVersion(name, &fn, 12080, cudaEnableDefault, &q) != cudaSuccess ||
         q != cudaDriverEntryPointSuccess || !fn) {
         (void)cudaGetLastError();
         return false;
@@ -53,6 +53,7 @@ bool entry(const char *name, F *out) {
 // partial creation.
 int green_setup(bph_ctx *c, int contract_sms) {
     c->green = false;
+    c->green_fail = 1;  // driver entry points
     PFN_getDevResource getRes;
     PFN_split split;
     PFN_genDesc gen;
@@ -63,13 +64,17 @@ int green_setup(bph_ctx *c, int contract_sms) {
         !entry("cuGreenCtxStreamCreate", &mkstream))
         return BPH_OK;
     CUdevResource all, part[1], rest;
+    c->green_fail = 2;  // device SM resource
     if (getRes((CUdevice)c->device, &all, CU_DEV_RESOURCE_TYPE_SM) != CUDA_SUCCESS) return BPH_OK;
+    c->green_fail = 3;  // split
     unsigned int ngroups = 1;
     if (split(part, &ngroups, &all, &rest, 0, (unsigned)contract_sms) != CUDA_SUCCESS || ngroups != 1) return BPH_OK;
     if (rest.sm.smCount < 8) return BPH_OK;
     CUdevResourceDesc da, db;
+    c->green_fail = 4;  // descriptors
     if (gen(&da, &part[0], 1) != CUDA_SUCCESS || gen(&db, &rest, 1) != CUDA_SUCCESS) return BPH_OK;
     CUgreenCtx ga = nullptr, gb = nullptr;
+    c->green_fail = 5;  // green contexts
     if (create(&ga, da, (CUdevice)c->device, CU_GREEN_CTX_DEFAULT_STREAM) != CUDA_SUCCESS) return BPH_OK;
     if (create(&gb, db, (CUdevice)c->device, CU_GREEN_CTX_DEFAULT_STREAM) != CUDA_SUCCESS) {
         PFN_greenDestroy destroy;
@@ -77,6 +82,7 @@ int green_setup(bph_ctx *c, int contract_sms) {
         return BPH_OK;
     }
     CUstream sa = nullptr, sb = nullptr;
+    c->green_fail = 6;  // streams
     if (mkstream(&sa, ga, CU_STREAM_NON_BLOCKING, 0) != CUDA_SUCCESS ||
         mkstream(&sb, gb, CU_STREAM_NON_BLOCKING, 0) != CUDA_SUCCESS) {
         c->green_ctx[0] = ga;
@@ -93,6 +99,7 @@ int green_setup(bph_ctx *c, int contract_sms) {
     c->green_sms[0] = (int)part[0].sm.smCount;
     c->green_sms[1] = (int)rest.sm.smCount;
     c->green = true;
+    c->green_fail = 0;
     return BPH_OK;
 }
 

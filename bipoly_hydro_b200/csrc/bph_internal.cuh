@@ -178,6 +178,7 @@ struct bph_ctx {
     void *green_ctx[2] = {nullptr, nullptr};
     cudaStream_t green_stream[2] = {nullptr, nullptr};
     int green_sms[2] = {0, 0};
+    int green_fail = 0;  // set-up step that failed (0: none or not requested)
     int adi_warp = 0;                  // warp-cooperative FP64 ADI shape (0: not used; bph_adi_warp.cu)
     int adi_warp_smem = 0;             // its dynamic shared bytes
     double *d_warp_coef = nullptr;     // its per-slot (elambdazb, alphaz, betaz) blocks

@@ -349,7 +349,8 @@ int bph_green_contract_noalloc(bph_ctx_t *ctx, const double *d_mom, double *d_S)
 #define BPH_INFO_ADI_KERNEL 10        /* FP64 drop-in ADI kernel in use (BPH_ADI_KERNEL_*) */
 #define BPH_INFO_ADI_WARP_SMEM 11     /* dynamic shared bytes of the warp-cooperative kernel (0: not used) */
 #define BPH_INFO_MIXED_WARP_NS 12     /* setup-time duration of a 5-step warp-cooperative refinement launch, ns */
-#define BPH_INFO_GREEN_SMS 13         /* SMs of the contraction's partition in the overlapped solve (0: no partitions) */
+#define BPH_INFO_GREEN_SMS 13         /* SMs of the contraction's partition in the overlapped solve (0: not requested,
+                                         negative: the set-up step that failed) */
 #define BPH_ADI_KERNEL_WARP 1         /* warp-cooperative line solves, shuffle carries (128x96, 64x64 interiors) */
 #define BPH_ADI_KERNEL_SEGMENTED 2    /* CTA-wide segmented line solves (other grids whose slot fits on chip) */
 #define BPH_ADI_KERNEL_ONCHIP 3       /* one thread per line, slot on chip */
