@@ -742,13 +742,16 @@ def run_gpu(args, world, rank, local):
     green = None
     if rank == 0 and not args.no_green:
         green = []
-        for sms in [int(x) for x in args.green_sms.split(",") if x]:
-            os.environ["BPH_GREEN"], os.environ["BPH_GREEN_SMS"] = "1", str(sms)
+        # the serialised schedule (no side stream) first, then SM partitions
+        configs = [("serial", {"BPH_OVERLAP": "0"})] + [
+            (int(x), {"BPH_GREEN": "1", "BPH_GREEN_SMS": x}) for x in args.green_sms.split(",") if x]
+        for sms, env in configs:
+            os.environ.update(env)
             try:
                 gs = B.PotentialSolver(**GRID)
             finally:
-                os.environ.pop("BPH_GREEN", None)
-                os.environ.pop("BPH_GREEN_SMS", None)
+                for k in env:
+                    os.environ.pop(k, None)
             gs.set_stream(stream)
             got = gs.info()["green_sms"]
             gp = torch.empty_like(d_pot)
@@ -919,31 +922,51 @@ def run_gpu(args, world, rank, local):
         nb_ = max(int(x) for x in args.batch_sizes.split(",") if x)
         ins = [rhos[(7 * i) % nrot] for i in range(nb_)]
         batched_conv = {"instances": nb_, "nsteps_per_cycle": args.conv_nsteps, "tol_update": args.conv_tol}
-        ref_outs = None
-        for key, mixed in (("fp64", False), ("mixed", True)):
+
+        def measure(ns, mixed):
             bt = B.Batch(solver, nb_)
             outs = [torch.empty(ntot, dtype=torch.float64, device=dev) for _ in range(nb_)]
-            bt.solve_converged_device(ins, outs, args.conv_nsteps, True, 1e-13, 100, mixed)
+            bt.solve_converged_device(ins, outs, ns, True, 1e-13, 100, mixed)
             ts, cyc = [], []
             for k in range(4):
                 ins_k = [rhos[(7 * i + k + 1) % nrot] for i in range(nb_)]
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
-                info = bt.solve_converged_device(ins_k, outs, args.conv_nsteps, False, args.conv_tol, 100, mixed)
+                info = bt.solve_converged_device(ins_k, outs, ns, False, args.conv_tol, 100, mixed)
                 torch.cuda.synchronize()
                 ts.append(time.perf_counter() - t0)
                 cyc.append(info.cycles)
-            r = {"solves_per_s": nb_ / float(np.median(ts)), "ms_per_call": 1e3 * float(np.median(ts)),
-                 "mean_cycles": float(np.mean(cyc))}
-            if mixed:
-                r["max_rel_err_vs_fp64"] = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
-                                               for a, b in zip(outs, ref_outs))
-            else:
-                ref_outs = [o.clone() for o in outs]
-            batched_conv[key] = r
             bt.close()
-            del outs
-        batched_conv["speedup_mixed_vs_fp64"] = batched_conv["mixed"]["solves_per_s"] / batched_conv["fp64"]["solves_per_s"]
+            return ({"solves_per_s": nb_ / float(np.median(ts)), "ms_per_call": 1e3 * float(np.median(ts)),
+                     "mean_cycles": float(np.mean(cyc))}, outs)
+
+        def err_vs(outs, ref):
+            return max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) for a, b in zip(outs, ref))
+
+        r64, ref_outs = measure(args.conv_nsteps, False)
+        batched_conv["fp64"] = r64
+        rmx, outs = measure(args.conv_nsteps, True)
+        rmx["max_rel_err_vs_fp64"] = err_vs(outs, ref_outs)
+        batched_conv["mixed"] = rmx
+        batched_conv["speedup_mixed_vs_fp64"] = rmx["solves_per_s"] / r64["solves_per_s"]
+        # each form at its own best cycle length (the converged answer does not depend on it)
+        sweep = sorted(set(int(x) for x in args.conv_nsteps_sweep.split(",") if x))
+        if sweep:
+            table = {"fp64": {}, "mixed": {}}
+            for ns in sweep:
+                for key, mixed in (("fp64", False), ("mixed", True)):
+                    if ns == args.conv_nsteps:
+                        table[key][str(ns)] = batched_conv[key]
+                        continue
+                    r, outs = measure(ns, mixed)
+                    r["max_rel_err_vs_fp64"] = err_vs(outs, ref_outs)
+                    table[key][str(ns)] = r
+                    del outs
+            best = {k: max(v.items(), key=lambda kv: kv[1]["solves_per_s"]) for k, v in table.items()}
+            batched_conv["nsteps_sweep"] = table
+            batched_conv["best"] = {k: {"nsteps_per_cycle": int(ns), **r} for k, (ns, r) in best.items()}
+            batched_conv["speedup_mixed_vs_fp64_best"] = (best["mixed"][1]["solves_per_s"] /
+                                                          best["fp64"][1]["solves_per_s"])
         del ref_outs
 
     # ---- batches over a mix of grids, one plan launch ------------------
@@ -1086,6 +1109,8 @@ def main():
                     help="warm converged solves timed per form (FP64 and mixed); 0 skips")
     ap.add_argument("--conv-nsteps", type=int, default=10, help="ADI steps per refinement cycle")
     ap.add_argument("--conv-tol", type=float, default=1e-11, help="stop when |dphi|/|phi| <= tol")
+    ap.add_argument("--conv-nsteps-sweep", default="6,8,10,14",
+                    help="cycle lengths of the batched converged sweep (each form at its best; empty skips)")
     ap.add_argument("--rotations", type=int, default=0,
                     help="resident density rotations (0: numphi); small values make a small profiling case")
     args = ap.parse_args()

@@ -1460,7 +1460,7 @@ cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {
     a.ver_pk = sch.d_ver_pk[1];
     a.pkr = packed_block<float>(c->nr);
     a.pkz = packed_block<float>(c->nz);
-    if (c->mixed_kind == BPH_MIXED_ADI_WARP) return launch_defect_warp(c, sch, c->d_P, c->d_R, 1, nullptr, c->d_red);
+    if (c->mixed_kind == BPH_MIXED_ADI_WARP) return launch_defect_warp(c, sch, c->d_P, c->d_R, 1, nullptr, c->d_red, c->d_r32);
     ++c->launches;
     void *args[] = {&a};
     if (c->mixed_kind == BPH_MIXED_ADI_GLOBAL) {
@@ -1478,7 +1478,7 @@ cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {
 cudaError_t launch_defect_batch(bph_ctx *c, const Schedule &sch, double *P, const double *R, int n, const int *d_map,
                                 double *norms) {
     if (!c->adi_mixed_smem || c->mixed_kind == BPH_MIXED_ADI_GLOBAL) return cudaErrorNotSupported;
-    if (c->mixed_kind == BPH_MIXED_ADI_WARP) return launch_defect_warp(c, sch, P, R, n, d_map, norms);
+    if (c->mixed_kind == BPH_MIXED_ADI_WARP) return cudaErrorNotSupported;  // launch_defect_batch_warp
     AdiArgs a = make_args(c, sch, 0, sch.nsteps, false);
     a.P = P;
     a.R = R;

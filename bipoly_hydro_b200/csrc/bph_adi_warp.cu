@@ -536,9 +536,40 @@ struct WarpDefArgs {
     const double *alphar, *betar, *bzb;
     double *norms;         // per (instance, slot) |delta|^2, |phi|^2
     const int *inst_map;   // instance of each block row (nullptr: row)
+    const float *r32;      // FP64 residual rounded to float, [row][N][nr*nz] (k_residual32)
     int N, numr, numz, isym, nsteps;
     double gamma;
 };
+
+// FP64 residual r = -4 pi rho_hat - A phi of the current potential (its
+// Dirichlet columns enter through the stencil), rounded to float: one CTA
+// per (block row, slot), consecutive threads on consecutive zones of a row
+// (coalesced loads of the slot plane), written row-major for the refinement
+// kernel's 16-byte copies.
+__global__ void __launch_bounds__(256) k_residual32(WarpDefArgs a, int nr, int nz) {
+    const int s = blockIdx.x % a.N, row = blockIdx.x / a.N;
+    const long long blk = (long long)(a.inst_map ? a.inst_map[row] : row) * a.N + s;
+    const int numr = a.numr;
+    const double *Pg = a.P + blk * (long long)numr * a.numz;
+    const double *Rg = a.R + blk * (long long)nr * nz;
+    float *out = const_cast<float *>(a.r32) + ((long long)row * a.N + s) * (long long)nr * nz;
+    const double *brb = a.brb + (long long)s * numr;
+    const bool sym_bottom = (a.isym != 1);
+    const double gamma = a.gamma;
+    pdl_wait();
+    const long long tot = (long long)nr * nz;
+#pragma unroll 4
+    for (long long e = threadIdx.x; e < tot; e += 256) {
+        const int k = (int)(e / nr), j = (int)(e % nr);
+        const double *pc = Pg + (long long)numr * (k + 1) + 1 + j;
+        const double c = pc[0], ea = pc[1], no = pc[numr];
+        const double we = (j > 0) ? pc[-1] : 0.0;
+        const double so = (k > 0 || !sym_bottom) ? pc[-numr] : 0.0;
+        const double ar = brb[j + 1] * c + a.alphar[j + 1] * ea + a.betar[j + 1] * we;
+        const double az = a.bzb[k + 1] * c - gamma * no - gamma * so;
+        out[e] = (float)(Rg[e] - ar - az);
+    }
+}
 
 template <int NLR, int NLZ>
 __global__ void __launch_bounds__(kWThreads, 2) k_adi_warp_defect(WarpDefArgs a) {
@@ -557,50 +588,38 @@ __global__ void __launch_bounds__(kWThreads, 2) k_adi_warp_defect(WarpDefArgs a)
     const long long blk = (long long)(a.inst_map ? a.inst_map[row] : row) * a.N + s;
     const int numr = a.numr, numz = a.numz;
     double *Pg = a.P + blk * (long long)numr * numz;
-    const double *Rg = a.R + blk * (long long)NR * NZ;
     const size_t rad_step = (size_t)a.N * F::RAD;
     const float *rad_src = a.rad + (size_t)s * F::RAD;
     const double gamma = a.gamma;
     const float gf = (float)gamma;
     const bool sym_bottom = (a.isym != 1);
     const int n = a.nsteps;
-    const double *brb = a.brb + (long long)s * numr;
 
     copy_block(radb, rad_src, F::RAD, tid);
     copy_block(verb, a.ver, F::VER, tid);
     copy_block(const_cast<float *>(coefb), a.coef + (size_t)s * F::COEF, F::COEF, tid);
     cp_commit();
     pdl_wait();
-    cp_wait_all();
-    __syncthreads();
-    // FP64 residual of the current potential, 8 zones per thread in flight
+    // the float residual (k_residual32), 16-byte chunks into their swizzled places
     {
-        const float *ibr = radb + fo_ib(LR);
         constexpr int kTot = NR * NZ;
-#pragma unroll 1
-        for (int e0 = tid; e0 < kTot; e0 += kWThreads * 8) {
-            double rr[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int e = e0 + u * kWThreads;
-                const int k = e / NR, j = e % NR;
-                const double *pc = Pg + (long long)numr * (k + 1) + 1 + j;
-                const double c = pc[0], ea = pc[1], no = pc[numr];
-                const double we = (j > 0) ? pc[-1] : 0.0;
-                const double so = (k > 0 || !sym_bottom) ? pc[-numr] : 0.0;
-                const double ar = brb[j + 1] * c + a.alphar[j + 1] * ea + a.betar[j + 1] * we;
-                const double az = a.bzb[k + 1] * c - gamma * no - gamma * so;
-                rr[u] = Rg[e] - ar - az;
-            }
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int e = e0 + u * kWThreads;
-                const int k = e / NR, j = e % NR;
-                const int off = swzf<NLR, NLZ>(k, j);
-                const float r32 = (float)rr[u];
-                Rv[off] = r32;
-                W[off] = r32 * ibr[j];
-            }
+        const float *rs = a.r32 + ((long long)row * a.N + s) * (long long)kTot;
+        for (int q = tid; q < kTot / 4; q += kWThreads) {
+            const int e = 4 * q;
+            cp16(Rv + swzf<NLR, NLZ>(e / NR, e % NR), rs + e);
+        }
+        cp_commit();
+        cp_wait_all();
+        __syncthreads();
+        // first radial right-hand side: delta = 0, so r (1/bet) -- four floats of a chunk per thread
+        const float *ibr = radb + fo_ib(LR);
+        for (int q = tid; q < kTot / 4; q += kWThreads) {
+            const int e = 4 * q;
+            const int k = e / NR, j = e % NR;
+            const int off = swzf<NLR, NLZ>(k, j);
+            const float4 r = *reinterpret_cast<const float4 *>(Rv + off);
+            const float4 ib = *reinterpret_cast<const float4 *>(ibr + j);
+            *reinterpret_cast<float4 *>(W + off) = make_float4(r.x * ib.x, r.y * ib.y, r.z * ib.z, r.w * ib.w);
         }
     }
     __syncthreads();
@@ -900,6 +919,10 @@ int warp_configure(bph_ctx *c) {
         e = cudaMalloc((void **)&c->d_warp_coef32, sizeof(float) * coef);
         if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(warp coefficients, float)");
         c->bytes += sizeof(float) * coef;
+        const size_t r32 = (size_t)c->N * c->np;
+        e = cudaMalloc((void **)&c->d_r32, sizeof(float) * r32);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(rounded residual)");
+        c->bytes += sizeof(float) * r32;
         k_pack_warp_coef<float><<<c->N, 128, 0, c->stream>>>(c->d_elz, c->d_alphar, c->d_betar, c->d_warp_coef32, c->N,
                                                                c->g.numr, c->nr);
         ++c->launches;
@@ -913,8 +936,8 @@ int warp_configure(bph_ctx *c) {
 }
 
 cudaError_t launch_defect_warp(bph_ctx *c, const Schedule &s, double *P, const double *R, int nrows,
-                               const int *inst_map, double *norms) {
-    if (!c->mixed_warp || !s.d_warp_rad32 || !norms) return cudaErrorNotSupported;
+                               const int *inst_map, double *norms, float *r32) {
+    if (!c->mixed_warp || !s.d_warp_rad32 || !norms || !r32) return cudaErrorNotSupported;
     WarpDefArgs a;
     a.P = P;
     a.R = R;
@@ -928,13 +951,17 @@ cudaError_t launch_defect_warp(bph_ctx *c, const Schedule &s, double *P, const d
     a.bzb = c->d_bzb;
     a.norms = norms;
     a.inst_map = inst_map;
+    a.r32 = r32;
     a.N = c->N;
     a.numr = c->g.numr;
     a.numz = c->g.numz;
     a.isym = c->g.isym;
     a.nsteps = s.nsteps;
     a.gamma = c->gamma;
-    ++c->launches;
+    c->launches += 2;
+    k_residual32<<<(unsigned)(c->N * nrows), 256, 0, c->stream>>>(a, c->nr, c->nz);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     void *args[] = {&a};
     return cudaLaunchKernel(warp_defect_kernel(), dim3((unsigned)(c->N * nrows)), dim3(kWThreads), args,
                             (size_t)warp_defect_smem(), c->stream);

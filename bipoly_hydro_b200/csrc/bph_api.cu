@@ -619,6 +619,7 @@ int bph_destroy(bph_ctx_t *c) {
     dev_free(c->d_work32);
     dev_free(c->d_warp_coef);
     dev_free(c->d_warp_coef32);
+    dev_free(c->d_r32);
     dev_free(c->d_scf);
     if (c->side_stream) {
         cudaStreamSynchronize(c->side_stream);

@@ -44,7 +44,8 @@ struct bph_batch {
     int stage_cap = 0;         // positions of the host-array staging buffers
     double *d_LW = nullptr, *d_LQ = nullptr;  // grid-wide ADI scratch [cap][N][np] (large slots)
     double *d_prev = nullptr;         // converged FP64 solves: slot arrays of the previous cycle (on first use)
-    double *d_work32 = nullptr;       // mixed converged on grid-wide kernels: 4 * cap * N * np floats
+    double *d_work32 = nullptr;       // FP32 work arrays of the mixed converged forms (kind-dependent size)
+    size_t work32_doubles = 0;        // its size in doubles
     double *d_cnorm = nullptr;        // converged solves: per (instance, slot) norm pairs [cap][N][2]
     double *h_cnorm = nullptr;        // its pinned host copy
     double *d_cpart = nullptr;        // split-K partial sums of the batched contraction
@@ -804,10 +805,22 @@ int batch_reserve_converged(bph_batch *b, bool mixed) {
     if (!mixed && !c->adi_seg && !b->d_prev &&
         (rc = batch_alloc(b, &b->d_prev, (size_t)b->cap * c->N * c->nplane)))
         return rc;
-    // the grid-wide refinement cycle keeps r, delta and two right-hand sides per position (FP32)
-    if (mixed && c->mixed_kind == BPH_MIXED_ADI_GLOBAL && !b->d_work32 &&
-        (rc = batch_alloc(b, &b->d_work32, 2ull * b->cap * c->N * c->np)))
-        return rc;
+    // FP32 work arrays of the refinement: the grid-wide cycle keeps r, delta and two right-hand
+    // sides per position; the warp-cooperative one the rounded residual per position
+    size_t need = 0;
+    if (mixed && c->mixed_kind == BPH_MIXED_ADI_GLOBAL) need = 2ull * b->cap * c->N * c->np;
+    if (mixed && c->mixed_kind == BPH_MIXED_ADI_WARP) need = ((size_t)b->cap * c->N * c->np + 1) / 2;
+    if (need > b->work32_doubles) {
+        if (b->d_work32) {
+            cudaStreamSynchronize(c->stream);
+            cudaFree(b->d_work32);
+            b->bytes -= sizeof(double) * b->work32_doubles;
+            b->d_work32 = nullptr;
+            b->work32_doubles = 0;
+        }
+        if ((rc = batch_alloc(b, &b->d_work32, need))) return rc;
+        b->work32_doubles = need;
+    }
     return BPH_OK;
 }
 
@@ -853,6 +866,9 @@ int batch_converged_run(bph_batch *b, int n, const int *inst, const int *d_map, 
             if (c->mixed_kind == BPH_MIXED_ADI_GLOBAL)
                 BPH_CUDA(launch_adi_defect_large_batch(c, *s, b->d_P, b->d_R, n, d_map,
                                                        reinterpret_cast<float *>(b->d_work32), b->d_cnorm));
+            else if (c->mixed_kind == BPH_MIXED_ADI_WARP)
+                BPH_CUDA(launch_defect_warp(c, *s, b->d_P, b->d_R, n, d_map, b->d_cnorm,
+                                            reinterpret_cast<float *>(b->d_work32)));
             else
                 BPH_CUDA(launch_defect_batch(c, *s, b->d_P, b->d_R, n, d_map, b->d_cnorm));
         } else if (c->adi_seg) {  // update norms from the sweep's write-back

@@ -184,6 +184,7 @@ struct bph_ctx {
     double *d_warp_coef = nullptr;     // its per-slot (elambdazb, alphaz, betaz) blocks
     int mixed_warp = 0;                // FP32 warp-cooperative refinement kernel available
     float *d_warp_coef32 = nullptr;    // its coefficient blocks
+    float *d_r32 = nullptr;            // its rounded residual of one solve [N][np]
     double *d_scf = nullptr;           // SCF-step mass partials and scale (bph_scf.cu)
     void *noalloc_scratch = nullptr;   // device address of the allocation-free contraction's scratch array
     long long launches = 0;
@@ -350,9 +351,10 @@ size_t warp_block_doubles(int n);
 cudaError_t launch_pack_warp(bph_ctx *c, Schedule &s);
 // One FP32 refinement cycle of the warp-cooperative kind on nrows instance
 // rows of the slot arrays P/R (row r: instance inst_map[r]); per (instance,
-// slot) norms into norms[2 (i N + s) + 0/1].
+// slot) norms into norms[2 (i N + s) + 0/1]; r32: nrows * N * np floats of
+// scratch for the rounded residual.
 cudaError_t launch_defect_warp(bph_ctx *c, const Schedule &s, double *P, const double *R, int nrows,
-                               const int *inst_map, double *norms);
+                               const int *inst_map, double *norms, float *r32);
 cudaError_t launch_adi_warp(bph_ctx *c, const Schedule &s, int step0, int nsteps_run, bool cold, double *P,
                             const double *R, int nrows, const int *inst_map, const int *slot_map, int nslots,
                             double *norms, cudaStream_t st, bool pdl);
