@@ -188,7 +188,9 @@ cudaError_t contract_batch_launch(bph_ctx *c, bph_batch *b, long long mstride) {
 //     b0 (k = t, n = group), b1 (k = t + 4, n = group)
 //     d0 (group, 2t), d1 (group, 2t + 1), d2 (group + 8, 2t), d3 (group + 8, 2t + 1)
 constexpr int kDmmaWarps = 8;
-constexpr int kDmmaStages = 4;
+constexpr int kDmmaStages = 4;  // 8-zone steps per staged chunk
+constexpr int kDmmaPipe = 3;    // chunks in flight (cp.async stages)
+
 constexpr int kDmmaMaxTiles = 8;  // column tiles of 8 per launch (64 columns)
 
 __device__ __forceinline__ void dmma16x8x8(double (&d)[4], const double (&a)[4], double b0, double b1) {
@@ -199,18 +201,30 @@ __device__ __forceinline__ void dmma16x8x8(double (&d)[4], const double (&a)[4],
 }
 
 template <int NT>
-__global__ void __launch_bounds__(kDmmaWarps * 32, 2)
+struct DmmaSmem {
+    static constexpr int KC = 8 * kDmmaStages;   // zones per chunk
+    static constexpr int KS = KC + 4;            // padded row (doubles): a half-warp's fragment reads hit 16 banks
+    static constexpr int NCP = 8 * NT;           // moment columns of the launch's block
+    static constexpr int ROWS = kDmmaWarps * 16;  // table rows of a CTA
+    static constexpr int A = ROWS * KS, B = NCP * KS;  // doubles per stage
+    static constexpr size_t bytes = sizeof(double) * (size_t)kDmmaPipe * (A + B);
+};
+
+template <int NT>
+__global__ void __launch_bounds__(kDmmaWarps * 32, 1)
 k_contract_dmma(const double *__restrict__ G, const double *__restrict__ mom, long long mstride, long long np, int nb,
                 int c0, int ncol, double *__restrict__ C, long long cstride, unsigned int *__restrict__ counters,
                 double *__restrict__ partials) {
+    using L = DmmaSmem<NT>;
+    constexpr int KC = L::KC, KS = L::KS, NCP = L::NCP, ROWS = L::ROWS;
+    extern __shared__ __align__(16) double dsm[];
+    double *As = dsm;                       // [kDmmaPipe][ROWS][KS]
+    double *Bs = dsm + kDmmaPipe * L::A;    // [kDmmaPipe][NCP][KS]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grp = lane >> 2, t = lane & 3;
     const int m = blockIdx.y, split = blockIdx.z, nsplit = gridDim.z;
-    const int b0 = (blockIdx.x * kDmmaWarps + warp) * 16;
-    // table rows of this thread's fragments (clamped: rows beyond nb read row 0 and are never stored)
-    const int ra = b0 + grp, rb = b0 + grp + 8;
-    const double *ga = G + ((long long)m * nb + (ra < nb ? ra : 0)) * np;
-    const double *gb = G + ((long long)m * nb + (rb < nb ? rb : 0)) * np;
+    const int rows_base = blockIdx.x * ROWS;
+    const int b0 = rows_base + warp * 16;
     const bool live = b0 < nb;
     const long long nk = (np + 7) / 8;  // 8-zone steps (the last one may be partial)
     const long long per = (nk + nsplit - 1) / nsplit;
@@ -218,86 +232,83 @@ k_contract_dmma(const double *__restrict__ G, const double *__restrict__ mom, lo
     double acc[NT][4];
 #pragma unroll
     for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
-    auto load_a = [&](long long k, double (&a)[4]) {
-        const long long z0 = 8 * k + t, z1 = z0 + 4;
-        if (live && k < k_end) {
-            a[0] = z0 < np ? __ldcs(ga + z0) : 0.0;
-            a[1] = z0 < np ? __ldcs(gb + z0) : 0.0;
-            a[2] = z1 < np ? __ldcs(ga + z1) : 0.0;
-            a[3] = z1 < np ? __ldcs(gb + z1) : 0.0;
-        } else {
-            a[0] = a[1] = a[2] = a[3] = 0.0;
-        }
-    };
-    // the tables are set-up data: the first steps load before the moments are ready
-    double ab[kDmmaStages][4];
-#pragma unroll
-    for (int st = 0; st < kDmmaStages; ++st) load_a(k_begin + st, ab[st]);
-    // Moment columns staged per chunk of kDmmaStages steps (32 zones) in
-    // shared memory by cp.async, double-buffered: Ms[buf][column][zone],
-    // rows padded to 36 doubles (the B-fragment reads of a half-warp hit 16
-    // different banks); columns beyond ncol and zones beyond np read zero.
-    constexpr int NCP = 8 * NT;
-    constexpr int KC = 8 * kDmmaStages, KS = KC + 4;
-    __shared__ __align__(16) double Ms[2][NCP][KS];
+    // Chunk ch = zones [8 (k_begin + 4 ch), +32): the CTA's 128 table rows and the NCP
+    // moment columns, copied by cp.async into stage ch % kDmmaPipe; rows beyond nb,
+    // columns beyond ncol and zones beyond np are zero-filled.
+    const double *gbase = G + (long long)m * nb * np;
     const double *mbase = mom + m * mstride;
     const long long nchunk = (k_end - k_begin + kDmmaStages - 1) / kDmmaStages;
     const bool even_np = (np & 1) == 0;
-    auto issue_chunk = [&](long long ch, int buf) {
+    // L2 policy of the table stream: evict first (each element is read once per call)
+    unsigned long long evict_first;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(evict_first));
+    auto issue_chunk = [&](long long ch, int st) {
         const long long zc = 8 * (k_begin + ch * kDmmaStages);
+        double *as = As + st * L::A, *bs = Bs + st * L::B;
         if (even_np) {
-            for (int q = threadIdx.x; q < NCP * (KC / 2); q += kDmmaWarps * 32) {
-                const int cc = q / (KC / 2), zz = 2 * (q % (KC / 2));
-                const int col = c0 + cc;
+            for (int q = threadIdx.x; q < (ROWS + NCP) * (KC / 2); q += kDmmaWarps * 32) {
+                const int rr = q / (KC / 2), zz = 2 * (q % (KC / 2));
                 const long long z = zc + zz;
-                const int bytes = (col < ncol && z < np) ? 16 : 0;
-                const double *src = (bytes ? mbase + (long long)col * np + z : mbase);
-                asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
-                                 (uint32_t)__cvta_generic_to_shared(&Ms[buf][cc][zz])),
-                             "l"(src), "r"(bytes)
-                             : "memory");
+                const bool tab = rr < ROWS;
+                const int idx = tab ? rows_base + rr : c0 + rr - ROWS;
+                const bool ok = (tab ? idx < nb : idx < ncol) && z < np;
+                const double *src = ok ? (tab ? gbase : mbase) + (long long)idx * np + z : gbase;
+                double *dst = tab ? as + rr * KS + zz : bs + (rr - ROWS) * KS + zz;
+                if (tab)
+                    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2, %3;" ::"r"(
+                                     (uint32_t)__cvta_generic_to_shared(dst)),
+                                 "l"(src), "r"(ok ? 16 : 0), "l"(evict_first)
+                                 : "memory");
+                else
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                                     (uint32_t)__cvta_generic_to_shared(dst)),
+                                 "l"(src), "r"(ok ? 16 : 0)
+                                 : "memory");
             }
         } else {
-            for (int q = threadIdx.x; q < NCP * KC; q += kDmmaWarps * 32) {
-                const int cc = q / KC, zz = q % KC;
-                const int col = c0 + cc;
+            for (int q = threadIdx.x; q < (ROWS + NCP) * KC; q += kDmmaWarps * 32) {
+                const int rr = q / KC, zz = q % KC;
                 const long long z = zc + zz;
-                const int bytes = (col < ncol && z < np) ? 8 : 0;
-                const double *src = (bytes ? mbase + (long long)col * np + z : mbase);
+                const bool tab = rr < ROWS;
+                const int idx = tab ? rows_base + rr : c0 + rr - ROWS;
+                const bool ok = (tab ? idx < nb : idx < ncol) && z < np;
+                const double *src = ok ? (tab ? gbase : mbase) + (long long)idx * np + z : gbase;
+                double *dst = tab ? as + rr * KS + zz : bs + (rr - ROWS) * KS + zz;
                 asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(
-                                 (uint32_t)__cvta_generic_to_shared(&Ms[buf][cc][zz])),
-                             "l"(src), "r"(bytes)
+                                 (uint32_t)__cvta_generic_to_shared(dst)),
+                             "l"(src), "r"(ok ? 8 : 0)
                              : "memory");
             }
         }
-        asm volatile("cp.async.commit_group;" ::: "memory");
     };
     pdl_wait();
-    if (nchunk > 0) issue_chunk(0, 0);
-    for (long long ch = 0; ch < nchunk; ++ch) {
-        const int buf = (int)(ch & 1);
-        if (ch + 1 < nchunk) {
-            issue_chunk(ch + 1, buf ^ 1);
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
-        }
-        __syncthreads();
 #pragma unroll
-        for (int st = 0; st < kDmmaStages; ++st) {
-            const long long kk = k_begin + ch * kDmmaStages + st;
-            if (kk < k_end) {
-                double a[4] = {ab[st][0], ab[st][1], ab[st][2], ab[st][3]};
-                load_a(kk + kDmmaStages, ab[st]);  // the step kDmmaStages ahead
+    for (int st = 0; st < kDmmaPipe - 1; ++st) {
+        if (st < nchunk) issue_chunk(st, st);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    for (long long ch = 0; ch < nchunk; ++ch) {
+        asm volatile("cp.async.wait_group %0;" ::"n"(kDmmaPipe - 2) : "memory");
+        __syncthreads();  // chunk ch has landed; every warp is done with chunk ch - 1
+        const long long nxt = ch + kDmmaPipe - 1;
+        if (nxt < nchunk) issue_chunk(nxt, (int)(nxt % kDmmaPipe));
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        const int st_buf = (int)(ch % kDmmaPipe);
+        const double *as = As + st_buf * L::A + (warp * 16 + grp) * KS + t;
+        const double *bs = Bs + st_buf * L::B + grp * KS + t;
+        if (live) {
+#pragma unroll
+            for (int st = 0; st < kDmmaStages; ++st) {
+                const double a[4] = {as[8 * st], as[8 * KS + 8 * st], as[8 * st + 4], as[8 * KS + 8 * st + 4]};
 #pragma unroll
                 for (int j = 0; j < NT; ++j) {
-                    const double *mj = &Ms[buf][8 * j + grp][8 * st + t];
-                    dmma16x8x8(acc[j], a, mj[0], mj[4]);
+                    const double *bj = bs + 8 * j * KS + 8 * st;
+                    dmma16x8x8(acc[j], a, bj[0], bj[4]);
                 }
             }
         }
-        __syncthreads();  // the buffer is refilled two chunks later
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     pdl_trigger();
     const int rows0 = blockIdx.x * kDmmaWarps * 16;
     const int nrows = min(kDmmaWarps * 16, nb - rows0);
@@ -352,7 +363,10 @@ cudaError_t contract_dmma_launch_nt(bph_ctx *c, bph_batch *b, long long mstride,
     dim3 grid((unsigned)groups, (unsigned)c->g.mmax, (unsigned)nsplit);
     ++c->launches;
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = launch_config(c, grid, dim3(kDmmaWarps * 32), 0, attr);
+    const size_t smem = DmmaSmem<NT>::bytes;
+    cudaError_t e = raise_smem_limit((const void *)k_contract_dmma<NT>, (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = launch_config(c, grid, dim3(kDmmaWarps * 32), smem, attr);
     const double *G = c->d_green;
     const double *mom = b->d_mom;
     long long np = c->np, cstride = 2LL * b->cap * c->nb;
@@ -365,17 +379,28 @@ cudaError_t contract_dmma_launch_nt(bph_ctx *c, bph_batch *b, long long mstride,
     return cudaLaunchKernelExC(&cfg, (const void *)k_contract_dmma<NT>, args);
 }
 
-// Slices of the zone range: about four CTAs per SM over the launch, at least
-// 64 steps of 8 zones per slice, at most kBatchSplitMax.
+// Slices of the zone range (one CTA per SM): the count, up to kBatchSplitMax
+// with at least 64 steps of 8 zones per slice and at least two waves, whose
+// last wave is the fullest.
 int dmma_splits(const bph_ctx *c) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     const long long groups = (c->nb + kDmmaWarps * 16 - 1) / (kDmmaWarps * 16);
     const long long base = groups * c->g.mmax;
     const long long nk = (c->np + 7) / 8;
-    int nsplit = 1;
-    while (nsplit < kBatchSplitMax && base * (nsplit + 1) <= 4LL * sms && nk / (nsplit + 1) >= 64) ++nsplit;
-    return nsplit;
+    int best = 1;
+    double best_eff = -1.0;
+    for (int ns = 1; ns <= kBatchSplitMax; ++ns) {
+        if (ns > 1 && nk / ns < 64) break;
+        const long long ctas = base * ns;
+        const long long waves = (ctas + sms - 1) / sms;
+        const double eff = (double)ctas / (double)(waves * sms) + (waves >= 2 ? 0.25 : 0.0);
+        if (eff > best_eff + 1e-9) {
+            best_eff = eff;
+            best = ns;
+        }
+    }
+    return best;
 }
 
 // C for the 2n columns of n batch positions: one launch per block of 64 columns.
