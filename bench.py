@@ -743,7 +743,8 @@ def run_gpu(args, world, rank, local):
     if rank == 0 and not args.no_green:
         green = []
         # the serialised schedule (no side stream) first, then SM partitions
-        configs = [("serial", {"BPH_OVERLAP": "0"})] + [
+        configs = [("serial", {"BPH_OVERLAP": "0"}), ("fft_dense", {"BPH_FFT_DENSE": "1"}),
+                   ("serial+fft_dense", {"BPH_OVERLAP": "0", "BPH_FFT_DENSE": "1"})] + [
             (int(x), {"BPH_GREEN": "1", "BPH_GREEN_SMS": x}) for x in args.green_sms.split(",") if x]
         for sms, env in configs:
             os.environ.update(env)

@@ -13,6 +13,7 @@
 //
 // Forward convention (realft isign=+1): F_k = sum_l f_l exp(+2 pi i k l / N).
 #include <cmath>
+#include <cstdlib>
 
 #include "bph_internal.cuh"
 
@@ -113,13 +114,15 @@ struct FftBatch {
     int status_stride = 0;  // 1: a flag per position, 0: one shared flag
 };
 
-template <int M>
+template <int M, int Dense = 0>
 struct FftShape {
     static constexpr int kThreads = (M >= 256) ? 256 : 128;
     // resident CTAs per SM the register budget is sized for (the loads of a
-    // tile are all in flight at once; more CTAs hide more of their latency)
-    static constexpr int kMinBlocksFwd = (M >= 256) ? 2 : 5;
-    static constexpr int kMinBlocksInv = (M >= 256) ? 1 : 4;
+    // tile are all in flight at once; more CTAs hide more of their latency).
+    // Dense = 1: eight CTAs of 64 registers per SM for the 128-thread tiles
+    // (no spills), chosen at set-up with BPH_FFT_DENSE=1.
+    static constexpr int kMinBlocksFwd = (M >= 256) ? 2 : (Dense ? 8 : 5);
+    static constexpr int kMinBlocksInv = (M >= 256) ? 1 : (Dense ? 8 : 4);
     static constexpr size_t kSmem = sizeof(double2) * ((size_t)M * tile_cols<M>() + M + (M + 1));
 };
 
@@ -128,8 +131,8 @@ struct FftShape {
 // moments of the unzeroed density (bessel.F90:179-185, 226-274) obtained
 // from the same spectrum: sum_l rho_l e^{i k (l - 1/2) dphi} = e^{i pi k/N} F_k.
 // !kRho: write the warm-start potential into P's interior.
-template <int M, bool kRho>
-__global__ void __launch_bounds__(FftShape<M>::kThreads, FftShape<M>::kMinBlocksFwd)
+template <int M, bool kRho, int Dense = 0>
+__global__ void __launch_bounds__(FftShape<M>::kThreads, (FftShape<M, Dense>::kMinBlocksFwd))
 k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__restrict__ mom,
           const double2 *__restrict__ g_tw, const double2 *__restrict__ g_tw2, const double2 *__restrict__ g_ph,
           int numr, int numz, int nr, int nz, int mmax, int fm, int isym, double four_pi,
@@ -276,8 +279,8 @@ k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__re
 // With phieff != nullptr the epilogue also writes the effective potential
 // phieff = pot - 0.5 omega^2 rhf(J)^2 that the hydro source step forms from
 // pot (source.F90:156, make_source_temp.F90:121), saving it a full pass.
-template <int M>
-__global__ void __launch_bounds__(FftShape<M>::kThreads, FftShape<M>::kMinBlocksInv)
+template <int M, int Dense = 0>
+__global__ void __launch_bounds__(FftShape<M>::kThreads, (FftShape<M, Dense>::kMinBlocksInv))
 k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 *__restrict__ g_tw,
           const double2 *__restrict__ g_tw2, int numr, int numz, int isym, double *__restrict__ phieff,
           const double *__restrict__ rhf, double omega, FftBatch bt) {
@@ -398,6 +401,10 @@ cudaError_t set_fft_attrs(bph_ctx *c) {
         e = cudaFuncSetAttribute(k_fft_fwd<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_fft_inv<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_fft_fwd<M, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_fft_inv<M, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     c->fft_smem_fwd = c->fft_smem_inv = (int)smem;
     return e;
 }
@@ -410,6 +417,10 @@ cudaError_t fwd_rho(bph_ctx *c, const double *rho, double *R, double *mom, long 
     cudaLaunchAttribute attr[1];
     cudaLaunchConfig_t cfg =
         launch_config(c, dim3(blocks, (unsigned)npos), dim3(FftShape<M>::kThreads), FftShape<M>::kSmem, attr);
+    if (c->fft_dense)
+        return cudaLaunchKernelEx(&cfg, k_fft_fwd<M, true, 1>, rho, R, mom, (const double2 *)c->d_tw,
+                                  (const double2 *)c->d_tw2, (const double2 *)c->d_ph, c->g.numr, c->g.numz, c->nr,
+                                  c->nz, c->g.mmax, c->fm, c->g.isym, c->four_pi, status, mstride, bt);
     return cudaLaunchKernelEx(&cfg, k_fft_fwd<M, true>, rho, R, mom, (const double2 *)c->d_tw,
                               (const double2 *)c->d_tw2, (const double2 *)c->d_ph, c->g.numr, c->g.numz, c->nr,
                               c->nz, c->g.mmax, c->fm, c->g.isym, c->four_pi, status, mstride, bt);
@@ -432,6 +443,9 @@ cudaError_t inv(bph_ctx *c, double *pot, double *phieff, double omega, const dou
     cudaLaunchAttribute attr[1];
     cudaLaunchConfig_t cfg =
         launch_config(c, dim3(blocks, (unsigned)npos), dim3(FftShape<M>::kThreads), FftShape<M>::kSmem, attr);
+    if (c->fft_dense)
+        return cudaLaunchKernelEx(&cfg, k_fft_inv<M, 1>, P, pot, (const double2 *)c->d_tw, (const double2 *)c->d_tw2,
+                                  c->g.numr, c->g.numz, c->g.isym, phieff, (const double *)c->d_grid, omega, bt);
     return cudaLaunchKernelEx(&cfg, k_fft_inv<M>, P, pot, (const double2 *)c->d_tw, (const double2 *)c->d_tw2,
                               c->g.numr, c->g.numz, c->g.isym, phieff, (const double *)c->d_grid, omega, bt);
 }
@@ -461,6 +475,8 @@ cudaError_t inv_dispatch(bph_ctx *c, double *pot, double *phieff, double omega, 
 }  // namespace
 
 int fft_configure(bph_ctx *c) {
+    const char *dense = std::getenv("BPH_FFT_DENSE");
+    c->fft_dense = dense && dense[0] == '1';
     cudaError_t e = set_attrs_dispatch(c);
     if (e != cudaSuccess) return cuda_fail(e, "fft_configure");
     return BPH_OK;

@@ -159,6 +159,7 @@ struct bph_ctx {
     float *d_work32 = nullptr;                // global-memory refinement kernels: [4][N][np] (lazy)
     int adi_threads = 256;
     int fft_smem_fwd = 0, fft_smem_inv = 0;
+    bool fft_dense = false;      // FFT tiles compiled for eight CTAs per SM (BPH_FFT_DENSE=1)
     bool have_warm = false;
     bool pdl = true;             // launch solve kernels with programmatic dependent launch
     // Overlapped solve: slots whose mode carries no boundary data (k not a
