@@ -542,33 +542,29 @@ struct WarpDefArgs {
 };
 
 // FP64 residual r = -4 pi rho_hat - A phi of the current potential (its
-// Dirichlet columns enter through the stencil), rounded to float: one CTA
-// per (block row, slot), consecutive threads on consecutive zones of a row
-// (coalesced loads of the slot plane), written row-major for the refinement
-// kernel's 16-byte copies.
-__global__ void __launch_bounds__(256) k_residual32(WarpDefArgs a, int nr, int nz) {
-    const int s = blockIdx.x % a.N, row = blockIdx.x / a.N;
+// Dirichlet columns enter through the stencil), rounded to float: one
+// thread per zone, `bps` CTAs per (block row, slot), consecutive threads on
+// consecutive zones of a row (coalesced loads of the slot plane), written
+// row-major for the refinement kernel's 16-byte copies.  Enough CTAs
+// (nr nz / 256 per slot) to keep every SM's loads in flight.
+__global__ void __launch_bounds__(256) k_residual32(WarpDefArgs a, int nr, int nz, int bps) {
+    const int q = blockIdx.x / bps;
+    const int s = q % a.N, row = q / a.N;
+    const int e = (blockIdx.x - q * bps) * 256 + threadIdx.x;
+    const int tot = nr * nz;
+    pdl_wait();
+    if (e >= tot) return;
     const long long blk = (long long)(a.inst_map ? a.inst_map[row] : row) * a.N + s;
     const int numr = a.numr;
-    const double *Pg = a.P + blk * (long long)numr * a.numz;
-    const double *Rg = a.R + blk * (long long)nr * nz;
-    float *out = const_cast<float *>(a.r32) + ((long long)row * a.N + s) * (long long)nr * nz;
-    const double *brb = a.brb + (long long)s * numr;
-    const bool sym_bottom = (a.isym != 1);
-    const double gamma = a.gamma;
-    pdl_wait();
-    const long long tot = (long long)nr * nz;
-#pragma unroll 4
-    for (long long e = threadIdx.x; e < tot; e += 256) {
-        const int k = (int)(e / nr), j = (int)(e % nr);
-        const double *pc = Pg + (long long)numr * (k + 1) + 1 + j;
-        const double c = pc[0], ea = pc[1], no = pc[numr];
-        const double we = (j > 0) ? pc[-1] : 0.0;
-        const double so = (k > 0 || !sym_bottom) ? pc[-numr] : 0.0;
-        const double ar = brb[j + 1] * c + a.alphar[j + 1] * ea + a.betar[j + 1] * we;
-        const double az = a.bzb[k + 1] * c - gamma * no - gamma * so;
-        out[e] = (float)(Rg[e] - ar - az);
-    }
+    const int k = e / nr, j = e - k * nr;
+    const double *pc = a.P + blk * (long long)numr * a.numz + numr * (k + 1) + 1 + j;
+    const double c = pc[0], ea = pc[1], no = pc[numr];
+    const double we = (j > 0) ? pc[-1] : 0.0;
+    const double so = (k > 0 || a.isym == 1) ? pc[-numr] : 0.0;
+    const double ar = a.brb[(long long)s * numr + j + 1] * c + a.alphar[j + 1] * ea + a.betar[j + 1] * we;
+    const double az = a.bzb[k + 1] * c - a.gamma * no - a.gamma * so;
+    float *out = const_cast<float *>(a.r32) + ((long long)row * a.N + s) * tot;
+    out[e] = (float)(a.R[blk * tot + e] - ar - az);
 }
 
 template <int NLR, int NLZ>
@@ -959,12 +955,17 @@ cudaError_t launch_defect_warp(bph_ctx *c, const Schedule &s, double *P, const d
     a.nsteps = s.nsteps;
     a.gamma = c->gamma;
     c->launches += 2;
-    k_residual32<<<(unsigned)(c->N * nrows), 256, 0, c->stream>>>(a, c->nr, c->nz);
+    const int bps = (c->nr * c->nz + 255) / 256;
+    k_residual32<<<(unsigned)((long long)bps * c->N * nrows), 256, 0, c->stream>>>(a, c->nr, c->nz, bps);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    // programmatic dependent launch: the factor-block copies of the
+    // refinement kernel's prologue overlap the residual kernel's tail
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = launch_config(c, dim3((unsigned)(c->N * nrows)), dim3(kWThreads),
+                                           (size_t)warp_defect_smem(), attr);
     void *args[] = {&a};
-    return cudaLaunchKernel(warp_defect_kernel(), dim3((unsigned)(c->N * nrows)), dim3(kWThreads), args,
-                            (size_t)warp_defect_smem(), c->stream);
+    return cudaLaunchKernelExC(&cfg, warp_defect_kernel(), args);
 }
 
 cudaError_t launch_pack_warp(bph_ctx *c, Schedule &s) {

@@ -565,6 +565,48 @@ int check_ctx(const bph_ctx *c) {
 int batch_schedule(bph_ctx *c, int nsteps, Schedule **out) { return get_schedule(c, nsteps, out); }
 int context_status(bph_ctx *c) { return read_status(c); }
 
+// The device state of a context, once nothing holds it.
+static void ctx_free(bph_ctx *c) {
+    DeviceScope scope_(c->device);
+    if (c->own_stream) cudaStreamSynchronize(c->own_stream);
+    if (c->stream && c->stream != c->own_stream) cudaStreamSynchronize(c->stream);
+    for (auto &s : c->sched) free_schedule(c, s);
+    double *bufs[] = {c->d_green, c->d_brb,  c->d_elz, c->d_alphar, c->d_betar,     c->d_bzb,
+                      c->d_qcoef, c->d_grid, c->d_R,   c->d_P,      c->d_prev,      c->d_mom,
+                      c->d_S,     c->d_W,    c->d_W2,  c->d_P2,     c->d_red,       c->d_rho_stage, c->d_pot_stage,
+                      c->d_phieff_stage};
+    for (double *p : bufs) dev_free(p);
+    dev_free(c->d_tw);
+    dev_free(c->d_tw2);
+    dev_free(c->d_ph);
+    dev_free(c->d_status);
+    dev_free(c->d_ccnt);
+    dev_free(c->d_cpart);
+    conv_graphs_free(c);
+    dev_free(c->d_work32);
+    dev_free(c->d_warp_coef);
+    dev_free(c->d_warp_coef32);
+    dev_free(c->d_r32);
+    dev_free(c->d_scf);
+    if (c->side_stream) {
+        cudaStreamSynchronize(c->side_stream);
+        cudaStreamDestroy(c->side_stream);
+    }
+    if (c->ev_fft) cudaEventDestroy(c->ev_fft);
+    if (c->ev_free) cudaEventDestroy(c->ev_free);
+    if (c->ev_contract) cudaEventDestroy(c->ev_contract);
+    green_free(c);
+    if (c->d_slot_map) cudaFree(c->d_slot_map);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+void ctx_retain(bph_ctx *c) { c->refs.fetch_add(1, std::memory_order_relaxed); }
+
+void ctx_release(bph_ctx *c) {
+    if (c->refs.fetch_sub(1, std::memory_order_acq_rel) == 1) ctx_free(c);
+}
+
 }  // namespace bph
 
 using namespace bph;
@@ -600,38 +642,7 @@ int bph_setup(const bph_grid_t *grid, bph_ctx_t **ctx) {
 
 int bph_destroy(bph_ctx_t *c) {
     if (!c) return BPH_OK;
-    ::bph::DeviceScope scope_(c->device);
-    if (c->own_stream) cudaStreamSynchronize(c->own_stream);
-    if (c->stream && c->stream != c->own_stream) cudaStreamSynchronize(c->stream);
-    for (auto &s : c->sched) free_schedule(c, s);
-    double *bufs[] = {c->d_green, c->d_brb,  c->d_elz, c->d_alphar, c->d_betar,     c->d_bzb,
-                      c->d_qcoef, c->d_grid, c->d_R,   c->d_P,      c->d_prev,      c->d_mom,
-                      c->d_S,     c->d_W,    c->d_W2,  c->d_P2,     c->d_red,       c->d_rho_stage, c->d_pot_stage,
-                      c->d_phieff_stage};
-    for (double *p : bufs) dev_free(p);
-    dev_free(c->d_tw);
-    dev_free(c->d_tw2);
-    dev_free(c->d_ph);
-    dev_free(c->d_status);
-    dev_free(c->d_ccnt);
-    dev_free(c->d_cpart);
-    conv_graphs_free(c);
-    dev_free(c->d_work32);
-    dev_free(c->d_warp_coef);
-    dev_free(c->d_warp_coef32);
-    dev_free(c->d_r32);
-    dev_free(c->d_scf);
-    if (c->side_stream) {
-        cudaStreamSynchronize(c->side_stream);
-        cudaStreamDestroy(c->side_stream);
-    }
-    if (c->ev_fft) cudaEventDestroy(c->ev_fft);
-    if (c->ev_free) cudaEventDestroy(c->ev_free);
-    if (c->ev_contract) cudaEventDestroy(c->ev_contract);
-    green_free(c);
-    if (c->d_slot_map) cudaFree(c->d_slot_map);
-    if (c->own_stream) cudaStreamDestroy(c->own_stream);
-    delete c;
+    ::bph::ctx_release(c);
     return BPH_OK;
 }
 

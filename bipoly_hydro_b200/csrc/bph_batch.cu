@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "bph_internal.cuh"
+#include "bph_slices.h"
 
 struct bph_batch {
     bph_ctx *c = nullptr;
@@ -226,15 +227,15 @@ k_contract_dmma(const double *__restrict__ G, const double *__restrict__ mom, lo
     const int rows_base = blockIdx.x * ROWS;
     const int b0 = rows_base + warp * 16;
     const bool live = b0 < nb;
-    const long long nk = (np + 7) / 8;  // 8-zone steps (the last one may be partial)
-    const long long per = (nk + nsplit - 1) / nsplit;
-    const long long k_begin = split * per, k_end = min(nk, k_begin + per);
+    // slices of whole chunks; a chunk never reads past its slice's last zone
+    const ZoneSlice sl = zone_slice(np, nsplit, split, kDmmaStages);
+    const long long k_begin = sl.k_begin, k_end = sl.k_end, zend = sl.z_end;
     double acc[NT][4];
 #pragma unroll
     for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
     // Chunk ch = zones [8 (k_begin + 4 ch), +32): the CTA's 128 table rows and the NCP
     // moment columns, copied by cp.async into stage ch % kDmmaPipe; rows beyond nb,
-    // columns beyond ncol and zones beyond np are zero-filled.
+    // columns beyond ncol and zones beyond the slice (or np) are zero-filled.
     const double *gbase = G + (long long)m * nb * np;
     const double *mbase = mom + m * mstride;
     const long long nchunk = (k_end - k_begin + kDmmaStages - 1) / kDmmaStages;
@@ -251,7 +252,7 @@ k_contract_dmma(const double *__restrict__ G, const double *__restrict__ mom, lo
                 const long long z = zc + zz;
                 const bool tab = rr < ROWS;
                 const int idx = tab ? rows_base + rr : c0 + rr - ROWS;
-                const bool ok = (tab ? idx < nb : idx < ncol) && z < np;
+                const bool ok = (tab ? idx < nb : idx < ncol) && z < zend;
                 const double *src = ok ? (tab ? gbase : mbase) + (long long)idx * np + z : gbase;
                 double *dst = tab ? as + rr * KS + zz : bs + (rr - ROWS) * KS + zz;
                 if (tab)
@@ -271,7 +272,7 @@ k_contract_dmma(const double *__restrict__ G, const double *__restrict__ mom, lo
                 const long long z = zc + zz;
                 const bool tab = rr < ROWS;
                 const int idx = tab ? rows_base + rr : c0 + rr - ROWS;
-                const bool ok = (tab ? idx < nb : idx < ncol) && z < np;
+                const bool ok = (tab ? idx < nb : idx < ncol) && z < zend;
                 const double *src = ok ? (tab ? gbase : mbase) + (long long)idx * np + z : gbase;
                 double *dst = tab ? as + rr * KS + zz : bs + (rr - ROWS) * KS + zz;
                 asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(
@@ -531,6 +532,7 @@ int bph_batch_create(bph_ctx_t *c, int capacity, bph_batch_t **out) {
     }
     bph_batch *b = new bph_batch();
     b->c = c;
+    ctx_retain(c);  // the context's device state stays until this batch is destroyed
     b->cap = capacity;
     int rc = BPH_OK;
     if (!rc) rc = batch_alloc(b, &b->d_P, (size_t)capacity * c->N * c->nplane);
@@ -608,6 +610,7 @@ int bph_batch_destroy(bph_batch_t *b) {
     if (b->d_stat) cudaFree(b->d_stat);
     if (b->h_stat) cudaFreeHost(b->h_stat);
     if (b->h_cnorm) cudaFreeHost(b->h_cnorm);
+    if (b->c) ctx_release(b->c);
     delete b;
     return BPH_OK;
 }

@@ -19,6 +19,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 
@@ -190,6 +191,10 @@ struct bph_ctx {
     void *noalloc_scratch = nullptr;   // device address of the allocation-free contraction's scratch array
     long long launches = 0;
     size_t bytes = 0;
+    // Holders of the device state: the caller's handle (until bph_destroy)
+    // and each batch on the context (until bph_batch_destroy); the state is
+    // freed when the last one lets go, in whichever order they do.
+    std::atomic<int> refs{1};
 };
 
 namespace bph {
@@ -363,5 +368,9 @@ cudaError_t launch_adi_warp(bph_ctx *c, const Schedule &s, int step0, int nsteps
 // array for a context being set up (bph_noalloc.cu).
 int noalloc_setup(bph_ctx *c);
 int fft_configure(bph_ctx *c);
+// Context references (bph_api.cu): a batch takes one at creation and gives
+// it back at its destruction; the last release frees the device state.
+void ctx_retain(bph_ctx *c);
+void ctx_release(bph_ctx *c);
 
 }  // namespace bph

@@ -5,7 +5,7 @@
 // partials[split][m][b][cos|sin].  This header decides, from the grid alone,
 // whether a grid fits and how many splits of the interior the kernel uses.
 // Plain C++ with no CUDA dependence, so that the limits are testable on a
-// machine without a GPU (tests/test_noalloc_plan.py).
+// machine without a GPU (tests/test_host_logic_cpp.py).
 #pragma once
 
 #include <cstddef>

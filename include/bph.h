@@ -278,7 +278,10 @@ int bph_set_stream(bph_ctx_t *ctx, void *cuda_stream);
  * (e.g. BPH_ERR_NONFINITE) of the calls since the last synchronize. */
 int bph_synchronize(bph_ctx_t *ctx);
 
-/* Frees every device allocation of the context. */
+/* Releases the caller's handle: no call may use `ctx` afterwards.  The
+ * device state is freed at once, or, while batches created on the context
+ * still exist, when the last of them is destroyed (so the two may be
+ * destroyed in either order, as a garbage-collected host does). */
 int bph_destroy(bph_ctx_t *ctx);
 
 /* Text of the last error on this thread ("" if none). */

@@ -165,3 +165,48 @@ def test_tensor_core_contraction_production_grid(bph):
     single.close()
     batch.close()
     solver.close()
+
+
+@pytest.mark.parametrize("grid", [(202, 152, 16, 1.0 / 200.0, 2, 4), (35, 27, 32, 1.0 / 31.0, 2, 12),
+                                  (100, 70, 32, 1.0 / 96.0, 1, 8)],
+                         ids=["np30000-mmax4", "odd-np", "isym1"])
+def test_tensor_core_contraction_slice_boundaries(bph, grid):
+    """Grids whose zone slices are not whole multiples of the kernel's staged
+    chunk (30000 zones in 12 slices, an odd zone count, the isym 1 bottom
+    rows): S per position against its single solve to 1e-13."""
+    n = 3
+    rhos = _densities(grid, n)
+    solver = bph.PotentialSolver(*grid)
+    batch = bph.Batch(solver, capacity=n)
+    batch.solve(rhos, 0)
+    got = batch.moments_S(n)
+    single = bph.PotentialSolver(*grid)
+    for i in range(n):
+        single.potential_solver(rhos[i], 0)
+        assert rel_l2(got[i], single.moments_S()) <= 1e-13, i
+    single.close()
+    batch.close()
+    solver.close()
+
+
+def test_context_and_batch_destroyed_in_either_order(bph):
+    """A garbage-collected host may release the context's handle before a
+    batch on it: the batch keeps the device state alive, still solves, and
+    frees it when it is destroyed."""
+    grid = (34, 26, 64, 1.0 / 30.0, 2, 30)
+    rhos = _densities(grid, 2)
+    solver = bph.PotentialSolver(*grid)
+    batch = bph.Batch(solver, capacity=2)
+    ref = bph.Batch(solver, capacity=2)
+    ref.solve(rhos, 0)
+    want = ref.solve(rhos, 2)
+    ref.close()
+    batch.solve(rhos, 0)
+    lib, h = solver._lib, solver._h
+    solver._h = None
+    solver._dependents = ()
+    assert lib.bph_destroy(h) == 0
+    got = batch.solve(rhos, 2)
+    for i in range(2):
+        assert rel_l2(got[i], want[i]) <= 1e-13, i
+    batch.close()

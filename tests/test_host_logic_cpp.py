@@ -7,6 +7,10 @@
 * bph_noalloc_plan.h: the scratch sizing of the allocation-free contraction
   (rejection beyond the 8 MiB array, split-count clamps), including limits
   no constructible context on one GPU reaches.
+* bph_slices.h: the zone slices of the split-K tensor-core contraction
+  cover every interior zone exactly once for every slice count and chunk
+  length (a chunk that read into the next slice would add those zones
+  twice).
 """
 import os
 import re
@@ -34,6 +38,10 @@ def test_device_scope_restores_callers_device(tmp_path):
 
 def test_noalloc_plan_limits_and_clamps(tmp_path):
     assert "all checks passed" in _run(tmp_path, "noalloc_plan_check")
+
+
+def test_zone_slices_cover_each_zone_once(tmp_path):
+    assert "all checks passed" in _run(tmp_path, "zone_slice_check")
 
 
 def test_library_selects_devices_only_through_the_scope():
