@@ -6,13 +6,15 @@ potential_solver on the 130x98x256 grid (dr = dz = 1/126, isym 2, mmax 30):
 a bipolytropic binary (R1 0.3, R2 0.22, separation 0.9, mass ratio 0.5, core
 density x2 inside 0.4 R) rigidly rotated by one azimuthal zone per solve,
 each solve warm-started from the previous potential (5 ADI steps).  Every
-solve streams the 660 MB of FP64 Green tables, so the per-step working set is
-larger than the 126 MB L2.
+solve streams the FP64 Green tables (212 MB in the compact form, 660 MB in
+full), so the per-step working set is larger than the 126 MB L2.
 
   value      solves/s with rho resident in HBM (device-array C ABI call)
   e2e        solves/s through the host-array C ABI call: pinned rho copied in
              and pot copied out inside every step
-  roofline   k_green_contract (the dominant kernel) against measured HBM
+  roofline   the boundary contraction (the dominant kernel: k_green_compact
+             on the compact tables, k_green_contract on the full ones)
+             against measured HBM
   batched    warm solves of n independent instances per call (one pass over
              the Green tables for all n): solves/s per batch size
   converged  the same sequence solved to convergence in FP64 and in the
@@ -63,6 +65,31 @@ def contract_bytes(numr, numz, mmax, isym):
     return 8 * (nr * nz * rows * mmax + 2 * mmax * nr * nz + 2 * mmax * rows)
 
 
+def compact_dims(numr, numz, isym):
+    """The compact-table layout of bph_compact.h: tiles, side-vector stride, sets."""
+    nr, nz = numr - 2, numz - 2
+    nb8 = (nr + 7) // 8
+    kpl = (nz + 31) // 32
+    return dict(nr=nr, nz=nz, npair=nb8 * (nb8 + 1) // 2, nsets=2 if isym == 1 else 1, stride=nz + 32 * kpl,
+                side_ctas=(nr + 7) // 8)
+
+
+def compact_table_bytes(numr, numz, mmax, isym):
+    """Bytes of the compact tables: symmetric 8x8 tiles per height plus the side vectors."""
+    d = compact_dims(numr, numz, isym)
+    return 8 * mmax * (d["nsets"] * d["npair"] * d["nz"] * 64 + d["nr"] * 2 * d["stride"])
+
+
+def compact_contract_bytes(numr, numz, mmax, isym):
+    """Algorithmic bytes of one k_green_compact launch: compact tables + moment vectors
+    + partial sums written and read once + S."""
+    d = compact_dims(numr, numz, isym)
+    nr, nz = d["nr"], d["nz"]
+    rows = nr + nz + (nr if isym == 1 else 0)
+    parts = mmax * (d["nsets"] * d["npair"] * 32 + d["side_ctas"] * nz * 2)
+    return compact_table_bytes(numr, numz, mmax, isym) + 8 * (2 * mmax * nr * nz + 2 * parts + 2 * mmax * rows)
+
+
 def hbm_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -72,9 +99,11 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def committed_traffic():
-    """dram bytes per launch of k_green_contract from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "green_contract_130x98x256.md")
+def committed_traffic(kernel="k_green_contract"):
+    """dram bytes per launch of the contraction kernel from its committed ncu summary, if any."""
+    name = {"k_green_contract": "green_contract_130x98x256.md",
+            "k_green_compact": "green_compact_130x98x256.md"}[kernel]
+    path = os.path.join(ROOT, "profiles", name)
     try:
         text = open(path).read()
     except OSError:
@@ -794,10 +823,22 @@ def run_gpu(args, world, rank, local):
     }
     solver.synchronize()
     peak, peak_kind = hbm_peak()
-    cb = contract_bytes(numr, numz, GRID["mmax"], GRID["isym"])
+    compact = solver.info()["contract_kind"] == B.solver.CONTRACT_COMPACT
+    contract_kernel = "k_green_compact" if compact else "k_green_contract"
+    if compact:
+        cb = compact_contract_bytes(numr, numz, GRID["mmax"], GRID["isym"])
+    else:
+        cb = contract_bytes(numr, numz, GRID["mmax"], GRID["isym"])
     achieved = cb / (phases["green_contract"] / 1e3) / 1e9
-    traffic = committed_traffic()
-    b_alg = compulsory_bytes(numr, numz, numphi, GRID["mmax"], GRID["isym"], warm=True)
+    traffic = committed_traffic(contract_kernel)
+    # compulsory bytes of the solve as the reference forms it (full tables) and as run
+    b_alg_full = compulsory_bytes(numr, numz, numphi, GRID["mmax"], GRID["isym"], warm=True)
+    b_alg = b_alg_full
+    if compact:
+        nr_, nz_ = numr - 2, numz - 2
+        rows = nr_ + nz_ + (nr_ if GRID["isym"] == 1 else 0)
+        b_alg = b_alg_full - 8 * nr_ * nz_ * rows * GRID["mmax"] + compact_table_bytes(
+            numr, numz, GRID["mmax"], GRID["isym"])
     solve_gbs = b_alg / (ms_per_step / 1e3) / 1e9
 
     # ---- e2e: host-array C ABI call with pinned buffers ----------------
@@ -1040,7 +1081,7 @@ def run_gpu(args, world, rank, local):
             "config": {"workload": "130x98x256 warm time-step solves, bipolytrope pair rotated 1 zone/solve",
                        **GRID, "nsteps_adi": 5},
             "parallelism": f"independent sequence per GPU x{world}",
-            "l2": "per-solve working set (660 MB Green tables) > 126 MB L2, no flush needed",
+            "l2": "per-solve working set (212 MB compact Green tables, 660 MB full) > 126 MB L2, no flush needed",
             "zone_updates_per_s": value * ntot * 5,
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 8 * ntot,
                     "d2h_bytes_per_step": 8 * ntot, "host_memory": "pinned (torch pin_memory)",
@@ -1051,10 +1092,12 @@ def run_gpu(args, world, rank, local):
                     "registered_vs_pinned": e2e_registered["value"] / e2e_value},
             "parity": parity,
             "parity_rel_l2": parity["last_timed_rel_l2"] if parity else None,
-            "roofline": {"bound": "hbm", "kernel": "k_green_contract", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": contract_kernel, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "alg_bytes_per_launch": cb,
-                         "solve_alg_bytes": b_alg, "solve_gbs": solve_gbs, "solve_frac": solve_gbs / peak},
+                         "solve_alg_bytes": b_alg, "solve_gbs": solve_gbs, "solve_frac": solve_gbs / peak,
+                         "solve_alg_bytes_full_tables": b_alg_full,
+                         "solve_frac_full_tables": b_alg_full / (ms_per_step / 1e3) / 1e9 / peak},
             "phase_ms": phases,
             "converged": conv,
             "batched": batched,

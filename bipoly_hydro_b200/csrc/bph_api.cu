@@ -411,6 +411,7 @@ int setup_impl(bph_ctx *c) {
     }
     BPH_CUDA(launch_qcoef(c));
     BPH_CUDA(launch_green_tables(c));
+    if ((rc = compact_configure(c))) return rc;
     if ((rc = fft_configure(c))) return rc;
     if ((rc = adi_configure(c))) return rc;
     if ((rc = warp_configure(c))) return rc;
@@ -582,6 +583,10 @@ static void ctx_free(bph_ctx *c) {
     dev_free(c->d_status);
     dev_free(c->d_ccnt);
     dev_free(c->d_cpart);
+    dev_free(c->d_gtile);
+    dev_free(c->d_gside);
+    dev_free(c->d_kpart);
+    dev_free(c->d_kcnt);
     conv_graphs_free(c);
     dev_free(c->d_work32);
     dev_free(c->d_warp_coef);
@@ -1005,6 +1010,7 @@ long long bph_info(const bph_ctx_t *c, int what) {
         case BPH_INFO_ADI_WARP_SMEM: return c->adi_warp_smem;
         case BPH_INFO_MIXED_WARP_NS: return (long long)(1e3f * c->mixed_tuned_us[BPH_MIXED_ADI_WARP]);
         case BPH_INFO_GREEN_SMS: return c->green ? c->green_sms[0] : -c->green_fail;
+        case BPH_INFO_CONTRACT_KIND: return c->compact ? BPH_CONTRACT_COMPACT : BPH_CONTRACT_FULL;
         default: return -1;
     }
 }

@@ -17,7 +17,9 @@
 //   F_0 = N factor S_C0,  F_k = e^{-i pi k/N} N factor (S_Cm + i S_Sm),
 // and zero at every other frequency, so the slots are written directly.
 #include <cmath>
+#include <cstdlib>
 
+#include "bph_compact.h"
 #include "bph_internal.cuh"
 
 namespace bph {
@@ -42,6 +44,30 @@ struct SlotOut {
     int numr, numz, nr, nz, M, fm;
     double nfactor;     // N * factor
 };
+
+// Dirichlet slot of boundary row b, mode m from (S_C, S_S): the cosine
+// slot fm m (part 0) or the sine slot M + fm m (part 1, m > 0).
+__device__ __forceinline__ void write_slot(const SlotOut &so, int m, int b, double sc, double ss, int part) {
+    int jz, kz;
+    if (b < so.nr) {
+        jz = b + 1;
+        kz = so.numz - 1;
+    } else if (b < so.nr + so.nz) {
+        jz = so.numr - 1;
+        kz = b - so.nr + 1;
+    } else {
+        jz = b - so.nr - so.nz + 1;
+        kz = 0;
+    }
+    const long long nplane = (long long)so.numr * so.numz;
+    const long long pos = jz + (long long)so.numr * kz;
+    const int k = so.fm * m;
+    const double2 w = so.ph[m];
+    if (part == 0)
+        so.P[(long long)k * nplane + pos] = so.nfactor * (w.x * sc + w.y * ss);
+    else if (m > 0)
+        so.P[(long long)(so.M + k) * nplane + pos] = so.nfactor * (w.y * sc - w.x * ss);
+}
 
 template <bool kVec>
 __global__ void __launch_bounds__(kContractThreads, 2)
@@ -128,26 +154,7 @@ k_green_contract(const double *__restrict__ G, const double *__restrict__ mom, d
         if (!so.P) return;
         const double sc = cs ? other : mine;
         const double ss = (m == 0) ? 0.0 : (cs ? mine : other);
-        const int b = b0 + r;
-        int jz, kz;
-        if (b < so.nr) {
-            jz = b + 1;
-            kz = so.numz - 1;
-        } else if (b < so.nr + so.nz) {
-            jz = so.numr - 1;
-            kz = b - so.nr + 1;
-        } else {
-            jz = b - so.nr - so.nz + 1;
-            kz = 0;
-        }
-        const long long nplane = (long long)so.numr * so.numz;
-        const long long pos = jz + (long long)so.numr * kz;
-        const int k = so.fm * m;
-        const double2 w = so.ph[m];
-        if (cs == 0)
-            so.P[(long long)k * nplane + pos] = so.nfactor * (w.x * sc + w.y * ss);
-        else if (m > 0)
-            so.P[(long long)(so.M + k) * nplane + pos] = so.nfactor * (w.y * sc - w.x * ss);
+        write_slot(so, m, b0 + r, sc, ss, cs);
     };
     if (nsplit == 1) {
         if (threadIdx.x < 32) finish(v);
@@ -211,6 +218,237 @@ __global__ void k_boundary_slots(const double *__restrict__ S, const double2 *__
     P[(long long)s * nplane + jz + (long long)numr * kz] = v;
 }
 
+// ---------------------------------------------------------------------------
+// k_green_compact: the same S (and Dirichlet slots) from the compact tables
+// of bph_compact.h.  Grid: mmax x (top_ctas + side_ctas) CTAs of 8 warps.
+//
+// Tile warps (one tile (I, J) of one mode over every height k): lane
+// (r = lane / 4, c0 = 2 (lane % 4)) streams elements (r, c0), (r, c0 + 1)
+// of the tile, one 16-byte evict-first load per height, and accumulates
+//   row part:    sum_k H(8I + r, 8J + c, k) mom(8J + c, k)   -> S[8I + r]
+//   column part: sum_k H(8I + r, 8J + c, k) mom(8I + r, k)   -> S[8J + c]
+// (the column part is the mirrored tile (J, I), unused when I == J).  The
+// radii r_j of G = H r_j scale the sums at the end; shuffles reduce them
+// over the tile's rows and columns in a fixed order.
+//
+// Side warps (one radial zone j of one mode): lane holds side rows
+// kb = KPL lane + i and slides windows of U_j(kb - k), V_j(kb + k) over k
+// (one new U and one new V value per height), so the side rows cost
+// compute, not table bytes.  The CTA adds its eight zones in shared memory.
+//
+// Every CTA writes partial sums; the last CTA of each mode to arrive adds
+// them in a fixed order (deterministic), writes S and the slots, and resets
+// the mode's arrival counter for the next launch.
+struct CompactArgs {
+    const double *T;    // tiles [m][set][tile][k][64]
+    const double *U;    // side vectors [m][j][U | V][stride]
+    const double *mom;  // moments [2m + cs][np]
+    const double *rw;   // r_j, j < nr
+    double *S;          // [m][nb][2]
+    double *part;       // per mode: tile parts [set][tile][32], then side parts [side CTA][nz][2]
+    unsigned int *cnt;  // [mmax]
+    long long np, part_m;
+    int nr, nz, nb, nb8, npair, nsets, stride, top_ctas, side_ctas;
+    SlotOut so;
+};
+
+template <int KPL, bool kVec>
+__global__ void __launch_bounds__(256) k_green_compact(CompactArgs a) {
+    using namespace compact;
+    constexpr int kU = 8;  // heights per batch of table loads
+    const int per_m = a.top_ctas + a.side_ctas;
+    const int m = blockIdx.x / per_m, role = blockIdx.x % per_m;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nr = a.nr, nz = a.nz;
+    const long long np = a.np;
+    const double *mc = a.mom + 2LL * m * np, *ms = mc + np;
+    double *part = a.part + (long long)m * a.part_m;
+    __shared__ double red[kWarps][64];
+    __shared__ bool last;
+    if (role < a.top_ctas) {
+        const int q = role * kWarps + warp;
+        if (q < a.nsets * a.npair) {
+            const int set = q / a.npair, tile = q % a.npair;
+            int I, J;
+            pair_blocks(tile, a.nb8, &I, &J);
+            const int r = lane >> 2, c0 = 2 * (lane & 3);
+            const int jr = min(kTile * I + r, nr - 1);
+            // column pair (even start when vectorised: nr even keeps it in bounds and aligned)
+            const int jc0 = kVec ? min(kTile * J + c0, nr - 2) : min(kTile * J + c0, nr - 1);
+            const int jc1 = kVec ? jc0 + 1 : min(kTile * J + c0 + 1, nr - 1);
+            const double2 *src =
+                reinterpret_cast<const double2 *>(a.T + (((long long)m * a.nsets + set) * a.npair + tile) * nz * 64) +
+                lane;
+            double r0c = 0.0, r0s = 0.0, r1c = 0.0, r1s = 0.0, k0c = 0.0, k0s = 0.0, k1c = 0.0, k1s = 0.0;
+            double2 t[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) t[u] = (u < nz) ? __ldcs(src + u * 32) : make_double2(0.0, 0.0);
+            pdl_wait();  // the moments come from the forward transform
+            for (int k0 = 0; k0 < nz; k0 += kU) {
+                double2 tn[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u)
+                    tn[u] = (k0 + kU + u < nz) ? __ldcs(src + (k0 + kU + u) * 32) : make_double2(0.0, 0.0);
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    if (k0 + u < nz) {
+                        const long long off = (long long)nr * (k0 + u);
+                        double xc0, xc1, xs0, xs1;
+                        if (kVec) {
+                            const double2 vc = __ldg(reinterpret_cast<const double2 *>(mc + off + jc0));
+                            const double2 vs = __ldg(reinterpret_cast<const double2 *>(ms + off + jc0));
+                            xc0 = vc.x;
+                            xc1 = vc.y;
+                            xs0 = vs.x;
+                            xs1 = vs.y;
+                        } else {
+                            xc0 = __ldg(mc + off + jc0);
+                            xc1 = __ldg(mc + off + jc1);
+                            xs0 = __ldg(ms + off + jc0);
+                            xs1 = __ldg(ms + off + jc1);
+                        }
+                        const double yc = __ldg(mc + off + jr), ys = __ldg(ms + off + jr);
+                        r0c = fma(t[u].x, xc0, r0c);
+                        r0s = fma(t[u].x, xs0, r0s);
+                        r1c = fma(t[u].y, xc1, r1c);
+                        r1s = fma(t[u].y, xs1, r1s);
+                        k0c = fma(t[u].x, yc, k0c);
+                        k0s = fma(t[u].x, ys, k0s);
+                        k1c = fma(t[u].y, yc, k1c);
+                        k1s = fma(t[u].y, ys, k1s);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) t[u] = tn[u];
+            }
+            // G = H r_j: the row part takes the columns' radii, the column part the row's
+            const double wr = a.rw[jr], w0 = a.rw[jc0], w1 = a.rw[jc1];
+            double rc = w0 * r0c + w1 * r1c, rs = w0 * r0s + w1 * r1s;
+            double cc0 = wr * k0c, cs0 = wr * k0s, cc1 = wr * k1c, cs1 = wr * k1s;
+#pragma unroll
+            for (int off = 1; off <= 2; off <<= 1) {
+                rc += __shfl_xor_sync(0xffffffffu, rc, off);
+                rs += __shfl_xor_sync(0xffffffffu, rs, off);
+            }
+#pragma unroll
+            for (int off = 4; off <= 16; off <<= 1) {
+                cc0 += __shfl_xor_sync(0xffffffffu, cc0, off);
+                cs0 += __shfl_xor_sync(0xffffffffu, cs0, off);
+                cc1 += __shfl_xor_sync(0xffffffffu, cc1, off);
+                cs1 += __shfl_xor_sync(0xffffffffu, cs1, off);
+            }
+            double *pp = part + (long long)q * kPartPair;  // [row | column][8][cos, sin]
+            if ((lane & 3) == 0) {
+                pp[2 * r] = rc;
+                pp[2 * r + 1] = rs;
+            }
+            if (lane < 4) {
+                pp[16 + 2 * c0] = cc0;
+                pp[16 + 2 * c0 + 1] = cs0;
+                pp[16 + 2 * c0 + 2] = cc1;
+                pp[16 + 2 * c0 + 3] = cs1;
+            }
+        } else {
+            pdl_wait();
+        }
+    } else {
+        const int g = role - a.top_ctas;
+        const int j = g * kWarps + warp;
+        double acc_c[KPL], acc_s[KPL];
+#pragma unroll
+        for (int i = 0; i < KPL; ++i) acc_c[i] = acc_s[i] = 0.0;
+        if (j < nr) {
+            const double *Uv = a.U + ((long long)m * nr + j) * 2 * a.stride, *Vv = Uv + a.stride;
+            const int base = KPL * lane;
+            double u[KPL], v[KPL];
+#pragma unroll
+            for (int i = 0; i < KPL; ++i) {
+                u[i] = __ldg(Uv + base + i + nz - 1);
+                v[i] = __ldg(Vv + base + i);
+            }
+            pdl_wait();
+            const double *mcj = mc + j, *msj = ms + j;
+#pragma unroll 4
+            for (int k = 0; k < nz; ++k) {
+                const double xc = __ldg(mcj + (long long)nr * k), xs = __ldg(msj + (long long)nr * k);
+                const double un = (k + 1 < nz) ? __ldg(Uv + base + nz - 2 - k) : 0.0;
+                const double vn = (k + 1 < nz) ? __ldg(Vv + base + KPL + k) : 0.0;
+#pragma unroll
+                for (int i = 0; i < KPL; ++i) {
+                    const double w = u[i] + v[i];
+                    acc_c[i] = fma(w, xc, acc_c[i]);
+                    acc_s[i] = fma(w, xs, acc_s[i]);
+                }
+#pragma unroll
+                for (int i = KPL - 1; i > 0; --i) u[i] = u[i - 1];
+                u[0] = un;
+#pragma unroll
+                for (int i = 0; i + 1 < KPL; ++i) v[i] = v[i + 1];
+                v[KPL - 1] = vn;
+            }
+        } else {
+            pdl_wait();
+        }
+        // the CTA's eight zones, added in warp order, one window position at a time
+        double *ps = part + (long long)a.nsets * a.npair * kPartPair + (long long)g * nz * 2;
+#pragma unroll
+        for (int i = 0; i < KPL; ++i) {
+            red[warp][2 * lane] = acc_c[i];
+            red[warp][2 * lane + 1] = acc_s[i];
+            __syncthreads();
+            if (threadIdx.x < 64) {
+                double val = 0.0;
+#pragma unroll
+                for (int w = 0; w < kWarps; ++w) val += red[w][threadIdx.x];
+                const int kb = KPL * (threadIdx.x >> 1) + i;
+                if (kb < nz) ps[2 * kb + (threadIdx.x & 1)] = val;
+            }
+            __syncthreads();
+        }
+    }
+    pdl_trigger();
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(a.cnt + m, 1u) == (unsigned)(per_m - 1));
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const double *pside = part + (long long)a.nsets * a.npair * kPartPair;
+    for (int b = threadIdx.x; b < a.nb; b += blockDim.x) {
+        double sc = 0.0, ss = 0.0;
+        if (b < nr || b >= nr + nz) {
+            const int set = (b < nr) ? 0 : 1;
+            const int jb = (b < nr) ? b : b - nr - nz;
+            const int I = jb / kTile, r = jb % kTile;
+            const double *pt = part + (long long)set * a.npair * kPartPair;
+            for (int Ip = 0; Ip < I; ++Ip) {
+                const double *pp = pt + (long long)pair_index(Ip, I, a.nb8) * kPartPair + 16 + 2 * r;
+                sc += __ldcg(pp);
+                ss += __ldcg(pp + 1);
+            }
+            for (int Jp = I; Jp < a.nb8; ++Jp) {
+                const double *pp = pt + (long long)pair_index(I, Jp, a.nb8) * kPartPair + 2 * r;
+                sc += __ldcg(pp);
+                ss += __ldcg(pp + 1);
+            }
+        } else {
+            const int kb = b - nr;
+            for (int g = 0; g < a.side_ctas; ++g) {
+                sc += __ldcg(pside + ((long long)g * nz + kb) * 2);
+                ss += __ldcg(pside + ((long long)g * nz + kb) * 2 + 1);
+            }
+        }
+        if (m == 0) ss = 0.0;
+        a.S[((long long)m * a.nb + b) * 2] = sc;
+        a.S[((long long)m * a.nb + b) * 2 + 1] = ss;
+        if (a.so.P) {
+            write_slot(a.so, m, b, sc, ss, 0);
+            write_slot(a.so, m, b, sc, ss, 1);
+        }
+    }
+    if (threadIdx.x == 0) a.cnt[m] = 0u;
+}
+
 }  // namespace
 
 int contract_configure(bph_ctx *c) {
@@ -238,7 +476,82 @@ int contract_configure(bph_ctx *c) {
     return BPH_OK;
 }
 
+int compact_configure(bph_ctx *c) {
+    c->compact = 0;
+    const char *env = std::getenv("BPH_COMPACT");
+    if (env && env[0] == '0') return BPH_OK;
+    const compact::Dims d = compact::dims(c->nr, c->nz, c->g.isym);
+    if (!d.ok) return BPH_OK;
+    const size_t mm = (size_t)c->g.mmax;
+    const size_t nt = mm * (size_t)compact::pair_doubles(d), ns = mm * (size_t)compact::side_doubles(d),
+                 np = mm * (size_t)compact::part_doubles(d);
+    cudaError_t e = cudaMalloc((void **)&c->d_gtile, sizeof(double) * nt);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_gside, sizeof(double) * ns);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_kpart, sizeof(double) * np);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_kcnt, sizeof(unsigned int) * mm);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_kcnt, 0, sizeof(unsigned int) * mm, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "compact Green tables");
+    c->bytes += sizeof(double) * (nt + ns + np) + sizeof(unsigned int) * mm;
+    e = launch_green_compact(c);
+    if (e != cudaSuccess) return cuda_fail(e, "k_green_compact_tiles / k_green_compact_side");
+    c->compact = 1;
+    return BPH_OK;
+}
+
+template <int KPL>
+cudaError_t launch_compact_kpl(bph_ctx *c, const CompactArgs &a, unsigned grid) {
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = launch_config(c, dim3(grid), dim3(256), 0, attr);
+    if (c->nr % 2 == 0) return cudaLaunchKernelEx(&cfg, k_green_compact<KPL, true>, a);
+    return cudaLaunchKernelEx(&cfg, k_green_compact<KPL, false>, a);
+}
+
+cudaError_t launch_green_compact_contract(bph_ctx *c, bool write_slots) {
+    const compact::Dims d = compact::dims(c->nr, c->nz, c->g.isym);
+    CompactArgs a;
+    a.T = c->d_gtile;
+    a.U = c->d_gside;
+    a.mom = c->d_mom;
+    a.rw = c->d_grid + 1;  // rhf[j + 1]
+    a.S = c->d_S;
+    a.part = c->d_kpart;
+    a.cnt = c->d_kcnt;
+    a.np = c->np;
+    a.part_m = compact::part_doubles(d);
+    a.nr = c->nr;
+    a.nz = c->nz;
+    a.nb = c->nb;
+    a.nb8 = d.nb8;
+    a.npair = d.npair;
+    a.nsets = d.nsets;
+    a.stride = d.stride;
+    a.top_ctas = d.top_ctas;
+    a.side_ctas = d.side_ctas;
+    a.so.P = write_slots ? c->d_P : nullptr;
+    a.so.ph = c->d_ph;
+    a.so.numr = c->g.numr;
+    a.so.numz = c->g.numz;
+    a.so.nr = c->nr;
+    a.so.nz = c->nz;
+    a.so.M = c->M;
+    a.so.fm = c->fm;
+    a.so.nfactor = (double)c->N * c->factor;
+    ++c->launches;
+    const unsigned grid = (unsigned)(c->g.mmax * (d.top_ctas + d.side_ctas));
+    switch (d.kpl) {
+        case 1: return launch_compact_kpl<1>(c, a, grid);
+        case 2: return launch_compact_kpl<2>(c, a, grid);
+        case 3: return launch_compact_kpl<3>(c, a, grid);
+        case 4: return launch_compact_kpl<4>(c, a, grid);
+        case 5: return launch_compact_kpl<5>(c, a, grid);
+        case 6: return launch_compact_kpl<6>(c, a, grid);
+        case 7: return launch_compact_kpl<7>(c, a, grid);
+        default: return launch_compact_kpl<8>(c, a, grid);
+    }
+}
+
 cudaError_t launch_green_contract(bph_ctx *c, bool write_slots) {
+    if (c->compact) return launch_green_compact_contract(c, write_slots);
     dim3 grid((unsigned)((c->nb + kContractRows - 1) / kContractRows), (unsigned)c->g.mmax,
               (unsigned)c->contract_split);
     SlotOut so;

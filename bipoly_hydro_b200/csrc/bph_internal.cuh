@@ -143,6 +143,12 @@ struct bph_ctx {
     unsigned int *d_ccnt = nullptr;  // contraction arrival counters [mmax][row groups]
     double *d_cpart = nullptr;       // contraction partial sums [split][mmax][nb][2]
     int contract_split = 1;
+    // compact Green tables (bph_compact.h) and the contraction that reads them
+    int compact = 0;                 // 1: the single-solve contraction streams the compact tables
+    double *d_gtile = nullptr;       // symmetric tiles of the top (and bottom) rows [m][set][tile][k][64]
+    double *d_gside = nullptr;       // side-row vectors [m][j][U | V][stride]
+    double *d_kpart = nullptr;       // partial sums [m][tile parts | side parts]
+    unsigned int *d_kcnt = nullptr;  // arrival counters [mmax]
 
     int adi_smem = 0;            // dynamic shared bytes of the on-chip ADI kernel (0: global variant)
     int adi_seg = 0;             // threads of the segmented on-chip ADI kernel (0: not used)
@@ -337,6 +343,10 @@ int select_mixed_kind(bph_ctx *c, int kind);
 // Work area of the global-memory refinement kernel (allocated on first use).
 int ensure_mixed_work(bph_ctx *c);
 int contract_configure(bph_ctx *c);
+// Compact tables: allocation and build at set-up (BPH_COMPACT=0 leaves them
+// off), bph_setup.cu builds them.
+int compact_configure(bph_ctx *c);
+cudaError_t launch_green_compact(bph_ctx *c);
 // Warp-cooperative FP64 ADI (bph_adi_warp.cu).  warp_configure selects it
 // for the grids it covers (c->adi_warp != 0) and packs the per-slot
 // coefficients; launch_pack_warp fills a schedule's factor blocks;

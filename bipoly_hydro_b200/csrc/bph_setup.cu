@@ -7,6 +7,7 @@
 // context and its speed does not matter next to its fidelity.
 #include <cmath>
 
+#include "bph_compact.h"
 #include "bph_internal.cuh"
 
 namespace bph {
@@ -209,6 +210,105 @@ __global__ void k_green_tables(const double *__restrict__ grid, const double *__
     }
 }
 
+// Compact tables (bph_compact.h).  Tiles of the top (set 0) and bottom
+// (set 1, isym 1) rows: one thread per (set, tile, height k, element);
+// element (r, c) of tile (I, J) is H(jb = 8I + r, j = 8J + c, k) =
+// G(jb, j, k) / r_j with G as k_green_tables forms it; zero outside the
+// nr x nr plane.  Layout [m][set][tile][k][64].
+__global__ void k_green_compact_tiles(const double *__restrict__ grid, const double *__restrict__ qc,
+                                      double *__restrict__ T, int numr, int numz, int nr, int nz, int nb8, int npair,
+                                      int nsets, int mmax, int isym, double piinv) {
+    const long long per_m = (long long)nsets * npair * nz * 64;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= per_m) return;
+    const double *rhf = grid, *rhfinv = grid + numr, *zhf = grid + 2 * numr;
+    const int e = (int)(t % 64);
+    long long rest = t / 64;
+    const int k = (int)(rest % nz);
+    rest /= nz;
+    const int q = (int)(rest % npair), set = (int)(rest / npair);
+    int I, J;
+    compact::pair_blocks(q, nb8, &I, &J);
+    const int jb = 8 * I + (e >> 3), j = 8 * J + (e & 7);
+    double *out = T + t;
+    if (jb >= nr || j >= nr) {
+        for (int m = 0; m < mmax; ++m) out[m * per_m] = 0.0;
+        return;
+    }
+    const double rs = rhf[j + 1], rsinv = rhfinv[j + 1], zs = zhf[k + 1];
+    const double rb = rhf[jb + 1], rbinv = rhfinv[jb + 1];
+    const double zb = (set == 0) ? zhf[numz - 1] : zhf[0];
+    const bool img = (set == 0) && (isym != 1);
+    const double coef = sqrt(rs * rbinv) * piinv;
+    const double dmi = zb - zs, dpl = zb + zs;
+    const double xm = (isym != 1) ? 0.5 * rsinv * rbinv * (dmi * dmi + rs * rs + rb * rb)
+                                  : 0.5 * rsinv * rbinv * (dmi * dmi + rb * rb + rs * rs);
+    Toroidal tm_, tp_;
+    tor_init(tm_, xm, isym);
+    if (img) tor_init(tp_, 0.5 * rsinv * rbinv * (dpl * dpl + rs * rs + rb * rb), isym);
+    for (int m = 0; m < mmax; ++m) {
+        const double qm = tor_next(tm_, m, qc, mmax, isym);
+        double v;
+        if (img) {
+            const double qp = tor_next(tp_, m, qc, mmax, isym);
+            v = coef * (qp + qm);
+        } else {
+            v = coef * qm;
+        }
+        out[m * per_m] = v * rsinv;
+    }
+}
+
+// Side vectors: one thread per (radial zone j, position in U or V).
+// U_j(d), d = kb - k in [-(nz-1), nz-1], is evaluated at the pair
+// (kb, k) = (|d|, 0); V_j(s), s = kb + k in [0, 2 nz - 2], at
+// (min(s, nz-1), s - min(s, nz-1)); both zero-padded to `stride`.
+// Layout [m][j][U | V][stride].
+__global__ void k_green_compact_side(const double *__restrict__ grid, const double *__restrict__ qc,
+                                     double *__restrict__ Sd, int numr, int nr, int nz, int stride, int mmax,
+                                     int isym, double piinv) {
+    const long long per_m = (long long)nr * 2 * stride;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= per_m) return;
+    const double *rhf = grid, *rhfinv = grid + numr, *zhf = grid + 2 * numr;
+    const int pos = (int)(t % stride);
+    const int which = (int)((t / stride) % 2);  // 0: U, 1: V
+    const int j = (int)(t / (2LL * stride));
+    double *out = Sd + t;
+    int kb, k;
+    bool valid;
+    if (which == 0) {
+        const int d = pos - (nz - 1);
+        kb = d < 0 ? -d : d;
+        k = 0;
+        valid = pos <= 2 * nz - 2;
+    } else {
+        kb = pos < nz - 1 ? pos : nz - 1;
+        k = pos - kb;
+        valid = (isym != 1) && pos <= 2 * nz - 2;
+    }
+    if (!valid) {
+        for (int m = 0; m < mmax; ++m) out[m * per_m] = 0.0;
+        return;
+    }
+    const double rs = rhf[j + 1], rsinv = rhfinv[j + 1], zs = zhf[k + 1];
+    const double rb = rhf[numr - 1], rbinv = 1.0 / rb;
+    const double zb = zhf[kb + 1];
+    const double coef = sqrt(rs * rbinv) * piinv;
+    double x;
+    if (which == 0) {
+        const double dmi = zb - zs;
+        x = (isym != 1) ? 0.5 * rsinv * rbinv * (dmi * dmi + rs * rs + rb * rb)
+                        : 0.5 * rsinv * rbinv * (dmi * dmi + rb * rb + rs * rs);
+    } else {
+        const double dpl = zb + zs;
+        x = 0.5 * rsinv * rbinv * (dpl * dpl + rs * rs + rb * rb);
+    }
+    Toroidal tq;
+    tor_init(tq, x, isym);
+    for (int m = 0; m < mmax; ++m) out[m * per_m] = coef * tor_next(tq, m, qc, mmax, isym);
+}
+
 // Thomas factorisations for one ADI schedule (tridagr.F90:41-60,
 // tridagz.F90:115-132).  Radial: one thread per (step, slot); vertical: one
 // thread per step.  For a line of n unknowns, five arrays of n:
@@ -301,6 +401,20 @@ cudaError_t launch_green_tables(bph_ctx *c) {
                                                                 c->g.numz, c->nr, c->nz, c->nb, c->g.mmax,
                                                                 c->g.isym, 1.0 / c->pi);
     ++c->launches;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_green_compact(bph_ctx *c) {
+    const compact::Dims d = compact::dims(c->nr, c->nz, c->g.isym);
+    const int threads = 128;
+    const long long nt = (long long)d.nsets * d.npair * d.nz * 64;
+    k_green_compact_tiles<<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(
+        c->d_grid, c->d_qcoef, c->d_gtile, c->g.numr, c->g.numz, c->nr, c->nz, d.nb8, d.npair, d.nsets, c->g.mmax,
+        c->g.isym, 1.0 / c->pi);
+    const long long ns = (long long)c->nr * 2 * d.stride;
+    k_green_compact_side<<<(unsigned)((ns + threads - 1) / threads), threads, 0, c->stream>>>(
+        c->d_grid, c->d_qcoef, c->d_gside, c->g.numr, c->nr, c->nz, d.stride, c->g.mmax, c->g.isym, 1.0 / c->pi);
+    c->launches += 2;
     return cudaGetLastError();
 }
 

@@ -63,6 +63,7 @@ MIXED_ADI_AUTO, MIXED_ADI_FORWARD, MIXED_ADI_INCREMENT, MIXED_ADI_GLOBAL, MIXED_
 
 #: bph_info(BPH_INFO_ADI_KERNEL) values.
 ADI_KERNEL_WARP, ADI_KERNEL_SEGMENTED, ADI_KERNEL_ONCHIP, ADI_KERNEL_GRID_WIDE = 1, 2, 3, 4
+CONTRACT_FULL, CONTRACT_COMPACT = 1, 2
 
 #: bph_run_phase phase ids.
 PHASE_FFT_RHO, PHASE_CONTRACT, PHASE_SLOTS, PHASE_ADI, PHASE_FFT_INV = range(5)
@@ -393,7 +394,7 @@ class PotentialSolver:
         """Launch-configuration facts (bph_info)."""
         names = ("adi_threads", "adi_smem", "mixed_threads", "mixed_smem", "mixed_ctas_per_sm", "contract_split",
                  "mixed_kind", "mixed_forward_ns", "mixed_increment_ns", "adi_prefetch", "adi_kernel",
-                 "adi_warp_smem", "mixed_warp_ns", "green_sms")
+                 "adi_warp_smem", "mixed_warp_ns", "green_sms", "contract_kind")
         return {n: int(self._lib.bph_info(self._h, i)) for i, n in enumerate(names)}
 
     def set_mixed_adi(self, kind: int) -> None:

@@ -354,6 +354,9 @@ int bph_green_contract_noalloc(bph_ctx_t *ctx, const double *d_mom, double *d_S)
 #define BPH_INFO_MIXED_WARP_NS 12     /* setup-time duration of a 5-step warp-cooperative refinement launch, ns */
 #define BPH_INFO_GREEN_SMS 13         /* SMs of the contraction's partition in the overlapped solve (0: not requested,
                                          negative: the set-up step that failed) */
+#define BPH_INFO_CONTRACT_KIND 14     /* boundary contraction of the single solve (BPH_CONTRACT_*) */
+#define BPH_CONTRACT_FULL 1           /* streams the full tables G[m][b][p] */
+#define BPH_CONTRACT_COMPACT 2        /* streams the symmetric tiles and side vectors (2/3 fewer bytes) */
 #define BPH_ADI_KERNEL_WARP 1         /* warp-cooperative line solves, shuffle carries (128x96, 64x64 interiors) */
 #define BPH_ADI_KERNEL_SEGMENTED 2    /* CTA-wide segmented line solves (other grids whose slot fits on chip) */
 #define BPH_ADI_KERNEL_ONCHIP 3       /* one thread per line, slot on chip */

@@ -61,6 +61,35 @@ def test_cold_then_warm_matches_oracle(oracle_mod, bph, grid):
     g.close()
 
 
+@pytest.mark.parametrize("kind", ["compact", "full"])
+@pytest.mark.parametrize("grid", SMALL_GRIDS, ids=lambda g: "x".join(map(str, g[:3])) + f"-isym{g[4]}")
+def test_compact_and_full_contractions_match_oracle(oracle_mod, bph, monkeypatch, grid, kind):
+    """The boundary moments S and the potential from the compact tables
+    (symmetric tiles, side windows: the default) and from the full tables
+    (BPH_COMPACT=0 at set-up) against the oracle, which forms every G[m][b][p]."""
+    monkeypatch.setenv("BPH_COMPACT", "1" if kind == "compact" else "0")
+    numr, numz, numphi, dr, isym, _ = grid
+    o, g = _pair(oracle_mod, bph, grid)
+    want = bph.solver.CONTRACT_COMPACT if kind == "compact" else bph.solver.CONTRACT_FULL
+    assert g.info()["contract_kind"] == want
+    rho = smooth_density(numr, numz, numphi, dr, isym, seed=7)
+    pg, po = g.potential_solver(rho, 0), o.potential_solver(rho, 0)
+    assert rel_l2(g.moments_S(), o.moments_S()) <= 1e-13
+    assert rel_l2(pg, po) <= POT_TOL
+    g.close()
+
+
+def test_tall_grid_falls_back_to_full_tables(oracle_mod, bph):
+    """More than 256 interior heights: the side windows do not fit a warp's
+    lanes, so the single solve streams the full tables."""
+    grid = (10, 262, 16, 1.0 / 6.0, 2, 4)
+    o, g = _pair(oracle_mod, bph, grid)
+    assert g.info()["contract_kind"] == bph.solver.CONTRACT_FULL
+    rho = smooth_density(10, 262, 16, 1.0 / 6.0, 2)
+    assert rel_l2(g.potential_solver(rho, 0), o.potential_solver(rho, 0)) <= POT_TOL
+    g.close()
+
+
 def test_tstep_one_is_cold(oracle_mod, bph):
     """tstep > 1 selects the warm start, tstep = 1 is cold (potential_solver.F90:80)."""
     grid = SMALL_GRIDS[0]

@@ -11,6 +11,10 @@
   cover every interior zone exactly once for every slice count and chunk
   length (a chunk that read into the next slice would add those zones
   twice).
+* bph_compact.h: the compact Green-table layout (symmetric tiles of the
+  top and bottom rows, sliding U/V windows of the side rows) contracted
+  with the kernel's index arithmetic equals the dense contraction, for
+  ragged tile edges, odd radial counts and both symmetry classes.
 """
 import os
 import re
@@ -42,6 +46,10 @@ def test_noalloc_plan_limits_and_clamps(tmp_path):
 
 def test_zone_slices_cover_each_zone_once(tmp_path):
     assert "all checks passed" in _run(tmp_path, "zone_slice_check")
+
+
+def test_compact_table_layout_matches_dense_contraction(tmp_path):
+    assert "all checks passed" in _run(tmp_path, "compact_layout_check")
 
 
 def test_library_selects_devices_only_through_the_scope():
