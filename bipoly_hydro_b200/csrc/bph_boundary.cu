@@ -221,17 +221,22 @@ __global__ void k_boundary_slots(const double *__restrict__ S, const double2 *__
 // ---------------------------------------------------------------------------
 // k_green_compact: the same S (and Dirichlet slots) from the compact tables
 // of bph_compact.h.  Grid: mmax x (top_ctas + side_ctas) CTAs of 8 warps.
+// Both roles stage what they read in shared memory with cp.async, so the
+// bytes in flight do not cost registers.
 //
-// Tile warps (one tile (I, J) of one mode over every height k): lane
-// (r = lane / 4, c0 = 2 (lane % 4)) streams elements (r, c0), (r, c0 + 1)
-// of the tile, one 16-byte evict-first load per height, and accumulates
+// Tile warps (one tile (I, J) of one mode over every height k): a ring of
+// kStages heights per warp; lane l copies its 16 bytes of the tile's 512
+// (evict-first) and one of the 32 moments the height needs (cos, sin of
+// the rows 8I.. and the columns 8J..).  Lane (r = l / 4, c0 = 2 (l % 4))
+// then accumulates
 //   row part:    sum_k H(8I + r, 8J + c, k) mom(8J + c, k)   -> S[8I + r]
 //   column part: sum_k H(8I + r, 8J + c, k) mom(8I + r, k)   -> S[8J + c]
-// (the column part is the mirrored tile (J, I), unused when I == J).  The
-// radii r_j of G = H r_j scale the sums at the end; shuffles reduce them
-// over the tile's rows and columns in a fixed order.
+// for c = c0, c0 + 1 (the column part is the mirrored tile (J, I), unused
+// when I == J).  The radii r_j of G = H r_j scale the sums at the end;
+// shuffles reduce them over the tile's rows and columns in a fixed order.
 //
-// Side warps (one radial zone j of one mode): lane holds side rows
+// Side warps (one radial zone j of one mode): the CTA stages the moments of
+// its eight zones and each warp its U and V vectors; lane holds side rows
 // kb = KPL lane + i and slides windows of U_j(kb - k), V_j(kb + k) over k
 // (one new U and one new V value per height), so the side rows cost
 // compute, not table bytes.  The CTA adds its eight zones in shared memory.
@@ -252,16 +257,45 @@ struct CompactArgs {
     SlotOut so;
 };
 
-template <int KPL, bool kVec>
-__global__ void __launch_bounds__(256) k_green_compact(CompactArgs a) {
+constexpr int kStages = 8;       // heights in a tile warp's ring
+constexpr int kStageDoubles = 96;  // 64 tile elements + 32 moments
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cpa16_ef(void *dst, const void *src, unsigned long long pol) {
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src),
+                 "l"(pol)
+                 : "memory");
+}
+__device__ __forceinline__ void cpa16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpa8(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Dynamic shared bytes of a launch: the larger of the tile ring and the
+// side staging (moments of eight zones, U and V of each warp).
+inline size_t compact_smem(int nz, int stride) {
+    const size_t ring = sizeof(double) * compact::kWarps * kStages * kStageDoubles;
+    const size_t side = sizeof(double) * ((size_t)2 * nz * compact::kWarps + (size_t)compact::kWarps * 2 * stride);
+    return ring > side ? ring : side;
+}
+
+template <int KPL>
+__global__ void __launch_bounds__(256, KPL <= 4 ? 3 : 2) k_green_compact(CompactArgs a) {
     using namespace compact;
-    constexpr int kU = 8;  // heights per batch of table loads
+    extern __shared__ __align__(16) double csm[];
     const int per_m = a.top_ctas + a.side_ctas;
     const int m = blockIdx.x / per_m, role = blockIdx.x % per_m;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nr = a.nr, nz = a.nz;
     const long long np = a.np;
-    const double *mc = a.mom + 2LL * m * np, *ms = mc + np;
+    const double *mc = a.mom + 2LL * m * np;
     double *part = a.part + (long long)m * a.part_m;
     __shared__ double red[kWarps][64];
     __shared__ bool last;
@@ -271,57 +305,56 @@ __global__ void __launch_bounds__(256) k_green_compact(CompactArgs a) {
             const int set = q / a.npair, tile = q % a.npair;
             int I, J;
             pair_blocks(tile, a.nb8, &I, &J);
-            const int r = lane >> 2, c0 = 2 * (lane & 3);
-            const int jr = min(kTile * I + r, nr - 1);
-            // column pair (even start when vectorised: nr even keeps it in bounds and aligned)
-            const int jc0 = kVec ? min(kTile * J + c0, nr - 2) : min(kTile * J + c0, nr - 1);
-            const int jc1 = kVec ? jc0 + 1 : min(kTile * J + c0 + 1, nr - 1);
-            const double2 *src =
-                reinterpret_cast<const double2 *>(a.T + (((long long)m * a.nsets + set) * a.npair + tile) * nz * 64) +
-                lane;
-            double r0c = 0.0, r0s = 0.0, r1c = 0.0, r1s = 0.0, k0c = 0.0, k0s = 0.0, k1c = 0.0, k1s = 0.0;
-            double2 t[kU];
+            double *ring = csm + warp * kStages * kStageDoubles;
+            const double *src = a.T + (((long long)m * a.nsets + set) * a.npair + tile) * nz * 64 + 2 * lane;
+            // the moment lane l stages per height: (cos | sin) of row 8I + l % 8 (l % 16 < 8)
+            // or of column 8J + l % 8 (l % 16 >= 8), at slot l of the stage's 32
+            const int cs_l = lane >> 4, idx = lane & 15;
+            const int jl = min(idx < 8 ? kTile * I + idx : kTile * J + idx - 8, nr - 1);
+            const double *msrc = mc + (long long)cs_l * np + jl;
+            unsigned long long evict_first;
+            asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(evict_first));
+            // the first heights' tile bytes before the wait for the producer of the moments
 #pragma unroll
-            for (int u = 0; u < kU; ++u) t[u] = (u < nz) ? __ldcs(src + u * 32) : make_double2(0.0, 0.0);
-            pdl_wait();  // the moments come from the forward transform
-            for (int k0 = 0; k0 < nz; k0 += kU) {
-                double2 tn[kU];
-#pragma unroll
-                for (int u = 0; u < kU; ++u)
-                    tn[u] = (k0 + kU + u < nz) ? __ldcs(src + (k0 + kU + u) * 32) : make_double2(0.0, 0.0);
-#pragma unroll
-                for (int u = 0; u < kU; ++u) {
-                    if (k0 + u < nz) {
-                        const long long off = (long long)nr * (k0 + u);
-                        double xc0, xc1, xs0, xs1;
-                        if (kVec) {
-                            const double2 vc = __ldg(reinterpret_cast<const double2 *>(mc + off + jc0));
-                            const double2 vs = __ldg(reinterpret_cast<const double2 *>(ms + off + jc0));
-                            xc0 = vc.x;
-                            xc1 = vc.y;
-                            xs0 = vs.x;
-                            xs1 = vs.y;
-                        } else {
-                            xc0 = __ldg(mc + off + jc0);
-                            xc1 = __ldg(mc + off + jc1);
-                            xs0 = __ldg(ms + off + jc0);
-                            xs1 = __ldg(ms + off + jc1);
-                        }
-                        const double yc = __ldg(mc + off + jr), ys = __ldg(ms + off + jr);
-                        r0c = fma(t[u].x, xc0, r0c);
-                        r0s = fma(t[u].x, xs0, r0s);
-                        r1c = fma(t[u].y, xc1, r1c);
-                        r1s = fma(t[u].y, xs1, r1s);
-                        k0c = fma(t[u].x, yc, k0c);
-                        k0s = fma(t[u].x, ys, k0s);
-                        k1c = fma(t[u].y, yc, k1c);
-                        k1s = fma(t[u].y, ys, k1s);
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < kU; ++u) t[u] = tn[u];
+            for (int u = 0; u < kStages - 1; ++u) {
+                if (u < nz) cpa16_ef(ring + u * kStageDoubles + 2 * lane, src + (long long)u * 64, evict_first);
             }
+            pdl_wait();
+#pragma unroll
+            for (int u = 0; u < kStages - 1; ++u) {
+                if (u < nz) cpa8(ring + u * kStageDoubles + 64 + lane, msrc + (long long)nr * u);
+                cpa_commit();
+            }
+            const int r = lane >> 2, c0 = 2 * (lane & 3);
+            double r0c = 0.0, r0s = 0.0, r1c = 0.0, r1s = 0.0, k0c = 0.0, k0s = 0.0, k1c = 0.0, k1s = 0.0;
+            for (int k = 0; k < nz; ++k) {
+                cpa_wait<kStages - 2>();
+                __syncwarp();  // every lane's copies of height k have landed; height k - 1 is consumed
+                const int kn = k + kStages - 1;
+                if (kn < nz) {
+                    double *st = ring + (kn % kStages) * kStageDoubles;
+                    cpa16_ef(st + 2 * lane, src + (long long)kn * 64, evict_first);
+                    cpa8(st + 64 + lane, msrc + (long long)nr * kn);
+                }
+                cpa_commit();
+                const double *st = ring + (k % kStages) * kStageDoubles;
+                const double2 t = *reinterpret_cast<const double2 *>(st + 2 * lane);
+                const double2 xc = *reinterpret_cast<const double2 *>(st + 64 + 8 + c0);
+                const double2 xs = *reinterpret_cast<const double2 *>(st + 64 + 16 + 8 + c0);
+                const double yc = st[64 + r], ys = st[64 + 16 + r];
+                r0c = fma(t.x, xc.x, r0c);
+                r0s = fma(t.x, xs.x, r0s);
+                r1c = fma(t.y, xc.y, r1c);
+                r1s = fma(t.y, xs.y, r1s);
+                k0c = fma(t.x, yc, k0c);
+                k0s = fma(t.x, ys, k0s);
+                k1c = fma(t.y, yc, k1c);
+                k1s = fma(t.y, ys, k1s);
+            }
+            cpa_wait<0>();
             // G = H r_j: the row part takes the columns' radii, the column part the row's
+            const int jr = min(kTile * I + r, nr - 1);
+            const int jc0 = min(kTile * J + c0, nr - 1), jc1 = min(kTile * J + c0 + 1, nr - 1);
             const double wr = a.rw[jr], w0 = a.rw[jc0], w1 = a.rw[jc1];
             double rc = w0 * r0c + w1 * r1c, rs = w0 * r0s + w1 * r1s;
             double cc0 = wr * k0c, cs0 = wr * k0s, cc1 = wr * k1c, cs1 = wr * k1s;
@@ -354,25 +387,40 @@ __global__ void __launch_bounds__(256) k_green_compact(CompactArgs a) {
     } else {
         const int g = role - a.top_ctas;
         const int j = g * kWarps + warp;
+        // staging: moments [cs][k][8 zones], then U | V of each warp
+        double *msh = csm;
+        double *uvw = csm + 2 * nz * kWarps + (long long)warp * 2 * a.stride;
+        if (j < nr) {
+            const double *Uv = a.U + ((long long)m * nr + j) * 2 * a.stride;
+            for (int c = lane; c < a.stride; c += 32) cpa16(uvw + 2 * c, Uv + 2 * c);  // 2 stride doubles
+        }
+        pdl_wait();
+        for (int e = threadIdx.x; e < 2 * nz * kWarps; e += blockDim.x) {
+            const int jj = e % kWarps, k = (e / kWarps) % nz, cs = e / (kWarps * nz);
+            const int jz = min(g * kWarps + jj, nr - 1);
+            cpa8(msh + e, mc + (long long)cs * np + jz + (long long)nr * k);
+        }
+        cpa_commit();
+        cpa_wait<0>();
+        __syncthreads();
         double acc_c[KPL], acc_s[KPL];
 #pragma unroll
         for (int i = 0; i < KPL; ++i) acc_c[i] = acc_s[i] = 0.0;
         if (j < nr) {
-            const double *Uv = a.U + ((long long)m * nr + j) * 2 * a.stride, *Vv = Uv + a.stride;
+            const double *Uv = uvw, *Vv = uvw + a.stride;
             const int base = KPL * lane;
             double u[KPL], v[KPL];
 #pragma unroll
             for (int i = 0; i < KPL; ++i) {
-                u[i] = __ldg(Uv + base + i + nz - 1);
-                v[i] = __ldg(Vv + base + i);
+                u[i] = Uv[base + i + nz - 1];
+                v[i] = Vv[base + i];
             }
-            pdl_wait();
-            const double *mcj = mc + j, *msj = ms + j;
+            const double *mcol = msh + warp, *mcol_s = msh + nz * kWarps + warp;
 #pragma unroll 4
             for (int k = 0; k < nz; ++k) {
-                const double xc = __ldg(mcj + (long long)nr * k), xs = __ldg(msj + (long long)nr * k);
-                const double un = (k + 1 < nz) ? __ldg(Uv + base + nz - 2 - k) : 0.0;
-                const double vn = (k + 1 < nz) ? __ldg(Vv + base + KPL + k) : 0.0;
+                const double xc = mcol[k * kWarps], xs = mcol_s[k * kWarps];
+                const double un = (k + 1 < nz) ? Uv[base + nz - 2 - k] : 0.0;
+                const double vn = (k + 1 < nz) ? Vv[base + KPL + k] : 0.0;
 #pragma unroll
                 for (int i = 0; i < KPL; ++i) {
                     const double w = u[i] + v[i];
@@ -386,8 +434,6 @@ __global__ void __launch_bounds__(256) k_green_compact(CompactArgs a) {
                 for (int i = 0; i + 1 < KPL; ++i) v[i] = v[i + 1];
                 v[KPL - 1] = vn;
             }
-        } else {
-            pdl_wait();
         }
         // the CTA's eight zones, added in warp order, one window position at a time
         double *ps = part + (long long)a.nsets * a.npair * kPartPair + (long long)g * nz * 2;
@@ -449,6 +495,19 @@ __global__ void __launch_bounds__(256) k_green_compact(CompactArgs a) {
     if (threadIdx.x == 0) a.cnt[m] = 0u;
 }
 
+const void *compact_kernel(int kpl) {
+    switch (kpl) {
+        case 1: return (const void *)k_green_compact<1>;
+        case 2: return (const void *)k_green_compact<2>;
+        case 3: return (const void *)k_green_compact<3>;
+        case 4: return (const void *)k_green_compact<4>;
+        case 5: return (const void *)k_green_compact<5>;
+        case 6: return (const void *)k_green_compact<6>;
+        case 7: return (const void *)k_green_compact<7>;
+        default: return (const void *)k_green_compact<8>;
+    }
+}
+
 }  // namespace
 
 int contract_configure(bph_ctx *c) {
@@ -492,18 +551,12 @@ int compact_configure(bph_ctx *c) {
     if (e == cudaSuccess) e = cudaMemsetAsync(c->d_kcnt, 0, sizeof(unsigned int) * mm, c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "compact Green tables");
     c->bytes += sizeof(double) * (nt + ns + np) + sizeof(unsigned int) * mm;
+    e = raise_smem_limit(compact_kernel(d.kpl), (int)compact_smem(d.nz, d.stride));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_green_compact)");
     e = launch_green_compact(c);
     if (e != cudaSuccess) return cuda_fail(e, "k_green_compact_tiles / k_green_compact_side");
     c->compact = 1;
     return BPH_OK;
-}
-
-template <int KPL>
-cudaError_t launch_compact_kpl(bph_ctx *c, const CompactArgs &a, unsigned grid) {
-    cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = launch_config(c, dim3(grid), dim3(256), 0, attr);
-    if (c->nr % 2 == 0) return cudaLaunchKernelEx(&cfg, k_green_compact<KPL, true>, a);
-    return cudaLaunchKernelEx(&cfg, k_green_compact<KPL, false>, a);
 }
 
 cudaError_t launch_green_compact_contract(bph_ctx *c, bool write_slots) {
@@ -538,16 +591,10 @@ cudaError_t launch_green_compact_contract(bph_ctx *c, bool write_slots) {
     a.so.nfactor = (double)c->N * c->factor;
     ++c->launches;
     const unsigned grid = (unsigned)(c->g.mmax * (d.top_ctas + d.side_ctas));
-    switch (d.kpl) {
-        case 1: return launch_compact_kpl<1>(c, a, grid);
-        case 2: return launch_compact_kpl<2>(c, a, grid);
-        case 3: return launch_compact_kpl<3>(c, a, grid);
-        case 4: return launch_compact_kpl<4>(c, a, grid);
-        case 5: return launch_compact_kpl<5>(c, a, grid);
-        case 6: return launch_compact_kpl<6>(c, a, grid);
-        case 7: return launch_compact_kpl<7>(c, a, grid);
-        default: return launch_compact_kpl<8>(c, a, grid);
-    }
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = launch_config(c, dim3(grid), dim3(256), compact_smem(d.nz, d.stride), attr);
+    void *args[] = {&a};
+    return cudaLaunchKernelExC(&cfg, compact_kernel(d.kpl), args);
 }
 
 cudaError_t launch_green_contract(bph_ctx *c, bool write_slots) {

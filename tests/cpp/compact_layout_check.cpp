@@ -78,10 +78,8 @@ static void check(int nr, int nz, int isym) {
         double lane_r[32][2], lane_c[32][2][2];
         for (int lane = 0; lane < 32; ++lane) {
             const int r = lane >> 2, c0 = 2 * (lane & 3);
-            const bool vec = nr % 2 == 0;
             const int jr = std::min(kTile * I + r, nr - 1);
-            const int jc0 = vec ? std::min(kTile * J + c0, nr - 2) : std::min(kTile * J + c0, nr - 1);
-            const int jc1 = vec ? jc0 + 1 : std::min(kTile * J + c0 + 1, nr - 1);
+            const int jc0 = std::min(kTile * J + c0, nr - 1), jc1 = std::min(kTile * J + c0 + 1, nr - 1);
             double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             for (int k = 0; k < nz; ++k) {
                 const double *t = &T[(((size_t)set * d.npair + tile) * nz + k) * 64 + 2 * lane];

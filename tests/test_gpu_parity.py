@@ -433,6 +433,7 @@ def test_converged_loop_on_device_equals_host_loop(bph, monkeypatch):
     for flag in ("1", "0"):
         monkeypatch.setenv("BPH_CONV_GRAPH", flag)
         g = bph.PotentialSolver(*grid)
+        g.set_mixed_adi(bph.solver.MIXED_ADI_FORWARD)  # the same refinement kernel in both (no timing-based choice)
         p1, i1 = g.solve_converged(rho, 10, True, 1e-12, 100)
         p2, i2 = g.solve_converged(rho2, 10, False, 1e-12, 100)
         m1, j1 = g.solve_converged_mixed(rho2, 10, False, 1e-12, 100)
