@@ -26,9 +26,12 @@
 #include <utility>
 
 #include "bph_internal.cuh"
+#include "bph_bulk.h"
 
 namespace bph {
 namespace {
+
+using namespace bulk;
 
 constexpr int kAdiThreads = 256;
 
@@ -306,47 +309,6 @@ __device__ inline void fac_load(T *base, int n, const double *src, int tid, int 
 // before its first read).  Waits are bounded: an expired wait sets
 // kStatusTimeout and the kernel runs on (its results are then reported
 // invalid), so no CTA can hang on a copy.
-__device__ __forceinline__ uint32_t smem_addr(const void *p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-
-// One thread: order this CTA's earlier generic-proxy accesses of dst before
-// the async-proxy write, then copy bytes (multiple of 16, both addresses
-// 16-byte aligned) from global src to shared dst, completing on bar.
-__device__ __forceinline__ void bulk_fill(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_addr(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-constexpr int kWaitSpins = 1 << 20;  // try_wait rounds (each suspends at most a short hardware interval)
-
-__device__ __forceinline__ void mbar_wait(uint64_t *bar, uint32_t parity, int *status) {
-    for (int i = 0; i < kWaitSpins; ++i)
-        if (mbar_try_wait(bar, parity)) return;
-    atomicOr(status, kStatusTimeout);
-}
-
 // Shared-memory layout of the prefetching segmented kernel, byte offsets.
 struct PfLayout {
     int ps, Pr, Pz, xsz, fpf;  // fpf: elements per factor block (both directions)

@@ -18,6 +18,7 @@
 #include <cstring>
 #include <vector>
 
+#include "bph_compact.h"
 #include "bph_internal.cuh"
 
 namespace bph {
@@ -348,7 +349,7 @@ int setup_impl(bph_ctx *c) {
     if ((rc = dev_alloc(c, &c->d_green, (size_t)g.mmax * c->nb * c->np))) return rc;
     if ((rc = dev_alloc(c, &c->d_R, (size_t)c->N * c->np))) return rc;
     if ((rc = dev_alloc(c, &c->d_P, (size_t)c->N * c->nplane))) return rc;
-    if ((rc = dev_alloc(c, &c->d_mom, (size_t)2 * g.mmax * c->np))) return rc;
+    if ((rc = dev_alloc(c, &c->d_mom, (size_t)2 * g.mmax * c->np + compact::kMomPad))) return rc;
     if ((rc = dev_alloc(c, &c->d_S, (size_t)2 * g.mmax * c->nb))) return rc;
     if ((rc = dev_alloc(c, &c->d_brb, (size_t)c->N * g.numr))) return rc;
     if ((rc = dev_alloc(c, &c->d_elz, (size_t)c->N * g.numr))) return rc;
@@ -375,6 +376,7 @@ int setup_impl(bph_ctx *c) {
     if ((rc = upload(c, c->d_ph, ph.data(), sizeof(double2) * ph.size()))) return rc;
     BPH_CUDA(cudaMemsetAsync(c->d_P, 0, sizeof(double) * (size_t)c->N * c->nplane, c->stream));
     BPH_CUDA(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+    BPH_CUDA(cudaMemsetAsync(c->d_mom + (size_t)2 * g.mmax * c->np, 0, sizeof(double) * compact::kMomPad, c->stream));
 
     {
         const char *pdl = std::getenv("BPH_PDL");
@@ -535,7 +537,7 @@ int read_status(bph_ctx *c) {
         return BPH_ERR_NONFINITE;
     }
     if (st & kStatusTimeout) {
-        set_error("a bounded device wait expired (ADI factor bulk copy); results are not valid");
+        set_error("a bounded device wait expired (bulk copy of ADI factors or Green tables); results are not valid");
         return BPH_ERR_TIMEOUT;
     }
     return BPH_OK;

@@ -220,45 +220,54 @@ __global__ void k_boundary_slots(const double *__restrict__ S, const double2 *__
 
 // ---------------------------------------------------------------------------
 // k_green_compact: the same S (and Dirichlet slots) from the compact tables
-// of bph_compact.h.  Grid: mmax x (top_ctas + side_ctas) CTAs of 8 warps.
+// of bph_compact.h.  One CTA of 8 warps per work item, items mode-major;
+// an item is one height part (compact::kHeightParts of them; splitting
+// the heights evens out the last wave but costs more than it saves at
+// 130x98, so one part is the default) of a mode's set of 8 tiles or of a
+// group of 8 side zones.
 // Both roles stage what they read in shared memory with cp.async, so the
 // bytes in flight do not cost registers.
 //
-// Tile warps (one tile (I, J) of one mode over every height k): a ring of
-// kStages heights per warp; lane l copies its 16 bytes of the tile's 512
-// (evict-first) and one of the 32 moments the height needs (cos, sin of
-// the rows 8I.. and the columns 8J..).  Lane (r = l / 4, c0 = 2 (l % 4))
-// then accumulates
+// Tile warps (one tile (I, J) over the item's heights): a ring of kRing
+// stages of kStageH heights per warp; lane l copies its 16 bytes of each
+// height's 512 (evict-first) and one of the 32 moments a height needs
+// ((cos, sin) pairs of the rows 8I.. and the columns 8J..).  Lane
+// (r = l / 4, c0 = 2 (l % 4)) then accumulates
 //   row part:    sum_k H(8I + r, 8J + c, k) mom(8J + c, k)   -> S[8I + r]
 //   column part: sum_k H(8I + r, 8J + c, k) mom(8I + r, k)   -> S[8J + c]
 // for c = c0, c0 + 1 (the column part is the mirrored tile (J, I), unused
 // when I == J).  The radii r_j of G = H r_j scale the sums at the end;
 // shuffles reduce them over the tile's rows and columns in a fixed order.
 //
-// Side warps (one radial zone j of one mode): the CTA stages the moments of
-// its eight zones and each warp its U and V vectors; lane holds side rows
-// kb = KPL lane + i and slides windows of U_j(kb - k), V_j(kb + k) over k
-// (one new U and one new V value per height), so the side rows cost
-// compute, not table bytes.  The CTA adds its eight zones in shared memory.
+// Side warps (one radial zone j over the item's heights): the CTA stages
+// the moments of its eight zones and each warp its U and V vectors; lane
+// holds side rows kb = KPL lane + i and slides windows of U_j(kb - k),
+// V_j(kb + k) over k (one new U and one new V value per height), so the
+// side rows cost compute, not table bytes.  The CTA adds its eight zones in
+// shared memory.
 //
-// Every CTA writes partial sums; the last CTA of each mode to arrive adds
-// them in a fixed order (deterministic), writes S and the slots, and resets
-// the mode's arrival counter for the next launch.
+// Reduction in three fixed-order levels (deterministic): every item writes
+// its partial sums; the last of a tile set's (or side group's) height parts
+// to arrive adds the parts; the last of a mode's tile sets and side groups
+// adds those per boundary row, writes S and the slots, and resets the
+// counters for the next launch.
 struct CompactArgs {
-    const double *T;    // tiles [m][set][tile][k][64]
+    const double *T;    // tiles [m][set][k < nzp][tile][64]
     const double *U;    // side vectors [m][j][U | V][stride]
     const double *mom;  // moments [2m + cs][np]
     const double *rw;   // r_j, j < nr
     double *S;          // [m][nb][2]
-    double *part;       // per mode: tile parts [set][tile][32], then side parts [side CTA][nz][2]
-    unsigned int *cnt;  // [mmax]
-    long long np, part_m;
-    int nr, nz, nb, nb8, npair, nsets, stride, top_ctas, side_ctas;
+    double *part;       // per mode and height part: tile parts [set][tile][32], then side parts [group][nz][2]
+    unsigned int *cnt;  // arrival counters (compact::counters)
+    long long np, part_m, part_h;
+    int nr, nz, nzp, nb, nb8, npair, nsets, stride, top_ctas, side_ctas, mmax, nh, hp;
     SlotOut so;
 };
 
-constexpr int kStages = 8;       // heights in a tile warp's ring
-constexpr int kStageDoubles = 96;  // 64 tile elements + 32 moments
+constexpr int kRing = 4;                            // stages in a tile warp's ring
+constexpr int kStageH = compact::kStageHeights;     // heights per stage
+constexpr int kHeightDoubles = 64 + 32;     // a height: 64 tile elements, 16 (cos, sin) moment pairs
+constexpr int kStageDoubles = kStageH * kHeightDoubles;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void cpa16_ef(void *dst, const void *src, unsigned long long pol) {
@@ -272,84 +281,129 @@ __device__ __forceinline__ void cpa16(void *dst, const void *src) {
 __device__ __forceinline__ void cpa8(void *dst, const void *src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cpa16_ef_u(uint32_t dst, const void *src, unsigned long long pol) {
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "l"(pol)
+                 : "memory");
+}
+__device__ __forceinline__ void cpa8_u(uint32_t dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cpa_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Dynamic shared bytes of a launch: the larger of the tile ring and the
-// side staging (moments of eight zones, U and V of each warp).
-inline size_t compact_smem(int nz, int stride) {
-    const size_t ring = sizeof(double) * compact::kWarps * kStages * kStageDoubles;
-    const size_t side = sizeof(double) * ((size_t)2 * nz * compact::kWarps + (size_t)compact::kWarps * 2 * stride);
+// Dynamic shared bytes: the larger of the tile rings and the side staging
+// (moment pairs of eight zones over a height part, U and V of each warp).
+inline size_t compact_smem(int hp, int stride) {
+    const size_t ring = sizeof(double) * compact::kWarps * kRing * kStageDoubles;
+    const size_t side = sizeof(double) * ((size_t)2 * compact::kWarps * hp + (size_t)compact::kWarps * 2 * stride);
     return ring > side ? ring : side;
 }
 
+// One work item (see k_green_compact below); `it` is the item's index.
 template <int KPL>
-__global__ void __launch_bounds__(256, KPL <= 4 ? 3 : 2) k_green_compact(CompactArgs a) {
+__device__ __forceinline__ void compact_item(const CompactArgs &a, int it, double *csm, double (*red)[64],
+                                             bool &last) {
     using namespace compact;
-    extern __shared__ __align__(16) double csm[];
-    const int per_m = a.top_ctas + a.side_ctas;
-    const int m = blockIdx.x / per_m, role = blockIdx.x % per_m;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nr = a.nr, nz = a.nz;
     const long long np = a.np;
+    const int per_m = a.top_ctas + a.side_ctas;
+    const int per_mode_items = a.nh * per_m;
+    const int m = it / per_mode_items;
+    const int rem = it % per_mode_items;
+    const int h = rem / per_m, role = rem % per_m;
+    const int k0 = min(h * a.hp, nz), k1 = min(k0 + a.hp, nz);
     const double *mc = a.mom + 2LL * m * np;
-    double *part = a.part + (long long)m * a.part_m;
-    __shared__ double red[kWarps][64];
-    __shared__ bool last;
+    double *pmode = a.part + (long long)m * a.part_m;
+    double *part = pmode + (long long)h * a.part_h;
+    const long long top_doubles = (long long)a.nsets * a.npair * kPartPair;
     if (role < a.top_ctas) {
         const int q = role * kWarps + warp;
-        if (q < a.nsets * a.npair) {
+        if (q < a.nsets * a.npair && k1 > k0) {
             const int set = q / a.npair, tile = q % a.npair;
             int I, J;
             pair_blocks(tile, a.nb8, &I, &J);
-            double *ring = csm + warp * kStages * kStageDoubles;
-            const double *src = a.T + (((long long)m * a.nsets + set) * a.npair + tile) * nz * 64 + 2 * lane;
-            // the moment lane l stages per height: (cos | sin) of row 8I + l % 8 (l % 16 < 8)
-            // or of column 8J + l % 8 (l % 16 >= 8), at slot l of the stage's 32
-            const int cs_l = lane >> 4, idx = lane & 15;
-            const int jl = min(idx < 8 ? kTile * I + idx : kTile * J + idx - 8, nr - 1);
-            const double *msrc = mc + (long long)cs_l * np + jl;
-            unsigned long long evict_first;
-            asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(evict_first));
-            // the first heights' tile bytes before the wait for the producer of the moments
-#pragma unroll
-            for (int u = 0; u < kStages - 1; ++u) {
-                if (u < nz) cpa16_ef(ring + u * kStageDoubles + 2 * lane, src + (long long)u * 64, evict_first);
-            }
-            pdl_wait();
-#pragma unroll
-            for (int u = 0; u < kStages - 1; ++u) {
-                if (u < nz) cpa8(ring + u * kStageDoubles + 64 + lane, msrc + (long long)nr * u);
-                cpa_commit();
-            }
+            double *ring = csm + warp * kRing * kStageDoubles;
+            const long long hstride = (long long)a.npair * 64;  // doubles between heights of a tile
+            const int nst = (k1 - k0 + kStageH - 1) / kStageH;
             const int r = lane >> 2, c0 = 2 * (lane & 3);
             double r0c = 0.0, r0s = 0.0, r1c = 0.0, r1s = 0.0, k0c = 0.0, k0s = 0.0, k1c = 0.0, k1s = 0.0;
-            for (int k = 0; k < nz; ++k) {
-                cpa_wait<kStages - 2>();
-                __syncwarp();  // every lane's copies of height k have landed; height k - 1 is consumed
-                const int kn = k + kStages - 1;
-                if (kn < nz) {
-                    double *st = ring + (kn % kStages) * kStageDoubles;
-                    cpa16_ef(st + 2 * lane, src + (long long)kn * 64, evict_first);
-                    cpa8(st + 64 + lane, msrc + (long long)nr * kn);
+            unsigned long long evict_first;
+            asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(evict_first));
+            // the lane's table bytes and moment of height k0; both advance by fixed strides per height
+            const double *tnext =
+                a.T + ((long long)m * a.nsets + set) * a.nzp * hstride + (long long)k0 * hstride + tile * 64 + 2 * lane;
+            // moment lane l stages per height: pair l / 2 (rows 8I.. for l / 2 < 8, columns 8J.. after),
+            // component l % 2 (cos, sin), at slot l of the height's 32; heights past nz (zero tiles)
+            // read the last height's moment
+            const int idx = lane >> 1, cs_l = lane & 1;
+            const int jl = min(idx < 8 ? kTile * I + idx : kTile * J + idx - 8, nr - 1);
+            const double *mnext = mc + (long long)cs_l * np + jl + (long long)nr * k0;
+            const double *mlast = mc + (long long)cs_l * np + jl + (long long)nr * (nz - 1);
+            int knext = k0;
+            const uint32_t tdst = smem_u32(ring) + 16 * lane, mdst = smem_u32(ring) + 8 * (64 + lane);
+            constexpr uint32_t kStageBytes = 8 * kStageDoubles, kHeightBytes = 8 * kHeightDoubles;
+            // the first stages' table bytes, then their moments
+            {
+                const double *t = tnext;
+#pragma unroll
+                for (int u = 0; u < kRing - 1; ++u)
+#pragma unroll
+                    for (int hh = 0; hh < kStageH; ++hh) {
+                        if (u < nst) cpa16_ef_u(tdst + u * kStageBytes + hh * kHeightBytes, t, evict_first);
+                        t += hstride;
+                    }
+            }
+            pdl_wait();  // the moments come from the forward transform
+#pragma unroll
+            for (int u = 0; u < kRing - 1; ++u) {
+                if (u < nst) {
+#pragma unroll
+                    for (int hh = 0; hh < kStageH; ++hh) {
+                        cpa8_u(mdst + u * kStageBytes + hh * kHeightBytes, knext < nz ? mnext : mlast);
+                        tnext += hstride;
+                        mnext += nr;
+                        ++knext;
+                    }
                 }
                 cpa_commit();
-                const double *st = ring + (k % kStages) * kStageDoubles;
-                const double2 t = *reinterpret_cast<const double2 *>(st + 2 * lane);
-                const double2 xc = *reinterpret_cast<const double2 *>(st + 64 + 8 + c0);
-                const double2 xs = *reinterpret_cast<const double2 *>(st + 64 + 16 + 8 + c0);
-                const double yc = st[64 + r], ys = st[64 + 16 + r];
-                r0c = fma(t.x, xc.x, r0c);
-                r0s = fma(t.x, xs.x, r0s);
-                r1c = fma(t.y, xc.y, r1c);
-                r1s = fma(t.y, xs.y, r1s);
-                k0c = fma(t.x, yc, k0c);
-                k0s = fma(t.x, ys, k0s);
-                k1c = fma(t.y, yc, k1c);
-                k1s = fma(t.y, ys, k1s);
+            }
+            for (int sidx = 0; sidx < nst; ++sidx) {
+                cpa_wait<kRing - 2>();
+                __syncwarp();  // stage sidx has landed for every lane; stage sidx - 1 is consumed
+                if (sidx + kRing - 1 < nst) {
+                    const uint32_t so = ((sidx + kRing - 1) & (kRing - 1)) * kStageBytes;
+#pragma unroll
+                    for (int hh = 0; hh < kStageH; ++hh) {
+                        cpa16_ef_u(tdst + so + hh * kHeightBytes, tnext, evict_first);
+                        cpa8_u(mdst + so + hh * kHeightBytes, knext < nz ? mnext : mlast);
+                        tnext += hstride;
+                        mnext += nr;
+                        ++knext;
+                    }
+                }
+                cpa_commit();
+                const double *st = ring + (sidx & (kRing - 1)) * kStageDoubles;
+#pragma unroll
+                for (int hh = 0; hh < kStageH; ++hh) {
+                    // heights past k1 within the last stage are zero tiles (padding above nz)
+                    const double *sh = st + hh * kHeightDoubles;
+                    const double2 t = *reinterpret_cast<const double2 *>(sh + 2 * lane);
+                    const double2 x0 = *reinterpret_cast<const double2 *>(sh + 64 + 2 * (8 + c0));
+                    const double2 x1 = *reinterpret_cast<const double2 *>(sh + 64 + 2 * (9 + c0));
+                    const double2 y = *reinterpret_cast<const double2 *>(sh + 64 + 2 * r);
+                    r0c = fma(t.x, x0.x, r0c);
+                    r0s = fma(t.x, x0.y, r0s);
+                    r1c = fma(t.y, x1.x, r1c);
+                    r1s = fma(t.y, x1.y, r1s);
+                    k0c = fma(t.x, y.x, k0c);
+                    k0s = fma(t.x, y.y, k0s);
+                    k1c = fma(t.y, y.x, k1c);
+                    k1s = fma(t.y, y.y, k1s);
+                }
             }
             cpa_wait<0>();
             // G = H r_j: the row part takes the columns' radii, the column part the row's
@@ -383,22 +437,24 @@ __global__ void __launch_bounds__(256, KPL <= 4 ? 3 : 2) k_green_compact(Compact
             }
         } else {
             pdl_wait();
+            if (q < a.nsets * a.npair) part[(long long)q * kPartPair + lane] = 0.0;  // an empty height part
         }
     } else {
         const int g = role - a.top_ctas;
         const int j = g * kWarps + warp;
-        // staging: moments [cs][k][8 zones], then U | V of each warp
+        const int hk = k1 - k0;
+        // staging: moment pairs [k - k0][8 zones][cos, sin], then U | V of each warp
         double *msh = csm;
-        double *uvw = csm + 2 * nz * kWarps + (long long)warp * 2 * a.stride;
+        double *uvw = csm + 2 * kWarps * a.hp + (long long)warp * 2 * a.stride;
         if (j < nr) {
             const double *Uv = a.U + ((long long)m * nr + j) * 2 * a.stride;
             for (int c = lane; c < a.stride; c += 32) cpa16(uvw + 2 * c, Uv + 2 * c);  // 2 stride doubles
         }
         pdl_wait();
-        for (int e = threadIdx.x; e < 2 * nz * kWarps; e += blockDim.x) {
-            const int jj = e % kWarps, k = (e / kWarps) % nz, cs = e / (kWarps * nz);
+        for (int e = threadIdx.x; e < 2 * kWarps * hk; e += blockDim.x) {
+            const int cs = e & 1, jj = (e >> 1) & (kWarps - 1), kk = e >> 4;
             const int jz = min(g * kWarps + jj, nr - 1);
-            cpa8(msh + e, mc + (long long)cs * np + jz + (long long)nr * k);
+            cpa8(msh + e, mc + (long long)cs * np + jz + (long long)nr * (k0 + kk));
         }
         cpa_commit();
         cpa_wait<0>();
@@ -406,37 +462,45 @@ __global__ void __launch_bounds__(256, KPL <= 4 ? 3 : 2) k_green_compact(Compact
         double acc_c[KPL], acc_s[KPL];
 #pragma unroll
         for (int i = 0; i < KPL; ++i) acc_c[i] = acc_s[i] = 0.0;
-        if (j < nr) {
+        if (j < nr && hk > 0) {
             const double *Uv = uvw, *Vv = uvw + a.stride;
             const int base = KPL * lane;
-            double u[KPL], v[KPL];
+            // windows as rings: at step s = k - kb of a block of KPL heights,
+            // U_j(kb_i - k) = uu[(i - s) mod KPL] and V_j(kb_i + k) = vv[(i + s) mod KPL];
+            // the value that leaves each window is replaced in place (no moves)
+            double uu[KPL], vv[KPL];
 #pragma unroll
             for (int i = 0; i < KPL; ++i) {
-                u[i] = Uv[base + i + nz - 1];
-                v[i] = Vv[base + i];
+                uu[i] = Uv[base + i + nz - 1 - k0];
+                vv[i] = Vv[base + i + k0];
             }
-            const double *mcol = msh + warp, *mcol_s = msh + nz * kWarps + warp;
-#pragma unroll 4
-            for (int k = 0; k < nz; ++k) {
-                const double xc = mcol[k * kWarps], xs = mcol_s[k * kWarps];
-                const double un = (k + 1 < nz) ? Uv[base + nz - 2 - k] : 0.0;
-                const double vn = (k + 1 < nz) ? Vv[base + KPL + k] : 0.0;
+            const double2 *mp = reinterpret_cast<const double2 *>(msh) + warp;
+            // the values entering the windows at the next height; after the last height the U
+            // pointer reads one element before this warp's vectors (staged memory, never used)
+            const double *up = Uv + base + nz - 2 - k0, *vp = Vv + base + KPL + k0;
+            for (int kb = k0; kb < k1; kb += KPL) {
 #pragma unroll
-                for (int i = 0; i < KPL; ++i) {
-                    const double w = u[i] + v[i];
-                    acc_c[i] = fma(w, xc, acc_c[i]);
-                    acc_s[i] = fma(w, xs, acc_s[i]);
+                for (int st = 0; st < KPL; ++st) {
+                    if (kb + st < k1) {
+                        const double2 x = *mp;
+                        const double un = *up, vn = *vp;
+                        mp += kWarps;
+                        --up;
+                        ++vp;
+#pragma unroll
+                        for (int i = 0; i < KPL; ++i) {
+                            const double w = uu[(i - st + KPL) % KPL] + vv[(i + st) % KPL];
+                            acc_c[i] = fma(w, x.x, acc_c[i]);
+                            acc_s[i] = fma(w, x.y, acc_s[i]);
+                        }
+                        uu[KPL - 1 - st] = un;
+                        vv[st] = vn;
+                    }
                 }
-#pragma unroll
-                for (int i = KPL - 1; i > 0; --i) u[i] = u[i - 1];
-                u[0] = un;
-#pragma unroll
-                for (int i = 0; i + 1 < KPL; ++i) v[i] = v[i + 1];
-                v[KPL - 1] = vn;
             }
         }
         // the CTA's eight zones, added in warp order, one window position at a time
-        double *ps = part + (long long)a.nsets * a.npair * kPartPair + (long long)g * nz * 2;
+        double *ps = part + top_doubles + (long long)g * nz * 2;
 #pragma unroll
         for (int i = 0; i < KPL; ++i) {
             red[warp][2 * lane] = acc_c[i];
@@ -453,35 +517,61 @@ __global__ void __launch_bounds__(256, KPL <= 4 ? 3 : 2) k_green_compact(Compact
         }
     }
     pdl_trigger();
+    // level 2: the last height part of this tile set / side group adds the parts
+    unsigned int *mcnt = a.cnt, *rcnt = a.cnt + a.mmax;
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = (atomicAdd(a.cnt + m, 1u) == (unsigned)(per_m - 1));
+    if (threadIdx.x == 0) last = (atomicAdd(rcnt + (long long)m * per_m + role, 1u) == (unsigned)(a.nh - 1));
     __syncthreads();
     if (!last) return;
     __threadfence();
-    const double *pside = part + (long long)a.nsets * a.npair * kPartPair;
+    double *merged = pmode + (long long)a.nh * a.part_h;
+    if (role < a.top_ctas) {
+        const int q = role * kWarps + warp;
+        if (q < a.nsets * a.npair) {
+            double t = 0.0;
+            for (int hh = 0; hh < a.nh; ++hh) t += __ldcg(pmode + (long long)hh * a.part_h + (long long)q * kPartPair + lane);
+            merged[(long long)q * kPartPair + lane] = t;
+        }
+    } else {
+        const long long off = top_doubles + (long long)(role - a.top_ctas) * nz * 2;
+        for (int e = threadIdx.x; e < 2 * nz; e += blockDim.x) {
+            double t = 0.0;
+            for (int hh = 0; hh < a.nh; ++hh) t += __ldcg(pmode + (long long)hh * a.part_h + off + e);
+            merged[off + e] = t;
+        }
+    }
+    if (threadIdx.x == 0) rcnt[(long long)m * per_m + role] = 0u;
+    // level 3: the last tile set / side group of the mode adds the merged parts per boundary row
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(mcnt + m, 1u) == (unsigned)(per_m - 1));
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
     for (int b = threadIdx.x; b < a.nb; b += blockDim.x) {
         double sc = 0.0, ss = 0.0;
         if (b < nr || b >= nr + nz) {
             const int set = (b < nr) ? 0 : 1;
             const int jb = (b < nr) ? b : b - nr - nz;
             const int I = jb / kTile, r = jb % kTile;
-            const double *pt = part + (long long)set * a.npair * kPartPair;
-            for (int Ip = 0; Ip < I; ++Ip) {
-                const double *pp = pt + (long long)pair_index(Ip, I, a.nb8) * kPartPair + 16 + 2 * r;
-                sc += __ldcg(pp);
-                ss += __ldcg(pp + 1);
-            }
-            for (int Jp = I; Jp < a.nb8; ++Jp) {
-                const double *pp = pt + (long long)pair_index(I, Jp, a.nb8) * kPartPair + 2 * r;
-                sc += __ldcg(pp);
-                ss += __ldcg(pp + 1);
+            const double *pt = merged + (long long)set * a.npair * kPartPair;
+            // column parts of tiles (I', I), I' < I, then row parts of tiles (I, J), J >= I
+#pragma unroll 8
+            for (int t = 0; t < a.nb8; ++t) {
+                const double *pp = (t < I) ? pt + (long long)pair_index(t, I, a.nb8) * kPartPair + 16 + 2 * r
+                                           : pt + (long long)pair_index(I, t, a.nb8) * kPartPair + 2 * r;
+                const double2 v = __ldcg(reinterpret_cast<const double2 *>(pp));
+                sc += v.x;
+                ss += v.y;
             }
         } else {
-            const int kb = b - nr;
-            for (int g = 0; g < a.side_ctas; ++g) {
-                sc += __ldcg(pside + ((long long)g * nz + kb) * 2);
-                ss += __ldcg(pside + ((long long)g * nz + kb) * 2 + 1);
+            const double *pside = merged + top_doubles + 2 * (b - nr);
+#pragma unroll 8
+            for (int gg = 0; gg < a.side_ctas; ++gg) {
+                const double2 v = __ldcg(reinterpret_cast<const double2 *>(pside + (long long)gg * nz * 2));
+                sc += v.x;
+                ss += v.y;
             }
         }
         if (m == 0) ss = 0.0;
@@ -492,7 +582,18 @@ __global__ void __launch_bounds__(256, KPL <= 4 ? 3 : 2) k_green_compact(Compact
             write_slot(a.so, m, b, sc, ss, 1);
         }
     }
-    if (threadIdx.x == 0) a.cnt[m] = 0u;
+    if (threadIdx.x == 0) mcnt[m] = 0u;
+}
+
+// One CTA per work item.  (A persistent grid that fetched items from a
+// counter balanced the last wave but cost more in per-item overhead at
+// 130x98.)
+template <int KPL>
+__global__ void __launch_bounds__(256, KPL <= 4 ? 3 : 2) k_green_compact(CompactArgs a) {
+    extern __shared__ __align__(16) double csm[];
+    __shared__ double red[compact::kWarps][64];
+    __shared__ bool last;
+    compact_item<KPL>(a, (int)blockIdx.x, csm, red, last);  // waits for the previous kernel before its first write
 }
 
 const void *compact_kernel(int kpl) {
@@ -547,12 +648,15 @@ int compact_configure(bph_ctx *c) {
     cudaError_t e = cudaMalloc((void **)&c->d_gtile, sizeof(double) * nt);
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_gside, sizeof(double) * ns);
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_kpart, sizeof(double) * np);
-    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_kcnt, sizeof(unsigned int) * mm);
-    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_kcnt, 0, sizeof(unsigned int) * mm, c->stream);
+    const size_t ncnt = (size_t)compact::counters(d, c->g.mmax);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_kcnt, sizeof(unsigned int) * ncnt);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_kcnt, 0, sizeof(unsigned int) * ncnt, c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "compact Green tables");
-    c->bytes += sizeof(double) * (nt + ns + np) + sizeof(unsigned int) * mm;
-    e = raise_smem_limit(compact_kernel(d.kpl), (int)compact_smem(d.nz, d.stride));
+    c->bytes += sizeof(double) * (nt + ns + np) + sizeof(unsigned int) * ncnt;
+    const int smem = (int)compact_smem(d.hp, d.stride);
+    e = raise_smem_limit(compact_kernel(d.kpl), smem);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_green_compact)");
+
     e = launch_green_compact(c);
     if (e != cudaSuccess) return cuda_fail(e, "k_green_compact_tiles / k_green_compact_side");
     c->compact = 1;
@@ -589,10 +693,16 @@ cudaError_t launch_green_compact_contract(bph_ctx *c, bool write_slots) {
     a.so.M = c->M;
     a.so.fm = c->fm;
     a.so.nfactor = (double)c->N * c->factor;
+    a.mmax = c->g.mmax;
+    a.nh = d.nh;
+    a.hp = d.hp;
+    a.nzp = d.nzp;
+
+    a.part_h = compact::part_height_doubles(d);
     ++c->launches;
-    const unsigned grid = (unsigned)(c->g.mmax * (d.top_ctas + d.side_ctas));
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = launch_config(c, dim3(grid), dim3(256), compact_smem(d.nz, d.stride), attr);
+    cudaLaunchConfig_t cfg = launch_config(c, dim3((unsigned)compact::items(d, c->g.mmax)), dim3(256),
+                                           compact_smem(d.hp, d.stride), attr);
     void *args[] = {&a};
     return cudaLaunchKernelExC(&cfg, compact_kernel(d.kpl), args);
 }

@@ -11,7 +11,7 @@
 //     H(jb, j, k) = G(jb, j, k) / r_j = Q / (pi sqrt(r_jb r_j)) is symmetric
 //     in (jb, j).  Only the 8 x 8 tiles (I, J), I <= J, of the jb x j plane
 //     are stored, one per interior height k: tile[k][r][c] = H(8I + r,
-//     8J + c, k).  A tile serves row jb = 8I + r with columns 8J + c and, by
+//     8J + c, k), the tiles of one height contiguous.  A tile serves row jb = 8I + r with columns 8J + c and, by
 //     symmetry, row 8J + c with columns 8I + r.
 //   * side rows: the boundary point sits at r_B = r_{numr} and height
 //     z_kb, so on the uniform vertical grid G depends on k only through
@@ -36,6 +36,9 @@ constexpr int kTile = 8;         // rows and columns of a tile
 constexpr int kWarps = 8;        // warps of a contraction CTA
 constexpr int kMaxKpl = 8;       // side rows per lane: nz <= 256
 constexpr int kPartPair = 32;    // partial sums of a tile: row / column x 8 x (cos, sin)
+constexpr int kHeightParts = 1;  // height ranges a tile or side group is split into (work items)
+constexpr int kStageHeights = 2; // heights per stage of the contraction's ring; the tiles are padded to a multiple
+constexpr int kMomPad = 8;       // zeroed doubles after the moment array: an 8-zone run of the last row stays in bounds
 
 struct Dims {
     int nr = 0, nz = 0;
@@ -46,6 +49,9 @@ struct Dims {
     int stride = 0;     // doubles per U or V vector (zero-padded)
     int top_ctas = 0;   // CTAs of tiles per mode (8 tiles each)
     int side_ctas = 0;  // CTAs of side vectors per mode (8 radial zones each)
+    int nh = 0;         // height parts (kHeightParts, or nz when smaller)
+    int hp = 0;         // heights per part, a multiple of kStageHeights (the last part may be shorter)
+    int nzp = 0;        // heights of the tile table: nz rounded up to kStageHeights (zero tiles above nz)
     bool ok = false;    // the compact form applies to this grid
 };
 
@@ -60,6 +66,10 @@ BPH_CHD inline Dims dims(int nr, int nz, int isym) {
     d.stride = nz + 32 * d.kpl;
     d.top_ctas = (d.nsets * d.npair + kWarps - 1) / kWarps;
     d.side_ctas = (nr + kWarps - 1) / kWarps;
+    d.nh = nz < kHeightParts ? nz : kHeightParts;
+    d.hp = d.nh > 0 ? (nz + d.nh - 1) / d.nh : 0;
+    d.hp = ((d.hp + kStageHeights - 1) / kStageHeights) * kStageHeights;
+    d.nzp = ((nz + kStageHeights - 1) / kStageHeights) * kStageHeights;
     d.ok = nr >= 1 && nz >= 1 && d.kpl <= kMaxKpl;
     return d;
 }
@@ -82,10 +92,31 @@ BPH_CHD inline int side_u(int kb, int k, int nz) { return kb - k + nz - 1; }
 BPH_CHD inline int side_v(int kb, int k) { return kb + k; }
 
 // Doubles of each table and of the partial-sum scratch, per mode.
-BPH_CHD inline long long pair_doubles(const Dims &d) { return (long long)d.nsets * d.npair * d.nz * kTile * kTile; }
+BPH_CHD inline long long pair_doubles(const Dims &d) { return (long long)d.nsets * d.npair * d.nzp * kTile * kTile; }
 BPH_CHD inline long long side_doubles(const Dims &d) { return (long long)d.nr * 2 * d.stride; }
-BPH_CHD inline long long part_doubles(const Dims &d) {
+// Partial sums of one mode: per height part, the tiles' then the side
+// groups'; after the nh parts, the same block once more for their sums.
+BPH_CHD inline long long part_height_doubles(const Dims &d) {
     return (long long)d.nsets * d.npair * kPartPair + (long long)d.side_ctas * d.nz * 2;
+}
+BPH_CHD inline long long part_doubles(const Dims &d) { return (long long)(d.nh + 1) * part_height_doubles(d); }
+
+// Arrival counters: one per mode, then one per (mode, tile set or side group).
+BPH_CHD inline long long counters(const Dims &d, int mmax) {
+    return (long long)mmax * (1 + d.top_ctas + d.side_ctas);
+}
+
+// Heights [k0, k1) of part h (empty when k0 >= nz).
+BPH_CHD inline void height_range(const Dims &d, int h, int *k0, int *k1) {
+    const int a = h * d.hp, b = a + d.hp;
+    *k0 = a < d.nz ? a : d.nz;
+    *k1 = b < d.nz ? b : d.nz;
+}
+
+// Work items of one launch: mode-major, then height part, then the mode's
+// tile sets and side groups.
+BPH_CHD inline long long items(const Dims &d, int mmax) {
+    return (long long)mmax * d.nh * (d.top_ctas + d.side_ctas);
 }
 
 }  // namespace compact

@@ -145,10 +145,10 @@ struct bph_ctx {
     int contract_split = 1;
     // compact Green tables (bph_compact.h) and the contraction that reads them
     int compact = 0;                 // 1: the single-solve contraction streams the compact tables
-    double *d_gtile = nullptr;       // symmetric tiles of the top (and bottom) rows [m][set][tile][k][64]
+    double *d_gtile = nullptr;       // symmetric tiles of the top (and bottom) rows [m][set][k][tile][64]
     double *d_gside = nullptr;       // side-row vectors [m][j][U | V][stride]
     double *d_kpart = nullptr;       // partial sums [m][tile parts | side parts]
-    unsigned int *d_kcnt = nullptr;  // arrival counters [mmax]
+    unsigned int *d_kcnt = nullptr;  // arrival counters [mmax] + [mmax][tile sets + side groups]
 
     int adi_smem = 0;            // dynamic shared bytes of the on-chip ADI kernel (0: global variant)
     int adi_seg = 0;             // threads of the segmented on-chip ADI kernel (0: not used)

@@ -214,24 +214,26 @@ __global__ void k_green_tables(const double *__restrict__ grid, const double *__
 // (set 1, isym 1) rows: one thread per (set, tile, height k, element);
 // element (r, c) of tile (I, J) is H(jb = 8I + r, j = 8J + c, k) =
 // G(jb, j, k) / r_j with G as k_green_tables forms it; zero outside the
-// nr x nr plane.  Layout [m][set][tile][k][64].
+// nr x nr plane and at the padding heights k >= nz.  Layout
+// [m][set][k < nzp][tile][64]: at one height the tiles are contiguous, so
+// the contraction's warps read neighbouring 512-byte tiles.
 __global__ void k_green_compact_tiles(const double *__restrict__ grid, const double *__restrict__ qc,
-                                      double *__restrict__ T, int numr, int numz, int nr, int nz, int nb8, int npair,
-                                      int nsets, int mmax, int isym, double piinv) {
-    const long long per_m = (long long)nsets * npair * nz * 64;
+                                      double *__restrict__ T, int numr, int numz, int nr, int nz, int nzp, int nb8,
+                                      int npair, int nsets, int mmax, int isym, double piinv) {
+    const long long per_m = (long long)nsets * npair * nzp * 64;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= per_m) return;
     const double *rhf = grid, *rhfinv = grid + numr, *zhf = grid + 2 * numr;
     const int e = (int)(t % 64);
     long long rest = t / 64;
-    const int k = (int)(rest % nz);
-    rest /= nz;
-    const int q = (int)(rest % npair), set = (int)(rest / npair);
+    const int q = (int)(rest % npair);
+    rest /= npair;
+    const int k = (int)(rest % nzp), set = (int)(rest / nzp);
     int I, J;
     compact::pair_blocks(q, nb8, &I, &J);
     const int jb = 8 * I + (e >> 3), j = 8 * J + (e & 7);
     double *out = T + t;
-    if (jb >= nr || j >= nr) {
+    if (jb >= nr || j >= nr || k >= nz) {
         for (int m = 0; m < mmax; ++m) out[m * per_m] = 0.0;
         return;
     }
@@ -407,10 +409,10 @@ cudaError_t launch_green_tables(bph_ctx *c) {
 cudaError_t launch_green_compact(bph_ctx *c) {
     const compact::Dims d = compact::dims(c->nr, c->nz, c->g.isym);
     const int threads = 128;
-    const long long nt = (long long)d.nsets * d.npair * d.nz * 64;
+    const long long nt = (long long)d.nsets * d.npair * d.nzp * 64;
     k_green_compact_tiles<<<(unsigned)((nt + threads - 1) / threads), threads, 0, c->stream>>>(
-        c->d_grid, c->d_qcoef, c->d_gtile, c->g.numr, c->g.numz, c->nr, c->nz, d.nb8, d.npair, d.nsets, c->g.mmax,
-        c->g.isym, 1.0 / c->pi);
+        c->d_grid, c->d_qcoef, c->d_gtile, c->g.numr, c->g.numz, c->nr, c->nz, d.nzp, d.nb8, d.npair, d.nsets,
+        c->g.mmax, c->g.isym, 1.0 / c->pi);
     const long long ns = (long long)c->nr * 2 * d.stride;
     k_green_compact_side<<<(unsigned)((ns + threads - 1) / threads), threads, 0, c->stream>>>(
         c->d_grid, c->d_qcoef, c->d_gside, c->g.numr, c->nr, c->nz, d.stride, c->g.mmax, c->g.isym, 1.0 / c->pi);

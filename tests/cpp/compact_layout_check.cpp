@@ -61,7 +61,7 @@ static void check(int nr, int nz, int isym) {
                 for (int e = 0; e < 64; ++e) {
                     const int jb = kTile * I + (e >> 3), j = kTile * J + (e & 7);
                     if (jb < nr && j < nr)
-                        T[(((size_t)set * d.npair + q) * nz + k) * 64 + e] = h_sym(set, jb, j, k);
+                        T[(((size_t)set * d.nzp + k) * d.npair + q) * 64 + e] = h_sym(set, jb, j, k);
                 }
         }
     for (int j = 0; j < nr; ++j)
@@ -69,8 +69,12 @@ static void check(int nr, int nz, int isym) {
             if (pos <= 2 * nz - 2) Sd[((size_t)j * 2) * d.stride + pos] = u_fn(j, pos - (nz - 1));
             if (image && pos <= 2 * nz - 2) Sd[((size_t)j * 2 + 1) * d.stride + pos] = v_fn(j, pos);
         }
-    // the kernel's partial sums
+    // the kernel's partial sums, per height part
     std::vector<double> part((size_t)part_doubles(d), 0.0);
+    for (int h = 0; h < d.nh; ++h) {
+    int k0, k1;
+    height_range(d, h, &k0, &k1);
+    double *parth = &part[(size_t)h * part_height_doubles(d)];
     for (int q = 0; q < d.nsets * d.npair; ++q) {
         const int set = q / d.npair, tile = q % d.npair;
         int I, J;
@@ -81,8 +85,8 @@ static void check(int nr, int nz, int isym) {
             const int jr = std::min(kTile * I + r, nr - 1);
             const int jc0 = std::min(kTile * J + c0, nr - 1), jc1 = std::min(kTile * J + c0 + 1, nr - 1);
             double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            for (int k = 0; k < nz; ++k) {
-                const double *t = &T[(((size_t)set * d.npair + tile) * nz + k) * 64 + 2 * lane];
+            for (int k = k0; k < k1; ++k) {
+                const double *t = &T[(((size_t)set * d.nzp + k) * d.npair + tile) * 64 + 2 * lane];
                 const long long off = (long long)nr * k;
                 const double xc0 = mom[off + jc0], xc1 = mom[off + jc1], xs0 = mom[np + off + jc0],
                              xs1 = mom[np + off + jc1], yc = mom[off + jr], ys = mom[np + off + jr];
@@ -102,7 +106,7 @@ static void check(int nr, int nz, int isym) {
             lane_c[lane][1][0] = rw[jr] * acc[6];
             lane_c[lane][1][1] = rw[jr] * acc[7];
         }
-        double *pp = &part[(size_t)q * kPartPair];
+        double *pp = &parth[(size_t)q * kPartPair];
         for (int r = 0; r < 8; ++r)
             for (int cs = 0; cs < 2; ++cs) {
                 double v = 0.0;
@@ -125,45 +129,51 @@ static void check(int nr, int nz, int isym) {
             const double *Uv = &Sd[(size_t)j * 2 * d.stride], *Vv = Uv + d.stride;
             for (int lane = 0; lane < 32; ++lane) {
                 const int base = d.kpl * lane;
-                double u[kMaxKpl], v[kMaxKpl], ac[kMaxKpl] = {0}, as[kMaxKpl] = {0};
-                for (int i = 0; i < d.kpl; ++i) {
-                    u[i] = Uv[base + i + nz - 1];
-                    v[i] = Vv[base + i];
+                const int K = d.kpl;
+                double uu[kMaxKpl], vv[kMaxKpl], ac[kMaxKpl] = {0}, as[kMaxKpl] = {0};
+                for (int i = 0; i < K; ++i) {
+                    uu[i] = Uv[base + i + nz - 1 - k0];
+                    vv[i] = Vv[base + i + k0];
                 }
-                for (int k = 0; k < nz; ++k) {
-                    const double xc = mom[j + (long long)nr * k], xs = mom[np + j + (long long)nr * k];
-                    const double un = (k + 1 < nz) ? Uv[base + nz - 2 - k] : 0.0;
-                    const int vi = base + d.kpl + k;
-                    if (vi >= d.stride) {
-                        std::printf("nr %d nz %d: V window index %d past stride %d\n", nr, nz, vi, d.stride);
-                        ++fails;
-                        return;
+                for (int kb = k0; kb < k1; kb += K)
+                    for (int st = 0; st < K; ++st) {
+                        const int k = kb + st;
+                        if (k >= k1) continue;
+                        const double xc = mom[j + (long long)nr * k], xs = mom[np + j + (long long)nr * k];
+                        const int vi = base + K + k;
+                        if (vi >= d.stride) {
+                            std::printf("nr %d nz %d: V window index %d past stride %d\n", nr, nz, vi, d.stride);
+                            ++fails;
+                            return;
+                        }
+                        const double un = (k + 1 < k1) ? Uv[base + nz - 2 - k] : 0.0;
+                        const double vn = (k + 1 < k1) ? Vv[vi] : 0.0;
+                        for (int i = 0; i < K; ++i) {
+                            const double ww = uu[(i - st + K) % K] + vv[(i + st) % K];
+                            ac[i] += ww * xc;
+                            as[i] += ww * xs;
+                        }
+                        uu[K - 1 - st] = un;
+                        vv[st] = vn;
                     }
-                    const double vn = (k + 1 < nz) ? Vv[vi] : 0.0;
-                    for (int i = 0; i < d.kpl; ++i) {
-                        const double ww = u[i] + v[i];
-                        ac[i] += ww * xc;
-                        as[i] += ww * xs;
-                    }
-                    for (int i = d.kpl - 1; i > 0; --i) u[i] = u[i - 1];
-                    u[0] = un;
-                    for (int i = 0; i + 1 < d.kpl; ++i) v[i] = v[i + 1];
-                    v[d.kpl - 1] = vn;
-                }
                 for (int i = 0; i < d.kpl; ++i) {
                     cta[2 * (base + i)] += ac[i];
                     cta[2 * (base + i) + 1] += as[i];
                 }
             }
         }
-        double *ps = &part[(size_t)d.nsets * d.npair * kPartPair + (size_t)g * nz * 2];
+        double *ps = &parth[(size_t)d.nsets * d.npair * kPartPair + (size_t)g * nz * 2];
         for (int kb = 0; kb < nz; ++kb) {
             ps[2 * kb] = cta[2 * kb];
             ps[2 * kb + 1] = cta[2 * kb + 1];
         }
     }
-    // the last CTA's sums
-    const double *pside = &part[(size_t)d.nsets * d.npair * kPartPair];
+    }
+    // level 2: each tile set's / side group's height parts added; level 3: per boundary row
+    const size_t ph = (size_t)part_height_doubles(d);
+    std::vector<double> merged(ph, 0.0);
+    for (size_t e = 0; e < ph; ++e)
+        for (int h = 0; h < d.nh; ++h) merged[e] += part[(size_t)h * ph + e];
     double worst = 0.0, scale = 0.0;
     for (int b = 0; b < nb; ++b) {
         double sc = 0.0, ss = 0.0;
@@ -171,18 +181,15 @@ static void check(int nr, int nz, int isym) {
             const int set = (b < nr) ? 0 : 1;
             const int jb = (b < nr) ? b : b - nr - nz;
             const int I = jb / kTile, r = jb % kTile;
-            const double *pt = &part[(size_t)set * d.npair * kPartPair];
-            for (int Ip = 0; Ip < I; ++Ip) {
-                const double *pp = pt + (size_t)pair_index(Ip, I, d.nb8) * kPartPair + 16 + 2 * r;
-                sc += pp[0];
-                ss += pp[1];
-            }
-            for (int Jp = I; Jp < d.nb8; ++Jp) {
-                const double *pp = pt + (size_t)pair_index(I, Jp, d.nb8) * kPartPair + 2 * r;
+            const double *pt = &merged[(size_t)set * d.npair * kPartPair];
+            for (int t = 0; t < d.nb8; ++t) {
+                const double *pp = (t < I) ? pt + (size_t)pair_index(t, I, d.nb8) * kPartPair + 16 + 2 * r
+                                           : pt + (size_t)pair_index(I, t, d.nb8) * kPartPair + 2 * r;
                 sc += pp[0];
                 ss += pp[1];
             }
         } else {
+            const double *pside = &merged[(size_t)d.nsets * d.npair * kPartPair];
             for (int g = 0; g < d.side_ctas; ++g) {
                 sc += pside[((size_t)g * nz + (b - nr)) * 2];
                 ss += pside[((size_t)g * nz + (b - nr)) * 2 + 1];
@@ -200,14 +207,16 @@ static void check(int nr, int nz, int isym) {
 
 int main() {
     const int nrs[] = {3, 8, 13, 16, 33, 64};
-    const int nzs[] = {1, 5, 32, 33, 70, 96};
+    const int nzs[] = {1, 2, 3, 5, 7, 32, 33, 70, 96};
     for (int nr : nrs)
         for (int nz : nzs)
             for (int isym : {1, 2}) check(nr, nz, isym);
     // parts and tiles of the production grid 130 x 98
     const Dims d = dims(128, 96, 2);
-    if (d.npair != 136 || d.kpl != 3 || d.top_ctas != 17 || d.side_ctas != 16) {
-        std::printf("130 x 98 dims: npair %d kpl %d top %d side %d\n", d.npair, d.kpl, d.top_ctas, d.side_ctas);
+    if (d.npair != 136 || d.kpl != 3 || d.top_ctas != 17 || d.side_ctas != 16 || d.nh != 1 || d.hp != 96 || d.nzp != 96 ||
+        items(d, 30) != 30 * 33) {
+        std::printf("130 x 98 dims: npair %d kpl %d top %d side %d nh %d hp %d\n", d.npair, d.kpl, d.top_ctas,
+                    d.side_ctas, d.nh, d.hp);
         ++fails;
     }
     if (dims(128, 257, 2).ok) {
