@@ -245,14 +245,87 @@ int upload(bph_ctx *c, void *dst, const void *src, size_t bytes) {
 }
 // Times each fitting refinement ADI kernel (one 5-step cycle over the
 // zeroed slot array: r = 0, so the state stays zero) and keeps the faster.
+// Set-up autotuning of the per-grid kernel choices: the boundary contraction
+// (compact or full tables), the FFT tiles (regular or dense) and the FP64
+// ADI kernel (warp-cooperative or segmented, where both apply).  Each
+// candidate runs once untimed and three times timed on zero data, and the
+// faster stays; BPH_COMPACT, BPH_FFT_DENSE and BPH_ADI_WARP in the
+// environment force their choice, BPH_AUTOTUNE=0 skips all of it.
+int autotune_setup(bph_ctx *c) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    auto timed = [&](auto &&launch, float *us) {
+        if (e == cudaSuccess) e = launch();
+        if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
+        for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = launch();
+        if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        *us = 1e3f * ms / 3.f;
+    };
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_P, 0, sizeof(double) * (size_t)c->N * c->nplane, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_mom, 0, sizeof(double) * 2 * (size_t)c->g.mmax * c->np, c->stream);
+    // boundary contraction
+    if (e == cudaSuccess && c->compact && !std::getenv("BPH_COMPACT")) {
+        c->compact = 0;
+        timed([&] { return launch_green_contract(c); }, &c->tuned_contract_us[0]);
+        c->compact = 1;
+        timed([&] { return launch_green_contract(c); }, &c->tuned_contract_us[1]);
+        c->compact = (c->tuned_contract_us[1] <= c->tuned_contract_us[0]) ? 1 : 0;
+    }
+    // FFT tiles: the forward transform of a zero field, the inverse into scratch
+    if (e == cudaSuccess && !std::getenv("BPH_FFT_DENSE")) {
+        double *scratch = nullptr;
+        e = cudaMalloc((void **)&scratch, sizeof(double) * (size_t)c->ntot);
+        for (int dense = 0; dense < 2 && e == cudaSuccess; ++dense) {
+            c->fft_dense = dense != 0;
+            timed(
+                [&] {
+                    cudaError_t f = launch_fft_fwd_rho(c, c->d_P);
+                    return f == cudaSuccess ? launch_fft_inv(c, scratch) : f;
+                },
+                &c->tuned_fft_us[dense]);
+        }
+        c->fft_dense = c->tuned_fft_us[1] < c->tuned_fft_us[0];
+        if (scratch) {
+            cudaStreamSynchronize(c->stream);
+            cudaFree(scratch);
+        }
+    }
+    // FP64 ADI kernel
+    if (e == cudaSuccess && c->adi_warp && c->adi_seg && !std::getenv("BPH_ADI_WARP")) {
+        Schedule *s;
+        int rc = get_schedule(c, 5, &s);
+        if (rc) return rc;
+        const int shape = c->adi_warp;
+        c->adi_warp = 0;
+        timed([&] { return launch_adi(c, *s, 0, 5, false); }, &c->tuned_adi_us[0]);
+        c->adi_warp = shape;
+        timed([&] { return launch_adi(c, *s, 0, 5, false); }, &c->tuned_adi_us[1]);
+        if (c->tuned_adi_us[0] < c->tuned_adi_us[1]) c->adi_warp = 0;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_fail(e, "set-up autotune");
+    BPH_CUDA(cudaMemsetAsync(c->d_P, 0, sizeof(double) * (size_t)c->N * c->nplane, c->stream));
+    BPH_CUDA(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+    BPH_CUDA(cudaStreamSynchronize(c->stream));
+    return BPH_OK;
+}
+
 int autotune_mixed(bph_ctx *c) {
     const int kinds[3] = {BPH_MIXED_ADI_FORWARD, BPH_MIXED_ADI_INCREMENT, BPH_MIXED_ADI_WARP};
     int avail = 0;
     for (int k : kinds) avail += c->mixed_smem_kind[k] ? 1 : 0;
     if (avail < 2) return BPH_OK;
+    // one refinement cycle of the converged forms' usual length (10 steps): the kinds
+    // differ in per-launch work (the warp kind adds its residual kernel), so a short
+    // schedule would favour the others
     Schedule *s;
     int rc;
-    if ((rc = get_schedule(c, 5, &s))) return rc;
+    if ((rc = get_schedule(c, 10, &s))) return rc;
     BPH_CUDA(cudaMemsetAsync(c->d_R, 0, sizeof(double) * (size_t)c->N * c->np, c->stream));
     BPH_CUDA(cudaMemsetAsync(c->d_P, 0, sizeof(double) * (size_t)c->N * c->nplane, c->stream));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -449,6 +522,7 @@ int setup_impl(bph_ctx *c) {
     BPH_CUDA(cudaStreamSynchronize(c->stream));
     const char *tune = std::getenv("BPH_AUTOTUNE");
     if (!(tune && tune[0] == '0')) {
+        if ((rc = autotune_setup(c))) return rc;
         if ((rc = autotune_mixed(c))) return rc;
     }
     return BPH_OK;
@@ -1013,6 +1087,13 @@ long long bph_info(const bph_ctx_t *c, int what) {
         case BPH_INFO_MIXED_WARP_NS: return (long long)(1e3f * c->mixed_tuned_us[BPH_MIXED_ADI_WARP]);
         case BPH_INFO_GREEN_SMS: return c->green ? c->green_sms[0] : -c->green_fail;
         case BPH_INFO_CONTRACT_KIND: return c->compact ? BPH_CONTRACT_COMPACT : BPH_CONTRACT_FULL;
+        case BPH_INFO_FFT_DENSE: return c->fft_dense ? 1 : 0;
+        case BPH_INFO_CONTRACT_FULL_NS: return (long long)(1e3f * c->tuned_contract_us[0]);
+        case BPH_INFO_CONTRACT_COMPACT_NS: return (long long)(1e3f * c->tuned_contract_us[1]);
+        case BPH_INFO_FFT_NS: return (long long)(1e3f * c->tuned_fft_us[0]);
+        case BPH_INFO_FFT_DENSE_NS: return (long long)(1e3f * c->tuned_fft_us[1]);
+        case BPH_INFO_ADI_SEG_NS: return (long long)(1e3f * c->tuned_adi_us[0]);
+        case BPH_INFO_ADI_WARP_NS: return (long long)(1e3f * c->tuned_adi_us[1]);
         default: return -1;
     }
 }

@@ -163,6 +163,10 @@ struct bph_ctx {
     int mixed_smem_kind[5] = {0, 0, 0, 0, 0};    // per kind: dynamic shared bytes (0: does not fit)
     int mixed_per_sm_kind[5] = {0, 0, 0, 0, 0};  // per kind: resident CTAs per SM
     float mixed_tuned_us[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // per kind: setup-time measurement (0: not timed)
+    // set-up autotuning (autotune_setup): timings of the candidates, us (0: not timed)
+    float tuned_contract_us[2] = {0.f, 0.f};  // full tables, compact tables
+    float tuned_fft_us[2] = {0.f, 0.f};       // forward + inverse FFT: regular tiles, dense tiles
+    float tuned_adi_us[2] = {0.f, 0.f};       // 5 ADI steps of every slot: segmented, warp-cooperative
     float *d_work32 = nullptr;                // global-memory refinement kernels: [4][N][np] (lazy)
     int adi_threads = 256;
     int fft_smem_fwd = 0, fft_smem_inv = 0;

@@ -394,7 +394,8 @@ class PotentialSolver:
         """Launch-configuration facts (bph_info)."""
         names = ("adi_threads", "adi_smem", "mixed_threads", "mixed_smem", "mixed_ctas_per_sm", "contract_split",
                  "mixed_kind", "mixed_forward_ns", "mixed_increment_ns", "adi_prefetch", "adi_kernel",
-                 "adi_warp_smem", "mixed_warp_ns", "green_sms", "contract_kind")
+                 "adi_warp_smem", "mixed_warp_ns", "green_sms", "contract_kind", "fft_dense", "contract_full_ns",
+                 "contract_compact_ns", "fft_ns", "fft_dense_ns", "adi_seg_ns", "adi_warp_ns")
         return {n: int(self._lib.bph_info(self._h, i)) for i, n in enumerate(names)}
 
     def set_mixed_adi(self, kind: int) -> None:

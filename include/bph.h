@@ -346,15 +346,22 @@ int bph_green_contract_noalloc(bph_ctx_t *ctx, const double *d_mom, double *d_S)
 #define BPH_INFO_MIXED_CTAS_PER_SM 4  /* its resident CTAs per SM */
 #define BPH_INFO_CONTRACT_SPLIT 5     /* slices of the split-K Green contraction */
 #define BPH_INFO_MIXED_KIND 6         /* refinement ADI kernel in use (BPH_MIXED_ADI_*) */
-#define BPH_INFO_MIXED_FORWARD_NS 7   /* setup-time duration of a 5-step forwarding-form launch, ns (0: not timed) */
+#define BPH_INFO_MIXED_FORWARD_NS 7   /* setup-time duration of a 10-step forwarding-form launch, ns (0: not timed) */
 #define BPH_INFO_MIXED_INCREMENT_NS 8 /* the same for the increment form */
 #define BPH_INFO_ADI_PREFETCH 9       /* bulk-copy factor prefetch: bit 0 FP64 ADI, bit 1 FP32 refinement ADI */
 #define BPH_INFO_ADI_KERNEL 10        /* FP64 drop-in ADI kernel in use (BPH_ADI_KERNEL_*) */
 #define BPH_INFO_ADI_WARP_SMEM 11     /* dynamic shared bytes of the warp-cooperative kernel (0: not used) */
-#define BPH_INFO_MIXED_WARP_NS 12     /* setup-time duration of a 5-step warp-cooperative refinement launch, ns */
+#define BPH_INFO_MIXED_WARP_NS 12     /* setup-time duration of a 10-step warp-cooperative refinement launch, ns */
 #define BPH_INFO_GREEN_SMS 13         /* SMs of the contraction's partition in the overlapped solve (0: not requested,
                                          negative: the set-up step that failed) */
 #define BPH_INFO_CONTRACT_KIND 14     /* boundary contraction of the single solve (BPH_CONTRACT_*) */
+#define BPH_INFO_FFT_DENSE 15         /* 1: FFT tiles compiled for eight CTAs per SM (autotuned, or BPH_FFT_DENSE) */
+#define BPH_INFO_CONTRACT_FULL_NS 16  /* set-up autotune: one full-table contraction, ns (0: not timed) */
+#define BPH_INFO_CONTRACT_COMPACT_NS 17 /* the same for the compact contraction */
+#define BPH_INFO_FFT_NS 18            /* set-up autotune: forward + inverse FFT with regular tiles, ns */
+#define BPH_INFO_FFT_DENSE_NS 19      /* the same with dense tiles */
+#define BPH_INFO_ADI_SEG_NS 20        /* set-up autotune: 5 ADI steps of every slot, segmented kernel, ns */
+#define BPH_INFO_ADI_WARP_NS 21       /* the same with the warp-cooperative kernel */
 #define BPH_CONTRACT_FULL 1           /* streams the full tables G[m][b][p] */
 #define BPH_CONTRACT_COMPACT 2        /* streams the symmetric tiles and side vectors (2/3 fewer bytes) */
 #define BPH_ADI_KERNEL_WARP 1         /* warp-cooperative line solves, shuffle carries (128x96, 64x64 interiors) */

@@ -204,3 +204,27 @@ def test_sm_partitioned_solve_matches_oracle(oracle_130, pair_rho, bph, monkeypa
         po = oracle_130.potential_solver(rhos[i], 0 if i == 0 else i + 1)
         assert rel_l2(d_pot[i].cpu().numpy().reshape(rhos[i].shape, order="F"), po) <= POT_TOL, i
     g.close()
+
+
+def test_setup_autotune_keeps_the_faster_candidates(bph, monkeypatch):
+    """bph_setup times both boundary contractions, both FFT tile variants and
+    both FP64 ADI kernels on the grid and keeps the faster of each (reported
+    by bph_info); BPH_AUTOTUNE=0 keeps the defaults and times nothing."""
+    S = bph.solver
+    g = bph.PotentialSolver(*GRID_130)
+    i = g.info()
+    g.close()
+    assert i["contract_full_ns"] > 0 and i["contract_compact_ns"] > 0, i
+    want = S.CONTRACT_COMPACT if i["contract_compact_ns"] <= i["contract_full_ns"] else S.CONTRACT_FULL
+    assert i["contract_kind"] == want, i
+    assert i["fft_ns"] > 0 and i["fft_dense_ns"] > 0, i
+    assert i["fft_dense"] == (1 if i["fft_dense_ns"] < i["fft_ns"] else 0), i
+    assert i["adi_seg_ns"] > 0 and i["adi_warp_ns"] > 0, i
+    want = S.ADI_KERNEL_SEGMENTED if i["adi_seg_ns"] < i["adi_warp_ns"] else S.ADI_KERNEL_WARP
+    assert i["adi_kernel"] == want, i
+    monkeypatch.setenv("BPH_AUTOTUNE", "0")
+    g = bph.PotentialSolver(*GRID_130)
+    i = g.info()
+    g.close()
+    assert i["contract_full_ns"] == 0 and i["fft_ns"] == 0 and i["adi_seg_ns"] == 0, i
+    assert i["contract_kind"] == S.CONTRACT_COMPACT and i["adi_kernel"] == S.ADI_KERNEL_WARP and i["fft_dense"] == 0
