@@ -989,8 +989,30 @@ def run_gpu(args, world, rank, local):
         batched_conv["fp64"] = r64
         rmx, outs = measure(args.conv_nsteps, True)
         rmx["max_rel_err_vs_fp64"] = err_vs(outs, ref_outs)
+        kind_names = {B.solver.MIXED_ADI_FORWARD: "adi_forward", B.solver.MIXED_ADI_INCREMENT: "adi_increment",
+                      B.solver.MIXED_ADI_GLOBAL: "adi_global", B.solver.MIXED_ADI_WARP: "adi_warp",
+                      B.solver.MIXED_DIRECT: "direct"}
+        tuned = solver.info()["mixed_kind"]
+        rmx["inner_solver"] = kind_names.get(tuned, str(tuned))
         batched_conv["mixed"] = rmx
         batched_conv["speedup_mixed_vs_fp64"] = rmx["solves_per_s"] / r64["solves_per_s"]
+        # the mixed form with its fastest FP32 ADI inner solver as well (the precision's share
+        # of the speed-up, without the direct solve)
+        if tuned == B.solver.MIXED_DIRECT:
+            info0 = solver.info()
+            adi_kinds = [(info0["mixed_warp_ns"], B.solver.MIXED_ADI_WARP),
+                         (info0["mixed_forward_ns"], B.solver.MIXED_ADI_FORWARD),
+                         (info0["mixed_increment_ns"], B.solver.MIXED_ADI_INCREMENT)]
+            adi_kinds = [k for k in adi_kinds if k[0] > 0]
+            if adi_kinds:
+                solver.set_mixed_adi(min(adi_kinds)[1])
+                radi, outs2 = measure(args.conv_nsteps, True)
+                radi["max_rel_err_vs_fp64"] = err_vs(outs2, ref_outs)
+                radi["inner_solver"] = kind_names[min(adi_kinds)[1]]
+                batched_conv["mixed_adi"] = radi
+                batched_conv["speedup_mixed_adi_vs_fp64"] = radi["solves_per_s"] / r64["solves_per_s"]
+                del outs2
+                solver.set_mixed_adi(tuned)
         # each form at its own best cycle length (the converged answer does not depend on it)
         sweep = sorted(set(int(x) for x in args.conv_nsteps_sweep.split(",") if x))
         if sweep:
@@ -1036,6 +1058,8 @@ def run_gpu(args, world, rank, local):
                     ("mixed_increment", B.solver.MIXED_ADI_INCREMENT)]
         if solver.info()["mixed_warp_ns"] > 0:
             variants.append(("mixed_warp", B.solver.MIXED_ADI_WARP))
+        if solver.info()["mixed_direct_ns"] > 0:
+            variants.append(("mixed_direct", B.solver.MIXED_DIRECT))
         for key, kind in variants:
             if kind is not None:
                 solver.set_mixed_adi(kind)
@@ -1065,7 +1089,7 @@ def run_gpu(args, world, rank, local):
         conv["nsteps_per_cycle"] = args.conv_nsteps
         conv["tol_update"] = args.conv_tol
         names = {B.solver.MIXED_ADI_FORWARD: "mixed_forward", B.solver.MIXED_ADI_INCREMENT: "mixed_increment",
-                 B.solver.MIXED_ADI_WARP: "mixed_warp"}
+                 B.solver.MIXED_ADI_WARP: "mixed_warp", B.solver.MIXED_DIRECT: "mixed_direct"}
         conv["autotuned_kind"] = names.get(tuned_kind, str(tuned_kind))
         best = max(conv[k]["solves_per_s"] for k, kind in variants if kind is not None)
         conv["speedup_mixed_vs_fp64"] = best / conv["fp64"]["solves_per_s"]

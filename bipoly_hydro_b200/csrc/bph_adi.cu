@@ -1313,7 +1313,7 @@ int adi_configure(bph_ctx *c) {
 }
 
 int select_mixed_kind(bph_ctx *c, int kind) {
-    if (kind < 1 || kind > 4 || !c->mixed_smem_kind[kind]) {
+    if (kind < 1 || kind > 5 || !c->mixed_smem_kind[kind]) {
         c->adi_mixed_smem = 0;
         c->adi_mixed_per_sm = 0;
         return (kind == 0) ? BPH_OK : BPH_ERR_INVALID;
@@ -1416,6 +1416,7 @@ cudaError_t launch_adi_slots(bph_ctx *c, const Schedule &sch, bool cold, const i
 
 cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {
     if (!c->adi_mixed_smem) return cudaErrorNotSupported;
+    if (c->mixed_kind == BPH_MIXED_DIRECT) return launch_defect_direct(c, c->d_P, c->d_R, 1, nullptr, c->d_red);
     AdiArgs a = make_args(c, sch, 0, sch.nsteps, false);
     a.norms = c->d_red;
     a.rad_pk = sch.d_rad_pk[1];  // float blocks for the FP32 kernels
@@ -1441,6 +1442,7 @@ cudaError_t launch_defect_batch(bph_ctx *c, const Schedule &sch, double *P, cons
                                 double *norms) {
     if (!c->adi_mixed_smem || c->mixed_kind == BPH_MIXED_ADI_GLOBAL) return cudaErrorNotSupported;
     if (c->mixed_kind == BPH_MIXED_ADI_WARP) return cudaErrorNotSupported;  // launch_defect_batch_warp
+    if (c->mixed_kind == BPH_MIXED_DIRECT) return launch_defect_direct(c, P, R, n, d_map, norms);
     AdiArgs a = make_args(c, sch, 0, sch.nsteps, false);
     a.P = P;
     a.R = R;

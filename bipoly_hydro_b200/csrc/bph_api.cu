@@ -316,7 +316,7 @@ int autotune_setup(bph_ctx *c) {
 }
 
 int autotune_mixed(bph_ctx *c) {
-    const int kinds[3] = {BPH_MIXED_ADI_FORWARD, BPH_MIXED_ADI_INCREMENT, BPH_MIXED_ADI_WARP};
+    const int kinds[4] = {BPH_MIXED_ADI_FORWARD, BPH_MIXED_ADI_INCREMENT, BPH_MIXED_ADI_WARP, BPH_MIXED_DIRECT};
     int avail = 0;
     for (int k : kinds) avail += c->mixed_smem_kind[k] ? 1 : 0;
     if (avail < 2) return BPH_OK;
@@ -490,6 +490,7 @@ int setup_impl(bph_ctx *c) {
     if ((rc = fft_configure(c))) return rc;
     if ((rc = adi_configure(c))) return rc;
     if ((rc = warp_configure(c))) return rc;
+    if ((rc = direct_configure(c))) return rc;
     if ((rc = contract_configure(c))) return rc;
     if ((rc = noalloc_setup(c))) return rc;
     {
@@ -668,6 +669,7 @@ static void ctx_free(bph_ctx *c) {
     dev_free(c->d_warp_coef);
     dev_free(c->d_warp_coef32);
     dev_free(c->d_r32);
+    dev_free(c->d_dir32);
     dev_free(c->d_scf);
     if (c->side_stream) {
         cudaStreamSynchronize(c->side_stream);
@@ -1094,6 +1096,7 @@ long long bph_info(const bph_ctx_t *c, int what) {
         case BPH_INFO_FFT_DENSE_NS: return (long long)(1e3f * c->tuned_fft_us[1]);
         case BPH_INFO_ADI_SEG_NS: return (long long)(1e3f * c->tuned_adi_us[0]);
         case BPH_INFO_ADI_WARP_NS: return (long long)(1e3f * c->tuned_adi_us[1]);
+        case BPH_INFO_MIXED_DIRECT_NS: return (long long)(1e3f * c->mixed_tuned_us[BPH_MIXED_DIRECT]);
         default: return -1;
     }
 }
@@ -1108,7 +1111,7 @@ int bph_configure(bph_ctx_t *c, int key, int value) {
     BPH_DEVICE_SCOPE(c);
     if (value == BPH_MIXED_ADI_AUTO) return autotune_mixed(c);
     if (value != BPH_MIXED_ADI_FORWARD && value != BPH_MIXED_ADI_INCREMENT && value != BPH_MIXED_ADI_GLOBAL &&
-        value != BPH_MIXED_ADI_WARP) {
+        value != BPH_MIXED_ADI_WARP && value != BPH_MIXED_DIRECT) {
         set_error("unknown refinement ADI kind %d", value);
         return BPH_ERR_INVALID;
     }

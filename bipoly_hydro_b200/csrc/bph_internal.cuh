@@ -160,9 +160,10 @@ struct bph_ctx {
     int adi_mixed_smem = 0;      // dynamic shared bytes of the one in use (0: mixed form unavailable)
     int adi_mixed_per_sm = 0;    // its resident CTAs per SM
     int mixed_kind = 0;          // refinement ADI in use: BPH_MIXED_ADI_FORWARD or _INCREMENT
-    int mixed_smem_kind[5] = {0, 0, 0, 0, 0};    // per kind: dynamic shared bytes (0: does not fit)
-    int mixed_per_sm_kind[5] = {0, 0, 0, 0, 0};  // per kind: resident CTAs per SM
-    float mixed_tuned_us[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // per kind: setup-time measurement (0: not timed)
+    int mixed_smem_kind[6] = {0, 0, 0, 0, 0, 0};    // per kind: dynamic shared bytes (0: does not fit)
+    int mixed_per_sm_kind[6] = {0, 0, 0, 0, 0, 0};  // per kind: resident CTAs per SM
+    float mixed_tuned_us[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // per kind: setup-time measurement (0: not timed)
+    float *d_dir32 = nullptr;  // direct defect solve: E, E^T (padded), vertical eigenvalues (bph_direct.cu)
     // set-up autotuning (autotune_setup): timings of the candidates, us (0: not timed)
     float tuned_contract_us[2] = {0.f, 0.f};  // full tables, compact tables
     float tuned_fft_us[2] = {0.f, 0.f};       // forward + inverse FFT: regular tiles, dense tiles
@@ -350,6 +351,11 @@ int contract_configure(bph_ctx *c);
 // Compact tables: allocation and build at set-up (BPH_COMPACT=0 leaves them
 // off), bph_setup.cu builds them.
 int compact_configure(bph_ctx *c);
+// Direct FP32 defect solve (bph_direct.cu): set-up of its tables, and one
+// refinement cycle for nrows block rows (instance of a row: inst_map).
+int direct_configure(bph_ctx *c);
+cudaError_t launch_defect_direct(bph_ctx *c, double *P, const double *R, int nrows, const int *inst_map,
+                                 double *norms);
 cudaError_t launch_green_compact(bph_ctx *c);
 // Warp-cooperative FP64 ADI (bph_adi_warp.cu).  warp_configure selects it
 // for the grids it covers (c->adi_warp != 0) and packs the per-slot

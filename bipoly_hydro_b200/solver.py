@@ -60,6 +60,7 @@ EXPORTED_SYMBOLS = (
 #: bph_configure keys and values.
 CFG_MIXED_ADI = 0
 MIXED_ADI_AUTO, MIXED_ADI_FORWARD, MIXED_ADI_INCREMENT, MIXED_ADI_GLOBAL, MIXED_ADI_WARP = 0, 1, 2, 3, 4
+MIXED_DIRECT = 5  # the defect equation solved directly in FP32 (not an ADI)
 
 #: bph_info(BPH_INFO_ADI_KERNEL) values.
 ADI_KERNEL_WARP, ADI_KERNEL_SEGMENTED, ADI_KERNEL_ONCHIP, ADI_KERNEL_GRID_WIDE = 1, 2, 3, 4
@@ -395,12 +396,14 @@ class PotentialSolver:
         names = ("adi_threads", "adi_smem", "mixed_threads", "mixed_smem", "mixed_ctas_per_sm", "contract_split",
                  "mixed_kind", "mixed_forward_ns", "mixed_increment_ns", "adi_prefetch", "adi_kernel",
                  "adi_warp_smem", "mixed_warp_ns", "green_sms", "contract_kind", "fft_dense", "contract_full_ns",
-                 "contract_compact_ns", "fft_ns", "fft_dense_ns", "adi_seg_ns", "adi_warp_ns")
+                 "contract_compact_ns", "fft_ns", "fft_dense_ns", "adi_seg_ns", "adi_warp_ns", "mixed_direct_ns")
         return {n: int(self._lib.bph_info(self._h, i)) for i, n in enumerate(names)}
 
     def set_mixed_adi(self, kind: int) -> None:
-        """Refinement ADI kernel of the mixed form: MIXED_ADI_AUTO (time both
-        and keep the faster), MIXED_ADI_FORWARD or MIXED_ADI_INCREMENT."""
+        """Inner solver of the mixed form's refinement cycles: MIXED_ADI_AUTO
+        (time every kind that fits and keep the fastest cycle), an FP32 ADI
+        kernel (MIXED_ADI_FORWARD, MIXED_ADI_INCREMENT, MIXED_ADI_GLOBAL,
+        MIXED_ADI_WARP) or MIXED_DIRECT (the defect equation solved directly)."""
         _check(self._lib.bph_configure(self._h, CFG_MIXED_ADI, int(kind)))
 
     @property

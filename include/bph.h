@@ -362,6 +362,7 @@ int bph_green_contract_noalloc(bph_ctx_t *ctx, const double *d_mom, double *d_S)
 #define BPH_INFO_FFT_DENSE_NS 19      /* the same with dense tiles */
 #define BPH_INFO_ADI_SEG_NS 20        /* set-up autotune: 5 ADI steps of every slot, segmented kernel, ns */
 #define BPH_INFO_ADI_WARP_NS 21       /* the same with the warp-cooperative kernel */
+#define BPH_INFO_MIXED_DIRECT_NS 22   /* setup-time duration of one direct FP32 defect solve, ns (0: not timed) */
 #define BPH_CONTRACT_FULL 1           /* streams the full tables G[m][b][p] */
 #define BPH_CONTRACT_COMPACT 2        /* streams the symmetric tiles and side vectors (2/3 fewer bytes) */
 #define BPH_ADI_KERNEL_WARP 1         /* warp-cooperative line solves, shuffle carries (128x96, 64x64 interiors) */
@@ -397,6 +398,12 @@ long long bph_info(const bph_ctx_t *ctx, int what);
 /* the forwarding form with warp-cooperative line solves (shuffle carries,
  * two CTAs per SM), for 128 x 96 interiors (130x98 grids) */
 #define BPH_MIXED_ADI_WARP 4
+/* not an ADI: the defect equation solved directly in FP32 (eigen-transform of
+ * the vertical operator, one radial tridiagonal per vertical mode, inverse
+ * transform), for slots whose FP32 residual fits in shared memory; each
+ * refinement cycle then gains about the FP32 accuracy of the solve instead of
+ * one ADI cycle's reduction.  The cycle's nsteps is not used. */
+#define BPH_MIXED_DIRECT 5
 int bph_configure(bph_ctx_t *ctx, int key, int value);
 
 /* Number of kernels this context has launched so far. */

@@ -228,3 +228,27 @@ def test_setup_autotune_keeps_the_faster_candidates(bph, monkeypatch):
     g.close()
     assert i["contract_full_ns"] == 0 and i["fft_ns"] == 0 and i["adi_seg_ns"] == 0, i
     assert i["contract_kind"] == S.CONTRACT_COMPACT and i["adi_kernel"] == S.ADI_KERNEL_WARP and i["fft_dense"] == 0
+
+
+def test_direct_refinement_at_the_production_grid(oracle_130, pair_rho, bph):
+    """MIXED_DIRECT at 130x98x256: cold and warm converged solves and a
+    converged batch within 1e-9 of the oracle's converged FP64 potentials."""
+    from bipoly_hydro_b200 import fields
+
+    g = bph.PotentialSolver(*GRID_130)
+    g.set_mixed_adi(bph.solver.MIXED_DIRECT)
+    po, co, _ = oracle_130.solve_converged(pair_rho, 10, True, 1e-12, 60)
+    pm, im = g.solve_converged_mixed(pair_rho, 10, True, 1e-12, 60)
+    assert rel_l2(pm, po) <= 1e-9, (rel_l2(pm, po), im.cycles, co)
+    rho2 = fields.rotate(pair_rho)
+    po2, _, _ = oracle_130.solve_converged(rho2, 10, False, 1e-12, 60)
+    pm2, im2 = g.solve_converged_mixed(rho2, 10, False, 1e-12, 60)
+    assert rel_l2(pm2, po2) <= 1e-9, (rel_l2(pm2, po2), im2.cycles)
+    batch = bph.Batch(g, capacity=3)
+    rhos = [fields.rotate(pair_rho, i) for i in range(3)]
+    pots, info = batch.solve_converged(rhos, 10, True, 1e-12, 60, mixed=True)
+    for i in (0, 2):
+        ref = oracle_130.solve_converged(rhos[i], 10, True, 1e-12, 60)[0]
+        assert rel_l2(pots[i], ref) <= 1e-9, (i, rel_l2(pots[i], ref), info.cycles)
+    batch.close()
+    g.close()

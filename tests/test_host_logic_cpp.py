@@ -15,6 +15,9 @@
   top and bottom rows, sliding U/V windows of the side rows) contracted
   with the kernel's index arithmetic equals the dense contraction, for
   ragged tile edges, odd radial counts and both symmetry classes.
+* bph_direct.h: the closed-form eigenvectors of the vertical second
+  difference (reflecting or Dirichlet bottom) are orthonormal and
+  diagonalise it, the basis of the direct defect solve.
 """
 import os
 import re
@@ -50,6 +53,10 @@ def test_zone_slices_cover_each_zone_once(tmp_path):
 
 def test_compact_table_layout_matches_dense_contraction(tmp_path):
     assert "all checks passed" in _run(tmp_path, "compact_layout_check")
+
+
+def test_vertical_eigen_decomposition(tmp_path):
+    assert "all checks passed" in _run(tmp_path, "direct_eigen_check")
 
 
 def test_library_selects_devices_only_through_the_scope():
