@@ -114,16 +114,21 @@ struct FftBatch {
     int status_stride = 0;  // 1: a flag per position, 0: one shared flag
 };
 
-template <int M, int Dense = 0>
-struct FftShape {
+// Threads and shared bytes of a tile (the same for both register budgets).
+template <int M>
+struct FftTile {
     static constexpr int kThreads = (M >= 256) ? 256 : 128;
-    // resident CTAs per SM the register budget is sized for (the loads of a
-    // tile are all in flight at once; more CTAs hide more of their latency).
-    // Dense = 1: eight CTAs of 64 registers per SM for the 128-thread tiles
-    // (no spills), chosen at set-up with BPH_FFT_DENSE=1.
+    static constexpr size_t kSmem = sizeof(double2) * ((size_t)M * tile_cols<M>() + M + (M + 1));
+};
+
+// Resident CTAs per SM the register budget is sized for (the loads of a
+// tile are all in flight at once; more CTAs hide more of their latency).
+// Dense = 1: eight CTAs of 64 registers per SM for the 128-thread tiles (no
+// spills), chosen by the set-up autotuner or with BPH_FFT_DENSE=1.
+template <int M, int Dense = 0>
+struct FftShape : FftTile<M> {
     static constexpr int kMinBlocksFwd = (M >= 256) ? 2 : (Dense ? 8 : 5);
     static constexpr int kMinBlocksInv = (M >= 256) ? 1 : (Dense ? 8 : 4);
-    static constexpr size_t kSmem = sizeof(double2) * ((size_t)M * tile_cols<M>() + M + (M + 1));
 };
 
 // Forward transform of interior columns.  kRho: write R = -4 pi rho_hat
@@ -132,13 +137,13 @@ struct FftShape {
 // from the same spectrum: sum_l rho_l e^{i k (l - 1/2) dphi} = e^{i pi k/N} F_k.
 // !kRho: write the warm-start potential into P's interior.
 template <int M, bool kRho, int Dense = 0>
-__global__ void __launch_bounds__(FftShape<M>::kThreads, (FftShape<M, Dense>::kMinBlocksFwd))
+__global__ void __launch_bounds__(FftTile<M>::kThreads, (FftShape<M, Dense>::kMinBlocksFwd))
 k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__restrict__ mom,
           const double2 *__restrict__ g_tw, const double2 *__restrict__ g_tw2, const double2 *__restrict__ g_ph,
           int numr, int numz, int nr, int nz, int mmax, int fm, int isym, double four_pi,
           int *__restrict__ status, long long mstride, FftBatch bt) {
     constexpr int kTile = tile_cols<M>();
-    constexpr int NT = FftShape<M>::kThreads;
+    constexpr int NT = FftTile<M>::kThreads;
     extern __shared__ double2 smem[];
     double2 *C = smem;
     double2 *tw = C + M * kTile;
@@ -280,12 +285,12 @@ k_fft_fwd(const double *__restrict__ src, double *__restrict__ out, double *__re
 // phieff = pot - 0.5 omega^2 rhf(J)^2 that the hydro source step forms from
 // pot (source.F90:156, make_source_temp.F90:121), saving it a full pass.
 template <int M, int Dense = 0>
-__global__ void __launch_bounds__(FftShape<M>::kThreads, (FftShape<M, Dense>::kMinBlocksInv))
+__global__ void __launch_bounds__(FftTile<M>::kThreads, (FftShape<M, Dense>::kMinBlocksInv))
 k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 *__restrict__ g_tw,
           const double2 *__restrict__ g_tw2, int numr, int numz, int isym, double *__restrict__ phieff,
           const double *__restrict__ rhf, double omega, FftBatch bt) {
     constexpr int kTile = tile_cols<M>();
-    constexpr int NT = FftShape<M>::kThreads;
+    constexpr int NT = FftTile<M>::kThreads;
     extern __shared__ double2 smem[];
     double2 *C = smem;
     double2 *tw = C + M * kTile;
@@ -395,7 +400,7 @@ k_fft_inv(const double *__restrict__ P, double *__restrict__ pot, const double2 
 
 template <int M>
 cudaError_t set_fft_attrs(bph_ctx *c) {
-    size_t smem = FftShape<M>::kSmem;
+    size_t smem = FftTile<M>::kSmem;
     cudaError_t e = cudaFuncSetAttribute(k_fft_fwd<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_fft_fwd<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -416,7 +421,7 @@ cudaError_t fwd_rho(bph_ctx *c, const double *rho, double *R, double *mom, long 
     unsigned blocks = (unsigned)((c->np + kTile - 1) / kTile);
     cudaLaunchAttribute attr[1];
     cudaLaunchConfig_t cfg =
-        launch_config(c, dim3(blocks, (unsigned)npos), dim3(FftShape<M>::kThreads), FftShape<M>::kSmem, attr);
+        launch_config(c, dim3(blocks, (unsigned)npos), dim3(FftTile<M>::kThreads), FftTile<M>::kSmem, attr);
     if (c->fft_dense)
         return cudaLaunchKernelEx(&cfg, k_fft_fwd<M, true, 1>, rho, R, mom, (const double2 *)c->d_tw,
                                   (const double2 *)c->d_tw2, (const double2 *)c->d_ph, c->g.numr, c->g.numz, c->nr,
@@ -430,7 +435,7 @@ template <int M>
 cudaError_t fwd_pot(bph_ctx *c, const double *pot) {
     constexpr int kTile = tile_cols<M>();
     unsigned blocks = (unsigned)((c->np + kTile - 1) / kTile);
-    k_fft_fwd<M, false><<<blocks, FftShape<M>::kThreads, FftShape<M>::kSmem, c->stream>>>(
+    k_fft_fwd<M, false><<<blocks, FftTile<M>::kThreads, FftTile<M>::kSmem, c->stream>>>(
         pot, c->d_P, nullptr, c->d_tw, c->d_tw2, c->d_ph, c->g.numr, c->g.numz, c->nr, c->nz, c->g.mmax, c->fm,
         c->g.isym, c->four_pi, c->d_status, 0, FftBatch());
     return cudaGetLastError();
@@ -442,7 +447,7 @@ cudaError_t inv(bph_ctx *c, double *pot, double *phieff, double omega, const dou
     unsigned blocks = (unsigned)((c->nplane + kTile - 1) / kTile);
     cudaLaunchAttribute attr[1];
     cudaLaunchConfig_t cfg =
-        launch_config(c, dim3(blocks, (unsigned)npos), dim3(FftShape<M>::kThreads), FftShape<M>::kSmem, attr);
+        launch_config(c, dim3(blocks, (unsigned)npos), dim3(FftTile<M>::kThreads), FftTile<M>::kSmem, attr);
     if (c->fft_dense)
         return cudaLaunchKernelEx(&cfg, k_fft_inv<M, 1>, P, pot, (const double2 *)c->d_tw, (const double2 *)c->d_tw2,
                                   c->g.numr, c->g.numz, c->g.isym, phieff, (const double *)c->d_grid, omega, bt);

@@ -65,6 +65,11 @@ MIXED_DIRECT = 5  # the defect equation solved directly in FP32 (not an ADI)
 #: bph_info(BPH_INFO_ADI_KERNEL) values.
 ADI_KERNEL_WARP, ADI_KERNEL_SEGMENTED, ADI_KERNEL_ONCHIP, ADI_KERNEL_GRID_WIDE = 1, 2, 3, 4
 CONTRACT_FULL, CONTRACT_COMPACT = 1, 2
+# bph_info keys in index order: BPH_INFO_<KEY> of include/bph.h, lower case
+INFO_KEYS = ("adi_threads", "adi_smem", "mixed_threads", "mixed_smem", "mixed_ctas_per_sm", "contract_split",
+             "mixed_kind", "mixed_forward_ns", "mixed_increment_ns", "adi_prefetch", "adi_kernel", "adi_warp_smem",
+             "mixed_warp_ns", "green_sms", "contract_kind", "fft_dense", "contract_full_ns", "contract_compact_ns",
+             "fft_ns", "fft_dense_ns", "adi_seg_ns", "adi_warp_ns", "mixed_direct_ns")
 
 #: bph_run_phase phase ids.
 PHASE_FFT_RHO, PHASE_CONTRACT, PHASE_SLOTS, PHASE_ADI, PHASE_FFT_INV = range(5)
@@ -393,11 +398,7 @@ class PotentialSolver:
 
     def info(self) -> dict:
         """Launch-configuration facts (bph_info)."""
-        names = ("adi_threads", "adi_smem", "mixed_threads", "mixed_smem", "mixed_ctas_per_sm", "contract_split",
-                 "mixed_kind", "mixed_forward_ns", "mixed_increment_ns", "adi_prefetch", "adi_kernel",
-                 "adi_warp_smem", "mixed_warp_ns", "green_sms", "contract_kind", "fft_dense", "contract_full_ns",
-                 "contract_compact_ns", "fft_ns", "fft_dense_ns", "adi_seg_ns", "adi_warp_ns", "mixed_direct_ns")
-        return {n: int(self._lib.bph_info(self._h, i)) for i, n in enumerate(names)}
+        return {n: int(self._lib.bph_info(self._h, i)) for i, n in enumerate(INFO_KEYS)}
 
     def set_mixed_adi(self, kind: int) -> None:
         """Inner solver of the mixed form's refinement cycles: MIXED_ADI_AUTO

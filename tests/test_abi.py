@@ -92,3 +92,20 @@ def test_null_handles_of_batches_plans_and_servers_are_errors(bph):
     assert lib.bph_plan_destroy(None) == bph.BPH_OK
     assert lib.bph_server_set_converged(None, 10, 1e-11, 10, 0) == inv
     assert lib.bph_server_destroy(None) in (bph.BPH_OK, inv)
+
+
+def test_info_keys_follow_the_header(bph):
+    """PotentialSolver.info() names every BPH_INFO_* index of include/bph.h,
+    in order, and the mixed kinds and contraction kinds match their defines."""
+    import os
+    import re
+
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "bph.h")).read()
+    defs = {int(v): k.lower() for k, v in re.findall(r"#define BPH_INFO_([A-Z0-9_]+) (\d+)", hdr)}
+    assert sorted(defs) == list(range(len(defs)))
+    assert tuple(defs[i] for i in range(len(defs))) == bph.solver.INFO_KEYS
+    kinds = dict(re.findall(r"#define (BPH_MIXED_[A-Z_]+|BPH_CONTRACT_[A-Z]+) (\d+)", hdr))
+    S = bph.solver
+    assert int(kinds["BPH_MIXED_ADI_WARP"]) == S.MIXED_ADI_WARP
+    assert int(kinds["BPH_MIXED_DIRECT"]) == S.MIXED_DIRECT
+    assert int(kinds["BPH_CONTRACT_COMPACT"]) == S.CONTRACT_COMPACT and int(kinds["BPH_CONTRACT_FULL"]) == S.CONTRACT_FULL
