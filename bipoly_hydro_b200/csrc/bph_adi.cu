@@ -1416,7 +1416,7 @@ cudaError_t launch_adi_slots(bph_ctx *c, const Schedule &sch, bool cold, const i
 
 cudaError_t launch_adi_defect(bph_ctx *c, const Schedule &sch) {
     if (!c->adi_mixed_smem) return cudaErrorNotSupported;
-    if (c->mixed_kind == BPH_MIXED_DIRECT) return launch_defect_direct(c, c->d_P, c->d_R, 1, nullptr, c->d_red, c->d_r32);
+    if (c->mixed_kind == BPH_MIXED_DIRECT) return launch_defect_direct(c, c->d_P, c->d_R, 1, nullptr, c->d_red);
     AdiArgs a = make_args(c, sch, 0, sch.nsteps, false);
     a.norms = c->d_red;
     a.rad_pk = sch.d_rad_pk[1];  // float blocks for the FP32 kernels

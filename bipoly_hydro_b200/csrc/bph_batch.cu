@@ -837,7 +837,7 @@ int batch_reserve_converged(bph_batch *b, bool mixed) {
     // sides per position; the warp-cooperative one the rounded residual per position
     size_t need = 0;
     if (mixed && c->mixed_kind == BPH_MIXED_ADI_GLOBAL) need = 2ull * b->cap * c->N * c->np;
-    if (mixed && (c->mixed_kind == BPH_MIXED_ADI_WARP || c->mixed_kind == BPH_MIXED_DIRECT))
+    if (mixed && c->mixed_kind == BPH_MIXED_ADI_WARP)
         need = ((size_t)b->cap * c->N * c->np + 1) / 2;
     if (need > b->work32_doubles) {
         if (b->d_work32) {
@@ -899,8 +899,7 @@ int batch_converged_run(bph_batch *b, int n, const int *inst, const int *d_map, 
                 BPH_CUDA(launch_defect_warp(c, *s, b->d_P, b->d_R, n, d_map, b->d_cnorm,
                                             reinterpret_cast<float *>(b->d_work32)));
             else if (c->mixed_kind == BPH_MIXED_DIRECT)
-                BPH_CUDA(launch_defect_direct(c, b->d_P, b->d_R, n, d_map, b->d_cnorm,
-                                              reinterpret_cast<float *>(b->d_work32)));
+                BPH_CUDA(launch_defect_direct(c, b->d_P, b->d_R, n, d_map, b->d_cnorm));
             else
                 BPH_CUDA(launch_defect_batch(c, *s, b->d_P, b->d_R, n, d_map, b->d_cnorm));
         } else if (c->adi_seg) {  // update norms from the sweep's write-back

@@ -13,18 +13,18 @@
 //   (A_r + gamma lambda_q) y_q = Y_q     one radial tridiagonal per mode q
 //   delta = E^T y
 //
-// Three kernels per cycle: the FP64 residual rounded to float (one thread
-// per zone), the solve, and phi += delta with the per-slot norms (one CTA
-// per slot and block row, many resident per SM).  The solve takes one CTA
-// per (block row, slot), everything in shared memory: the residual
-// and the transformed matrix (FP32, [k][j] rows padded to 16 bytes), the
-// transform matrix (E, then E^T) and the radial sub-diagonal.
+// One kernel per cycle, one CTA per (block row, slot), two per SM: it
+// forms the residual of its slot, solves, and adds delta to phi with the
+// slot's norms, everything between in shared memory: the residual as X^T
+// ([j][k], FP32, transformed in place), the transform matrix (E, then E^T)
+// and the radial sub-diagonal.
 // The transforms run on the tensor cores (TF32 mma.sync, split in hi and
 // lo parts for FP32 accuracy), the tridiagonals one thread per mode
 // (Thomas with factors computed at set-up in FP64: the radial operator is
 // diagonally dominant and every shift gamma lambda_q is positive).  Each
 // cycle shrinks the error by about the FP32 forward error of the solve, so
 // a converged solve takes three cycles instead of four of ten ADI steps.
+#include <algorithm>
 #include <cstdlib>
 #include <vector>
 
@@ -34,19 +34,18 @@
 namespace bph {
 namespace {
 
-constexpr int kDThreads = 384;
+constexpr int kDThreads = direct::kThreads;
 
 struct DirectArgs {
     double *P;                 // slot arrays [inst][N][numr*numz], updated in place
     const double *R;           // [inst][N][nr*nz]
     const float *E, *Et;       // [nzp][lda] row-major and transposed, zero-padded
-    const float *lam;          // [nz]
     const float2 *F;           // radial Thomas factors (1/m_j, c'_j) [N][nr][nz]
     const double *brb;         // [N][numr] radial diagonal
     const double *alphar, *betar, *bzb;
     double *norms;             // per (instance, slot) |delta|^2, |phi|^2
     const int *inst_map;       // instance of each block row (nullptr: row)
-    int N, numr, numz, nr, nz, nrp, nzp, ldx, lda, isym;
+    int N, numr, numz, nr, nz, nrp, nzp, ldk, lda, cpb, isym;  // cpb: column pairs per transform block
     double gamma;
 };
 
@@ -68,44 +67,78 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// out (nzp x nrp) = A in, A in shared memory row-major with row length
-// lda (= nzp + 4: the 8 fragment rows of a load fall on different banks),
-// in and out shared [nzp][ldx].  Warp tiles of 16 rows x 32 columns
-// (four m16n8k8 tiles), three split-TF32 products per k-step:
+// X <- A X in place on the transposed layout: X^T is [nrp][ldk] in shared
+// memory (row j of X^T is column j of X; ldk = nzp + 4) and A (nzp x nzp)
+// is row-major [nzp][lda] (lda = nzp + 4).  Warp tiles of 32 rows x 16
+// columns (2 x 2 m16n8k8 tiles, three split-TF32 products each per k-step,
+// every split fragment used twice).  The column pairs are taken in blocks of
+// cpb, at most kTilesPerWarp warp tiles per warp: all products of a block
+// are formed in registers, then, after a barrier, written over it.  With both
+// strides 4 modulo 32 words the fragment loads (A row g, column t; X^T row g,
+// column t) and the accumulator stores (X^T row 2t, column g) touch 32
+// different banks.  Fragments of m16n8k8:
 //   a0 (g, t), a1 (g + 8, t), a2 (g, t + 4), a3 (g + 8, t + 4);
 //   b0 (k = t, n = g), b1 (k = t + 4, n = g);
 //   d0 (g, 2t), d1 (g, 2t + 1), d2 (g + 8, 2t), d3 (g + 8, 2t + 1).
-__device__ __forceinline__ void tc_product(const float *A, int lda, const float *in, float *out, int nzp, int nrp,
-                                           int ldx) {
+constexpr int kWarpsD = direct::kWarps;
+constexpr int kRows = 8;  // rows (radii) whose loads a thread issues together in the residual and Thomas loops
+constexpr int kTilesPerWarp = direct::kTilesPerWarp;
+
+__device__ __forceinline__ void tc_transform(const float *A, int lda, float *Xt, int ldk, int nzp, int nrp, int cpb) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    const int nti = nzp / 16, ntj = nrp / 32;
-    for (int wt = warp; wt < nti * ntj; wt += kDThreads / 32) {
-        const int i0 = 16 * (wt / ntj), j0 = 32 * (wt % ntj);
-        float acc[4][4];
+    const int cp = nrp / 16;
+    for (int cp0 = 0; cp0 < cp; cp0 += cpb) {
+        const int ncp = min(cpb, cp - cp0), tiles = (nzp / 32) * ncp;
+        float acc[kTilesPerWarp][2][2][4];
 #pragma unroll
-        for (int n = 0; n < 4; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
-        for (int k0 = 0; k0 < nzp; k0 += 8) {
-            uint32_t ah[4], al[4];
-            split_tf32(A[(i0 + g) * lda + k0 + t], ah[0], al[0]);
-            split_tf32(A[(i0 + g + 8) * lda + k0 + t], ah[1], al[1]);
-            split_tf32(A[(i0 + g) * lda + k0 + t + 4], ah[2], al[2]);
-            split_tf32(A[(i0 + g + 8) * lda + k0 + t + 4], ah[3], al[3]);
+        for (int r = 0; r < kTilesPerWarp; ++r) {
 #pragma unroll
-            for (int n = 0; n < 4; ++n) {
-                uint32_t bh0, bl0, bh1, bl1;
-                split_tf32(in[(k0 + t) * ldx + j0 + 8 * n + g], bh0, bl0);
-                split_tf32(in[(k0 + t + 4) * ldx + j0 + 8 * n + g], bh1, bl1);
-                mma_tf32(acc[n], al, bh0, bh1);
-                mma_tf32(acc[n], ah, bl0, bl1);
-                mma_tf32(acc[n], ah, bh0, bh1);
+            for (int m = 0; m < 2; ++m)
+#pragma unroll
+                for (int n = 0; n < 2; ++n)
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) acc[r][m][n][v] = 0.f;
+            const int tile = warp + kWarpsD * r;
+            if (tile >= tiles) continue;
+            int i0, c0;
+            direct::warp_tile(tile, cp0, ncp, i0, c0);
+            for (int k0 = 0; k0 < nzp; k0 += 8) {
+                uint32_t ah[2][4], al[2][4], bh[2][2], bl[2][2];
+#pragma unroll
+                for (int m = 0; m < 2; ++m)
+#pragma unroll
+                    for (int v = 0; v < 4; ++v)
+                        split_tf32(A[direct::a_offset(i0, m, k0, g, t, lda, v)], ah[m][v], al[m][v]);
+#pragma unroll
+                for (int n = 0; n < 2; ++n)
+#pragma unroll
+                    for (int v = 0; v < 2; ++v)
+                        split_tf32(Xt[direct::b_offset(c0, n, k0, g, t, ldk, v)], bh[n][v], bl[n][v]);
+#pragma unroll
+                for (int m = 0; m < 2; ++m)
+#pragma unroll
+                    for (int n = 0; n < 2; ++n) {
+                        mma_tf32(acc[r][m][n], al[m], bh[n][0], bh[n][1]);
+                        mma_tf32(acc[r][m][n], ah[m], bl[n][0], bl[n][1]);
+                        mma_tf32(acc[r][m][n], ah[m], bh[n][0], bh[n][1]);
+                    }
             }
         }
+        __syncthreads();  // every product of this block has read its columns
 #pragma unroll
-        for (int n = 0; n < 4; ++n) {
-            *reinterpret_cast<float2 *>(out + (i0 + g) * ldx + j0 + 8 * n + 2 * t) = make_float2(acc[n][0], acc[n][1]);
-            *reinterpret_cast<float2 *>(out + (i0 + g + 8) * ldx + j0 + 8 * n + 2 * t) =
-                make_float2(acc[n][2], acc[n][3]);
+        for (int r = 0; r < kTilesPerWarp; ++r) {
+            const int tile = warp + kWarpsD * r;
+            if (tile >= tiles) continue;
+            int i0, c0;
+            direct::warp_tile(tile, cp0, ncp, i0, c0);
+#pragma unroll
+            for (int m = 0; m < 2; ++m)
+#pragma unroll
+                for (int n = 0; n < 2; ++n)
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) Xt[direct::d_offset(i0, m, c0, n, g, t, ldk, v)] = acc[r][m][n][v];
         }
+        __syncthreads();
     }
 }
 
@@ -115,128 +148,173 @@ __device__ __forceinline__ void load_matrix(float *dst, const float *__restrict_
         reinterpret_cast<float4 *>(dst)[e] = __ldg(reinterpret_cast<const float4 *>(M) + e);
 }
 
-// FP64 residual r = R - A phi of the current potential, rounded to float:
-// one thread per zone, `bps` CTAs per (block row, slot), consecutive threads
-// on consecutive zones of a row; written [row][slot][k][j].
-__global__ void __launch_bounds__(256) k_direct_residual(DirectArgs a, float *r32, int bps) {
-    const int qq = blockIdx.x / bps;
-    const int s = qq % a.N, row = qq / a.N;
-    const int nr = a.nr, tot = nr * a.nz;
-    const int e = (blockIdx.x - qq * bps) * 256 + threadIdx.x;
-    pdl_wait();
-    if (e >= tot) return;
-    const long long blk = (long long)(a.inst_map ? a.inst_map[row] : row) * a.N + s;
-    const int numr = a.numr;
-    const int k = e / nr, j = e - k * nr;
-    const double *pc = a.P + blk * (long long)numr * a.numz + numr * (k + 1) + 1 + j;
-    const double c = pc[0], ea = pc[1], no = pc[numr];
-    const double we = (j > 0) ? pc[-1] : 0.0;
-    const double so = (k > 0 || a.isym == 1) ? pc[-numr] : 0.0;
-    const double ar = a.brb[(long long)s * numr + j + 1] * c + a.alphar[j + 1] * ea + a.betar[j + 1] * we;
-    const double az = a.bzb[k + 1] * c - a.gamma * no - a.gamma * so;
-    r32[((long long)row * a.N + s) * tot + e] = (float)(a.R[blk * tot + e] - ar - az);
-}
-
-// phi += delta (delta rounded to float, [row][slot][k][j]) in FP64, with the
-// per-slot |delta|^2 and |phi|^2: one CTA per (block row, slot).
-__global__ void __launch_bounds__(256) k_direct_update(DirectArgs a, const float *d32) {
+// One refinement cycle of a slot: one CTA per (block row, slot), two per SM.
+//  1. r = R - A phi in FP64, rounded into X^T.  A warp takes 32 columns and
+//     a band of rows and sweeps up the band with the rows below and at hand
+//     in registers (east and west neighbours by shuffle), so every potential
+//     value is read once; the Dirichlet columns enter through the stencil.
+//  2. X <- E X.  3. (A_r + gamma lambda_q) y_q = (E r)_q for every mode q:
+//     Thomas sweeps, one thread per mode, with the slot's factors
+//     (1/m_j, c'_j) from set-up read coalesced over q.  4. X <- E^T X.
+//  5. phi += delta in FP64, with the slot's |delta|^2 and |phi|^2.
+__global__ void __launch_bounds__(kDThreads, 2) k_defect_direct(DirectArgs a) {
+    extern __shared__ __align__(16) float dsm[];
+    __shared__ double red[2][kWarpsD];
+    const int nzp = a.nzp, ldk = a.ldk, nr = a.nr, nz = a.nz, numr = a.numr;
+    float *Xt = dsm;                  // [nrp][ldk]: residual, E r, the radial solutions, delta
+    float *Ms = Xt + a.nrp * ldk;     // E, then E^T ([nzp][lda])
+    float *cl = Ms + nzp * a.lda;     // radial coefficient of j - 1
     const int s = blockIdx.x % a.N, row = blockIdx.x / a.N;
-    const long long blk = (long long)(a.inst_map ? a.inst_map[row] : row) * a.N + s;
-    const int nr = a.nr, tot = nr * a.nz, numr = a.numr;
-    double *Pg = a.P + blk * (long long)numr * a.numz;
-    const float *dg = d32 + ((long long)row * a.N + s) * tot;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int j = threadIdx.x; j < nr; j += kDThreads) cl[j] = (float)a.betar[j + 1];
+    load_matrix(Ms, a.E, nzp, a.lda);
+    for (int e = threadIdx.x; e < a.nrp * nzp; e += kDThreads) {  // padding: columns j >= nr, rows k >= nz
+        const int j = e / nzp, k = e - j * nzp;
+        if (j >= nr || k >= nz) Xt[j * ldk + k] = 0.f;
+    }
     pdl_wait();
-    double sd = 0.0, sp = 0.0;
+    const long long blk = (long long)(a.inst_map ? a.inst_map[row] : row) * a.N + s;
+    double *Pg = a.P + blk * (long long)numr * a.numz;
+    const double *Rg = a.R + blk * (long long)nr * nz;
+    {
+        for (int it = warp; it < direct::sweep_items(nr); it += kWarpsD) {
+            int jc, k0, k1;
+            direct::sweep_item(it, nr, nz, jc, k0, k1);
+            if (k0 >= k1) continue;  // warp-uniform
+            const int j = jc + lane;
+            const bool on = j < nr;
+            const double *col = Pg + min(j, nr) + 1;  // interior column, or the outer Dirichlet column
+            const double br = on ? a.brb[(long long)s * numr + j + 1] : 0.0;
+            const double al = on ? a.alphar[j + 1] : 0.0;
+            const double be = on ? a.betar[j + 1] : 0.0;
+            double so = (k0 > 0 || a.isym == 1) ? col[(long long)numr * k0] : 0.0;
+            double c = col[(long long)numr * (k0 + 1)];
+            for (int kb = k0; kb < k1; kb += kRows) {  // the loads of kRows rows in flight at once
+                // edge: the east neighbour of lane 31, the west neighbour of lane 0
+                double no[kRows], rr[kRows], edge[kRows], bz[kRows];
+#pragma unroll
+                for (int u = 0; u < kRows; ++u) {
+                    const int k = kb + u;
+                    if (k >= k1) break;  // warp-uniform
+                    no[u] = col[(long long)numr * (k + 2)];
+                    rr[u] = on ? Rg[(long long)k * nr + j] : 0.0;
+                    edge[u] = (lane == 31 && on)  ? col[(long long)numr * (k + 1) + 1]
+                              : (lane == 0 && j > 0) ? col[(long long)numr * (k + 1) - 1]
+                                                     : 0.0;
+                    bz[u] = a.bzb[k + 1];
+                }
+#pragma unroll
+                for (int u = 0; u < kRows; ++u) {
+                    const int k = kb + u;
+                    if (k >= k1) break;
+                    const double e_ = __shfl_down_sync(0xffffffffu, c, 1);
+                    const double w_ = __shfl_up_sync(0xffffffffu, c, 1);
+                    const double east = (lane == 31) ? edge[u] : e_;
+                    const double west = (lane == 0) ? edge[u] : w_;
+                    const double ar = br * c + al * east + be * west;
+                    const double az = bz[u] * c - a.gamma * no[u] - a.gamma * so;
+                    if (on) Xt[j * ldk + k] = (float)(rr[u] - ar - az);
+                    so = c;
+                    c = no[u];
+                }
+            }
+        }
+    }
+    __syncthreads();
+    tc_transform(Ms, a.lda, Xt, ldk, nzp, a.nrp, a.cpb);  // 2. X <- E X
+    load_matrix(Ms, a.Et, nzp, a.lda);                     // for step 4; E has no reader left
+    const float2 *fs = a.F + (long long)s * nr * nz;
+    for (int q = threadIdx.x; q < nz; q += kDThreads) {    // 3. one radial tridiagonal per mode
+        float *yq = Xt + q;
+        const float2 *fq = fs + q;
+        // the factors of kRows radii are loaded while the previous kRows are used
+        auto load = [&](float2 (&f)[kRows], int j0, int dir) {
+#pragma unroll
+            for (int u = 0; u < kRows; ++u) {
+                const int j = j0 + dir * u;
+                f[u] = (j >= 0 && j < nr) ? __ldg(fq + (long long)j * nz) : make_float2(0.f, 0.f);
+            }
+        };
+        // a batch of kRows radii: the values and coefficients are read first (the
+        // stores of the previous radii cannot then delay them), then the recurrence
+        float dp = 0.f;
+        auto forward = [&](const float2 (&f)[kRows], int j0) {
+            float v[kRows], lo[kRows];
+#pragma unroll
+            for (int u = 0; u < kRows; ++u) {
+                const int j = j0 + u;
+                v[u] = (j < nr) ? yq[j * ldk] : 0.f;
+                lo[u] = (j > 0 && j < nr) ? cl[j] : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < kRows; ++u) {
+                if (j0 + u >= nr) break;  // the last value carries into the backward sweep
+                dp = (v[u] - lo[u] * dp) * f[u].x;
+                v[u] = dp;
+            }
+#pragma unroll
+            for (int u = 0; u < kRows; ++u)
+                if (j0 + u < nr) yq[(j0 + u) * ldk] = v[u];
+        };
+        float2 f0[kRows], f1[kRows];
+        load(f0, 0, 1);
+        for (int j0 = 0; j0 < nr; j0 += 2 * kRows) {
+            load(f1, j0 + kRows, 1);
+            forward(f0, j0);
+            load(f0, j0 + 2 * kRows, 1);
+            forward(f1, j0 + kRows);
+        }
+        float y = dp;
+        auto backward = [&](const float2 (&f)[kRows], int j0) {
+            float v[kRows];
+#pragma unroll
+            for (int u = 0; u < kRows; ++u) v[u] = (j0 - u >= 0) ? yq[(j0 - u) * ldk] : 0.f;
+#pragma unroll
+            for (int u = 0; u < kRows; ++u) {
+                if (j0 - u < 0) break;
+                y = v[u] - f[u].y * y;
+                v[u] = y;
+            }
+#pragma unroll
+            for (int u = 0; u < kRows; ++u)
+                if (j0 - u >= 0) yq[(j0 - u) * ldk] = v[u];
+        };
+        load(f0, nr - 2, -1);
+        for (int j0 = nr - 2; j0 >= 0; j0 -= 2 * kRows) {
+            load(f1, j0 - kRows, -1);
+            backward(f0, j0);
+            load(f0, j0 - 2 * kRows, -1);
+            backward(f1, j0 - kRows);
+        }
+    }
+    __syncthreads();
+    tc_transform(Ms, a.lda, Xt, ldk, nzp, a.nrp, a.cpb);  // 4. delta = E^T y
+    double sd = 0.0, sp = 0.0;                              // 5. phi += delta
 #pragma unroll 4
-    for (int e = threadIdx.x; e < tot; e += 256) {
+    for (int e = threadIdx.x; e < nr * nz; e += kDThreads) {
         const int k = e / nr, j = e - k * nr;
-        const double d = (double)dg[e];
-        double *pp = Pg + numr * (k + 1) + 1 + j;
+        const double d = (double)Xt[j * ldk + k];
+        double *pp = Pg + (long long)numr * (k + 1) + 1 + j;
         const double ph = *pp + d;
         *pp = ph;
         sd += d * d;
         sp += ph * ph;
     }
-    __shared__ double red[2][8];
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         sd += __shfl_down_sync(0xffffffffu, sd, off);
         sp += __shfl_down_sync(0xffffffffu, sp, off);
     }
-    if ((threadIdx.x & 31) == 0) {
-        red[0][threadIdx.x >> 5] = sd;
-        red[1][threadIdx.x >> 5] = sp;
+    if (lane == 0) {
+        red[0][warp] = sd;
+        red[1][warp] = sp;
     }
     __syncthreads();
     if (threadIdx.x < 2) {
         double t = 0.0;
-        for (int w = 0; w < 8; ++w) t += red[threadIdx.x][w];
+        for (int w = 0; w < kWarpsD; ++w) t += red[threadIdx.x][w];
         const double wgt = (s == 0 || s == a.N / 2) ? 1.0 : 2.0;
         a.norms[2 * blk + threadIdx.x] = wgt * t;
-    }
-}
-
-__device__ __forceinline__ void cp4(float *dst, const float *src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
-                 : "memory");
-}
-
-__global__ void __launch_bounds__(kDThreads, 1) k_defect_direct(DirectArgs a, float *r32) {
-    extern __shared__ __align__(16) float dsm[];
-    const int nzp = a.nzp, ldx = a.ldx, nr = a.nr, nz = a.nz, numr = a.numr;
-    float *X = dsm;                   // residual, then the Thomas carries, then delta
-    float *Y = dsm + nzp * ldx;       // E X, then the radial solutions
-    float *Ms = Y + nzp * ldx;        // E, then E^T ([nzp][lda])
-    float *cl = Ms + nzp * a.lda;     // radial coefficient of j - 1
-    const int s = blockIdx.x % a.N, row = blockIdx.x / a.N;
-    float *rg = r32 + ((long long)row * a.N + s) * (long long)nr * nz;  // residual in, delta out
-    for (int j = threadIdx.x; j < nr; j += kDThreads) cl[j] = (float)a.betar[j + 1];
-    load_matrix(Ms, a.E, nzp, a.lda);
-    // zero padding of X (rows k >= nz, columns j >= nr), then the residual by cp.async
-    for (int e = threadIdx.x; e < nzp * ldx; e += kDThreads) {
-        const int k = e / ldx, j = e - k * ldx;
-        if (k >= nz || j >= nr) X[e] = 0.f;
-    }
-    pdl_wait();
-    for (int e = threadIdx.x; e < nz * nr; e += kDThreads) {
-        const int k = e / nr, j = e - k * nr;
-        cp4(X + k * ldx + j, rg + e);
-    }
-    asm volatile("cp.async.commit_group;\ncp.async.wait_all;" ::: "memory");
-    __syncthreads();
-    // 2. Y = E X
-    tc_product(Ms, a.lda, X, Y, nzp, a.nrp, ldx);
-    __syncthreads();
-    load_matrix(Ms, a.Et, nzp, a.lda);  // for step 4; no reader of E is left
-    // 3. (A_r + gamma lambda_q) y_q = Y_q for every mode q: Thomas sweeps with the
-    //    slot's factors (1/m_j, c'_j) from set-up, read coalesced over q
-    const float2 *fs = a.F + (long long)s * nr * nz;
-    for (int q = threadIdx.x; q < nz; q += kDThreads) {
-        float *yq = Y + q * ldx;
-        float dp = 0.f;
-#pragma unroll 8
-        for (int j = 0; j < nr; ++j) {
-            const float lo = (j > 0) ? cl[j] : 0.f;
-            const float2 f = __ldg(fs + (long long)j * nz + q);
-            dp = (yq[j] - lo * dp) * f.x;
-            yq[j] = dp;
-        }
-        float y = dp;
-#pragma unroll 8
-        for (int j = nr - 2; j >= 0; --j) {
-            const float2 f = __ldg(fs + (long long)j * nz + q);
-            y = yq[j] - f.y * y;
-            yq[j] = y;
-        }
-    }
-    __syncthreads();
-    // 4. delta = E^T y (into X)
-    tc_product(Ms, a.lda, Y, X, nzp, a.nrp, ldx);
-    __syncthreads();
-    // 5. delta (float) over the residual, for k_direct_update
-    for (int e = threadIdx.x; e < nz * nr; e += kDThreads) {
-        const int k = e / nr, j = e - k * nr;
-        rg[e] = X[k * ldx + j];
     }
     pdl_trigger();
 }
@@ -259,35 +337,20 @@ __global__ void k_direct_factors(const double *__restrict__ brb, const double *_
     }
 }
 
-struct DirectShape {
-    int nrp, nzp, ldx, lda;
-    size_t smem;
-};
-
-DirectShape direct_shape(int nr, int nz) {
-    DirectShape d;
-    d.nrp = (nr + 31) / 32 * 32;  // warp tiles of 32 columns
-    d.nzp = (nz + 15) / 16 * 16;  // and 16 rows
-    d.ldx = d.nrp + 4;            // rows stay 16-byte aligned; the Thomas threads spread over 8 banks
-    d.lda = d.nzp + 4;            // fragment rows of E on different banks
-    d.smem = sizeof(float) * ((size_t)2 * d.nzp * d.ldx + (size_t)d.nzp * d.lda + (size_t)nr);
-    return d;
-}
-
 }  // namespace
 
 int direct_configure(bph_ctx *c) {
     c->mixed_smem_kind[BPH_MIXED_DIRECT] = 0;
-    const DirectShape d = direct_shape(c->nr, c->nz);
+    const direct::Shape d = direct::shape(c->nr, c->nz);
     int dev_max = 0;
     cudaError_t e = cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
-    if (d.smem + 2 * sizeof(double) * (kDThreads / 32) > (size_t)dev_max) return BPH_OK;  // slot beyond shared memory
+    const size_t smem = sizeof(float) * d.floats;
+    if (d.cpb == 0 || smem > (size_t)dev_max) return BPH_OK;  // slot beyond one CTA: kind not offered
     std::vector<long double> E, lam;
     direct::vertical_eigen(c->nz, c->g.isym, E, lam);
-    std::vector<float> hE((size_t)d.nzp * d.lda, 0.f), hEt((size_t)d.nzp * d.lda, 0.f), hl((size_t)c->nz);
+    std::vector<float> hE((size_t)d.nzp * d.lda, 0.f), hEt((size_t)d.nzp * d.lda, 0.f);
     for (int q = 0; q < c->nz; ++q) {
-        hl[q] = (float)lam[q];
         for (int k = 0; k < c->nz; ++k) {
             const float v = (float)E[(size_t)q * c->nz + k];
             hE[(size_t)q * d.lda + k] = v;
@@ -295,17 +358,15 @@ int direct_configure(bph_ctx *c) {
         }
     }
     const size_t ne = hE.size();
-    e = cudaMalloc((void **)&c->d_dir32, sizeof(float) * (2 * ne + (size_t)c->nz));
+    e = cudaMalloc((void **)&c->d_dir32, sizeof(float) * 2 * ne);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(direct solve tables)");
-    c->bytes += sizeof(float) * (2 * ne + (size_t)c->nz);
+    c->bytes += sizeof(float) * 2 * ne;
     e = cudaMemcpy(c->d_dir32, hE.data(), sizeof(float) * ne, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(c->d_dir32 + ne, hEt.data(), sizeof(float) * ne, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess)
-        e = cudaMemcpy(c->d_dir32 + 2 * ne, hl.data(), sizeof(float) * (size_t)c->nz, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = raise_smem_limit((const void *)k_defect_direct, (int)d.smem);
+    if (e == cudaSuccess) e = raise_smem_limit((const void *)k_defect_direct, (int)smem);
     int per_sm = 0;
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_defect_direct, kDThreads, d.smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_defect_direct, kDThreads, smem);
     if (e != cudaSuccess) return cuda_fail(e, "direct solve set-up");
     {
         // radial factors for every (slot, mode), from the eigenvalues in FP64
@@ -329,29 +390,21 @@ int direct_configure(bph_ctx *c) {
         if (e != cudaSuccess) return cuda_fail(e, "direct solve factors");
         c->bytes += sizeof(float2) * nf;
     }
-    if (!c->d_r32) {
-        const size_t n32 = (size_t)c->N * c->np;
-        e = cudaMalloc((void **)&c->d_r32, sizeof(float) * n32);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(rounded residual)");
-        c->bytes += sizeof(float) * n32;
-    }
-    c->mixed_smem_kind[BPH_MIXED_DIRECT] = (int)d.smem;
+    c->mixed_smem_kind[BPH_MIXED_DIRECT] = (int)smem;
     c->mixed_per_sm_kind[BPH_MIXED_DIRECT] = per_sm;
     return BPH_OK;
 }
 
 cudaError_t launch_defect_direct(bph_ctx *c, double *P, const double *R, int nrows, const int *inst_map,
-                                 double *norms, float *r32) {
-    if (!c->mixed_smem_kind[BPH_MIXED_DIRECT] || !c->d_dir32 || !c->d_dirF || !norms || !r32)
-        return cudaErrorNotSupported;
-    const DirectShape d = direct_shape(c->nr, c->nz);
+                                 double *norms) {
+    if (!c->mixed_smem_kind[BPH_MIXED_DIRECT] || !c->d_dir32 || !c->d_dirF || !norms) return cudaErrorNotSupported;
+    const direct::Shape d = direct::shape(c->nr, c->nz);
     const size_t ne = (size_t)d.nzp * d.lda;
     DirectArgs a;
     a.P = P;
     a.R = R;
     a.E = c->d_dir32;
     a.Et = c->d_dir32 + ne;
-    a.lam = c->d_dir32 + 2 * ne;
     a.F = reinterpret_cast<const float2 *>(c->d_dirF);
     a.brb = c->d_brb;
     a.alphar = c->d_alphar;
@@ -366,21 +419,15 @@ cudaError_t launch_defect_direct(bph_ctx *c, double *P, const double *R, int nro
     a.nz = c->nz;
     a.nrp = d.nrp;
     a.nzp = d.nzp;
-    a.ldx = d.ldx;
+    a.ldk = d.ldk;
     a.lda = d.lda;
+    a.cpb = d.cpb;
     a.isym = c->g.isym;
     a.gamma = c->gamma;
-    c->launches += 3;
-    const int bps = (c->nr * c->nz + 255) / 256;
+    c->launches += 1;
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = launch_config(c, dim3((unsigned)((long long)bps * c->N * nrows)), dim3(256), 0, attr);
-    cudaError_t e = cudaLaunchKernelEx(&cfg, k_direct_residual, a, r32, bps);
-    if (e != cudaSuccess) return e;
-    cfg = launch_config(c, dim3((unsigned)(c->N * nrows)), dim3(kDThreads), d.smem, attr);
-    e = cudaLaunchKernelEx(&cfg, k_defect_direct, a, r32);
-    if (e != cudaSuccess) return e;
-    cfg = launch_config(c, dim3((unsigned)(c->N * nrows)), dim3(256), 0, attr);
-    return cudaLaunchKernelEx(&cfg, k_direct_update, a, (const float *)r32);
+    cudaLaunchConfig_t cfg = launch_config(c, dim3((unsigned)(c->N * nrows)), dim3(kDThreads), sizeof(float) * d.floats, attr);
+    return cudaLaunchKernelEx(&cfg, k_defect_direct, a);
 }
 
 }  // namespace bph

@@ -16,14 +16,85 @@
 // With E the orthonormal eigenvector matrix (rows q), A x = r becomes
 // (A_r + gamma lambda_q) y_q = (E r)_q for every vertical mode q, and
 // x = E^T y: one transform, nz radial tridiagonal solves, one transform.
-// Plain C++ (long double), shared by the set-up and a host-side check.
+// Plain C++ (long double), shared by the set-up and a host-side check,
+// with the index arithmetic of the solve kernel (host and device).
 #pragma once
 
 #include <cmath>
+#include <cstddef>
 #include <vector>
+
+#if defined(__CUDACC__)
+#define BPH_DIRECT_HD __host__ __device__ __forceinline__
+#else
+#define BPH_DIRECT_HD inline
+#endif
 
 namespace bph {
 namespace direct {
+
+constexpr int kThreads = 256;                      // one CTA per (block row, slot), two per SM
+constexpr int kWarps = kThreads / 32;
+constexpr int kTilesPerWarp = 3;                   // 32 x 16 warp tiles per warp and transform block
+constexpr int kBlockTiles = kTilesPerWarp * kWarps;  // 24: a 96 x 128 slot in one block
+
+// Shared-memory shape of a slot of nr x nz interior zones: X^T [nrp][ldk]
+// (row j = column j of the [k][j] slot matrix), the transform [nzp][lda],
+// the radial sub-diagonal [nr].  Both strides are 4 modulo the 32 banks.
+// cpb = column pairs (16 columns) per transform block; 0 when one block
+// row of 32 modes already needs more warp tiles than the CTA holds.
+struct Shape {
+    int nrp, nzp, ldk, lda, cpb;
+    size_t floats;
+};
+BPH_DIRECT_HD Shape shape(int nr, int nz) {
+    Shape d;
+    d.nrp = (nr + 15) / 16 * 16;
+    d.nzp = (nz + 31) / 32 * 32;
+    d.ldk = d.nzp + 4;
+    d.lda = d.nzp + 4;
+    const int rp = d.nzp / 32, cp = d.nrp / 16;
+    d.cpb = (rp > kBlockTiles) ? 0 : ((cp < kBlockTiles / rp) ? cp : kBlockTiles / rp);
+    d.floats = (size_t)d.nrp * d.ldk + (size_t)d.nzp * d.lda + (size_t)nr;
+    return d;
+}
+
+// Warp tile `tile` of the transform block starting at column pair cp0 with
+// ncp column pairs: its first output row (mode) i0 and column c0.
+BPH_DIRECT_HD void warp_tile(int tile, int cp0, int ncp, int &i0, int &c0) {
+    i0 = 32 * (tile / ncp);
+    c0 = 16 * (cp0 + tile % ncp);
+}
+// m16n8k8 fragments of lane (g = lane / 4, t = lane % 4) in the warp tile
+// (i0, c0), sub-tile (m, n), k-step k0, as word offsets:
+//   A [nzp][lda]: a0 (g, t), a1 (g + 8, t), a2 (g, t + 4), a3 (g + 8, t + 4);
+//   X^T [nrp][ldk]: b0 (k = t, n = g), b1 (k = t + 4, n = g);
+//   X^T for the result: d0 (g, 2t), d1 (g, 2t + 1), d2 (g + 8, 2t),
+//   d3 (g + 8, 2t + 1) of the 16 x 8 sub-tile, row = mode, column = j.
+BPH_DIRECT_HD int a_offset(int i0, int m, int k0, int g, int t, int lda, int v) {
+    return (i0 + 16 * m + g + 8 * (v & 1)) * lda + k0 + t + 4 * (v >> 1);
+}
+BPH_DIRECT_HD int b_offset(int c0, int n, int k0, int g, int t, int ldk, int v) {
+    return (c0 + 8 * n + g) * ldk + k0 + t + 4 * v;
+}
+BPH_DIRECT_HD int d_offset(int i0, int m, int c0, int n, int g, int t, int ldk, int v) {
+    return (c0 + 8 * n + 2 * t + (v & 1)) * ldk + i0 + 16 * m + g + 8 * (v >> 1);
+}
+
+// Residual sweep item `it` of kWarps warps: columns jc .. jc + 31 and rows
+// [k0, k1) (k0 >= k1: nothing); items = column chunks x bands.
+BPH_DIRECT_HD int sweep_items(int nr) {
+    const int nchunk = (nr + 31) / 32;
+    return nchunk * ((kWarps / nchunk > 1) ? kWarps / nchunk : 1);
+}
+BPH_DIRECT_HD void sweep_item(int it, int nr, int nz, int &jc, int &k0, int &k1) {
+    const int nchunk = (nr + 31) / 32;
+    const int nband = (kWarps / nchunk > 1) ? kWarps / nchunk : 1;
+    const int band_rows = (nz + nband - 1) / nband;
+    jc = (it % nchunk) * 32;
+    k0 = (it / nchunk) * band_rows;
+    k1 = (k0 + band_rows < nz) ? k0 + band_rows : nz;
+}
 
 // E (nz x nz, row q = eigenvector q, orthonormal) and lambda (nz) of T.
 inline void vertical_eigen(int nz, int isym, std::vector<long double> &E, std::vector<long double> &lambda) {

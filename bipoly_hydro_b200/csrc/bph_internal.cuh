@@ -198,7 +198,7 @@ struct bph_ctx {
     double *d_warp_coef = nullptr;     // its per-slot (elambdazb, alphaz, betaz) blocks
     int mixed_warp = 0;                // FP32 warp-cooperative refinement kernel available
     float *d_warp_coef32 = nullptr;    // its coefficient blocks
-    float *d_r32 = nullptr;            // rounded residual of one solve [N][np] (FP32 warp and direct refinement)
+    float *d_r32 = nullptr;            // rounded residual of one solve [N][np] (FP32 warp refinement)
     double *d_scf = nullptr;           // SCF-step mass partials and scale (bph_scf.cu)
     void *noalloc_scratch = nullptr;   // device address of the allocation-free contraction's scratch array
     long long launches = 0;
@@ -353,11 +353,11 @@ int contract_configure(bph_ctx *c);
 // off), bph_setup.cu builds them.
 int compact_configure(bph_ctx *c);
 // Direct FP32 defect solve (bph_direct.cu): set-up of its tables, and one
-// refinement cycle for nrows block rows (instance of a row: inst_map;
-// r32: nrows x N x np floats of scratch).
+// refinement cycle for nrows block rows (instance of a row: inst_map), in
+// one launch with no scratch in global memory.
 int direct_configure(bph_ctx *c);
 cudaError_t launch_defect_direct(bph_ctx *c, double *P, const double *R, int nrows, const int *inst_map,
-                                 double *norms, float *r32);
+                                 double *norms);
 cudaError_t launch_green_compact(bph_ctx *c);
 // Warp-cooperative FP64 ADI (bph_adi_warp.cu).  warp_configure selects it
 // for the grids it covers (c->adi_warp != 0) and packs the per-slot

@@ -333,13 +333,14 @@ def test_warm_start_from_checkpointed_potential(oracle_mod, bph):
 
 
 def test_mixed_adi_autotune_and_selection(bph):
-    """Setup times the on-chip refinement ADI kernels at 130x98x256 (forwarding,
-    increment, warp-cooperative) and keeps the fastest; an explicit choice
-    sticks; an unknown kind is rejected."""
+    """Setup times the on-chip refinement kernels at 130x98x256 (forwarding,
+    increment, warp-cooperative ADI, direct solve) and keeps the fastest; an
+    explicit choice sticks; an unknown kind is rejected."""
     g = bph.PotentialSolver(130, 98, 256, 1.0 / 126.0, 2, 30)
     info = g.info()
-    assert info["mixed_kind"] in (1, 2, 4)
-    times = {1: info["mixed_forward_ns"], 2: info["mixed_increment_ns"], 4: info["mixed_warp_ns"]}
+    assert info["mixed_kind"] in (1, 2, 4, 5)
+    times = {1: info["mixed_forward_ns"], 2: info["mixed_increment_ns"], 4: info["mixed_warp_ns"],
+             5: info["mixed_direct_ns"]}
     assert all(t > 0 for t in times.values()), times
     assert info["mixed_kind"] == min(times, key=times.get)
     g.set_mixed_adi(2)

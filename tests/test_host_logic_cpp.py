@@ -17,7 +17,11 @@
   ragged tile edges, odd radial counts and both symmetry classes.
 * bph_direct.h: the closed-form eigenvectors of the vertical second
   difference (reflecting or Dirichlet bottom) are orthonormal and
-  diagonalise it, the basis of the direct defect solve.
+  diagonalise it, the basis of the direct defect solve; and the solve
+  kernel's index arithmetic, emulated lane by lane: the fragment offsets
+  follow the m16n8k8 lane layout, the in-place transform over the warp
+  tiles equals the dense product with every output written once, and the
+  residual sweep equals the per-zone FP64 residual bit for bit.
 """
 import os
 import re
@@ -70,3 +74,9 @@ def test_library_selects_devices_only_through_the_scope():
         for m in re.finditer(r"cudaSetDevice\s*\(", text):
             offenders.append(f"{name}:{text[:m.start()].count(chr(10)) + 1}")
     assert not offenders, offenders
+
+
+def test_direct_kernel_index_arithmetic(tmp_path):
+    out = _run(tmp_path, "direct_tiles_check")
+    assert "all checks passed" in out
+    assert "nr 128 nz  96: cpb 8, 90112 bytes" in out
