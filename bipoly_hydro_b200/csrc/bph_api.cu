@@ -670,7 +670,7 @@ static void ctx_free(bph_ctx *c) {
     dev_free(c->d_warp_coef32);
     dev_free(c->d_r32);
     dev_free(c->d_dir32);
-    dev_free(c->d_dirF);
+    dev_free(c->d_dirS);
     dev_free(c->d_scf);
     if (c->side_stream) {
         cudaStreamSynchronize(c->side_stream);

@@ -16,11 +16,11 @@
 // One kernel per cycle, one CTA per (block row, slot), two per SM: it
 // forms the residual of its slot, solves, and adds delta to phi with the
 // slot's norms, everything between in shared memory: the residual as X^T
-// ([j][k], FP32, transformed in place), the transform matrix (E, then E^T)
-// and the radial sub-diagonal.
+// ([j][k], FP32, transformed in place), the transform matrix (E, then E^T),
+// the radial coefficients of the slot and the Thomas ratios.
 // The transforms run on the tensor cores (TF32 mma.sync, split in hi and
 // lo parts for FP32 accuracy), the tridiagonals one thread per mode
-// (Thomas with factors computed at set-up in FP64: the radial operator is
+// (Thomas in FP32 with factors formed on the way: the radial operator is
 // diagonally dominant and every shift gamma lambda_q is positive).  Each
 // cycle shrinks the error by about the FP32 forward error of the solve, so
 // a converged solve takes three cycles instead of four of ten ADI steps.
@@ -40,12 +40,13 @@ struct DirectArgs {
     double *P;                 // slot arrays [inst][N][numr*numz], updated in place
     const double *R;           // [inst][N][nr*nz]
     const float *E, *Et;       // [nzp][lda] row-major and transposed, zero-padded
-    const float2 *F;           // radial Thomas factors (1/m_j, c'_j) [N][nr][nz]
+    const double *sig;         // [nz] vertical shifts gamma lambda_q (FP64)
     const double *brb;         // [N][numr] radial diagonal
     const double *alphar, *betar, *bzb;
     double *norms;             // per (instance, slot) |delta|^2, |phi|^2
     const int *inst_map;       // instance of each block row (nullptr: row)
     int N, numr, numz, nr, nz, nrp, nzp, ldk, lda, cpb, isym;  // cpb: column pairs per transform block
+    int off_bd, off_ms, off_lo, off_up;                        // shared-memory regions (floats)
     double gamma;
 };
 
@@ -154,19 +155,24 @@ __device__ __forceinline__ void load_matrix(float *dst, const float *__restrict_
 //     in registers (east and west neighbours by shuffle), so every potential
 //     value is read once; the Dirichlet columns enter through the stencil.
 //  2. X <- E X.  3. (A_r + gamma lambda_q) y_q = (E r)_q for every mode q:
-//     Thomas sweeps, one thread per mode, with the slot's factors
-//     (1/m_j, c'_j) from set-up read coalesced over q.  4. X <- E^T X.
+//     Thomas sweeps, one thread per mode, from the slot's radial
+//     coefficients in shared memory.  4. X <- E^T X.
 //  5. phi += delta in FP64, with the slot's |delta|^2 and |phi|^2.
 __global__ void __launch_bounds__(kDThreads, 2) k_defect_direct(DirectArgs a) {
     extern __shared__ __align__(16) float dsm[];
     __shared__ double red[2][kWarpsD];
     const int nzp = a.nzp, ldk = a.ldk, nr = a.nr, nz = a.nz, numr = a.numr;
-    float *Xt = dsm;                  // [nrp][ldk]: residual, E r, the radial solutions, delta
-    float *Ms = Xt + a.nrp * ldk;     // E, then E^T ([nzp][lda])
-    float *cl = Ms + nzp * a.lda;     // radial coefficient of j - 1
+    float *Xt = dsm;                                              // [nrp][ldk]: r, E r, y, delta
+    double *bd = reinterpret_cast<double *>(dsm + a.off_bd);      // radial diagonal of the slot
+    float *Ms = dsm + a.off_ms;                                   // E; the ratios c' [nr][nz]; E^T
+    float *cl = dsm + a.off_lo, *cu = dsm + a.off_up;             // radial coefficients of j - 1, j + 1
     const int s = blockIdx.x % a.N, row = blockIdx.x / a.N;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int j = threadIdx.x; j < nr; j += kDThreads) cl[j] = (float)a.betar[j + 1];
+    for (int j = threadIdx.x; j < nr; j += kDThreads) {
+        bd[j] = a.brb[(long long)s * numr + j + 1];
+        cl[j] = (float)a.betar[j + 1];
+        cu[j] = (float)a.alphar[j + 1];
+    }
     load_matrix(Ms, a.E, nzp, a.lda);
     for (int e = threadIdx.x; e < a.nrp * nzp; e += kDThreads) {  // padding: columns j >= nr, rows k >= nz
         const int j = e / nzp, k = e - j * nzp;
@@ -222,71 +228,64 @@ __global__ void __launch_bounds__(kDThreads, 2) k_defect_direct(DirectArgs a) {
     }
     __syncthreads();
     tc_transform(Ms, a.lda, Xt, ldk, nzp, a.nrp, a.cpb);  // 2. X <- E X
-    load_matrix(Ms, a.Et, nzp, a.lda);                     // for step 4; E has no reader left
-    const float2 *fs = a.F + (long long)s * nr * nz;
-    for (int q = threadIdx.x; q < nz; q += kDThreads) {    // 3. one radial tridiagonal per mode
+    // 3. (A_r + gamma lambda_q) y_q = (E r)_q for every mode q, one thread per mode:
+    //    Thomas sweeps with the factors formed on the way down (m_j = b_j + gamma
+    //    lambda_q - beta_j c'_{j-1}, c'_j = alpha_j / m_j; the ratios kept in the
+    //    transform's region for the way up).  A batch of kRows radii reads its
+    //    values and coefficients first, then runs the recurrence.
+    float *cr = Ms;  // [nr][nz]; E has no reader left
+    for (int q = threadIdx.x; q < nz; q += kDThreads) {
         float *yq = Xt + q;
-        const float2 *fq = fs + q;
-        // the factors of kRows radii are loaded while the previous kRows are used
-        auto load = [&](float2 (&f)[kRows], int j0, int dir) {
+        const double sq = a.sig[q];
+        float cp = 0.f, dp = 0.f;
+        for (int j0 = 0; j0 < nr; j0 += kRows) {
+            float v[kRows], lo[kRows], up[kRows], dg[kRows];
 #pragma unroll
             for (int u = 0; u < kRows; ++u) {
-                const int j = j0 + dir * u;
-                f[u] = (j >= 0 && j < nr) ? __ldg(fq + (long long)j * nz) : make_float2(0.f, 0.f);
-            }
-        };
-        // a batch of kRows radii: the values and coefficients are read first (the
-        // stores of the previous radii cannot then delay them), then the recurrence
-        float dp = 0.f;
-        auto forward = [&](const float2 (&f)[kRows], int j0) {
-            float v[kRows], lo[kRows];
-#pragma unroll
-            for (int u = 0; u < kRows; ++u) {
-                const int j = j0 + u;
-                v[u] = (j < nr) ? yq[j * ldk] : 0.f;
-                lo[u] = (j > 0 && j < nr) ? cl[j] : 0.f;
+                const int j = (j0 + u < nr) ? j0 + u : nr - 1;
+                v[u] = yq[j * ldk];
+                lo[u] = (j > 0) ? cl[j] : 0.f;
+                up[u] = cu[j];
+                dg[u] = (float)(bd[j] + sq);
             }
 #pragma unroll
             for (int u = 0; u < kRows; ++u) {
-                if (j0 + u >= nr) break;  // the last value carries into the backward sweep
-                dp = (v[u] - lo[u] * dp) * f[u].x;
+                if (j0 + u >= nr) break;  // the last values carry into the way up
+                const float rm = __frcp_rn(dg[u] - lo[u] * cp);
+                dp = (v[u] - lo[u] * dp) * rm;
+                cp = up[u] * rm;
                 v[u] = dp;
+                up[u] = cp;
             }
 #pragma unroll
             for (int u = 0; u < kRows; ++u)
-                if (j0 + u < nr) yq[(j0 + u) * ldk] = v[u];
-        };
-        float2 f0[kRows], f1[kRows];
-        load(f0, 0, 1);
-        for (int j0 = 0; j0 < nr; j0 += 2 * kRows) {
-            load(f1, j0 + kRows, 1);
-            forward(f0, j0);
-            load(f0, j0 + 2 * kRows, 1);
-            forward(f1, j0 + kRows);
+                if (j0 + u < nr) {
+                    yq[(j0 + u) * ldk] = v[u];
+                    cr[(j0 + u) * nz + q] = up[u];
+                }
         }
         float y = dp;
-        auto backward = [&](const float2 (&f)[kRows], int j0) {
-            float v[kRows];
+        for (int j0 = nr - 2; j0 >= 0; j0 -= kRows) {
+            float v[kRows], c[kRows];
 #pragma unroll
-            for (int u = 0; u < kRows; ++u) v[u] = (j0 - u >= 0) ? yq[(j0 - u) * ldk] : 0.f;
+            for (int u = 0; u < kRows; ++u) {
+                const int j = (j0 - u >= 0) ? j0 - u : 0;
+                v[u] = yq[j * ldk];
+                c[u] = cr[j * nz + q];
+            }
 #pragma unroll
             for (int u = 0; u < kRows; ++u) {
                 if (j0 - u < 0) break;
-                y = v[u] - f[u].y * y;
+                y = v[u] - c[u] * y;
                 v[u] = y;
             }
 #pragma unroll
             for (int u = 0; u < kRows; ++u)
                 if (j0 - u >= 0) yq[(j0 - u) * ldk] = v[u];
-        };
-        load(f0, nr - 2, -1);
-        for (int j0 = nr - 2; j0 >= 0; j0 -= 2 * kRows) {
-            load(f1, j0 - kRows, -1);
-            backward(f0, j0);
-            load(f0, j0 - 2 * kRows, -1);
-            backward(f1, j0 - kRows);
         }
     }
+    __syncthreads();
+    load_matrix(Ms, a.Et, nzp, a.lda);  // the ratios have no reader left
     __syncthreads();
     tc_transform(Ms, a.lda, Xt, ldk, nzp, a.nrp, a.cpb);  // 4. delta = E^T y
     double sd = 0.0, sp = 0.0;                              // 5. phi += delta
@@ -317,24 +316,6 @@ __global__ void __launch_bounds__(kDThreads, 2) k_defect_direct(DirectArgs a) {
         a.norms[2 * blk + threadIdx.x] = wgt * t;
     }
     pdl_trigger();
-}
-
-// Thomas factors of (A_r(s) + gamma lambda_q) for every slot s and mode q,
-// in FP64, stored as float (1/m_j, c'_j) at [s][j][q]: one thread per (s, q).
-__global__ void k_direct_factors(const double *__restrict__ brb, const double *__restrict__ alphar,
-                                 const double *__restrict__ betar, const double *__restrict__ lam, float2 *F, int N,
-                                 int numr, int nr, int nz, double gamma) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= N * nz) return;
-    const int s = t / nz, q = t % nz;
-    const double shift = gamma * lam[q];
-    double cp = 0.0;
-    for (int j = 0; j < nr; ++j) {
-        const double lo = (j > 0) ? betar[j + 1] : 0.0;
-        const double m = brb[(long long)s * numr + j + 1] + shift - lo * cp;
-        cp = alphar[j + 1] / m;
-        F[((long long)s * nr + j) * nz + q] = make_float2((float)(1.0 / m), (float)cp);
-    }
 }
 
 }  // namespace
@@ -369,26 +350,13 @@ int direct_configure(bph_ctx *c) {
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_defect_direct, kDThreads, smem);
     if (e != cudaSuccess) return cuda_fail(e, "direct solve set-up");
     {
-        // radial factors for every (slot, mode), from the eigenvalues in FP64
-        std::vector<double> hl64((size_t)c->nz);
-        for (int q = 0; q < c->nz; ++q) hl64[q] = (double)lam[q];
-        double *d_l64 = nullptr;
-        const size_t nf = (size_t)c->N * c->nr * c->nz;
-        e = cudaMalloc((void **)&c->d_dirF, sizeof(float2) * nf);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&d_l64, sizeof(double) * (size_t)c->nz);
-        if (e == cudaSuccess) e = cudaMemcpy(d_l64, hl64.data(), sizeof(double) * (size_t)c->nz, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) {
-            const int n = c->N * c->nz;
-            k_direct_factors<<<(n + 127) / 128, 128, 0, c->stream>>>(c->d_brb, c->d_alphar, c->d_betar, d_l64,
-                                                                      reinterpret_cast<float2 *>(c->d_dirF), c->N,
-                                                                      c->g.numr, c->nr, c->nz, c->gamma);
-            ++c->launches;
-            e = cudaGetLastError();
-        }
-        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-        if (d_l64) cudaFree(d_l64);
-        if (e != cudaSuccess) return cuda_fail(e, "direct solve factors");
-        c->bytes += sizeof(float2) * nf;
+        // the shifts gamma lambda_q of the radial systems, in FP64
+        std::vector<double> hs((size_t)c->nz);
+        for (int q = 0; q < c->nz; ++q) hs[q] = (double)((long double)c->gamma * lam[q]);
+        e = cudaMalloc((void **)&c->d_dirS, sizeof(double) * (size_t)c->nz);
+        if (e == cudaSuccess) e = cudaMemcpy(c->d_dirS, hs.data(), sizeof(double) * (size_t)c->nz, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_fail(e, "direct solve shifts");
+        c->bytes += sizeof(double) * (size_t)c->nz;
     }
     c->mixed_smem_kind[BPH_MIXED_DIRECT] = (int)smem;
     c->mixed_per_sm_kind[BPH_MIXED_DIRECT] = per_sm;
@@ -397,7 +365,7 @@ int direct_configure(bph_ctx *c) {
 
 cudaError_t launch_defect_direct(bph_ctx *c, double *P, const double *R, int nrows, const int *inst_map,
                                  double *norms) {
-    if (!c->mixed_smem_kind[BPH_MIXED_DIRECT] || !c->d_dir32 || !c->d_dirF || !norms) return cudaErrorNotSupported;
+    if (!c->mixed_smem_kind[BPH_MIXED_DIRECT] || !c->d_dir32 || !c->d_dirS || !norms) return cudaErrorNotSupported;
     const direct::Shape d = direct::shape(c->nr, c->nz);
     const size_t ne = (size_t)d.nzp * d.lda;
     DirectArgs a;
@@ -405,7 +373,7 @@ cudaError_t launch_defect_direct(bph_ctx *c, double *P, const double *R, int nro
     a.R = R;
     a.E = c->d_dir32;
     a.Et = c->d_dir32 + ne;
-    a.F = reinterpret_cast<const float2 *>(c->d_dirF);
+    a.sig = c->d_dirS;
     a.brb = c->d_brb;
     a.alphar = c->d_alphar;
     a.betar = c->d_betar;
@@ -422,6 +390,10 @@ cudaError_t launch_defect_direct(bph_ctx *c, double *P, const double *R, int nro
     a.ldk = d.ldk;
     a.lda = d.lda;
     a.cpb = d.cpb;
+    a.off_bd = (int)d.off_bd;
+    a.off_ms = (int)d.off_ms;
+    a.off_lo = (int)d.off_lo;
+    a.off_up = (int)d.off_up;
     a.isym = c->g.isym;
     a.gamma = c->gamma;
     c->launches += 1;

@@ -38,14 +38,17 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kTilesPerWarp = 3;                   // 32 x 16 warp tiles per warp and transform block
 constexpr int kBlockTiles = kTilesPerWarp * kWarps;  // 24: a 96 x 128 slot in one block
 
-// Shared-memory shape of a slot of nr x nz interior zones: X^T [nrp][ldk]
-// (row j = column j of the [k][j] slot matrix), the transform [nzp][lda],
-// the radial sub-diagonal [nr].  Both strides are 4 modulo the 32 banks.
+// Shared-memory shape of a slot of nr x nz interior zones, in floats from
+// the start: X^T [nrp][ldk] (row j = column j of the [k][j] slot matrix);
+// the radial diagonal of the slot [nr] (FP64, at off_bd); the transform
+// [nzp][lda], which holds the Thomas ratios c' [nr][nz] between the two
+// transforms (at off_ms); the radial sub- and super-diagonals [nr] (float,
+// at off_lo and off_up).  Both strides are 4 modulo the 32 banks.
 // cpb = column pairs (16 columns) per transform block; 0 when one block
 // row of 32 modes already needs more warp tiles than the CTA holds.
 struct Shape {
     int nrp, nzp, ldk, lda, cpb;
-    size_t floats;
+    size_t off_bd, off_ms, off_lo, off_up, floats;
 };
 BPH_DIRECT_HD Shape shape(int nr, int nz) {
     Shape d;
@@ -55,7 +58,12 @@ BPH_DIRECT_HD Shape shape(int nr, int nz) {
     d.lda = d.nzp + 4;
     const int rp = d.nzp / 32, cp = d.nrp / 16;
     d.cpb = (rp > kBlockTiles) ? 0 : ((cp < kBlockTiles / rp) ? cp : kBlockTiles / rp);
-    d.floats = (size_t)d.nrp * d.ldk + (size_t)d.nzp * d.lda + (size_t)nr;
+    const size_t ms = (size_t)d.nzp * d.lda, cr = (size_t)nr * nz;
+    d.off_bd = (size_t)d.nrp * d.ldk;                     // a multiple of 64 floats
+    d.off_ms = d.off_bd + 2 * (((size_t)nr + 1) / 2 * 2);  // 16-byte aligned for the vector copies
+    d.off_lo = d.off_ms + ((ms > cr ? ms : cr) + 3) / 4 * 4;
+    d.off_up = d.off_lo + (size_t)nr;
+    d.floats = d.off_up + (size_t)nr;
     return d;
 }
 

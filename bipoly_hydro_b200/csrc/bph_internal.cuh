@@ -163,8 +163,8 @@ struct bph_ctx {
     int mixed_smem_kind[6] = {0, 0, 0, 0, 0, 0};    // per kind: dynamic shared bytes (0: does not fit)
     int mixed_per_sm_kind[6] = {0, 0, 0, 0, 0, 0};  // per kind: resident CTAs per SM
     float mixed_tuned_us[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // per kind: setup-time measurement (0: not timed)
-    float *d_dir32 = nullptr;  // direct defect solve: E, E^T (padded), vertical eigenvalues (bph_direct.cu)
-    float *d_dirF = nullptr;   // its radial Thomas factors (1/m, c') per (slot, height, mode), float pairs
+    float *d_dir32 = nullptr;  // direct defect solve: E, E^T, zero-padded [nzp][lda] (bph_direct.cu)
+    double *d_dirS = nullptr;  // its radial shifts gamma lambda_q per vertical mode (FP64)
     // set-up autotuning (autotune_setup): timings of the candidates, us (0: not timed)
     float tuned_contract_us[2] = {0.f, 0.f};  // full tables, compact tables
     float tuned_fft_us[2] = {0.f, 0.f};       // forward + inverse FFT: regular tiles, dense tiles

@@ -249,6 +249,14 @@ int main() {
     const Shape p = shape(128, 96);
     CHECK(p.cpb == 8 && p.nzp == 96 && p.nrp == 128, "production shape cpb %d", p.cpb);
     CHECK(2 * (p.floats * sizeof(float) + 128 + 1024) <= 228u * 1024u, "two CTAs per SM: %zu bytes", p.floats * 4);
+    for (const auto &s : shapes) {  // the regions: aligned, and the Thomas ratios fit the transform's region
+        const Shape d = shape(s[0], s[1]);
+        CHECK(d.off_bd % 2 == 0 && d.off_ms % 4 == 0, "nr %d nz %d: region alignment", s[0], s[1]);
+        CHECK(d.off_lo - d.off_ms >= (size_t)d.nzp * d.lda && d.off_lo - d.off_ms >= (size_t)s[0] * s[1],
+              "nr %d nz %d: transform region", s[0], s[1]);
+        CHECK(d.off_ms - d.off_bd >= 2 * (size_t)s[0] && d.floats - d.off_up == (size_t)s[0], "nr %d nz %d: coefficients",
+              s[0], s[1]);
+    }
     CHECK(shape(30, 800).cpb == 0, "a slot of 800 modes is not offered");
     if (failures) {
         std::printf("%d failures\n", failures);

@@ -79,4 +79,4 @@ def test_library_selects_devices_only_through_the_scope():
 def test_direct_kernel_index_arithmetic(tmp_path):
     out = _run(tmp_path, "direct_tiles_check")
     assert "all checks passed" in out
-    assert "nr 128 nz  96: cpb 8, 90112 bytes" in out
+    assert "nr 128 nz  96: cpb 8, 102400 bytes" in out
