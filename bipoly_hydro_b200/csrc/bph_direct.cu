@@ -19,9 +19,10 @@
 // ([j][k], FP32, transformed in place), the transform matrix (E, then E^T),
 // the radial coefficients of the slot and the Thomas ratios.
 // The transforms run on the tensor cores (TF32 mma.sync, split in hi and
-// lo parts for FP32 accuracy), the tridiagonals one thread per mode
-// (Thomas in FP32 with factors formed on the way: the radial operator is
-// diagonally dominant and every shift gamma lambda_q is positive).  Each
+// lo parts for FP32 accuracy), the tridiagonals two threads per mode
+// (twisted factorization in FP32 with factors formed on the way: the radial
+// operator is diagonally dominant and every shift gamma lambda_q is
+// positive).  Each
 // cycle shrinks the error by about the FP32 forward error of the solve, so
 // a converged solve takes three cycles instead of four of ten ADI steps.
 #include <algorithm>
@@ -82,7 +83,7 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
 //   b0 (k = t, n = g), b1 (k = t + 4, n = g);
 //   d0 (g, 2t), d1 (g, 2t + 1), d2 (g + 8, 2t), d3 (g + 8, 2t + 1).
 constexpr int kWarpsD = direct::kWarps;
-constexpr int kRows = 8;  // rows (radii) whose loads a thread issues together in the residual and Thomas loops
+constexpr int kRows = 8;  // rows (radii) whose loads a thread issues together in the residual and radial loops
 constexpr int kTilesPerWarp = direct::kTilesPerWarp;
 
 __device__ __forceinline__ void tc_transform(const float *A, int lda, float *Xt, int ldk, int nzp, int nrp, int cpb) {
@@ -143,11 +144,17 @@ __device__ __forceinline__ void tc_transform(const float *A, int lda, float *Xt,
     }
 }
 
-// The nzp x lda matrix M (global, padded rows) into shared memory.
+// The nzp x lda matrix M (global, padded rows) into shared memory: every
+// 16-byte copy issued at once (cp.async, through L2), completed by
+// wait_copies() before the barrier that precedes the first reader.
 __device__ __forceinline__ void load_matrix(float *dst, const float *__restrict__ M, int nzp, int lda) {
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(dst);
     for (int e = threadIdx.x; e < nzp * lda / 4; e += kDThreads)
-        reinterpret_cast<float4 *>(dst)[e] = __ldg(reinterpret_cast<const float4 *>(M) + e);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(base + 16u * (uint32_t)e), "l"(M + 4 * e)
+                     : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
 }
+__device__ __forceinline__ void wait_copies() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // One refinement cycle of a slot: one CTA per (block row, slot), two per SM.
 //  1. r = R - A phi in FP64, rounded into X^T.  A warp takes 32 columns and
@@ -155,7 +162,7 @@ __device__ __forceinline__ void load_matrix(float *dst, const float *__restrict_
 //     in registers (east and west neighbours by shuffle), so every potential
 //     value is read once; the Dirichlet columns enter through the stencil.
 //  2. X <- E X.  3. (A_r + gamma lambda_q) y_q = (E r)_q for every mode q:
-//     Thomas sweeps, one thread per mode, from the slot's radial
+//     twisted factorization, two threads per mode, from the slot's radial
 //     coefficients in shared memory.  4. X <- E^T X.
 //  5. phi += delta in FP64, with the slot's |delta|^2 and |phi|^2.
 __global__ void __launch_bounds__(kDThreads, 2) k_defect_direct(DirectArgs a) {
@@ -168,12 +175,12 @@ __global__ void __launch_bounds__(kDThreads, 2) k_defect_direct(DirectArgs a) {
     float *cl = dsm + a.off_lo, *cu = dsm + a.off_up;             // radial coefficients of j - 1, j + 1
     const int s = blockIdx.x % a.N, row = blockIdx.x / a.N;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    load_matrix(Ms, a.E, nzp, a.lda);
     for (int j = threadIdx.x; j < nr; j += kDThreads) {
         bd[j] = a.brb[(long long)s * numr + j + 1];
         cl[j] = (float)a.betar[j + 1];
         cu[j] = (float)a.alphar[j + 1];
     }
-    load_matrix(Ms, a.E, nzp, a.lda);
     for (int e = threadIdx.x; e < a.nrp * nzp; e += kDThreads) {  // padding: columns j >= nr, rows k >= nz
         const int j = e / nzp, k = e - j * nzp;
         if (j >= nr || k >= nz) Xt[j * ldk + k] = 0.f;
@@ -226,66 +233,41 @@ __global__ void __launch_bounds__(kDThreads, 2) k_defect_direct(DirectArgs a) {
             }
         }
     }
+    wait_copies();  // E, issued before the residual
     __syncthreads();
     tc_transform(Ms, a.lda, Xt, ldk, nzp, a.nrp, a.cpb);  // 2. X <- E X
-    // 3. (A_r + gamma lambda_q) y_q = (E r)_q for every mode q, one thread per mode:
-    //    Thomas sweeps with the factors formed on the way down (m_j = b_j + gamma
-    //    lambda_q - beta_j c'_{j-1}, c'_j = alpha_j / m_j; the ratios kept in the
-    //    transform's region for the way up).  A batch of kRows radii reads its
-    //    values and coefficients first, then runs the recurrence.
+    // 3. (A_r + gamma lambda_q) y_q = (E r)_q for every mode q: the twisted
+    //    factorization, two threads per mode (rows 0 .. nr/2 - 1 downwards,
+    //    the rest upwards), factors formed on the way from the slot's radial
+    //    coefficients, the ratios kept in the transform's region.
     float *cr = Ms;  // [nr][nz]; E has no reader left
-    for (int q = threadIdx.x; q < nz; q += kDThreads) {
-        float *yq = Xt + q;
-        const double sq = a.sig[q];
-        float cp = 0.f, dp = 0.f;
-        for (int j0 = 0; j0 < nr; j0 += kRows) {
-            float v[kRows], lo[kRows], up[kRows], dg[kRows];
-#pragma unroll
-            for (int u = 0; u < kRows; ++u) {
-                const int j = (j0 + u < nr) ? j0 + u : nr - 1;
-                v[u] = yq[j * ldk];
-                lo[u] = (j > 0) ? cl[j] : 0.f;
-                up[u] = cu[j];
-                dg[u] = (float)(bd[j] + sq);
-            }
-#pragma unroll
-            for (int u = 0; u < kRows; ++u) {
-                if (j0 + u >= nr) break;  // the last values carry into the way up
-                const float rm = __frcp_rn(dg[u] - lo[u] * cp);
-                dp = (v[u] - lo[u] * dp) * rm;
-                cp = up[u] * rm;
-                v[u] = dp;
-                up[u] = cp;
-            }
-#pragma unroll
-            for (int u = 0; u < kRows; ++u)
-                if (j0 + u < nr) {
-                    yq[(j0 + u) * ldk] = v[u];
-                    cr[(j0 + u) * nz + q] = up[u];
-                }
-        }
-        float y = dp;
-        for (int j0 = nr - 2; j0 >= 0; j0 -= kRows) {
-            float v[kRows], c[kRows];
-#pragma unroll
-            for (int u = 0; u < kRows; ++u) {
-                const int j = (j0 - u >= 0) ? j0 - u : 0;
-                v[u] = yq[j * ldk];
-                c[u] = cr[j * nz + q];
-            }
-#pragma unroll
-            for (int u = 0; u < kRows; ++u) {
-                if (j0 - u < 0) break;
-                y = v[u] - c[u] * y;
-                v[u] = y;
-            }
-#pragma unroll
-            for (int u = 0; u < kRows; ++u)
-                if (j0 - u >= 0) yq[(j0 - u) * ldk] = v[u];
-        }
+    direct::Radial tr;
+    tr.b = bd;
+    tr.lo = cl;
+    tr.up = cu;
+    tr.n = nr;
+    for (int t = threadIdx.x; t < 2 * nz; t += kDThreads) {
+        const int q = t % nz;
+        tr.sigma = a.sig[q];
+        direct::twisted_eliminate<kRows>(tr, t / nz, Xt + q, ldk, cr + q, nz);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 2 * nz; t += kDThreads) {
+        const int q = t % nz, side = t / nz;
+        float x0, x1;
+        direct::twisted_meet(tr, Xt + q, ldk, cr + q, nz, x0, x1);
+        direct::twisted_substitute<kRows>(tr, side, side ? x1 : x0, Xt + q, ldk, cr + q, nz);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < nz; q += kDThreads) {  // the meeting rows, once both sides have read them
+        float x0, x1;
+        direct::twisted_meet(tr, Xt + q, ldk, cr + q, nz, x0, x1);
+        if (nr / 2 > 0) Xt[(nr / 2 - 1) * ldk + q] = x0;
+        Xt[(nr / 2) * ldk + q] = x1;
     }
     __syncthreads();
     load_matrix(Ms, a.Et, nzp, a.lda);  // the ratios have no reader left
+    wait_copies();
     __syncthreads();
     tc_transform(Ms, a.lda, Xt, ldk, nzp, a.nrp, a.cpb);  // 4. delta = E^T y
     double sd = 0.0, sp = 0.0;                              // 5. phi += delta

@@ -26,8 +26,10 @@
 
 #if defined(__CUDACC__)
 #define BPH_DIRECT_HD __host__ __device__ __forceinline__
+#define BPH_DIRECT_UNROLL _Pragma("unroll")
 #else
 #define BPH_DIRECT_HD inline
+#define BPH_DIRECT_UNROLL
 #endif
 
 namespace bph {
@@ -130,6 +132,110 @@ inline void apply_vertical(int nz, int isym, const long double *x, long double *
         const long double up = (k + 1 < nz) ? x[k + 1] : 0.0L;
         const long double diag = (k == 0 && isym != 1) ? 1.0L : 2.0L;
         y[k] = diag * x[k] - dn - up;
+    }
+}
+
+// The radial tridiagonal of one vertical mode q of a slot,
+//   lo_j x_{j-1} + (b_j + sigma) x_j + up_j x_{j+1} = v_j,  j = 0 .. n-1
+// (b_j FP64, lo_j = up_j = 0 outside the rows: the boundary values are in
+// the residual), solved in FP32 by the twisted factorization: side 0
+// eliminates rows 0 .. p-1 downwards (x_j + c_j x_{j+1} = g_j), side 1 rows
+// n-1 .. p upwards (x_j + e_j x_{j-1} = h_j), p = n / 2; the two meet in the
+// 2 x 2 system of rows p-1 and p and substitute back outwards.  Each chain
+// is half the radial length.  The values live at y[j * ys] (in place), the
+// ratios c_j / e_j at c[j * cs].  Loads of a batch of R rows are issued
+// before its recurrence.
+struct Radial {
+    const double *b;       // [n] diagonal without the shift
+    const float *lo, *up;  // [n] sub- and super-diagonal
+    double sigma;          // shift of the mode
+    int n;
+};
+
+BPH_DIRECT_HD float rcp32(float x) {
+#if defined(__CUDA_ARCH__)
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+#else
+    return 1.0f / x;
+#endif
+}
+
+// Side 0 (rows 0 .. p-1, downwards) or side 1 (rows n-1 .. p, upwards).
+template <int R>
+BPH_DIRECT_HD void twisted_eliminate(const Radial &t, int side, float *y, int ys, float *c, int cs) {
+    const int p = t.n / 2;
+    const int first = side ? t.n - 1 : 0, count = side ? t.n - p : p, dir = side ? -1 : 1;
+    const float *in = side ? t.up : t.lo;   // coupling to the row eliminated before
+    const float *out = side ? t.lo : t.up;  // coupling to the row eliminated next
+    float ratio = 0.f, val = 0.f;
+    for (int i0 = 0; i0 < count; i0 += R) {
+        float v[R], a[R], o[R], d[R];
+BPH_DIRECT_UNROLL
+        for (int u = 0; u < R; ++u) {
+            const int j = first + dir * ((i0 + u < count) ? i0 + u : count - 1);
+            v[u] = y[j * ys];
+            a[u] = (i0 + u > 0) ? in[j] : 0.f;
+            o[u] = out[j];
+            d[u] = (float)(t.b[j] + t.sigma);
+        }
+BPH_DIRECT_UNROLL
+        for (int u = 0; u < R; ++u) {
+            if (i0 + u >= count) break;
+            const float r = rcp32(d[u] - a[u] * ratio);
+            val = (v[u] - a[u] * val) * r;
+            ratio = o[u] * r;
+            v[u] = val;
+            o[u] = ratio;
+        }
+BPH_DIRECT_UNROLL
+        for (int u = 0; u < R; ++u)
+            if (i0 + u < count) {
+                const int j = first + dir * (i0 + u);
+                y[j * ys] = v[u];
+                c[j * cs] = o[u];
+            }
+    }
+}
+
+// The meeting rows p-1 and p after both eliminations: x_{p-1} (side 0) and
+// x_p (side 1).  With p = 0 (n = 1) side 1 alone holds the solution.
+BPH_DIRECT_HD void twisted_meet(const Radial &t, const float *y, int ys, const float *c, int cs, float &x0, float &x1) {
+    const int p = t.n / 2;
+    if (p == 0) {
+        x0 = 0.f;
+        x1 = y[0];
+        return;
+    }
+    const float g = y[(p - 1) * ys], cg = c[(p - 1) * cs], h = y[p * ys], eh = c[p * cs];
+    x0 = (g - cg * h) / (1.f - cg * eh);
+    x1 = h - eh * x0;
+}
+
+// Back substitution of one side from its meeting value, rows p-2 .. 0
+// (side 0) or p+1 .. n-1 (side 1); the meeting rows are written apart.
+template <int R>
+BPH_DIRECT_HD void twisted_substitute(const Radial &t, int side, float x, float *y, int ys, const float *c, int cs) {
+    const int p = t.n / 2;
+    const int first = side ? p + 1 : p - 2, count = side ? t.n - p - 1 : p - 1, dir = side ? 1 : -1;
+    for (int i0 = 0; i0 < count; i0 += R) {
+        float v[R], r[R];
+BPH_DIRECT_UNROLL
+        for (int u = 0; u < R; ++u) {
+            const int j = first + dir * ((i0 + u < count) ? i0 + u : count - 1);
+            v[u] = y[j * ys];
+            r[u] = c[j * cs];
+        }
+BPH_DIRECT_UNROLL
+        for (int u = 0; u < R; ++u) {
+            if (i0 + u >= count) break;
+            x = v[u] - r[u] * x;
+            v[u] = x;
+        }
+BPH_DIRECT_UNROLL
+        for (int u = 0; u < R; ++u)
+            if (i0 + u < count) y[(first + dir * (i0 + u)) * ys] = v[u];
     }
 }
 

@@ -8,7 +8,10 @@
 //    every access inside the shared-memory arrays;
 //  * the residual sweep (a warp per 32 columns and band of rows, neighbours
 //    by shuffle) gives the per-zone FP64 residual bit for bit and reads only
-//    inside the slot arrays.
+//    inside the slot arrays;
+//  * the twisted factorization of the radial systems (two sides, meeting
+//    rows, back substitution) solves them to FP32 accuracy for odd, even
+//    and single-row lengths.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -238,6 +241,55 @@ static void check_residual(int nr, int nz, int isym, std::mt19937 &rng) {
         CHECK(got[e] == ref[e], "nr %d nz %d isym %d: zone %zu %.17g vs %.17g", nr, nz, isym, e, got[e], ref[e]);
 }
 
+// The twisted factorization of the kernel (both sides' elimination, the
+// barrier, meeting, substitution, meeting rows) against an FP64 Thomas
+// solve of the same diagonally dominant system; strided storage as in
+// shared memory.
+static void check_twisted(int n, std::mt19937 &rng) {
+    std::uniform_real_distribution<double> u(-1.0, 1.0);
+    const int ys = 5, cs = 3;
+    std::vector<double> b(n);
+    std::vector<float> lo(n), up(n), y((size_t)n * ys, NAN), c((size_t)n * cs, NAN);
+    std::vector<double> v(n);
+    for (int j = 0; j < n; ++j) {
+        b[j] = 4.0 + u(rng);
+        lo[j] = (float)u(rng);
+        up[j] = (float)u(rng);
+        v[j] = u(rng);
+        y[(size_t)j * ys] = (float)v[j];
+    }
+    const double sigma = 0.37;
+    Radial t;
+    t.b = b.data();
+    t.lo = lo.data();
+    t.up = up.data();
+    t.sigma = sigma;
+    t.n = n;
+    for (int side = 0; side < 2; ++side) twisted_eliminate<8>(t, side, y.data(), ys, c.data(), cs);
+    float x0, x1;
+    for (int side = 0; side < 2; ++side) {
+        twisted_meet(t, y.data(), ys, c.data(), cs, x0, x1);
+        twisted_substitute<8>(t, side, side ? x1 : x0, y.data(), ys, c.data(), cs);
+    }
+    twisted_meet(t, y.data(), ys, c.data(), cs, x0, x1);
+    if (n / 2 > 0) y[(size_t)(n / 2 - 1) * ys] = x0;
+    y[(size_t)(n / 2) * ys] = x1;
+    // FP64 Thomas with the boundary couplings (lo_0, up_{n-1}) left out
+    std::vector<double> cp(n), dp(n), x(n);
+    for (int j = 0; j < n; ++j) {
+        const double l = (j > 0) ? lo[j] : 0.0, m = b[j] + sigma - l * (j > 0 ? cp[j - 1] : 0.0);
+        cp[j] = (j + 1 < n) ? up[j] / m : 0.0;
+        dp[j] = (v[j] - l * (j > 0 ? dp[j - 1] : 0.0)) / m;
+    }
+    for (int j = n - 1; j >= 0; --j) x[j] = dp[j] - ((j + 1 < n) ? cp[j] * x[j + 1] : 0.0);
+    double err = 0.0, nx = 0.0;
+    for (int j = 0; j < n; ++j) {
+        err = std::fmax(err, std::fabs((double)y[(size_t)j * ys] - x[j]));
+        nx = std::fmax(nx, std::fabs(x[j]));
+    }
+    CHECK(err <= 1e-5 * nx, "twisted solve n %d: error %g of %g", n, err, nx);
+}
+
 int main() {
     check_fragments();
     std::mt19937 rng(7);
@@ -246,6 +298,7 @@ int main() {
         check_transform(s[0], s[1], rng);
         for (int isym = 1; isym <= 3; ++isym) check_residual(s[0], s[1], isym, rng);
     }
+    for (int n : {1, 2, 3, 4, 8, 9, 17, 37, 128, 250}) check_twisted(n, rng);
     const Shape p = shape(128, 96);
     CHECK(p.cpb == 8 && p.nzp == 96 && p.nrp == 128, "production shape cpb %d", p.cpb);
     CHECK(2 * (p.floats * sizeof(float) + 128 + 1024) <= 228u * 1024u, "two CTAs per SM: %zu bytes", p.floats * 4);

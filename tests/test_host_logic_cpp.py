@@ -20,8 +20,9 @@
   diagonalise it, the basis of the direct defect solve; and the solve
   kernel's index arithmetic, emulated lane by lane: the fragment offsets
   follow the m16n8k8 lane layout, the in-place transform over the warp
-  tiles equals the dense product with every output written once, and the
-  residual sweep equals the per-zone FP64 residual bit for bit.
+  tiles equals the dense product with every output written once, the
+  residual sweep equals the per-zone FP64 residual bit for bit, and the
+  twisted factorization of the radial systems matches an FP64 Thomas solve.
 """
 import os
 import re
