@@ -270,11 +270,6 @@ constexpr int kHeightDoubles = 64 + 32;     // a height: 64 tile elements, 16 (c
 constexpr int kStageDoubles = kStageH * kHeightDoubles;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void cpa16_ef(void *dst, const void *src, unsigned long long pol) {
-    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src),
-                 "l"(pol)
-                 : "memory");
-}
 __device__ __forceinline__ void cpa16(void *dst, const void *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }

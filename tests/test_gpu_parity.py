@@ -447,7 +447,12 @@ def test_converged_loop_on_device_equals_host_loop(bph, monkeypatch):
         assert abs(a[k + 1].residual - b[k + 1].residual) <= 1e-12 * max(1.0, b[k + 1].residual)
 
 
-@pytest.mark.parametrize("grid", SMALL_GRIDS, ids=lambda g: "x".join(map(str, g[:3])) + f"-isym{g[4]}")
+# 140 vertical modes: more (mode, side) pairs of the radial solves than threads in a CTA
+TALL_DIRECT_GRID = (24, 142, 16, 1.0 / 20.0, 1, 6)
+
+
+@pytest.mark.parametrize("grid", SMALL_GRIDS + [TALL_DIRECT_GRID],
+                         ids=lambda g: "x".join(map(str, g[:3])) + f"-isym{g[4]}")
 def test_direct_refinement_converges_to_oracle(oracle_mod, bph, grid):
     """The mixed form with the direct FP32 defect solve (eigen-transform in z,
     radial tridiagonals) converges to the oracle's converged FP64 potential
