@@ -17,14 +17,14 @@
 // forms the residual of its slot, solves, and adds delta to phi with the
 // slot's norms, everything between in shared memory: the residual as X^T
 // ([j][k], FP32, transformed in place), the transform matrix (E, then E^T),
-// the radial coefficients of the slot and the Thomas ratios.
+// the radial coefficients of the slot and the elimination ratios.
 // The transforms run on the tensor cores (TF32 mma.sync, split in hi and
 // lo parts for FP32 accuracy), the tridiagonals two threads per mode
 // (twisted factorization in FP32 with factors formed on the way: the radial
 // operator is diagonally dominant and every shift gamma lambda_q is
-// positive).  Each
-// cycle shrinks the error by about the FP32 forward error of the solve, so
-// a converged solve takes three cycles instead of four of ten ADI steps.
+// positive).  Each cycle shrinks the error by about the FP32 forward error
+// of the solve, so a converged solve takes three cycles instead of four of
+// ten ADI steps.
 #include <algorithm>
 #include <cstdlib>
 #include <vector>
