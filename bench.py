@@ -996,6 +996,12 @@ def run_gpu(args, world, rank, local):
         rmx["inner_solver"] = kind_names.get(tuned, str(tuned))
         batched_conv["mixed"] = rmx
         batched_conv["speedup_mixed_vs_fp64"] = rmx["solves_per_s"] / r64["solves_per_s"]
+        # beside it, the ratio against the plain form: the batched 5-step drop-in of the same
+        # batch size (a converged solve does more work than a 5-step one)
+        if batched and str(nb_) in batched:
+            plain = batched[str(nb_)]["solves_per_s"]
+            batched_conv["vs_plain_form"] = {"plain_solves_per_s": plain,
+                                             "mixed_over_plain": rmx["solves_per_s"] / plain}
         # the mixed form with its fastest FP32 ADI inner solver as well (the precision's share
         # of the speed-up, without the direct solve)
         if tuned == B.solver.MIXED_DIRECT:
