@@ -400,9 +400,11 @@ long long bph_info(const bph_ctx_t *ctx, int what);
 #define BPH_MIXED_ADI_WARP 4
 /* not an ADI: the defect equation solved directly in FP32 (eigen-transform of
  * the vertical operator, one radial tridiagonal per vertical mode, inverse
- * transform), for slots whose FP32 residual fits in shared memory; each
- * refinement cycle then gains about the FP32 accuracy of the solve instead of
- * one ADI cycle's reduction.  The cycle's nsteps is not used. */
+ * transform), one kernel per cycle, for slots whose FP32 residual and vertical
+ * transform fit in one CTA's shared memory (128 x 96 interiors: 100 KB, two
+ * CTAs per SM); each refinement cycle then gains about the FP32 accuracy of
+ * the solve instead of one ADI cycle's reduction.  The cycle's nsteps is not
+ * used. */
 #define BPH_MIXED_DIRECT 5
 int bph_configure(bph_ctx_t *ctx, int key, int value);
 
